@@ -1,0 +1,200 @@
+/*
+ * sparsesolv_b200.h -- C ABI of the B200 (sm_100a) solve path.
+ *
+ * Every entry point takes plain pointers and sizes. Host pointers carry host
+ * data; the `_dev` variants take device pointers that the caller keeps
+ * resident in HBM. All calls are synchronous on return (the work runs on the
+ * handle's own CUDA stream). A handle is not safe for concurrent use from two
+ * threads (the reference's objects keep mutable work buffers the same way,
+ * include/sparsesolv/preconditioners/ic_preconditioner.hpp:555-563).
+ *
+ * Status: every function returns SSV_OK (0) or an SSV_ERR_* code; the message
+ * of the last failure on the calling thread is ssv_last_error(). The Python
+ * layer maps SSV_ERR_RUNTIME -> RuntimeError (reference std::runtime_error),
+ * SSV_ERR_INVALID_ARG -> ValueError (std::invalid_argument), SSV_ERR_TYPE ->
+ * TypeError (py::type_error).
+ *
+ * Scalars: SSV_F64 = double, SSV_C128 = complex<double> stored as interleaved
+ * (re, im) doubles, exactly the layout of std::complex<double>.
+ */
+#ifndef SPARSESOLV_B200_H
+#define SPARSESOLV_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SSV_VERSION_MAJOR 0
+#define SSV_VERSION_MINOR 1
+#define SSV_VERSION_PATCH 0
+
+enum ssv_status {
+    SSV_OK = 0,
+    SSV_ERR_INVALID_ARG = 1, /* std::invalid_argument in the reference     */
+    SSV_ERR_RUNTIME = 2,     /* std::runtime_error in the reference        */
+    SSV_ERR_CUDA = 3,        /* a CUDA runtime call failed                 */
+    SSV_ERR_NO_DEVICE = 4,   /* no CUDA device: this library has no CPU path */
+    SSV_ERR_TYPE = 5,        /* wrong scalar type for this object          */
+    SSV_ERR_TIMEOUT = 6,     /* a bounded device wait gave up              */
+    SSV_ERR_ALLOC = 7        /* device allocation failed                   */
+};
+
+enum ssv_dtype { SSV_F64 = 0, SSV_C128 = 1 };
+
+/* NormType, include/sparsesolv/core/types.hpp:43-47 */
+enum ssv_norm_type { SSV_NORM_RHS = 0, SSV_NORM_INITIAL_RESIDUAL = 1, SSV_NORM_CUSTOM = 2 };
+
+/* Krylov methods of SparseSolvSolver, include/sparsesolv/ngsolve/sparsesolv_solvers.hpp:112-128 */
+enum ssv_method { SSV_METHOD_ICCG = 0, SSV_METHOD_SGSMRTR = 1, SSV_METHOD_CG = 2, SSV_METHOD_COCR = 3 };
+
+/* Precision of a preconditioner application (new: no reference counterpart).
+ * FP64 is the drop-in; FP32 stores L / auxiliary matrices in float and applies
+ * in float while the outer Krylov recurrence stays in double. */
+enum ssv_precision { SSV_PREC_FP64 = 0, SSV_PREC_FP32 = 1 };
+
+/*
+ * Field-for-field mirror of sparsesolv::SolverConfig
+ * (include/sparsesolv/core/solver_config.hpp:33-159). Booleans are int 0/1.
+ * ssv_config_default() fills the reference defaults.
+ */
+typedef struct ssv_config {
+    double tolerance;                 /* 1e-10 */
+    int32_t max_iterations;           /* 1000  */
+    double abs_tolerance;             /* 1e-12 */
+    int32_t norm_type;                /* SSV_NORM_RHS */
+    double custom_norm;               /* 1.0   */
+    double shift_parameter;           /* 1.05  */
+    int32_t diagonal_scaling;         /* 0     */
+    int32_t auto_shift;               /* 0     */
+    double shift_increment;           /* 0.05  */
+    double max_shift_value;           /* 5.0   */
+    double min_diagonal_threshold;    /* 1e-6  */
+    double zero_diagonal_replacement; /* 1e-10 */
+    int32_t max_shift_trials;         /* 100   */
+    int32_t divergence_check;         /* 0 = None, 1 = StagnationCount */
+    double divergence_threshold;      /* 1000  */
+    int32_t divergence_count;         /* 100   */
+    int32_t save_best_result;         /* 1     */
+    int32_t save_residual_history;    /* 0     */
+    int32_t conjugate;                /* 0     */
+    int32_t use_abmc;                 /* 0     */
+    int32_t abmc_block_size;          /* 4     */
+    int32_t abmc_num_colors;          /* 4     */
+    int32_t abmc_reorder_spmv;        /* 0     */
+    int32_t abmc_use_rcm;             /* 0     */
+    int32_t precision;                /* SSV_PREC_FP64 (new knob) */
+} ssv_config;
+
+/* sparsesolv::SolverResult, include/sparsesolv/core/types.hpp:29-37.
+ * The residual history goes to a caller buffer (ssv_solver_solve). */
+typedef struct ssv_result {
+    int32_t converged;
+    int32_t iterations;
+    double final_residual;
+    int32_t history_len;      /* entries written (<= history_cap)           */
+    int32_t history_total;    /* entries the reference would have produced  */
+    double actual_shift;      /* IC shift after auto-shift (ICCG only)      */
+    double setup_seconds;     /* host wall time of preconditioner setup     */
+    double solve_seconds;     /* host wall time of the Krylov iteration     */
+} ssv_result;
+
+typedef struct ssv_matrix ssv_matrix;   /* device-resident CSR              */
+typedef struct ssv_solver ssv_solver;   /* SparseSolvSolver state           */
+typedef struct ssv_precond ssv_precond; /* IC / AMS / complex-AMS           */
+
+/* ---- library ----------------------------------------------------------- */
+void ssv_version(int* major, int* minor, int* patch);
+const char* ssv_last_error(void);
+/* Number of CUDA devices and the name of device 0 (no allocation). */
+int ssv_device_info(int* count, char* name, int name_cap);
+/* Reference defaults of SolverConfig (solver_config.hpp:39-157). */
+void ssv_config_default(ssv_config* cfg);
+
+/* ---- CSR matrix (replaces SparseMatrixView / SparseMatrixCSR,
+ *      include/sparsesolv/core/sparse_matrix_view.hpp:68-81,
+ *      include/sparsesolv/core/sparse_matrix_csr.hpp:19-30) ---------------- */
+/* Copies the CSR (int32 row_ptr[rows+1], col_idx[nnz], values[nnz] of dtype)
+ * into HBM. Column indices must be sorted within each row. */
+int ssv_matrix_create(int32_t rows, int32_t cols, const int32_t* row_ptr,
+                      const int32_t* col_idx, const void* values, int32_t dtype,
+                      ssv_matrix** out);
+/* Re-uploads the values (same pattern): the reference's "matrix modified in
+ * place, then Update()" semantics (compact_ams.hpp:82-86). */
+int ssv_matrix_update_values(ssv_matrix* A, const void* values);
+int ssv_matrix_destroy(ssv_matrix* A);
+int ssv_matrix_info(const ssv_matrix* A, int32_t* rows, int32_t* cols,
+                    int64_t* nnz, int32_t* dtype);
+/* y = A x (SparseMatrixView::multiply, sparse_matrix_view.hpp:139-147). */
+int ssv_matrix_spmv(ssv_matrix* A, const void* x, void* y);
+int ssv_matrix_spmv_dev(ssv_matrix* A, const void* d_x, void* d_y);
+
+/* ---- SparseSolvSolver (ngsolve/sparsesolv_solvers.hpp:33-239) ---------- */
+/* freedofs: one byte per row (nonzero = free) or NULL for all free. */
+int ssv_solver_create(ssv_matrix* A, const uint8_t* freedofs, ssv_solver** out);
+int ssv_solver_destroy(ssv_solver* s);
+/* SparseSolvSolver::Solve (sparsesolv_solvers.hpp:73-160): x is the initial
+ * guess on entry (free DOFs only) and the solution on return (free DOFs
+ * written, constrained DOFs untouched). method: "ICCG"/"iccg", "SGSMRTR"/
+ * "sgsmrtr", "CG"/"cg", "COCR"/"cocr"; any other string fails with
+ * SSV_ERR_RUNTIME and the reference's message. history may be NULL. */
+int ssv_solver_solve(ssv_solver* s, const char* method, const ssv_config* cfg,
+                     const void* b, void* x, ssv_result* res,
+                     double* history, int32_t history_cap);
+/* Same, with b and x in device memory (inputs resident in HBM). */
+int ssv_solver_solve_dev(ssv_solver* s, const char* method, const ssv_config* cfg,
+                         const void* d_b, void* d_x, ssv_result* res,
+                         double* history, int32_t history_cap);
+
+/* ---- preconditioners ---------------------------------------------------- */
+/* ICPreconditioner factory (sparsesolv_python_export.hpp:176-207) without the
+ * implicit Update(): call ssv_precond_update() to factorise. */
+int ssv_ic_create(ssv_matrix* A, const uint8_t* freedofs, double shift,
+                  ssv_precond** out);
+/* Options of SparseSolvICPreconditioner (sparsesolv_precond.hpp:200-223):
+ * use_abmc, abmc_block_size, abmc_num_colors, diagonal_scaling, shift and the
+ * auto-shift fields are read from cfg; they take effect at the next update. */
+int ssv_ic_set_config(ssv_precond* p, const ssv_config* cfg);
+/* Update(): BuildSparseMatrixView + ICPreconditioner::setup
+ * (sparsesolv_precond.hpp:188-191, ic_preconditioner.hpp:69-201). */
+int ssv_precond_update(ssv_precond* p);
+/* Mult (sparsesolv_precond.hpp:123-136): y = M^{-1} x, constrained DOFs 0. */
+int ssv_precond_apply(ssv_precond* p, const void* x, void* y);
+int ssv_precond_apply_dev(ssv_precond* p, const void* d_x, void* d_y);
+/* Actual IC shift after auto-shift (ICPreconditioner::actual_shift). */
+int ssv_ic_actual_shift(const ssv_precond* p, double* shift);
+int ssv_precond_destroy(ssv_precond* p);
+
+/* ---- COCRSolver with external preconditioner
+ *      (COCRSolverNGS::Mult, ngsolve/sparsesolv_solvers.hpp:273-369) ------- */
+/* x is zeroed on entry (the reference has no initial-guess path). pre may be
+ * NULL (identity). iterations receives COCRSolverNGS::GetIterations(). */
+int ssv_cocr_solve(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs,
+                   int32_t maxiter, double tol, int32_t printrates,
+                   const void* b, void* x, int32_t* iterations);
+int ssv_cocr_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs,
+                       int32_t maxiter, double tol, int32_t printrates,
+                       const void* d_b, void* d_x, int32_t* iterations);
+
+/* ---- host-side set-up logic exposed for parity checks (no device work) --- */
+/* ABMCSchedule::build (include/sparsesolv/core/abmc_ordering.hpp:83-121).
+ * color_offsets needs room for n+1 entries, block_offsets n+1, ordering and
+ * reverse n each. */
+int ssv_abmc_build(int32_t n, const int32_t* row_ptr, const int32_t* col_idx,
+                   int32_t block_size, int32_t target_colors,
+                   int32_t* num_colors, int32_t* num_blocks,
+                   int32_t* color_offsets, int32_t* block_offsets,
+                   int32_t* ordering, int32_t* reverse_ordering);
+/* LevelSchedule::build_from_lower / build_from_upper
+ * (include/sparsesolv/core/level_schedule.hpp:58-135): level_of[i] = level of
+ * row i; returns the level count in num_levels. upper != 0 builds from an
+ * upper-triangular pattern. */
+int ssv_level_schedule(int32_t n, const int32_t* row_ptr, const int32_t* col_idx,
+                       int32_t upper, int32_t* level_of, int32_t* num_levels);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPARSESOLV_B200_H */

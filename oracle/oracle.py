@@ -1,0 +1,191 @@
+"""ctypes front end of the oracle -- TEST INFRASTRUCTURE.
+
+Loads ``oracle/_build/libssv_oracle.so`` (the C restatement, rebuilt with gcc
+when missing) and, where present, ``oracle/_ref/libssv_ref.so`` (the
+reference's own headers). Only tests/, the smoke check and bench.py's CPU
+baseline use this module, as the checker.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(ROOT, "ngsolve-sparsesolv_b200"))
+
+from sparsesolv_ngsolve import _capi  # noqa: E402  (struct layouts only)
+from oracle import build_oracle  # noqa: E402
+
+ssv_config = _capi.ssv_config
+ssv_result = _capi.ssv_result
+default_config = _capi.default_config
+
+P = ctypes.c_void_p
+I32 = ctypes.c_int32
+PI32 = ctypes.POINTER(ctypes.c_int32)
+PU8 = ctypes.POINTER(ctypes.c_uint8)
+PD = ctypes.POINTER(ctypes.c_double)
+PRECOND_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
+
+_libs = {}
+
+
+def _bind(lib, prefix):
+    sig = {
+        "solve": (I32, [I32, PI32, PI32, P, I32, PU8, ctypes.c_char_p, ctypes.POINTER(ssv_config),
+                        P, P, ctypes.POINTER(ssv_result), PD, I32]),
+        "ic_mult": (I32, [I32, PI32, PI32, P, I32, PU8, ctypes.POINTER(ssv_config), P, P, PD]),
+        "abmc_build": (I32, [I32, PI32, PI32, I32, I32, PI32, PI32, PI32, PI32, PI32, PI32]),
+        "level_schedule": (I32, [I32, PI32, PI32, I32, PI32, PI32]),
+        "last_error": (ctypes.c_char_p, []),
+    }
+    if prefix == "orc_":
+        sig["cocr_solve"] = (I32, [I32, PI32, PI32, P, I32, PU8, PRECOND_FN, P, I32,
+                                   ctypes.c_double, P, P, PI32])
+        sig["spmv"] = (I32, [I32, PI32, PI32, P, I32, P, P])
+    else:
+        sig["set_threads"] = (None, [I32])
+        sig["get_threads"] = (I32, [])
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, prefix + name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+def port():
+    """The C restatement (always available: built with gcc on demand)."""
+    if "port" not in _libs:
+        path = build_oracle.build_oracle()
+        _libs["port"] = _bind(ctypes.CDLL(path), "orc_")
+    return _libs["port"]
+
+
+def reference():
+    """The reference's own headers compiled here, or None if not built."""
+    if "ref" not in _libs:
+        path = build_oracle.REF_SO
+        if not os.path.exists(path):
+            path = build_oracle.build_reference()
+        _libs["ref"] = _bind(ctypes.CDLL(path), "ref_") if path and os.path.exists(path) else None
+    return _libs["ref"]
+
+
+def _csr_parts(A):
+    rp = np.ascontiguousarray(A.indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(A.indices, dtype=np.int32)
+    cplx = np.iscomplexobj(A.data)
+    v = np.ascontiguousarray(A.data, dtype=np.complex128 if cplx else np.float64)
+    return rp, ci, v, (1 if cplx else 0)
+
+
+def _p(a, t=PI32):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def solve(A, b, method="ICCG", config=None, freedofs=None, x0=None, which="port",
+          history_cap=100000):
+    """SparseSolvSolver::Solve on the CPU. Returns (x, result, history)."""
+    lib = port() if which == "port" else reference()
+    if lib is None:
+        raise RuntimeError("reference library oracle/_ref/libssv_ref.so is not built")
+    rp, ci, v, dt = _csr_parts(A)
+    n = A.shape[0]
+    vdt = np.complex128 if dt else np.float64
+    bb = np.ascontiguousarray(b, dtype=vdt)
+    x = np.zeros(n, dtype=vdt) if x0 is None else np.array(x0, dtype=vdt, copy=True)
+    cfg = config if config is not None else default_config()
+    fd = None if freedofs is None else np.ascontiguousarray(freedofs, dtype=np.uint8)
+    res = ssv_result()
+    hist = np.zeros(max(history_cap, 1))
+    rc = getattr(lib, ("orc_" if which == "port" else "ref_") + "solve")(
+        n, _p(rp), _p(ci), P(v.ctypes.data), dt, _p(fd, PU8), method.encode(),
+        ctypes.byref(cfg), P(bb.ctypes.data), P(x.ctypes.data), ctypes.byref(res),
+        _p(hist, PD), history_cap)
+    if rc != 0:
+        msg = getattr(lib, ("orc_" if which == "port" else "ref_") + "last_error")().decode()
+        raise RuntimeError(msg)
+    return x, res, hist[: res.history_len].copy()
+
+
+def ic_mult(A, x, config=None, freedofs=None, which="port"):
+    """ICPreconditioner(A) followed by one Mult: returns (y, actual_shift)."""
+    lib = port() if which == "port" else reference()
+    rp, ci, v, dt = _csr_parts(A)
+    n = A.shape[0]
+    vdt = np.complex128 if dt else np.float64
+    xx = np.ascontiguousarray(x, dtype=vdt)
+    y = np.zeros(n, dtype=vdt)
+    cfg = config if config is not None else default_config()
+    fd = None if freedofs is None else np.ascontiguousarray(freedofs, dtype=np.uint8)
+    sh = ctypes.c_double(0.0)
+    rc = getattr(lib, ("orc_" if which == "port" else "ref_") + "ic_mult")(
+        n, _p(rp), _p(ci), P(v.ctypes.data), dt, _p(fd, PU8), ctypes.byref(cfg),
+        P(xx.ctypes.data), P(y.ctypes.data), ctypes.byref(sh))
+    if rc != 0:
+        raise RuntimeError(getattr(lib, ("orc_" if which == "port" else "ref_") + "last_error")().decode())
+    return y, sh.value
+
+
+def abmc(A, block_size=4, num_colors=4, which="port"):
+    """ABMCSchedule::build: returns dict of the schedule arrays."""
+    lib = port() if which == "port" else reference()
+    rp = np.ascontiguousarray(A.indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(A.indices, dtype=np.int32)
+    n = A.shape[0]
+    nc = ctypes.c_int32(0)
+    nb = ctypes.c_int32(0)
+    co = np.zeros(n + 1, np.int32)
+    bo = np.zeros(n + 1, np.int32)
+    od = np.zeros(n, np.int32)
+    rv = np.zeros(n, np.int32)
+    rc = getattr(lib, ("orc_" if which == "port" else "ref_") + "abmc_build")(
+        n, _p(rp), _p(ci), block_size, num_colors, ctypes.byref(nc), ctypes.byref(nb),
+        _p(co), _p(bo), _p(od), _p(rv))
+    if rc != 0:
+        raise RuntimeError("abmc build failed")
+    return {"num_colors": nc.value, "num_blocks": nb.value,
+            "color_offsets": co[: nc.value + 1].copy(), "block_offsets": bo[: nb.value + 1].copy(),
+            "ordering": od, "reverse": rv}
+
+
+def level_schedule(rp, ci, n, upper=False, which="port"):
+    lib = port() if which == "port" else reference()
+    rp = np.ascontiguousarray(rp, dtype=np.int32)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    lev = np.zeros(max(n, 1), np.int32)
+    nl = ctypes.c_int32(0)
+    getattr(lib, ("orc_" if which == "port" else "ref_") + "level_schedule")(
+        n, _p(rp), _p(ci), 1 if upper else 0, _p(lev), ctypes.byref(nl))
+    return lev[:n], nl.value
+
+
+def cocr_solve(A, b, precond=None, freedofs=None, maxiter=500, tol=1e-8):
+    """COCRSolverNGS::Mult on the CPU; precond is a python callable y=f(x)."""
+    lib = port()
+    rp, ci, v, dt = _csr_parts(A)
+    n = A.shape[0]
+    vdt = np.complex128 if dt else np.float64
+    bb = np.ascontiguousarray(b, dtype=vdt)
+    x = np.zeros(n, dtype=vdt)
+    fd = None if freedofs is None else np.ascontiguousarray(freedofs, dtype=np.uint8)
+    it = ctypes.c_int32(0)
+    cb = None
+    if precond is not None:
+        def _cb(ctx, xp, yp):
+            xs = np.ctypeslib.as_array(ctypes.cast(xp, ctypes.POINTER(ctypes.c_double)),
+                                       shape=(n * (2 if dt else 1),)).view(vdt)
+            ys = np.ctypeslib.as_array(ctypes.cast(yp, ctypes.POINTER(ctypes.c_double)),
+                                       shape=(n * (2 if dt else 1),)).view(vdt)
+            ys[:] = precond(xs.copy())
+        cb = PRECOND_FN(_cb)
+    rc = lib.orc_cocr_solve(n, _p(rp), _p(ci), P(v.ctypes.data), dt, _p(fd, PU8),
+                            cb if cb is not None else PRECOND_FN(), None, maxiter, tol,
+                            P(bb.ctypes.data), P(x.ctypes.data), ctypes.byref(it))
+    if rc != 0:
+        raise RuntimeError("oracle cocr failed")
+    return x, it.value
