@@ -98,7 +98,20 @@ typedef struct ssv_result {
     double actual_shift;      /* IC shift after auto-shift (ICCG only)      */
     double setup_seconds;     /* host wall time of preconditioner setup     */
     double solve_seconds;     /* host wall time of the Krylov iteration     */
+    int64_t kernel_launches;  /* device kernels this call launched          */
 } ssv_result;
+
+/* Per-phase timing of one Krylov iteration (measurement hook, no reference
+ * counterpart): each phase is re-launched `reps` times on the library's
+ * stream between CUDA events, after a solve on the same handle. */
+#define SSV_MAX_PHASES 8
+typedef struct ssv_phase_profile {
+    int32_t num_phases;
+    char names[SSV_MAX_PHASES][24];
+    double ms[SSV_MAX_PHASES];        /* mean device time per phase execution */
+    double bytes[SSV_MAX_PHASES];     /* algorithmic bytes per phase execution */
+    int32_t kernels[SSV_MAX_PHASES];  /* kernel launches per phase execution */
+} ssv_phase_profile;
 
 typedef struct ssv_matrix ssv_matrix;   /* device-resident CSR              */
 typedef struct ssv_solver ssv_solver;   /* SparseSolvSolver state           */
@@ -146,6 +159,11 @@ int ssv_solver_solve(ssv_solver* s, const char* method, const ssv_config* cfg,
 int ssv_solver_solve_dev(ssv_solver* s, const char* method, const ssv_config* cfg,
                          const void* d_b, void* d_x, ssv_result* res,
                          double* history, int32_t history_cap);
+
+/* Times each phase of one iteration of `method` on the buffers of the last
+ * ssv_solver_solve[_dev] call of this handle (same method and options). */
+int ssv_solver_profile(ssv_solver* s, const char* method, const ssv_config* cfg, int32_t reps,
+                       ssv_phase_profile* out);
 
 /* ---- preconditioners ---------------------------------------------------- */
 /* ICPreconditioner factory (sparsesolv_python_export.hpp:176-207) without the

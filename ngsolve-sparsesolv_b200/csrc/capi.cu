@@ -1,0 +1,389 @@
+// capi.cu -- the extern "C" boundary (include/sparsesolv_b200.h). Every entry
+// point converts exceptions into a status code plus a thread-local message.
+#include <cstring>
+#include <string>
+
+#include "solver_api.hpp"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        g_last_error.clear();
+        return SSV_OK;
+    } catch (const ssv::Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return SSV_ERR_ALLOC;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return SSV_ERR_RUNTIME;
+    }
+}
+
+void require_device() {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count <= 0)
+        ssv::fail(SSV_ERR_NO_DEVICE,
+                  "sparsesolv_b200: no CUDA device available (this library has no CPU path)");
+}
+
+size_t scalar_bytes(int dtype) { return dtype == SSV_F64 ? sizeof(double) : 2 * sizeof(double); }
+
+void check_mask(const uint8_t* fd, int n, std::vector<uint8_t>& h, ssv::DevBuf<uint8_t>& d, bool& has) {
+    has = fd != nullptr;
+    h.clear();
+    d.release();
+    if (!fd) return;
+    h.assign(fd, fd + n);
+    for (auto& v : h) v = v ? 1 : 0;
+    d.upload(h.data(), h.size(), ssv::stream());
+}
+
+// Staging buffer for host-pointer calls.
+struct Stage {
+    ssv::DevBuf<double> a, b;
+};
+Stage& stage() {
+    static Stage s;
+    return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+void ssv_version(int* major, int* minor, int* patch) {
+    if (major) *major = SSV_VERSION_MAJOR;
+    if (minor) *minor = SSV_VERSION_MINOR;
+    if (patch) *patch = SSV_VERSION_PATCH;
+}
+
+const char* ssv_last_error(void) { return g_last_error.c_str(); }
+
+int ssv_device_info(int* count, char* name, int name_cap) {
+    return guarded([&] {
+        int c = 0;
+        if (cudaGetDeviceCount(&c) != cudaSuccess) c = 0;
+        if (count) *count = c;
+        if (name && name_cap > 0) {
+            name[0] = 0;
+            if (c > 0) {
+                cudaDeviceProp p;
+                SSV_CUDA(cudaGetDeviceProperties(&p, 0));
+                std::strncpy(name, p.name, name_cap - 1);
+                name[name_cap - 1] = 0;
+            }
+        }
+    });
+}
+
+void ssv_config_default(ssv_config* c) {
+    std::memset(c, 0, sizeof(*c));
+    c->tolerance = 1e-10;
+    c->max_iterations = 1000;
+    c->abs_tolerance = 1e-12;
+    c->norm_type = SSV_NORM_RHS;
+    c->custom_norm = 1.0;
+    c->shift_parameter = 1.05;
+    c->shift_increment = 0.05;
+    c->max_shift_value = 5.0;
+    c->min_diagonal_threshold = 1e-6;
+    c->zero_diagonal_replacement = 1e-10;
+    c->max_shift_trials = 100;
+    c->divergence_threshold = 1000.0;
+    c->divergence_count = 100;
+    c->save_best_result = 1;
+    c->abmc_block_size = 4;
+    c->abmc_num_colors = 4;
+    c->precision = SSV_PREC_FP64;
+}
+
+int ssv_matrix_create(int32_t rows, int32_t cols, const int32_t* row_ptr, const int32_t* col_idx,
+                      const void* values, int32_t dtype, ssv_matrix** out) {
+    return guarded([&] {
+        if (!out) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_create: out is NULL");
+        *out = nullptr;
+        if (rows < 0 || cols < 0) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_create: negative size");
+        if (dtype != SSV_F64 && dtype != SSV_C128) ssv::fail(SSV_ERR_TYPE, "ssv_matrix_create: unknown dtype");
+        if (!row_ptr || (!col_idx && row_ptr[rows] > 0) || (!values && row_ptr[rows] > 0))
+            ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_create: NULL array");
+        if (row_ptr[0] != 0) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_create: row_ptr[0] must be 0");
+        const int64_t nnz = row_ptr[rows];
+        for (int i = 0; i < rows; ++i) {
+            if (row_ptr[i + 1] < row_ptr[i]) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_create: row_ptr not monotone");
+            for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
+                if (col_idx[k] < 0 || col_idx[k] >= cols)
+                    ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_create: column index out of range in row " +
+                                                       std::to_string(i));
+                if (k > row_ptr[i] && col_idx[k] <= col_idx[k - 1])
+                    ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_create: columns of row " + std::to_string(i) +
+                                                       " are not sorted and unique");
+            }
+        }
+        require_device();
+        auto* A = new ssv_matrix();
+        try {
+            cudaStream_t s = ssv::stream();
+            A->rows = rows;
+            A->cols = cols;
+            A->nnz = nnz;
+            A->dtype = dtype;
+            A->h_rp.assign(row_ptr, row_ptr + rows + 1);
+            A->h_ci.assign(col_idx, col_idx + nnz);
+            A->rp.upload(A->h_rp.data(), A->h_rp.size(), s);
+            A->ci.upload(A->h_ci.data(), A->h_ci.size(), s);
+            const size_t words = (size_t)nnz * (dtype == SSV_F64 ? 1 : 2);
+            A->val.upload(static_cast<const double*>(values), words, s);
+            A->lanes = ssv::pick_lanes(rows > 0 ? (double)nnz / rows : 1.0);
+            SSV_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            delete A;
+            throw;
+        }
+        *out = A;
+    });
+}
+
+int ssv_matrix_update_values(ssv_matrix* A, const void* values) {
+    return guarded([&] {
+        if (!A || !values) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_update_values: NULL argument");
+        const size_t words = (size_t)A->nnz * (A->dtype == SSV_F64 ? 1 : 2);
+        A->val.upload(static_cast<const double*>(values), words, ssv::stream());
+        SSV_CUDA(cudaStreamSynchronize(ssv::stream()));
+    });
+}
+
+int ssv_matrix_destroy(ssv_matrix* A) {
+    return guarded([&] {
+        if (!A) return;
+        ssv::cocr_forget(A);
+        delete A;
+    });
+}
+
+int ssv_matrix_info(const ssv_matrix* A, int32_t* rows, int32_t* cols, int64_t* nnz, int32_t* dtype) {
+    return guarded([&] {
+        if (!A) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_info: NULL matrix");
+        if (rows) *rows = A->rows;
+        if (cols) *cols = A->cols;
+        if (nnz) *nnz = A->nnz;
+        if (dtype) *dtype = A->dtype;
+    });
+}
+
+int ssv_matrix_spmv_dev(ssv_matrix* A, const void* d_x, void* d_y) {
+    return guarded([&] {
+        if (!A || !d_x || !d_y) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_spmv_dev: NULL argument");
+        ssv::matrix_spmv_dev(A, d_x, d_y);
+    });
+}
+
+int ssv_matrix_spmv(ssv_matrix* A, const void* x, void* y) {
+    return guarded([&] {
+        if (!A || !x || !y) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_spmv: NULL argument");
+        cudaStream_t s = ssv::stream();
+        const size_t bytes_x = (size_t)A->cols * scalar_bytes(A->dtype);
+        const size_t bytes_y = (size_t)A->rows * scalar_bytes(A->dtype);
+        Stage& st = stage();
+        st.a.alloc(bytes_x / sizeof(double) + 1);
+        st.b.alloc(bytes_y / sizeof(double) + 1);
+        SSV_CUDA(cudaMemcpyAsync(st.a.get(), x, bytes_x, cudaMemcpyHostToDevice, s));
+        ssv::matrix_spmv_dev(A, st.a.get(), st.b.get());
+        SSV_CUDA(cudaMemcpyAsync(y, st.b.get(), bytes_y, cudaMemcpyDeviceToHost, s));
+        SSV_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int ssv_solver_create(ssv_matrix* A, const uint8_t* freedofs, ssv_solver** out) {
+    return guarded([&] {
+        if (!A || !out) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_solver_create: NULL argument");
+        if (A->rows != A->cols) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_solver_create: matrix must be square");
+        auto* s = new ssv_solver();
+        s->A = A;
+        try {
+            check_mask(freedofs, A->rows, s->h_fd, s->fd, s->has_fd);
+            SSV_CUDA(cudaStreamSynchronize(ssv::stream()));
+        } catch (...) {
+            delete s;
+            throw;
+        }
+        *out = s;
+    });
+}
+
+int ssv_solver_destroy(ssv_solver* s) {
+    return guarded([&] {
+        if (!s) return;
+        ssv::mrtr_forget(s);
+        delete s;
+    });
+}
+
+int ssv_solver_solve_dev(ssv_solver* s, const char* method, const ssv_config* cfg, const void* d_b, void* d_x,
+                         ssv_result* res, double* history, int32_t history_cap) {
+    return guarded([&] {
+        if (!s || !cfg || !res || !d_b || !d_x) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_solver_solve_dev: NULL argument");
+        ssv::solver_solve_dev(s, method, *cfg, d_b, d_x, res, history, history_cap);
+    });
+}
+
+int ssv_solver_solve(ssv_solver* s, const char* method, const ssv_config* cfg, const void* b, void* x,
+                     ssv_result* res, double* history, int32_t history_cap) {
+    return guarded([&] {
+        if (!s || !cfg || !res || !b || !x) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_solver_solve: NULL argument");
+        if (ssv::parse_method(method) < 0)
+            ssv::fail(SSV_ERR_RUNTIME, std::string("SparseSolvSolver: Unknown method '") + (method ? method : "") +
+                                           "'. Available: ICCG, SGSMRTR, CG, COCR");
+        cudaStream_t st = ssv::stream();
+        const size_t bytes = (size_t)s->A->rows * scalar_bytes(s->A->dtype);
+        s->io_b.alloc(bytes / sizeof(double) + 1);
+        s->io_x.alloc(bytes / sizeof(double) + 1);
+        SSV_CUDA(cudaMemcpyAsync(s->io_b.get(), b, bytes, cudaMemcpyHostToDevice, st));
+        SSV_CUDA(cudaMemcpyAsync(s->io_x.get(), x, bytes, cudaMemcpyHostToDevice, st));
+        ssv::solver_solve_dev(s, method, *cfg, s->io_b.get(), s->io_x.get(), res, history, history_cap);
+        SSV_CUDA(cudaMemcpyAsync(x, s->io_x.get(), bytes, cudaMemcpyDeviceToHost, st));
+        SSV_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+int ssv_solver_profile(ssv_solver* s, const char* method, const ssv_config* cfg, int32_t reps,
+                       ssv_phase_profile* out) {
+    return guarded([&] {
+        if (!s || !cfg || !out) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_solver_profile: NULL argument");
+        ssv::solver_profile(s, method, *cfg, reps, out);
+    });
+}
+
+int ssv_ic_create(ssv_matrix* A, const uint8_t* freedofs, double shift, ssv_precond** out) {
+    return guarded([&] {
+        if (!A || !out) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ic_create: NULL argument");
+        if (A->rows != A->cols) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ic_create: matrix must be square");
+        auto* p = new ssv_precond();
+        p->kind = 1;
+        p->A = A;
+        ssv_config_default(&p->cfg);
+        p->cfg.shift_parameter = shift;
+        try {
+            check_mask(freedofs, A->rows, p->h_fd, p->fd, p->has_fd);
+            SSV_CUDA(cudaStreamSynchronize(ssv::stream()));
+        } catch (...) {
+            delete p;
+            throw;
+        }
+        *out = p;
+    });
+}
+
+int ssv_ic_set_config(ssv_precond* p, const ssv_config* cfg) {
+    return guarded([&] {
+        if (!p || !cfg) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ic_set_config: NULL argument");
+        p->cfg = *cfg;
+    });
+}
+
+int ssv_precond_update(ssv_precond* p) {
+    return guarded([&] {
+        if (!p) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_precond_update: NULL preconditioner");
+        ssv::precond_update(p);
+    });
+}
+
+int ssv_precond_apply_dev(ssv_precond* p, const void* d_x, void* d_y) {
+    return guarded([&] {
+        if (!p || !d_x || !d_y) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_precond_apply_dev: NULL argument");
+        ssv::precond_apply_dev(p, d_x, d_y);
+    });
+}
+
+int ssv_precond_apply(ssv_precond* p, const void* x, void* y) {
+    return guarded([&] {
+        if (!p || !x || !y) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_precond_apply: NULL argument");
+        if (!p->ready) ssv::fail(SSV_ERR_RUNTIME, "ICPreconditioner::apply called before setup");
+        cudaStream_t s = ssv::stream();
+        const size_t bytes = (size_t)p->A->rows * scalar_bytes(p->A->dtype);
+        p->io_x.alloc(bytes / sizeof(double) + 1);
+        p->io_y.alloc(bytes / sizeof(double) + 1);
+        SSV_CUDA(cudaMemcpyAsync(p->io_x.get(), x, bytes, cudaMemcpyHostToDevice, s));
+        ssv::precond_apply_dev(p, p->io_x.get(), p->io_y.get());
+        SSV_CUDA(cudaMemcpyAsync(y, p->io_y.get(), bytes, cudaMemcpyDeviceToHost, s));
+        SSV_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int ssv_ic_actual_shift(const ssv_precond* p, double* shift) {
+    return guarded([&] {
+        if (!p || !shift) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ic_actual_shift: NULL argument");
+        *shift = ssv::precond_actual_shift(p);
+    });
+}
+
+int ssv_precond_destroy(ssv_precond* p) {
+    return guarded([&] { delete p; });
+}
+
+int ssv_cocr_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, int32_t maxiter, double tol,
+                       int32_t printrates, const void* d_b, void* d_x, int32_t* iterations) {
+    return guarded([&] {
+        if (!A || !d_b || !d_x || !iterations) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_cocr_solve_dev: NULL argument");
+        ssv::cocr_solve_dev(A, pre, freedofs, maxiter, tol, printrates, d_b, d_x, iterations);
+    });
+}
+
+int ssv_cocr_solve(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, int32_t maxiter, double tol,
+                   int32_t printrates, const void* b, void* x, int32_t* iterations) {
+    return guarded([&] {
+        if (!A || !b || !x || !iterations) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_cocr_solve: NULL argument");
+        cudaStream_t s = ssv::stream();
+        const int n = A->rows;
+        const size_t bytes = (size_t)n * scalar_bytes(A->dtype);
+        Stage& st = stage();
+        st.a.alloc(bytes / sizeof(double) + 1);
+        st.b.alloc(bytes / sizeof(double) + 1);
+        ssv::DevBuf<uint8_t> dfd;
+        if (freedofs) {
+            std::vector<uint8_t> h(freedofs, freedofs + n);
+            for (auto& v : h) v = v ? 1 : 0;
+            dfd.upload(h.data(), h.size(), s);
+        }
+        SSV_CUDA(cudaMemcpyAsync(st.a.get(), b, bytes, cudaMemcpyHostToDevice, s));
+        ssv::cocr_solve_dev(A, pre, dfd.get(), maxiter, tol, printrates, st.a.get(), st.b.get(), iterations);
+        SSV_CUDA(cudaMemcpyAsync(x, st.b.get(), bytes, cudaMemcpyDeviceToHost, s));
+        SSV_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int ssv_abmc_build(int32_t n, const int32_t* row_ptr, const int32_t* col_idx, int32_t block_size,
+                   int32_t target_colors, int32_t* num_colors, int32_t* num_blocks, int32_t* color_offsets,
+                   int32_t* block_offsets, int32_t* ordering, int32_t* reverse_ordering) {
+    return guarded([&] {
+        if (n < 0 || (n > 0 && (!row_ptr || !col_idx))) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_abmc_build: bad input");
+        ssv::AbmcSchedule s;
+        ssv::build_abmc(n, row_ptr, col_idx, block_size, target_colors, s);
+        *num_colors = s.num_colors;
+        *num_blocks = s.num_blocks;
+        if (n <= 0) return;
+        std::memcpy(color_offsets, s.color_offsets.data(), sizeof(int) * s.color_offsets.size());
+        std::memcpy(block_offsets, s.block_offsets.data(), sizeof(int) * s.block_offsets.size());
+        std::memcpy(ordering, s.ordering.data(), sizeof(int) * n);
+        std::memcpy(reverse_ordering, s.reverse.data(), sizeof(int) * n);
+    });
+}
+
+int ssv_level_schedule(int32_t n, const int32_t* row_ptr, const int32_t* col_idx, int32_t upper,
+                       int32_t* level_of, int32_t* num_levels) {
+    return guarded([&] {
+        std::vector<int> lev;
+        *num_levels = ssv::build_levels(n, row_ptr, col_idx, upper != 0, lev);
+        if (n > 0) std::memcpy(level_of, lev.data(), sizeof(int) * n);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,254 @@
+// cocr_ngs.cu -- COCRSolver with an external preconditioner
+// (COCRSolverNGS::Mult, include/sparsesolv/ngsolve/sparsesolv_solvers.hpp:273-369)
+// as one CUDA graph: the preconditioner's kernels are captured into the same
+// iteration body, and the scalar steps run in the reductions' last block.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+
+#include "objects.cuh"
+#include "solver_api.hpp"
+
+namespace ssv {
+
+enum NgsOp : int { NGS_MU = 100, NGS_RHO = 101 };
+
+template <typename S>
+__device__ inline void ngs_finish(double2 total, KState* st, int op) {
+    if (op == NGS_MU) {  // :323-327
+        const S mu = s_from2<S>(total);
+        if (ST<S>::abs(mu) < 1e-30) { st->done = 1; st->iters = st->it; return; }
+        st->alpha = s_to2<S>(ST<S>::div(s_from2<S>(st->rho), mu));
+    } else if (op == NGS_RHO) {  // :354-359
+        const S rho = s_from2<S>(st->rho);
+        if (ST<S>::abs(rho) < 1e-30) { st->done = 1; st->iters = st->it; return; }
+        st->beta = s_to2<S>(ST<S>::div(s_from2<S>(total), rho));
+        st->rho = total;
+    }
+}
+
+// mu = qt^T q (unconjugated)
+template <typename S>
+__global__ void __launch_bounds__(kBlock)
+k_ngs_dot(int n, const S* __restrict__ a, const S* __restrict__ b, KState* st, int op, RedBuf red) {
+    if (st->done) return;
+    double2 part = make_double2(0.0, 0.0);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        part = add2(part, s_to2<S>(a[i] * b[i]));
+    double2 total;
+    if (grid_reduce2(part, red.partials, red.ticket, total)) ngs_finish<S>(total, st, op);
+}
+
+// t = A rt, projected; rho_new = rt^T t
+template <typename S, int LANES>
+__global__ void __launch_bounds__(kBlock)
+k_ngs_spmv_dot(int n, const int* __restrict__ rp, const int* __restrict__ ci, const S* __restrict__ v,
+               const S* __restrict__ x, S* __restrict__ y, const uint8_t* __restrict__ mask, KState* st,
+               RedBuf red) {
+    if (st->done) return;
+    const int sub = threadIdx.x % LANES;
+    const int rpb = kBlock / LANES;
+    const int lane_row = (threadIdx.x & 31) / LANES;  // warp-uniform trip count (full-mask shuffles)
+    double2 part = make_double2(0.0, 0.0);
+    for (int row = blockIdx.x * rpb + threadIdx.x / LANES; row - lane_row < n; row += gridDim.x * rpb) {
+        const bool valid = row < n;
+        S acc = ST<S>::zero();
+        if (valid)
+            for (int k = rp[row] + sub; k < rp[row + 1]; k += LANES) acc = ST<S>::fma(v[k], x[ci[k]], acc);
+#pragma unroll
+        for (int o = LANES / 2; o > 0; o >>= 1) {
+            if constexpr (ST<S>::cplx) {
+                acc.x += __shfl_down_sync(0xffffffffu, acc.x, o, LANES);
+                acc.y += __shfl_down_sync(0xffffffffu, acc.y, o, LANES);
+            } else {
+                acc += __shfl_down_sync(0xffffffffu, acc, o, LANES);
+            }
+        }
+        if (sub == 0 && valid) {
+            if (mask && !mask[row]) acc = ST<S>::zero();
+            y[row] = acc;
+            part = add2(part, s_to2<S>(x[row] * acc));
+        }
+    }
+    double2 total;
+    if (grid_reduce2(part, red.partials, red.ticket, total)) ngs_finish<S>(total, st, NGS_RHO);
+}
+
+// sol += alpha p ; r -= alpha q ; rt -= alpha qt ; res = sqrt(|r^H r|)
+template <typename S>
+__global__ void __launch_bounds__(kBlock)
+k_ngs_update(int n, S* __restrict__ x, const S* __restrict__ p, const S* __restrict__ q,
+             const S* __restrict__ qt, S* __restrict__ r, S* __restrict__ rt, KState* st, RedBuf red) {
+    if (st->done) return;
+    const S alpha = s_from2<S>(st->alpha);
+    double2 part = make_double2(0.0, 0.0);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        x[i] = ST<S>::fma(alpha, p[i], x[i]);
+        const S ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        rt[i] = rt[i] - alpha * qt[i];
+        part.x += ST<S>::norm2(ri);
+    }
+    double2 total;
+    if (grid_reduce2(part, red.partials, red.ticket, total)) {
+        const double res = std::sqrt(std::fabs(total.x));
+        st->norm_r = res;
+        if (st->save_hist) {
+            if (st->hist_len < st->hist_cap) st->hist[st->hist_len] = res / st->normalizer;
+            st->hist_len++;
+        }
+        if (res / st->normalizer <= st->tol) {  // :344-347
+            st->done = 1;
+            st->converged = 1;
+            st->iters = st->it + 1;
+        }
+    }
+}
+
+__global__ void k_ngs_loop_ctl(KState* st, cudaGraphConditionalHandle h, int use_cond) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (!st->done) {
+        st->it++;
+        if (st->it >= st->maxiter) { st->done = 1; st->iters = st->maxiter; }  // :368
+    }
+    st->loops++;
+    if (!st->done && st->loops >= st->max_loops) { st->done = 1; st->status = SSV_ERR_TIMEOUT; }
+    if (use_cond) cudaGraphSetConditional(h, st->done ? 0u : 1u);
+}
+
+struct CocrCtx {
+    KrylovWork<double> w_d;
+    KrylovWork<zdouble> w_z;
+    GraphLoop loop;
+};
+
+static std::map<const ssv_matrix*, std::unique_ptr<CocrCtx>>& cocr_table() {
+    static std::map<const ssv_matrix*, std::unique_ptr<CocrCtx>> t;
+    return t;
+}
+
+void cocr_forget(const ssv_matrix* A) { cocr_table().erase(A); }
+
+template <typename S> KrylovWork<S>& cw_of(CocrCtx& c);
+template <> KrylovWork<double>& cw_of<double>(CocrCtx& c) { return c.w_d; }
+template <> KrylovWork<zdouble>& cw_of<zdouble>(CocrCtx& c) { return c.w_z; }
+
+template <typename S>
+static void apply_pre(ssv_precond* pre, const S* x, S* y, const KState* st, int n, cudaStream_t s) {
+    if (pre) ic_apply_dev<S>(pre, x, y, st, s);
+    else k_copy<S><<<grid_for(n, kBlock), kBlock, 0, s>>>(n, x, y);
+}
+
+template <typename S>
+static void run_cocr_ngs(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, int maxiter, double tol,
+                         int printrates, const S* d_b, S* d_x, int* iterations) {
+    cudaStream_t s = stream();
+    const int n = A->rows;
+    auto& ctx_ptr = cocr_table()[A];
+    if (!ctx_ptr) ctx_ptr.reset(new CocrCtx());
+    CocrCtx& ctx = *ctx_ptr;
+    KrylovWork<S>& w = cw_of<S>(ctx);
+    const int dev_hist = printrates ? std::max(maxiter, 0) + 2 : 1;
+    w.ensure(n, dev_hist);
+    const RedBuf red = w.red();
+    const int g = grid_for(n, kBlock);
+    const S* v = reinterpret_cast<const S*>(A->val.get());
+    S *x = d_x, *r = w.r.get(), *rt = w.z.get(), *p = w.p.get(), *q = w.Ap.get(), *qt = w.qt.get(),
+      *t = w.t.get();
+    // sol = 0 ; r = rhs projected ; ||rhs|| (:274-299)
+    SSV_CUDA(cudaMemsetAsync(x, 0, sizeof(S) * n, s));
+    k_gather_perm<S><<<g, kBlock, 0, s>>>(n, nullptr, d_b, r, fd, 1);
+    k_norm2<S><<<g, kBlock, 0, s>>>(n, r, red, w.scal.get());
+    SSV_LAUNCH_CHECK();
+    double2 nb;
+    SSV_CUDA(cudaMemcpyAsync(&nb, w.scal.get(), sizeof(nb), cudaMemcpyDeviceToHost, s));
+    SSV_CUDA(cudaStreamSynchronize(s));
+    const double rhs_norm = std::sqrt(std::fabs(nb.x));
+    if (rhs_norm < 1e-30) { *iterations = 0; return; }
+    // rt = M^{-1} r ; p = rt ; q = A p projected ; rho = rt^T q
+    KState* dst = w.st.get();
+    apply_pre<S>(pre, r, rt, nullptr, n, s);
+    k_copy<S><<<g, kBlock, 0, s>>>(n, rt, p);
+    launch_spmv<S, S, 0>(A->lanes, n, A->rp.get(), A->ci.get(), v, p, q, nullptr, fd, nullptr, RED_STORE, red,
+                         nullptr, s);
+    SSV_LAUNCH_CHECK();
+    KState h;
+    std::memset(&h, 0, sizeof(h));
+    h.normalizer = rhs_norm;
+    h.tol = tol;
+    h.maxiter = maxiter;
+    h.save_hist = printrates ? 1 : 0;
+    h.hist_cap = dev_hist;
+    h.hist = w.hist.get();
+    h.max_loops = std::max(maxiter, 0) + 4;
+    if (maxiter <= 0) { h.done = 1; h.iters = 0; }
+    {
+        // state first, then rho = rt^T q into it
+        SSV_CUDA(cudaMemcpyAsync(dst, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+        k_dot<S><<<g, kBlock, 0, s>>>(n, rt, q, 0, nullptr, RED_STORE, red, &dst->rho);
+        SSV_LAUNCH_CHECK();
+    }
+    std::string key = "ngs;" + std::to_string(n) + ";" + std::to_string((size_t)pre) + ";" +
+                      std::to_string((size_t)fd) + ";" + std::to_string((size_t)x) + ";" +
+                      std::to_string((size_t)dst) + ";" + std::to_string(A->lanes) + ";" +
+                      std::to_string((size_t)red.partials);
+    if (pre) {
+        const ICDevice<S>* ic = nullptr;
+        if constexpr (std::is_same<S, double>::value) ic = &pre->ic_d;
+        else ic = &pre->ic_z;
+        key += ";" + std::to_string((size_t)ic) + ";" + std::to_string(ic->gen) + ";" +
+               std::to_string((size_t)ic->Lv.get()) + std::to_string(ic->lo) + ";" +
+               std::to_string((size_t)pre->xw.get()) + ";" + std::to_string(ic->abmc);
+    }
+    build_graph_loop(ctx.loop, key, [&](cudaGraphConditionalHandle hc, int use_cond) {
+        apply_pre<S>(pre, q, qt, dst, n, s);
+        k_ngs_dot<S><<<g, kBlock, 0, s>>>(n, qt, q, dst, NGS_MU, red);
+        k_ngs_update<S><<<g, kBlock, 0, s>>>(n, x, p, q, qt, r, rt, dst, red);
+        {
+            const int L = A->lanes;
+            const int rpb = kBlock / L;
+            int gg = std::max(1, std::min((n + rpb - 1) / rpb, sm_count() * 8));
+            switch (L) {
+                case 2: k_ngs_spmv_dot<S, 2><<<gg, kBlock, 0, s>>>(n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
+                case 4: k_ngs_spmv_dot<S, 4><<<gg, kBlock, 0, s>>>(n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
+                case 8: k_ngs_spmv_dot<S, 8><<<gg, kBlock, 0, s>>>(n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
+                case 16: k_ngs_spmv_dot<S, 16><<<gg, kBlock, 0, s>>>(n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
+                default: k_ngs_spmv_dot<S, 32><<<gg, kBlock, 0, s>>>(n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red);
+            }
+        }
+        k_cocr_pq<S><<<g, kBlock, 0, s>>>(n, rt, t, p, q, dst);
+        k_ngs_loop_ctl<<<1, 32, 0, s>>>(dst, hc, use_cond);
+        SSV_LAUNCH_CHECK();
+    });
+    if (maxiter > 0) run_graph_loop(ctx.loop, dst, maxiter);
+    SSV_CUDA(cudaMemcpyAsync(&h, dst, sizeof(h), cudaMemcpyDeviceToHost, s));
+    SSV_CUDA(cudaStreamSynchronize(s));
+    if (h.status == SSV_ERR_TIMEOUT) fail(SSV_ERR_TIMEOUT, "COCR loop guard fired");
+    *iterations = h.iters;
+    if (printrates) {
+        std::vector<double> hs(std::min(h.hist_len, dev_hist));
+        if (!hs.empty())
+            SSV_CUDA(cudaMemcpy(hs.data(), w.hist.get(), sizeof(double) * hs.size(), cudaMemcpyDeviceToHost));
+        std::printf("COCR iter 0: res = 1\n");
+        for (size_t k = 0; k < hs.size(); ++k) std::printf("COCR iter %zu: res = %g\n", k + 1, hs[k]);
+        std::fflush(stdout);
+    }
+}
+
+void cocr_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, int maxiter, double tol,
+                    int printrates, const void* d_b, void* d_x, int* iterations) {
+    if (pre && !pre->ready) fail(SSV_ERR_RUNTIME, "COCRSolver: preconditioner is not set up (call Update())");
+    if (pre && pre->A->dtype != A->dtype)
+        fail(SSV_ERR_TYPE, "COCRSolver: preconditioner scalar type differs from the matrix");
+    if (A->dtype == SSV_F64)
+        run_cocr_ngs<double>(A, pre, d_fd, maxiter, tol, printrates, static_cast<const double*>(d_b),
+                             static_cast<double*>(d_x), iterations);
+    else
+        run_cocr_ngs<zdouble>(A, pre, d_fd, maxiter, tol, printrates, static_cast<const zdouble*>(d_b),
+                              static_cast<zdouble*>(d_x), iterations);
+}
+
+}  // namespace ssv

@@ -1,0 +1,200 @@
+// objects.cuh -- the device objects behind the C ABI handles.
+#pragma once
+
+#include <algorithm>
+#include <memory>
+#include <string>
+
+#include "host_order.hpp"
+#include "kernels.cuh"
+
+namespace ssv {
+
+cudaStream_t stream();
+
+// Sub-warp width of the CSR kernels from the mean row length.
+int pick_lanes(double nnz_per_row);
+
+// Launch y = A x style SpMV for any lanes/mode (mask zeroes masked rows).
+template <typename S, typename SV, int MODE>
+void launch_spmv(int lanes, int n, const int* rp, const int* ci, const SV* v, const S* x, S* y,
+                 const S* b, const uint8_t* mask, KState* st, int op, RedBuf red, double2* out,
+                 cudaStream_t s);
+
+// Reusable reduction scratch + device state of one Krylov solve.
+template <typename S>
+struct KrylovWork {
+    int n = -1;
+    DevBuf<S> xb[3], r, z, p, Ap, t, qt, bw;
+    DevBuf<KState> st;
+    DevBuf<double> hist;
+    DevBuf<double2> partials, scal;
+    DevBuf<unsigned int> ticket;
+    void ensure(int n_, int hist_cap);
+    RedBuf red() const { return RedBuf{partials.get(), ticket.get()}; }
+};
+
+// A CUDA graph of one iteration body, looped on the device by a WHILE
+// conditional node (or, when SSV_GRAPH_MODE=chunk, a graph of `chunk` copies
+// relaunched by the host until the state says done).
+struct GraphLoop {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool cond = false;
+    int chunk = 1;
+    size_t body_nodes = 0;  // kernel nodes per iteration body
+    std::string key;
+    GraphLoop() = default;
+    GraphLoop(const GraphLoop&) = delete;
+    GraphLoop& operator=(const GraphLoop&) = delete;
+    ~GraphLoop() { reset(); }
+    void reset();
+};
+
+bool graph_while_mode();
+
+template <typename F>
+void build_graph_loop(GraphLoop& g, const std::string& key_in, F&& body) {
+    const std::string key = key_in + (graph_while_mode() ? "|while" : "|chunk");
+    if (g.exec && g.key == key) return;
+    g.reset();
+    cudaStream_t s = stream();
+    if (graph_while_mode()) {
+        SSV_CUDA(cudaGraphCreate(&g.graph, 0));
+        cudaGraphConditionalHandle h;
+        SSV_CUDA(cudaGraphConditionalHandleCreate(&h, g.graph, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        SSV_CUDA(cudaGraphAddNode(&node, g.graph, nullptr, 0, &cp));
+        cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+        SSV_CUDA(cudaStreamBeginCaptureToGraph(s, bodyg, nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal));
+        body(h, 1);
+        SSV_CUDA(cudaStreamEndCapture(s, &bodyg));
+        SSV_CUDA(cudaGraphGetNodes(bodyg, nullptr, &g.body_nodes));
+        SSV_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+        g.cond = true;
+    } else {
+        SSV_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        for (int c = 0; c < g.chunk; ++c) body(cudaGraphConditionalHandle(0), 0);
+        SSV_CUDA(cudaStreamEndCapture(s, &g.graph));
+        SSV_CUDA(cudaGraphGetNodes(g.graph, nullptr, &g.body_nodes));
+        g.body_nodes /= (size_t)std::max(g.chunk, 1);
+        SSV_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+        g.cond = false;
+    }
+    g.key = key;
+}
+
+// Runs the loop until the device state reports done (bounded).
+void run_graph_loop(GraphLoop& g, KState* d_st, int max_iters);
+
+// ---------------------------------------------------------------------------
+// IC(0) preconditioner on the device (ic_preconditioner.hpp)
+// ---------------------------------------------------------------------------
+template <typename S>
+struct ICDevice {
+    using SL = typename ST<S>::lo;
+    int n = 0;
+    // pattern cache key (ICPreconditioner caches its ordering per pattern,
+    // ic_preconditioner.hpp:74-81)
+    bool built = false, abmc = false;
+    int bs = 0, nct = 0;
+    unsigned gen = 0;  // bumped on every pattern rebuild (part of graph keys)
+    // schedule: launches in processing order, each a unit range
+    std::vector<std::pair<int, int>> fwd_launch, bwd_launch;
+    DevBuf<int> uoff, rows_f, rows_b;  // uoff: ABMC block row offsets
+    int num_colors = 0, num_blocks = 0, num_levels_f = 0, num_levels_b = 0;
+    std::vector<int> h_perm;           // ordering[old] = new (ABMC)
+    std::vector<int> h_boff;           // ABMC block row offsets
+    DevBuf<int> perm;
+    // working matrix in ABMC numbering (values gathered through Asrc)
+    std::vector<int> h_Arp;
+    DevBuf<int> Arp, Aci, Asrc;
+    DevBuf<S> Av;
+    int lanes = 8;
+    // factor L (diag last), U = L^T (diag first)
+    std::vector<int> h_Lrp, h_Lci;
+    DevBuf<int> Lrp, Lci, Lsrc, Urp, Uci, Usrc;
+    DevBuf<S> Lv, Uv, inv;
+    DevBuf<SL> Lv_lo, Uv_lo, inv_lo;
+    DevBuf<double> scaling;
+    DevBuf<int> flag;
+    bool scaled_apply = false, lo = false;
+    int missing_row = -1;
+    double actual_shift = 0.0;
+    DevBuf<S> tw;  // forward-sweep output
+    // ABMC block-sweep layout (k_ic_fwd_blk / k_ic_bwd_blk): external parts of
+    // L and U rows, packed strictly-lower intra-block table, diagonal
+    bool blk = false;
+    int blk_lanes = 0, tri = 1;
+    DevBuf<int> erp, eci, esrc, urpe, ucie, usrce, isrc, dsrc;
+    DevBuf<S> ev, uev, iv, dv;
+    DevBuf<SL> ev_lo, uev_lo, iv_lo, dv_lo;
+
+    // Pattern set-up from the matrix pattern (host) for the given options.
+    void build_pattern(int n, const std::vector<int>& rp, const std::vector<int>& ci,
+                       const ssv_config& cfg);
+    // Gathers values (vals = BC-modified matrix values, original numbering),
+    // factorises with auto-shift on the device, builds U and the FP32 form.
+    // Returns the number of kernels launched.
+    int factorize(const S* vals, const ssv_config& cfg);
+    // y = M^{-1} x in the working numbering (ABMC numbering or natural).
+    void apply(const S* x, S* y, const KState* st, cudaStream_t s) const {
+        apply_fwd(x, st, s);
+        apply_bwd(y, st, s);
+    }
+    void apply_fwd(const S* x, const KState* st, cudaStream_t s) const;  // x -> tw
+    void apply_bwd(S* y, const KState* st, cudaStream_t s) const;        // tw -> y
+    int kernels_per_apply() const {
+        return (int)(fwd_launch.size() + bwd_launch.size()) + (scaled_apply ? 1 : 0);
+    }
+};
+
+}  // namespace ssv
+
+// ---------------------------------------------------------------------------
+// Handles of the C ABI
+// ---------------------------------------------------------------------------
+struct ssv_matrix {
+    int rows = 0, cols = 0;
+    int64_t nnz = 0;
+    int dtype = SSV_F64;
+    std::vector<int> h_rp, h_ci;
+    ssv::DevBuf<int> rp, ci;
+    ssv::DevBuf<double> val;  // nnz (F64) or 2*nnz (C128) doubles
+    int lanes = 8;
+};
+
+struct ssv_solver {
+    ssv_matrix* A = nullptr;
+    bool has_fd = false;
+    std::vector<uint8_t> h_fd;
+    ssv::DevBuf<uint8_t> fd;
+    ssv::DevBuf<double> vals_bc;
+    ssv::DevBuf<double> io_b, io_x;  // staging for host-pointer solves
+    ssv::ICDevice<double> ic_d;
+    ssv::ICDevice<ssv::zdouble> ic_z;
+    ssv::KrylovWork<double> w_d;
+    ssv::KrylovWork<ssv::zdouble> w_z;
+    ssv::GraphLoop loop;
+};
+
+struct ssv_precond {
+    int kind = 0;  // 1 = IC
+    ssv_matrix* A = nullptr;
+    bool has_fd = false;
+    std::vector<uint8_t> h_fd;
+    ssv::DevBuf<uint8_t> fd;
+    ssv::DevBuf<double> vals_bc;
+    ssv_config cfg{};
+    bool ready = false;
+    ssv::ICDevice<double> ic_d;
+    ssv::ICDevice<ssv::zdouble> ic_z;
+    ssv::DevBuf<double> xw, yw, io_x, io_y;
+    virtual ~ssv_precond() = default;
+};

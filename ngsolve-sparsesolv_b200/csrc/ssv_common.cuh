@@ -1,0 +1,174 @@
+// ssv_common.cuh -- shared definitions of the B200 solve path: scalar types,
+// error plumbing, device buffers and the launch geometry of B200 (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sparsesolv_b200.h"
+
+namespace ssv {
+
+// ---------------------------------------------------------------------------
+// Errors: C++ exceptions inside the library, status codes at the C ABI.
+// ---------------------------------------------------------------------------
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] inline void fail(int code, const std::string& msg) { throw Error(code, msg); }
+
+inline void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
+    if (e != cudaSuccess) {
+        int code = (e == cudaErrorMemoryAllocation) ? SSV_ERR_ALLOC
+                 : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? SSV_ERR_NO_DEVICE
+                 : SSV_ERR_CUDA;
+        fail(code, std::string("CUDA error in ") + what + " (" + file + ":" + std::to_string(line) +
+                       "): " + cudaGetErrorString(e));
+    }
+}
+#define SSV_CUDA(call) ::ssv::cuda_check((call), #call, __FILE__, __LINE__)
+#define SSV_LAUNCH_CHECK() ::ssv::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+
+// ---------------------------------------------------------------------------
+// Scalars. zdouble has the layout of std::complex<double> (two doubles,
+// 16-byte aligned so a pair moves in one 128-bit load).
+// ---------------------------------------------------------------------------
+struct __align__(16) zdouble {
+    double x, y;
+};
+struct __align__(8) zfloat {
+    float x, y;
+};
+
+__host__ __device__ inline zdouble operator+(zdouble a, zdouble b) { return {a.x + b.x, a.y + b.y}; }
+__host__ __device__ inline zdouble operator-(zdouble a, zdouble b) { return {a.x - b.x, a.y - b.y}; }
+__host__ __device__ inline zdouble operator-(zdouble a) { return {-a.x, -a.y}; }
+__host__ __device__ inline zdouble operator*(zdouble a, zdouble b) {
+    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+__host__ __device__ inline zdouble operator*(double s, zdouble a) { return {s * a.x, s * a.y}; }
+__host__ __device__ inline zdouble& operator+=(zdouble& a, zdouble b) { a.x += b.x; a.y += b.y; return a; }
+__host__ __device__ inline zdouble& operator-=(zdouble& a, zdouble b) { a.x -= b.x; a.y -= b.y; return a; }
+__host__ __device__ inline zfloat operator+(zfloat a, zfloat b) { return {a.x + b.x, a.y + b.y}; }
+__host__ __device__ inline zfloat operator-(zfloat a, zfloat b) { return {a.x - b.x, a.y - b.y}; }
+__host__ __device__ inline zfloat operator*(zfloat a, zfloat b) {
+    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+__host__ __device__ inline zfloat& operator+=(zfloat& a, zfloat b) { a.x += b.x; a.y += b.y; return a; }
+__host__ __device__ inline zfloat& operator-=(zfloat& a, zfloat b) { a.x -= b.x; a.y -= b.y; return a; }
+
+// Complex division with the scaling of Smith's method (numerically safe for
+// the magnitudes met in Krylov recurrences).
+__host__ __device__ inline zdouble zdiv(zdouble a, zdouble b) {
+    if (fabs(b.x) >= fabs(b.y)) {
+        double r = b.y / b.x, d = b.x + b.y * r;
+        return {(a.x + a.y * r) / d, (a.y - a.x * r) / d};
+    } else {
+        double r = b.x / b.y, d = b.x * r + b.y;
+        return {(a.x * r + a.y) / d, (a.y * r - a.x) / d};
+    }
+}
+
+// Scalar traits: one code path for double and complex<double>.
+template <typename S> struct ST;
+template <> struct ST<double> {
+    using lo = float;  // storage type of the FP32 preconditioner form
+    static constexpr bool cplx = false;
+    __host__ __device__ static double zero() { return 0.0; }
+    __host__ __device__ static double one() { return 1.0; }
+    __host__ __device__ static double real(double a) { return a; }
+    __host__ __device__ static double from(double a) { return a; }
+    __host__ __device__ static double conj(double a) { return a; }
+    __host__ __device__ static double norm2(double a) { return a * a; }
+    __host__ __device__ static double abs(double a) { return fabs(a); }
+    __host__ __device__ static double div(double a, double b) { return a / b; }
+    __host__ __device__ static double scale(double s, double a) { return s * a; }
+    __host__ __device__ static double fma(double a, double b, double c) { return a * b + c; }
+    __host__ __device__ static double to_d2_x(double a) { return a; }
+};
+template <> struct ST<zdouble> {
+    using lo = zfloat;
+    static constexpr bool cplx = true;
+    __host__ __device__ static zdouble zero() { return {0.0, 0.0}; }
+    __host__ __device__ static zdouble one() { return {1.0, 0.0}; }
+    __host__ __device__ static double real(zdouble a) { return a.x; }
+    __host__ __device__ static zdouble from(double a) { return {a, 0.0}; }
+    __host__ __device__ static zdouble conj(zdouble a) { return {a.x, -a.y}; }
+    __host__ __device__ static double norm2(zdouble a) { return a.x * a.x + a.y * a.y; }
+    __host__ __device__ static double abs(zdouble a) { return hypot(a.x, a.y); }
+    __host__ __device__ static zdouble div(zdouble a, zdouble b) { return zdiv(a, b); }
+    __host__ __device__ static zdouble scale(double s, zdouble a) { return {s * a.x, s * a.y}; }
+    __host__ __device__ static zdouble fma(zdouble a, zdouble b, zdouble c) { return a * b + c; }
+};
+
+// Conversions between the FP64 and FP32 forms.
+__host__ __device__ inline float lo_of(double a) { return (float)a; }
+__host__ __device__ inline zfloat lo_of(zdouble a) { return {(float)a.x, (float)a.y}; }
+__host__ __device__ inline double hi_of(float a) { return (double)a; }
+__host__ __device__ inline zdouble hi_of(zfloat a) { return {(double)a.x, (double)a.y}; }
+// Widen a stored coefficient (FP64 or FP32 form) to the arithmetic type.
+__host__ __device__ inline double hi_of_any(double a) { return a; }
+__host__ __device__ inline double hi_of_any(float a) { return (double)a; }
+__host__ __device__ inline zdouble hi_of_any(zdouble a) { return a; }
+__host__ __device__ inline zdouble hi_of_any(zfloat a) { return {(double)a.x, (double)a.y}; }
+
+// ---------------------------------------------------------------------------
+// Device memory
+// ---------------------------------------------------------------------------
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t count) { alloc(count); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void alloc(size_t count) {
+        if (count == n && p) return;
+        release();
+        n = count;
+        if (count) SSV_CUDA(cudaMalloc(&p, sizeof(T) * count));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void upload(const T* h, size_t count, cudaStream_t s) {
+        alloc(count);
+        if (count) SSV_CUDA(cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, s));
+    }
+    void zero(cudaStream_t s) {
+        if (n) SSV_CUDA(cudaMemsetAsync(p, 0, sizeof(T) * n, s));
+    }
+    T* get() const { return p; }
+    size_t size() const { return n; }
+};
+
+// Launch geometry: 148 SMs on B200; grids are sized in multiples of the SM
+// count (queried once) for grid-stride kernels.
+int sm_count();
+inline int grid_for(int64_t work, int block, int per_sm = 8) {
+    int64_t g = (work + block - 1) / block;
+    int64_t cap = (int64_t)sm_count() * per_sm;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+double wall_seconds();
+
+}  // namespace ssv

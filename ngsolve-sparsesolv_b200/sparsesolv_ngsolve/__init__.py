@@ -1,1 +1,494 @@
-"""placeholder"""
+"""sparsesolv_ngsolve -- the reference's Python API on the B200 solve path.
+
+Same factories, keyword arguments, defaults, typed classes and error types as
+ksugahar/ngsolve-sparsesolv's pybind11 module
+(include/sparsesolv/ngsolve/sparsesolv_python_export.hpp), backed by the
+sm_100a kernels of ``libsparsesolv_b200.so`` through its C ABI. There is no
+CPU path: without a CUDA device every solve raises.
+
+Matrices: a ``scipy.sparse`` matrix, or any object with NGSolve's
+``SparseMatrix.CSR()`` (returning ``(values, col_indices, row_ptr)``).
+Vectors: numpy arrays, or NGSolve vectors (``.FV().NumPy()``).
+FreeDofs: a boolean/uint8 array, or an NGSolve ``BitArray``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi
+from ._capi import check
+
+__all__ = [
+    "SparseSolvResult", "SparseSolvSolver", "SparseSolvSolverD", "SparseSolvSolverC",
+    "ICPreconditioner", "ICPreconditionerD", "ICPreconditionerC",
+    "COCRSolver", "COCRSolverD", "COCRSolverC", "has_compact_ams",
+]
+
+
+# ---------------------------------------------------------------------------
+# input adapters
+# ---------------------------------------------------------------------------
+
+def _csr_arrays(mat):
+    """(indptr int32, indices int32, data, is_complex) of a sparse matrix."""
+    if hasattr(mat, "tocsr") and hasattr(mat, "indptr") or hasattr(mat, "tocsr"):
+        A = mat.tocsr()
+        if not A.has_sorted_indices:
+            A = A.sorted_indices()
+        ip = np.ascontiguousarray(A.indptr, dtype=np.int32)
+        ix = np.ascontiguousarray(A.indices, dtype=np.int32)
+        data = A.data
+        shape = A.shape
+    elif hasattr(mat, "CSR"):  # NGSolve SparseMatrix
+        vals, cols, rows = mat.CSR()
+        data = np.asarray(vals)
+        ix = np.ascontiguousarray(np.asarray(cols), dtype=np.int32)
+        ip = np.ascontiguousarray(np.asarray(rows), dtype=np.int32)
+        shape = (mat.height, mat.width)
+    else:
+        raise TypeError("expected SparseMatrix (scipy.sparse or NGSolve SparseMatrix)")
+    cplx = np.iscomplexobj(data)
+    data = np.ascontiguousarray(data, dtype=np.complex128 if cplx else np.float64)
+    return ip, ix, data, cplx, shape
+
+
+def _freedofs_array(freedofs, n):
+    if freedofs is None:
+        return None
+    if hasattr(freedofs, "__len__") and not isinstance(freedofs, np.ndarray) and hasattr(freedofs, "__getitem__") \
+            and not isinstance(freedofs, (list, tuple)):
+        fd = np.fromiter((1 if freedofs[i] else 0 for i in range(len(freedofs))), dtype=np.uint8, count=len(freedofs))
+    else:
+        fd = np.asarray(freedofs).astype(bool).astype(np.uint8)
+    if fd.shape[0] != n:
+        raise ValueError(f"freedofs has {fd.shape[0]} entries, matrix has {n} rows")
+    return np.ascontiguousarray(fd)
+
+
+def _vec_view(v):
+    """Writable numpy view of a vector (numpy array or NGSolve BaseVector)."""
+    if isinstance(v, np.ndarray):
+        return v
+    if hasattr(v, "FV"):
+        return v.FV().NumPy()
+    return np.asarray(v)
+
+
+class _Matrix:
+    """Device copy of a CSR matrix (ssv_matrix handle)."""
+
+    def __init__(self, mat):
+        self.src = mat
+        ip, ix, data, cplx, shape = _csr_arrays(mat)
+        self.n, self.m = int(shape[0]), int(shape[1])
+        self.cplx = bool(cplx)
+        self.dtype = np.complex128 if cplx else np.float64
+        self.nnz = int(ip[-1])
+        lib = _capi.load()
+        h = ctypes.c_void_p()
+        check(lib.ssv_matrix_create(self.n, self.m, _capi.i32ptr(ip), _capi.i32ptr(ix), _capi.vptr(data),
+                                    _capi.SSV_C128 if cplx else _capi.SSV_F64, ctypes.byref(h)))
+        self.h = h
+        self._lib = lib
+
+    def refresh(self):
+        """Re-read the source matrix values (the matrix may be modified in place)."""
+        _, _, data, cplx, _ = _csr_arrays(self.src)
+        if bool(cplx) != self.cplx or data.shape[0] != self.nnz:
+            raise ValueError("matrix pattern or scalar type changed; create a new object")
+        check(self._lib.ssv_matrix_update_values(self.h, _capi.vptr(data)))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            try:
+                self._lib.ssv_matrix_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+
+# ---------------------------------------------------------------------------
+# SparseSolvResult (sparsesolv_python_export.hpp:32-49)
+# ---------------------------------------------------------------------------
+
+class SparseSolvResult:
+    """Result of a SparseSolv iterative solve (converged, iterations, final_residual, residual_history)."""
+
+    __slots__ = ("converged", "iterations", "final_residual", "residual_history",
+                 "actual_shift", "setup_seconds", "solve_seconds", "kernel_launches")
+
+    def __init__(self, converged=False, iterations=0, final_residual=0.0, residual_history=(),
+                 actual_shift=0.0, setup_seconds=0.0, solve_seconds=0.0, kernel_launches=0):
+        self.converged = bool(converged)
+        self.iterations = int(iterations)
+        self.final_residual = float(final_residual)
+        self.residual_history = list(residual_history)
+        self.actual_shift = actual_shift
+        self.setup_seconds = setup_seconds
+        self.solve_seconds = solve_seconds
+        self.kernel_launches = int(kernel_launches)
+
+    def __repr__(self):
+        return (f"SparseSolvResult(converged={'True' if self.converged else 'False'}, "
+                f"iterations={self.iterations}, residual={self.final_residual:f})")
+
+
+# ---------------------------------------------------------------------------
+# SparseSolvSolver (ngsolve/sparsesolv_solvers.hpp:33-239)
+# ---------------------------------------------------------------------------
+
+class _SparseSolvSolverBase:
+    _cplx = False
+
+    def __init__(self, mat, method="ICCG", freedofs=None, tol=1e-10, maxiter=1000, shift=1.05,
+                 save_best_result=True, save_residual_history=False, printrates=False):
+        self._mat = _Matrix(mat)
+        self._fd = _freedofs_array(freedofs, self._mat.n)
+        self.method = method
+        self._cfg = _capi.default_config(tolerance=tol, max_iterations=maxiter, shift_parameter=shift,
+                                         save_best_result=save_best_result,
+                                         save_residual_history=save_residual_history)
+        self.printrates = bool(printrates)
+        self._last = SparseSolvResult()
+        lib = _capi.load()
+        h = ctypes.c_void_p()
+        check(lib.ssv_solver_create(self._mat.h, _capi.u8ptr(self._fd), ctypes.byref(h)))
+        self._h = h
+        self._lib = lib
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self._lib.ssv_solver_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # -- solve ----------------------------------------------------------------
+    def Solve(self, rhs, sol):
+        """Solve A x = b with sol as the initial guess; returns SparseSolvResult."""
+        b = np.ascontiguousarray(_vec_view(rhs), dtype=self._mat.dtype)
+        xv = _vec_view(sol)
+        x = np.ascontiguousarray(xv, dtype=self._mat.dtype)
+        if b.shape[0] != self._mat.n or x.shape[0] != self._mat.n:
+            raise ValueError("vector size does not match the matrix")
+        self._mat.refresh()
+        cfg = _capi.ssv_config()
+        ctypes.pointer(cfg)[0] = self._cfg
+        if self.printrates:
+            cfg.save_residual_history = 1
+        cap = max(int(cfg.max_iterations), 0) + 2 if cfg.save_residual_history else 0
+        hist = np.zeros(max(cap, 1))
+        res = _capi.ssv_result()
+        check(self._lib.ssv_solver_solve(self._h, str(self.method).encode(), ctypes.byref(cfg),
+                                         _capi.vptr(b), _capi.vptr(x), ctypes.byref(res),
+                                         hist.ctypes.data_as(_capi.PD), cap))
+        if x is not xv:
+            xv[...] = x
+        r = SparseSolvResult(res.converged, res.iterations, res.final_residual,
+                             hist[: res.history_len].tolist() if cfg.save_residual_history else [],
+                             res.actual_shift, res.setup_seconds, res.solve_seconds, res.kernel_launches)
+        if self.printrates and r.residual_history:
+            for i, v in enumerate(r.residual_history):
+                print(f"{self.method} iteration {i}, residual = {v}")
+            state = "converged in" if r.converged else "NOT converged after"
+            print(f"{self.method} {state} {r.iterations} iterations, residual = {r.final_residual}")
+        self._last = r
+        return r
+
+    def Mult(self, x, y):
+        """y = A^{-1} x with zero initial guess (BaseMatrix::Mult)."""
+        yv = _vec_view(y)
+        yv[...] = 0
+        self.Solve(x, yv)
+
+    def __mul__(self, vec):
+        y = np.zeros(self._mat.n, dtype=self._mat.dtype)
+        self.Mult(vec, y)
+        return y
+
+    def MultAdd(self, s, x, y):
+        t = self * x
+        yv = _vec_view(y)
+        yv += s * t
+
+    @property
+    def height(self):
+        return self._mat.n
+
+    @property
+    def width(self):
+        return self._mat.m
+
+    def IsComplex(self):
+        return self._cplx
+
+    @property
+    def last_result(self):
+        return self._last
+
+    # -- properties (sparsesolv_python_export.hpp:101-156) ---------------------
+    def _get(self, f):
+        return getattr(self._cfg, f)
+
+    def _set(self, f, v):
+        setattr(self._cfg, f, v)
+
+    tol = property(lambda s: s._cfg.tolerance, lambda s, v: s._set("tolerance", float(v)))
+    maxiter = property(lambda s: s._cfg.max_iterations, lambda s, v: s._set("max_iterations", int(v)))
+    shift = property(lambda s: s._cfg.shift_parameter, lambda s, v: s._set("shift_parameter", float(v)))
+    save_best_result = property(lambda s: bool(s._cfg.save_best_result),
+                                lambda s, v: s._set("save_best_result", int(bool(v))))
+    save_residual_history = property(lambda s: bool(s._cfg.save_residual_history),
+                                     lambda s, v: s._set("save_residual_history", int(bool(v))))
+    auto_shift = property(lambda s: bool(s._cfg.auto_shift), lambda s, v: s._set("auto_shift", int(bool(v))))
+    diagonal_scaling = property(lambda s: bool(s._cfg.diagonal_scaling),
+                                lambda s, v: s._set("diagonal_scaling", int(bool(v))))
+    divergence_check = property(lambda s: bool(s._cfg.divergence_check),
+                                lambda s, v: s._set("divergence_check", int(bool(v))))
+    divergence_threshold = property(lambda s: s._cfg.divergence_threshold,
+                                    lambda s, v: s._set("divergence_threshold", float(v)))
+    divergence_count = property(lambda s: s._cfg.divergence_count,
+                                lambda s, v: s._set("divergence_count", int(v)))
+    conjugate = property(lambda s: bool(s._cfg.conjugate), lambda s, v: s._set("conjugate", int(bool(v))))
+    use_abmc = property(lambda s: bool(s._cfg.use_abmc), lambda s, v: s._set("use_abmc", int(bool(v))))
+    abmc_block_size = property(lambda s: s._cfg.abmc_block_size, lambda s, v: s._set("abmc_block_size", int(v)))
+    abmc_num_colors = property(lambda s: s._cfg.abmc_num_colors, lambda s, v: s._set("abmc_num_colors", int(v)))
+    abmc_reorder_spmv = property(lambda s: bool(s._cfg.abmc_reorder_spmv),
+                                 lambda s, v: s._set("abmc_reorder_spmv", int(bool(v))))
+    abmc_use_rcm = property(lambda s: bool(s._cfg.abmc_use_rcm),
+                            lambda s, v: s._set("abmc_use_rcm", int(bool(v))))
+    # new knob: FP32 storage of the preconditioner ("fp64" | "fp32")
+    precision = property(lambda s: "fp32" if s._cfg.precision == _capi.SSV_PREC_FP32 else "fp64",
+                         lambda s, v: s._set("precision", _capi.SSV_PREC_FP32 if str(v).lower() == "fp32"
+                                             else _capi.SSV_PREC_FP64))
+
+
+class SparseSolvSolverD(_SparseSolvSolverBase):
+    _cplx = False
+
+
+class SparseSolvSolverC(_SparseSolvSolverBase):
+    _cplx = True
+
+
+def SparseSolvSolver(mat, method="ICCG", freedofs=None, tol=1e-10, maxiter=1000, shift=1.05,
+                     save_best_result=True, save_residual_history=False, printrates=False, conjugate=False,
+                     use_abmc=False, abmc_block_size=4, abmc_num_colors=4, abmc_reorder_spmv=False,
+                     abmc_use_rcm=False):
+    """Iterative solver (ICCG / SGSMRTR / CG / COCR). Auto-detects real/complex.
+
+    Factory of sparsesolv_python_export.hpp:242-294 (same arguments and
+    defaults); returns SparseSolvSolverD or SparseSolvSolverC.
+    """
+    ip, ix, data, cplx, shape = _csr_arrays(mat)
+    cls = SparseSolvSolverC if cplx else SparseSolvSolverD
+    s = cls(mat, method, freedofs, tol, maxiter, shift, save_best_result, save_residual_history, printrates)
+    s.conjugate = conjugate
+    s.use_abmc = use_abmc
+    s.abmc_block_size = abmc_block_size
+    s.abmc_num_colors = abmc_num_colors
+    s.abmc_reorder_spmv = abmc_reorder_spmv
+    s.abmc_use_rcm = abmc_use_rcm
+    return s
+
+
+# ---------------------------------------------------------------------------
+# ICPreconditioner (ngsolve/sparsesolv_precond.hpp:177-224)
+# ---------------------------------------------------------------------------
+
+class _PrecondBase:
+    """Common part of the preconditioner handles (BaseMatrix-like)."""
+
+    _cplx = False
+
+    def _init_handle(self, h):
+        self._h = h
+        self._lib = _capi.load()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self._lib.ssv_precond_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def Mult(self, x, y):
+        xv = np.ascontiguousarray(_vec_view(x), dtype=self._dtype)
+        yv = _vec_view(y)
+        out = np.empty(self._n, dtype=self._dtype)
+        check(self._lib.ssv_precond_apply(self._h, _capi.vptr(xv), _capi.vptr(out)))
+        yv[...] = out
+
+    def MultTrans(self, x, y):
+        self.Mult(x, y)
+
+    def MultAdd(self, s, x, y):
+        t = self * x
+        yv = _vec_view(y)
+        if self._fd is not None:
+            yv += s * np.where(self._fd.astype(bool), t, 0)
+        else:
+            yv += s * t
+
+    def __mul__(self, vec):
+        y = np.zeros(self._n, dtype=self._dtype)
+        self.Mult(vec, y)
+        return y
+
+    @property
+    def height(self):
+        return self._n
+
+    @property
+    def width(self):
+        return self._n
+
+    def IsComplex(self):
+        return self._cplx
+
+
+class _ICPreconditionerBase(_PrecondBase):
+    def __init__(self, mat, freedofs=None, shift=1.05):
+        self._mat = _Matrix(mat)
+        self._n = self._mat.n
+        self._dtype = self._mat.dtype
+        self._fd = _freedofs_array(freedofs, self._n)
+        self._shift = float(shift)
+        self._cfg = _capi.default_config(shift_parameter=self._shift)
+        lib = _capi.load()
+        h = ctypes.c_void_p()
+        check(lib.ssv_ic_create(self._mat.h, _capi.u8ptr(self._fd), self._shift, ctypes.byref(h)))
+        self._init_handle(h)
+
+    def _sync(self):
+        self._cfg.shift_parameter = self._shift
+        check(self._lib.ssv_ic_set_config(self._h, ctypes.byref(self._cfg)))
+
+    def Update(self):
+        """Re-read the matrix and refactorise (SparseSolvICPreconditioner::Update)."""
+        self._mat.refresh()
+        self._sync()
+        check(self._lib.ssv_precond_update(self._h))
+
+    @property
+    def shift(self):
+        return self._shift
+
+    @shift.setter
+    def shift(self, v):
+        self._shift = float(v)
+        self._sync()
+
+    use_abmc = property(lambda s: bool(s._cfg.use_abmc),
+                        lambda s, v: (setattr(s._cfg, "use_abmc", int(bool(v))), s._sync()))
+    abmc_block_size = property(lambda s: s._cfg.abmc_block_size,
+                               lambda s, v: (setattr(s._cfg, "abmc_block_size", int(v)), s._sync()))
+    abmc_num_colors = property(lambda s: s._cfg.abmc_num_colors,
+                               lambda s, v: (setattr(s._cfg, "abmc_num_colors", int(v)), s._sync()))
+    diagonal_scaling = property(lambda s: bool(s._cfg.diagonal_scaling),
+                                lambda s, v: (setattr(s._cfg, "diagonal_scaling", int(bool(v))), s._sync()))
+    precision = property(lambda s: "fp32" if s._cfg.precision == _capi.SSV_PREC_FP32 else "fp64",
+                         lambda s, v: (setattr(s._cfg, "precision", _capi.SSV_PREC_FP32
+                                               if str(v).lower() == "fp32" else _capi.SSV_PREC_FP64), s._sync()))
+
+    @property
+    def actual_shift(self):
+        v = ctypes.c_double()
+        check(self._lib.ssv_ic_actual_shift(self._h, ctypes.byref(v)))
+        return v.value
+
+
+class ICPreconditionerD(_ICPreconditionerBase):
+    _cplx = False
+
+
+class ICPreconditionerC(_ICPreconditionerBase):
+    _cplx = True
+
+
+def ICPreconditioner(mat, freedofs=None, shift=1.05):
+    """Incomplete Cholesky (IC) preconditioner; calls Update() (factory :176-207)."""
+    _, _, _, cplx, _ = _csr_arrays(mat)
+    p = (ICPreconditionerC if cplx else ICPreconditionerD)(mat, freedofs, shift)
+    p.Update()
+    return p
+
+
+# ---------------------------------------------------------------------------
+# COCRSolver (ngsolve/sparsesolv_solvers.hpp:255-396)
+# ---------------------------------------------------------------------------
+
+class _COCRSolverBase:
+    _cplx = False
+
+    def __init__(self, mat, pre, freedofs=None, maxiter=500, tol=1e-8, printrates=False):
+        self._mat = mat if isinstance(mat, _Matrix) else _Matrix(mat)
+        self._pre = pre
+        self._fd = _freedofs_array(freedofs, self._mat.n)
+        self.maxiter = int(maxiter)
+        self.tol = float(tol)
+        self.printrates = bool(printrates)
+        self._iterations = 0
+        self._lib = _capi.load()
+
+    @property
+    def iterations(self):
+        return self._iterations
+
+    def Mult(self, rhs, sol):
+        b = np.ascontiguousarray(_vec_view(rhs), dtype=self._mat.dtype)
+        sv = _vec_view(sol)
+        x = np.zeros(self._mat.n, dtype=self._mat.dtype)
+        it = ctypes.c_int32(0)
+        pre_h = None
+        if self._pre is not None:
+            pre_h = self._pre._h
+        self._mat.refresh()
+        check(self._lib.ssv_cocr_solve(self._mat.h, pre_h, _capi.u8ptr(self._fd), self.maxiter, self.tol,
+                                       1 if self.printrates else 0, _capi.vptr(b), _capi.vptr(x),
+                                       ctypes.byref(it)))
+        self._iterations = it.value
+        sv[...] = x
+
+    def __mul__(self, vec):
+        y = np.zeros(self._mat.n, dtype=self._mat.dtype)
+        self.Mult(vec, y)
+        return y
+
+    @property
+    def height(self):
+        return self._mat.n
+
+    @property
+    def width(self):
+        return self._mat.m
+
+    def IsComplex(self):
+        return self._cplx
+
+
+class COCRSolverD(_COCRSolverBase):
+    _cplx = False
+
+
+class COCRSolverC(_COCRSolverBase):
+    _cplx = True
+
+
+def COCRSolver(mat, pre, freedofs=None, maxiter=500, tol=1e-8, printrates=False):
+    """COCR for complex-symmetric systems with an external preconditioner (factory :577-599)."""
+    m = mat if isinstance(mat, _Matrix) else _Matrix(mat)
+    cls = COCRSolverC if m.cplx else COCRSolverD
+    return cls(m, pre, freedofs, maxiter, tol, printrates)
+
+
+def has_compact_ams():
+    """True when Compact AMG/AMS support is available."""
+    return False

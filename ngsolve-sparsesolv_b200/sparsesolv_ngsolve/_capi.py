@@ -74,7 +74,25 @@ class ssv_result(ctypes.Structure):
         ("actual_shift", ctypes.c_double),
         ("setup_seconds", ctypes.c_double),
         ("solve_seconds", ctypes.c_double),
+        ("kernel_launches", ctypes.c_int64),
     ]
+
+
+SSV_MAX_PHASES = 8
+
+
+class ssv_phase_profile(ctypes.Structure):
+    _fields_ = [
+        ("num_phases", ctypes.c_int32),
+        ("names", (ctypes.c_char * 24) * SSV_MAX_PHASES),
+        ("ms", ctypes.c_double * SSV_MAX_PHASES),
+        ("bytes", ctypes.c_double * SSV_MAX_PHASES),
+        ("kernels", ctypes.c_int32 * SSV_MAX_PHASES),
+    ]
+
+    def as_list(self):
+        return [{"name": self.names[i].value.decode(), "ms": self.ms[i], "bytes": self.bytes[i],
+                 "kernels": self.kernels[i]} for i in range(self.num_phases)]
 
 
 def default_config(**overrides) -> ssv_config:
@@ -143,6 +161,8 @@ SIGNATURES = [
                                ctypes.POINTER(ssv_result), PD, I32]),
     ("ssv_solver_solve_dev", I32, [P, ctypes.c_char_p, ctypes.POINTER(ssv_config), P, P,
                                    ctypes.POINTER(ssv_result), PD, I32]),
+    ("ssv_solver_profile", I32, [P, ctypes.c_char_p, ctypes.POINTER(ssv_config), I32,
+                                 ctypes.POINTER(ssv_phase_profile)]),
     ("ssv_ic_create", I32, [P, PU8, ctypes.c_double, PP]),
     ("ssv_ic_set_config", I32, [P, ctypes.POINTER(ssv_config)]),
     ("ssv_precond_update", I32, [P]),

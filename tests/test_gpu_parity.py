@@ -1,0 +1,184 @@
+"""Parity of the sm_100a path against the reference (golden fixtures made by
+the reference's own headers) and the oracle, through the C ABI / Python API.
+
+Bars: iteration count within +/-2% of the reference's (equal on these small
+cases), solution within 1e-8 relative (max-norm), true residual <= tol where
+converged."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_cases, golden_system
+
+pytestmark = pytest.mark.gpu
+
+X_RTOL = 1e-8
+
+
+def _solver(A, method, fd, items):
+    import sparsesolv_ngsolve as ss
+    d = dict(items)
+    s = ss.SparseSolvSolver(A, method=method, freedofs=fd, tol=d["tolerance"], maxiter=d["max_iterations"],
+                            shift=d["shift_parameter"], save_best_result=bool(d["save_best_result"]),
+                            save_residual_history=bool(d["save_residual_history"]),
+                            conjugate=bool(d["conjugate"]), use_abmc=bool(d["use_abmc"]),
+                            abmc_block_size=d["abmc_block_size"], abmc_num_colors=d["abmc_num_colors"],
+                            abmc_reorder_spmv=bool(d["abmc_reorder_spmv"]))
+    s.auto_shift = bool(d["auto_shift"])
+    s.diagonal_scaling = bool(d["diagonal_scaling"])
+    s.divergence_check = bool(d["divergence_check"])
+    s.divergence_threshold = d["divergence_threshold"]
+    s.divergence_count = d["divergence_count"]
+    s._cfg.min_diagonal_threshold = d["min_diagonal_threshold"]
+    return s
+
+
+def _cases():
+    g = np.load(__import__("conftest").GOLDEN)
+    return golden_cases(g)
+
+
+@pytest.mark.parametrize("case,sysname,method,items", _cases(), ids=[c[0] for c in _cases()])
+def test_golden_case(golden, case, sysname, method, items):
+    A, b, fd = golden_system(golden, sysname)
+    s = _solver(A, method, fd, items)
+    x = np.zeros(A.shape[0], dtype=A.dtype)
+    r = s.Solve(b, x)
+    conv, iters, fres = golden[f"case/{case}/meta"]
+    xr = golden[f"case/{case}/x"]
+    assert r.converged == bool(conv)
+    assert abs(r.iterations - int(iters)) <= max(0, int(0.02 * iters))
+    assert np.abs(x - xr).max() <= X_RTOL * np.abs(xr).max()
+    hr = golden[f"case/{case}/hist"]
+    assert len(r.residual_history) == len(hr)
+    np.testing.assert_allclose(r.residual_history, hr, rtol=1e-5, atol=1e-9)
+    np.testing.assert_allclose(r.final_residual, fres, rtol=1e-5, atol=1e-14)
+    # SGS-MRTR stops on the preconditioned residual ||rd||/||L b2||
+    # (sgs_mrtr_solver.hpp:118-121,229-230), not on the true residual
+    if r.converged and method != "SGSMRTR":
+        bb = b if fd is None else np.where(fd.astype(bool), b, 0)
+        # true residual on the free DOFs of the BC-modified system
+        Am = A.tolil()
+        if fd is not None:
+            free = fd.astype(bool)
+            Am = A.multiply(np.outer(free, free)).tolil()
+            for i in np.where(~free)[0]:
+                Am[i, i] = 1.0
+        xx = x if fd is None else np.where(fd.astype(bool), x, 0)
+        tres = np.linalg.norm(bb - Am.tocsr() @ xx) / np.linalg.norm(bb)
+        assert tres <= 10 * items_dict(items)["tolerance"] + 1e-12
+
+
+def items_dict(items):
+    return dict(items)
+
+
+@pytest.mark.parametrize("sysname", ["lap3d_6", "lap3d_8_fd", "cplx3d_8_fd"])
+@pytest.mark.parametrize("kind", ["abmc", "level"])
+def test_ic_preconditioner_mult(golden, sysname, kind):
+    import sparsesolv_ngsolve as ss
+    A, b, fd = golden_system(golden, sysname)
+    p = ss.ICPreconditioner(A, freedofs=fd, shift=1.05)
+    if kind == "abmc":
+        p.use_abmc = True
+        p.Update()
+    y = p * b
+    yr = golden[f"icmult/{sysname}/{kind}"]
+    assert np.abs(y - yr).max() <= 1e-12 * np.abs(yr).max()
+
+
+def test_config1_iccg_abmc_full_size():
+    """64^3 7-point Laplacian, ICCG + ABMC (block 4, 4 colours), tol 1e-10."""
+    import sparsesolv_ngsolve as ss
+    from oracle import oracle as O
+    from sparsesolv_ngsolve import problems as P
+    A = P.laplacian_7pt(64)
+    b = P.random_rhs(A.shape[0], 0)
+    s = ss.SparseSolvSolver(A, method="ICCG", tol=1e-10, maxiter=2000, shift=1.05, use_abmc=True,
+                            abmc_block_size=4, abmc_num_colors=4)
+    x = np.zeros_like(b)
+    r = s.Solve(b, x)
+    xo, ro, _ = O.solve(A, b, "ICCG", O.default_config(use_abmc=1, max_iterations=2000), which="port")
+    assert r.converged and ro.converged
+    assert abs(r.iterations - ro.iterations) <= int(0.02 * ro.iterations)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= X_RTOL
+    assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) <= 1e-10
+
+
+def test_deterministic_reruns():
+    import sparsesolv_ngsolve as ss
+    from sparsesolv_ngsolve import problems as P
+    A = P.laplacian_7pt(20)
+    b = P.random_rhs(A.shape[0], 5)
+    s = ss.SparseSolvSolver(A, method="ICCG", use_abmc=True)
+    x1 = np.zeros_like(b)
+    x2 = np.zeros_like(b)
+    r1 = s.Solve(b, x1)
+    r2 = s.Solve(b, x2)
+    assert r1.iterations == r2.iterations
+    assert np.array_equal(x1, x2)
+
+
+@pytest.mark.parametrize("method", ["ICCG", "CG", "COCR", "SGSMRTR"])
+def test_graph_chunk_mode_matches_while_mode(method, monkeypatch):
+    import sparsesolv_ngsolve as ss
+    from sparsesolv_ngsolve import problems as P
+    A = P.laplacian_7pt(12)
+    b = P.random_rhs(A.shape[0], 9)
+    s = ss.SparseSolvSolver(A, method=method, use_abmc=True)
+    x1 = np.zeros_like(b)
+    r1 = s.Solve(b, x1)
+    monkeypatch.setenv("SSV_GRAPH_MODE", "chunk")
+    x2 = np.zeros_like(b)
+    r2 = s.Solve(b, x2)
+    assert r1.iterations == r2.iterations
+    assert np.array_equal(x1, x2)
+
+
+def test_fp32_preconditioner_form():
+    """FP32 storage of L: same tolerance reached; error vs the FP64 solution stated."""
+    import sparsesolv_ngsolve as ss
+    from sparsesolv_ngsolve import problems as P
+    A = P.laplacian_7pt(24)
+    b = P.random_rhs(A.shape[0], 1)
+    s = ss.SparseSolvSolver(A, method="ICCG", use_abmc=True)
+    x64 = np.zeros_like(b)
+    r64 = s.Solve(b, x64)
+    s.precision = "fp32"
+    x32 = np.zeros_like(b)
+    r32 = s.Solve(b, x32)
+    assert r32.converged
+    assert abs(r32.iterations - r64.iterations) <= 3
+    assert np.linalg.norm(x32 - x64) / np.linalg.norm(x64) < 1e-8
+    assert np.linalg.norm(b - A @ x32) / np.linalg.norm(b) <= 1e-10
+
+
+def test_cocr_solver_with_ic_matches_oracle():
+    import sparsesolv_ngsolve as ss
+    from oracle import oracle as O
+    from sparsesolv_ngsolve import problems as P
+    A = P.complex_shifted(P.laplacian_7pt(8), 0.2 + 1.0j)
+    b = P.random_rhs(A.shape[0], 4, np.complex128)
+    fd = P.boundary_freedofs_7pt(8)
+    pre = ss.ICPreconditioner(A, freedofs=fd)
+    inv = ss.COCRSolver(A, pre, freedofs=fd, maxiter=500, tol=1e-10)
+    x = inv * b
+    cfg = O.default_config()
+    xo, it = O.cocr_solve(A, b, precond=lambda v: O.ic_mult(A, v, cfg, freedofs=fd)[0], freedofs=fd,
+                          maxiter=500, tol=1e-10)
+    assert inv.iterations == it
+    assert np.abs(x - xo).max() <= X_RTOL * np.abs(xo).max()
+
+
+def test_cocr_solver_identity_preconditioner():
+    import sparsesolv_ngsolve as ss
+    from oracle import oracle as O
+    from sparsesolv_ngsolve import problems as P
+    A = P.complex_shifted(P.laplacian_7pt(7), 0.5 + 0.5j)
+    b = P.random_rhs(A.shape[0], 2, np.complex128)
+    inv = ss.COCRSolver(A, None, maxiter=300, tol=1e-9)
+    x = inv * b
+    xo, it = O.cocr_solve(A, b, None, maxiter=300, tol=1e-9)
+    assert inv.iterations == it
+    assert np.abs(x - xo).max() <= X_RTOL * np.abs(xo).max()
