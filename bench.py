@@ -262,6 +262,7 @@ def main():
     clocks = ClockSampler(local)
     clocks.start()
     step_ms, launches, iters, conv = [], 0, 0, True
+    setup_s, solve_s = [], []
     for _ in range(args.steps):
         flush.fill_(1.0)
         torch.cuda.synchronize()
@@ -273,6 +274,8 @@ def main():
         torch.cuda.synchronize()
         step_ms.append(e0.elapsed_time(e1))
         launches += r.kernel_launches
+        setup_s.append(r.setup_seconds)
+        solve_s.append(r.solve_seconds)
         iters = r.iterations
         conv = conv and bool(r.converged)
     torch.cuda.synchronize()
@@ -350,6 +353,7 @@ def main():
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(desc, iterations=iters, converged=conv, parallelism=f"replicas{world}",
                            l2="flushed between timed steps (256 MB write)",
+                           cold_setup_s=statistics.mean(setup_s), cold_iterate_s=statistics.mean(solve_s),
                            warm_time_to_solution_s=statistics.mean(warm_ms) / 1e3,
                            ms_per_iter_warm=statistics.mean(warm_ms) / max(iters, 1),
                            true_rel_residual=true_res),

@@ -649,4 +649,49 @@ __global__ void k_gather_or_zero(int64_t m, const int* __restrict__ map, const S
     }
 }
 
+// ---------------------------------------------------------------------------
+// Oversized ABMC blocks (the aggregation's leftover rows): one CTA walks the
+// block's level sets, rows of a level in parallel, __syncthreads() between
+// levels (global writes of the CTA are visible to it after the barrier).
+// lev[0..nlev] are offsets into rows[].
+// ---------------------------------------------------------------------------
+template <typename S, typename SL>
+__global__ void __launch_bounds__(256)
+k_ic_fwd_cta(int nlev, const int* __restrict__ lev, const int* __restrict__ rows, const int* __restrict__ Lrp,
+             const int* __restrict__ Lci, const SL* __restrict__ Lv, const S* __restrict__ x,
+             const double* __restrict__ sc, S* y, const KState* st) {
+    if (st && st->done) return;
+    for (int l = 0; l < nlev; ++l) {
+        const int q1 = lev[l + 1];
+        for (int q = lev[l] + threadIdx.x; q < q1; q += blockDim.x) {
+            const int i = rows[q];
+            S s = x[i];
+            if (sc) s = ST<S>::scale(sc[i], s);
+            const int ke = Lrp[i + 1] - 1;
+            for (int k = Lrp[i]; k < ke; ++k) s = s - hi_of_any(Lv[k]) * y[Lci[k]];
+            y[i] = ST<S>::div(s, hi_of_any(Lv[ke]));
+        }
+        __syncthreads();
+    }
+}
+
+template <typename S, typename SL>
+__global__ void __launch_bounds__(256)
+k_ic_bwd_cta(int nlev, const int* __restrict__ lev, const int* __restrict__ rows, const int* __restrict__ Urp,
+             const int* __restrict__ Uci, const SL* __restrict__ Uv, const SL* __restrict__ inv_diag,
+             const S* __restrict__ x, S* y, const KState* st) {
+    if (st && st->done) return;
+    for (int l = 0; l < nlev; ++l) {
+        const int q1 = lev[l + 1];
+        for (int q = lev[l] + threadIdx.x; q < q1; q += blockDim.x) {
+            const int i = rows[q];
+            S s = ST<S>::zero();
+            const int ke = Urp[i + 1];
+            for (int k = Urp[i] + 1; k < ke; ++k) s = s - hi_of_any(Uv[k]) * y[Uci[k]];
+            y[i] = s * hi_of_any(inv_diag[i]) + x[i];
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace ssv

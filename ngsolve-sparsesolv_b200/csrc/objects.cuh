@@ -111,6 +111,7 @@ struct ICDevice {
     int num_colors = 0, num_blocks = 0, num_levels_f = 0, num_levels_b = 0;
     std::vector<int> h_perm;           // ordering[old] = new (ABMC)
     std::vector<int> h_boff;           // ABMC block row offsets
+    std::vector<int> sched_color_offsets;
     DevBuf<int> perm;
     // working matrix in ABMC numbering (values gathered through Asrc)
     std::vector<int> h_Arp;
@@ -132,6 +133,14 @@ struct ICDevice {
     // L and U rows, packed strictly-lower intra-block table, diagonal
     bool blk = false;
     int blk_lanes = 0, tri = 1;
+    // launches of the block sweeps in processing order: kind 0 = range of
+    // ordinary blocks [a, b) (sub-warp kernels), kind 1 = range [a, b) of the
+    // rows_f / rows_b lists (one level of an oversized block; factorisation),
+    // kind 2 = an oversized block swept by one CTA over the level offsets
+    // lev_f / lev_b [a, b] (apply)
+    struct Launch { int kind, a, b; };
+    std::vector<Launch> fwd_blk, bwd_blk, fwd_cta, bwd_cta;
+    DevBuf<int> lev_f, lev_b;
     DevBuf<int> erp, eci, esrc, urpe, ucie, usrce, isrc, dsrc;
     DevBuf<S> ev, uev, iv, dv;
     DevBuf<SL> ev_lo, uev_lo, iv_lo, dv_lo;
@@ -151,6 +160,7 @@ struct ICDevice {
     void apply_fwd(const S* x, const KState* st, cudaStream_t s) const;  // x -> tw
     void apply_bwd(S* y, const KState* st, cudaStream_t s) const;        // tw -> y
     int kernels_per_apply() const {
+        if (blk) return (int)(fwd_cta.size() + bwd_cta.size()) + (scaled_apply ? 1 : 0);
         return (int)(fwd_launch.size() + bwd_launch.size()) + (scaled_apply ? 1 : 0);
     }
 };

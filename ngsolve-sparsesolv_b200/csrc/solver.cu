@@ -174,6 +174,7 @@ void ICDevice<S>::build_pattern(int n_, const std::vector<int>& rp, const std::v
         perm.upload(h_perm.data(), h_perm.size(), s);
         uoff.upload(sched.block_offsets.data(), sched.block_offsets.size(), s);
         h_boff = sched.block_offsets;
+        sched_color_offsets = sched.color_offsets;
         rows_f.release();
         rows_b.release();
         for (int c = 0; c < num_colors; ++c)
@@ -220,49 +221,123 @@ void ICDevice<S>::build_pattern(int n_, const std::vector<int>& rp, const std::v
     tw.alloc(n);
     if (!flag.get()) flag.alloc(1);
     blk = false;
-    if (abmc && missing_row < 0) {
+    fwd_blk.clear();
+    bwd_blk.clear();
+    fwd_cta.clear();
+    bwd_cta.clear();
+    if (abmc && missing_row < 0 && cfg.abmc_block_size <= 32) {
+        // Ordinary blocks hold <= block_size rows; the aggregation appends any
+        // rows it could not place to the last block
+        // (abmc_ordering.hpp:217-226), which can be far larger. Such a block
+        // is swept row-parallel by its own intra-block level sets.
         const std::vector<int>& bo = h_boff;
+        const int cap = std::max(1, cfg.abmc_block_size);
         int bsmax = 1;
-        for (int b = 0; b < num_blocks; ++b) bsmax = std::max(bsmax, bo[b + 1] - bo[b]);
-        if (bsmax <= 32) {
-            blk = true;
-            blk_lanes = 1;
-            while (blk_lanes < bsmax) blk_lanes <<= 1;
-            tri = std::max(1, bsmax * (bsmax - 1) / 2);
-            std::vector<int> h_erp(n + 1, 0), h_eci, h_esrc, h_urp(n + 1, 0), h_uci, h_usrc, h_dsrc(n);
-            std::vector<int> h_isrc((size_t)num_blocks * tri, -1);
-            h_eci.reserve(lci.size());
-            h_esrc.reserve(lci.size());
-            h_uci.reserve(uci.size());
-            h_usrc.reserve(uci.size());
-            for (int b = 0; b < num_blocks; ++b) {
-                const int r0 = bo[b], r1 = bo[b + 1];
-                for (int i = r0; i < r1; ++i) {
-                    for (int k = lrp[i]; k < lrp[i + 1] - 1; ++k) {
-                        const int c = lci[k];
-                        if (c < r0) { h_eci.push_back(c); h_esrc.push_back(k); }
-                        else {
-                            const int j = i - r0, t = c - r0;
-                            h_isrc[(size_t)b * tri + j * (j - 1) / 2 + t] = k;
-                        }
+        for (int b = 0; b < num_blocks; ++b) {
+            const int sz = bo[b + 1] - bo[b];
+            if (sz <= cap) bsmax = std::max(bsmax, sz);
+        }
+        blk = true;
+        blk_lanes = 1;
+        while (blk_lanes < bsmax) blk_lanes <<= 1;
+        tri = std::max(1, bsmax * (bsmax - 1) / 2);
+        std::vector<int> h_erp(n + 1, 0), h_eci, h_esrc, h_urp(n + 1, 0), h_uci, h_usrc, h_dsrc(n);
+        std::vector<int> h_isrc((size_t)num_blocks * tri, -1);
+        std::vector<int> h_rows_f, h_rows_b, h_lev_f, h_lev_b;
+        h_eci.reserve(lci.size());
+        h_esrc.reserve(lci.size());
+        h_uci.reserve(uci.size());
+        h_usrc.reserve(uci.size());
+        std::vector<int> lev;
+        for (int b = 0; b < num_blocks; ++b) {
+            const int r0 = bo[b], r1 = bo[b + 1];
+            const bool big = (r1 - r0) > cap;
+            for (int i = r0; i < r1; ++i) {
+                for (int k = lrp[i]; k < lrp[i + 1] - 1; ++k) {
+                    const int c = lci[k];
+                    if (c < r0 || big) { h_eci.push_back(c); h_esrc.push_back(k); }
+                    else {
+                        const int j = i - r0, t = c - r0;
+                        h_isrc[(size_t)b * tri + j * (j - 1) / 2 + t] = k;
                     }
-                    h_erp[i + 1] = (int)h_eci.size();
-                    h_dsrc[i] = lrp[i + 1] - 1;
+                }
+                h_erp[i + 1] = (int)h_eci.size();
+                h_dsrc[i] = lrp[i + 1] - 1;
+                for (int k = urp[i] + 1; k < urp[i + 1]; ++k)
+                    if (uci[k] >= r1 || big) { h_uci.push_back(uci[k]); h_usrc.push_back(usrc[k]); }
+                h_urp[i + 1] = (int)h_uci.size();
+            }
+        }
+        // launch lists: colour by colour; runs of ordinary blocks, and the
+        // level sets of oversized blocks (forward: dependencies on earlier
+        // rows of the block, backward: on later rows)
+        auto add_big = [&](int r0, int r1, bool fwd) {
+            const int m = r1 - r0;
+            lev.assign(m, 0);
+            int nl = 0;
+            if (fwd) {
+                for (int i = r0; i < r1; ++i) {
+                    int d = -1;
+                    for (int k = lrp[i]; k < lrp[i + 1] - 1; ++k)
+                        if (lci[k] >= r0) d = std::max(d, lev[lci[k] - r0]);
+                    lev[i - r0] = d + 1;
+                    nl = std::max(nl, d + 2);
+                }
+            } else {
+                for (int i = r1 - 1; i >= r0; --i) {
+                    int d = -1;
                     for (int k = urp[i] + 1; k < urp[i + 1]; ++k)
-                        if (uci[k] >= r1) { h_uci.push_back(uci[k]); h_usrc.push_back(usrc[k]); }
-                    h_urp[i + 1] = (int)h_uci.size();
+                        if (uci[k] < r1) d = std::max(d, lev[uci[k] - r0]);
+                    lev[i - r0] = d + 1;
+                    nl = std::max(nl, d + 2);
                 }
             }
-            erp.upload(h_erp.data(), h_erp.size(), s);
-            eci.upload(h_eci.data(), h_eci.size(), s);
-            esrc.upload(h_esrc.data(), h_esrc.size(), s);
-            urpe.upload(h_urp.data(), h_urp.size(), s);
-            ucie.upload(h_uci.data(), h_uci.size(), s);
-            usrce.upload(h_usrc.data(), h_usrc.size(), s);
-            isrc.upload(h_isrc.data(), h_isrc.size(), s);
-            dsrc.upload(h_dsrc.data(), h_dsrc.size(), s);
-            ev.alloc(h_eci.size()); uev.alloc(h_uci.size()); iv.alloc(h_isrc.size()); dv.alloc(n);
-        }
+            std::vector<int>& rows = fwd ? h_rows_f : h_rows_b;
+            std::vector<int>& lv = fwd ? h_lev_f : h_lev_b;
+            const int p0 = (int)lv.size();
+            lv.push_back((int)rows.size());
+            for (int l = 0; l < nl; ++l) {
+                const int a = (int)rows.size();
+                for (int i = r0; i < r1; ++i)
+                    if (lev[i - r0] == l) rows.push_back(i);
+                (fwd ? fwd_blk : bwd_blk).push_back({1, a, (int)rows.size()});
+                lv.push_back((int)rows.size());
+            }
+            (fwd ? fwd_cta : bwd_cta).push_back({2, p0, p0 + nl});
+        };
+        auto add_colour = [&](int c, bool fwd) {
+            const int b0 = sched_color_offsets[c], b1 = sched_color_offsets[c + 1];
+            int run = b0;
+            for (int b = b0; b < b1; ++b) {
+                if (bo[b + 1] - bo[b] > cap) {
+                    if (b > run) {
+                        (fwd ? fwd_blk : bwd_blk).push_back({0, run, b});
+                        (fwd ? fwd_cta : bwd_cta).push_back({0, run, b});
+                    }
+                    add_big(bo[b], bo[b + 1], fwd);
+                    run = b + 1;
+                }
+            }
+            if (b1 > run) {
+                (fwd ? fwd_blk : bwd_blk).push_back({0, run, b1});
+                (fwd ? fwd_cta : bwd_cta).push_back({0, run, b1});
+            }
+        };
+        for (int c = 0; c < num_colors; ++c) add_colour(c, true);
+        for (int c = num_colors - 1; c >= 0; --c) add_colour(c, false);
+        erp.upload(h_erp.data(), h_erp.size(), s);
+        eci.upload(h_eci.data(), h_eci.size(), s);
+        esrc.upload(h_esrc.data(), h_esrc.size(), s);
+        urpe.upload(h_urp.data(), h_urp.size(), s);
+        ucie.upload(h_uci.data(), h_uci.size(), s);
+        usrce.upload(h_usrc.data(), h_usrc.size(), s);
+        isrc.upload(h_isrc.data(), h_isrc.size(), s);
+        dsrc.upload(h_dsrc.data(), h_dsrc.size(), s);
+        if (!h_rows_f.empty()) rows_f.upload(h_rows_f.data(), h_rows_f.size(), s);
+        if (!h_rows_b.empty()) rows_b.upload(h_rows_b.data(), h_rows_b.size(), s);
+        if (!h_lev_f.empty()) lev_f.upload(h_lev_f.data(), h_lev_f.size(), s);
+        if (!h_lev_b.empty()) lev_b.upload(h_lev_b.data(), h_lev_b.size(), s);
+        ev.alloc(h_eci.size()); uev.alloc(h_uci.size()); iv.alloc(h_isrc.size()); dv.alloc(n);
     }
     built = true;
     SSV_CUDA(cudaStreamSynchronize(s));
@@ -325,15 +400,27 @@ int ICDevice<S>::factorize(const S* vals, const ssv_config& cfg) {
             SSV_LAUNCH_CHECK();
         }
         flag.zero(s);
-        for (const auto& g : fwd_launch) {
-            const int units = g.second - g.first;
-            if (units <= 0) continue;
-            k_ic_factor<S><<<(units + 127) / 128, 128, 0, s>>>(
-                g.first, g.second, abmc ? uoff.get() : nullptr, abmc ? nullptr : rows_f.get(), Lrp.get(),
-                Lci.get(), Lv.get(), inv.get(), shift, cfg.min_diagonal_threshold,
-                cfg.zero_diagonal_replacement, cfg.auto_shift, flag.get());
-            SSV_LAUNCH_CHECK();
+        if (blk) {
+            for (const auto& g : fwd_blk) {
+                const int units = g.b - g.a;
+                if (units <= 0) continue;
+                k_ic_factor<S><<<(units + 127) / 128, 128, 0, s>>>(
+                    g.a, g.b, g.kind == 0 ? uoff.get() : nullptr, g.kind == 0 ? nullptr : rows_f.get(), Lrp.get(),
+                    Lci.get(), Lv.get(), inv.get(), shift, cfg.min_diagonal_threshold, cfg.zero_diagonal_replacement,
+                    cfg.auto_shift, flag.get());
+            }
+            nk += (int)fwd_blk.size() - (int)fwd_launch.size();
+        } else {
+            for (const auto& g : fwd_launch) {
+                const int units = g.second - g.first;
+                if (units <= 0) continue;
+                k_ic_factor<S><<<(units + 127) / 128, 128, 0, s>>>(
+                    g.first, g.second, abmc ? uoff.get() : nullptr, abmc ? nullptr : rows_f.get(), Lrp.get(),
+                    Lci.get(), Lv.get(), inv.get(), shift, cfg.min_diagonal_threshold,
+                    cfg.zero_diagonal_replacement, cfg.auto_shift, flag.get());
+            }
         }
+        SSV_LAUNCH_CHECK();
         int need = 0;
         SSV_CUDA(cudaMemcpyAsync(&need, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         SSV_CUDA(cudaStreamSynchronize(s));
@@ -381,11 +468,16 @@ template <typename S, typename SL, int L>
 static void launch_fwd_blk(const ICDevice<S>& ic, const SL* ev, const SL* iv, const SL* dv, const S* x,
                            const double* sc, const KState* st, cudaStream_t s) {
     constexpr int per_cta = 128 / L;
-    for (const auto& g : ic.fwd_launch) {
-        const int units = g.second - g.first;
+    const SL* Lfull = ic.lo ? reinterpret_cast<const SL*>(ic.Lv_lo.get()) : reinterpret_cast<const SL*>(ic.Lv.get());
+    for (const auto& g : ic.fwd_cta) {
+        const int units = g.b - g.a;
         if (units <= 0) continue;
-        k_ic_fwd_blk<S, SL, L><<<(units + per_cta - 1) / per_cta, 128, 0, s>>>(
-            g.first, g.second, ic.uoff.get(), ic.erp.get(), ic.eci.get(), ev, iv, ic.tri, dv, x, sc, ic.tw.get(), st);
+        if (g.kind == 0)
+            k_ic_fwd_blk<S, SL, L><<<(units + per_cta - 1) / per_cta, 128, 0, s>>>(
+                g.a, g.b, ic.uoff.get(), ic.erp.get(), ic.eci.get(), ev, iv, ic.tri, dv, x, sc, ic.tw.get(), st);
+        else
+            k_ic_fwd_cta<S, SL><<<1, 256, 0, s>>>(units, ic.lev_f.get() + g.a, ic.rows_f.get(), ic.Lrp.get(),
+                                                  ic.Lci.get(), Lfull, x, sc, ic.tw.get(), st);
     }
 }
 
@@ -393,11 +485,16 @@ template <typename S, typename SL, int L>
 static void launch_bwd_blk(const ICDevice<S>& ic, const SL* uev, const SL* iv, const SL* inv, S* y,
                            const KState* st, cudaStream_t s) {
     constexpr int per_cta = 128 / L;
-    for (const auto& g : ic.bwd_launch) {
-        const int units = g.second - g.first;
+    const SL* Ufull = ic.lo ? reinterpret_cast<const SL*>(ic.Uv_lo.get()) : reinterpret_cast<const SL*>(ic.Uv.get());
+    for (const auto& g : ic.bwd_cta) {
+        const int units = g.b - g.a;
         if (units <= 0) continue;
-        k_ic_bwd_blk<S, SL, L><<<(units + per_cta - 1) / per_cta, 128, 0, s>>>(
-            g.first, g.second, ic.uoff.get(), ic.urpe.get(), ic.ucie.get(), uev, iv, ic.tri, inv, ic.tw.get(), y, st);
+        if (g.kind == 0)
+            k_ic_bwd_blk<S, SL, L><<<(units + per_cta - 1) / per_cta, 128, 0, s>>>(
+                g.a, g.b, ic.uoff.get(), ic.urpe.get(), ic.ucie.get(), uev, iv, ic.tri, inv, ic.tw.get(), y, st);
+        else
+            k_ic_bwd_cta<S, SL><<<1, 256, 0, s>>>(units, ic.lev_b.get() + g.a, ic.rows_b.get(), ic.Urp.get(),
+                                                  ic.Uci.get(), Ufull, inv, ic.tw.get(), y, st);
     }
 }
 
@@ -784,10 +881,12 @@ static void profile_krylov(ssv_solver* sv, int method, const ssv_config& cfg, in
         if (ic) {
             const double ZL = (double)ic->h_Lci.size();
             const double lb = ic->lo ? sizeof(typename ST<S>::lo) : sb;
-            timed("ic_forward", ZL * (4 + lb) + (N + 1) * 4 + 2 * N * sb, (int)ic->fwd_launch.size(),
+            const int kf = ic->blk ? (int)ic->fwd_cta.size() : (int)ic->fwd_launch.size();
+            const int kb = ic->blk ? (int)ic->bwd_cta.size() : (int)ic->bwd_launch.size();
+            timed("ic_forward", ZL * (4 + lb) + (N + 1) * 4 + 2 * N * sb, kf,
                   [&] { ic->apply_fwd(w.r.get(), dst, s); });
             timed("ic_backward", ZL * (4 + lb) + (N + 1) * 4 + N * lb + 2 * N * sb,
-                  (int)ic->bwd_launch.size() + (ic->scaled_apply ? 1 : 0), [&] { ic->apply_bwd(w.z.get(), dst, s); });
+                  kb + (ic->scaled_apply ? 1 : 0), [&] { ic->apply_bwd(w.z.get(), dst, s); });
         }
         timed("dot_beta", 2 * N * sb, 1, [&] {
             k_dot<S><<<g, kBlock, 0, s>>>(n, w.r.get(), z, cfg.conjugate, dst, RED_CG_BETA, red, nullptr);
