@@ -211,6 +211,21 @@ int ssv_abmc_build(int32_t n, const int32_t* row_ptr, const int32_t* col_idx,
 int ssv_level_schedule(int32_t n, const int32_t* row_ptr, const int32_t* col_idx,
                        int32_t upper, int32_t* level_of, int32_t* num_levels);
 
+/* ---- allocation-free SpMV + dot (no counterpart in the reference) -------- */
+/* y = A x and *d_dot = x^T y for a real CSR matrix (int32 row_ptr/col_idx,
+ * double values), every pointer in device memory, for callers that must not
+ * allocate device memory (a framework that owns the device's memory pool, a
+ * fixed memory budget, a real-time loop where an allocation could stall or
+ * fail). It calls no cudaMalloc/cudaFree or allocating library routine: its
+ * scratch (one partial sum per 32 rows plus a counter) is a fixed ~512 KB
+ * array inside the library, held by every GPU that loads it until exit.
+ * Limit: rows <= 2,097,152 (larger sizes fail with SSV_ERR_INVALID_ARG).
+ * The first call on a device looks up the array's device address (make it
+ * before any stream capture); calls that overlap on the GPU share the array
+ * and race. Runs on the default stream and is synchronous on return. */
+int ssv_spmv_dot_noalloc(int32_t rows, const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                         const double* d_values, const double* d_x, double* d_y, double* d_dot);
+
 #ifdef __cplusplus
 }
 #endif

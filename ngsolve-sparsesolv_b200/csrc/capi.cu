@@ -387,3 +387,12 @@ int ssv_level_schedule(int32_t n, const int32_t* row_ptr, const int32_t* col_idx
 }
 
 }  // extern "C"
+
+// Error text for ssv_spmv_dot_noalloc (noalloc.cu), which reports through the
+// same thread-local message as every other entry point.
+namespace ssv {
+const char* noalloc_set_error(const std::string& m) {
+    g_last_error = m;
+    return g_last_error.c_str();
+}
+}  // namespace ssv
