@@ -195,6 +195,43 @@ int ssv_cocr_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs,
                        int32_t maxiter, double tol, int32_t printrates,
                        const void* d_b, void* d_x, int32_t* iterations);
 
+/* ---- Compact AMS (include/sparsesolv/preconditioners/compact_ams.hpp,
+ *      complex_compact_ams.hpp; factories sparsesolv_python_export.hpp:410-530) */
+/* CompactAMS(mat, grad, freedofs, coord_x/y/z, cycle_type, num_smooth,
+ * theta, print_level, correction_weight) ctor + Setup (compact_ams.hpp:53-77,
+ * 243-271), or with complex_form != 0 ComplexCompactAMS (complex_compact_ams.hpp:
+ * 31-89): A is the real HCurl (auxiliary) matrix, G the discrete gradient
+ * (rows = HCurl DOFs, cols = H1 DOFs), coordinates of the H1 vertices. The
+ * complex form applies to complex vectors of length ndof_complex (0 = rows of
+ * A). Applied with ssv_precond_apply[_dev]; used by ssv_pcg_solve and
+ * ssv_cocr_solve. */
+int ssv_ams_create(ssv_matrix* A, ssv_matrix* G, const uint8_t* freedofs,
+                   const double* coord_x, const double* coord_y, const double* coord_z,
+                   int32_t cycle_type, int32_t num_smooth, double theta,
+                   double correction_weight, int32_t complex_form, int32_t ndof_complex,
+                   ssv_precond** out);
+/* Update() / Update(new_mat) (compact_ams.hpp:82-97): rebuild the matrix part
+ * (BC matrix, Galerkin products, AMG hierarchies) keeping the geometry.
+ * new_A may be NULL (re-read A's current values). Dimension mismatch ->
+ * SSV_ERR_INVALID_ARG (the reference's std::invalid_argument). */
+int ssv_ams_update(ssv_precond* p, ssv_matrix* new_A);
+/* Hierarchy of subspace s (0 = gradient, 1..3 = Nedelec x, y, z): per level
+ * rows and nnz into sizes[2l], sizes[2l+1]. */
+int ssv_ams_levels(const ssv_precond* p, int32_t subspace, int32_t* sizes, int32_t cap,
+                   int32_t* num_levels);
+
+/* ---- CG with an external preconditioner (new: the reference's AMS scripts
+ *      drive it with NGSolve's krylovspace.CGSolver) ---------------------------
+ * The sparsesolv::CGSolver recurrence (solvers/cg_solver.hpp:64-146,
+ * iterative_solver.hpp:135-279) on the FreeDofs view of A, z = M^{-1} r by
+ * pre (NULL = identity); x is the initial guess on entry (free entries) and
+ * the solution on return. */
+int ssv_pcg_solve(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, const ssv_config* cfg,
+                  const void* b, void* x, ssv_result* res, double* history, int32_t history_cap);
+int ssv_pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, const ssv_config* cfg,
+                      const void* d_b, void* d_x, ssv_result* res, double* history,
+                      int32_t history_cap);
+
 /* ---- host-side set-up logic exposed for parity checks (no device work) --- */
 /* ABMCSchedule::build (include/sparsesolv/core/abmc_ordering.hpp:83-121).
  * color_offsets needs room for n+1 entries, block_offsets n+1, ordering and

@@ -1,0 +1,50 @@
+// amg_setup.hpp -- host set-up of the Compact AMS / AMG hierarchy
+// (include/sparsesolv/preconditioners/compact_amg.hpp:66-156,292-632 and
+// compact_ams.hpp:243-504,605-659). Produces the matrices the device cycle
+// applies; runs once per Update().
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace ssv {
+
+struct HostCsr {
+    int n = 0, m = 0;
+    std::vector<int> rp, ci;
+    std::vector<double> v;
+    int nnz() const { return rp.empty() ? 0 : rp[n]; }
+};
+
+HostCsr csr_transpose(const HostCsr& A);
+// P^T A P with the structural product pattern (explicit zeros kept, columns
+// sorted) -- the semantics of NGSolve's SparseMatrix::Restrict.
+HostCsr csr_rap(const HostCsr& A, const HostCsr& P);
+
+struct AmgHostLevel {
+    HostCsr A, P, Pt;
+    std::vector<double> l1;
+    bool direct = false;          // coarsest: solved with the dense pseudo-inverse
+    std::vector<double> inv;      // n x n row-major pseudo-inverse (direct only)
+};
+
+struct AmgHost {
+    double theta = 0.25;
+    int max_levels = 25, min_coarse = 500, num_smooth = 1;
+    std::vector<AmgHostLevel> levels;
+    void setup(const HostCsr& A0);
+};
+
+struct AmsHost {
+    int nhc = 0, nh1 = 0;
+    HostCsr A_bc, G, Gt, Pi[3], Pit[3];
+    std::vector<double> fine_l1;
+    AmgHost amg[4];  // 0 = gradient space, 1..3 = Nedelec interpolation x, y, z
+    double theta = 0.25;
+    // Geometry (Pi from G and the vertex coordinates), once.
+    void setup_geometry(const HostCsr& grad, const double* cx, const double* cy, const double* cz);
+    // Matrix part: A_bc, Galerkin products, AMG hierarchies, fine l1 norms.
+    void rebuild(const HostCsr& A, const uint8_t* freedofs);
+};
+
+}  // namespace ssv

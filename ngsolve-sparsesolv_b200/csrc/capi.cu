@@ -269,6 +269,8 @@ int ssv_ic_create(ssv_matrix* A, const uint8_t* freedofs, double shift, ssv_prec
         auto* p = new ssv_precond();
         p->kind = 1;
         p->A = A;
+        p->vdtype = A->dtype;
+        p->n = A->rows;
         ssv_config_default(&p->cfg);
         p->cfg.shift_parameter = shift;
         try {
@@ -282,6 +284,96 @@ int ssv_ic_create(ssv_matrix* A, const uint8_t* freedofs, double shift, ssv_prec
     });
 }
 
+int ssv_ams_create(ssv_matrix* A, ssv_matrix* G, const uint8_t* freedofs, const double* coord_x,
+                   const double* coord_y, const double* coord_z, int32_t cycle_type, int32_t num_smooth,
+                   double theta, double correction_weight, int32_t complex_form, int32_t ndof_complex,
+                   ssv_precond** out) {
+    return guarded([&] {
+        if (!A || !G || !out) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_create: NULL argument");
+        if (A->dtype != SSV_F64 || G->dtype != SSV_F64)
+            ssv::fail(SSV_ERR_TYPE, complex_form ? "ComplexCompactAMSPreconditioner: a_real_mat and grad_mat must be real"
+                                                 : "CompactAMSPreconditioner: expected real SparseMatrix<double>");
+        if (A->rows != A->cols || G->rows != A->rows)
+            ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_create: grad_mat must have one row per row of the matrix");
+        if (!coord_x || !coord_y || !coord_z)  // compact_ams.hpp:71-74
+            ssv::fail(SSV_ERR_RUNTIME, "CompactAMS: coordinate size mismatch with H1 DOFs");
+        const int nc = complex_form && ndof_complex > 0 ? ndof_complex : A->rows;
+        if (nc != A->rows)
+            ssv::fail(SSV_ERR_INVALID_ARG, "ComplexCompactAMS: ndof_complex must equal the HCurl dimension");
+        auto* p = new ssv_precond();
+        p->kind = complex_form ? 3 : 2;
+        p->A = A;
+        p->vdtype = complex_form ? SSV_C128 : SSV_F64;
+        p->n = A->rows;
+        try {
+            check_mask(freedofs, A->rows, p->h_fd, p->fd, p->has_fd);
+            p->ams.reset(ssv::ams_create(A, G, p->has_fd ? p->h_fd.data() : nullptr, coord_x, coord_y, coord_z,
+                                         cycle_type, num_smooth, theta, correction_weight, complex_form, nc));
+            p->ready = true;
+        } catch (...) {
+            delete p;
+            throw;
+        }
+        *out = p;
+    });
+}
+
+int ssv_ams_update(ssv_precond* p, ssv_matrix* new_A) {
+    return guarded([&] {
+        if (!p || !p->ams) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_update: not an AMS preconditioner");
+        if (new_A) {  // compact_ams.hpp:89-96
+            if (new_A->rows != p->A->rows || new_A->cols != p->A->cols)
+                ssv::fail(SSV_ERR_INVALID_ARG, "CompactAMS::Update: new matrix dimension (" +
+                                                   std::to_string(new_A->rows) + "x" + std::to_string(new_A->cols) +
+                                                   ") does not match original (" + std::to_string(p->A->rows) +
+                                                   "x" + std::to_string(p->A->cols) + ")");
+            if (new_A->dtype != SSV_F64) ssv::fail(SSV_ERR_TYPE, "CompactAMS::Update: expected a real matrix");
+            p->A = new_A;
+        }
+        ssv::ams_update(p->ams.get(), p->A);
+    });
+}
+
+int ssv_ams_levels(const ssv_precond* p, int32_t subspace, int32_t* sizes, int32_t cap, int32_t* num_levels) {
+    return guarded([&] {
+        if (!p || !p->ams || !sizes || !num_levels || subspace < 0 || subspace > 3)
+            ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_levels: bad argument");
+        *num_levels = ssv::ams_levels(p->ams.get(), subspace, sizes, cap);
+    });
+}
+
+int ssv_pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, const ssv_config* cfg,
+                      const void* d_b, void* d_x, ssv_result* res, double* history, int32_t history_cap) {
+    return guarded([&] {
+        if (!A || !cfg || !res || !d_b || !d_x) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_pcg_solve_dev: NULL argument");
+        ssv::pcg_solve_dev(A, pre, freedofs, *cfg, d_b, d_x, res, history, history_cap);
+    });
+}
+
+int ssv_pcg_solve(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, const ssv_config* cfg, const void* b,
+                  void* x, ssv_result* res, double* history, int32_t history_cap) {
+    return guarded([&] {
+        if (!A || !cfg || !res || !b || !x) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_pcg_solve: NULL argument");
+        cudaStream_t s = ssv::stream();
+        const int n = A->rows;
+        const size_t bytes = (size_t)n * scalar_bytes(A->dtype);
+        Stage& st = stage();
+        st.a.alloc(bytes / sizeof(double) + 1);
+        st.b.alloc(bytes / sizeof(double) + 1);
+        ssv::DevBuf<uint8_t> dfd;
+        if (freedofs) {
+            std::vector<uint8_t> h(freedofs, freedofs + n);
+            for (auto& v : h) v = v ? 1 : 0;
+            dfd.upload(h.data(), h.size(), s);
+        }
+        SSV_CUDA(cudaMemcpyAsync(st.a.get(), b, bytes, cudaMemcpyHostToDevice, s));
+        SSV_CUDA(cudaMemcpyAsync(st.b.get(), x, bytes, cudaMemcpyHostToDevice, s));
+        ssv::pcg_solve_dev(A, pre, dfd.get(), *cfg, st.a.get(), st.b.get(), res, history, history_cap);
+        SSV_CUDA(cudaMemcpyAsync(x, st.b.get(), bytes, cudaMemcpyDeviceToHost, s));
+        SSV_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 int ssv_ic_set_config(ssv_precond* p, const ssv_config* cfg) {
     return guarded([&] {
         if (!p || !cfg) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ic_set_config: NULL argument");
@@ -292,7 +384,8 @@ int ssv_ic_set_config(ssv_precond* p, const ssv_config* cfg) {
 int ssv_precond_update(ssv_precond* p) {
     return guarded([&] {
         if (!p) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_precond_update: NULL preconditioner");
-        ssv::precond_update(p);
+        if (p->ams) ssv::ams_update(p->ams.get(), p->A);
+        else ssv::precond_update(p);
     });
 }
 
@@ -308,7 +401,7 @@ int ssv_precond_apply(ssv_precond* p, const void* x, void* y) {
         if (!p || !x || !y) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_precond_apply: NULL argument");
         if (!p->ready) ssv::fail(SSV_ERR_RUNTIME, "ICPreconditioner::apply called before setup");
         cudaStream_t s = ssv::stream();
-        const size_t bytes = (size_t)p->A->rows * scalar_bytes(p->A->dtype);
+        const size_t bytes = (size_t)p->n * scalar_bytes(p->vdtype);
         p->io_x.alloc(bytes / sizeof(double) + 1);
         p->io_y.alloc(bytes / sizeof(double) + 1);
         SSV_CUDA(cudaMemcpyAsync(p->io_x.get(), x, bytes, cudaMemcpyHostToDevice, s));

@@ -3,6 +3,7 @@
 // as one CUDA graph: the preconditioner's kernels are captured into the same
 // iteration body, and the scalar steps run in the reductions' last block.
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -122,7 +123,8 @@ __global__ void k_ngs_loop_ctl(KState* st, cudaGraphConditionalHandle h, int use
 struct CocrCtx {
     KrylovWork<double> w_d;
     KrylovWork<zdouble> w_z;
-    GraphLoop loop;
+    GraphLoop loop, pcg_loop;
+    DevBuf<double> vals_bc;
 };
 
 static std::map<const ssv_matrix*, std::unique_ptr<CocrCtx>>& cocr_table() {
@@ -138,8 +140,19 @@ template <> KrylovWork<zdouble>& cw_of<zdouble>(CocrCtx& c) { return c.w_z; }
 
 template <typename S>
 static void apply_pre(ssv_precond* pre, const S* x, S* y, const KState* st, int n, cudaStream_t s) {
-    if (pre) ic_apply_dev<S>(pre, x, y, st, s);
+    if (pre) precond_apply_any<S>(pre, x, y, st, s);
     else k_copy<S><<<grid_for(n, kBlock), kBlock, 0, s>>>(n, x, y);
+}
+
+static std::string pre_key(const ssv_precond* pre) {
+    if (!pre) return "nopre";
+    std::string k = std::to_string((size_t)pre) + ":" + std::to_string(pre->kind) + ":" +
+                    std::to_string(precond_generation(pre)) + ":" + std::to_string((size_t)pre->xw.get());
+    if (pre->kind == 1) {
+        k += ":" + std::to_string(pre->A->dtype == SSV_F64 ? pre->ic_d.lo : pre->ic_z.lo) + ":" +
+             std::to_string(pre->A->dtype == SSV_F64 ? pre->ic_d.abmc : pre->ic_z.abmc);
+    }
+    return k;
 }
 
 template <typename S>
@@ -195,14 +208,7 @@ static void run_cocr_ngs(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, int
                       std::to_string((size_t)fd) + ";" + std::to_string((size_t)x) + ";" +
                       std::to_string((size_t)dst) + ";" + std::to_string(A->lanes) + ";" +
                       std::to_string((size_t)red.partials);
-    if (pre) {
-        const ICDevice<S>* ic = nullptr;
-        if constexpr (std::is_same<S, double>::value) ic = &pre->ic_d;
-        else ic = &pre->ic_z;
-        key += ";" + std::to_string((size_t)ic) + ";" + std::to_string(ic->gen) + ";" +
-               std::to_string((size_t)ic->Lv.get()) + std::to_string(ic->lo) + ";" +
-               std::to_string((size_t)pre->xw.get()) + ";" + std::to_string(ic->abmc);
-    }
+    key += ";" + pre_key(pre);
     build_graph_loop(ctx.loop, key, [&](cudaGraphConditionalHandle hc, int use_cond) {
         apply_pre<S>(pre, q, qt, dst, n, s);
         k_ngs_dot<S><<<g, kBlock, 0, s>>>(n, qt, q, dst, NGS_MU, red);
@@ -238,11 +244,147 @@ static void run_cocr_ngs(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, int
     }
 }
 
+// CG with an external preconditioner and an initial guess: the
+// sparsesolv::CGSolver recurrence (solvers/cg_solver.hpp:64-146 with
+// iterative_solver.hpp's bookkeeping) on the FreeDofs view of A (identity
+// rows, zero columns; ngsolve/sparsesolv_precond.hpp:60-74), z = M^{-1} r by
+// the given preconditioner, x on entry the initial guess (free entries) and on
+// return the solution (free entries written). This is the Krylov driver of the
+// AMS configurations, where the reference's scripts use NGSolve's CGSolver.
+template <typename S>
+static void run_pcg(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, const ssv_config& cfg, const S* d_b,
+                    S* d_x, ssv_result* res, double* hist, int hist_cap) {
+    cudaStream_t s = stream();
+    const int n = A->rows;
+    const double t0 = wall_seconds();
+    auto& ctx_ptr = cocr_table()[A];
+    if (!ctx_ptr) ctx_ptr.reset(new CocrCtx());
+    CocrCtx& ctx = *ctx_ptr;
+    KrylovWork<S>& w = cw_of<S>(ctx);
+    const int dev_hist = cfg.save_residual_history ? std::max(cfg.max_iterations, 0) + 2 : 1;
+    w.ensure(n, dev_hist);
+    const RedBuf red = w.red();
+    const int g = grid_for(n, kBlock);
+    int64_t nk = 0;
+    const S* v = reinterpret_cast<const S*>(A->val.get());
+    if (fd) {
+        ctx.vals_bc.alloc(A->val.size());
+        k_bc_values<S><<<g, kBlock, 0, s>>>(n, A->rp.get(), A->ci.get(), v, fd, reinterpret_cast<S*>(ctx.vals_bc.get()));
+        v = reinterpret_cast<const S*>(ctx.vals_bc.get());
+        ++nk;
+    }
+    k_gather_perm<S><<<g, kBlock, 0, s>>>(n, nullptr, d_b, w.bw.get(), fd, 1);
+    k_gather_perm<S><<<g, kBlock, 0, s>>>(n, nullptr, d_x, w.xb[0].get(), fd, 1);
+    launch_spmv<S, S, 2>(A->lanes, n, A->rp.get(), A->ci.get(), v, w.xb[0].get(), w.r.get(), w.bw.get(), nullptr,
+                         nullptr, RED_STORE, red, nullptr, s);
+    k_norm2<S><<<g, kBlock, 0, s>>>(n, w.bw.get(), red, w.scal.get());
+    k_norm2<S><<<g, kBlock, 0, s>>>(n, w.r.get(), red, w.scal.get() + 1);
+    SSV_LAUNCH_CHECK();
+    nk += 5;
+    double2 nrm[2];
+    SSV_CUDA(cudaMemcpyAsync(nrm, w.scal.get(), sizeof(nrm), cudaMemcpyDeviceToHost, s));
+    SSV_CUDA(cudaStreamSynchronize(s));
+    const double norm_b = std::sqrt(nrm[0].x), r0 = std::sqrt(nrm[1].x);
+    double normalizer = cfg.norm_type == SSV_NORM_RHS ? norm_b
+                      : cfg.norm_type == SSV_NORM_INITIAL_RESIDUAL ? r0 : cfg.custom_norm;
+    if (normalizer < 1e-15) normalizer = 1.0;
+    KState h;
+    std::memset(&h, 0, sizeof(h));
+    h.cur = 0;
+    h.best = -1;
+    h.normalizer = normalizer;
+    h.best_residual = DBL_MAX;
+    h.norm_r = r0;
+    h.final_norm = r0;
+    h.tol = cfg.tolerance;
+    h.abs_tol = cfg.abs_tolerance;
+    h.div_threshold = cfg.divergence_threshold;
+    h.maxiter = cfg.max_iterations;
+    h.div_check = cfg.divergence_check;
+    h.div_count = cfg.divergence_count;
+    h.save_best = cfg.save_best_result;
+    h.save_hist = cfg.save_residual_history;
+    h.conj = cfg.conjugate;
+    h.hist_cap = dev_hist;
+    h.hist = w.hist.get();
+    h.max_loops = std::max(cfg.max_iterations, 0) + 4;
+    if (cfg.save_residual_history) {
+        const double h0 = r0 / normalizer;
+        SSV_CUDA(cudaMemcpyAsync(w.hist.get(), &h0, sizeof(double), cudaMemcpyHostToDevice, s));
+        h.hist_len = 1;
+    }
+    if (cfg.max_iterations <= 0) { h.done = 1; h.iters = std::max(cfg.max_iterations, 0); }
+    KState* dst = w.st.get();
+    SSV_CUDA(cudaMemcpyAsync(dst, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+    S* z = pre ? w.z.get() : w.r.get();
+    if (pre) apply_pre<S>(pre, w.r.get(), w.z.get(), nullptr, n, s);
+    k_dot<S><<<g, kBlock, 0, s>>>(n, w.r.get(), z, cfg.conjugate, nullptr, RED_STORE, red, &dst->rho);
+    k_copy<S><<<g, kBlock, 0, s>>>(n, z, w.p.get());
+    SSV_LAUNCH_CHECK();
+    const std::string key = "pcg;" + std::to_string(n) + ";" + std::to_string((size_t)v) + ";" +
+                            std::to_string((size_t)dst) + ";" + std::to_string((size_t)red.partials) + ";" +
+                            std::to_string((size_t)w.r.get()) + ";" + pre_key(pre);
+    build_graph_loop(ctx.pcg_loop, key, [&](cudaGraphConditionalHandle hc, int use_cond) {
+        launch_spmv<S, S, 1>(A->lanes, n, A->rp.get(), A->ci.get(), v, w.p.get(), w.Ap.get(), nullptr, nullptr,
+                             dst, RED_CG_ALPHA, red, nullptr, s);
+        k_cg_update<S><<<g, kBlock, 0, s>>>(n, w.xb[0].get(), w.xb[1].get(), w.xb[2].get(), w.p.get(), w.Ap.get(),
+                                           w.r.get(), dst, red);
+        if (pre) apply_pre<S>(pre, w.r.get(), w.z.get(), dst, n, s);
+        k_dot<S><<<g, kBlock, 0, s>>>(n, w.r.get(), z, cfg.conjugate, dst, RED_CG_BETA, red, nullptr);
+        k_pupdate<S><<<g, kBlock, 0, s>>>(n, z, w.p.get(), dst);
+        k_loop_ctl<<<1, 32, 0, s>>>(dst, hc, use_cond);
+        SSV_LAUNCH_CHECK();
+    });
+    SSV_CUDA(cudaStreamSynchronize(s));
+    const double t1 = wall_seconds();
+    if (cfg.max_iterations > 0) run_graph_loop(ctx.pcg_loop, dst, cfg.max_iterations);
+    SSV_CUDA(cudaMemcpyAsync(&h, dst, sizeof(h), cudaMemcpyDeviceToHost, s));
+    SSV_CUDA(cudaStreamSynchronize(s));
+    if (h.status == SSV_ERR_TIMEOUT) fail(SSV_ERR_TIMEOUT, "CG loop guard fired");
+    std::memset(res, 0, sizeof(*res));
+    res->converged = h.converged;
+    res->iterations = h.iters;
+    res->final_residual = h.final_norm / h.normalizer;
+    int xbuf = h.cur;
+    if (!h.converged && cfg.save_best_result) {
+        res->final_residual = h.best_residual;
+        xbuf = h.best;
+    }
+    const S* xsrc;
+    if (xbuf < 0) { w.t.zero(s); xsrc = w.t.get(); }
+    else xsrc = w.xb[xbuf].get();
+    k_gather_perm<S><<<g, kBlock, 0, s>>>(n, nullptr, xsrc, d_x, fd, 0);
+    SSV_LAUNCH_CHECK();
+    res->kernel_launches = nk + 3 + (int64_t)ctx.pcg_loop.body_nodes * h.loops;
+    res->history_total = cfg.save_residual_history ? h.hist_len : 0;
+    res->history_len = std::min(std::min(res->history_total, dev_hist), std::max(hist_cap, 0));
+    if (hist && res->history_len > 0)
+        SSV_CUDA(cudaMemcpyAsync(hist, w.hist.get(), sizeof(double) * res->history_len, cudaMemcpyDeviceToHost, s));
+    SSV_CUDA(cudaStreamSynchronize(s));
+    res->setup_seconds = t1 - t0;
+    res->solve_seconds = wall_seconds() - t1;
+}
+
+void pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, const ssv_config& cfg, const void* d_b,
+                   void* d_x, ssv_result* res, double* hist, int hist_cap) {
+    if (A->rows != A->cols) fail(SSV_ERR_INVALID_ARG, "CG: matrix must be square");
+    if (pre && !pre->ready) fail(SSV_ERR_RUNTIME, "CG: preconditioner is not set up (call Update())");
+    if (pre && pre->vdtype != A->dtype) fail(SSV_ERR_TYPE, "CG: preconditioner scalar type differs from the matrix");
+    if (pre && pre->n != A->rows) fail(SSV_ERR_INVALID_ARG, "CG: preconditioner size differs from the matrix");
+    if (A->dtype == SSV_F64)
+        run_pcg<double>(A, pre, d_fd, cfg, static_cast<const double*>(d_b), static_cast<double*>(d_x), res, hist,
+                        hist_cap);
+    else
+        run_pcg<zdouble>(A, pre, d_fd, cfg, static_cast<const zdouble*>(d_b), static_cast<zdouble*>(d_x), res,
+                         hist, hist_cap);
+}
+
 void cocr_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, int maxiter, double tol,
                     int printrates, const void* d_b, void* d_x, int* iterations) {
     if (pre && !pre->ready) fail(SSV_ERR_RUNTIME, "COCRSolver: preconditioner is not set up (call Update())");
-    if (pre && pre->A->dtype != A->dtype)
+    if (pre && pre->vdtype != A->dtype)
         fail(SSV_ERR_TYPE, "COCRSolver: preconditioner scalar type differs from the matrix");
+    if (pre && pre->n != A->rows) fail(SSV_ERR_INVALID_ARG, "COCRSolver: preconditioner size differs from the matrix");
     if (A->dtype == SSV_F64)
         run_cocr_ngs<double>(A, pre, d_fd, maxiter, tol, printrates, static_cast<const double*>(d_b),
                              static_cast<double*>(d_x), iterations);

@@ -194,8 +194,15 @@ struct ssv_solver {
     ssv::GraphLoop loop;
 };
 
+namespace ssv {
+struct AmsState;
+void ams_free(AmsState* a);
+}  // namespace ssv
+
 struct ssv_precond {
-    int kind = 0;  // 1 = IC
+    int kind = 0;    // 1 = IC, 2 = CompactAMS (real), 3 = ComplexCompactAMS
+    int vdtype = 0;  // scalar type of the vectors it applies to
+    int n = 0;       // vector length
     ssv_matrix* A = nullptr;
     bool has_fd = false;
     std::vector<uint8_t> h_fd;
@@ -206,5 +213,6 @@ struct ssv_precond {
     ssv::ICDevice<double> ic_d;
     ssv::ICDevice<ssv::zdouble> ic_z;
     ssv::DevBuf<double> xw, yw, io_x, io_y;
+    std::unique_ptr<ssv::AmsState, void (*)(ssv::AmsState*)> ams{nullptr, ssv::ams_free};
     virtual ~ssv_precond() = default;
 };

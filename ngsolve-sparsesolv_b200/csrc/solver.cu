@@ -986,10 +986,11 @@ void precond_update(ssv_precond* p) {
 
 void precond_apply_dev(ssv_precond* p, const void* d_x, void* d_y) {
     if (!p->ready) fail(SSV_ERR_RUNTIME, "ICPreconditioner::apply called before setup");
-    if (p->A->dtype == SSV_F64)
-        ic_apply_dev<double>(p, static_cast<const double*>(d_x), static_cast<double*>(d_y), nullptr, stream());
+    if (p->vdtype == SSV_F64)
+        precond_apply_any<double>(p, static_cast<const double*>(d_x), static_cast<double*>(d_y), nullptr, stream());
     else
-        ic_apply_dev<zdouble>(p, static_cast<const zdouble*>(d_x), static_cast<zdouble*>(d_y), nullptr, stream());
+        precond_apply_any<zdouble>(p, static_cast<const zdouble*>(d_x), static_cast<zdouble*>(d_y), nullptr,
+                                   stream());
     SSV_CUDA(cudaStreamSynchronize(stream()));
 }
 

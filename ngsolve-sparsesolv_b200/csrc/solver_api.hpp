@@ -23,4 +23,26 @@ void cocr_forget(const ssv_matrix* A);
 template <typename S>
 void ic_apply_dev(ssv_precond* p, const S* x, S* y, const KState* st, cudaStream_t s);
 
+// y = M^{-1} x for any preconditioner handle, stream-ordered, no host sync
+// (so it can sit inside a captured iteration graph).
+template <typename S>
+void precond_apply_any(ssv_precond* p, const S* x, S* y, const KState* st, cudaStream_t s);
+template <>
+void precond_apply_any<double>(ssv_precond* p, const double* x, double* y, const KState* st, cudaStream_t s);
+template <>
+void precond_apply_any<zdouble>(ssv_precond* p, const zdouble* x, zdouble* y, const KState* st, cudaStream_t s);
+// Changes whenever the preconditioner's device structures are rebuilt.
+unsigned precond_generation(const ssv_precond* p);
+
+// Compact AMS (ams.cu)
+AmsState* ams_create(const ssv_matrix* A, const ssv_matrix* G, const uint8_t* fd, const double* cx,
+                     const double* cy, const double* cz, int cycle_type, int num_smooth, double theta, double w,
+                     int complex_form, int ndof_complex);
+void ams_update(AmsState* a, const ssv_matrix* A);
+int ams_levels(const AmsState* a, int sub, int* sizes, int cap);
+
+// CG with an external preconditioner and an initial guess (cocr_ngs.cu)
+void pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, const ssv_config& cfg, const void* d_b,
+                   void* d_x, ssv_result* res, double* hist, int hist_cap);
+
 }  // namespace ssv

@@ -490,5 +490,165 @@ def COCRSolver(mat, pre, freedofs=None, maxiter=500, tol=1e-8, printrates=False)
 
 
 def has_compact_ams():
-    """True when Compact AMG/AMS support is available."""
-    return False
+    """True when Compact AMG/AMS support is available (sparsesolv_python_export.hpp:559-560)."""
+    return True
+
+
+# ---------------------------------------------------------------------------
+# Compact AMS (preconditioners/compact_ams.hpp, complex_compact_ams.hpp)
+# ---------------------------------------------------------------------------
+
+def _coords(c, nh1):
+    a = np.ascontiguousarray(np.asarray(c, dtype=np.float64).ravel())
+    if a.shape[0] != nh1:  # compact_ams.hpp:71-74
+        raise RuntimeError("CompactAMS: coordinate size mismatch with H1 DOFs")
+    return a
+
+
+class _AmsBase(_PrecondBase):
+    _complex_form = 0
+
+    def __init__(self, mat, grad_mat, freedofs, coord_x, coord_y, coord_z, cycle_type, num_smooth,
+                 correction_weight, ndof_complex=0):
+        ip, ix, data, cplx, shape = _csr_arrays(mat)
+        if cplx:
+            raise TypeError("CompactAMSPreconditioner: expected real SparseMatrix<double>")
+        _, _, gdata, gcplx, gshape = _csr_arrays(grad_mat)
+        if gcplx:
+            raise TypeError("CompactAMSPreconditioner: grad_mat must be real SparseMatrix<double>")
+        self._mat = _Matrix(mat)
+        self._grad = _Matrix(grad_mat)
+        self._n = self._mat.n
+        self._dtype = np.complex128 if self._complex_form else np.float64
+        self._fd = _freedofs_array(freedofs, self._n)
+        nh1 = self._grad.m
+        self._cx, self._cy, self._cz = (_coords(c, nh1) for c in (coord_x, coord_y, coord_z))
+        D = _capi.PD
+        lib = _capi.load()
+        h = ctypes.c_void_p()
+        check(lib.ssv_ams_create(self._mat.h, self._grad.h, _capi.u8ptr(self._fd),
+                                 self._cx.ctypes.data_as(D), self._cy.ctypes.data_as(D), self._cz.ctypes.data_as(D),
+                                 int(cycle_type), int(num_smooth), 0.25, float(correction_weight),
+                                 self._complex_form, int(ndof_complex), ctypes.byref(h)))
+        self._init_handle(h)
+
+    def Update(self, new_mat=None):
+        """Rebuild with the current matrix values, or with new_mat (geometry kept)."""
+        if new_mat is None:
+            self._mat.refresh()
+            check(self._lib.ssv_ams_update(self._h, None))
+            return
+        m = _Matrix(new_mat)
+        if m.cplx:
+            raise TypeError("CompactAMS::Update: expected a real SparseMatrix<double>")
+        check(self._lib.ssv_ams_update(self._h, m.h))
+        self._mat = m  # the handle now refers to the new matrix
+
+    def levels(self, subspace):
+        """AMG hierarchy of a subspace (0 gradient, 1..3 Nedelec x/y/z): [(rows, nnz), ...]."""
+        buf = np.zeros(256, np.int32)
+        nl = ctypes.c_int32()
+        check(self._lib.ssv_ams_levels(self._h, subspace, _capi.i32ptr(buf), 256, ctypes.byref(nl)))
+        return [(int(buf[2 * l]), int(buf[2 * l + 1])) for l in range(nl.value)]
+
+
+class CompactAMSPreconditionerImpl(_AmsBase):
+    _cplx = False
+    _complex_form = 0
+
+
+class ComplexCompactAMSPreconditionerImpl(_AmsBase):
+    _cplx = True
+    _complex_form = 1
+
+
+def CompactAMSPreconditioner(mat, grad_mat, freedofs=None, coord_x=(), coord_y=(), coord_z=(), cycle_type=1,
+                             print_level=0, subspace_solver=0, num_smooth=1):
+    """Compact AMS preconditioner for real HCurl curl-curl + mass systems (factory :410-474)."""
+    if subspace_solver != 0:
+        raise ValueError("subspace_solver=1 (sparse Cholesky subspace solves, diagnostic) is not provided")
+    return CompactAMSPreconditionerImpl(mat, grad_mat, freedofs, coord_x, coord_y, coord_z, cycle_type,
+                                        num_smooth, 1.0)
+
+
+def ComplexCompactAMSPreconditioner(a_real_mat, grad_mat, freedofs=None, coord_x=(), coord_y=(), coord_z=(),
+                                    ndof_complex=0, cycle_type=1, print_level=0, correction_weight=1.0,
+                                    subspace_solver=0, num_smooth=1):
+    """Complex Compact AMS: one real AMS hierarchy on a_real applied to Re and Im in fused passes
+    (factory :476-557; complex_compact_ams.hpp)."""
+    if subspace_solver != 0:
+        raise ValueError("subspace_solver=1 (sparse Cholesky subspace solves, diagnostic) is not provided")
+    return ComplexCompactAMSPreconditionerImpl(a_real_mat, grad_mat, freedofs, coord_x, coord_y, coord_z,
+                                               cycle_type, num_smooth, correction_weight, ndof_complex)
+
+
+# ---------------------------------------------------------------------------
+# PCGSolver -- CG with an external preconditioner and an initial guess (new:
+# the reference's AMS scripts use NGSolve's krylovspace.CGSolver here)
+# ---------------------------------------------------------------------------
+
+class PCGSolver:
+    """CG (sparsesolv::CGSolver recurrence) with any preconditioner of this module.
+
+    ``Solve(rhs, sol)`` uses ``sol`` as the initial guess and returns a
+    SparseSolvResult; ``inv * rhs`` starts from zero. Convergence rule of
+    sparsesolv::CGSolver: ||r||/||b|| < tol or ||r|| < 1e-12.
+    """
+
+    def __init__(self, mat, pre=None, freedofs=None, maxiter=1000, tol=1e-10, printrates=False,
+                 save_residual_history=False, conjugate=False):
+        self._mat = mat if isinstance(mat, _Matrix) else _Matrix(mat)
+        self._pre = pre
+        self._fd = _freedofs_array(freedofs, self._mat.n)
+        self._cfg = _capi.default_config(tolerance=tol, max_iterations=maxiter,
+                                         save_residual_history=save_residual_history, conjugate=conjugate)
+        self.printrates = bool(printrates)
+        self._lib = _capi.load()
+        self._last = SparseSolvResult()
+
+    tol = property(lambda s: s._cfg.tolerance, lambda s, v: setattr(s._cfg, "tolerance", float(v)))
+    maxiter = property(lambda s: s._cfg.max_iterations, lambda s, v: setattr(s._cfg, "max_iterations", int(v)))
+
+    @property
+    def iterations(self):
+        return self._last.iterations
+
+    @property
+    def last_result(self):
+        return self._last
+
+    def Solve(self, rhs, sol):
+        b = np.ascontiguousarray(_vec_view(rhs), dtype=self._mat.dtype)
+        sv = _vec_view(sol)
+        x = np.ascontiguousarray(sv, dtype=self._mat.dtype)
+        cfg = _capi.ssv_config()
+        ctypes.pointer(cfg)[0] = self._cfg
+        if self.printrates:
+            cfg.save_residual_history = 1
+        cap = max(int(cfg.max_iterations), 0) + 2 if cfg.save_residual_history else 0
+        hist = np.zeros(max(cap, 1))
+        res = _capi.ssv_result()
+        self._mat.refresh()
+        check(self._lib.ssv_pcg_solve(self._mat.h, None if self._pre is None else self._pre._h,
+                                      _capi.u8ptr(self._fd), ctypes.byref(cfg), _capi.vptr(b), _capi.vptr(x),
+                                      ctypes.byref(res), hist.ctypes.data_as(_capi.PD), cap))
+        if x is not sv:
+            sv[...] = x
+        r = SparseSolvResult(res.converged, res.iterations, res.final_residual,
+                             hist[: res.history_len].tolist() if cfg.save_residual_history else [],
+                             0.0, res.setup_seconds, res.solve_seconds, res.kernel_launches)
+        if self.printrates:
+            for i, v in enumerate(r.residual_history):
+                print(f"CG iteration {i}, residual = {v}")
+        self._last = r
+        return r
+
+    def Mult(self, rhs, sol):
+        sv = _vec_view(sol)
+        sv[...] = 0
+        self.Solve(rhs, sv)
+
+    def __mul__(self, vec):
+        y = np.zeros(self._mat.n, dtype=self._mat.dtype)
+        self.Mult(vec, y)
+        return y

@@ -17,6 +17,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_INCLUDE = os.environ.get("SSV_REFERENCE_INCLUDE", "/root/reference/include")
 ORACLE_SO = os.path.join(HERE, "_build", "libssv_oracle.so")
+AMS_SO = os.path.join(HERE, "_build", "libssv_ams_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libssv_ref.so")
 
 
@@ -41,6 +42,14 @@ def build_oracle(force: bool = False) -> str:
     return ORACLE_SO
 
 
+def build_ams_oracle(force: bool = False) -> str:
+    srcs = [os.path.join(HERE, "ams_oracle.cpp"), os.path.join(HERE, "..", "include", "sparsesolv_b200.h")]
+    if force or _stale(AMS_SO, srcs):
+        os.makedirs(os.path.dirname(AMS_SO), exist_ok=True)
+        _run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-o", AMS_SO, srcs[0]])
+    return AMS_SO
+
+
 def build_reference(force: bool = False) -> str | None:
     hdr = os.path.join(REF_INCLUDE, "sparsesolv", "sparsesolv.hpp")
     if not os.path.exists(hdr):
@@ -58,4 +67,5 @@ def build_reference(force: bool = False) -> str | None:
 if __name__ == "__main__":
     force = "--force" in sys.argv
     print(build_oracle(force))
+    print(build_ams_oracle(force))
     print(build_reference(force))

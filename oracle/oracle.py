@@ -164,6 +164,124 @@ def level_schedule(rp, ci, n, upper=False, which="port"):
     return lev[:n], nl.value
 
 
+class AmsOracle:
+    """CPU restatement of CompactAMS / ComplexCompactAMS (oracle/ams_oracle.cpp)."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            lib = ctypes.CDLL(build_oracle.build_ams_oracle())
+            D = ctypes.POINTER(ctypes.c_double)
+            lib.ams_oracle_create.restype = ctypes.c_void_p
+            lib.ams_oracle_create.argtypes = [I32, PI32, PI32, D, I32, PI32, PI32, D, PU8, D, D, D, I32, I32,
+                                              ctypes.c_double, ctypes.c_double]
+            lib.ams_oracle_update.argtypes = [P, D]
+            lib.ams_oracle_destroy.argtypes = [P]
+            lib.ams_oracle_apply.argtypes = [P, D, D]
+            lib.ams_oracle_apply_complex.argtypes = [P, D, D]
+            lib.ams_oracle_levels.restype = I32
+            lib.ams_oracle_levels.argtypes = [P, I32, PI32, I32]
+            lib.ams_oracle_level_matrix.restype = I32
+            lib.ams_oracle_level_matrix.argtypes = [P, I32, I32, I32, PI32, PI32, D, I32]
+            lib.ams_oracle_pcg.restype = I32
+            lib.ams_oracle_pcg.argtypes = [P, D, D, ctypes.POINTER(ssv_config), ctypes.POINTER(ssv_result), D, I32]
+            lib.ams_oracle_cocr.restype = I32
+            lib.ams_oracle_cocr.argtypes = [P, I32, PI32, PI32, D, PU8, I32, ctypes.c_double, D, D, PI32, D, I32,
+                                            PI32]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, A, G, freedofs, cx, cy, cz, cycle_type=1, num_smooth=1, theta=0.25, weight=1.0):
+        lib = self.lib()
+        D = ctypes.POINTER(ctypes.c_double)
+        self._keep = []
+
+        def arr(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            self._keep.append(a)
+            return a
+
+        self.A = A
+        arp, aci, av = arr(A.indptr, np.int32), arr(A.indices, np.int32), arr(A.data, np.float64)
+        grp, gci, gv = arr(G.indptr, np.int32), arr(G.indices, np.int32), arr(G.data, np.float64)
+        self.fd = None if freedofs is None else arr(freedofs, np.uint8)
+        cxs = [arr(c, np.float64) for c in (cx, cy, cz)]
+        self.n = A.shape[0]
+        self.h = lib.ams_oracle_create(self.n, _p(arp), _p(aci), av.ctypes.data_as(D), G.shape[1], _p(grp), _p(gci),
+                                       gv.ctypes.data_as(D), _p(self.fd, PU8), *[c.ctypes.data_as(D) for c in cxs],
+                                       cycle_type, num_smooth, theta, weight)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib().ams_oracle_destroy(self.h)
+            self.h = None
+
+    def update(self, values):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self.lib().ams_oracle_update(self.h, v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+
+    def apply(self, b):
+        D = ctypes.POINTER(ctypes.c_double)
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n)
+        self.lib().ams_oracle_apply(self.h, bb.ctypes.data_as(D), x.ctypes.data_as(D))
+        return x
+
+    def apply_complex(self, f):
+        D = ctypes.POINTER(ctypes.c_double)
+        ff = np.ascontiguousarray(f, dtype=np.complex128)
+        u = np.zeros(self.n, dtype=np.complex128)
+        self.lib().ams_oracle_apply_complex(self.h, ff.ctypes.data_as(D), u.ctypes.data_as(D))
+        return u
+
+    def levels(self, s):
+        buf = np.zeros(256, np.int32)
+        nl = self.lib().ams_oracle_levels(self.h, s, _p(buf), 256)
+        return [(int(buf[2 * l]), int(buf[2 * l + 1])) for l in range(nl)]
+
+    def level_matrix(self, s, l, what=0):
+        import scipy.sparse as sp
+        D = ctypes.POINTER(ctypes.c_double)
+        nnz = self.lib().ams_oracle_level_matrix(self.h, s, l, what, None, None, None, 0)
+        sizes = self.levels(s)
+        n = sizes[l][0]
+        rp = np.zeros(n + 1, np.int32)
+        ci = np.zeros(nnz, np.int32)
+        v = np.zeros(nnz)
+        self.lib().ams_oracle_level_matrix(self.h, s, l, what, _p(rp), _p(ci), v.ctypes.data_as(D), nnz)
+        m = n if what == 0 else sizes[l + 1][0]
+        return sp.csr_matrix((v, ci, rp), shape=(n, m))
+
+    def pcg(self, b, x0=None, config=None, history_cap=100000):
+        D = ctypes.POINTER(ctypes.c_double)
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
+        cfg = config if config is not None else default_config()
+        res = ssv_result()
+        hist = np.zeros(max(history_cap, 1))
+        self.lib().ams_oracle_pcg(self.h, bb.ctypes.data_as(D), x.ctypes.data_as(D), ctypes.byref(cfg),
+                                  ctypes.byref(res), hist.ctypes.data_as(D), history_cap)
+        return x, res, hist[: res.history_len].copy()
+
+    def cocr(self, Ac, f, freedofs=None, maxiter=500, tol=1e-8, history_cap=100000):
+        D = ctypes.POINTER(ctypes.c_double)
+        rp = np.ascontiguousarray(Ac.indptr, np.int32)
+        ci = np.ascontiguousarray(Ac.indices, np.int32)
+        v = np.ascontiguousarray(Ac.data, np.complex128)
+        ff = np.ascontiguousarray(f, np.complex128)
+        fd = None if freedofs is None else np.ascontiguousarray(freedofs, np.uint8)
+        x = np.zeros(Ac.shape[0], np.complex128)
+        it = ctypes.c_int32(0)
+        hl = ctypes.c_int32(0)
+        hist = np.zeros(max(history_cap, 1))
+        self.lib().ams_oracle_cocr(self.h, Ac.shape[0], _p(rp), _p(ci), v.ctypes.data_as(D), _p(fd, PU8), maxiter,
+                                   tol, ff.ctypes.data_as(D), x.ctypes.data_as(D), ctypes.byref(it),
+                                   hist.ctypes.data_as(D), history_cap, ctypes.byref(hl))
+        return x, it.value, hist[: hl.value].copy()
+
+
 def cocr_solve(A, b, precond=None, freedofs=None, maxiter=500, tol=1e-8):
     """COCRSolverNGS::Mult on the CPU; precond is a python callable y=f(x)."""
     lib = port()
