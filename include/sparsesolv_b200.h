@@ -219,6 +219,13 @@ int ssv_ams_update(ssv_precond* p, ssv_matrix* new_A);
  * rows and nnz into sizes[2l], sizes[2l+1]. */
 int ssv_ams_levels(const ssv_precond* p, int32_t subspace, int32_t* sizes, int32_t cap,
                    int32_t* num_levels);
+/* New (no reference counterpart): the FP32-preconditioner form. With
+ * SSV_PREC_FP32 every matrix of the AMS hierarchy, the l1 norms and the work
+ * vectors of the cycle are FP32; the coarsest solve and the cycle's FP64
+ * input/output stay FP64. Switching re-uploads the hierarchy (no new set-up);
+ * Update() keeps the current form. */
+int ssv_ams_set_precision(ssv_precond* p, int32_t precision);
+int ssv_ams_get_precision(const ssv_precond* p, int32_t* precision);
 
 /* ---- CG with an external preconditioner (new: the reference's AMS scripts
  *      drive it with NGSolve's krylovspace.CGSolver) ---------------------------

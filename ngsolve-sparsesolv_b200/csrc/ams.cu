@@ -5,11 +5,19 @@
 // ([row][column]): NV = 1 is CompactAMS on a real vector, NV = 2 is
 // ComplexCompactAMS on a complex vector (Re/Im interleaved exactly as
 // std::complex<double> stores them), larger NV serve several right-hand sides
-// at once. One pass over a matrix row feeds all NV columns, which is the
-// reference's fused Re/Im idea taken to its end (DualSpMV, FusedResidual ...).
+// at once (NV = 4 real, NV = 8 = four complex). One pass over a matrix row
+// feeds all NV columns, which is the reference's fused Re/Im idea taken to its
+// end (DualSpMV, FusedResidual ...).
 // RECIP selects the l1 update of the fused complex operators, x += r * (1/l1)
 // (complex_compact_ams.hpp:197-201, compact_amg.hpp:724-728), instead of the
 // real one, x += r / l1 (compact_ams.hpp:538-540, compact_amg.hpp:654-656).
+//
+// T is the storage and arithmetic type of the whole cycle: double is the
+// drop-in form; float is the FP32-preconditioner form, where every matrix of
+// the hierarchy (A_bc, G, Pi, A_l, P_l, P_l^T), the l1 norms and the work
+// vectors are FP32 and only the coarsest solve stays FP64 (its pseudo-inverse
+// is FP64 and the product accumulates in FP64). The cycle's input and output
+// are FP64 in both forms: the Krylov recurrences around it never see FP32.
 #include <algorithm>
 #include <cstring>
 
@@ -24,38 +32,68 @@ namespace ssv {
 // ---------------------------------------------------------------------------
 enum MvMode : int { MV_AX = 0, MV_RES = 1, MV_ADD = 2, MV_JAC = 3 };
 
+// One row of NV columns in the widest aligned accesses the row allows (work
+// vectors come from cudaMalloc, so row r starts at r * NV * sizeof(T)).
 template <int NV>
-struct Acc {
-    double a[NV];
-};
+__device__ __forceinline__ void load_row(const double* __restrict__ p, double (&o)[NV]) {
+    if constexpr (NV % 2 == 0) {
+#pragma unroll
+        for (int i = 0; i < NV / 2; ++i) {
+            const double2 t = reinterpret_cast<const double2*>(p)[i];
+            o[2 * i] = t.x;
+            o[2 * i + 1] = t.y;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < NV; ++c) o[c] = p[c];
+    }
+}
+template <int NV>
+__device__ __forceinline__ void load_row(const float* __restrict__ p, float (&o)[NV]) {
+    if constexpr (NV % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < NV / 4; ++i) {
+            const float4 t = reinterpret_cast<const float4*>(p)[i];
+            o[4 * i] = t.x;
+            o[4 * i + 1] = t.y;
+            o[4 * i + 2] = t.z;
+            o[4 * i + 3] = t.w;
+        }
+    } else if constexpr (NV % 2 == 0) {
+#pragma unroll
+        for (int i = 0; i < NV / 2; ++i) {
+            const float2 t = reinterpret_cast<const float2*>(p)[i];
+            o[2 * i] = t.x;
+            o[2 * i + 1] = t.y;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < NV; ++c) o[c] = p[c];
+    }
+}
 
-template <int NV, int LANES, int MODE, bool RECIP>
+template <typename T, int NV, int LANES, int MODE, bool RECIP>
 __global__ void __launch_bounds__(kBlock)
-k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
-          const double* __restrict__ x, double* __restrict__ y, const double* __restrict__ b,
-          const double* __restrict__ d, double w, const KState* st) {
+k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ v,
+          const T* __restrict__ x, T* __restrict__ y, const T* __restrict__ b, const T* __restrict__ d, T w,
+          const KState* st) {
     if (st && st->done) return;
     const int sub = threadIdx.x % LANES;
     const int rpb = kBlock / LANES;
     const int lane_row = (threadIdx.x & 31) / LANES;  // warp-uniform trip count
     for (int row = blockIdx.x * rpb + threadIdx.x / LANES; row - lane_row < n; row += gridDim.x * rpb) {
         const bool valid = row < n;
-        double acc[NV];
+        T acc[NV];
 #pragma unroll
-        for (int c = 0; c < NV; ++c) acc[c] = 0.0;
+        for (int c = 0; c < NV; ++c) acc[c] = T(0);
         if (valid) {
             const int k1 = rp[row + 1];
             for (int k = rp[row] + sub; k < k1; k += LANES) {
-                const double a = v[k];
-                const double* xr = x + (size_t)ci[k] * NV;
-                if constexpr (NV == 2) {
-                    const double2 xv = *reinterpret_cast<const double2*>(xr);
-                    acc[0] += a * xv.x;
-                    acc[1] += a * xv.y;
-                } else {
+                const T a = v[k];
+                T xv[NV];
+                load_row<NV>(x + (size_t)ci[k] * NV, xv);
 #pragma unroll
-                    for (int c = 0; c < NV; ++c) acc[c] += a * xr[c];
-                }
+                for (int c = 0; c < NV; ++c) acc[c] += a * xv[c];
             }
         }
 #pragma unroll
@@ -73,7 +111,7 @@ k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const d
                 } else if constexpr (MODE == MV_ADD) {
                     y[base + c] += w * acc[c];
                 } else {
-                    const double r = b[base + c] - acc[c];
+                    const T r = b[base + c] - acc[c];
                     y[base + c] = RECIP ? x[base + c] + r * d[row] : x[base + c] + r / d[row];
                 }
             }
@@ -82,30 +120,30 @@ k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const d
 }
 
 // rx/ry/rz = Pi_{x,y,z}^T r over the shared pattern of G^T (one pass over r)
-template <int NV, int LANES>
+template <typename T, int NV, int LANES>
 __global__ void __launch_bounds__(kBlock)
-k_mv_pi_restrict(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ px,
-                 const double* __restrict__ py, const double* __restrict__ pz, const double* __restrict__ r,
-                 double* __restrict__ ox, double* __restrict__ oy, double* __restrict__ oz, const KState* st) {
+k_mv_pi_restrict(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ px,
+                 const T* __restrict__ py, const T* __restrict__ pz, const T* __restrict__ r, T* __restrict__ ox,
+                 T* __restrict__ oy, T* __restrict__ oz, const KState* st) {
     if (st && st->done) return;
     const int sub = threadIdx.x % LANES;
     const int rpb = kBlock / LANES;
     const int lane_row = (threadIdx.x & 31) / LANES;
     for (int row = blockIdx.x * rpb + threadIdx.x / LANES; row - lane_row < n; row += gridDim.x * rpb) {
         const bool valid = row < n;
-        double ax[NV], ay[NV], az[NV];
+        T ax[NV], ay[NV], az[NV];
 #pragma unroll
-        for (int c = 0; c < NV; ++c) ax[c] = ay[c] = az[c] = 0.0;
+        for (int c = 0; c < NV; ++c) ax[c] = ay[c] = az[c] = T(0);
         if (valid)
             for (int k = rp[row] + sub; k < rp[row + 1]; k += LANES) {
-                const double* rr = r + (size_t)ci[k] * NV;
-                const double vx = px[k], vy = py[k], vz = pz[k];
+                T rr[NV];
+                load_row<NV>(r + (size_t)ci[k] * NV, rr);
+                const T vx = px[k], vy = py[k], vz = pz[k];
 #pragma unroll
                 for (int c = 0; c < NV; ++c) {
-                    const double t = rr[c];
-                    ax[c] += vx * t;
-                    ay[c] += vy * t;
-                    az[c] += vz * t;
+                    ax[c] += vx * rr[c];
+                    ay[c] += vy * rr[c];
+                    az[c] += vz * rr[c];
                 }
             }
 #pragma unroll
@@ -128,30 +166,33 @@ k_mv_pi_restrict(int n, const int* __restrict__ rp, const int* __restrict__ ci, 
 
 // x += w Pix gx; x += w Piy gy; x += w Piz gz (in this order per row, as the
 // reference's three MultAdd calls) over the shared pattern of G
-template <int NV, int LANES>
+template <typename T, int NV, int LANES>
 __global__ void __launch_bounds__(kBlock)
-k_mv_pi_prolong(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ px,
-                const double* __restrict__ py, const double* __restrict__ pz, const double* __restrict__ gx,
-                const double* __restrict__ gy, const double* __restrict__ gz, double* __restrict__ x, double w,
-                const KState* st) {
+k_mv_pi_prolong(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ px,
+                const T* __restrict__ py, const T* __restrict__ pz, const T* __restrict__ gx,
+                const T* __restrict__ gy, const T* __restrict__ gz, T* __restrict__ x, T w, const KState* st) {
     if (st && st->done) return;
     const int sub = threadIdx.x % LANES;
     const int rpb = kBlock / LANES;
     const int lane_row = (threadIdx.x & 31) / LANES;
     for (int row = blockIdx.x * rpb + threadIdx.x / LANES; row - lane_row < n; row += gridDim.x * rpb) {
         const bool valid = row < n;
-        double sx[NV], sy[NV], sz[NV];
+        T sx[NV], sy[NV], sz[NV];
 #pragma unroll
-        for (int c = 0; c < NV; ++c) sx[c] = sy[c] = sz[c] = 0.0;
+        for (int c = 0; c < NV; ++c) sx[c] = sy[c] = sz[c] = T(0);
         if (valid)
             for (int k = rp[row] + sub; k < rp[row + 1]; k += LANES) {
                 const size_t j = (size_t)ci[k] * NV;
-                const double vx = px[k], vy = py[k], vz = pz[k];
+                T vgx[NV], vgy[NV], vgz[NV];
+                load_row<NV>(gx + j, vgx);
+                load_row<NV>(gy + j, vgy);
+                load_row<NV>(gz + j, vgz);
+                const T vx = px[k], vy = py[k], vz = pz[k];
 #pragma unroll
                 for (int c = 0; c < NV; ++c) {
-                    sx[c] += vx * gx[j + c];
-                    sy[c] += vy * gy[j + c];
-                    sz[c] += vz * gz[j + c];
+                    sx[c] += vx * vgx[c];
+                    sy[c] += vy * vgy[c];
+                    sz[c] += vz * vgz[c];
                 }
             }
 #pragma unroll
@@ -165,7 +206,7 @@ k_mv_pi_prolong(int n, const int* __restrict__ rp, const int* __restrict__ ci, c
         if (valid && sub == 0)
 #pragma unroll
             for (int c = 0; c < NV; ++c) {
-                double t = x[(size_t)row * NV + c];
+                T t = x[(size_t)row * NV + c];
                 t += w * sx[c];
                 t += w * sy[c];
                 t += w * sz[c];
@@ -175,9 +216,9 @@ k_mv_pi_prolong(int n, const int* __restrict__ rp, const int* __restrict__ ci, c
 }
 
 // x = b (/ or *) d  -- the first Jacobi sweep from x = 0
-template <int NV, bool RECIP>
-__global__ void k_mv_first_sweep(int n, const double* __restrict__ b, const double* __restrict__ d,
-                                 double* __restrict__ x, const KState* st) {
+template <typename T, int NV, bool RECIP>
+__global__ void k_mv_first_sweep(int n, const T* __restrict__ b, const T* __restrict__ d, T* __restrict__ x,
+                                 const KState* st) {
     if (st && st->done) return;
     const int64_t total = (int64_t)n * NV;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
@@ -186,23 +227,24 @@ __global__ void k_mv_first_sweep(int n, const double* __restrict__ b, const doub
     }
 }
 
-// out = mask ? in : 0
-template <int NV>
-__global__ void k_mv_mask_copy(int n, const double* __restrict__ in, const uint8_t* __restrict__ fd,
-                               double* __restrict__ out, const KState* st) {
+// out = mask ? in : 0, converting between the Krylov type (FP64) and the
+// cycle's type at the two ends of the cycle
+template <typename TI, typename TO, int NV>
+__global__ void k_mv_mask_copy(int n, const TI* __restrict__ in, const uint8_t* __restrict__ fd,
+                               TO* __restrict__ out, const KState* st) {
     if (st && st->done) return;
     const int64_t total = (int64_t)n * NV;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(q / NV);
-        out[q] = (!fd || fd[i]) ? in[q] : 0.0;
+        out[q] = (!fd || fd[i]) ? (TO)in[q] : TO(0);
     }
 }
 
-// y = X b, X dense n x n row-major (coarsest pseudo-inverse); warp per row
-template <int NV>
+// y = X b, X dense n x n row-major FP64 (coarsest pseudo-inverse), FP64
+// accumulation in both forms; warp per row
+template <typename T, int NV>
 __global__ void __launch_bounds__(kBlock)
-k_mv_gemv(int n, const double* __restrict__ X, const double* __restrict__ b, double* __restrict__ y,
-          const KState* st) {
+k_mv_gemv(int n, const double* __restrict__ X, const T* __restrict__ b, T* __restrict__ y, const KState* st) {
     if (st && st->done) return;
     const int lane = threadIdx.x & 31;
     for (int row = blockIdx.x * (kBlock / 32) + threadIdx.x / 32; row < n; row += gridDim.x * (kBlock / 32)) {
@@ -213,7 +255,7 @@ k_mv_gemv(int n, const double* __restrict__ X, const double* __restrict__ b, dou
         for (int k = lane; k < n; k += 32) {
             const double a = xr[k];
 #pragma unroll
-            for (int c = 0; c < NV; ++c) acc[c] += a * b[(size_t)k * NV + c];
+            for (int c = 0; c < NV; ++c) acc[c] += a * (double)b[(size_t)k * NV + c];
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
@@ -221,52 +263,78 @@ k_mv_gemv(int n, const double* __restrict__ X, const double* __restrict__ b, dou
             for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
         if (lane == 0)
 #pragma unroll
-            for (int c = 0; c < NV; ++c) y[(size_t)row * NV + c] = acc[c];
+            for (int c = 0; c < NV; ++c) y[(size_t)row * NV + c] = (T)acc[c];
     }
-}
-
-__global__ void k_recip(int n, const double* __restrict__ a, double* __restrict__ b) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = 1.0 / a[i];
 }
 
 // ---------------------------------------------------------------------------
 // Device hierarchy
 // ---------------------------------------------------------------------------
+static std::vector<float> to_float(const std::vector<double>& h) { return std::vector<float>(h.begin(), h.end()); }
+
+// A real array held in exactly one of the two forms.
+struct DualVec {
+    DevBuf<double> d;
+    DevBuf<float> f;
+    void set(const std::vector<double>& h, bool fp32, cudaStream_t s) {
+        if (fp32) {
+            d.release();
+            const std::vector<float> t = to_float(h);
+            f.upload(t.data(), t.size(), s);  // pageable source: staged before return
+        } else {
+            f.release();
+            d.upload(h.data(), h.size(), s);
+        }
+    }
+    template <typename T> const T* get() const;
+};
+template <> inline const double* DualVec::get<double>() const { return d.get(); }
+template <> inline const float* DualVec::get<float>() const { return f.get(); }
+
 struct DevCsr {
     int n = 0, m = 0;
     int64_t nnz = 0;
     int lanes = 8;
     DevBuf<int> rp, ci;
-    DevBuf<double> v;
-    void upload(const HostCsr& A, cudaStream_t s) {
+    DualVec v;
+    void upload(const HostCsr& A, bool fp32, cudaStream_t s) {
         n = A.n;
         m = A.m;
         nnz = A.nnz();
         rp.upload(A.rp.data(), A.rp.size(), s);
         ci.upload(A.ci.data(), A.ci.size(), s);
-        v.upload(A.v.data(), A.v.size(), s);
+        v.set(A.v, fp32, s);
         lanes = pick_lanes(n > 0 ? (double)nnz / n : 1.0);
     }
+    template <typename T> const T* val() const { return v.get<T>(); }
+};
+
+// Work vector: raw FP64-sized storage, used as T.
+struct WorkVec {
+    DevBuf<double> raw;
+    void alloc(size_t elems) { raw.alloc(elems); }
+    template <typename T> T* as() const { return reinterpret_cast<T*>(raw.get()); }
 };
 
 struct AmgDevLevel {
     DevCsr A, P, Pt;
-    DevBuf<double> l1, il1;
+    DualVec l1, il1;
     bool direct = false;
     DevBuf<double> X;
-    DevBuf<double> b, xa, xb, r;  // NV-column work vectors of this level
+    WorkVec b, xa, xb, r;  // NV-column work vectors of this level
 };
 
 struct AmsState {
     int nhc = 0, nh1 = 0, cycle_type = 1, num_smooth = 1, nv_alloc = 0;
     double w = 1.0;
     bool complex_form = false;
+    bool fp32 = false;
     int ndof_complex = 0;
     AmsHost host;
     DevCsr A_bc, G, Gt;
-    DevBuf<double> fine_l1, fine_il1, Piv[3], Pitv[3];
+    DualVec fine_l1, fine_il1, Piv[3], Pitv[3];
     std::vector<AmgDevLevel> amg[4];
-    DevBuf<double> b0, xa, xb, r, rs[4];
+    WorkVec b0, xa, xb, r, rs[4];
     DevBuf<uint8_t> fd;
     bool has_fd = false;
     std::vector<uint8_t> h_fd;
@@ -275,151 +343,157 @@ struct AmsState {
 
 void ams_free(AmsState* a) { delete a; }
 
-template <int NV, int MODE, bool RECIP>
-static void mv_spmv(const DevCsr& A, const double* x, double* y, const double* b, const double* d, double w,
-                    const KState* st, cudaStream_t s) {
+template <typename T, int NV, int MODE, bool RECIP>
+static void mv_spmv(const DevCsr& A, const T* x, T* y, const T* b, const T* d, T w, const KState* st,
+                    cudaStream_t s) {
     const int lanes = A.lanes;
     const int rpb = kBlock / lanes;
     const int grid = std::max(1, std::min((A.n + rpb - 1) / rpb, sm_count() * 8));
+    const T* v = A.val<T>();
     switch (lanes) {
-        case 2: k_mv_spmv<NV, 2, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), A.v.get(), x, y, b, d, w, st); break;
-        case 4: k_mv_spmv<NV, 4, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), A.v.get(), x, y, b, d, w, st); break;
-        case 8: k_mv_spmv<NV, 8, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), A.v.get(), x, y, b, d, w, st); break;
-        case 16: k_mv_spmv<NV, 16, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), A.v.get(), x, y, b, d, w, st); break;
-        default: k_mv_spmv<NV, 32, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), A.v.get(), x, y, b, d, w, st); break;
+        case 2: k_mv_spmv<T, NV, 2, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, b, d, w, st); break;
+        case 4: k_mv_spmv<T, NV, 4, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, b, d, w, st); break;
+        case 8: k_mv_spmv<T, NV, 8, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, b, d, w, st); break;
+        case 16: k_mv_spmv<T, NV, 16, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, b, d, w, st); break;
+        default: k_mv_spmv<T, NV, 32, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, b, d, w, st); break;
     }
 }
 
-template <int NV, bool RECIP>
-static void first_sweep(int n, const double* b, const double* d, double* x, const KState* st, cudaStream_t s) {
-    k_mv_first_sweep<NV, RECIP><<<grid_for((int64_t)n * NV, kBlock), kBlock, 0, s>>>(n, b, d, x, st);
+template <typename T, int NV, bool RECIP>
+static void first_sweep(int n, const T* b, const T* d, T* x, const KState* st, cudaStream_t s) {
+    k_mv_first_sweep<T, NV, RECIP><<<grid_for((int64_t)n * NV, kBlock), kBlock, 0, s>>>(n, b, d, x, st);
+}
+
+template <typename T, bool RECIP>
+static const T* l1_of(const AmgDevLevel& lv) {
+    return RECIP ? lv.il1.get<T>() : lv.l1.get<T>();
 }
 
 // One AMG V-cycle (VCycle / DualVCycle, compact_amg.hpp:662-706,801-841) on
 // level l: b -> x (x starts at zero). Returns the buffer holding x.
-template <int NV, bool RECIP>
-static double* vcycle(std::vector<AmgDevLevel>& L, int l, const double* b, int num_smooth, const KState* st,
-                      cudaStream_t s) {
+template <typename T, int NV, bool RECIP>
+static T* vcycle(std::vector<AmgDevLevel>& L, int l, const T* b, int num_smooth, const KState* st, cudaStream_t s) {
     AmgDevLevel& lv = L[l];
-    const double* d = RECIP ? lv.il1.get() : lv.l1.get();
-    double* cur = lv.xa.get();
-    double* alt = lv.xb.get();
+    const T* d = l1_of<T, RECIP>(lv);
+    T* cur = lv.xa.as<T>();
+    T* alt = lv.xb.as<T>();
     auto sweep = [&](int count) {
         for (int k = 0; k < count; ++k) {
-            mv_spmv<NV, MV_JAC, RECIP>(lv.A, cur, alt, b, d, 0.0, st, s);
+            mv_spmv<T, NV, MV_JAC, RECIP>(lv.A, cur, alt, b, d, T(0), st, s);
             std::swap(cur, alt);
         }
     };
     if (l == (int)L.size() - 1) {
         if (lv.direct) {
-            k_mv_gemv<NV><<<std::max(1, std::min((lv.A.n + 7) / 8, sm_count() * 4)), kBlock, 0, s>>>(
+            k_mv_gemv<T, NV><<<std::max(1, std::min((lv.A.n + 7) / 8, sm_count() * 4)), kBlock, 0, s>>>(
                 lv.A.n, lv.X.get(), b, cur, st);
         } else {  // 10 l1-Jacobi sweeps from x = 0
-            first_sweep<NV, RECIP>(lv.A.n, b, d, cur, st, s);
+            first_sweep<T, NV, RECIP>(lv.A.n, b, d, cur, st, s);
             sweep(9);
         }
         return cur;
     }
     // pre-smoothing from x = 0: the first sweep is x = b / l1
-    first_sweep<NV, RECIP>(lv.A.n, b, d, cur, st, s);
+    first_sweep<T, NV, RECIP>(lv.A.n, b, d, cur, st, s);
     sweep(num_smooth - 1);
-    mv_spmv<NV, MV_RES, RECIP>(lv.A, cur, lv.r.get(), b, nullptr, 0.0, st, s);
+    mv_spmv<T, NV, MV_RES, RECIP>(lv.A, cur, lv.r.as<T>(), b, nullptr, T(0), st, s);
     AmgDevLevel& nx = L[l + 1];
-    mv_spmv<NV, MV_AX, RECIP>(lv.Pt, lv.r.get(), nx.b.get(), nullptr, nullptr, 0.0, st, s);
-    double* ec = vcycle<NV, RECIP>(L, l + 1, nx.b.get(), num_smooth, st, s);
-    mv_spmv<NV, MV_ADD, RECIP>(lv.P, ec, cur, nullptr, nullptr, 1.0, st, s);
+    mv_spmv<T, NV, MV_AX, RECIP>(lv.Pt, lv.r.as<T>(), nx.b.as<T>(), nullptr, nullptr, T(0), st, s);
+    T* ec = vcycle<T, NV, RECIP>(L, l + 1, nx.b.as<T>(), num_smooth, st, s);
+    mv_spmv<T, NV, MV_ADD, RECIP>(lv.P, ec, cur, nullptr, nullptr, T(1), st, s);
     sweep(num_smooth);
     return cur;
 }
 
-template <int NV, int LANES>
-static void pi_restrict_l(const AmsState& a, const double* r, double* ox, double* oy, double* oz, const KState* st,
-                          cudaStream_t s) {
+template <typename T, int NV, int LANES>
+static void pi_restrict_l(const AmsState& a, const T* r, T* ox, T* oy, T* oz, const KState* st, cudaStream_t s) {
     const int rpb = kBlock / LANES;
     const int grid = std::max(1, std::min((a.Gt.n + rpb - 1) / rpb, sm_count() * 8));
-    k_mv_pi_restrict<NV, LANES><<<grid, kBlock, 0, s>>>(a.Gt.n, a.Gt.rp.get(), a.Gt.ci.get(), a.Pitv[0].get(),
-                                                        a.Pitv[1].get(), a.Pitv[2].get(), r, ox, oy, oz, st);
+    k_mv_pi_restrict<T, NV, LANES><<<grid, kBlock, 0, s>>>(a.Gt.n, a.Gt.rp.get(), a.Gt.ci.get(),
+                                                           a.Pitv[0].get<T>(), a.Pitv[1].get<T>(),
+                                                           a.Pitv[2].get<T>(), r, ox, oy, oz, st);
 }
 
-template <int NV, int LANES>
-static void pi_prolong_l(const AmsState& a, const double* gx, const double* gy, const double* gz, double* x,
-                         const KState* st, cudaStream_t s) {
+template <typename T, int NV, int LANES>
+static void pi_prolong_l(const AmsState& a, const T* gx, const T* gy, const T* gz, T* x, const KState* st,
+                         cudaStream_t s) {
     const int rpb = kBlock / LANES;
     const int grid = std::max(1, std::min((a.G.n + rpb - 1) / rpb, sm_count() * 8));
-    k_mv_pi_prolong<NV, LANES><<<grid, kBlock, 0, s>>>(a.G.n, a.G.rp.get(), a.G.ci.get(), a.Piv[0].get(),
-                                                       a.Piv[1].get(), a.Piv[2].get(), gx, gy, gz, x, a.w, st);
+    k_mv_pi_prolong<T, NV, LANES><<<grid, kBlock, 0, s>>>(a.G.n, a.G.rp.get(), a.G.ci.get(), a.Piv[0].get<T>(),
+                                                          a.Piv[1].get<T>(), a.Piv[2].get<T>(), gx, gy, gz, x,
+                                                          (T)a.w, st);
 }
 
-template <int NV>
-static void pi_restrict(const AmsState& a, const double* r, double* ox, double* oy, double* oz, const KState* st,
-                        cudaStream_t s) {
+template <typename T, int NV>
+static void pi_restrict(const AmsState& a, const T* r, T* ox, T* oy, T* oz, const KState* st, cudaStream_t s) {
     switch (a.Gt.lanes) {
-        case 2: pi_restrict_l<NV, 2>(a, r, ox, oy, oz, st, s); break;
-        case 4: pi_restrict_l<NV, 4>(a, r, ox, oy, oz, st, s); break;
-        case 8: pi_restrict_l<NV, 8>(a, r, ox, oy, oz, st, s); break;
-        case 16: pi_restrict_l<NV, 16>(a, r, ox, oy, oz, st, s); break;
-        default: pi_restrict_l<NV, 32>(a, r, ox, oy, oz, st, s); break;
+        case 2: pi_restrict_l<T, NV, 2>(a, r, ox, oy, oz, st, s); break;
+        case 4: pi_restrict_l<T, NV, 4>(a, r, ox, oy, oz, st, s); break;
+        case 8: pi_restrict_l<T, NV, 8>(a, r, ox, oy, oz, st, s); break;
+        case 16: pi_restrict_l<T, NV, 16>(a, r, ox, oy, oz, st, s); break;
+        default: pi_restrict_l<T, NV, 32>(a, r, ox, oy, oz, st, s); break;
     }
 }
 
-template <int NV>
-static void pi_prolong(const AmsState& a, const double* gx, const double* gy, const double* gz, double* x,
-                       const KState* st, cudaStream_t s) {
+template <typename T, int NV>
+static void pi_prolong(const AmsState& a, const T* gx, const T* gy, const T* gz, T* x, const KState* st,
+                       cudaStream_t s) {
     switch (a.G.lanes) {
-        case 2: pi_prolong_l<NV, 2>(a, gx, gy, gz, x, st, s); break;
-        case 4: pi_prolong_l<NV, 4>(a, gx, gy, gz, x, st, s); break;
-        case 8: pi_prolong_l<NV, 8>(a, gx, gy, gz, x, st, s); break;
-        case 16: pi_prolong_l<NV, 16>(a, gx, gy, gz, x, st, s); break;
-        default: pi_prolong_l<NV, 32>(a, gx, gy, gz, x, st, s); break;
+        case 2: pi_prolong_l<T, NV, 2>(a, gx, gy, gz, x, st, s); break;
+        case 4: pi_prolong_l<T, NV, 4>(a, gx, gy, gz, x, st, s); break;
+        case 8: pi_prolong_l<T, NV, 8>(a, gx, gy, gz, x, st, s); break;
+        case 16: pi_prolong_l<T, NV, 16>(a, gx, gy, gz, x, st, s); break;
+        default: pi_prolong_l<T, NV, 32>(a, gx, gy, gz, x, st, s); break;
     }
 }
 
 // One AMS cycle (CompactAMS::Mult, compact_ams.hpp:136-195, or the fused
-// ComplexCompactAMS::Mult, complex_compact_ams.hpp:112-154): in -> out.
-template <int NV, bool RECIP>
+// ComplexCompactAMS::Mult, complex_compact_ams.hpp:112-154): in -> out, both
+// FP64 with NV columns.
+template <typename T, int NV, bool RECIP>
 static void ams_cycle(AmsState& a, const double* in, double* out, const KState* st, cudaStream_t s) {
     const int n = a.nhc;
     const uint8_t* fd = a.has_fd ? a.fd.get() : nullptr;
-    const double* d = RECIP ? a.fine_il1.get() : a.fine_l1.get();
-    double* b0 = a.b0.get();
-    double* cur = a.xa.get();
-    double* alt = a.xb.get();
-    double* r = a.r.get();
+    const T* d = RECIP ? a.fine_il1.get<T>() : a.fine_l1.get<T>();
+    T* b0 = a.b0.as<T>();
+    T* cur = a.xa.as<T>();
+    T* alt = a.xb.as<T>();
+    T* r = a.r.as<T>();
     const int gm = grid_for((int64_t)n * NV, kBlock);
-    k_mv_mask_copy<NV><<<gm, kBlock, 0, s>>>(n, in, fd, b0, st);
+    k_mv_mask_copy<double, T, NV><<<gm, kBlock, 0, s>>>(n, in, fd, b0, st);
     bool fresh = true;  // x == 0
     auto fine_smooth = [&]() {
         for (int k = 0; k < a.num_smooth; ++k) {
             if (fresh) {
-                first_sweep<NV, RECIP>(n, b0, d, cur, st, s);
+                first_sweep<T, NV, RECIP>(n, b0, d, cur, st, s);
                 fresh = false;
             } else {
-                mv_spmv<NV, MV_JAC, RECIP>(a.A_bc, cur, alt, b0, d, 0.0, st, s);
+                mv_spmv<T, NV, MV_JAC, RECIP>(a.A_bc, cur, alt, b0, d, T(0), st, s);
                 std::swap(cur, alt);
             }
         }
     };
     auto ensure_x = [&]() {
         if (fresh) {
-            SSV_CUDA(cudaMemsetAsync(cur, 0, sizeof(double) * (size_t)n * NV, s));
+            SSV_CUDA(cudaMemsetAsync(cur, 0, sizeof(T) * (size_t)n * NV, s));
             fresh = false;
         }
     };
     auto gradient = [&]() {
         ensure_x();
-        mv_spmv<NV, MV_RES, RECIP>(a.A_bc, cur, r, b0, nullptr, 0.0, st, s);
-        mv_spmv<NV, MV_AX, RECIP>(a.Gt, r, a.rs[0].get(), nullptr, nullptr, 0.0, st, s);
-        double* g = vcycle<NV, RECIP>(a.amg[0], 0, a.rs[0].get(), 1, st, s);
-        mv_spmv<NV, MV_ADD, RECIP>(a.G, g, cur, nullptr, nullptr, a.w, st, s);
+        mv_spmv<T, NV, MV_RES, RECIP>(a.A_bc, cur, r, b0, nullptr, T(0), st, s);
+        mv_spmv<T, NV, MV_AX, RECIP>(a.Gt, r, a.rs[0].as<T>(), nullptr, nullptr, T(0), st, s);
+        T* g = vcycle<T, NV, RECIP>(a.amg[0], 0, a.rs[0].as<T>(), 1, st, s);
+        mv_spmv<T, NV, MV_ADD, RECIP>(a.G, g, cur, nullptr, nullptr, (T)a.w, st, s);
     };
     auto nodal = [&]() {
         ensure_x();
-        mv_spmv<NV, MV_RES, RECIP>(a.A_bc, cur, r, b0, nullptr, 0.0, st, s);
-        pi_restrict<NV>(a, r, a.rs[1].get(), a.rs[2].get(), a.rs[3].get(), st, s);
-        double* gx = vcycle<NV, RECIP>(a.amg[1], 0, a.rs[1].get(), 1, st, s);
-        double* gy = vcycle<NV, RECIP>(a.amg[2], 0, a.rs[2].get(), 1, st, s);
-        double* gz = vcycle<NV, RECIP>(a.amg[3], 0, a.rs[3].get(), 1, st, s);
-        pi_prolong<NV>(a, gx, gy, gz, cur, st, s);
+        mv_spmv<T, NV, MV_RES, RECIP>(a.A_bc, cur, r, b0, nullptr, T(0), st, s);
+        pi_restrict<T, NV>(a, r, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), st, s);
+        T* gx = vcycle<T, NV, RECIP>(a.amg[1], 0, a.rs[1].as<T>(), 1, st, s);
+        T* gy = vcycle<T, NV, RECIP>(a.amg[2], 0, a.rs[2].as<T>(), 1, st, s);
+        T* gz = vcycle<T, NV, RECIP>(a.amg[3], 0, a.rs[3].as<T>(), 1, st, s);
+        pi_prolong<T, NV>(a, gx, gy, gz, cur, st, s);
     };
     if (a.cycle_type == 7) {
         fine_smooth(); gradient(); fine_smooth(); nodal(); fine_smooth(); gradient(); fine_smooth();
@@ -427,7 +501,7 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
         fine_smooth(); gradient(); nodal(); gradient(); fine_smooth();
     }
     ensure_x();
-    k_mv_mask_copy<NV><<<gm, kBlock, 0, s>>>(n, cur, fd, out, st);
+    k_mv_mask_copy<T, double, NV><<<gm, kBlock, 0, s>>>(n, cur, fd, out, st);
     SSV_LAUNCH_CHECK();
 }
 
@@ -442,7 +516,10 @@ static HostCsr host_csr_of(const ssv_matrix* M) {
     return H;
 }
 
-static void upload_level_work(AmsState& a, int nv) {
+// Work vectors for blocks of up to nv real columns (allocation only, so the
+// cycle itself never allocates and can be captured).
+static void ams_reserve(AmsState& a, int nv) {
+    if (nv <= a.nv_alloc) return;
     for (int s = 0; s < 4; ++s)
         for (auto& lv : a.amg[s]) {
             const size_t m = (size_t)lv.A.n * nv;
@@ -460,35 +537,55 @@ static void upload_level_work(AmsState& a, int nv) {
     a.nv_alloc = nv;
 }
 
-// Rebuild the matrix-dependent part (RebuildMatrix) and upload it.
-static void ams_rebuild(AmsState& a, const ssv_matrix* A) {
-    cudaStream_t s = stream();
-    HostCsr H = host_csr_of(A);
-    a.host.rebuild(H, a.has_fd ? a.h_fd.data() : nullptr);
-    a.A_bc.upload(a.host.A_bc, s);
-    a.fine_l1.upload(a.host.fine_l1.data(), a.host.fine_l1.size(), s);
-    a.fine_il1.alloc(a.nhc);
-    k_recip<<<grid_for(a.nhc, kBlock), kBlock, 0, s>>>(a.nhc, a.fine_l1.get(), a.fine_il1.get());
+static std::vector<double> reciprocal(const std::vector<double>& v) {
+    std::vector<double> r(v.size());
+    for (size_t i = 0; i < v.size(); ++i) r[i] = 1.0 / v[i];
+    return r;
+}
+
+// Geometry part (G, G^T, Pi) in the chosen form.
+static void ams_upload_geometry(AmsState& a, cudaStream_t s) {
+    a.G.upload(a.host.G, a.fp32, s);
+    a.Gt.upload(a.host.Gt, a.fp32, s);
+    for (int d = 0; d < 3; ++d) {
+        a.Piv[d].set(a.host.Pi[d].v, a.fp32, s);
+        a.Pitv[d].set(a.host.Pit[d].v, a.fp32, s);
+    }
+}
+
+// Matrix part (A_bc, l1 norms, the four AMG hierarchies) in the chosen form.
+static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
+    const int nv = std::max(a.nv_alloc, a.complex_form ? 2 : 1);
+    a.A_bc.upload(a.host.A_bc, a.fp32, s);
+    a.fine_l1.set(a.host.fine_l1, a.fp32, s);
+    a.fine_il1.set(reciprocal(a.host.fine_l1), a.fp32, s);
     for (int sub = 0; sub < 4; ++sub) {
         const auto& hl = a.host.amg[sub].levels;
         a.amg[sub].clear();
         a.amg[sub].resize(hl.size());
         for (size_t l = 0; l < hl.size(); ++l) {
             AmgDevLevel& dl = a.amg[sub][l];
-            dl.A.upload(hl[l].A, s);
-            dl.l1.upload(hl[l].l1.data(), hl[l].l1.size(), s);
-            dl.il1.alloc(hl[l].A.n);
-            k_recip<<<grid_for(hl[l].A.n, kBlock), kBlock, 0, s>>>(hl[l].A.n, dl.l1.get(), dl.il1.get());
+            dl.A.upload(hl[l].A, a.fp32, s);
+            dl.l1.set(hl[l].l1, a.fp32, s);
+            dl.il1.set(reciprocal(hl[l].l1), a.fp32, s);
             if (l + 1 < hl.size()) {
-                dl.P.upload(hl[l].P, s);
-                dl.Pt.upload(hl[l].Pt, s);
+                dl.P.upload(hl[l].P, a.fp32, s);
+                dl.Pt.upload(hl[l].Pt, a.fp32, s);
             }
             dl.direct = hl[l].direct;
-            if (dl.direct) dl.X.upload(hl[l].inv.data(), hl[l].inv.size(), s);
+            if (dl.direct) dl.X.upload(hl[l].inv.data(), hl[l].inv.size(), s);  // FP64 in both forms
         }
     }
-    SSV_LAUNCH_CHECK();
-    upload_level_work(a, a.complex_form ? 2 : 1);
+    a.nv_alloc = 0;
+    ams_reserve(a, nv);
+}
+
+// Rebuild the matrix-dependent part (RebuildMatrix) and upload it.
+static void ams_rebuild(AmsState& a, const ssv_matrix* A) {
+    cudaStream_t s = stream();
+    HostCsr H = host_csr_of(A);
+    a.host.rebuild(H, a.has_fd ? a.h_fd.data() : nullptr);
+    ams_upload_matrix(a, s);
     ++a.gen;
     SSV_CUDA(cudaStreamSynchronize(s));
 }
@@ -515,12 +612,7 @@ AmsState* ams_create(const ssv_matrix* A, const ssv_matrix* G, const uint8_t* fd
         }
         HostCsr Gh = host_csr_of(G);
         a->host.setup_geometry(Gh, cx, cy, cz);
-        a->G.upload(a->host.G, s);
-        a->Gt.upload(a->host.Gt, s);
-        for (int d = 0; d < 3; ++d) {
-            a->Piv[d].upload(a->host.Pi[d].v.data(), a->host.Pi[d].v.size(), s);
-            a->Pitv[d].upload(a->host.Pit[d].v.data(), a->host.Pit[d].v.size(), s);
-        }
+        ams_upload_geometry(*a, s);
         ams_rebuild(*a, A);
         if (a->w <= 0.0) a->w = 1.0;  // Setup (:260-262)
     } catch (...) {
@@ -532,20 +624,68 @@ AmsState* ams_create(const ssv_matrix* A, const ssv_matrix* G, const uint8_t* fd
 
 void ams_update(AmsState* a, const ssv_matrix* A) { ams_rebuild(*a, A); }
 
+// Switch between the FP64 and FP32 forms: the host keeps the hierarchy, so
+// this is a re-upload, no new set-up.
+void ams_set_precision(AmsState* a, int precision) {
+    const bool lo = precision == SSV_PREC_FP32;
+    if (lo == a->fp32) return;
+    cudaStream_t s = stream();
+    a->fp32 = lo;
+    ams_upload_geometry(*a, s);
+    ams_upload_matrix(*a, s);
+    ++a->gen;
+    SSV_CUDA(cudaStreamSynchronize(s));
+}
+
+int ams_precision(const AmsState* a) { return a->fp32 ? SSV_PREC_FP32 : SSV_PREC_FP64; }
+
+void ams_reserve_block(AmsState* a, int nrhs) {
+    ams_reserve(*a, nrhs * (a->complex_form ? 2 : 1));
+    SSV_CUDA(cudaStreamSynchronize(stream()));
+}
+
+template <typename T>
+static void ams_block_t(AmsState& a, const double* in, double* out, int nrhs, const KState* st, cudaStream_t s) {
+    if (a.complex_form) {
+        switch (nrhs) {
+            case 1: ams_cycle<T, 2, true>(a, in, out, st, s); return;
+            case 4: ams_cycle<T, 8, true>(a, in, out, st, s); return;
+        }
+    } else {
+        switch (nrhs) {
+            case 1: ams_cycle<T, 1, false>(a, in, out, st, s); return;
+            case 4: ams_cycle<T, 4, false>(a, in, out, st, s); return;
+        }
+    }
+    fail(SSV_ERR_INVALID_ARG, "AMS block apply: nrhs must be 1 or 4");
+}
+
+// nrhs right-hand sides, row-interleaved ([row][rhs], complex as Re/Im pairs).
+void ams_apply_block(AmsState* a, const double* in, double* out, int nrhs, const KState* st, cudaStream_t s) {
+    if (nrhs * (a->complex_form ? 2 : 1) > a->nv_alloc) fail(SSV_ERR_INVALID_ARG, "AMS block apply: reserve first");
+    if (a->fp32) ams_block_t<float>(*a, in, out, nrhs, st, s);
+    else ams_block_t<double>(*a, in, out, nrhs, st, s);
+}
+
 // y = M^{-1} x for the preconditioner p, stream-ordered and capturable.
 template <>
 void precond_apply_any<double>(ssv_precond* p, const double* x, double* y, const KState* st, cudaStream_t s) {
     if (p->kind == 1) ic_apply_dev<double>(p, x, y, st, s);
-    else if (p->kind == 2) ams_cycle<1, false>(*p->ams, x, y, st, s);
-    else fail(SSV_ERR_TYPE, "preconditioner is complex; the matrix is real");
+    else if (p->kind == 2) {
+        if (p->ams->fp32) ams_cycle<float, 1, false>(*p->ams, x, y, st, s);
+        else ams_cycle<double, 1, false>(*p->ams, x, y, st, s);
+    } else fail(SSV_ERR_TYPE, "preconditioner is complex; the matrix is real");
 }
 
 template <>
 void precond_apply_any<zdouble>(ssv_precond* p, const zdouble* x, zdouble* y, const KState* st, cudaStream_t s) {
     if (p->kind == 1) ic_apply_dev<zdouble>(p, x, y, st, s);
-    else if (p->kind == 3)
-        ams_cycle<2, true>(*p->ams, reinterpret_cast<const double*>(x), reinterpret_cast<double*>(y), st, s);
-    else fail(SSV_ERR_TYPE, "preconditioner is real; the matrix is complex");
+    else if (p->kind == 3) {
+        const double* xi = reinterpret_cast<const double*>(x);
+        double* yo = reinterpret_cast<double*>(y);
+        if (p->ams->fp32) ams_cycle<float, 2, true>(*p->ams, xi, yo, st, s);
+        else ams_cycle<double, 2, true>(*p->ams, xi, yo, st, s);
+    } else fail(SSV_ERR_TYPE, "preconditioner is real; the matrix is complex");
 }
 
 unsigned precond_generation(const ssv_precond* p) {

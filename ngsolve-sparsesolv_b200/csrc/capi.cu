@@ -342,6 +342,22 @@ int ssv_ams_levels(const ssv_precond* p, int32_t subspace, int32_t* sizes, int32
     });
 }
 
+int ssv_ams_set_precision(ssv_precond* p, int32_t precision) {
+    return guarded([&] {
+        if (!p || !p->ams) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_set_precision: not an AMS preconditioner");
+        if (precision != SSV_PREC_FP64 && precision != SSV_PREC_FP32)
+            ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_set_precision: precision must be SSV_PREC_FP64 or SSV_PREC_FP32");
+        ssv::ams_set_precision(p->ams.get(), precision);
+    });
+}
+
+int ssv_ams_get_precision(const ssv_precond* p, int32_t* precision) {
+    return guarded([&] {
+        if (!p || !p->ams || !precision) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_get_precision: bad argument");
+        *precision = ssv::ams_precision(p->ams.get());
+    });
+}
+
 int ssv_pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, const ssv_config* cfg,
                       const void* d_b, void* d_x, ssv_result* res, double* history, int32_t history_cap) {
     return guarded([&] {

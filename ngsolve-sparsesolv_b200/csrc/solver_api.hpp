@@ -40,6 +40,12 @@ AmsState* ams_create(const ssv_matrix* A, const ssv_matrix* G, const uint8_t* fd
                      int complex_form, int ndof_complex);
 void ams_update(AmsState* a, const ssv_matrix* A);
 int ams_levels(const AmsState* a, int sub, int* sizes, int cap);
+void ams_set_precision(AmsState* a, int precision);
+int ams_precision(const AmsState* a);
+// Block application to nrhs right-hand sides ([row][rhs] interleaved; complex
+// form: Re/Im pairs), after ams_reserve_block(a, nrhs).
+void ams_reserve_block(AmsState* a, int nrhs);
+void ams_apply_block(AmsState* a, const double* in, double* out, int nrhs, const KState* st, cudaStream_t s);
 
 // CG with an external preconditioner and an initial guess (cocr_ngs.cu)
 void pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, const ssv_config& cfg, const void* d_b,

@@ -24,6 +24,8 @@ __all__ = [
     "SparseSolvResult", "SparseSolvSolver", "SparseSolvSolverD", "SparseSolvSolverC",
     "ICPreconditioner", "ICPreconditionerD", "ICPreconditionerC",
     "COCRSolver", "COCRSolverD", "COCRSolverC", "has_compact_ams",
+    "CompactAMSPreconditioner", "CompactAMSPreconditionerImpl",
+    "ComplexCompactAMSPreconditioner", "ComplexCompactAMSPreconditionerImpl", "PCGSolver",
 ]
 
 
@@ -544,6 +546,20 @@ class _AmsBase(_PrecondBase):
         check(self._lib.ssv_ams_update(self._h, m.h))
         self._mat = m  # the handle now refers to the new matrix
 
+    @property
+    def precision(self):
+        """"fp64" (drop-in) or "fp32" (new: FP32 hierarchy and cycle, FP64 coarsest solve and in/out)."""
+        v = ctypes.c_int32()
+        check(self._lib.ssv_ams_get_precision(self._h, ctypes.byref(v)))
+        return "fp32" if v.value == _capi.SSV_PREC_FP32 else "fp64"
+
+    @precision.setter
+    def precision(self, value):
+        v = str(value).lower()
+        if v not in ("fp32", "fp64"):
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        check(self._lib.ssv_ams_set_precision(self._h, _capi.SSV_PREC_FP32 if v == "fp32" else _capi.SSV_PREC_FP64))
+
     def levels(self, subspace):
         """AMG hierarchy of a subspace (0 gradient, 1..3 Nedelec x/y/z): [(rows, nnz), ...]."""
         buf = np.zeros(256, np.int32)
@@ -563,23 +579,31 @@ class ComplexCompactAMSPreconditionerImpl(_AmsBase):
 
 
 def CompactAMSPreconditioner(mat, grad_mat, freedofs=None, coord_x=(), coord_y=(), coord_z=(), cycle_type=1,
-                             print_level=0, subspace_solver=0, num_smooth=1):
-    """Compact AMS preconditioner for real HCurl curl-curl + mass systems (factory :410-474)."""
+                             print_level=0, subspace_solver=0, num_smooth=1, precision="fp64"):
+    """Compact AMS preconditioner for real HCurl curl-curl + mass systems (factory :410-474).
+
+    ``precision="fp32"`` (new keyword, default the drop-in "fp64") selects the FP32-preconditioner form."""
     if subspace_solver != 0:
         raise ValueError("subspace_solver=1 (sparse Cholesky subspace solves, diagnostic) is not provided")
-    return CompactAMSPreconditionerImpl(mat, grad_mat, freedofs, coord_x, coord_y, coord_z, cycle_type,
-                                        num_smooth, 1.0)
+    p = CompactAMSPreconditionerImpl(mat, grad_mat, freedofs, coord_x, coord_y, coord_z, cycle_type,
+                                     num_smooth, 1.0)
+    if str(precision).lower() != "fp64":
+        p.precision = precision
+    return p
 
 
 def ComplexCompactAMSPreconditioner(a_real_mat, grad_mat, freedofs=None, coord_x=(), coord_y=(), coord_z=(),
                                     ndof_complex=0, cycle_type=1, print_level=0, correction_weight=1.0,
-                                    subspace_solver=0, num_smooth=1):
+                                    subspace_solver=0, num_smooth=1, precision="fp64"):
     """Complex Compact AMS: one real AMS hierarchy on a_real applied to Re and Im in fused passes
-    (factory :476-557; complex_compact_ams.hpp)."""
+    (factory :476-557; complex_compact_ams.hpp). ``precision`` as in CompactAMSPreconditioner."""
     if subspace_solver != 0:
         raise ValueError("subspace_solver=1 (sparse Cholesky subspace solves, diagnostic) is not provided")
-    return ComplexCompactAMSPreconditionerImpl(a_real_mat, grad_mat, freedofs, coord_x, coord_y, coord_z,
-                                               cycle_type, num_smooth, correction_weight, ndof_complex)
+    p = ComplexCompactAMSPreconditionerImpl(a_real_mat, grad_mat, freedofs, coord_x, coord_y, coord_z,
+                                            cycle_type, num_smooth, correction_weight, ndof_complex)
+    if str(precision).lower() != "fp64":
+        p.precision = precision
+    return p
 
 
 # ---------------------------------------------------------------------------

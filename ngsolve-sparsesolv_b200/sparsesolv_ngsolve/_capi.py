@@ -178,6 +178,8 @@ SIGNATURES = [
     ("ssv_ams_create", I32, [P, P, PU8, PD, PD, PD, I32, I32, ctypes.c_double, ctypes.c_double, I32, I32, PP]),
     ("ssv_ams_update", I32, [P, P]),
     ("ssv_ams_levels", I32, [P, I32, PI32, I32, PI32]),
+    ("ssv_ams_set_precision", I32, [P, I32]),
+    ("ssv_ams_get_precision", I32, [P, PI32]),
     ("ssv_pcg_solve", I32, [P, P, PU8, ctypes.POINTER(ssv_config), P, P, ctypes.POINTER(ssv_result), PD, I32]),
     ("ssv_pcg_solve_dev", I32, [P, P, PU8, ctypes.POINTER(ssv_config), P, P, ctypes.POINTER(ssv_result), PD, I32]),
 ]

