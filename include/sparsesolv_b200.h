@@ -116,6 +116,15 @@ typedef struct ssv_phase_profile {
 typedef struct ssv_matrix ssv_matrix;   /* device-resident CSR              */
 typedef struct ssv_solver ssv_solver;   /* SparseSolvSolver state           */
 typedef struct ssv_precond ssv_precond; /* IC / AMS / complex-AMS           */
+typedef struct ssv_batch ssv_batch;     /* batched COCR over a frequency family */
+
+/* One timed SpMM launch shape of the batch autotuner. */
+typedef struct ssv_batch_tune_entry {
+    int32_t freq_tile;    /* frequencies whose columns one pass over K and M forms */
+    int32_t lanes;        /* threads per matrix row (32 / lanes rows per warp)     */
+    int32_t grid_x;       /* blocks per frequency tile                             */
+    double microseconds;  /* mean time of one SpMM launch                          */
+} ssv_batch_tune_entry;
 
 /* ---- library ----------------------------------------------------------- */
 void ssv_version(int* major, int* minor, int* patch);
@@ -254,6 +263,40 @@ int ssv_abmc_build(int32_t n, const int32_t* row_ptr, const int32_t* col_idx,
  * upper-triangular pattern. */
 int ssv_level_schedule(int32_t n, const int32_t* row_ptr, const int32_t* col_idx,
                        int32_t upper, int32_t* level_of, int32_t* num_levels);
+
+/* ---- batched COCR over a frequency family (new: no reference counterpart) -
+ * A_f = K + j*omega_f*M for num_freq frequencies (K, M real, square, one size;
+ * their patterns are merged), nrhs right-hand sides per frequency (1 or 4),
+ * one ComplexCompactAMS preconditioner per frequency (pre[f], NULL =
+ * identity; FP64 or FP32 form). Every one of the num_freq*nrhs columns runs
+ * the COCRSolverNGS recurrence (ngsolve/sparsesolv_solvers.hpp:273-369) on the
+ * FreeDofs view: x0 = 0, stop when ||r||/||b|| <= tol, iterations = j+1 on
+ * convergence, maxiter otherwise; a finished column is frozen while the rest
+ * continue. One SpMM pass reads K and M once per tile of frequencies; the tile,
+ * lanes per row and grid are picked at create time by timing the candidates
+ * on this matrix (ssv_batch_tuning lists them). The iteration is one CUDA
+ * graph. The preconditioners and matrices must outlive the batch; Update() of
+ * a preconditioner is picked up by the next solve. */
+int ssv_batch_create(ssv_matrix* K, ssv_matrix* M, int32_t num_freq, const double* omegas,
+                     ssv_precond* const* pre, int32_t nrhs, const uint8_t* freedofs,
+                     ssv_batch** out);
+int ssv_batch_destroy(ssv_batch* b);
+/* rhs, sol: num_freq*nrhs complex vectors of n entries, [f][r][row]
+ * (host pointers; _dev: device pointers). iterations, converged (int32) and
+ * residuals (final ||r||/||b||, double) get num_freq*nrhs entries; each may be
+ * NULL. */
+int ssv_batch_cocr_solve(ssv_batch* b, int32_t maxiter, double tol, const void* rhs, void* sol,
+                         int32_t* iterations, int32_t* converged, double* residuals);
+int ssv_batch_cocr_solve_dev(ssv_batch* b, int32_t maxiter, double tol, const void* d_rhs, void* d_sol,
+                             int32_t* iterations, int32_t* converged, double* residuals);
+/* Autotuner record: up to cap entries, *count = entries measured, *chosen =
+ * index of the shape in use. */
+int ssv_batch_tuning(const ssv_batch* b, ssv_batch_tune_entry* entries, int32_t cap, int32_t* count,
+                     int32_t* chosen);
+/* Device time of the last solve (CUDA events on the library's stream): the
+ * whole solve and its iteration loop, executed loop bodies, kernel launches. */
+int ssv_batch_last_timing(const ssv_batch* b, double* device_ms, double* loop_ms, int32_t* loops,
+                          int64_t* kernel_launches);
 
 /* ---- allocation-free SpMV + dot (no counterpart in the reference) -------- */
 /* y = A x and *d_dot = x^T y for a real CSR matrix (int32 row_ptr/col_idx,

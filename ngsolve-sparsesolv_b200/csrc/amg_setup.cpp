@@ -235,9 +235,19 @@ void l1_norms(const HostCsr& A, std::vector<double>& out) {
 // Pseudo-inverse of the small coarsest matrix through LDL^T: pivots below
 // 1e-13 of the row's diagonal count as zero and drop their component (the
 // gradient-space matrix is singular, constants being in the kernel of G).
-void dense_pseudo_inverse(const HostCsr& A, std::vector<double>& X) {
+// The factors stay separate: the device applies x = L^{-T} (D^+ (L^{-1} b))
+// as two triangular products with the pivot division between them, which is
+// the substitution's arithmetic regrouped. A single explicit X = L^{-T} D^+
+// L^{-1} is not used: when the pivots span many decades (a conducting region
+// next to the 1e-6 mass weight of air gives ~1e13) X's entries are dominated
+// by the smallest pivots and X b loses the other components, enough to stall
+// COCR on the eddy-current systems.
+void dense_ldlt_pseudo(const HostCsr& A, std::vector<double>& linv, std::vector<double>& linvt,
+                       std::vector<double>& piv) {
     const int n = A.n;
-    std::vector<double> L((size_t)n * n, 0.0), d(n, 0.0), w(n), diag0(n);
+    std::vector<double> L((size_t)n * n, 0.0), w(n), diag0(n);
+    piv.assign(n, 0.0);
+    std::vector<double>& d = piv;
     for (int i = 0; i < n; ++i)
         for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) L[(size_t)i * n + A.ci[k]] += A.v[k];
     for (int i = 0; i < n; ++i) diag0[i] = std::abs(L[(size_t)i * n + i]);
@@ -255,8 +265,10 @@ void dense_pseudo_inverse(const HostCsr& A, std::vector<double>& X) {
         }
         for (int k = j + 1; k < n; ++k) L[(size_t)j * n + k] = 0.0;
     }
-    // X = L^{-T} D^+ L^{-1}, column by column (columns in parallel)
-    X.assign((size_t)n * n, 0.0);
+    // L^{-1} (unit lower) by forward substitution, columns in parallel;
+    // linv row-major, linvt = its transpose (row i holds column i of L^{-1})
+    linv.assign((size_t)n * n, 0.0);
+    linvt.assign((size_t)n * n, 0.0);
     auto columns = [&](int c0, int c1) {
         std::vector<double> y(n);
         for (int c = c0; c < c1; ++c) {
@@ -265,13 +277,10 @@ void dense_pseudo_inverse(const HostCsr& A, std::vector<double>& X) {
                 for (int k = 0; k < i; ++k) s -= L[(size_t)i * n + k] * y[k];
                 y[i] = s;
             }
-            for (int i = 0; i < n; ++i) y[i] = d[i] != 0.0 ? y[i] / d[i] : 0.0;
-            for (int i = n - 1; i >= 0; --i) {
-                double s = y[i];
-                for (int k = i + 1; k < n; ++k) s -= L[(size_t)k * n + i] * y[k];
-                y[i] = s;
+            for (int i = 0; i < n; ++i) {
+                linv[(size_t)i * n + c] = y[i];
+                linvt[(size_t)c * n + i] = y[i];
             }
-            for (int i = 0; i < n; ++i) X[(size_t)i * n + c] = y[i];
         }
     };
     const int nt = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
@@ -312,7 +321,7 @@ void AmgHost::setup(const HostCsr& A0) {
     AmgHostLevel& co = levels.back();
     if (co.A.n <= min_coarse * 10) {
         co.direct = true;
-        dense_pseudo_inverse(co.A, co.inv);
+        dense_ldlt_pseudo(co.A, co.linv, co.linvt, co.piv);
     }
 }
 

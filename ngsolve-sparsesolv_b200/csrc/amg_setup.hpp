@@ -24,8 +24,10 @@ HostCsr csr_rap(const HostCsr& A, const HostCsr& P);
 struct AmgHostLevel {
     HostCsr A, P, Pt;
     std::vector<double> l1;
-    bool direct = false;          // coarsest: solved with the dense pseudo-inverse
-    std::vector<double> inv;      // n x n row-major pseudo-inverse (direct only)
+    bool direct = false;          // coarsest: solved through the dense LDL^T pseudo-inverse
+    std::vector<double> linv;     // n x n row-major L^{-1} (unit lower; direct only)
+    std::vector<double> linvt;    // its transpose
+    std::vector<double> piv;      // D, dropped pivots as 0
 };
 
 struct AmgHost {

@@ -12,14 +12,19 @@
 // (complex_compact_ams.hpp:197-201, compact_amg.hpp:724-728), instead of the
 // real one, x += r / l1 (compact_ams.hpp:538-540, compact_amg.hpp:654-656).
 //
-// T is the storage and arithmetic type of the whole cycle: double is the
-// drop-in form; float is the FP32-preconditioner form, where every matrix of
-// the hierarchy (A_bc, G, Pi, A_l, P_l, P_l^T), the l1 norms and the work
-// vectors are FP32 and only the coarsest solve stays FP64 (its pseudo-inverse
-// is FP64 and the product accumulates in FP64). The cycle's input and output
-// are FP64 in both forms: the Krylov recurrences around it never see FP32.
+// T is the storage and arithmetic type of the four subspace AMG hierarchies:
+// double is the drop-in form; float is the FP32-preconditioner form, where the
+// hierarchies' matrices (A_l, P_l, P_l^T), their l1 norms and vectors are FP32
+// while the fine level (A_bc, its l1 norms, the HCurl vectors, the G and Pi
+// transfers) and the coarsest LDL^T solves stay FP64. The fine level cannot be
+// FP32 on the systems this serves: an entry of K + 1e-6 nu M (and the iron's
+// nu = 1e-3) carries its mass part below FP32 resolution, so an FP32 residual
+// has no gradient-space content left and the gradient correction diverges.
+// Kernels that cross between the two accumulate in FP64. The cycle's input
+// and output are FP64 in both forms.
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 #include "amg_setup.hpp"
 #include "objects.cuh"
@@ -72,28 +77,34 @@ __device__ __forceinline__ void load_row(const float* __restrict__ p, float (&o)
     }
 }
 
-template <typename T, int NV, int LANES, int MODE, bool RECIP>
+template <typename A, typename B>
+using wider_t = std::conditional_t<(sizeof(A) >= sizeof(B)), A, B>;
+
+// y (op)= A x with matrix values TV, input TX, output TY; accumulation in the
+// wider of TV and TX.
+template <typename TV, typename TX, typename TY, int NV, int LANES, int MODE, bool RECIP>
 __global__ void __launch_bounds__(kBlock)
-k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ v,
-          const T* __restrict__ x, T* __restrict__ y, const T* __restrict__ b, const T* __restrict__ d, T w,
+k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const TV* __restrict__ v,
+          const TX* __restrict__ x, TY* __restrict__ y, const TY* __restrict__ b, const TY* __restrict__ d, TY w,
           const KState* st) {
+    using TA = wider_t<TV, TX>;
     if (st && st->done) return;
     const int sub = threadIdx.x % LANES;
     const int rpb = kBlock / LANES;
     const int lane_row = (threadIdx.x & 31) / LANES;  // warp-uniform trip count
     for (int row = blockIdx.x * rpb + threadIdx.x / LANES; row - lane_row < n; row += gridDim.x * rpb) {
         const bool valid = row < n;
-        T acc[NV];
+        TA acc[NV];
 #pragma unroll
-        for (int c = 0; c < NV; ++c) acc[c] = T(0);
+        for (int c = 0; c < NV; ++c) acc[c] = TA(0);
         if (valid) {
             const int k1 = rp[row + 1];
             for (int k = rp[row] + sub; k < k1; k += LANES) {
-                const T a = v[k];
-                T xv[NV];
+                const TA a = (TA)v[k];
+                TX xv[NV];
                 load_row<NV>(x + (size_t)ci[k] * NV, xv);
 #pragma unroll
-                for (int c = 0; c < NV; ++c) acc[c] += a * xv[c];
+                for (int c = 0; c < NV; ++c) acc[c] += a * (TA)xv[c];
             }
         }
 #pragma unroll
@@ -104,41 +115,44 @@ k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T
             const size_t base = (size_t)row * NV;
 #pragma unroll
             for (int c = 0; c < NV; ++c) {
+                const TY ac = (TY)acc[c];
                 if constexpr (MODE == MV_AX) {
-                    y[base + c] = acc[c];
+                    y[base + c] = ac;
                 } else if constexpr (MODE == MV_RES) {
-                    y[base + c] = b[base + c] - acc[c];
+                    y[base + c] = b[base + c] - ac;
                 } else if constexpr (MODE == MV_ADD) {
-                    y[base + c] += w * acc[c];
+                    y[base + c] += w * ac;
                 } else {
-                    const T r = b[base + c] - acc[c];
-                    y[base + c] = RECIP ? x[base + c] + r * d[row] : x[base + c] + r / d[row];
+                    const TY r = b[base + c] - ac;
+                    const TY xo = (TY)x[base + c];
+                    y[base + c] = RECIP ? xo + r * d[row] : xo + r / d[row];
                 }
             }
         }
     }
 }
 
-// rx/ry/rz = Pi_{x,y,z}^T r over the shared pattern of G^T (one pass over r)
-template <typename T, int NV, int LANES>
+// rx/ry/rz = Pi_{x,y,z}^T r over the shared pattern of G^T (one pass over r);
+// FP64 values and accumulation, outputs in the hierarchy type TO
+template <typename TO, int NV, int LANES>
 __global__ void __launch_bounds__(kBlock)
-k_mv_pi_restrict(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ px,
-                 const T* __restrict__ py, const T* __restrict__ pz, const T* __restrict__ r, T* __restrict__ ox,
-                 T* __restrict__ oy, T* __restrict__ oz, const KState* st) {
+k_mv_pi_restrict(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ px,
+                 const double* __restrict__ py, const double* __restrict__ pz, const double* __restrict__ r,
+                 TO* __restrict__ ox, TO* __restrict__ oy, TO* __restrict__ oz, const KState* st) {
     if (st && st->done) return;
     const int sub = threadIdx.x % LANES;
     const int rpb = kBlock / LANES;
     const int lane_row = (threadIdx.x & 31) / LANES;
     for (int row = blockIdx.x * rpb + threadIdx.x / LANES; row - lane_row < n; row += gridDim.x * rpb) {
         const bool valid = row < n;
-        T ax[NV], ay[NV], az[NV];
+        double ax[NV], ay[NV], az[NV];
 #pragma unroll
-        for (int c = 0; c < NV; ++c) ax[c] = ay[c] = az[c] = T(0);
+        for (int c = 0; c < NV; ++c) ax[c] = ay[c] = az[c] = 0.0;
         if (valid)
             for (int k = rp[row] + sub; k < rp[row + 1]; k += LANES) {
-                T rr[NV];
+                double rr[NV];
                 load_row<NV>(r + (size_t)ci[k] * NV, rr);
-                const T vx = px[k], vy = py[k], vz = pz[k];
+                const double vx = px[k], vy = py[k], vz = pz[k];
 #pragma unroll
                 for (int c = 0; c < NV; ++c) {
                     ax[c] += vx * rr[c];
@@ -157,42 +171,44 @@ k_mv_pi_restrict(int n, const int* __restrict__ rp, const int* __restrict__ ci, 
         if (valid && sub == 0)
 #pragma unroll
             for (int c = 0; c < NV; ++c) {
-                ox[(size_t)row * NV + c] = ax[c];
-                oy[(size_t)row * NV + c] = ay[c];
-                oz[(size_t)row * NV + c] = az[c];
+                ox[(size_t)row * NV + c] = (TO)ax[c];
+                oy[(size_t)row * NV + c] = (TO)ay[c];
+                oz[(size_t)row * NV + c] = (TO)az[c];
             }
     }
 }
 
 // x += w Pix gx; x += w Piy gy; x += w Piz gz (in this order per row, as the
-// reference's three MultAdd calls) over the shared pattern of G
-template <typename T, int NV, int LANES>
+// reference's three MultAdd calls) over the shared pattern of G; x FP64,
+// corrections in the hierarchy type TG, FP64 accumulation
+template <typename TG, int NV, int LANES>
 __global__ void __launch_bounds__(kBlock)
-k_mv_pi_prolong(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ px,
-                const T* __restrict__ py, const T* __restrict__ pz, const T* __restrict__ gx,
-                const T* __restrict__ gy, const T* __restrict__ gz, T* __restrict__ x, T w, const KState* st) {
+k_mv_pi_prolong(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ px,
+                const double* __restrict__ py, const double* __restrict__ pz, const TG* __restrict__ gx,
+                const TG* __restrict__ gy, const TG* __restrict__ gz, double* __restrict__ x, double w,
+                const KState* st) {
     if (st && st->done) return;
     const int sub = threadIdx.x % LANES;
     const int rpb = kBlock / LANES;
     const int lane_row = (threadIdx.x & 31) / LANES;
     for (int row = blockIdx.x * rpb + threadIdx.x / LANES; row - lane_row < n; row += gridDim.x * rpb) {
         const bool valid = row < n;
-        T sx[NV], sy[NV], sz[NV];
+        double sx[NV], sy[NV], sz[NV];
 #pragma unroll
-        for (int c = 0; c < NV; ++c) sx[c] = sy[c] = sz[c] = T(0);
+        for (int c = 0; c < NV; ++c) sx[c] = sy[c] = sz[c] = 0.0;
         if (valid)
             for (int k = rp[row] + sub; k < rp[row + 1]; k += LANES) {
                 const size_t j = (size_t)ci[k] * NV;
-                T vgx[NV], vgy[NV], vgz[NV];
+                TG vgx[NV], vgy[NV], vgz[NV];
                 load_row<NV>(gx + j, vgx);
                 load_row<NV>(gy + j, vgy);
                 load_row<NV>(gz + j, vgz);
-                const T vx = px[k], vy = py[k], vz = pz[k];
+                const double vx = px[k], vy = py[k], vz = pz[k];
 #pragma unroll
                 for (int c = 0; c < NV; ++c) {
-                    sx[c] += vx * vgx[c];
-                    sy[c] += vy * vgy[c];
-                    sz[c] += vz * vgz[c];
+                    sx[c] += vx * (double)vgx[c];
+                    sy[c] += vy * (double)vgy[c];
+                    sz[c] += vz * (double)vgz[c];
                 }
             }
 #pragma unroll
@@ -206,7 +222,7 @@ k_mv_pi_prolong(int n, const int* __restrict__ rp, const int* __restrict__ ci, c
         if (valid && sub == 0)
 #pragma unroll
             for (int c = 0; c < NV; ++c) {
-                T t = x[(size_t)row * NV + c];
+                double t = x[(size_t)row * NV + c];
                 t += w * sx[c];
                 t += w * sy[c];
                 t += w * sz[c];
@@ -240,20 +256,23 @@ __global__ void k_mv_mask_copy(int n, const TI* __restrict__ in, const uint8_t* 
     }
 }
 
-// y = X b, X dense n x n row-major FP64 (coarsest pseudo-inverse), FP64
-// accumulation in both forms; warp per row
+// Coarsest solve x = L^{-T} (D^+ (L^{-1} b)) (the LDL^T pseudo-inverse kept
+// factored), FP64 factors and FP64 accumulation in both forms; warp per row.
+// Forward part: z_i = (sum_{k<=i} Linv[i][k] b_k) / d_i, or 0 for a dropped
+// pivot; z is FP64 scratch.
 template <typename T, int NV>
 __global__ void __launch_bounds__(kBlock)
-k_mv_gemv(int n, const double* __restrict__ X, const T* __restrict__ b, T* __restrict__ y, const KState* st) {
+k_mv_coarse_fwd(int n, const double* __restrict__ Li, const double* __restrict__ piv, const T* __restrict__ b,
+                double* __restrict__ z, const KState* st) {
     if (st && st->done) return;
     const int lane = threadIdx.x & 31;
     for (int row = blockIdx.x * (kBlock / 32) + threadIdx.x / 32; row < n; row += gridDim.x * (kBlock / 32)) {
         double acc[NV];
 #pragma unroll
         for (int c = 0; c < NV; ++c) acc[c] = 0.0;
-        const double* xr = X + (size_t)row * n;
-        for (int k = lane; k < n; k += 32) {
-            const double a = xr[k];
+        const double* lr = Li + (size_t)row * n;
+        for (int k = lane; k <= row; k += 32) {
+            const double a = lr[k];
 #pragma unroll
             for (int c = 0; c < NV; ++c) acc[c] += a * (double)b[(size_t)k * NV + c];
         }
@@ -261,9 +280,38 @@ k_mv_gemv(int n, const double* __restrict__ X, const T* __restrict__ b, T* __res
         for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
             for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
+        if (lane == 0) {
+            const double d = piv[row];
+#pragma unroll
+            for (int c = 0; c < NV; ++c) z[(size_t)row * NV + c] = d != 0.0 ? acc[c] / d : 0.0;
+        }
+    }
+}
+
+// Backward part: x_i = sum_{k>=i} Linv[k][i] z_k, read from the transposed copy.
+template <typename T, int NV>
+__global__ void __launch_bounds__(kBlock)
+k_mv_coarse_bwd(int n, const double* __restrict__ LiT, const double* __restrict__ z, T* __restrict__ x,
+                const KState* st) {
+    if (st && st->done) return;
+    const int lane = threadIdx.x & 31;
+    for (int row = blockIdx.x * (kBlock / 32) + threadIdx.x / 32; row < n; row += gridDim.x * (kBlock / 32)) {
+        double acc[NV];
+#pragma unroll
+        for (int c = 0; c < NV; ++c) acc[c] = 0.0;
+        const double* lr = LiT + (size_t)row * n;
+        for (int k = row + lane; k < n; k += 32) {
+            const double a = lr[k];
+#pragma unroll
+            for (int c = 0; c < NV; ++c) acc[c] += a * z[(size_t)k * NV + c];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
         if (lane == 0)
 #pragma unroll
-            for (int c = 0; c < NV; ++c) y[(size_t)row * NV + c] = (T)acc[c];
+            for (int c = 0; c < NV; ++c) x[(size_t)row * NV + c] = (T)acc[c];
     }
 }
 
@@ -320,7 +368,8 @@ struct AmgDevLevel {
     DevCsr A, P, Pt;
     DualVec l1, il1;
     bool direct = false;
-    DevBuf<double> X;
+    DevBuf<double> Li, LiT, piv;  // coarsest: LDL^T factors (FP64 in both forms)
+    DevBuf<double> cz;            // coarsest: FP64 scratch between the two triangular products
     WorkVec b, xa, xb, r;  // NV-column work vectors of this level
 };
 
@@ -331,10 +380,11 @@ struct AmsState {
     bool fp32 = false;
     int ndof_complex = 0;
     AmsHost host;
-    DevCsr A_bc, G, Gt;
-    DualVec fine_l1, fine_il1, Piv[3], Pitv[3];
+    DevCsr A_bc, G, Gt;                          // FP64 in both forms
+    DevBuf<double> fine_l1, fine_il1, Piv[3], Pitv[3];
     std::vector<AmgDevLevel> amg[4];
-    WorkVec b0, xa, xb, r, rs[4];
+    DevBuf<double> b0, xa, xb, r;                // fine level, FP64
+    WorkVec rs[4];                               // subspace right-hand sides, hierarchy type
     DevBuf<uint8_t> fd;
     bool has_fd = false;
     std::vector<uint8_t> h_fd;
@@ -343,20 +393,28 @@ struct AmsState {
 
 void ams_free(AmsState* a) { delete a; }
 
-template <typename T, int NV, int MODE, bool RECIP>
-static void mv_spmv(const DevCsr& A, const T* x, T* y, const T* b, const T* d, T w, const KState* st,
+template <typename TV, typename TX, typename TY, int NV, int MODE, bool RECIP>
+static void mv_spmv(const DevCsr& A, const TX* x, TY* y, const TY* b, const TY* d, TY w, const KState* st,
                     cudaStream_t s) {
     const int lanes = A.lanes;
     const int rpb = kBlock / lanes;
     const int grid = std::max(1, std::min((A.n + rpb - 1) / rpb, sm_count() * 8));
-    const T* v = A.val<T>();
+    const TV* v = A.val<TV>();
+#define SSV_MV_CASE(L)                                                                                   \
+    case L:                                                                                              \
+        k_mv_spmv<TV, TX, TY, NV, L, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, \
+                                                                           y, b, d, w, st);              \
+        break;
     switch (lanes) {
-        case 2: k_mv_spmv<T, NV, 2, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, b, d, w, st); break;
-        case 4: k_mv_spmv<T, NV, 4, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, b, d, w, st); break;
-        case 8: k_mv_spmv<T, NV, 8, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, b, d, w, st); break;
-        case 16: k_mv_spmv<T, NV, 16, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, b, d, w, st); break;
-        default: k_mv_spmv<T, NV, 32, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, b, d, w, st); break;
+        SSV_MV_CASE(2)
+        SSV_MV_CASE(4)
+        SSV_MV_CASE(8)
+        SSV_MV_CASE(16)
+        default:
+            k_mv_spmv<TV, TX, TY, NV, 32, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x,
+                                                                                y, b, d, w, st);
     }
+#undef SSV_MV_CASE
 }
 
 template <typename T, int NV, bool RECIP>
@@ -379,14 +437,15 @@ static T* vcycle(std::vector<AmgDevLevel>& L, int l, const T* b, int num_smooth,
     T* alt = lv.xb.as<T>();
     auto sweep = [&](int count) {
         for (int k = 0; k < count; ++k) {
-            mv_spmv<T, NV, MV_JAC, RECIP>(lv.A, cur, alt, b, d, T(0), st, s);
+            mv_spmv<T, T, T, NV, MV_JAC, RECIP>(lv.A, cur, alt, b, d, T(0), st, s);
             std::swap(cur, alt);
         }
     };
     if (l == (int)L.size() - 1) {
         if (lv.direct) {
-            k_mv_gemv<T, NV><<<std::max(1, std::min((lv.A.n + 7) / 8, sm_count() * 4)), kBlock, 0, s>>>(
-                lv.A.n, lv.X.get(), b, cur, st);
+            const int g = std::max(1, std::min((lv.A.n + 7) / 8, sm_count() * 4));
+            k_mv_coarse_fwd<T, NV><<<g, kBlock, 0, s>>>(lv.A.n, lv.Li.get(), lv.piv.get(), b, lv.cz.get(), st);
+            k_mv_coarse_bwd<T, NV><<<g, kBlock, 0, s>>>(lv.A.n, lv.LiT.get(), lv.cz.get(), cur, st);
         } else {  // 10 l1-Jacobi sweeps from x = 0
             first_sweep<T, NV, RECIP>(lv.A.n, b, d, cur, st, s);
             sweep(9);
@@ -396,36 +455,36 @@ static T* vcycle(std::vector<AmgDevLevel>& L, int l, const T* b, int num_smooth,
     // pre-smoothing from x = 0: the first sweep is x = b / l1
     first_sweep<T, NV, RECIP>(lv.A.n, b, d, cur, st, s);
     sweep(num_smooth - 1);
-    mv_spmv<T, NV, MV_RES, RECIP>(lv.A, cur, lv.r.as<T>(), b, nullptr, T(0), st, s);
+    mv_spmv<T, T, T, NV, MV_RES, RECIP>(lv.A, cur, lv.r.as<T>(), b, nullptr, T(0), st, s);
     AmgDevLevel& nx = L[l + 1];
-    mv_spmv<T, NV, MV_AX, RECIP>(lv.Pt, lv.r.as<T>(), nx.b.as<T>(), nullptr, nullptr, T(0), st, s);
+    mv_spmv<T, T, T, NV, MV_AX, RECIP>(lv.Pt, lv.r.as<T>(), nx.b.as<T>(), nullptr, nullptr, T(0), st, s);
     T* ec = vcycle<T, NV, RECIP>(L, l + 1, nx.b.as<T>(), num_smooth, st, s);
-    mv_spmv<T, NV, MV_ADD, RECIP>(lv.P, ec, cur, nullptr, nullptr, T(1), st, s);
+    mv_spmv<T, T, T, NV, MV_ADD, RECIP>(lv.P, ec, cur, nullptr, nullptr, T(1), st, s);
     sweep(num_smooth);
     return cur;
 }
 
 template <typename T, int NV, int LANES>
-static void pi_restrict_l(const AmsState& a, const T* r, T* ox, T* oy, T* oz, const KState* st, cudaStream_t s) {
+static void pi_restrict_l(const AmsState& a, const double* r, T* ox, T* oy, T* oz, const KState* st,
+                          cudaStream_t s) {
     const int rpb = kBlock / LANES;
     const int grid = std::max(1, std::min((a.Gt.n + rpb - 1) / rpb, sm_count() * 8));
-    k_mv_pi_restrict<T, NV, LANES><<<grid, kBlock, 0, s>>>(a.Gt.n, a.Gt.rp.get(), a.Gt.ci.get(),
-                                                           a.Pitv[0].get<T>(), a.Pitv[1].get<T>(),
-                                                           a.Pitv[2].get<T>(), r, ox, oy, oz, st);
+    k_mv_pi_restrict<T, NV, LANES><<<grid, kBlock, 0, s>>>(a.Gt.n, a.Gt.rp.get(), a.Gt.ci.get(), a.Pitv[0].get(),
+                                                           a.Pitv[1].get(), a.Pitv[2].get(), r, ox, oy, oz, st);
 }
 
 template <typename T, int NV, int LANES>
-static void pi_prolong_l(const AmsState& a, const T* gx, const T* gy, const T* gz, T* x, const KState* st,
+static void pi_prolong_l(const AmsState& a, const T* gx, const T* gy, const T* gz, double* x, const KState* st,
                          cudaStream_t s) {
     const int rpb = kBlock / LANES;
     const int grid = std::max(1, std::min((a.G.n + rpb - 1) / rpb, sm_count() * 8));
-    k_mv_pi_prolong<T, NV, LANES><<<grid, kBlock, 0, s>>>(a.G.n, a.G.rp.get(), a.G.ci.get(), a.Piv[0].get<T>(),
-                                                          a.Piv[1].get<T>(), a.Piv[2].get<T>(), gx, gy, gz, x,
-                                                          (T)a.w, st);
+    k_mv_pi_prolong<T, NV, LANES><<<grid, kBlock, 0, s>>>(a.G.n, a.G.rp.get(), a.G.ci.get(), a.Piv[0].get(),
+                                                          a.Piv[1].get(), a.Piv[2].get(), gx, gy, gz, x, a.w, st);
 }
 
 template <typename T, int NV>
-static void pi_restrict(const AmsState& a, const T* r, T* ox, T* oy, T* oz, const KState* st, cudaStream_t s) {
+static void pi_restrict(const AmsState& a, const double* r, T* ox, T* oy, T* oz, const KState* st,
+                        cudaStream_t s) {
     switch (a.Gt.lanes) {
         case 2: pi_restrict_l<T, NV, 2>(a, r, ox, oy, oz, st, s); break;
         case 4: pi_restrict_l<T, NV, 4>(a, r, ox, oy, oz, st, s); break;
@@ -436,7 +495,7 @@ static void pi_restrict(const AmsState& a, const T* r, T* ox, T* oy, T* oz, cons
 }
 
 template <typename T, int NV>
-static void pi_prolong(const AmsState& a, const T* gx, const T* gy, const T* gz, T* x, const KState* st,
+static void pi_prolong(const AmsState& a, const T* gx, const T* gy, const T* gz, double* x, const KState* st,
                        cudaStream_t s) {
     switch (a.G.lanes) {
         case 2: pi_prolong_l<T, NV, 2>(a, gx, gy, gz, x, st, s); break;
@@ -454,41 +513,41 @@ template <typename T, int NV, bool RECIP>
 static void ams_cycle(AmsState& a, const double* in, double* out, const KState* st, cudaStream_t s) {
     const int n = a.nhc;
     const uint8_t* fd = a.has_fd ? a.fd.get() : nullptr;
-    const T* d = RECIP ? a.fine_il1.get<T>() : a.fine_l1.get<T>();
-    T* b0 = a.b0.as<T>();
-    T* cur = a.xa.as<T>();
-    T* alt = a.xb.as<T>();
-    T* r = a.r.as<T>();
+    const double* d = RECIP ? a.fine_il1.get() : a.fine_l1.get();
+    double* b0 = a.b0.get();
+    double* cur = a.xa.get();
+    double* alt = a.xb.get();
+    double* r = a.r.get();
     const int gm = grid_for((int64_t)n * NV, kBlock);
-    k_mv_mask_copy<double, T, NV><<<gm, kBlock, 0, s>>>(n, in, fd, b0, st);
+    k_mv_mask_copy<double, double, NV><<<gm, kBlock, 0, s>>>(n, in, fd, b0, st);
     bool fresh = true;  // x == 0
     auto fine_smooth = [&]() {
         for (int k = 0; k < a.num_smooth; ++k) {
             if (fresh) {
-                first_sweep<T, NV, RECIP>(n, b0, d, cur, st, s);
+                first_sweep<double, NV, RECIP>(n, b0, d, cur, st, s);
                 fresh = false;
             } else {
-                mv_spmv<T, NV, MV_JAC, RECIP>(a.A_bc, cur, alt, b0, d, T(0), st, s);
+                mv_spmv<double, double, double, NV, MV_JAC, RECIP>(a.A_bc, cur, alt, b0, d, 0.0, st, s);
                 std::swap(cur, alt);
             }
         }
     };
     auto ensure_x = [&]() {
         if (fresh) {
-            SSV_CUDA(cudaMemsetAsync(cur, 0, sizeof(T) * (size_t)n * NV, s));
+            SSV_CUDA(cudaMemsetAsync(cur, 0, sizeof(double) * (size_t)n * NV, s));
             fresh = false;
         }
     };
     auto gradient = [&]() {
         ensure_x();
-        mv_spmv<T, NV, MV_RES, RECIP>(a.A_bc, cur, r, b0, nullptr, T(0), st, s);
-        mv_spmv<T, NV, MV_AX, RECIP>(a.Gt, r, a.rs[0].as<T>(), nullptr, nullptr, T(0), st, s);
+        mv_spmv<double, double, double, NV, MV_RES, RECIP>(a.A_bc, cur, r, b0, nullptr, 0.0, st, s);
+        mv_spmv<double, double, T, NV, MV_AX, RECIP>(a.Gt, r, a.rs[0].as<T>(), nullptr, nullptr, T(0), st, s);
         T* g = vcycle<T, NV, RECIP>(a.amg[0], 0, a.rs[0].as<T>(), 1, st, s);
-        mv_spmv<T, NV, MV_ADD, RECIP>(a.G, g, cur, nullptr, nullptr, (T)a.w, st, s);
+        mv_spmv<double, T, double, NV, MV_ADD, RECIP>(a.G, g, cur, nullptr, nullptr, a.w, st, s);
     };
     auto nodal = [&]() {
         ensure_x();
-        mv_spmv<T, NV, MV_RES, RECIP>(a.A_bc, cur, r, b0, nullptr, T(0), st, s);
+        mv_spmv<double, double, double, NV, MV_RES, RECIP>(a.A_bc, cur, r, b0, nullptr, 0.0, st, s);
         pi_restrict<T, NV>(a, r, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), st, s);
         T* gx = vcycle<T, NV, RECIP>(a.amg[1], 0, a.rs[1].as<T>(), 1, st, s);
         T* gy = vcycle<T, NV, RECIP>(a.amg[2], 0, a.rs[2].as<T>(), 1, st, s);
@@ -501,7 +560,7 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
         fine_smooth(); gradient(); nodal(); gradient(); fine_smooth();
     }
     ensure_x();
-    k_mv_mask_copy<T, double, NV><<<gm, kBlock, 0, s>>>(n, cur, fd, out, st);
+    k_mv_mask_copy<double, double, NV><<<gm, kBlock, 0, s>>>(n, cur, fd, out, st);
     SSV_LAUNCH_CHECK();
 }
 
@@ -527,6 +586,7 @@ static void ams_reserve(AmsState& a, int nv) {
             lv.xa.alloc(m);
             lv.xb.alloc(m);
             lv.r.alloc(m);
+            if (lv.direct) lv.cz.alloc(m);
         }
     const size_t mh = (size_t)a.nhc * nv, m1 = (size_t)a.nh1 * nv;
     a.b0.alloc(mh);
@@ -535,6 +595,7 @@ static void ams_reserve(AmsState& a, int nv) {
     a.r.alloc(mh);
     for (int s = 0; s < 4; ++s) a.rs[s].alloc(m1);
     a.nv_alloc = nv;
+    ++a.gen;  // new work buffers: graphs that captured the old ones must be rebuilt
 }
 
 static std::vector<double> reciprocal(const std::vector<double>& v) {
@@ -543,22 +604,24 @@ static std::vector<double> reciprocal(const std::vector<double>& v) {
     return r;
 }
 
-// Geometry part (G, G^T, Pi) in the chosen form.
+// Geometry part (G, G^T, Pi): FP64 in both forms.
 static void ams_upload_geometry(AmsState& a, cudaStream_t s) {
-    a.G.upload(a.host.G, a.fp32, s);
-    a.Gt.upload(a.host.Gt, a.fp32, s);
+    a.G.upload(a.host.G, false, s);
+    a.Gt.upload(a.host.Gt, false, s);
     for (int d = 0; d < 3; ++d) {
-        a.Piv[d].set(a.host.Pi[d].v, a.fp32, s);
-        a.Pitv[d].set(a.host.Pit[d].v, a.fp32, s);
+        a.Piv[d].upload(a.host.Pi[d].v.data(), a.host.Pi[d].v.size(), s);
+        a.Pitv[d].upload(a.host.Pit[d].v.data(), a.host.Pit[d].v.size(), s);
     }
 }
 
-// Matrix part (A_bc, l1 norms, the four AMG hierarchies) in the chosen form.
+// Matrix part: A_bc and its l1 norms (FP64), the four AMG hierarchies (in the
+// chosen form; the coarsest factors FP64).
 static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
     const int nv = std::max(a.nv_alloc, a.complex_form ? 2 : 1);
-    a.A_bc.upload(a.host.A_bc, a.fp32, s);
-    a.fine_l1.set(a.host.fine_l1, a.fp32, s);
-    a.fine_il1.set(reciprocal(a.host.fine_l1), a.fp32, s);
+    a.A_bc.upload(a.host.A_bc, false, s);
+    a.fine_l1.upload(a.host.fine_l1.data(), a.host.fine_l1.size(), s);
+    const std::vector<double> il1 = reciprocal(a.host.fine_l1);
+    a.fine_il1.upload(il1.data(), il1.size(), s);
     for (int sub = 0; sub < 4; ++sub) {
         const auto& hl = a.host.amg[sub].levels;
         a.amg[sub].clear();
@@ -573,7 +636,11 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
                 dl.Pt.upload(hl[l].Pt, a.fp32, s);
             }
             dl.direct = hl[l].direct;
-            if (dl.direct) dl.X.upload(hl[l].inv.data(), hl[l].inv.size(), s);  // FP64 in both forms
+            if (dl.direct) {  // FP64 in both forms
+                dl.Li.upload(hl[l].linv.data(), hl[l].linv.size(), s);
+                dl.LiT.upload(hl[l].linvt.data(), hl[l].linvt.size(), s);
+                dl.piv.upload(hl[l].piv.data(), hl[l].piv.size(), s);
+            }
         }
     }
     a.nv_alloc = 0;
@@ -631,7 +698,6 @@ void ams_set_precision(AmsState* a, int precision) {
     if (lo == a->fp32) return;
     cudaStream_t s = stream();
     a->fp32 = lo;
-    ams_upload_geometry(*a, s);
     ams_upload_matrix(*a, s);
     ++a->gen;
     SSV_CUDA(cudaStreamSynchronize(s));

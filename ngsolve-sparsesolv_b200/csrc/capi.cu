@@ -358,6 +358,55 @@ int ssv_ams_get_precision(const ssv_precond* p, int32_t* precision) {
     });
 }
 
+int ssv_batch_create(ssv_matrix* K, ssv_matrix* M, int32_t num_freq, const double* omegas,
+                     ssv_precond* const* pre, int32_t nrhs, const uint8_t* freedofs, ssv_batch** out) {
+    return guarded([&] {
+        if (!out) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_batch_create: NULL out");
+        *out = ssv::batch_create(K, M, num_freq, omegas, pre, nrhs, freedofs);
+    });
+}
+
+int ssv_batch_destroy(ssv_batch* b) {
+    return guarded([&] { ssv::batch_destroy(b); });
+}
+
+int ssv_batch_cocr_solve(ssv_batch* b, int32_t maxiter, double tol, const void* rhs, void* sol,
+                         int32_t* iterations, int32_t* converged, double* residuals) {
+    return guarded([&] {
+        if (!b || !rhs || !sol) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_batch_cocr_solve: NULL argument");
+        ssv::batch_cocr_solve_host(b, maxiter, tol, rhs, sol, iterations, converged, residuals);
+    });
+}
+
+int ssv_batch_cocr_solve_dev(ssv_batch* b, int32_t maxiter, double tol, const void* d_rhs, void* d_sol,
+                             int32_t* iterations, int32_t* converged, double* residuals) {
+    return guarded([&] {
+        if (!b || !d_rhs || !d_sol) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_batch_cocr_solve_dev: NULL argument");
+        ssv::batch_cocr_solve_dev(b, maxiter, tol, d_rhs, d_sol, iterations, converged, residuals);
+    });
+}
+
+int ssv_batch_tuning(const ssv_batch* b, ssv_batch_tune_entry* entries, int32_t cap, int32_t* count,
+                     int32_t* chosen) {
+    return guarded([&] {
+        if (!b || !count || !chosen || (cap > 0 && !entries))
+            ssv::fail(SSV_ERR_INVALID_ARG, "ssv_batch_tuning: bad argument");
+        int ch = -1;
+        *count = ssv::batch_tuning(b, entries, cap, &ch);
+        *chosen = ch;
+    });
+}
+
+int ssv_batch_last_timing(const ssv_batch* b, double* device_ms, double* loop_ms, int32_t* loops,
+                          int64_t* kernel_launches) {
+    return guarded([&] {
+        if (!b) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_batch_last_timing: NULL batch");
+        int lp = 0;
+        ssv::batch_last_timing(b, device_ms, loop_ms, &lp, kernel_launches);
+        if (loops) *loops = lp;
+    });
+}
+
 int ssv_pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, const ssv_config* cfg,
                       const void* d_b, void* d_x, ssv_result* res, double* history, int32_t history_cap) {
     return guarded([&] {

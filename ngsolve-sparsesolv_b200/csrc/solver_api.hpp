@@ -47,6 +47,17 @@ int ams_precision(const AmsState* a);
 void ams_reserve_block(AmsState* a, int nrhs);
 void ams_apply_block(AmsState* a, const double* in, double* out, int nrhs, const KState* st, cudaStream_t s);
 
+// Batched COCR over a frequency family (batch.cu)
+ssv_batch* batch_create(ssv_matrix* K, ssv_matrix* M, int F, const double* omegas, ssv_precond* const* pre, int R,
+                        const uint8_t* fd);
+void batch_destroy(ssv_batch* B);
+void batch_cocr_solve_dev(ssv_batch* B, int maxiter, double tol, const void* d_b, void* d_x, int* iters, int* conv,
+                          double* res);
+void batch_cocr_solve_host(ssv_batch* B, int maxiter, double tol, const void* b, void* x, int* iters, int* conv,
+                           double* res);
+int batch_tuning(const ssv_batch* B, ssv_batch_tune_entry* e, int cap, int* chosen);
+void batch_last_timing(const ssv_batch* B, double* ms, double* loop_ms, int* loops, int64_t* launches);
+
 // CG with an external preconditioner and an initial guess (cocr_ngs.cu)
 void pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, const ssv_config& cfg, const void* d_b,
                    void* d_x, ssv_result* res, double* hist, int hist_cap);

@@ -26,6 +26,7 @@ __all__ = [
     "COCRSolver", "COCRSolverD", "COCRSolverC", "has_compact_ams",
     "CompactAMSPreconditioner", "CompactAMSPreconditionerImpl",
     "ComplexCompactAMSPreconditioner", "ComplexCompactAMSPreconditionerImpl", "PCGSolver",
+    "BatchedCOCRSolver",
 ]
 
 
@@ -676,3 +677,94 @@ class PCGSolver:
         y = np.zeros(self._mat.n, dtype=self._mat.dtype)
         self.Mult(vec, y)
         return y
+
+
+# ---------------------------------------------------------------------------
+# BatchedCOCRSolver -- many frequencies x right-hand sides in one launch graph
+# (new: no reference counterpart; each column runs COCRSolver's recurrence)
+# ---------------------------------------------------------------------------
+
+class BatchedCOCRSolver:
+    """COCR on the family A_f = K + 1j*omegas[f]*M for every frequency f and
+    ``nrhs`` right-hand sides per frequency, advanced together.
+
+    K, M: real sparse matrices of one size (patterns merged). ``pres``: one
+    ComplexCompactAMSPreconditioner per frequency (or None = identity), FP64 or
+    FP32 form. ``Solve(B)`` takes B of shape (F, nrhs, n) complex and returns X
+    of the same shape; ``iterations``, ``converged`` and ``residuals`` are then
+    (F, nrhs) arrays with the COCRSolver meaning per column. The SpMM launch
+    shape is autotuned at construction (``tuning``).
+    """
+
+    def __init__(self, K, M, omegas, pres, nrhs=1, freedofs=None, maxiter=500, tol=1e-8):
+        self._K = K if isinstance(K, _Matrix) else _Matrix(K)
+        self._M = M if isinstance(M, _Matrix) else _Matrix(M)
+        if self._K.cplx or self._M.cplx:
+            raise TypeError("BatchedCOCRSolver: K and M must be real")
+        self._om = np.ascontiguousarray(np.asarray(omegas, dtype=np.float64).ravel())
+        self.F = int(self._om.shape[0])
+        self.nrhs = int(nrhs)
+        self.n = self._K.n
+        pres = list(pres) if pres is not None else [None] * self.F
+        if len(pres) != self.F:
+            raise ValueError("BatchedCOCRSolver: one preconditioner (or None) per frequency")
+        self._pres = pres  # the batch keeps raw handles: hold the objects
+        self._fd = _freedofs_array(freedofs, self.n)
+        self.maxiter = int(maxiter)
+        self.tol = float(tol)
+        self._lib = _capi.load()
+        harr = (ctypes.c_void_p * self.F)(*[(p._h.value if p is not None else None) for p in pres])
+        h = ctypes.c_void_p()
+        check(self._lib.ssv_batch_create(self._K.h, self._M.h, self.F, self._om.ctypes.data_as(_capi.PD),
+                                         ctypes.cast(harr, _capi.PP), self.nrhs, _capi.u8ptr(self._fd),
+                                         ctypes.byref(h)))
+        self._h = h
+        shape = (self.F, self.nrhs)
+        self.iterations = np.zeros(shape, np.int32)
+        self.converged = np.zeros(shape, np.int32)
+        self.residuals = np.zeros(shape)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self._lib.ssv_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def Solve(self, B):
+        b = np.ascontiguousarray(np.asarray(B, dtype=np.complex128))
+        if b.shape != (self.F, self.nrhs, self.n):
+            raise ValueError(f"BatchedCOCRSolver: right-hand sides must have shape {(self.F, self.nrhs, self.n)}")
+        x = np.empty_like(b)
+        check(self._lib.ssv_batch_cocr_solve(self._h, self.maxiter, self.tol, _capi.vptr(b), _capi.vptr(x),
+                                             _capi.i32ptr(self.iterations), _capi.i32ptr(self.converged),
+                                             self.residuals.ctypes.data_as(_capi.PD)))
+        return x
+
+    def solve_dev(self, d_b, d_x):
+        """Device-pointer form (integers: addresses of (F, nrhs, n) complex128 arrays in HBM)."""
+        check(self._lib.ssv_batch_cocr_solve_dev(self._h, self.maxiter, self.tol, ctypes.c_void_p(d_b),
+                                                 ctypes.c_void_p(d_x), _capi.i32ptr(self.iterations),
+                                                 _capi.i32ptr(self.converged),
+                                                 self.residuals.ctypes.data_as(_capi.PD)))
+
+    @property
+    def tuning(self):
+        """{"candidates": [(freq_tile, lanes, grid_x, us), ...], "chosen": (freq_tile, lanes, grid_x, us)}"""
+        cap = 64
+        arr = (_capi.ssv_batch_tune_entry * cap)()
+        cnt, ch = ctypes.c_int32(), ctypes.c_int32()
+        check(self._lib.ssv_batch_tuning(self._h, arr, cap, ctypes.byref(cnt), ctypes.byref(ch)))
+        rows = [(e.freq_tile, e.lanes, e.grid_x, e.microseconds) for e in arr[: min(cnt.value, cap)]]
+        return {"candidates": rows, "chosen": rows[ch.value] if 0 <= ch.value < len(rows) else None}
+
+    @property
+    def last_timing(self):
+        """Device time of the last solve: {"device_ms", "loop_ms", "loops", "kernel_launches"}."""
+        ms, lms = ctypes.c_double(), ctypes.c_double()
+        loops, nk = ctypes.c_int32(), ctypes.c_int64()
+        check(self._lib.ssv_batch_last_timing(self._h, ctypes.byref(ms), ctypes.byref(lms), ctypes.byref(loops),
+                                              ctypes.byref(nk)))
+        return {"device_ms": ms.value, "loop_ms": lms.value, "loops": loops.value, "kernel_launches": nk.value}

@@ -78,6 +78,15 @@ class ssv_result(ctypes.Structure):
     ]
 
 
+class ssv_batch_tune_entry(ctypes.Structure):
+    _fields_ = [
+        ("freq_tile", ctypes.c_int32),
+        ("lanes", ctypes.c_int32),
+        ("grid_x", ctypes.c_int32),
+        ("microseconds", ctypes.c_double),
+    ]
+
+
 SSV_MAX_PHASES = 8
 
 
@@ -179,6 +188,12 @@ SIGNATURES = [
     ("ssv_ams_update", I32, [P, P]),
     ("ssv_ams_levels", I32, [P, I32, PI32, I32, PI32]),
     ("ssv_ams_set_precision", I32, [P, I32]),
+    ("ssv_batch_create", I32, [P, P, I32, PD, PP, I32, PU8, PP]),
+    ("ssv_batch_destroy", I32, [P]),
+    ("ssv_batch_cocr_solve", I32, [P, I32, ctypes.c_double, P, P, PI32, PI32, PD]),
+    ("ssv_batch_cocr_solve_dev", I32, [P, I32, ctypes.c_double, P, P, PI32, PI32, PD]),
+    ("ssv_batch_tuning", I32, [P, ctypes.POINTER(ssv_batch_tune_entry), I32, PI32, PI32]),
+    ("ssv_batch_last_timing", I32, [P, PD, PD, PI32, ctypes.POINTER(ctypes.c_int64)]),
     ("ssv_ams_get_precision", I32, [P, PI32]),
     ("ssv_pcg_solve", I32, [P, P, PU8, ctypes.POINTER(ssv_config), P, P, ctypes.POINTER(ssv_result), PD, I32]),
     ("ssv_pcg_solve_dev", I32, [P, P, PU8, ctypes.POINTER(ssv_config), P, P, ctypes.POINTER(ssv_result), PD, I32]),

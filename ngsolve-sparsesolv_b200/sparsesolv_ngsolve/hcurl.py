@@ -224,3 +224,60 @@ def eddy_current(nc: int, freq: float = 3e4, sigma: float = 5.8e7, nu_r_core: fl
     f = loop_source(m, z_levels=(0.5,), squares=((0.1, 0.9), (0.15, 0.85))) * fd
     return dict(mesh=m, A=A, a_real=a_real, G=G, freedofs=fd, f=f.astype(np.complex128), omega=omega,
                 coords=(m.coords[:, 0].copy(), m.coords[:, 1].copy(), m.coords[:, 2].copy()))
+
+
+def _eddy_fields(m: KuhnMesh, sigma: float, nu_r_core: float):
+    c = m.centroids
+    core = _inside(c, 0.35, 0.65)
+    ring = (_inside(c, np.array([0.2, 0.2, 0.4]), np.array([0.8, 0.8, 0.6]))
+            & ~_inside(c, np.array([0.3, 0.3, 0.4]), np.array([0.7, 0.7, 0.6])))
+    return NU0 * np.where(core, nu_r_core, 1.0), np.where(ring, sigma, 0.0)
+
+
+def _csr32(X):
+    X = X.tocsr()
+    X.sort_indices()
+    X.indptr = X.indptr.astype(np.int32)
+    X.indices = X.indices.astype(np.int32)
+    return X
+
+
+def eddy_family(nc: int, freqs=None, nrhs: int = 4, seed: int = 1, sigma: float = 5.8e7,
+                nu_r_core: float = 1e-3, mass_eps: float = 1e-6):
+    """Frequency family of the eddy-current configuration for batched solves:
+    A_f = K + mass_eps nu M + j omega_f sigma M_cond = Kr + j omega_f Mc for
+    freqs (default 8 log-spaced from 1 kHz to 100 kHz), a_real_f = K +
+    |omega_f| sigma M_cond + mass_eps nu M per frequency, and nrhs source
+    patterns (random square current loops in air: height, extent and amplitude
+    drawn from numpy.random.default_rng(seed), snapped to interior grid lines)
+    shared by every frequency.
+    Returns Kr, Mc (real CSR), omegas, the per-frequency A and a_real, G,
+    freedofs, coordinates and B of shape (F, nrhs, ne) complex."""
+    freqs = np.logspace(3, 5, 8) if freqs is None else np.asarray(freqs, dtype=np.float64)
+    m = kuhn_mesh(nc)
+    Ke, Me = element_matrices(m)
+    nu, sig = _eddy_fields(m, sigma, nu_r_core)
+    K = assemble(m, nu, Ke)
+    Mc = assemble(m, sig, Me)
+    Mn = assemble(m, nu, Me)
+    Kr = _csr32(K + mass_eps * Mn)
+    omegas = 2.0 * np.pi * freqs
+    A = [_csr32(K.astype(np.complex128) + 1j * w * Mc.astype(np.complex128) + mass_eps * Mn) for w in omegas]
+    a_real = [_csr32(K + abs(w) * Mc + mass_eps * Mn) for w in omegas]
+    fd = boundary_freedofs(m)
+    rng = np.random.default_rng(seed)
+    src = []
+    for _ in range(nrhs):
+        z = rng.uniform(0.25, 0.75)
+        a0, b0 = rng.uniform(0.05, 0.15), rng.uniform(0.85, 0.95)
+        amp = rng.uniform(0.5, 2.0)
+        # snap to interior grid lines: a loop touching the boundary would be cut by the
+        # Dirichlet mask and lose its zero divergence
+        z = min(max(round(z * nc), 1), nc - 1) / nc
+        a0 = max(round(a0 * nc), 1) / nc
+        b0 = min(round(b0 * nc), nc - 1) / nc
+        src.append(loop_source(m, z_levels=(z,), squares=((a0, b0),), scale=amp) * fd)
+    B = np.broadcast_to(np.asarray(src, dtype=np.complex128), (len(omegas), nrhs, m.ne)).copy()
+    return dict(mesh=m, K=Kr, M=_csr32(Mc), omegas=omegas, freqs=freqs, A=A, a_real=a_real,
+                G=gradient_matrix(m), freedofs=fd, B=B,
+                coords=(m.coords[:, 0].copy(), m.coords[:, 1].copy(), m.coords[:, 2].copy()))

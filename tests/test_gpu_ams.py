@@ -8,12 +8,11 @@ applies to 1e-11, iteration counts within 2%, solutions to 1e-8 relative.
 The SI systems of the benchmarks (iron nu_r = 1e-3, mass weight 1e-6) have
 cond(A) ~ 1e8..1e11: a 1e-16 rounding difference between the device's
 reduction order and the sequential host sums grows to ~1e-8 of max|y| in an
-apply (measured), so applies are compared at 1e-7 there. COCR on the SI
-eddy-current system is sensitive in its iteration count (the oracle's own count
-moves from 77 to 90 when its preconditioner output carries 1e-8 relative
-noise) and its solution is only determined to ~cond * tol in the max norm, so
-that test bounds the count by a band and checks the true residual and the
-energy-norm difference."""
+apply (measured), so applies are compared at 1e-7 there; the Krylov solves
+must still match the oracle's iteration counts within 2% and reach the same
+true residual. COCR on the SI eddy-current system is what exposed a coarse
+solve done through an explicit pseudo-inverse (it stalls at a true residual
+of 1e-2): the coarsest levels are solved through the kept LDL^T factors."""
 from __future__ import annotations
 
 import numpy as np
@@ -158,8 +157,10 @@ def test_complex_ams_cocr_matches_oracle(eddy):
     xo, it, _ = o.cocr(eddy["A"], eddy["f"], freedofs=eddy["freedofs"], maxiter=500, tol=1e-8)
     fd = eddy["freedofs"].astype(bool)
     res = (eddy["f"] - eddy["A"] @ np.where(fd, x, 0))[fd]
-    assert np.linalg.norm(res) / np.linalg.norm(eddy["f"][fd]) <= 2e-7
-    assert 0.75 * it <= inv.iterations <= 1.3 * it
+    reso = (eddy["f"] - eddy["A"] @ np.where(fd, xo, 0))[fd]
+    nf = np.linalg.norm(eddy["f"][fd])
+    assert np.linalg.norm(res) / nf <= max(1e-8, 2 * np.linalg.norm(reso) / nf)
+    assert abs(inv.iterations - it) <= max(1, int(0.02 * it))
     Ar = eddy["a_real"]
     e = np.where(fd, x - xo, 0)
     x0 = np.where(fd, xo, 0)
