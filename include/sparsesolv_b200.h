@@ -289,6 +289,11 @@ int ssv_batch_cocr_solve(ssv_batch* b, int32_t maxiter, double tol, const void* 
                          int32_t* iterations, int32_t* converged, double* residuals);
 int ssv_batch_cocr_solve_dev(ssv_batch* b, int32_t maxiter, double tol, const void* d_rhs, void* d_sol,
                              int32_t* iterations, int32_t* converged, double* residuals);
+/* Residual replacement: every `every`-th step sets the preconditioned
+ * residual to M^{-1} r instead of its recurrence (0 = never, < 0 = automatic:
+ * every 10th step when a preconditioner is in the FP32 form, whose rounding
+ * makes it not exactly linear, so the recurrence drifts; never otherwise). */
+int ssv_batch_set_replacement(ssv_batch* b, int32_t every);
 /* Autotuner record: up to cap entries, *count = entries measured, *chosen =
  * index of the shape in use. */
 int ssv_batch_tuning(const ssv_batch* b, ssv_batch_tune_entry* entries, int32_t cap, int32_t* count,

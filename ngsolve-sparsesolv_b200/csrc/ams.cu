@@ -23,6 +23,7 @@
 // Kernels that cross between the two accumulate in FP64. The cycle's input
 // and output are FP64 in both forms.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <type_traits>
 
@@ -604,7 +605,8 @@ static std::vector<double> reciprocal(const std::vector<double>& v) {
     return r;
 }
 
-// Geometry part (G, G^T, Pi): FP64 in both forms.
+// Geometry part (G, G^T, Pi): FP64 in both forms. (The FP32 form replaces
+// the values by scaled ones in ams_upload_matrix.)
 static void ams_upload_geometry(AmsState& a, cudaStream_t s) {
     a.G.upload(a.host.G, false, s);
     a.Gt.upload(a.host.Gt, false, s);
@@ -614,8 +616,48 @@ static void ams_upload_geometry(AmsState& a, cudaStream_t s) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP32 form: every subspace hierarchy is stored diagonally scaled,
+// A^_l = S_l^{-1} A_l S_l^{-1} with s_i = sqrt|a_ii| (1 for a zero diagonal),
+// P^_l = S_l P_l S_{l+1}^{-1}, P^_l^T its transpose, l1^ = l1 / s^2, the
+// coarsest factors L^{-1} -> S^{-1} L^{-1} S and D -> S^{-1} D S^{-1} (the
+// same pivots dropped), and the level-0 scaling folded into the transfers
+// (G^T and Pi^T rows times 1/s, G and Pi columns times 1/s). In exact
+// arithmetic this is the same cycle; in FP32 every row is stored and
+// rounded relative to its own scale, which the eddy-current hierarchies
+// (conductor |omega| sigma M next to the 1e-6 mass weight of air: diagonals
+// 13 decades apart) need.
+// ---------------------------------------------------------------------------
+static std::vector<double> diag_scale(const HostCsr& A) {
+    std::vector<double> sc(A.n, 1.0);
+    for (int i = 0; i < A.n; ++i)
+        for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+            if (A.ci[k] == i && A.v[k] != 0.0) sc[i] = std::sqrt(std::fabs(A.v[k]));
+    return sc;
+}
+
+// v_k *= rmul[row] * cmul[col] (either may be null = 1)
+static HostCsr scaled_csr(const HostCsr& A, const std::vector<double>* rmul, const std::vector<double>* cmul) {
+    HostCsr B = A;
+    for (int i = 0; i < A.n; ++i)
+        for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+            double f = 1.0;
+            if (rmul) f *= (*rmul)[i];
+            if (cmul) f *= (*cmul)[A.ci[k]];
+            B.v[k] = A.v[k] * f;
+        }
+    return B;
+}
+
+static std::vector<double> inverted(const std::vector<double>& v) {
+    std::vector<double> r(v.size());
+    for (size_t i = 0; i < v.size(); ++i) r[i] = 1.0 / v[i];
+    return r;
+}
+
 // Matrix part: A_bc and its l1 norms (FP64), the four AMG hierarchies (in the
-// chosen form; the coarsest factors FP64).
+// chosen form; the coarsest factors FP64), and in the FP32 form the scaled
+// transfer values.
 static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
     const int nv = std::max(a.nv_alloc, a.complex_form ? 2 : 1);
     a.A_bc.upload(a.host.A_bc, false, s);
@@ -626,21 +668,63 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
         const auto& hl = a.host.amg[sub].levels;
         a.amg[sub].clear();
         a.amg[sub].resize(hl.size());
+        std::vector<std::vector<double>> sc(hl.size()), isc(hl.size());
+        for (size_t l = 0; l < hl.size(); ++l) {
+            sc[l] = a.fp32 ? diag_scale(hl[l].A) : std::vector<double>(hl[l].A.n, 1.0);
+            isc[l] = inverted(sc[l]);
+        }
         for (size_t l = 0; l < hl.size(); ++l) {
             AmgDevLevel& dl = a.amg[sub][l];
-            dl.A.upload(hl[l].A, a.fp32, s);
-            dl.l1.set(hl[l].l1, a.fp32, s);
-            dl.il1.set(reciprocal(hl[l].l1), a.fp32, s);
-            if (l + 1 < hl.size()) {
-                dl.P.upload(hl[l].P, a.fp32, s);
-                dl.Pt.upload(hl[l].Pt, a.fp32, s);
+            const int nl = hl[l].A.n;
+            if (a.fp32) {
+                dl.A.upload(scaled_csr(hl[l].A, &isc[l], &isc[l]), true, s);
+                std::vector<double> l1s(nl);
+                for (int i = 0; i < nl; ++i) l1s[i] = hl[l].l1[i] * isc[l][i] * isc[l][i];
+                dl.l1.set(l1s, true, s);
+                dl.il1.set(reciprocal(l1s), true, s);
+                if (l + 1 < hl.size()) {
+                    dl.P.upload(scaled_csr(hl[l].P, &sc[l], &isc[l + 1]), true, s);
+                    dl.Pt.upload(scaled_csr(hl[l].Pt, &isc[l + 1], &sc[l]), true, s);
+                }
+            } else {
+                dl.A.upload(hl[l].A, false, s);
+                dl.l1.set(hl[l].l1, false, s);
+                dl.il1.set(reciprocal(hl[l].l1), false, s);
+                if (l + 1 < hl.size()) {
+                    dl.P.upload(hl[l].P, false, s);
+                    dl.Pt.upload(hl[l].Pt, false, s);
+                }
             }
             dl.direct = hl[l].direct;
             if (dl.direct) {  // FP64 in both forms
-                dl.Li.upload(hl[l].linv.data(), hl[l].linv.size(), s);
-                dl.LiT.upload(hl[l].linvt.data(), hl[l].linvt.size(), s);
-                dl.piv.upload(hl[l].piv.data(), hl[l].piv.size(), s);
+                if (a.fp32) {
+                    std::vector<double> li = hl[l].linv, lt = hl[l].linvt, pv = hl[l].piv;
+                    for (int i = 0; i < nl; ++i)
+                        for (int k = 0; k < nl; ++k) {
+                            li[(size_t)i * nl + k] *= isc[l][i] * sc[l][k];
+                            lt[(size_t)i * nl + k] *= sc[l][i] * isc[l][k];
+                        }
+                    for (int i = 0; i < nl; ++i) pv[i] *= isc[l][i] * isc[l][i];
+                    dl.Li.upload(li.data(), li.size(), s);
+                    dl.LiT.upload(lt.data(), lt.size(), s);
+                    dl.piv.upload(pv.data(), pv.size(), s);
+                } else {
+                    dl.Li.upload(hl[l].linv.data(), hl[l].linv.size(), s);
+                    dl.LiT.upload(hl[l].linvt.data(), hl[l].linvt.size(), s);
+                    dl.piv.upload(hl[l].piv.data(), hl[l].piv.size(), s);
+                }
             }
+        }
+        // level-0 scaling folded into this subspace's transfers
+        if (sub == 0) {
+            a.G.upload(a.fp32 ? scaled_csr(a.host.G, nullptr, &isc[0]) : a.host.G, false, s);
+            a.Gt.upload(a.fp32 ? scaled_csr(a.host.Gt, &isc[0], nullptr) : a.host.Gt, false, s);
+        } else {
+            const int d = sub - 1;
+            const HostCsr pi = a.fp32 ? scaled_csr(a.host.Pi[d], nullptr, &isc[0]) : a.host.Pi[d];
+            const HostCsr pit = a.fp32 ? scaled_csr(a.host.Pit[d], &isc[0], nullptr) : a.host.Pit[d];
+            a.Piv[d].upload(pi.v.data(), pi.v.size(), s);
+            a.Pitv[d].upload(pit.v.data(), pit.v.size(), s);
         }
     }
     a.nv_alloc = 0;

@@ -222,8 +222,9 @@ k_bt_dot(int n, const zdouble* __restrict__ a, const zdouble* __restrict__ b, BS
         for (int q = threadIdx.x; q < R; q += blockDim.x) bt_finish(bs, cols, f * R + q, tot[q], op);
 }
 
-// sol += alpha p ; r -= alpha q ; rt -= alpha qt ; ||r||^2 per live column
-template <int R>
+// sol += alpha p ; r -= alpha q ; rt -= alpha qt (unless the step replaces
+// rt by M^{-1} r afterwards) ; ||r||^2 per live column
+template <int R, bool UPD_RT>
 __global__ void __launch_bounds__(kBlock)
 k_bt_update(int n, zdouble* __restrict__ x, const zdouble* __restrict__ p, const zdouble* __restrict__ q,
             const zdouble* __restrict__ qt, zdouble* __restrict__ r, zdouble* __restrict__ rt, BState* bs,
@@ -254,7 +255,7 @@ k_bt_update(int n, zdouble* __restrict__ x, const zdouble* __restrict__ p, const
             x[idx] = ST<zdouble>::fma(al, p[idx], x[idx]);
             const zdouble ri = r[idx] - al * q[idx];
             r[idx] = ri;
-            rt[idx] = rt[idx] - al * qt[idx];
+            if constexpr (UPD_RT) rt[idx] = rt[idx] - al * qt[idx];
             part[c].x += ST<zdouble>::norm2(ri);
         }
     }
@@ -360,6 +361,11 @@ struct ssv_batch {
     int gx_cap = 0, gx_elem = 0;
     // SpMM launch shape chosen by the autotuner
     int fb = 1, lanes = 8, gx = 1, chosen = -1;
+    // residual replacement: every `replace_every`-th step sets rt = M^{-1} r
+    // instead of the recurrence (0 = never; -1 = automatic: 10 when a
+    // preconditioner is in the FP32 form, whose rounding makes M^{-1} not
+    // exactly linear so the recurrence drifts from M^{-1} r)
+    int replace_every = -1;
     std::vector<ssv_batch_tune_entry> table;
     ssv::GraphLoop loop;
     // last solve
@@ -431,17 +437,23 @@ static void bt_dot(const ssv_batch& B, const zdouble* a, const zdouble* b, int o
     SSV_LAUNCH_CHECK();
 }
 
-static void bt_update(ssv_batch& B, cudaStream_t s) {
+template <bool UPD_RT>
+static void bt_update_t(ssv_batch& B, cudaStream_t s) {
     dim3 grid(B.gx_elem, B.F);
     if (B.R == 1)
-        k_bt_update<1><<<grid, kBlock, 0, s>>>(B.n, B.x.get(), B.p.get(), B.q.get(), B.qt.get(), B.r.get(),
-                                               B.rt.get(), B.bs.get(), B.cols.get(), B.partials.get(),
-                                               B.tickets.get(), B.gx_cap);
+        k_bt_update<1, UPD_RT><<<grid, kBlock, 0, s>>>(B.n, B.x.get(), B.p.get(), B.q.get(), B.qt.get(),
+                                                       B.r.get(), B.rt.get(), B.bs.get(), B.cols.get(),
+                                                       B.partials.get(), B.tickets.get(), B.gx_cap);
     else
-        k_bt_update<4><<<grid, kBlock, 0, s>>>(B.n, B.x.get(), B.p.get(), B.q.get(), B.qt.get(), B.r.get(),
-                                               B.rt.get(), B.bs.get(), B.cols.get(), B.partials.get(),
-                                               B.tickets.get(), B.gx_cap);
+        k_bt_update<4, UPD_RT><<<grid, kBlock, 0, s>>>(B.n, B.x.get(), B.p.get(), B.q.get(), B.qt.get(),
+                                                       B.r.get(), B.rt.get(), B.bs.get(), B.cols.get(),
+                                                       B.partials.get(), B.tickets.get(), B.gx_cap);
     SSV_LAUNCH_CHECK();
+}
+
+static void bt_update(ssv_batch& B, bool upd_rt, cudaStream_t s) {
+    if (upd_rt) bt_update_t<true>(B, s);
+    else bt_update_t<false>(B, s);
 }
 
 static void bt_pq(ssv_batch& B, cudaStream_t s) {
@@ -624,9 +636,16 @@ ssv_batch* batch_create(ssv_matrix* K, ssv_matrix* M, int F, const double* omega
 
 void batch_destroy(ssv_batch* B) { delete B; }
 
+static int replace_period(const ssv_batch& B) {
+    if (B.replace_every >= 0) return B.replace_every;
+    for (const ssv_precond* p : B.pre)
+        if (p && ams_precision(p->ams.get()) == SSV_PREC_FP32) return 10;
+    return 0;
+}
+
 static std::string batch_key(const ssv_batch& B) {
     std::string k = "batch;" + std::to_string((size_t)&B) + ";" + std::to_string(B.fb) + ";" +
-                    std::to_string(B.lanes) + ";" + std::to_string(B.gx);
+                    std::to_string(B.lanes) + ";" + std::to_string(B.gx) + ";" + std::to_string(replace_period(B));
     for (const ssv_precond* p : B.pre)
         k += ";" + (p ? std::to_string((size_t)p) + ":" + std::to_string(precond_generation(p)) : std::string("-"));
     return k;
@@ -640,14 +659,20 @@ void batch_cocr_solve_dev(ssv_batch* Bp, int maxiter, double tol, const void* d_
     cudaStream_t s = stream();
     KState* kst = &B.bs.get()->ks;
     // the iteration graph first (capture only), so the events below time device work alone
+    const int period = replace_period(B);
     build_graph_loop(B.loop, batch_key(B), [&](cudaGraphConditionalHandle hc, int use_cond) {
-        bt_precond(B, B.q.get(), B.qt.get(), kst, s);
-        bt_dot(B, B.qt.get(), B.q.get(), BT_MU, false, s);
-        bt_update(B, s);
-        spmm(B, B.rt.get(), B.t.get(), BT_RHO, s);
-        bt_pq(B, s);
-        k_bt_loop_ctl<<<1, 32, 0, s>>>(B.bs.get(), B.cols.get(), hc, use_cond);
-        SSV_LAUNCH_CHECK();
+        const int steps = std::max(period, 1);  // the body holds one replacement period
+        for (int u = 0; u < steps; ++u) {
+            const bool replace = period > 0 && u == steps - 1;
+            bt_precond(B, B.q.get(), B.qt.get(), kst, s);
+            bt_dot(B, B.qt.get(), B.q.get(), BT_MU, false, s);
+            bt_update(B, !replace, s);
+            if (replace) bt_precond(B, B.r.get(), B.rt.get(), kst, s);
+            spmm(B, B.rt.get(), B.t.get(), BT_RHO, s);
+            bt_pq(B, s);
+            k_bt_loop_ctl<<<1, 32, 0, s>>>(B.bs.get(), B.cols.get(), hc, use_cond);
+            SSV_LAUNCH_CHECK();
+        }
     });
     cudaEvent_t e0, e1, e2;
     SSV_CUDA(cudaEventCreate(&e0));
@@ -708,7 +733,7 @@ void batch_cocr_solve_dev(ssv_batch* Bp, int maxiter, double tol, const void* d_
     B.last_ms = ms_all;
     B.last_loop_ms = ms_loop;
     B.last_loops = h.ks.loops;
-    B.last_launches = nk + 2 + (int64_t)B.loop.body_nodes * h.ks.loops;
+    B.last_launches = nk + 2 + (int64_t)B.loop.body_nodes * h.ks.loops / std::max(period, 1);
 }
 
 void batch_cocr_solve_host(ssv_batch* B, int maxiter, double tol, const void* b, void* x, int* iters, int* conv,
@@ -728,6 +753,8 @@ int batch_tuning(const ssv_batch* B, ssv_batch_tune_entry* e, int cap, int* chos
     for (size_t i = 0; i < B->table.size() && (int)i < cap; ++i) e[i] = B->table[i];
     return (int)B->table.size();
 }
+
+void batch_set_replacement(ssv_batch* B, int every) { B->replace_every = every < 0 ? -1 : every; }
 
 void batch_last_timing(const ssv_batch* B, double* ms, double* loop_ms, int* loops, int64_t* launches) {
     if (ms) *ms = B->last_ms;

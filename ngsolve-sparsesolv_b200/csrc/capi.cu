@@ -397,6 +397,13 @@ int ssv_batch_tuning(const ssv_batch* b, ssv_batch_tune_entry* entries, int32_t 
     });
 }
 
+int ssv_batch_set_replacement(ssv_batch* b, int32_t every) {
+    return guarded([&] {
+        if (!b) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_batch_set_replacement: NULL batch");
+        ssv::batch_set_replacement(b, every);
+    });
+}
+
 int ssv_batch_last_timing(const ssv_batch* b, double* device_ms, double* loop_ms, int32_t* loops,
                           int64_t* kernel_launches) {
     return guarded([&] {

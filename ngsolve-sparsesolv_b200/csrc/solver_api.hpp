@@ -57,6 +57,7 @@ void batch_cocr_solve_host(ssv_batch* B, int maxiter, double tol, const void* b,
                            double* res);
 int batch_tuning(const ssv_batch* B, ssv_batch_tune_entry* e, int cap, int* chosen);
 void batch_last_timing(const ssv_batch* B, double* ms, double* loop_ms, int* loops, int64_t* launches);
+void batch_set_replacement(ssv_batch* B, int every);
 
 // CG with an external preconditioner and an initial guess (cocr_ngs.cu)
 void pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, const ssv_config& cfg, const void* d_b,

@@ -693,10 +693,13 @@ class BatchedCOCRSolver:
     FP32 form. ``Solve(B)`` takes B of shape (F, nrhs, n) complex and returns X
     of the same shape; ``iterations``, ``converged`` and ``residuals`` are then
     (F, nrhs) arrays with the COCRSolver meaning per column. The SpMM launch
-    shape is autotuned at construction (``tuning``).
+    shape is autotuned at construction (``tuning``). ``residual_replacement``:
+    every k-th step recomputes the preconditioned residual (None = automatic,
+    k = 10 with FP32 preconditioners; 0 = never).
     """
 
-    def __init__(self, K, M, omegas, pres, nrhs=1, freedofs=None, maxiter=500, tol=1e-8):
+    def __init__(self, K, M, omegas, pres, nrhs=1, freedofs=None, maxiter=500, tol=1e-8,
+                 residual_replacement=None):
         self._K = K if isinstance(K, _Matrix) else _Matrix(K)
         self._M = M if isinstance(M, _Matrix) else _Matrix(M)
         if self._K.cplx or self._M.cplx:
@@ -719,6 +722,8 @@ class BatchedCOCRSolver:
                                          ctypes.cast(harr, _capi.PP), self.nrhs, _capi.u8ptr(self._fd),
                                          ctypes.byref(h)))
         self._h = h
+        if residual_replacement is not None:
+            check(self._lib.ssv_batch_set_replacement(self._h, int(residual_replacement)))
         shape = (self.F, self.nrhs)
         self.iterations = np.zeros(shape, np.int32)
         self.converged = np.zeros(shape, np.int32)

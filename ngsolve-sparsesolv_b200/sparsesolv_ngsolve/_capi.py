@@ -193,6 +193,7 @@ SIGNATURES = [
     ("ssv_batch_cocr_solve", I32, [P, I32, ctypes.c_double, P, P, PI32, PI32, PD]),
     ("ssv_batch_cocr_solve_dev", I32, [P, I32, ctypes.c_double, P, P, PI32, PI32, PD]),
     ("ssv_batch_tuning", I32, [P, ctypes.POINTER(ssv_batch_tune_entry), I32, PI32, PI32]),
+    ("ssv_batch_set_replacement", I32, [P, I32]),
     ("ssv_batch_last_timing", I32, [P, PD, PD, PI32, ctypes.POINTER(ctypes.c_int64)]),
     ("ssv_ams_get_precision", I32, [P, PI32]),
     ("ssv_pcg_solve", I32, [P, P, PU8, ctypes.POINTER(ssv_config), P, P, ctypes.POINTER(ssv_result), PD, I32]),
