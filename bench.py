@@ -1,17 +1,25 @@
 """Benchmark of the B200 solve path (one JSON line on rank 0).
 
-Workload (default ``iccg64``): the plain FP64 ICCG drop-in on a 3-D 7-point
-Laplacian, 64^3 interior grid (262,144 unknowns, 1,810,432 nonzeros), RHS
-uniform[-1,1] from numpy seed 0, IC shift 1.05, ABMC (block 4, 4 target
-colours), tol 1e-10, maxiter 2000. One step = one complete
-SparseSolvSolver.Solve (FreeDofs view, ABMC ordering, device IC(0)
-factorisation, CG to tolerance) on a fresh solver object with the matrix and
-b resident in HBM; metric = time-to-solution (s), lower is better.
+Default workload ``ams40``: real magnetostatic curl-curl on a Kuhn 6-tet mesh
+of a 40^3 unit cube (462,520 HCurl edges, 7,432,120 nonzeros, 68,921
+vertices; nu = 1, iron block nu = 1e-3, 1e-6 nu M mass term, Dirichlet
+boundary, square loop source), Compact AMS preconditioner + CG to 1e-10. One
+step = one PCG solve to tolerance with the preconditioner built, the matrix,
+b and x resident in HBM; metric = time-to-solution (s), lower is better. The
+line's value is the FP32-preconditioner (mixed) form; the plain FP64 form is
+measured in the same run (config.plain_fp64), and the batched form on the
+40^3 complex eddy-current family (8 frequencies x 4 right-hand sides, one
+launch graph) is measured against 32 sequential FP64 solves
+(config.batched_family) unless --no-extras.
 
-``--impl reference`` times the reference's own CPU implementation (its headers
-compiled into oracle/_ref/libssv_ref.so, OpenMP over all host cores) on the
-same workload. Multi-GPU: independent replicas (one per rank, no collective
-on the data path), max over ranks.
+``--workload iccg64``: the plain FP64 ICCG drop-in on the 64^3 7-point
+Laplacian (a complete SparseSolvSolver.Solve per step, set-up included).
+
+``--impl reference`` times the reference's CPU implementation of the same
+workload on the host cores: for ICCG its own headers (oracle/_ref); for the
+AMS workloads the reference's AMS needs NGSolve, so the C++ restatement in
+oracle/ (OpenMP over all host cores) stands in. Multi-GPU: independent
+replicas (one per rank, no collective on the data path), max over ranks.
 """
 from __future__ import annotations
 
@@ -29,7 +37,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "ngsolve-sparsesolv_b200"))
 
-METRIC = "time-to-solution @1e-10 (s)"
+METRIC = "time-to-solution @1e-10 (s), ms/iter, SpMV HBM GB/s: mixed/batched vs plain FP64 GPU"
 UNIT = "s"
 
 
@@ -178,6 +186,15 @@ def run_ncu_case(args):
     import numpy as np
 
     import sparsesolv_ngsolve as ss
+    if args.workload == "ams40":
+        d = _ams_system()
+        pre = _ams_pre(ss, d, args.precision)
+        inv = ss.PCGSolver(d["A"], pre, freedofs=d["freedofs"], maxiter=500, tol=1e-10)
+        x = np.zeros(d["A"].shape[0])
+        r = inv.Solve(d["f"], x)
+        print(json.dumps({"ncu_case": args.workload, "precision": args.precision, "iterations": r.iterations,
+                          "converged": r.converged, "kernels": r.kernel_launches}))
+        return
     A, b, cfg, desc = _workload(args.workload)
     s = ss.SparseSolvSolver(A, method=cfg["method"], tol=cfg["tol"], maxiter=cfg["maxiter"], shift=cfg["shift"],
                             use_abmc=cfg["use_abmc"], abmc_block_size=cfg["abmc_block_size"],
@@ -188,13 +205,290 @@ def run_ncu_case(args):
                       "kernels": r.kernel_launches}))
 
 
+# ---------------------------------------------------------------------------
+# AMS workloads
+# ---------------------------------------------------------------------------
+AMS_DESC = {"workload": "ams40: real magnetostatic curl-curl, Kuhn 6-tet mesh of a 40^3 cube (462,520 edges, "
+                        "7,432,120 nnz, 68,921 vertices), nu=1 / iron 1e-3, 1e-6 nu M, Compact AMS (cycle 1) + CG, "
+                        "tol 1e-10",
+            "tol": 1e-10, "rhs": "square loop current at mid-height (discretely divergence-free)"}
+
+
+def _ams_system():
+    from sparsesolv_ngsolve import hcurl as H
+    return H.magnetostatic(40)
+
+
+def _ams_pre(ss, d, precision):
+    return ss.CompactAMSPreconditioner(d["A"], d["G"], freedofs=d["freedofs"], coord_x=d["coords"][0],
+                                       coord_y=d["coords"][1], coord_z=d["coords"][2], precision=precision)
+
+
+def cpu_baseline_ams(d, budget_s=20.0):
+    """The AMS restatement (oracle/, NGSolve being absent) + sparsesolv::CGSolver on all host cores."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    O.AmsOracle.set_threads(cores)
+    t0 = time.perf_counter()
+    o = O.AmsOracle(d["A"], d["G"], d["freedofs"], *d["coords"])
+    setup = time.perf_counter() - t0
+    cfg = O.default_config(tolerance=1e-10, max_iterations=500)
+    times, iters = [], 0
+    t_end = time.perf_counter() + budget_s
+    while True:
+        t0 = time.perf_counter()
+        _, r, _ = o.pcg(d["f"], config=cfg)
+        times.append(time.perf_counter() - t0)
+        iters = r.iterations
+        if time.perf_counter() > t_end or len(times) >= 10:
+            break
+    return {"value": statistics.mean(times), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{len(times)} full PCG solves of the workload ({iters} iterations each) with the AMS "
+                      f"restatement on {cores} OpenMP threads; mean wall time per solve, preconditioner built "
+                      f"(its set-up took {setup:.2f} s)"}
+
+
+def run_reference_ams(args, rank, world):
+    if rank != 0:
+        return
+    d = _ams_system()
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    O.AmsOracle.set_threads(cores)
+    o = O.AmsOracle(d["A"], d["G"], d["freedofs"], *d["coords"])
+    cfg = O.default_config(tolerance=1e-10, max_iterations=500)
+    for _ in range(args.warmup):
+        o.pcg(d["f"], config=cfg)
+    times, iters = [], 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, r, _ = o.pcg(d["f"], config=cfg)
+        times.append(time.perf_counter() - t0)
+        iters = r.iterations
+    v = statistics.mean(times)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(AMS_DESC, iterations=iters, ms_per_iter=v * 1e3 / max(iters, 1)),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} full PCG solves with the AMS restatement on {cores} OpenMP "
+                                       f"threads (the reference's AMS needs NGSolve, absent here)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def batched_family_extra(ss, nc=40):
+    """Batched COCR (8 frequencies x 4 right-hand sides, FP64 preconditioners) vs 32 sequential solves."""
+    import numpy as np
+    from sparsesolv_ngsolve import hcurl as H
+    d = H.eddy_family(nc, nrhs=4)
+    fd = d["freedofs"].astype(bool)
+    pres = [ss.ComplexCompactAMSPreconditioner(a, d["G"], freedofs=d["freedofs"], coord_x=d["coords"][0],
+                                               coord_y=d["coords"][1], coord_z=d["coords"][2])
+            for a in d["a_real"]]
+    bs = ss.BatchedCOCRSolver(d["K"], d["M"], d["omegas"], pres, nrhs=4, freedofs=d["freedofs"], maxiter=1000,
+                              tol=1e-10)
+    bs.Solve(d["B"])
+    walls = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        X = bs.Solve(d["B"])
+        walls.append(time.perf_counter() - t0)
+    tm = bs.last_timing
+    its_b = bs.iterations.copy()
+
+    def tres(f, x, b):
+        return float(np.linalg.norm((b - d["A"][f] @ np.where(fd, x, 0))[fd]) / np.linalg.norm(b[fd]))
+
+    tr_b = max(tres(f, X[f, r], d["B"][f, r]) for f in range(8) for r in range(4))
+    seq, its_s, tr_s = 0.0, [], 0.0
+    for f in range(8):
+        inv = ss.COCRSolver(d["A"][f], pres[f], freedofs=d["freedofs"], maxiter=1000, tol=1e-10)
+        inv * d["B"][f, 0]
+        for r in range(4):
+            t0 = time.perf_counter()
+            x = inv * d["B"][f, r]
+            seq += time.perf_counter() - t0
+            its_s.append(inv.iterations)
+            tr_s = max(tr_s, tres(f, x, d["B"][f, r]))
+    return {"family": f"complex eddy current on the {nc}^3 Kuhn mesh ({d['K'].shape[0]} edges), 8 frequencies "
+                      f"1 kHz..100 kHz x 4 loop sources (default_rng(1)), ComplexCompactAMS per frequency (FP64) "
+                      f"+ COCR, tol 1e-10",
+            "batched_s": min(walls), "batched_device_ms": tm["device_ms"], "batched_loops": tm["loops"],
+            "batched_kernel_launches": tm["kernel_launches"], "sequential_fp64_s": seq,
+            "speedup": seq / min(walls), "iterations_batched": its_b.ravel().tolist(), "iterations_sequential": its_s,
+            "max_true_residual_batched": tr_b, "max_true_residual_sequential": tr_s,
+            "autotuned_spmm": bs.tuning["chosen"],
+            "fp32_preconditioner": "not used: COCR with an FP32-rounded preconditioner stops at a true residual of "
+                                   "~1e-7 on these systems (the FP64 oracle with only its output rounded to FP32 "
+                                   "does the same), above the 1e-10 target"}
+
+
+def run_ams(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    import sparsesolv_ngsolve as ss
+    from sparsesolv_ngsolve import _capi
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda:0")
+    lib = _capi.load()
+    d = _ams_system()
+    A = d["A"]
+    n = A.shape[0]
+    mat = ss._Matrix(A)
+    d_fd = torch.from_numpy(np.ascontiguousarray(d["freedofs"].astype(np.uint8))).to(dev)
+    d_b = torch.from_numpy(np.ascontiguousarray(d["f"])).to(dev)
+    d_x = torch.zeros(n, dtype=torch.float64, device=dev)
+    cfg = _capi.default_config(tolerance=1e-10, max_iterations=500)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+    t0 = time.perf_counter()
+    pre = _ams_pre(ss, d, "fp64")
+    setup_s = time.perf_counter() - t0
+
+    def solve_dev():
+        d_x.zero_()
+        res = _capi.ssv_result()
+        _capi.check(lib.ssv_pcg_solve_dev(mat.h, pre._h, ctypes.cast(d_fd.data_ptr(), _capi.PU8), ctypes.byref(cfg),
+                                          ctypes.c_void_p(d_b.data_ptr()), ctypes.c_void_p(d_x.data_ptr()),
+                                          ctypes.byref(res), None, 0))
+        return res
+
+    def timed_steps(k):
+        ms, launches, iters, conv = [], 0, 0, True
+        for _ in range(k):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r = solve_dev()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            launches += r.kernel_launches
+            iters = r.iterations
+            conv = conv and bool(r.converged)
+        return ms, launches, iters, conv
+
+    def true_res():
+        x = d_x.cpu().numpy()
+        fd = d["freedofs"].astype(bool)
+        return float(np.linalg.norm((d["f"] - A @ np.where(fd, x, 0))[fd]) / np.linalg.norm(d["f"]))
+
+    forms = {}
+    for prec in ("fp64", "fp32"):
+        pre.precision = prec
+        for _ in range(args.warmup):
+            solve_dev()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        clocks = ClockSampler(local)
+        clocks.start()
+        ms, launches, iters, conv = timed_steps(args.steps)
+        clock_info = clocks.stop()
+        total_ms = sum(ms)
+        if dist:
+            t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        prof = pre.profile(nrhs=1, reps=20)
+        forms[prec] = {"ms_per_step": total_ms / args.steps, "launches": launches, "iterations": iters,
+                       "converged": conv, "clocks": clock_info, "phases": prof, "true_rel_residual": true_res(),
+                       "x": d_x.cpu().numpy()}
+    peak, peak_kind = _peaks()
+    mixed, plain = forms["fp32"], forms["fp64"]
+
+    def gbps(p):
+        return p["bytes"] / (p["ms"] * 1e-3) / 1e9
+
+    def phase(form, name):
+        return next(p for p in form["phases"] if p["name"] == name)
+
+    spmv = phase(mixed, "fine_residual")
+    achieved = gbps(spmv)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": "k_mv_spmv fine residual (A_bc, 7.43M nnz, FP64)", "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": spmv["bytes"], "launch_ms": spmv["ms"],
+                "phases_mixed": [{**p, "GBps": gbps(p)} for p in mixed["phases"]],
+                "phases_plain_fp64": [{**p, "GBps": gbps(p)} for p in plain["phases"]]}
+    fdm = d["freedofs"].astype(bool)
+    xm, xp = mixed["x"], plain["x"]
+    e = np.where(fdm, xm - xp, 0)
+    xp0 = np.where(fdm, xp, 0)
+    err_energy = float(np.sqrt(abs(e @ (A @ e))) / np.sqrt(abs(xp0 @ (A @ xp0))))
+
+    # end to end through the public API with host buffers (mixed form)
+    solver = ss.PCGSolver(A, pre, freedofs=d["freedofs"], maxiter=500, tol=1e-10)
+    xh = np.zeros(n)
+    for _ in range(2):
+        xh[:] = 0
+        solver.Solve(d["f"], xh)
+    e2e_ms = []
+    for _ in range(max(3, args.steps // 2)):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        xh[:] = 0
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        solver.Solve(d["f"], xh)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    value = mixed["ms_per_step"] / 1e3
+    config = dict(AMS_DESC, parallelism=f"replicas{world}", l2="flushed between timed steps (256 MB write)",
+                  form="mixed: FP32 subspace AMG hierarchies (diagonally scaled) and V-cycles; FP64 fine level, "
+                       "transfers, coarsest LDL^T solves and CG",
+                  iterations=mixed["iterations"], converged=mixed["converged"],
+                  ms_per_iter=mixed["ms_per_step"] / max(mixed["iterations"], 1),
+                  spmv_GBps=achieved, true_rel_residual=mixed["true_rel_residual"],
+                  error_vs_fp64_energy_norm=err_energy,
+                  plain_fp64={"time_to_solution_s": plain["ms_per_step"] / 1e3, "iterations": plain["iterations"],
+                              "ms_per_iter": plain["ms_per_step"] / max(plain["iterations"], 1),
+                              "spmv_GBps": gbps(phase(plain, "fine_residual")),
+                              "true_rel_residual": plain["true_rel_residual"]},
+                  speedup_mixed_vs_plain=plain["ms_per_step"] / mixed["ms_per_step"],
+                  ams_setup_s=setup_s)
+    if not args.no_extras and rank == 0:
+        try:
+            config["batched_family"] = batched_family_extra(ss)
+        except Exception as exc:  # reported, not hidden
+            config["batched_family"] = {"error": repr(exc)}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"], "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 Krylov + f32 preconditioner hierarchy",
+            "data": "synthetic", "config": config,
+            "e2e": {"value": statistics.mean(e2e_ms) / 1e3, "unit": UNIT, "h2d_bytes_per_step": int(2 * n * 8),
+                    "d2h_bytes_per_step": int(n * 8 + 64)},
+            "roofline": roofline, "gpu_launches": int(mixed["launches"]), "clocks": mixed["clocks"]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_ams(d)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del solver
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="iccg64")
+    ap.add_argument("--workload", default="ams40", choices=["ams40", "iccg64"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched-family measurement")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"], help="AMS form of --ncu-case")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ncu-case", action="store_true",
                     help="run exactly one solve of the workload and exit (for ncu captures)")
@@ -210,9 +504,13 @@ def main():
         os.environ["CUDA_VISIBLE_DEVICES"] = ids[local]
 
     if args.impl == "reference":
+        if args.workload == "ams40":
+            return run_reference_ams(args, rank, world)
         return run_reference(args, rank, world)
     if args.ncu_case:
         return run_ncu_case(args)
+    if args.workload == "ams40":
+        return run_ams(args, rank, world, local)
 
     import numpy as np
     import torch

@@ -3,7 +3,9 @@
  *
  * Every entry point takes plain pointers and sizes. Host pointers carry host
  * data; the `_dev` variants take device pointers that the caller keeps
- * resident in HBM. All calls are synchronous on return (the work runs on the
+ * resident in HBM -- every array argument of a `_dev` call, freedofs masks
+ * included, is device memory (a host pointer is refused with
+ * SSV_ERR_INVALID_ARG). All calls are synchronous on return (the work runs on the
  * handle's own CUDA stream). A handle is not safe for concurrent use from two
  * threads (the reference's objects keep mutable work buffers the same way,
  * include/sparsesolv/preconditioners/ic_preconditioner.hpp:555-563).
@@ -235,6 +237,12 @@ int ssv_ams_levels(const ssv_precond* p, int32_t subspace, int32_t* sizes, int32
  * Update() keeps the current form. */
 int ssv_ams_set_precision(ssv_precond* p, int32_t precision);
 int ssv_ams_get_precision(const ssv_precond* p, int32_t* precision);
+/* Measurement hook (no reference counterpart): per-phase device time of one
+ * AMS cycle on nrhs (1 or 4) right-hand sides -- the whole cycle, one fine
+ * residual pass, one fine smoothing pass, the gradient V-cycle, the three
+ * nodal V-cycles, the G and Pi transfers -- each re-launched reps times
+ * between CUDA events, with the algorithmic bytes of one execution. */
+int ssv_ams_profile(ssv_precond* p, int32_t nrhs, int32_t reps, ssv_phase_profile* out);
 
 /* ---- CG with an external preconditioner (new: the reference's AMS scripts
  *      drive it with NGSolve's krylovspace.CGSolver) ---------------------------

@@ -24,6 +24,7 @@
 // and output are FP64 in both forms.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <type_traits>
 
@@ -343,7 +344,12 @@ template <> inline const float* DualVec::get<float>() const { return f.get(); }
 struct DevCsr {
     int n = 0, m = 0;
     int64_t nnz = 0;
-    int lanes = 8;
+    int lanes = 8;               // from the mean row length until tuned
+    int tuned[4] = {0, 0, 0, 0}; // lanes chosen by timing for NV = 1, 2, 4, 8 (0 = not tuned)
+    int lanes_for(int nv) const {
+        const int i = nv == 1 ? 0 : nv == 2 ? 1 : nv == 4 ? 2 : 3;
+        return tuned[i] ? tuned[i] : lanes;
+    }
     DevBuf<int> rp, ci;
     DualVec v;
     void upload(const HostCsr& A, bool fp32, cudaStream_t s) {
@@ -390,6 +396,7 @@ struct AmsState {
     bool has_fd = false;
     std::vector<uint8_t> h_fd;
     unsigned gen = 0;
+    ForkSet forks;  // the y and z nodal V-cycles run beside the x one
 };
 
 void ams_free(AmsState* a) { delete a; }
@@ -397,7 +404,7 @@ void ams_free(AmsState* a) { delete a; }
 template <typename TV, typename TX, typename TY, int NV, int MODE, bool RECIP>
 static void mv_spmv(const DevCsr& A, const TX* x, TY* y, const TY* b, const TY* d, TY w, const KState* st,
                     cudaStream_t s) {
-    const int lanes = A.lanes;
+    const int lanes = A.lanes_for(NV);
     const int rpb = kBlock / lanes;
     const int grid = std::max(1, std::min((A.n + rpb - 1) / rpb, sm_count() * 8));
     const TV* v = A.val<TV>();
@@ -486,7 +493,7 @@ static void pi_prolong_l(const AmsState& a, const T* gx, const T* gy, const T* g
 template <typename T, int NV>
 static void pi_restrict(const AmsState& a, const double* r, T* ox, T* oy, T* oz, const KState* st,
                         cudaStream_t s) {
-    switch (a.Gt.lanes) {
+    switch (a.Gt.lanes_for(NV)) {
         case 2: pi_restrict_l<T, NV, 2>(a, r, ox, oy, oz, st, s); break;
         case 4: pi_restrict_l<T, NV, 4>(a, r, ox, oy, oz, st, s); break;
         case 8: pi_restrict_l<T, NV, 8>(a, r, ox, oy, oz, st, s); break;
@@ -498,7 +505,7 @@ static void pi_restrict(const AmsState& a, const double* r, T* ox, T* oy, T* oz,
 template <typename T, int NV>
 static void pi_prolong(const AmsState& a, const T* gx, const T* gy, const T* gz, double* x, const KState* st,
                        cudaStream_t s) {
-    switch (a.G.lanes) {
+    switch (a.G.lanes_for(NV)) {
         case 2: pi_prolong_l<T, NV, 2>(a, gx, gy, gz, x, st, s); break;
         case 4: pi_prolong_l<T, NV, 4>(a, gx, gy, gz, x, st, s); break;
         case 8: pi_prolong_l<T, NV, 8>(a, gx, gy, gz, x, st, s); break;
@@ -550,9 +557,12 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
         ensure_x();
         mv_spmv<double, double, double, NV, MV_RES, RECIP>(a.A_bc, cur, r, b0, nullptr, 0.0, st, s);
         pi_restrict<T, NV>(a, r, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), st, s);
+        // the three V-cycles are independent (own hierarchies and vectors)
+        a.forks.fork(s, 2);
         T* gx = vcycle<T, NV, RECIP>(a.amg[1], 0, a.rs[1].as<T>(), 1, st, s);
-        T* gy = vcycle<T, NV, RECIP>(a.amg[2], 0, a.rs[2].as<T>(), 1, st, s);
-        T* gz = vcycle<T, NV, RECIP>(a.amg[3], 0, a.rs[3].as<T>(), 1, st, s);
+        T* gy = vcycle<T, NV, RECIP>(a.amg[2], 0, a.rs[2].as<T>(), 1, st, a.forks.side[0]);
+        T* gz = vcycle<T, NV, RECIP>(a.amg[3], 0, a.rs[3].as<T>(), 1, st, a.forks.side[1]);
+        a.forks.join(s, 2);
         pi_prolong<T, NV>(a, gx, gy, gz, cur, st, s);
     };
     if (a.cycle_type == 7) {
@@ -576,6 +586,87 @@ static HostCsr host_csr_of(const ssv_matrix* M) {
     return H;
 }
 
+// ---------------------------------------------------------------------------
+// Lanes autotuner: for every CSR of the cycle and every column count in use,
+// time y = A x for 2..32 lanes per row on the actual matrix (work vectors as
+// operands) and keep the fastest. Runs when work vectors are (re)allocated,
+// outside any capture.
+// ---------------------------------------------------------------------------
+template <typename TV, typename TX, typename TY, int NV>
+static void tune_csr(DevCsr& A, const TX* x, TY* y, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+    if (A.n == 0 || A.nnz == 0) return;
+    const TV* v = A.val<TV>();
+    float best = 1e30f;
+    int pick = A.lanes;
+    const int cand[5] = {2, 4, 8, 16, 32};
+    for (int L : cand) {
+        const int rpb = kBlock / L;
+        const int grid = std::max(1, std::min((A.n + rpb - 1) / rpb, sm_count() * 8));
+        auto launch = [&] {
+            switch (L) {
+                case 2: k_mv_spmv<TV, TX, TY, NV, 2, MV_AX, false><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, nullptr, nullptr, TY(0), nullptr); break;
+                case 4: k_mv_spmv<TV, TX, TY, NV, 4, MV_AX, false><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, nullptr, nullptr, TY(0), nullptr); break;
+                case 8: k_mv_spmv<TV, TX, TY, NV, 8, MV_AX, false><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, nullptr, nullptr, TY(0), nullptr); break;
+                case 16: k_mv_spmv<TV, TX, TY, NV, 16, MV_AX, false><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, nullptr, nullptr, TY(0), nullptr); break;
+                default: k_mv_spmv<TV, TX, TY, NV, 32, MV_AX, false><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, nullptr, nullptr, TY(0), nullptr); break;
+            }
+        };
+        launch();
+        SSV_CUDA(cudaEventRecord(e0, s));
+        const int reps = 4;
+        for (int k = 0; k < reps; ++k) launch();
+        SSV_CUDA(cudaEventRecord(e1, s));
+        SSV_CUDA(cudaEventSynchronize(e1));
+        SSV_LAUNCH_CHECK();
+        float ms = 0.f;
+        SSV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+            best = ms;
+            pick = L;
+        }
+    }
+    A.tuned[NV == 1 ? 0 : NV == 2 ? 1 : NV == 4 ? 2 : 3] = pick;
+}
+
+template <typename T, int NV>
+static void tune_all_nv(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+    tune_csr<double, double, double, NV>(a.A_bc, a.xa.get(), a.xb.get(), s, e0, e1);
+    tune_csr<double, double, T, NV>(a.Gt, a.r.get(), a.rs[0].as<T>(), s, e0, e1);
+    tune_csr<double, T, double, NV>(a.G, a.rs[0].as<T>(), a.xb.get(), s, e0, e1);
+    for (int sub = 0; sub < 4; ++sub) {
+        auto& L = a.amg[sub];
+        for (size_t l = 0; l < L.size(); ++l) {
+            tune_csr<T, T, T, NV>(L[l].A, L[l].xa.as<T>(), L[l].xb.as<T>(), s, e0, e1);
+            if (l + 1 < L.size()) {
+                tune_csr<T, T, T, NV>(L[l].P, L[l + 1].xa.as<T>(), L[l].r.as<T>(), s, e0, e1);
+                tune_csr<T, T, T, NV>(L[l].Pt, L[l].r.as<T>(), L[l + 1].b.as<T>(), s, e0, e1);
+            }
+        }
+    }
+}
+
+template <typename T>
+static void tune_lanes_t(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+    if (a.complex_form) {
+        tune_all_nv<T, 2>(a, s, e0, e1);
+        if (a.nv_alloc >= 8) tune_all_nv<T, 8>(a, s, e0, e1);
+    } else {
+        tune_all_nv<T, 1>(a, s, e0, e1);
+        if (a.nv_alloc >= 4) tune_all_nv<T, 4>(a, s, e0, e1);
+    }
+}
+
+static void tune_lanes(AmsState& a) {
+    cudaStream_t s = stream();
+    cudaEvent_t e0, e1;
+    SSV_CUDA(cudaEventCreate(&e0));
+    SSV_CUDA(cudaEventCreate(&e1));
+    if (a.fp32) tune_lanes_t<float>(a, s, e0, e1);
+    else tune_lanes_t<double>(a, s, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
 // Work vectors for blocks of up to nv real columns (allocation only, so the
 // cycle itself never allocates and can be captured).
 static void ams_reserve(AmsState& a, int nv) {
@@ -597,6 +688,7 @@ static void ams_reserve(AmsState& a, int nv) {
     for (int s = 0; s < 4; ++s) a.rs[s].alloc(m1);
     a.nv_alloc = nv;
     ++a.gen;  // new work buffers: graphs that captured the old ones must be rebuilt
+    tune_lanes(a);
 }
 
 static std::vector<double> reciprocal(const std::vector<double>& v) {
@@ -747,6 +839,7 @@ AmsState* ams_create(const ssv_matrix* A, const ssv_matrix* G, const uint8_t* fd
     auto* a = new AmsState();
     try {
         cudaStream_t s = stream();
+        a->forks.ensure(2);
         a->nhc = A->rows;
         a->nh1 = G->cols;
         a->cycle_type = cycle_type;
@@ -815,6 +908,121 @@ void ams_apply_block(AmsState* a, const double* in, double* out, int nrhs, const
     if (nrhs * (a->complex_form ? 2 : 1) > a->nv_alloc) fail(SSV_ERR_INVALID_ARG, "AMS block apply: reserve first");
     if (a->fp32) ams_block_t<float>(*a, in, out, nrhs, st, s);
     else ams_block_t<double>(*a, in, out, nrhs, st, s);
+}
+
+// ---------------------------------------------------------------------------
+// Per-phase profile of one cycle (measurement hook, no reference counterpart):
+// every phase is re-launched `reps` times between CUDA events on the
+// library's stream; bytes are the algorithmic bytes of one execution (CSR
+// with int32 indices, values of the stored type, every vector entry read or
+// written once, gathered x counted once).
+// ---------------------------------------------------------------------------
+static double csr_pass_bytes(const DevCsr& A, int vb) { return (double)A.nnz * (4 + vb) + 4.0 * (A.n + 1); }
+
+// one V-cycle from level l: matrix passes and vector streams
+static double vcycle_bytes(const std::vector<AmgDevLevel>& L, int l, int NV, int tb) {
+    const AmgDevLevel& lv = L[l];
+    const double n = lv.A.n, v = (double)NV * tb;
+    if (l == (int)L.size() - 1) {
+        if (lv.direct) return 8.0 * n * n + n * 8.0 + n * (2 * v + 2 * 8.0 * NV);
+        return n * (2 * v + tb) + 9 * (csr_pass_bytes(lv.A, tb) + n * (3 * v + tb));
+    }
+    const double nc = L[l + 1].A.n;
+    double b = n * (2 * v + tb);                            // first sweep x = b / l1
+    b += csr_pass_bytes(lv.A, tb) + 3 * n * v;              // residual
+    b += csr_pass_bytes(lv.Pt, tb) + (n + nc) * v;          // restriction
+    b += vcycle_bytes(L, l + 1, NV, tb);
+    b += csr_pass_bytes(lv.P, tb) + (nc + 2 * n) * v;       // prolongation add
+    b += csr_pass_bytes(lv.A, tb) + n * (3 * v + tb);       // post sweep
+    return b;
+}
+
+template <typename T, int NV, bool RECIP>
+static void ams_profile_t(AmsState& a, int reps, ssv_phase_profile* out) {
+    cudaStream_t s = stream();
+    const int n = a.nhc, n1 = a.nh1;
+    const int tb = (int)sizeof(T);
+    DevBuf<double> pin((size_t)n * NV), pout((size_t)n * NV);
+    pin.zero(s);
+    double* cur = a.xa.get();
+    double* alt = a.xb.get();
+    double* r = a.r.get();
+    const double* d = RECIP ? a.fine_il1.get() : a.fine_l1.get();
+    cudaEvent_t e0, e1;
+    SSV_CUDA(cudaEventCreate(&e0));
+    SSV_CUDA(cudaEventCreate(&e1));
+    std::memset(out, 0, sizeof(*out));
+    auto timed = [&](const char* name, double bytes, int kernels, auto&& launch) {
+        for (int k = 0; k < 2; ++k) launch();
+        SSV_CUDA(cudaEventRecord(e0, s));
+        for (int k = 0; k < reps; ++k) launch();
+        SSV_CUDA(cudaEventRecord(e1, s));
+        SSV_CUDA(cudaEventSynchronize(e1));
+        SSV_LAUNCH_CHECK();
+        float ms = 0.f;
+        SSV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        const int i = out->num_phases++;
+        std::snprintf(out->names[i], sizeof(out->names[i]), "%s", name);
+        out->ms[i] = (double)ms / reps;
+        out->bytes[i] = bytes;
+        out->kernels[i] = kernels;
+    };
+    const double N = n, N1 = n1, V = 8.0 * NV, Vt = (double)tb * NV;
+    const double fine_res = csr_pass_bytes(a.A_bc, 8) + 3 * N * V;
+    const double fine_jac = csr_pass_bytes(a.A_bc, 8) + N * (3 * V + 8);
+    const double grad_vc = vcycle_bytes(a.amg[0], 0, NV, tb);
+    double nod_vc = 0;
+    for (int k = 1; k < 4; ++k) nod_vc += vcycle_bytes(a.amg[k], 0, NV, tb);
+    const double g_tr = csr_pass_bytes(a.Gt, 8) + N * V + N1 * Vt + csr_pass_bytes(a.G, 8) + N1 * Vt + 2 * N * V;
+    const double pi_tr = (double)a.Gt.nnz * (4 + 24) + 4.0 * (n1 + 1) + N * V + 3 * N1 * Vt +
+                         (double)a.G.nnz * (4 + 24) + 4.0 * (n + 1) + 3 * N1 * Vt + 2 * N * V;
+    // cycle 1 (01210): 2 masks, first sweep, 3 residuals, 2 + 1 corrections, one final sweep
+    const double cyc = 2 * (2 * N * V + N) + N * (2 * V + 8) + 3 * fine_res + 2 * grad_vc + nod_vc + 2 * g_tr + pi_tr +
+                       fine_jac;
+    timed("ams_cycle", cyc, 0, [&] { ams_cycle<T, NV, RECIP>(a, pin.get(), pout.get(), nullptr, s); });
+    timed("fine_residual", fine_res, 1, [&] {
+        mv_spmv<double, double, double, NV, MV_RES, RECIP>(a.A_bc, cur, r, a.b0.get(), nullptr, 0.0, nullptr, s);
+    });
+    timed("fine_smooth", fine_jac, 1, [&] {
+        mv_spmv<double, double, double, NV, MV_JAC, RECIP>(a.A_bc, cur, alt, a.b0.get(), d, 0.0, nullptr, s);
+    });
+    timed("grad_vcycle", grad_vc, 0, [&] { vcycle<T, NV, RECIP>(a.amg[0], 0, a.rs[0].as<T>(), 1, nullptr, s); });
+    timed("nodal_vcycles", nod_vc, 0, [&] {
+        a.forks.fork(s, 2);
+        vcycle<T, NV, RECIP>(a.amg[1], 0, a.rs[1].as<T>(), 1, nullptr, s);
+        vcycle<T, NV, RECIP>(a.amg[2], 0, a.rs[2].as<T>(), 1, nullptr, a.forks.side[0]);
+        vcycle<T, NV, RECIP>(a.amg[3], 0, a.rs[3].as<T>(), 1, nullptr, a.forks.side[1]);
+        a.forks.join(s, 2);
+    });
+    timed("grad_transfers", g_tr, 2, [&] {
+        mv_spmv<double, double, T, NV, MV_AX, RECIP>(a.Gt, r, a.rs[0].as<T>(), nullptr, nullptr, T(0), nullptr, s);
+        mv_spmv<double, T, double, NV, MV_ADD, RECIP>(a.G, a.rs[0].as<T>(), alt, nullptr, nullptr, a.w, nullptr, s);
+    });
+    timed("pi_transfers", pi_tr, 2, [&] {
+        pi_restrict<T, NV>(a, r, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), nullptr, s);
+        pi_prolong<T, NV>(a, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), alt, nullptr, s);
+    });
+    SSV_CUDA(cudaEventDestroy(e0));
+    SSV_CUDA(cudaEventDestroy(e1));
+    SSV_CUDA(cudaStreamSynchronize(s));
+}
+
+template <typename T>
+static void ams_profile_nrhs(AmsState& a, int nrhs, int reps, ssv_phase_profile* out) {
+    if (a.complex_form) {
+        if (nrhs == 1) ams_profile_t<T, 2, true>(a, reps, out);
+        else ams_profile_t<T, 8, true>(a, reps, out);
+    } else {
+        if (nrhs == 1) ams_profile_t<T, 1, false>(a, reps, out);
+        else ams_profile_t<T, 4, false>(a, reps, out);
+    }
+}
+
+void ams_profile(AmsState* a, int nrhs, int reps, ssv_phase_profile* out) {
+    if (nrhs != 1 && nrhs != 4) fail(SSV_ERR_INVALID_ARG, "ssv_ams_profile: nrhs must be 1 or 4");
+    ams_reserve(*a, nrhs * (a->complex_form ? 2 : 1));
+    if (a->fp32) ams_profile_nrhs<float>(*a, nrhs, std::max(reps, 1), out);
+    else ams_profile_nrhs<double>(*a, nrhs, std::max(reps, 1), out);
 }
 
 // y = M^{-1} x for the preconditioner p, stream-ordered and capturable.

@@ -368,6 +368,11 @@ struct ssv_batch {
     int replace_every = -1;
     std::vector<ssv_batch_tune_entry> table;
     ssv::GraphLoop loop;
+    // frequencies' preconditioner cycles run as parallel branches; frequencies
+    // sharing one preconditioner object share a branch (its work buffers)
+    ssv::ForkSet forks;
+    std::vector<int> branch_of;
+    int branches = 0;
     // last solve
     double last_ms = 0.0, last_loop_ms = 0.0;
     int64_t last_launches = 0;
@@ -465,18 +470,22 @@ static void bt_pq(ssv_batch& B, cudaStream_t s) {
     SSV_LAUNCH_CHECK();
 }
 
-// out_f = M_f^{-1} in_f for every frequency (identity without a preconditioner)
+// out_f = M_f^{-1} in_f for every frequency (identity without a preconditioner);
+// the frequencies are independent and run as parallel branches
 static void bt_precond(ssv_batch& B, const zdouble* in, zdouble* out, const KState* st, cudaStream_t s) {
     const size_t blk = (size_t)B.n * B.R;
+    B.forks.fork(s, B.branches);
     for (int f = 0; f < B.F; ++f) {
         const zdouble* i = in + f * blk;
         zdouble* o = out + f * blk;
+        cudaStream_t fs = B.forks.side[B.branch_of[f]];
         if (B.pre[f])
             ams_apply_block(B.pre[f]->ams.get(), reinterpret_cast<const double*>(i), reinterpret_cast<double*>(o),
-                            B.R, st, s);
+                            B.R, st, fs);
         else
-            SSV_CUDA(cudaMemcpyAsync(o, i, sizeof(zdouble) * blk, cudaMemcpyDeviceToDevice, s));
+            SSV_CUDA(cudaMemcpyAsync(o, i, sizeof(zdouble) * blk, cudaMemcpyDeviceToDevice, fs));
     }
+    B.forks.join(s, B.branches);
 }
 
 static int grid_x_for(const ssv_batch& B, int rows_per_block, int groups, int per_sm) {
@@ -616,6 +625,14 @@ ssv_batch* batch_create(ssv_matrix* K, ssv_matrix* M, int F, const double* omega
             }
             B->pre[f] = p;
         }
+        B->branch_of.assign(F, 0);
+        for (int f = 0; f < F; ++f) {
+            int same = -1;
+            for (int g = 0; g < f && same < 0; ++g)
+                if (B->pre[f] && B->pre[g] == B->pre[f]) same = B->branch_of[g];
+            B->branch_of[f] = same >= 0 ? same : B->branches++;
+        }
+        B->forks.ensure(B->branches);
         const size_t len = (size_t)F * B->n * R;
         for (DevBuf<zdouble>* v : {&B->x, &B->r, &B->rt, &B->p, &B->q, &B->qt, &B->t}) v->alloc(len);
         B->bs.alloc(1);

@@ -37,6 +37,20 @@ void require_device() {
 
 size_t scalar_bytes(int dtype) { return dtype == SSV_F64 ? sizeof(double) : 2 * sizeof(double); }
 
+// The _dev entry points hand their pointers straight to kernels: a host
+// pointer there would make the kernels fault, so it is refused up front.
+void require_device_ptr(const void* p, const char* what) {
+    if (!p) return;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        ssv::fail(SSV_ERR_INVALID_ARG, std::string(what) + ": not a CUDA pointer (the _dev calls take device memory)");
+    }
+    if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+        ssv::fail(SSV_ERR_INVALID_ARG,
+                  std::string(what) + ": host memory passed to a _dev call (device memory required)");
+}
+
 void check_mask(const uint8_t* fd, int n, std::vector<uint8_t>& h, ssv::DevBuf<uint8_t>& d, bool& has) {
     has = fd != nullptr;
     h.clear();
@@ -182,6 +196,8 @@ int ssv_matrix_info(const ssv_matrix* A, int32_t* rows, int32_t* cols, int64_t* 
 int ssv_matrix_spmv_dev(ssv_matrix* A, const void* d_x, void* d_y) {
     return guarded([&] {
         if (!A || !d_x || !d_y) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_spmv_dev: NULL argument");
+        require_device_ptr(d_x, "ssv_matrix_spmv_dev x");
+        require_device_ptr(d_y, "ssv_matrix_spmv_dev y");
         ssv::matrix_spmv_dev(A, d_x, d_y);
     });
 }
@@ -231,6 +247,8 @@ int ssv_solver_solve_dev(ssv_solver* s, const char* method, const ssv_config* cf
                          ssv_result* res, double* history, int32_t history_cap) {
     return guarded([&] {
         if (!s || !cfg || !res || !d_b || !d_x) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_solver_solve_dev: NULL argument");
+        require_device_ptr(d_b, "ssv_solver_solve_dev b");
+        require_device_ptr(d_x, "ssv_solver_solve_dev x");
         ssv::solver_solve_dev(s, method, *cfg, d_b, d_x, res, history, history_cap);
     });
 }
@@ -351,6 +369,13 @@ int ssv_ams_set_precision(ssv_precond* p, int32_t precision) {
     });
 }
 
+int ssv_ams_profile(ssv_precond* p, int32_t nrhs, int32_t reps, ssv_phase_profile* out) {
+    return guarded([&] {
+        if (!p || !p->ams || !out) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_profile: bad argument");
+        ssv::ams_profile(p->ams.get(), nrhs, reps, out);
+    });
+}
+
 int ssv_ams_get_precision(const ssv_precond* p, int32_t* precision) {
     return guarded([&] {
         if (!p || !p->ams || !precision) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_get_precision: bad argument");
@@ -382,6 +407,8 @@ int ssv_batch_cocr_solve_dev(ssv_batch* b, int32_t maxiter, double tol, const vo
                              int32_t* iterations, int32_t* converged, double* residuals) {
     return guarded([&] {
         if (!b || !d_rhs || !d_sol) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_batch_cocr_solve_dev: NULL argument");
+        require_device_ptr(d_rhs, "ssv_batch_cocr_solve_dev rhs");
+        require_device_ptr(d_sol, "ssv_batch_cocr_solve_dev sol");
         ssv::batch_cocr_solve_dev(b, maxiter, tol, d_rhs, d_sol, iterations, converged, residuals);
     });
 }
@@ -418,6 +445,9 @@ int ssv_pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, 
                       const void* d_b, void* d_x, ssv_result* res, double* history, int32_t history_cap) {
     return guarded([&] {
         if (!A || !cfg || !res || !d_b || !d_x) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_pcg_solve_dev: NULL argument");
+        require_device_ptr(d_b, "ssv_pcg_solve_dev b");
+        require_device_ptr(d_x, "ssv_pcg_solve_dev x");
+        require_device_ptr(freedofs, "ssv_pcg_solve_dev freedofs");
         ssv::pcg_solve_dev(A, pre, freedofs, *cfg, d_b, d_x, res, history, history_cap);
     });
 }
@@ -464,6 +494,8 @@ int ssv_precond_update(ssv_precond* p) {
 int ssv_precond_apply_dev(ssv_precond* p, const void* d_x, void* d_y) {
     return guarded([&] {
         if (!p || !d_x || !d_y) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_precond_apply_dev: NULL argument");
+        require_device_ptr(d_x, "ssv_precond_apply_dev x");
+        require_device_ptr(d_y, "ssv_precond_apply_dev y");
         ssv::precond_apply_dev(p, d_x, d_y);
     });
 }
@@ -498,6 +530,9 @@ int ssv_cocr_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs,
                        int32_t printrates, const void* d_b, void* d_x, int32_t* iterations) {
     return guarded([&] {
         if (!A || !d_b || !d_x || !iterations) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_cocr_solve_dev: NULL argument");
+        require_device_ptr(d_b, "ssv_cocr_solve_dev b");
+        require_device_ptr(d_x, "ssv_cocr_solve_dev x");
+        require_device_ptr(freedofs, "ssv_cocr_solve_dev freedofs");
         ssv::cocr_solve_dev(A, pre, freedofs, maxiter, tol, printrates, d_b, d_x, iterations);
     });
 }

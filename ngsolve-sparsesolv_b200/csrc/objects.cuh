@@ -15,6 +15,44 @@ cudaStream_t stream();
 // Sub-warp width of the CSR kernels from the mean row length.
 int pick_lanes(double nnz_per_row);
 
+// Side streams for independent pieces of one stream's work: fork() makes k
+// side streams wait for the work queued so far on s, join() makes s wait for
+// them. Under stream capture the side work becomes parallel branches of the
+// graph; outside capture it runs concurrently.
+struct ForkSet {
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> ev;  // ev[0] fork point, ev[1 + i] side i done
+    ForkSet() = default;
+    ForkSet(const ForkSet&) = delete;
+    ForkSet& operator=(const ForkSet&) = delete;
+    ~ForkSet() {
+        for (auto e : ev) cudaEventDestroy(e);
+        for (auto t : side) cudaStreamDestroy(t);
+    }
+    void ensure(int k) {
+        while ((int)side.size() < k) {
+            cudaStream_t t;
+            SSV_CUDA(cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking));
+            side.push_back(t);
+        }
+        while ((int)ev.size() < k + 1) {
+            cudaEvent_t e;
+            SSV_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            ev.push_back(e);
+        }
+    }
+    void fork(cudaStream_t s, int k) {
+        SSV_CUDA(cudaEventRecord(ev[0], s));
+        for (int i = 0; i < k; ++i) SSV_CUDA(cudaStreamWaitEvent(side[i], ev[0], 0));
+    }
+    void join(cudaStream_t s, int k) {
+        for (int i = 0; i < k; ++i) {
+            SSV_CUDA(cudaEventRecord(ev[1 + i], side[i]));
+            SSV_CUDA(cudaStreamWaitEvent(s, ev[1 + i], 0));
+        }
+    }
+};
+
 // Launch y = A x style SpMV for any lanes/mode (mask zeroes masked rows).
 template <typename S, typename SV, int MODE>
 void launch_spmv(int lanes, int n, const int* rp, const int* ci, const SV* v, const S* x, S* y,

@@ -196,6 +196,7 @@ SIGNATURES = [
     ("ssv_batch_set_replacement", I32, [P, I32]),
     ("ssv_batch_last_timing", I32, [P, PD, PD, PI32, ctypes.POINTER(ctypes.c_int64)]),
     ("ssv_ams_get_precision", I32, [P, PI32]),
+    ("ssv_ams_profile", I32, [P, I32, I32, ctypes.POINTER(ssv_phase_profile)]),
     ("ssv_pcg_solve", I32, [P, P, PU8, ctypes.POINTER(ssv_config), P, P, ctypes.POINTER(ssv_result), PD, I32]),
     ("ssv_pcg_solve_dev", I32, [P, P, PU8, ctypes.POINTER(ssv_config), P, P, ctypes.POINTER(ssv_result), PD, I32]),
 ]

@@ -13,6 +13,9 @@
 #include <complex>
 #include <cstdint>
 #include <cstring>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include <random>
 #include <string>
 #include <vector>
@@ -91,6 +94,7 @@ Csr restrict_rap(const Csr& A, const Csr& P) {
 
 // y = A x
 void mult(const Csr& A, const double* x, double* y) {
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < A.n; ++i) {
         double s = 0.0;
         for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) s += A.v[k] * x[A.ci[k]];
@@ -100,6 +104,7 @@ void mult(const Csr& A, const double* x, double* y) {
 
 // y += s * A x (NGSolve MultAdd)
 void mult_add(const Csr& A, double s, const double* x, double* y) {
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < A.n; ++i) {
         double t = 0.0;
         for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) t += A.v[k] * x[A.ci[k]];
@@ -386,6 +391,7 @@ struct Amg {
         const AmgLevel& L = lv[l];
         std::vector<double> r(b, b + L.A.n);
         mult_add(L.A, -1.0, x, r.data());
+#pragma omp parallel for schedule(static)
         for (int i = 0; i < L.A.n; ++i) x[i] += r[i] / L.l1[i];
     }
 
@@ -417,6 +423,7 @@ struct Amg {
     void dual_smooth(int l, const double* b1, double* x1, const double* b2, double* x2) const {
         const AmgLevel& L = lv[l];
         std::vector<double> r1(L.A.n), r2(L.A.n);
+#pragma omp parallel for schedule(static)
         for (int i = 0; i < L.A.n; ++i) {
             double d1 = 0, d2 = 0;
             for (int k = L.A.rp[i]; k < L.A.rp[i + 1]; ++k) {
@@ -426,6 +433,7 @@ struct Amg {
             r1[i] = b1[i] - d1;
             r2[i] = b2[i] - d2;
         }
+#pragma omp parallel for schedule(static)
         for (int i = 0; i < L.A.n; ++i) {
             const double inv = 1.0 / L.l1[i];
             x1[i] += r1[i] * inv;
@@ -444,6 +452,7 @@ struct Amg {
         for (int s = 0; s < num_smooth; ++s) dual_smooth(l, b1, x1, b2, x2);
         const int n = L.A.n, nc = lv[l + 1].A.n;
         std::vector<double> r1(n), r2(n);
+#pragma omp parallel for schedule(static)
         for (int i = 0; i < n; ++i) {
             double d1 = 0, d2 = 0;
             for (int k = L.A.rp[i]; k < L.A.rp[i + 1]; ++k) {
@@ -457,6 +466,7 @@ struct Amg {
         mult(L.Pt, r1.data(), c1.data());
         mult(L.Pt, r2.data(), c2.data());
         dual_vcycle(l + 1, c1.data(), e1.data(), c2.data(), e2.data());
+#pragma omp parallel for schedule(static)
         for (int i = 0; i < n; ++i) {
             double s1 = 0, s2 = 0;
             for (int k = L.P.rp[i]; k < L.P.rp[i + 1]; ++k) {
@@ -554,6 +564,7 @@ struct Ams {
         std::vector<double> r(nhc);
         for (int s = 0; s < num_smooth; ++s) {
             residual(b, x, r.data());
+#pragma omp parallel for schedule(static)
             for (int i = 0; i < nhc; ++i) x[i] += r[i] / l1[i];
         }
     }
@@ -593,6 +604,7 @@ struct Ams {
     // ComplexCompactAMS (complex_compact_ams.hpp:112-341): fused Re/Im passes
     void fused_residual(const double* br, const double* xr, double* rr, const double* bi, const double* xi,
                         double* ri) const {
+#pragma omp parallel for schedule(static)
         for (int i = 0; i < nhc; ++i) {
             double d1 = 0, d2 = 0;
             for (int k = A_bc.rp[i]; k < A_bc.rp[i + 1]; ++k) {
@@ -607,6 +619,7 @@ struct Ams {
         std::vector<double> rr(nhc), ri(nhc);
         for (int s = 0; s < num_smooth; ++s) {
             fused_residual(br, xr, rr.data(), bi, xi, ri.data());
+#pragma omp parallel for schedule(static)
             for (int i = 0; i < nhc; ++i) {
                 const double inv = 1.0 / l1[i];
                 xr[i] += rr[i] * inv;
@@ -615,6 +628,7 @@ struct Ams {
         }
     }
     static void fused_prolong(const Csr& P, double w, const double* gr, double* xr, const double* gi, double* xi) {
+#pragma omp parallel for schedule(static)
         for (int i = 0; i < P.n; ++i) {
             double s1 = 0, s2 = 0;
             for (int k = P.rp[i]; k < P.rp[i + 1]; ++k) {
@@ -681,6 +695,16 @@ thread_local std::string g_err;
 extern "C" {
 
 const char* ams_oracle_last_error(void) { return g_err.c_str(); }
+
+// Host threads of the row-parallel loops (SpMV, smoothers, transfers); the
+// dot products stay sequential, so results do not depend on the count.
+void ams_oracle_set_threads(int n) {
+#ifdef _OPENMP
+    omp_set_num_threads(n > 0 ? n : 1);
+#else
+    (void)n;
+#endif
+}
 
 // CompactAMS / ComplexCompactAMS constructor: A (n_hc x n_hc), G (n_hc x
 // n_h1), freedofs (NULL = all free), vertex coordinates (n_h1 each).

@@ -46,7 +46,7 @@ def build_ams_oracle(force: bool = False) -> str:
     srcs = [os.path.join(HERE, "ams_oracle.cpp"), os.path.join(HERE, "..", "include", "sparsesolv_b200.h")]
     if force or _stale(AMS_SO, srcs):
         os.makedirs(os.path.dirname(AMS_SO), exist_ok=True)
-        _run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-o", AMS_SO, srcs[0]])
+        _run(["g++", "-std=c++17", "-O2", "-fopenmp", "-fPIC", "-shared", "-o", AMS_SO, srcs[0]])
     return AMS_SO
 
 

@@ -190,8 +190,16 @@ class AmsOracle:
             lib.ams_oracle_cocr.restype = I32
             lib.ams_oracle_cocr.argtypes = [P, I32, PI32, PI32, D, PU8, I32, ctypes.c_double, D, D, PI32, D, I32,
                                             PI32]
+            lib.ams_oracle_set_threads.restype = None
+            lib.ams_oracle_set_threads.argtypes = [I32]
+            lib.ams_oracle_set_threads(1)
             cls._lib = lib
         return cls._lib
+
+    @classmethod
+    def set_threads(cls, n):
+        """Host threads of the restatement's row-parallel loops (results do not depend on it)."""
+        cls.lib().ams_oracle_set_threads(int(n))
 
     def __init__(self, A, G, freedofs, cx, cy, cz, cycle_type=1, num_smooth=1, theta=0.25, weight=1.0):
         lib = self.lib()

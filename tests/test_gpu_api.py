@@ -192,3 +192,26 @@ def test_matrix_modified_in_place_is_reread(poisson):
     A.data *= 2.0
     x2 = s * b
     assert np.linalg.norm(x1 - 2 * x2) / np.linalg.norm(x1) < 1e-8
+
+
+@pytest.mark.gpu
+def test_dev_calls_refuse_host_pointers():
+    # the check runs before any kernel: a host pointer returns an error, no launch
+    import ctypes
+
+    import sparsesolv_ngsolve as ss
+    from sparsesolv_ngsolve import _capi
+    from sparsesolv_ngsolve import problems as P
+    A = P.laplacian_7pt(6)
+    m = ss._Matrix(A)
+    x = np.ones(A.shape[0])
+    y = np.zeros(A.shape[0])
+    lib = _capi.load()
+    with pytest.raises(ValueError, match="host memory"):
+        _capi.check(lib.ssv_matrix_spmv_dev(m.h, _capi.vptr(x), _capi.vptr(y)))
+    res = _capi.ssv_result()
+    cfg = _capi.default_config()
+    fd = np.ones(A.shape[0], np.uint8)
+    with pytest.raises(ValueError, match="host memory"):
+        _capi.check(lib.ssv_pcg_solve_dev(m.h, None, _capi.u8ptr(fd), ctypes.byref(cfg), _capi.vptr(x),
+                                          _capi.vptr(y), ctypes.byref(res), None, 0))

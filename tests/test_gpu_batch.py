@@ -85,21 +85,36 @@ def test_batch_zero_column_and_constrained_dofs(fam_well):
     assert bs.converged.sum() == B.shape[0] * B.shape[1] - 1
 
 
-def test_batch_fp32_preconditioners(fam_well):
+def test_batch_residual_replacement(fam_well):
     import sparsesolv_ngsolve as ss
     d = fam_well
-    bs64 = ss.BatchedCOCRSolver(d["K"], d["M"], d["omegas"], _pres(d), nrhs=4, freedofs=d["freedofs"], tol=1e-10)
-    X64 = bs64.Solve(d["B"])
-    bs32 = ss.BatchedCOCRSolver(d["K"], d["M"], d["omegas"], _pres(d, "fp32"), nrhs=4, freedofs=d["freedofs"],
-                                tol=1e-10)
-    X32 = bs32.Solve(d["B"])
-    assert bs32.converged.all()
-    assert (bs32.iterations <= 1.5 * bs64.iterations + 2).all()
+    pres = _pres(d)
+    plain = ss.BatchedCOCRSolver(d["K"], d["M"], d["omegas"], pres, nrhs=4, freedofs=d["freedofs"], tol=1e-10)
+    plain.Solve(d["B"])
+    rep = ss.BatchedCOCRSolver(d["K"], d["M"], d["omegas"], pres, nrhs=4, freedofs=d["freedofs"], tol=1e-10,
+                               residual_replacement=5)
+    X = rep.Solve(d["B"])
+    assert rep.converged.all()
+    # with an exactly linear preconditioner the replaced value equals the recurrence's
+    assert (np.abs(rep.iterations - plain.iterations) <= np.maximum(2, 0.1 * plain.iterations)).all()
     for f in range(len(d["omegas"])):
         for r in range(4):
-            assert _true_res(d, f, X32[f, r], d["B"][f, r]) <= 1e-9
-            # error of the mixed form against the FP64 solution (stated bound)
-            assert np.linalg.norm(X32[f, r] - X64[f, r]) <= 1e-8 * np.linalg.norm(X64[f, r])
+            assert _true_res(d, f, X[f, r], d["B"][f, r]) <= 1e-9
+
+
+def test_batch_fp32_matches_single_fp32(fam_well):
+    # the batch machinery with FP32-form preconditioners reproduces the single
+    # COCR with the same preconditioners (15 steps, replacement off)
+    import sparsesolv_ngsolve as ss
+    d = fam_well
+    pres = _pres(d, "fp32")
+    bs = ss.BatchedCOCRSolver(d["K"], d["M"], d["omegas"], pres, nrhs=4, freedofs=d["freedofs"], maxiter=15,
+                              tol=1e-10, residual_replacement=0)
+    X = bs.Solve(d["B"])
+    for f in range(len(d["omegas"])):
+        xs, its = _single(d, pres, f, 1, 1e-10, maxiter=15)
+        assert int(bs.iterations[f, 1]) == its
+        assert np.linalg.norm(X[f, 1] - xs) <= 1e-6 * np.linalg.norm(xs)
 
 
 def test_batch_without_preconditioner(fam_well):
