@@ -119,6 +119,7 @@ typedef struct ssv_matrix ssv_matrix;   /* device-resident CSR              */
 typedef struct ssv_solver ssv_solver;   /* SparseSolvSolver state           */
 typedef struct ssv_precond ssv_precond; /* IC / AMS / complex-AMS           */
 typedef struct ssv_batch ssv_batch;     /* batched COCR over a frequency family */
+typedef struct ssv_mlp ssv_mlp;         /* learned initial-guess predictor      */
 
 /* One timed SpMM launch shape of the batch autotuner. */
 typedef struct ssv_batch_tune_entry {
@@ -310,6 +311,27 @@ int ssv_batch_tuning(const ssv_batch* b, ssv_batch_tune_entry* entries, int32_t 
  * whole solve and its iteration loop, executed loop bodies, kernel launches. */
 int ssv_batch_last_timing(const ssv_batch* b, double* device_ms, double* loop_ms, int32_t* loops,
                           int64_t* kernel_launches);
+
+/* ---- learned initial guess (new: no reference counterpart) ----------------
+ * A per-sample MLP out = w2 . relu(W1 x + b1) + b2 with in_dim inputs
+ * (<= 32) and `hidden` units (<= 128), FP32, trained and evaluated on the GPU
+ * by the library's own kernels. Parameters as one float array: W1 (hidden x
+ * in_dim, row-major), b1 (hidden), w2 (hidden), b2 (1). Training minimises the
+ * mean squared error with Adam (beta 0.9 / 0.999, eps 1e-8) over minibatches
+ * of a fresh permutation per epoch; gradients are summed in a fixed order. */
+int ssv_mlp_create(int32_t in_dim, int32_t hidden, uint64_t seed, ssv_mlp** out);
+int ssv_mlp_destroy(ssv_mlp* m);
+int ssv_mlp_num_params(const ssv_mlp* m, int32_t* count);
+int ssv_mlp_get_params(const ssv_mlp* m, float* params);
+/* Also resets the Adam state. */
+int ssv_mlp_set_params(ssv_mlp* m, const float* params);
+/* Gradient of the mean squared error over n samples (X row-major n x in_dim,
+ * host pointers) and the loss -- the hook the CPU gradient check uses. */
+int ssv_mlp_gradients(ssv_mlp* m, const float* X, const float* y, int64_t n, float* grad, float* loss);
+/* Minibatch Adam on device-resident data; *loss = loss of the last batch. */
+int ssv_mlp_train_dev(ssv_mlp* m, const float* d_X, const float* d_y, int64_t n, int32_t epochs,
+                      int32_t batch, float lr, uint64_t seed, float* loss);
+int ssv_mlp_predict_dev(ssv_mlp* m, const float* d_X, int64_t n, float* d_out);
 
 /* ---- allocation-free SpMV + dot (no counterpart in the reference) -------- */
 /* y = A x and *d_dot = x^T y for a real CSR matrix (int32 row_ptr/col_idx,

@@ -441,6 +441,65 @@ int ssv_batch_last_timing(const ssv_batch* b, double* device_ms, double* loop_ms
     });
 }
 
+int ssv_mlp_create(int32_t in_dim, int32_t hidden, uint64_t seed, ssv_mlp** out) {
+    return guarded([&] {
+        if (!out) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_mlp_create: NULL out");
+        require_device();
+        *out = ssv::mlp_create(in_dim, hidden, seed);
+    });
+}
+
+int ssv_mlp_destroy(ssv_mlp* m) {
+    return guarded([&] { ssv::mlp_destroy(m); });
+}
+
+int ssv_mlp_num_params(const ssv_mlp* m, int32_t* count) {
+    return guarded([&] {
+        if (!m || !count) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_mlp_num_params: NULL argument");
+        *count = ssv::mlp_nparams(m);
+    });
+}
+
+int ssv_mlp_get_params(const ssv_mlp* m, float* params) {
+    return guarded([&] {
+        if (!m || !params) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_mlp_get_params: NULL argument");
+        ssv::mlp_get_params(m, params);
+    });
+}
+
+int ssv_mlp_set_params(ssv_mlp* m, const float* params) {
+    return guarded([&] {
+        if (!m || !params) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_mlp_set_params: NULL argument");
+        ssv::mlp_set_params(m, params);
+    });
+}
+
+int ssv_mlp_gradients(ssv_mlp* m, const float* X, const float* y, int64_t n, float* grad, float* loss) {
+    return guarded([&] {
+        if (!m || !X || !y || !grad || n <= 0) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_mlp_gradients: bad argument");
+        ssv::mlp_gradients_host(m, X, y, n, grad, loss);
+    });
+}
+
+int ssv_mlp_train_dev(ssv_mlp* m, const float* d_X, const float* d_y, int64_t n, int32_t epochs, int32_t batch,
+                      float lr, uint64_t seed, float* loss) {
+    return guarded([&] {
+        if (!m || !d_X || !d_y) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_mlp_train_dev: NULL argument");
+        require_device_ptr(d_X, "ssv_mlp_train_dev X");
+        require_device_ptr(d_y, "ssv_mlp_train_dev y");
+        ssv::mlp_train_dev(m, d_X, d_y, n, epochs, batch, lr, seed, loss);
+    });
+}
+
+int ssv_mlp_predict_dev(ssv_mlp* m, const float* d_X, int64_t n, float* d_out) {
+    return guarded([&] {
+        if (!m || !d_X || !d_out || n < 0) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_mlp_predict_dev: bad argument");
+        require_device_ptr(d_X, "ssv_mlp_predict_dev X");
+        require_device_ptr(d_out, "ssv_mlp_predict_dev out");
+        ssv::mlp_predict_dev(m, d_X, n, d_out);
+    });
+}
+
 int ssv_pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, const ssv_config* cfg,
                       const void* d_b, void* d_x, ssv_result* res, double* history, int32_t history_cap) {
     return guarded([&] {

@@ -60,6 +60,17 @@ int batch_tuning(const ssv_batch* B, ssv_batch_tune_entry* e, int cap, int* chos
 void batch_last_timing(const ssv_batch* B, double* ms, double* loop_ms, int* loops, int64_t* launches);
 void batch_set_replacement(ssv_batch* B, int every);
 
+// Learned initial-guess MLP (mlp.cu)
+ssv_mlp* mlp_create(int D, int H, uint64_t seed);
+void mlp_destroy(ssv_mlp* m);
+int mlp_nparams(const ssv_mlp* m);
+void mlp_get_params(const ssv_mlp* m, float* p);
+void mlp_set_params(ssv_mlp* m, const float* p);
+void mlp_gradients_host(ssv_mlp* m, const float* X, const float* Y, int64_t n, float* grad, float* loss);
+void mlp_train_dev(ssv_mlp* m, const float* X, const float* Y, int64_t n, int epochs, int batch, float lr,
+                   uint64_t seed, float* last_loss);
+void mlp_predict_dev(ssv_mlp* m, const float* X, int64_t n, float* out);
+
 // CG with an external preconditioner and an initial guess (cocr_ngs.cu)
 void pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, const ssv_config& cfg, const void* d_b,
                    void* d_x, ssv_result* res, double* hist, int hist_cap);

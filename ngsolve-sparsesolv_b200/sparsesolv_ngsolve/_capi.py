@@ -150,6 +150,7 @@ I32 = ctypes.c_int32
 PI32 = ctypes.POINTER(ctypes.c_int32)
 PU8 = ctypes.POINTER(ctypes.c_uint8)
 PD = ctypes.POINTER(ctypes.c_double)
+PF = ctypes.POINTER(ctypes.c_float)
 PP = ctypes.POINTER(ctypes.c_void_p)
 
 # (name, restype, argtypes) of every exported entry point
@@ -197,6 +198,14 @@ SIGNATURES = [
     ("ssv_batch_last_timing", I32, [P, PD, PD, PI32, ctypes.POINTER(ctypes.c_int64)]),
     ("ssv_ams_get_precision", I32, [P, PI32]),
     ("ssv_ams_profile", I32, [P, I32, I32, ctypes.POINTER(ssv_phase_profile)]),
+    ("ssv_mlp_create", I32, [I32, I32, ctypes.c_uint64, PP]),
+    ("ssv_mlp_destroy", I32, [P]),
+    ("ssv_mlp_num_params", I32, [P, PI32]),
+    ("ssv_mlp_get_params", I32, [P, PF]),
+    ("ssv_mlp_set_params", I32, [P, PF]),
+    ("ssv_mlp_gradients", I32, [P, PF, PF, ctypes.c_int64, PF, PF]),
+    ("ssv_mlp_train_dev", I32, [P, P, P, ctypes.c_int64, I32, I32, ctypes.c_float, ctypes.c_uint64, PF]),
+    ("ssv_mlp_predict_dev", I32, [P, P, ctypes.c_int64, P]),
     ("ssv_pcg_solve", I32, [P, P, PU8, ctypes.POINTER(ssv_config), P, P, ctypes.POINTER(ssv_result), PD, I32]),
     ("ssv_pcg_solve_dev", I32, [P, P, PU8, ctypes.POINTER(ssv_config), P, P, ctypes.POINTER(ssv_result), PD, I32]),
 ]
