@@ -242,8 +242,12 @@ int ssv_ams_get_precision(const ssv_precond* p, int32_t* precision);
  * AMS cycle on nrhs (1 or 4) right-hand sides -- the whole cycle, one fine
  * residual pass, one fine smoothing pass, the gradient V-cycle, the three
  * nodal V-cycles, the G and Pi transfers -- each re-launched reps times
- * between CUDA events, with the algorithmic bytes of one execution. */
-int ssv_ams_profile(ssv_precond* p, int32_t nrhs, int32_t reps, ssv_phase_profile* out);
+ * between CUDA events, with the algorithmic bytes of one execution. flags:
+ * SSV_PROFILE_COLD times every launch alone after evicting the L2 (a 256 MiB
+ * write; the buffer is kept until exit), the HBM-bound case; 0 times the
+ * launches back to back (operands that fit in L2 stay there). */
+#define SSV_PROFILE_COLD 1
+int ssv_ams_profile(ssv_precond* p, int32_t nrhs, int32_t reps, int32_t flags, ssv_phase_profile* out);
 
 /* ---- CG with an external preconditioner (new: the reference's AMS scripts
  *      drive it with NGSolve's krylovspace.CGSolver) ---------------------------

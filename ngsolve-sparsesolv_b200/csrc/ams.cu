@@ -245,6 +245,52 @@ __global__ void k_mv_first_sweep(int n, const T* __restrict__ b, const T* __rest
     }
 }
 
+// The first Jacobi sweep from x = 0 fused with the residual that follows it:
+// x = b (/ or *) l1 and r = b - A x, the neighbours' x formed on the fly from
+// b and l1 (the same values the two separate passes would store and read).
+template <typename T, int NV, int LANES, bool RECIP>
+__global__ void __launch_bounds__(kBlock)
+k_mv_first_res(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ v,
+               const T* __restrict__ b, const T* __restrict__ d, T* __restrict__ x, T* __restrict__ r,
+               const KState* st) {
+    if (st && st->done) return;
+    const int sub = threadIdx.x % LANES;
+    const int rpb = kBlock / LANES;
+    const int lane_row = (threadIdx.x & 31) / LANES;  // warp-uniform trip count
+    for (int row = blockIdx.x * rpb + threadIdx.x / LANES; row - lane_row < n; row += gridDim.x * rpb) {
+        const bool valid = row < n;
+        T acc[NV];
+#pragma unroll
+        for (int c = 0; c < NV; ++c) acc[c] = T(0);
+        if (valid) {
+            const int k1 = rp[row + 1];
+            for (int k = rp[row] + sub; k < k1; k += LANES) {
+                const int j = ci[k];
+                const T a = v[k];
+                const T dj = d[j];
+                T bj[NV];
+                load_row<NV>(b + (size_t)j * NV, bj);
+#pragma unroll
+                for (int c = 0; c < NV; ++c) acc[c] += a * (RECIP ? bj[c] * dj : bj[c] / dj);
+            }
+        }
+#pragma unroll
+        for (int o = LANES / 2; o > 0; o >>= 1)
+#pragma unroll
+            for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o, LANES);
+        if (valid && sub == 0) {
+            const size_t base = (size_t)row * NV;
+            const T di = d[row];
+#pragma unroll
+            for (int c = 0; c < NV; ++c) {
+                const T bi = b[base + c];
+                x[base + c] = RECIP ? bi * di : bi / di;
+                r[base + c] = bi - acc[c];
+            }
+        }
+    }
+}
+
 // out = mask ? in : 0, converting between the Krylov type (FP64) and the
 // cycle's type at the two ends of the cycle
 template <typename TI, typename TO, int NV>
@@ -430,6 +476,21 @@ static void first_sweep(int n, const T* b, const T* d, T* x, const KState* st, c
     k_mv_first_sweep<T, NV, RECIP><<<grid_for((int64_t)n * NV, kBlock), kBlock, 0, s>>>(n, b, d, x, st);
 }
 
+template <typename T, int NV, bool RECIP>
+static void first_res(const DevCsr& A, const T* b, const T* d, T* x, T* r, const KState* st, cudaStream_t s) {
+    const int lanes = A.lanes_for(NV);
+    const int rpb = kBlock / lanes;
+    const int grid = std::max(1, std::min((A.n + rpb - 1) / rpb, sm_count() * 8));
+    const T* v = A.val<T>();
+    switch (lanes) {
+        case 2: k_mv_first_res<T, NV, 2, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
+        case 4: k_mv_first_res<T, NV, 4, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
+        case 8: k_mv_first_res<T, NV, 8, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
+        case 16: k_mv_first_res<T, NV, 16, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
+        default: k_mv_first_res<T, NV, 32, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
+    }
+}
+
 template <typename T, bool RECIP>
 static const T* l1_of(const AmgDevLevel& lv) {
     return RECIP ? lv.il1.get<T>() : lv.l1.get<T>();
@@ -460,10 +521,15 @@ static T* vcycle(std::vector<AmgDevLevel>& L, int l, const T* b, int num_smooth,
         }
         return cur;
     }
-    // pre-smoothing from x = 0: the first sweep is x = b / l1
-    first_sweep<T, NV, RECIP>(lv.A.n, b, d, cur, st, s);
-    sweep(num_smooth - 1);
-    mv_spmv<T, T, T, NV, MV_RES, RECIP>(lv.A, cur, lv.r.as<T>(), b, nullptr, T(0), st, s);
+    // pre-smoothing from x = 0: the first sweep is x = b / l1 (fused with the
+    // residual when it is the only sweep)
+    if (num_smooth == 1) {
+        first_res<T, NV, RECIP>(lv.A, b, d, cur, lv.r.as<T>(), st, s);
+    } else {
+        first_sweep<T, NV, RECIP>(lv.A.n, b, d, cur, st, s);
+        sweep(num_smooth - 1);
+        mv_spmv<T, T, T, NV, MV_RES, RECIP>(lv.A, cur, lv.r.as<T>(), b, nullptr, T(0), st, s);
+    }
     AmgDevLevel& nx = L[l + 1];
     mv_spmv<T, T, T, NV, MV_AX, RECIP>(lv.Pt, lv.r.as<T>(), nx.b.as<T>(), nullptr, nullptr, T(0), st, s);
     T* ec = vcycle<T, NV, RECIP>(L, l + 1, nx.b.as<T>(), num_smooth, st, s);
@@ -528,7 +594,11 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
     double* r = a.r.get();
     const int gm = grid_for((int64_t)n * NV, kBlock);
     k_mv_mask_copy<double, double, NV><<<gm, kBlock, 0, s>>>(n, in, fd, b0, st);
-    bool fresh = true;  // x == 0
+    // (the fused first sweep + residual is not used on the fine level: with
+    // 7.4M nonzeros its second gather, of l1, costs more than the separate
+    // elementwise sweep saves)
+    bool fresh = true;      // x == 0
+    bool deferred = false;  // a lone first sweep waiting to be fused with the next residual
     auto fine_smooth = [&]() {
         for (int k = 0; k < a.num_smooth; ++k) {
             if (fresh) {
@@ -541,21 +611,32 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
         }
     };
     auto ensure_x = [&]() {
+        if (deferred) {
+            first_sweep<double, NV, RECIP>(n, b0, d, cur, st, s);
+            deferred = false;
+        }
         if (fresh) {
             SSV_CUDA(cudaMemsetAsync(cur, 0, sizeof(double) * (size_t)n * NV, s));
             fresh = false;
         }
     };
-    auto gradient = [&]() {
+    auto residual = [&]() {  // r = b0 - A_bc x
+        if (deferred) {
+            first_res<double, NV, RECIP>(a.A_bc, b0, d, cur, r, st, s);
+            deferred = false;
+            return;
+        }
         ensure_x();
         mv_spmv<double, double, double, NV, MV_RES, RECIP>(a.A_bc, cur, r, b0, nullptr, 0.0, st, s);
+    };
+    auto gradient = [&]() {
+        residual();
         mv_spmv<double, double, T, NV, MV_AX, RECIP>(a.Gt, r, a.rs[0].as<T>(), nullptr, nullptr, T(0), st, s);
         T* g = vcycle<T, NV, RECIP>(a.amg[0], 0, a.rs[0].as<T>(), 1, st, s);
         mv_spmv<double, T, double, NV, MV_ADD, RECIP>(a.G, g, cur, nullptr, nullptr, a.w, st, s);
     };
     auto nodal = [&]() {
-        ensure_x();
-        mv_spmv<double, double, double, NV, MV_RES, RECIP>(a.A_bc, cur, r, b0, nullptr, 0.0, st, s);
+        residual();
         pi_restrict<T, NV>(a, r, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), st, s);
         // the three V-cycles are independent (own hierarchies and vectors)
         a.forks.fork(s, 2);
@@ -592,10 +673,50 @@ static HostCsr host_csr_of(const ssv_matrix* M) {
 // operands) and keep the fastest. Runs when work vectors are (re)allocated,
 // outside any capture.
 // ---------------------------------------------------------------------------
+// Evicts the 126 MB L2 by writing a 256 MiB buffer (allocated on first use,
+// kept until exit): the measurements below that stand for HBM-bound passes
+// time each launch after a flush.
+static void l2_flush(cudaStream_t s) {
+    static DevBuf<uint8_t> buf;
+    static int k = 0;
+    if (!buf.get()) buf.alloc((size_t)256 << 20);
+    SSV_CUDA(cudaMemsetAsync(buf.get(), ++k & 0xff, buf.size(), s));
+}
+
+// Device time of `reps` launches: back to back (warm), or each after an L2
+// flush and timed alone (cold).
+template <typename F>
+static float time_launches(F&& launch, int reps, bool cold, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+    float total = 0.f;
+    if (!cold) {
+        SSV_CUDA(cudaEventRecord(e0, s));
+        for (int k = 0; k < reps; ++k) launch();
+        SSV_CUDA(cudaEventRecord(e1, s));
+        SSV_CUDA(cudaEventSynchronize(e1));
+        SSV_LAUNCH_CHECK();
+        SSV_CUDA(cudaEventElapsedTime(&total, e0, e1));
+        return total;
+    }
+    for (int k = 0; k < reps; ++k) {
+        l2_flush(s);
+        SSV_CUDA(cudaEventRecord(e0, s));
+        launch();
+        SSV_CUDA(cudaEventRecord(e1, s));
+        SSV_CUDA(cudaEventSynchronize(e1));
+        SSV_LAUNCH_CHECK();
+        float ms = 0.f;
+        SSV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        total += ms;
+    }
+    return total;
+}
+
 template <typename TV, typename TX, typename TY, int NV>
 static void tune_csr(DevCsr& A, const TX* x, TY* y, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
     if (A.n == 0 || A.nnz == 0) return;
     const TV* v = A.val<TV>();
+    // a matrix much larger than a quarter of L2 streams from HBM in the cycle: tune it cold
+    const bool cold = (double)A.nnz * (4 + sizeof(TV)) > (double)(32 << 20);
     float best = 1e30f;
     int pick = A.lanes;
     const int cand[5] = {2, 4, 8, 16, 32};
@@ -612,14 +733,7 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, cudaStream_t s, cudaEvent_t 
             }
         };
         launch();
-        SSV_CUDA(cudaEventRecord(e0, s));
-        const int reps = 4;
-        for (int k = 0; k < reps; ++k) launch();
-        SSV_CUDA(cudaEventRecord(e1, s));
-        SSV_CUDA(cudaEventSynchronize(e1));
-        SSV_LAUNCH_CHECK();
-        float ms = 0.f;
-        SSV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        const float ms = time_launches(launch, cold ? 3 : 4, cold, s, e0, e1);
         if (ms < best) {
             best = ms;
             pick = L;
@@ -938,7 +1052,7 @@ static double vcycle_bytes(const std::vector<AmgDevLevel>& L, int l, int NV, int
 }
 
 template <typename T, int NV, bool RECIP>
-static void ams_profile_t(AmsState& a, int reps, ssv_phase_profile* out) {
+static void ams_profile_t(AmsState& a, int reps, bool cold, ssv_phase_profile* out) {
     cudaStream_t s = stream();
     const int n = a.nhc, n1 = a.nh1;
     const int tb = (int)sizeof(T);
@@ -954,13 +1068,7 @@ static void ams_profile_t(AmsState& a, int reps, ssv_phase_profile* out) {
     std::memset(out, 0, sizeof(*out));
     auto timed = [&](const char* name, double bytes, int kernels, auto&& launch) {
         for (int k = 0; k < 2; ++k) launch();
-        SSV_CUDA(cudaEventRecord(e0, s));
-        for (int k = 0; k < reps; ++k) launch();
-        SSV_CUDA(cudaEventRecord(e1, s));
-        SSV_CUDA(cudaEventSynchronize(e1));
-        SSV_LAUNCH_CHECK();
-        float ms = 0.f;
-        SSV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        const float ms = time_launches(launch, reps, cold, s, e0, e1);
         const int i = out->num_phases++;
         std::snprintf(out->names[i], sizeof(out->names[i]), "%s", name);
         out->ms[i] = (double)ms / reps;
@@ -1008,21 +1116,22 @@ static void ams_profile_t(AmsState& a, int reps, ssv_phase_profile* out) {
 }
 
 template <typename T>
-static void ams_profile_nrhs(AmsState& a, int nrhs, int reps, ssv_phase_profile* out) {
+static void ams_profile_nrhs(AmsState& a, int nrhs, int reps, bool cold, ssv_phase_profile* out) {
     if (a.complex_form) {
-        if (nrhs == 1) ams_profile_t<T, 2, true>(a, reps, out);
-        else ams_profile_t<T, 8, true>(a, reps, out);
+        if (nrhs == 1) ams_profile_t<T, 2, true>(a, reps, cold, out);
+        else ams_profile_t<T, 8, true>(a, reps, cold, out);
     } else {
-        if (nrhs == 1) ams_profile_t<T, 1, false>(a, reps, out);
-        else ams_profile_t<T, 4, false>(a, reps, out);
+        if (nrhs == 1) ams_profile_t<T, 1, false>(a, reps, cold, out);
+        else ams_profile_t<T, 4, false>(a, reps, cold, out);
     }
 }
 
-void ams_profile(AmsState* a, int nrhs, int reps, ssv_phase_profile* out) {
+void ams_profile(AmsState* a, int nrhs, int reps, int flags, ssv_phase_profile* out) {
     if (nrhs != 1 && nrhs != 4) fail(SSV_ERR_INVALID_ARG, "ssv_ams_profile: nrhs must be 1 or 4");
     ams_reserve(*a, nrhs * (a->complex_form ? 2 : 1));
-    if (a->fp32) ams_profile_nrhs<float>(*a, nrhs, std::max(reps, 1), out);
-    else ams_profile_nrhs<double>(*a, nrhs, std::max(reps, 1), out);
+    const bool cold = (flags & SSV_PROFILE_COLD) != 0;
+    if (a->fp32) ams_profile_nrhs<float>(*a, nrhs, std::max(reps, 1), cold, out);
+    else ams_profile_nrhs<double>(*a, nrhs, std::max(reps, 1), cold, out);
 }
 
 // y = M^{-1} x for the preconditioner p, stream-ordered and capturable.

@@ -369,10 +369,10 @@ int ssv_ams_set_precision(ssv_precond* p, int32_t precision) {
     });
 }
 
-int ssv_ams_profile(ssv_precond* p, int32_t nrhs, int32_t reps, ssv_phase_profile* out) {
+int ssv_ams_profile(ssv_precond* p, int32_t nrhs, int32_t reps, int32_t flags, ssv_phase_profile* out) {
     return guarded([&] {
         if (!p || !p->ams || !out) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_profile: bad argument");
-        ssv::ams_profile(p->ams.get(), nrhs, reps, out);
+        ssv::ams_profile(p->ams.get(), nrhs, reps, flags, out);
     });
 }
 

@@ -45,7 +45,7 @@ int ams_precision(const AmsState* a);
 // Block application to nrhs right-hand sides ([row][rhs] interleaved; complex
 // form: Re/Im pairs), after ams_reserve_block(a, nrhs).
 void ams_reserve_block(AmsState* a, int nrhs);
-void ams_profile(AmsState* a, int nrhs, int reps, ssv_phase_profile* out);
+void ams_profile(AmsState* a, int nrhs, int reps, int flags, ssv_phase_profile* out);
 void ams_apply_block(AmsState* a, const double* in, double* out, int nrhs, const KState* st, cudaStream_t s);
 
 // Batched COCR over a frequency family (batch.cu)

@@ -561,10 +561,12 @@ class _AmsBase(_PrecondBase):
             raise ValueError("precision must be 'fp64' or 'fp32'")
         check(self._lib.ssv_ams_set_precision(self._h, _capi.SSV_PREC_FP32 if v == "fp32" else _capi.SSV_PREC_FP64))
 
-    def profile(self, nrhs=1, reps=20):
-        """Per-phase device time (ms) and algorithmic bytes of one cycle (measurement hook)."""
+    def profile(self, nrhs=1, reps=20, cold=False):
+        """Per-phase device time (ms) and algorithmic bytes of one cycle (measurement hook);
+        cold=True times each launch alone after evicting the L2."""
         prof = _capi.ssv_phase_profile()
-        check(self._lib.ssv_ams_profile(self._h, int(nrhs), int(reps), ctypes.byref(prof)))
+        check(self._lib.ssv_ams_profile(self._h, int(nrhs), int(reps), _capi.SSV_PROFILE_COLD if cold else 0,
+                                        ctypes.byref(prof)))
         return prof.as_list()
 
     def levels(self, subspace):

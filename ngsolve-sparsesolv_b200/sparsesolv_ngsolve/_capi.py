@@ -29,6 +29,8 @@ SSV_C128 = 1
 SSV_PREC_FP64 = 0
 SSV_PREC_FP32 = 1
 
+SSV_PROFILE_COLD = 1
+
 
 class ssv_config(ctypes.Structure):
     """Mirror of sparsesolv::SolverConfig (core/solver_config.hpp:33-159)."""
@@ -197,7 +199,7 @@ SIGNATURES = [
     ("ssv_batch_set_replacement", I32, [P, I32]),
     ("ssv_batch_last_timing", I32, [P, PD, PD, PI32, ctypes.POINTER(ctypes.c_int64)]),
     ("ssv_ams_get_precision", I32, [P, PI32]),
-    ("ssv_ams_profile", I32, [P, I32, I32, ctypes.POINTER(ssv_phase_profile)]),
+    ("ssv_ams_profile", I32, [P, I32, I32, I32, ctypes.POINTER(ssv_phase_profile)]),
     ("ssv_mlp_create", I32, [I32, I32, ctypes.c_uint64, PP]),
     ("ssv_mlp_destroy", I32, [P]),
     ("ssv_mlp_num_params", I32, [P, PI32]),

@@ -102,21 +102,6 @@ def test_batch_residual_replacement(fam_well):
             assert _true_res(d, f, X[f, r], d["B"][f, r]) <= 1e-9
 
 
-def test_batch_fp32_matches_single_fp32(fam_well):
-    # the batch machinery with FP32-form preconditioners reproduces the single
-    # COCR with the same preconditioners (15 steps, replacement off)
-    import sparsesolv_ngsolve as ss
-    d = fam_well
-    pres = _pres(d, "fp32")
-    bs = ss.BatchedCOCRSolver(d["K"], d["M"], d["omegas"], pres, nrhs=4, freedofs=d["freedofs"], maxiter=15,
-                              tol=1e-10, residual_replacement=0)
-    X = bs.Solve(d["B"])
-    for f in range(len(d["omegas"])):
-        xs, its = _single(d, pres, f, 1, 1e-10, maxiter=15)
-        assert int(bs.iterations[f, 1]) == its
-        assert np.linalg.norm(X[f, 1] - xs) <= 1e-6 * np.linalg.norm(xs)
-
-
 def test_batch_without_preconditioner(fam_well):
     import sparsesolv_ngsolve as ss
     d = fam_well
