@@ -22,9 +22,12 @@
 // has no gradient-space content left and the gradient correction diverges.
 // Kernels that cross between the two accumulate in FP64. The cycle's input
 // and output are FP64 in both forms.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 
@@ -38,6 +41,16 @@ namespace ssv {
 // Multi-vector kernels
 // ---------------------------------------------------------------------------
 enum MvMode : int { MV_AX = 0, MV_RES = 1, MV_ADD = 2, MV_JAC = 3 };
+
+// Programmatic dependent launch: the cycle's kernels are launched so that the
+// next one in the stream may be scheduled before this one ends. Each waits
+// here for its predecessor's completion and memory (griddepcontrol.wait)
+// before touching any data, then lets its own successor start launching.
+// Launched without the attribute, both instructions have no effect.
+__device__ __forceinline__ void pdl_gate() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 // One row of NV columns in the widest aligned accesses the row allows (work
 // vectors come from cudaMalloc, so row r starts at r * NV * sizeof(T)).
@@ -90,6 +103,7 @@ k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T
           const TX* __restrict__ x, TY* __restrict__ y, const TY* __restrict__ b, const TY* __restrict__ d, TY w,
           const KState* st) {
     using TA = wider_t<TV, TX>;
+    pdl_gate();
     if (st && st->done) return;
     const int sub = threadIdx.x % LANES;
     const int rpb = kBlock / LANES;
@@ -141,6 +155,7 @@ __global__ void __launch_bounds__(kBlock)
 k_mv_pi_restrict(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ px,
                  const double* __restrict__ py, const double* __restrict__ pz, const double* __restrict__ r,
                  TO* __restrict__ ox, TO* __restrict__ oy, TO* __restrict__ oz, const KState* st) {
+    pdl_gate();
     if (st && st->done) return;
     const int sub = threadIdx.x % LANES;
     const int rpb = kBlock / LANES;
@@ -189,6 +204,7 @@ k_mv_pi_prolong(int n, const int* __restrict__ rp, const int* __restrict__ ci, c
                 const double* __restrict__ py, const double* __restrict__ pz, const TG* __restrict__ gx,
                 const TG* __restrict__ gy, const TG* __restrict__ gz, double* __restrict__ x, double w,
                 const KState* st) {
+    pdl_gate();
     if (st && st->done) return;
     const int sub = threadIdx.x % LANES;
     const int rpb = kBlock / LANES;
@@ -237,6 +253,7 @@ k_mv_pi_prolong(int n, const int* __restrict__ rp, const int* __restrict__ ci, c
 template <typename T, int NV, bool RECIP>
 __global__ void k_mv_first_sweep(int n, const T* __restrict__ b, const T* __restrict__ d, T* __restrict__ x,
                                  const KState* st) {
+    pdl_gate();
     if (st && st->done) return;
     const int64_t total = (int64_t)n * NV;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
@@ -253,6 +270,7 @@ __global__ void __launch_bounds__(kBlock)
 k_mv_first_res(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ v,
                const T* __restrict__ b, const T* __restrict__ d, T* __restrict__ x, T* __restrict__ r,
                const KState* st) {
+    pdl_gate();
     if (st && st->done) return;
     const int sub = threadIdx.x % LANES;
     const int rpb = kBlock / LANES;
@@ -296,6 +314,7 @@ k_mv_first_res(int n, const int* __restrict__ rp, const int* __restrict__ ci, co
 template <typename TI, typename TO, int NV>
 __global__ void k_mv_mask_copy(int n, const TI* __restrict__ in, const uint8_t* __restrict__ fd,
                                TO* __restrict__ out, const KState* st) {
+    pdl_gate();
     if (st && st->done) return;
     const int64_t total = (int64_t)n * NV;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
@@ -312,6 +331,7 @@ template <typename T, int NV>
 __global__ void __launch_bounds__(kBlock)
 k_mv_coarse_fwd(int n, const double* __restrict__ Li, const double* __restrict__ piv, const T* __restrict__ b,
                 double* __restrict__ z, const KState* st) {
+    pdl_gate();
     if (st && st->done) return;
     const int lane = threadIdx.x & 31;
     for (int row = blockIdx.x * (kBlock / 32) + threadIdx.x / 32; row < n; row += gridDim.x * (kBlock / 32)) {
@@ -341,6 +361,7 @@ template <typename T, int NV>
 __global__ void __launch_bounds__(kBlock)
 k_mv_coarse_bwd(int n, const double* __restrict__ LiT, const double* __restrict__ z, T* __restrict__ x,
                 const KState* st) {
+    pdl_gate();
     if (st && st->done) return;
     const int lane = threadIdx.x & 31;
     for (int row = blockIdx.x * (kBlock / 32) + threadIdx.x / 32; row < n; row += gridDim.x * (kBlock / 32)) {
@@ -360,6 +381,226 @@ k_mv_coarse_bwd(int n, const double* __restrict__ LiT, const double* __restrict_
         if (lane == 0)
 #pragma unroll
             for (int c = 0; c < NV; ++c) x[(size_t)row * NV + c] = (T)acc[c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle tail on one thread-block cluster: every level from the first small
+// one down to the coarsest solve and back up, in one launch. The cluster's 8
+// CTAs split each step's rows and meet at cluster barriers, which replace the
+// kernel boundaries of the per-level launch chain (latency-bound on small
+// levels). The arithmetic per level is the chain's (num_smooth = 1): fused
+// first sweep + residual, restriction, coarsest LDL^T solve (FP64) or 10
+// l1-Jacobi sweeps, prolongation, post sweep.
+// ---------------------------------------------------------------------------
+constexpr int kTailCluster = 8;
+constexpr int kTailBlock = 512;
+constexpr int kTailLanes = 4;
+
+// One level as the tail kernel sees it (values and vectors in the hierarchy type).
+struct TailLevel {
+    int n, direct;
+    const int *Arp, *Aci;
+    const void* Av;
+    const int *Prp, *Pci;
+    const void* Pv;  // n x n_next (not at the coarsest level)
+    const int *Trp, *Tci;
+    const void* Tv;  // P^T
+    const void *l1, *il1;
+    void *b, *x, *xalt, *r;
+    const double *Li, *LiT, *piv;
+    double* cz;
+};
+
+// rows of a CSR pass split over the cluster, kTailLanes threads per row;
+// acc = sum_k a_k * xval(col_k), then out(row, acc)
+template <typename T, int NV, typename FX, typename FO>
+__device__ __forceinline__ void tail_rows(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                          const T* __restrict__ v, FX xval, FO out) {
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int G = gridDim.x * blockDim.x / kTailLanes;
+    const int sub = threadIdx.x % kTailLanes;
+    const int lane_row = (threadIdx.x & 31) / kTailLanes;  // warp-uniform trip count
+    for (int row = gt / kTailLanes; row - lane_row < n; row += G) {
+        const bool valid = row < n;
+        T acc[NV];
+#pragma unroll
+        for (int c = 0; c < NV; ++c) acc[c] = T(0);
+        if (valid)
+            for (int k = rp[row] + sub; k < rp[row + 1]; k += kTailLanes) {
+                const T a = v[k];
+                T xj[NV];
+                xval(ci[k], xj);
+#pragma unroll
+                for (int c = 0; c < NV; ++c) acc[c] += a * xj[c];
+            }
+#pragma unroll
+        for (int o = kTailLanes / 2; o > 0; o >>= 1)
+#pragma unroll
+            for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o, kTailLanes);
+        if (valid && sub == 0) out(row, acc);
+    }
+}
+
+template <typename T, int NV, bool RECIP>
+__global__ void __cluster_dims__(kTailCluster, 1, 1) __launch_bounds__(kTailBlock)
+k_vcycle_tail(const TailLevel* __restrict__ lv, int l0, int L, const T* __restrict__ b0, const KState* st) {
+    if (st && st->done) return;  // uniform: the state does not change while this runs
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    auto sync = [&]() {
+        __threadfence();
+        cl.sync();
+    };
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int gw = gt >> 5, GW = (gridDim.x * blockDim.x) >> 5;
+    auto dv = [&](int l) { return (const T*)(RECIP ? lv[l].il1 : lv[l].l1); };
+    auto rhs = [&](int l) { return l == l0 ? b0 : (const T*)lv[l].b; };
+    auto upd = [&](T xo, T r, T d) { return RECIP ? xo + r * d : xo + r / d; };
+    // down: fused first sweep + residual, then restriction
+    for (int l = l0; l < L - 1; ++l) {
+        const TailLevel& Lv = lv[l];
+        const T* b = rhs(l);
+        const T* d = dv(l);
+        T* x = (T*)Lv.x;
+        T* r = (T*)Lv.r;
+        tail_rows<T, NV>(Lv.n, Lv.Arp, Lv.Aci, (const T*)Lv.Av,
+                         [&](int j, T (&o)[NV]) {
+                             const T dj = d[j];
+#pragma unroll
+                             for (int c = 0; c < NV; ++c) o[c] = RECIP ? b[(size_t)j * NV + c] * dj : b[(size_t)j * NV + c] / dj;
+                         },
+                         [&](int row, T (&acc)[NV]) {
+                             const T di = d[row];
+#pragma unroll
+                             for (int c = 0; c < NV; ++c) {
+                                 const T bi = b[(size_t)row * NV + c];
+                                 x[(size_t)row * NV + c] = RECIP ? bi * di : bi / di;
+                                 r[(size_t)row * NV + c] = bi - acc[c];
+                             }
+                         });
+        sync();
+        T* bn = (T*)lv[l + 1].b;
+        tail_rows<T, NV>(lv[l + 1].n, Lv.Trp, Lv.Tci, (const T*)Lv.Tv,
+                         [&](int j, T (&o)[NV]) {
+#pragma unroll
+                             for (int c = 0; c < NV; ++c) o[c] = r[(size_t)j * NV + c];
+                         },
+                         [&](int row, T (&acc)[NV]) {
+#pragma unroll
+                             for (int c = 0; c < NV; ++c) bn[(size_t)row * NV + c] = acc[c];
+                         });
+        sync();
+    }
+    // coarsest
+    const TailLevel& C = lv[L - 1];
+    const T* bc = rhs(L - 1);
+    const T* res;
+    if (C.direct) {
+        const int n = C.n;
+        for (int row = gw; row < n; row += GW) {  // z = (L^{-1} b) / d, warp per row
+            double acc[NV];
+#pragma unroll
+            for (int c = 0; c < NV; ++c) acc[c] = 0.0;
+            const double* lr = C.Li + (size_t)row * n;
+            for (int k = lane; k <= row; k += 32) {
+                const double a = lr[k];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) acc[c] += a * (double)bc[(size_t)k * NV + c];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
+            if (lane == 0) {
+                const double dd = C.piv[row];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) C.cz[(size_t)row * NV + c] = dd != 0.0 ? acc[c] / dd : 0.0;
+            }
+        }
+        sync();
+        T* x = (T*)C.x;
+        for (int row = gw; row < n; row += GW) {  // x = L^{-T} z
+            double acc[NV];
+#pragma unroll
+            for (int c = 0; c < NV; ++c) acc[c] = 0.0;
+            const double* lr = C.LiT + (size_t)row * n;
+            for (int k = row + lane; k < n; k += 32) {
+                const double a = lr[k];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) acc[c] += a * C.cz[(size_t)k * NV + c];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
+            if (lane == 0)
+#pragma unroll
+                for (int c = 0; c < NV; ++c) x[(size_t)row * NV + c] = (T)acc[c];
+        }
+        sync();
+        res = x;
+    } else {  // 10 l1-Jacobi sweeps from x = 0
+        const T* d = dv(L - 1);
+        T* cur = (T*)C.x;
+        T* alt = (T*)C.xalt;
+        for (int q = gt; q < C.n * NV; q += gridDim.x * blockDim.x) {
+            const int i = q / NV;
+            cur[q] = RECIP ? bc[q] * d[i] : bc[q] / d[i];
+        }
+        sync();
+        for (int k = 0; k < 9; ++k) {
+            tail_rows<T, NV>(C.n, C.Arp, C.Aci, (const T*)C.Av,
+                             [&](int j, T (&o)[NV]) {
+#pragma unroll
+                                 for (int c = 0; c < NV; ++c) o[c] = cur[(size_t)j * NV + c];
+                             },
+                             [&](int row, T (&acc)[NV]) {
+#pragma unroll
+                                 for (int c = 0; c < NV; ++c) {
+                                     const size_t q = (size_t)row * NV + c;
+                                     alt[q] = upd(cur[q], bc[q] - acc[c], d[row]);
+                                 }
+                             });
+            sync();
+            T* t = cur;
+            cur = alt;
+            alt = t;
+        }
+        res = cur;
+    }
+    // up: prolongation, then the post sweep into the level's second buffer
+    for (int l = L - 2; l >= l0; --l) {
+        const TailLevel& Lv = lv[l];
+        const T* b = rhs(l);
+        const T* d = dv(l);
+        T* x = (T*)Lv.x;
+        T* xa = (T*)Lv.xalt;
+        const T* e = res;
+        tail_rows<T, NV>(Lv.n, Lv.Prp, Lv.Pci, (const T*)Lv.Pv,
+                         [&](int j, T (&o)[NV]) {
+#pragma unroll
+                             for (int c = 0; c < NV; ++c) o[c] = e[(size_t)j * NV + c];
+                         },
+                         [&](int row, T (&acc)[NV]) {
+#pragma unroll
+                             for (int c = 0; c < NV; ++c) x[(size_t)row * NV + c] += T(1) * acc[c];
+                         });
+        sync();
+        tail_rows<T, NV>(Lv.n, Lv.Arp, Lv.Aci, (const T*)Lv.Av,
+                         [&](int j, T (&o)[NV]) {
+#pragma unroll
+                             for (int c = 0; c < NV; ++c) o[c] = x[(size_t)j * NV + c];
+                         },
+                         [&](int row, T (&acc)[NV]) {
+#pragma unroll
+                             for (int c = 0; c < NV; ++c) {
+                                 const size_t q = (size_t)row * NV + c;
+                                 xa[q] = upd(x[q], b[q] - acc[c], d[row]);
+                             }
+                         });
+        sync();
+        res = xa;
     }
 }
 
@@ -426,6 +667,13 @@ struct AmgDevLevel {
     WorkVec b, xa, xb, r;  // NV-column work vectors of this level
 };
 
+// Levels of one hierarchy run by the cluster tail kernel (start = first such
+// level, -1 = none) and their descriptors on the device.
+struct TailSet {
+    int start = -1;
+    DevBuf<TailLevel> desc;
+};
+
 struct AmsState {
     int nhc = 0, nh1 = 0, cycle_type = 1, num_smooth = 1, nv_alloc = 0;
     double w = 1.0;
@@ -443,9 +691,35 @@ struct AmsState {
     std::vector<uint8_t> h_fd;
     unsigned gen = 0;
     ForkSet forks;  // the y and z nodal V-cycles run beside the x one
+    TailSet tails[4];
 };
 
 void ams_free(AmsState* a) { delete a; }
+
+// SSV_PDL=0 launches the cycle's kernels without programmatic dependence.
+static bool pdl_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("SSV_PDL");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v != 0;
+}
+
+template <typename... KArgs, typename... Args>
+static void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    SSV_CUDA(cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...));
+}
 
 template <typename TV, typename TX, typename TY, int NV, int MODE, bool RECIP>
 static void mv_spmv(const DevCsr& A, const TX* x, TY* y, const TY* b, const TY* d, TY w, const KState* st,
@@ -456,7 +730,7 @@ static void mv_spmv(const DevCsr& A, const TX* x, TY* y, const TY* b, const TY* 
     const TV* v = A.val<TV>();
 #define SSV_MV_CASE(L)                                                                                   \
     case L:                                                                                              \
-        k_mv_spmv<TV, TX, TY, NV, L, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, \
+        launch_k(k_mv_spmv<TV, TX, TY, NV, L, MODE, RECIP>, grid, kBlock, s, A.n, A.rp.get(), A.ci.get(), v, x, \
                                                                            y, b, d, w, st);              \
         break;
     switch (lanes) {
@@ -465,7 +739,7 @@ static void mv_spmv(const DevCsr& A, const TX* x, TY* y, const TY* b, const TY* 
         SSV_MV_CASE(8)
         SSV_MV_CASE(16)
         default:
-            k_mv_spmv<TV, TX, TY, NV, 32, MODE, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x,
+            launch_k(k_mv_spmv<TV, TX, TY, NV, 32, MODE, RECIP>, grid, kBlock, s, A.n, A.rp.get(), A.ci.get(), v, x,
                                                                                 y, b, d, w, st);
     }
 #undef SSV_MV_CASE
@@ -473,7 +747,7 @@ static void mv_spmv(const DevCsr& A, const TX* x, TY* y, const TY* b, const TY* 
 
 template <typename T, int NV, bool RECIP>
 static void first_sweep(int n, const T* b, const T* d, T* x, const KState* st, cudaStream_t s) {
-    k_mv_first_sweep<T, NV, RECIP><<<grid_for((int64_t)n * NV, kBlock), kBlock, 0, s>>>(n, b, d, x, st);
+    launch_k(k_mv_first_sweep<T, NV, RECIP>, grid_for((int64_t)n * NV, kBlock), kBlock, s, n, b, d, x, st);
 }
 
 template <typename T, int NV, bool RECIP>
@@ -483,11 +757,11 @@ static void first_res(const DevCsr& A, const T* b, const T* d, T* x, T* r, const
     const int grid = std::max(1, std::min((A.n + rpb - 1) / rpb, sm_count() * 8));
     const T* v = A.val<T>();
     switch (lanes) {
-        case 2: k_mv_first_res<T, NV, 2, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
-        case 4: k_mv_first_res<T, NV, 4, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
-        case 8: k_mv_first_res<T, NV, 8, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
-        case 16: k_mv_first_res<T, NV, 16, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
-        default: k_mv_first_res<T, NV, 32, RECIP><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
+        case 2: launch_k(k_mv_first_res<T, NV, 2, RECIP>, grid, kBlock, s, A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
+        case 4: launch_k(k_mv_first_res<T, NV, 4, RECIP>, grid, kBlock, s, A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
+        case 8: launch_k(k_mv_first_res<T, NV, 8, RECIP>, grid, kBlock, s, A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
+        case 16: launch_k(k_mv_first_res<T, NV, 16, RECIP>, grid, kBlock, s, A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
+        default: launch_k(k_mv_first_res<T, NV, 32, RECIP>, grid, kBlock, s, A.n, A.rp.get(), A.ci.get(), v, b, d, x, r, st); break;
     }
 }
 
@@ -499,8 +773,13 @@ static const T* l1_of(const AmgDevLevel& lv) {
 // One AMG V-cycle (VCycle / DualVCycle, compact_amg.hpp:662-706,801-841) on
 // level l: b -> x (x starts at zero). Returns the buffer holding x.
 template <typename T, int NV, bool RECIP>
-static T* vcycle(std::vector<AmgDevLevel>& L, int l, const T* b, int num_smooth, const KState* st, cudaStream_t s) {
+static T* vcycle(std::vector<AmgDevLevel>& L, const TailSet& tail, int l, const T* b, int num_smooth,
+                 const KState* st, cudaStream_t s) {
     AmgDevLevel& lv = L[l];
+    if (num_smooth == 1 && tail.start >= 0 && l == tail.start) {
+        k_vcycle_tail<T, NV, RECIP><<<kTailCluster, kTailBlock, 0, s>>>(tail.desc.get(), l, (int)L.size(), b, st);
+        return lv.xb.as<T>();  // the post sweep's buffer (the tail spans at least two levels)
+    }
     const T* d = l1_of<T, RECIP>(lv);
     T* cur = lv.xa.as<T>();
     T* alt = lv.xb.as<T>();
@@ -513,8 +792,8 @@ static T* vcycle(std::vector<AmgDevLevel>& L, int l, const T* b, int num_smooth,
     if (l == (int)L.size() - 1) {
         if (lv.direct) {
             const int g = std::max(1, std::min((lv.A.n + 7) / 8, sm_count() * 4));
-            k_mv_coarse_fwd<T, NV><<<g, kBlock, 0, s>>>(lv.A.n, lv.Li.get(), lv.piv.get(), b, lv.cz.get(), st);
-            k_mv_coarse_bwd<T, NV><<<g, kBlock, 0, s>>>(lv.A.n, lv.LiT.get(), lv.cz.get(), cur, st);
+            launch_k(k_mv_coarse_fwd<T, NV>, g, kBlock, s, lv.A.n, lv.Li.get(), lv.piv.get(), b, lv.cz.get(), st);
+            launch_k(k_mv_coarse_bwd<T, NV>, g, kBlock, s, lv.A.n, lv.LiT.get(), lv.cz.get(), cur, st);
         } else {  // 10 l1-Jacobi sweeps from x = 0
             first_sweep<T, NV, RECIP>(lv.A.n, b, d, cur, st, s);
             sweep(9);
@@ -532,7 +811,7 @@ static T* vcycle(std::vector<AmgDevLevel>& L, int l, const T* b, int num_smooth,
     }
     AmgDevLevel& nx = L[l + 1];
     mv_spmv<T, T, T, NV, MV_AX, RECIP>(lv.Pt, lv.r.as<T>(), nx.b.as<T>(), nullptr, nullptr, T(0), st, s);
-    T* ec = vcycle<T, NV, RECIP>(L, l + 1, nx.b.as<T>(), num_smooth, st, s);
+    T* ec = vcycle<T, NV, RECIP>(L, tail, l + 1, nx.b.as<T>(), num_smooth, st, s);
     mv_spmv<T, T, T, NV, MV_ADD, RECIP>(lv.P, ec, cur, nullptr, nullptr, T(1), st, s);
     sweep(num_smooth);
     return cur;
@@ -543,7 +822,7 @@ static void pi_restrict_l(const AmsState& a, const double* r, T* ox, T* oy, T* o
                           cudaStream_t s) {
     const int rpb = kBlock / LANES;
     const int grid = std::max(1, std::min((a.Gt.n + rpb - 1) / rpb, sm_count() * 8));
-    k_mv_pi_restrict<T, NV, LANES><<<grid, kBlock, 0, s>>>(a.Gt.n, a.Gt.rp.get(), a.Gt.ci.get(), a.Pitv[0].get(),
+    launch_k(k_mv_pi_restrict<T, NV, LANES>, grid, kBlock, s, a.Gt.n, a.Gt.rp.get(), a.Gt.ci.get(), a.Pitv[0].get(),
                                                            a.Pitv[1].get(), a.Pitv[2].get(), r, ox, oy, oz, st);
 }
 
@@ -552,7 +831,7 @@ static void pi_prolong_l(const AmsState& a, const T* gx, const T* gy, const T* g
                          cudaStream_t s) {
     const int rpb = kBlock / LANES;
     const int grid = std::max(1, std::min((a.G.n + rpb - 1) / rpb, sm_count() * 8));
-    k_mv_pi_prolong<T, NV, LANES><<<grid, kBlock, 0, s>>>(a.G.n, a.G.rp.get(), a.G.ci.get(), a.Piv[0].get(),
+    launch_k(k_mv_pi_prolong<T, NV, LANES>, grid, kBlock, s, a.G.n, a.G.rp.get(), a.G.ci.get(), a.Piv[0].get(),
                                                           a.Piv[1].get(), a.Piv[2].get(), gx, gy, gz, x, a.w, st);
 }
 
@@ -593,7 +872,7 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
     double* alt = a.xb.get();
     double* r = a.r.get();
     const int gm = grid_for((int64_t)n * NV, kBlock);
-    k_mv_mask_copy<double, double, NV><<<gm, kBlock, 0, s>>>(n, in, fd, b0, st);
+    launch_k(k_mv_mask_copy<double, double, NV>, gm, kBlock, s, n, in, fd, b0, st);
     // (the fused first sweep + residual is not used on the fine level: with
     // 7.4M nonzeros its second gather, of l1, costs more than the separate
     // elementwise sweep saves)
@@ -632,7 +911,7 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
     auto gradient = [&]() {
         residual();
         mv_spmv<double, double, T, NV, MV_AX, RECIP>(a.Gt, r, a.rs[0].as<T>(), nullptr, nullptr, T(0), st, s);
-        T* g = vcycle<T, NV, RECIP>(a.amg[0], 0, a.rs[0].as<T>(), 1, st, s);
+        T* g = vcycle<T, NV, RECIP>(a.amg[0], a.tails[0], 0, a.rs[0].as<T>(), 1, st, s);
         mv_spmv<double, T, double, NV, MV_ADD, RECIP>(a.G, g, cur, nullptr, nullptr, a.w, st, s);
     };
     auto nodal = [&]() {
@@ -640,9 +919,9 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
         pi_restrict<T, NV>(a, r, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), st, s);
         // the three V-cycles are independent (own hierarchies and vectors)
         a.forks.fork(s, 2);
-        T* gx = vcycle<T, NV, RECIP>(a.amg[1], 0, a.rs[1].as<T>(), 1, st, s);
-        T* gy = vcycle<T, NV, RECIP>(a.amg[2], 0, a.rs[2].as<T>(), 1, st, a.forks.side[0]);
-        T* gz = vcycle<T, NV, RECIP>(a.amg[3], 0, a.rs[3].as<T>(), 1, st, a.forks.side[1]);
+        T* gx = vcycle<T, NV, RECIP>(a.amg[1], a.tails[1], 0, a.rs[1].as<T>(), 1, st, s);
+        T* gy = vcycle<T, NV, RECIP>(a.amg[2], a.tails[2], 0, a.rs[2].as<T>(), 1, st, a.forks.side[0]);
+        T* gz = vcycle<T, NV, RECIP>(a.amg[3], a.tails[3], 0, a.rs[3].as<T>(), 1, st, a.forks.side[1]);
         a.forks.join(s, 2);
         pi_prolong<T, NV>(a, gx, gy, gz, cur, st, s);
     };
@@ -652,7 +931,7 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
         fine_smooth(); gradient(); nodal(); gradient(); fine_smooth();
     }
     ensure_x();
-    k_mv_mask_copy<double, double, NV><<<gm, kBlock, 0, s>>>(n, cur, fd, out, st);
+    launch_k(k_mv_mask_copy<double, double, NV>, gm, kBlock, s, n, cur, fd, out, st);
     SSV_LAUNCH_CHECK();
 }
 
@@ -781,6 +1060,66 @@ static void tune_lanes(AmsState& a) {
     cudaEventDestroy(e1);
 }
 
+// Which levels the cluster tail runs: the suffix of levels with at most 8192
+// rows and at most SSV_AMS_TAIL_NNZ nonzeros, when it spans at least two
+// levels. Off by default (0): on the 40^3 benchmark hierarchies it measured no
+// faster than the per-level launches (8 SMs stream the larger tail levels no
+// faster than the launch latency it saves). Descriptors are rebuilt whenever
+// the work vectors are.
+static void build_tails(AmsState& a) {
+    const char* env = std::getenv("SSV_AMS_TAIL_NNZ");
+    const long lim = env ? std::atol(env) : 0L;
+    for (int sub = 0; sub < 4; ++sub) {
+        auto& L = a.amg[sub];
+        TailSet& t = a.tails[sub];
+        t.start = -1;
+        if (lim <= 0 || a.num_smooth != 1) continue;
+        for (int l = (int)L.size() - 1; l >= 0; --l) {
+            if (L[l].A.n <= 8192 && L[l].A.nnz <= lim) t.start = l;
+            else break;
+        }
+        if (t.start >= 0 && (int)L.size() - t.start < 2) t.start = -1;
+        if (t.start < 0) continue;
+        std::vector<TailLevel> h(L.size());
+        std::memset(h.data(), 0, sizeof(TailLevel) * h.size());
+        auto vals = [&](const DevCsr& M) -> const void* {
+            return a.fp32 ? (const void*)M.val<float>() : (const void*)M.val<double>();
+        };
+        auto dual = [&](const DualVec& v) -> const void* {
+            return a.fp32 ? (const void*)v.get<float>() : (const void*)v.get<double>();
+        };
+        for (size_t l = t.start; l < L.size(); ++l) {
+            AmgDevLevel& lv = L[l];
+            TailLevel& d = h[l];
+            d.n = lv.A.n;
+            d.direct = lv.direct ? 1 : 0;
+            d.Arp = lv.A.rp.get();
+            d.Aci = lv.A.ci.get();
+            d.Av = vals(lv.A);
+            if (l + 1 < L.size()) {
+                d.Prp = lv.P.rp.get();
+                d.Pci = lv.P.ci.get();
+                d.Pv = vals(lv.P);
+                d.Trp = lv.Pt.rp.get();
+                d.Tci = lv.Pt.ci.get();
+                d.Tv = vals(lv.Pt);
+            }
+            d.l1 = dual(lv.l1);
+            d.il1 = dual(lv.il1);
+            d.b = lv.b.raw.get();
+            d.x = lv.xa.raw.get();
+            d.xalt = lv.xb.raw.get();
+            d.r = lv.r.raw.get();
+            d.Li = lv.Li.get();
+            d.LiT = lv.LiT.get();
+            d.piv = lv.piv.get();
+            d.cz = lv.cz.get();
+        }
+        t.desc.upload(h.data(), h.size(), stream());
+    }
+    SSV_CUDA(cudaStreamSynchronize(stream()));
+}
+
 // Work vectors for blocks of up to nv real columns (allocation only, so the
 // cycle itself never allocates and can be captured).
 static void ams_reserve(AmsState& a, int nv) {
@@ -803,6 +1142,7 @@ static void ams_reserve(AmsState& a, int nv) {
     a.nv_alloc = nv;
     ++a.gen;  // new work buffers: graphs that captured the old ones must be rebuilt
     tune_lanes(a);
+    build_tails(a);
 }
 
 static std::vector<double> reciprocal(const std::vector<double>& v) {
@@ -1094,12 +1434,12 @@ static void ams_profile_t(AmsState& a, int reps, bool cold, ssv_phase_profile* o
     timed("fine_smooth", fine_jac, 1, [&] {
         mv_spmv<double, double, double, NV, MV_JAC, RECIP>(a.A_bc, cur, alt, a.b0.get(), d, 0.0, nullptr, s);
     });
-    timed("grad_vcycle", grad_vc, 0, [&] { vcycle<T, NV, RECIP>(a.amg[0], 0, a.rs[0].as<T>(), 1, nullptr, s); });
+    timed("grad_vcycle", grad_vc, 0, [&] { vcycle<T, NV, RECIP>(a.amg[0], a.tails[0], 0, a.rs[0].as<T>(), 1, nullptr, s); });
     timed("nodal_vcycles", nod_vc, 0, [&] {
         a.forks.fork(s, 2);
-        vcycle<T, NV, RECIP>(a.amg[1], 0, a.rs[1].as<T>(), 1, nullptr, s);
-        vcycle<T, NV, RECIP>(a.amg[2], 0, a.rs[2].as<T>(), 1, nullptr, a.forks.side[0]);
-        vcycle<T, NV, RECIP>(a.amg[3], 0, a.rs[3].as<T>(), 1, nullptr, a.forks.side[1]);
+        vcycle<T, NV, RECIP>(a.amg[1], a.tails[1], 0, a.rs[1].as<T>(), 1, nullptr, s);
+        vcycle<T, NV, RECIP>(a.amg[2], a.tails[2], 0, a.rs[2].as<T>(), 1, nullptr, a.forks.side[0]);
+        vcycle<T, NV, RECIP>(a.amg[3], a.tails[3], 0, a.rs[3].as<T>(), 1, nullptr, a.forks.side[1]);
         a.forks.join(s, 2);
     });
     timed("grad_transfers", g_tr, 2, [&] {
