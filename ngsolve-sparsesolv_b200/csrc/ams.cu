@@ -385,6 +385,186 @@ k_mv_coarse_bwd(int n, const double* __restrict__ LiT, const double* __restrict_
 }
 
 // ---------------------------------------------------------------------------
+// The three nodal V-cycles in lockstep: one launch carries the same step of
+// the x, y and z hierarchies (blockIdx.y picks the subspace), so the three
+// chains of small per-level launches become one chain with three times the
+// work per launch. Same arithmetic per subspace as the single-hierarchy
+// kernels above.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Tri {
+    int n[3];
+    const int* rp[3];
+    const int* ci[3];
+    const T* v[3];
+    const T* x[3];
+    T* y[3];
+    const T* b[3];
+    const T* d[3];
+    T* r[3];
+};
+
+template <typename T, int NV, int LANES, int MODE, bool RECIP>
+__global__ void __launch_bounds__(kBlock)
+k_mv3_spmv(Tri<T> t, T w, const KState* st) {
+    pdl_gate();
+    if (st && st->done) return;
+    const int q = blockIdx.y;
+    const int n = t.n[q];
+    const int* __restrict__ rp = t.rp[q];
+    const int* __restrict__ ci = t.ci[q];
+    const T* __restrict__ v = t.v[q];
+    const T* __restrict__ x = t.x[q];
+    T* __restrict__ y = t.y[q];
+    const T* __restrict__ b = t.b[q];
+    const T* __restrict__ d = t.d[q];
+    const int sub = threadIdx.x % LANES;
+    const int rpb = kBlock / LANES;
+    const int lane_row = (threadIdx.x & 31) / LANES;
+    for (int row = blockIdx.x * rpb + threadIdx.x / LANES; row - lane_row < n; row += gridDim.x * rpb) {
+        const bool valid = row < n;
+        T acc[NV];
+#pragma unroll
+        for (int c = 0; c < NV; ++c) acc[c] = T(0);
+        if (valid) {
+            const int k1 = rp[row + 1];
+            for (int k = rp[row] + sub; k < k1; k += LANES) {
+                const T a = v[k];
+                T xv[NV];
+                load_row<NV>(x + (size_t)ci[k] * NV, xv);
+#pragma unroll
+                for (int c = 0; c < NV; ++c) acc[c] += a * xv[c];
+            }
+        }
+#pragma unroll
+        for (int o = LANES / 2; o > 0; o >>= 1)
+#pragma unroll
+            for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o, LANES);
+        if (valid && sub == 0) {
+            const size_t base = (size_t)row * NV;
+#pragma unroll
+            for (int c = 0; c < NV; ++c) {
+                if constexpr (MODE == MV_AX) {
+                    y[base + c] = acc[c];
+                } else if constexpr (MODE == MV_ADD) {
+                    y[base + c] += w * acc[c];
+                } else {  // MV_JAC
+                    const T rr = b[base + c] - acc[c];
+                    const T xo = x[base + c];
+                    y[base + c] = RECIP ? xo + rr * d[row] : xo + rr / d[row];
+                }
+            }
+        }
+    }
+}
+
+template <typename T, int NV, int LANES, bool RECIP>
+__global__ void __launch_bounds__(kBlock)
+k_mv3_first_res(Tri<T> t, const KState* st) {
+    pdl_gate();
+    if (st && st->done) return;
+    const int q = blockIdx.y;
+    const int n = t.n[q];
+    const int* __restrict__ rp = t.rp[q];
+    const int* __restrict__ ci = t.ci[q];
+    const T* __restrict__ v = t.v[q];
+    const T* __restrict__ b = t.b[q];
+    const T* __restrict__ d = t.d[q];
+    T* __restrict__ x = t.y[q];
+    T* __restrict__ r = t.r[q];
+    const int sub = threadIdx.x % LANES;
+    const int rpb = kBlock / LANES;
+    const int lane_row = (threadIdx.x & 31) / LANES;
+    for (int row = blockIdx.x * rpb + threadIdx.x / LANES; row - lane_row < n; row += gridDim.x * rpb) {
+        const bool valid = row < n;
+        T acc[NV];
+#pragma unroll
+        for (int c = 0; c < NV; ++c) acc[c] = T(0);
+        if (valid) {
+            const int k1 = rp[row + 1];
+            for (int k = rp[row] + sub; k < k1; k += LANES) {
+                const int j = ci[k];
+                const T a = v[k];
+                const T dj = d[j];
+                T bj[NV];
+                load_row<NV>(b + (size_t)j * NV, bj);
+#pragma unroll
+                for (int c = 0; c < NV; ++c) acc[c] += a * (RECIP ? bj[c] * dj : bj[c] / dj);
+            }
+        }
+#pragma unroll
+        for (int o = LANES / 2; o > 0; o >>= 1)
+#pragma unroll
+            for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o, LANES);
+        if (valid && sub == 0) {
+            const size_t base = (size_t)row * NV;
+            const T di = d[row];
+#pragma unroll
+            for (int c = 0; c < NV; ++c) {
+                const T bi = b[base + c];
+                x[base + c] = RECIP ? bi * di : bi / di;
+                r[base + c] = bi - acc[c];
+            }
+        }
+    }
+}
+
+// coarsest LDL^T solves of the three hierarchies: Li/LiT/piv/cz per subspace
+struct TriCoarse {
+    int n[3];
+    const double* M[3];    // L^{-1} (forward) or its transpose (backward)
+    const double* piv[3];
+    double* cz[3];
+    const void* io[3];     // forward: b (hierarchy type); backward: x output
+};
+
+template <typename T, int NV, bool FWD>
+__global__ void __launch_bounds__(kBlock)
+k_mv3_coarse(TriCoarse t, const KState* st) {
+    pdl_gate();
+    if (st && st->done) return;
+    const int q = blockIdx.y;
+    const int n = t.n[q];
+    const int lane = threadIdx.x & 31;
+    for (int row = blockIdx.x * (kBlock / 32) + threadIdx.x / 32; row < n; row += gridDim.x * (kBlock / 32)) {
+        double acc[NV];
+#pragma unroll
+        for (int c = 0; c < NV; ++c) acc[c] = 0.0;
+        const double* lr = t.M[q] + (size_t)row * n;
+        if constexpr (FWD) {
+            const T* b = (const T*)t.io[q];
+            for (int k = lane; k <= row; k += 32) {
+                const double a = lr[k];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) acc[c] += a * (double)b[(size_t)k * NV + c];
+            }
+        } else {
+            const double* z = t.cz[q];
+            for (int k = row + lane; k < n; k += 32) {
+                const double a = lr[k];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) acc[c] += a * z[(size_t)k * NV + c];
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
+        if (lane == 0) {
+            if constexpr (FWD) {
+                const double dd = t.piv[q][row];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) t.cz[q][(size_t)row * NV + c] = dd != 0.0 ? acc[c] / dd : 0.0;
+            } else {
+                T* x = (T*)t.io[q];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) x[(size_t)row * NV + c] = (T)acc[c];
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // V-cycle tail on one thread-block cluster: every level from the first small
 // one down to the coarsest solve and back up, in one launch. The cluster's 8
 // CTAs split each step's rows and meet at cluster barriers, which replace the
@@ -692,6 +872,7 @@ struct AmsState {
     unsigned gen = 0;
     ForkSet forks;  // the y and z nodal V-cycles run beside the x one
     TailSet tails[4];
+    bool tri = true;  // nodal V-cycles in lockstep launches (SSV_AMS_TRI=0: three branches)
 };
 
 void ams_free(AmsState* a) { delete a; }
@@ -817,6 +998,99 @@ static T* vcycle(std::vector<AmgDevLevel>& L, const TailSet& tail, int l, const 
     return cur;
 }
 
+// ---- the three nodal V-cycles in lockstep --------------------------------
+static bool tri_ok(const AmsState& a) {
+    if (!a.tri) return false;
+    const size_t L = a.amg[1].size();
+    if (L < 1 || a.amg[2].size() != L || a.amg[3].size() != L) return false;
+    for (int k = 1; k < 4; ++k) {
+        if (a.tails[k].start >= 0) return false;
+        if (a.amg[k].back().direct != a.amg[1].back().direct || !a.amg[k].back().direct) return false;
+    }
+    return true;
+}
+
+template <typename T, int NV, int MODE, bool RECIP>
+static void spmv3(const Tri<T>& t, int lanes, T w, const KState* st, cudaStream_t s) {
+    const int nmax = std::max(t.n[0], std::max(t.n[1], t.n[2]));
+    const int rpb = kBlock / lanes;
+    const dim3 grid(std::max(1, std::min((nmax + rpb - 1) / rpb, sm_count() * 8 / 3)), 3);
+    switch (lanes) {
+        case 2: launch_k(k_mv3_spmv<T, NV, 2, MODE, RECIP>, grid, kBlock, s, t, w, st); break;
+        case 4: launch_k(k_mv3_spmv<T, NV, 4, MODE, RECIP>, grid, kBlock, s, t, w, st); break;
+        case 8: launch_k(k_mv3_spmv<T, NV, 8, MODE, RECIP>, grid, kBlock, s, t, w, st); break;
+        case 16: launch_k(k_mv3_spmv<T, NV, 16, MODE, RECIP>, grid, kBlock, s, t, w, st); break;
+        default: launch_k(k_mv3_spmv<T, NV, 32, MODE, RECIP>, grid, kBlock, s, t, w, st); break;
+    }
+}
+
+template <typename T, int NV, bool RECIP>
+static void first_res3(const Tri<T>& t, int lanes, const KState* st, cudaStream_t s) {
+    const int nmax = std::max(t.n[0], std::max(t.n[1], t.n[2]));
+    const int rpb = kBlock / lanes;
+    const dim3 grid(std::max(1, std::min((nmax + rpb - 1) / rpb, sm_count() * 8 / 3)), 3);
+    switch (lanes) {
+        case 2: launch_k(k_mv3_first_res<T, NV, 2, RECIP>, grid, kBlock, s, t, st); break;
+        case 4: launch_k(k_mv3_first_res<T, NV, 4, RECIP>, grid, kBlock, s, t, st); break;
+        case 8: launch_k(k_mv3_first_res<T, NV, 8, RECIP>, grid, kBlock, s, t, st); break;
+        case 16: launch_k(k_mv3_first_res<T, NV, 16, RECIP>, grid, kBlock, s, t, st); break;
+        default: launch_k(k_mv3_first_res<T, NV, 32, RECIP>, grid, kBlock, s, t, st); break;
+    }
+}
+
+// V-cycles of subspaces 1..3 from their right-hand sides a.rs[1..3]; returns
+// the result buffers (each level 0's post-sweep buffer).
+template <typename T, int NV, bool RECIP>
+static void vcycle3(AmsState& a, const KState* st, cudaStream_t s, T* out[3]) {
+    const int L = (int)a.amg[1].size();
+    auto rhs = [&](int k, int l) -> const T* { return l == 0 ? a.rs[k + 1].as<T>() : a.amg[k + 1][l].b.as<T>(); };
+    auto lv = [&](int k, int l) -> AmgDevLevel& { return a.amg[k + 1][l]; };
+    for (int l = 0; l < L - 1; ++l) {
+        Tri<T> fr{}, rs{};
+        for (int k = 0; k < 3; ++k) {
+            AmgDevLevel& v = lv(k, l);
+            fr.n[k] = v.A.n; fr.rp[k] = v.A.rp.get(); fr.ci[k] = v.A.ci.get(); fr.v[k] = v.A.val<T>();
+            fr.b[k] = rhs(k, l); fr.d[k] = l1_of<T, RECIP>(v); fr.y[k] = v.xa.as<T>(); fr.r[k] = v.r.as<T>();
+            rs.n[k] = v.Pt.n; rs.rp[k] = v.Pt.rp.get(); rs.ci[k] = v.Pt.ci.get(); rs.v[k] = v.Pt.val<T>();
+            rs.x[k] = v.r.as<T>(); rs.y[k] = lv(k, l + 1).b.template as<T>();
+        }
+        first_res3<T, NV, RECIP>(fr, lv(0, l).A.lanes_for(NV), st, s);
+        spmv3<T, NV, MV_AX, RECIP>(rs, lv(0, l).Pt.lanes_for(NV), T(0), st, s);
+    }
+    {   // coarsest: LDL^T pseudo-inverse, FP64
+        TriCoarse f{}, b{};
+        int nmax = 0;
+        for (int k = 0; k < 3; ++k) {
+            AmgDevLevel& v = lv(k, L - 1);
+            nmax = std::max(nmax, v.A.n);
+            f.n[k] = b.n[k] = v.A.n;
+            f.M[k] = v.Li.get(); b.M[k] = v.LiT.get();
+            f.piv[k] = b.piv[k] = v.piv.get();
+            f.cz[k] = b.cz[k] = v.cz.get();
+            f.io[k] = rhs(k, L - 1);
+            b.io[k] = v.xa.raw.get();
+        }
+        const dim3 grid(std::max(1, std::min((nmax + 7) / 8, sm_count() * 4 / 3)), 3);
+        launch_k(k_mv3_coarse<T, NV, true>, grid, kBlock, s, f, st);
+        launch_k(k_mv3_coarse<T, NV, false>, grid, kBlock, s, b, st);
+    }
+    for (int l = L - 2; l >= 0; --l) {
+        Tri<T> pa{}, js{};
+        for (int k = 0; k < 3; ++k) {
+            AmgDevLevel& v = lv(k, l);
+            AmgDevLevel& nx = lv(k, l + 1);
+            const T* e = (l + 1 == L - 1) ? nx.xa.as<T>() : nx.xb.as<T>();
+            pa.n[k] = v.P.n; pa.rp[k] = v.P.rp.get(); pa.ci[k] = v.P.ci.get(); pa.v[k] = v.P.val<T>();
+            pa.x[k] = e; pa.y[k] = v.xa.as<T>();
+            js.n[k] = v.A.n; js.rp[k] = v.A.rp.get(); js.ci[k] = v.A.ci.get(); js.v[k] = v.A.val<T>();
+            js.x[k] = v.xa.as<T>(); js.y[k] = v.xb.as<T>(); js.b[k] = rhs(k, l); js.d[k] = l1_of<T, RECIP>(v);
+        }
+        spmv3<T, NV, MV_ADD, RECIP>(pa, lv(0, l).P.lanes_for(NV), T(1), st, s);
+        spmv3<T, NV, MV_JAC, RECIP>(js, lv(0, l).A.lanes_for(NV), T(0), st, s);
+    }
+    for (int k = 0; k < 3; ++k) out[k] = (L == 1) ? lv(k, 0).xa.template as<T>() : lv(k, 0).xb.template as<T>();
+}
+
 template <typename T, int NV, int LANES>
 static void pi_restrict_l(const AmsState& a, const double* r, T* ox, T* oy, T* oz, const KState* st,
                           cudaStream_t s) {
@@ -917,13 +1191,17 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
     auto nodal = [&]() {
         residual();
         pi_restrict<T, NV>(a, r, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), st, s);
-        // the three V-cycles are independent (own hierarchies and vectors)
-        a.forks.fork(s, 2);
-        T* gx = vcycle<T, NV, RECIP>(a.amg[1], a.tails[1], 0, a.rs[1].as<T>(), 1, st, s);
-        T* gy = vcycle<T, NV, RECIP>(a.amg[2], a.tails[2], 0, a.rs[2].as<T>(), 1, st, a.forks.side[0]);
-        T* gz = vcycle<T, NV, RECIP>(a.amg[3], a.tails[3], 0, a.rs[3].as<T>(), 1, st, a.forks.side[1]);
-        a.forks.join(s, 2);
-        pi_prolong<T, NV>(a, gx, gy, gz, cur, st, s);
+        T* g3[3];
+        if (tri_ok(a)) {  // one chain of launches carrying all three hierarchies
+            vcycle3<T, NV, RECIP>(a, st, s, g3);
+        } else {  // the three V-cycles are independent (own hierarchies and vectors)
+            a.forks.fork(s, 2);
+            g3[0] = vcycle<T, NV, RECIP>(a.amg[1], a.tails[1], 0, a.rs[1].as<T>(), 1, st, s);
+            g3[1] = vcycle<T, NV, RECIP>(a.amg[2], a.tails[2], 0, a.rs[2].as<T>(), 1, st, a.forks.side[0]);
+            g3[2] = vcycle<T, NV, RECIP>(a.amg[3], a.tails[3], 0, a.rs[3].as<T>(), 1, st, a.forks.side[1]);
+            a.forks.join(s, 2);
+        }
+        pi_prolong<T, NV>(a, g3[0], g3[1], g3[2], cur, st, s);
     };
     if (a.cycle_type == 7) {
         fine_smooth(); gradient(); fine_smooth(); nodal(); fine_smooth(); gradient(); fine_smooth();
@@ -1143,6 +1421,10 @@ static void ams_reserve(AmsState& a, int nv) {
     ++a.gen;  // new work buffers: graphs that captured the old ones must be rebuilt
     tune_lanes(a);
     build_tails(a);
+    {
+        const char* e = std::getenv("SSV_AMS_TRI");
+        a.tri = !(e && e[0] == '0');
+    }
 }
 
 static std::vector<double> reciprocal(const std::vector<double>& v) {
@@ -1436,6 +1718,11 @@ static void ams_profile_t(AmsState& a, int reps, bool cold, ssv_phase_profile* o
     });
     timed("grad_vcycle", grad_vc, 0, [&] { vcycle<T, NV, RECIP>(a.amg[0], a.tails[0], 0, a.rs[0].as<T>(), 1, nullptr, s); });
     timed("nodal_vcycles", nod_vc, 0, [&] {
+        if (tri_ok(a)) {
+            T* g3[3];
+            vcycle3<T, NV, RECIP>(a, nullptr, s, g3);
+            return;
+        }
         a.forks.fork(s, 2);
         vcycle<T, NV, RECIP>(a.amg[1], a.tails[1], 0, a.rs[1].as<T>(), 1, nullptr, s);
         vcycle<T, NV, RECIP>(a.amg[2], a.tails[2], 0, a.rs[2].as<T>(), 1, nullptr, a.forks.side[0]);

@@ -298,3 +298,21 @@ def test_cluster_tail_and_launch_chain_agree(mag_well, eddy_well, monkeypatch, c
     o = O.AmsOracle(d["a_real"] if complex_form else d["A"], d["G"], d["freedofs"], *d["coords"])
     yo = o.apply_complex(b) if complex_form else o.apply(b)
     assert np.abs(y_tail - yo).max() <= APPLY_RTOL_WELL * np.abs(yo).max()
+
+
+@pytest.mark.parametrize("complex_form", [False, True])
+def test_lockstep_nodal_cycles_and_branches_agree(mag_well, eddy_well, monkeypatch, complex_form):
+    # by default the three nodal V-cycles run as one chain of launches over
+    # all three hierarchies; SSV_AMS_TRI=0 runs them as three graph branches
+    d = eddy_well if complex_form else mag_well
+    rng = np.random.default_rng(12)
+    n = d["A"].shape[0]
+    b = rng.standard_normal(n) + (1j * rng.standard_normal(n) if complex_form else 0)
+    monkeypatch.setenv("SSV_AMS_TRI", "0")
+    y_br = _ams(d, complex_form=complex_form) * b
+    monkeypatch.setenv("SSV_AMS_TRI", "1")
+    y_tri = _ams(d, complex_form=complex_form) * b
+    assert np.abs(y_tri - y_br).max() <= APPLY_RTOL_WELL * np.abs(y_br).max()
+    o = O.AmsOracle(d["a_real"] if complex_form else d["A"], d["G"], d["freedofs"], *d["coords"])
+    yo = o.apply_complex(b) if complex_form else o.apply(b)
+    assert np.abs(y_tri - yo).max() <= APPLY_RTOL_WELL * np.abs(yo).max()
