@@ -96,8 +96,12 @@ template <typename A, typename B>
 using wider_t = std::conditional_t<(sizeof(A) >= sizeof(B)), A, B>;
 
 // y (op)= A x with matrix values TV, input TX, output TY; accumulation in the
-// wider of TV and TX.
-template <typename TV, typename TX, typename TY, int NV, int LANES, int MODE, bool RECIP>
+// wider of TV and TX. Each LANES-wide row group handles U rows per pass of the
+// row loop and issues the loads of all U rows before using any of them, so a
+// warp keeps U times as many HBM requests in flight (a cold fine-level pass
+// is bound by requests in flight, not by bandwidth, at U = 1). The sum of each
+// row runs in the same order for every U.
+template <typename TV, typename TX, typename TY, int NV, int LANES, int MODE, bool RECIP, int U = 1>
 __global__ void __launch_bounds__(kBlock)
 k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const TV* __restrict__ v,
           const TX* __restrict__ x, TY* __restrict__ y, const TY* __restrict__ b, const TY* __restrict__ d, TY w,
@@ -108,40 +112,63 @@ k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T
     const int sub = threadIdx.x % LANES;
     const int rpb = kBlock / LANES;
     const int lane_row = (threadIdx.x & 31) / LANES;  // warp-uniform trip count
-    for (int row = blockIdx.x * rpb + threadIdx.x / LANES; row - lane_row < n; row += gridDim.x * rpb) {
-        const bool valid = row < n;
-        TA acc[NV];
+    for (int row0 = blockIdx.x * rpb * U + threadIdx.x / LANES; row0 - lane_row < n; row0 += gridDim.x * rpb * U) {
+        int kk[U], ke[U];
+        TA acc[U][NV];
 #pragma unroll
-        for (int c = 0; c < NV; ++c) acc[c] = TA(0);
-        if (valid) {
-            const int k1 = rp[row + 1];
-            for (int k = rp[row] + sub; k < k1; k += LANES) {
-                const TA a = (TA)v[k];
-                TX xv[NV];
-                load_row<NV>(x + (size_t)ci[k] * NV, xv);
+        for (int u = 0; u < U; ++u) {
+            const int row = row0 + u * rpb;
+            kk[u] = row < n ? rp[row] + sub : 0;
+            ke[u] = row < n ? rp[row + 1] : 0;
 #pragma unroll
-                for (int c = 0; c < NV; ++c) acc[c] += a * (TA)xv[c];
+            for (int c = 0; c < NV; ++c) acc[u][c] = TA(0);
+        }
+        while (true) {
+            TA a[U];
+            int col[U];
+            bool any = false;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const bool on = kk[u] < ke[u];
+                a[u] = on ? (TA)v[kk[u]] : TA(0);
+                col[u] = on ? ci[kk[u]] : -1;
+                any |= on;
+            }
+            if (!any) break;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (col[u] >= 0) {
+                    TX xv[NV];
+                    load_row<NV>(x + (size_t)col[u] * NV, xv);
+#pragma unroll
+                    for (int c = 0; c < NV; ++c) acc[u][c] += a[u] * (TA)xv[c];
+                    kk[u] += LANES;
+                }
             }
         }
 #pragma unroll
-        for (int o = LANES / 2; o > 0; o >>= 1)
+        for (int u = 0; u < U; ++u) {
 #pragma unroll
-            for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o, LANES);
-        if (valid && sub == 0) {
-            const size_t base = (size_t)row * NV;
+            for (int o = LANES / 2; o > 0; o >>= 1)
 #pragma unroll
-            for (int c = 0; c < NV; ++c) {
-                const TY ac = (TY)acc[c];
-                if constexpr (MODE == MV_AX) {
-                    y[base + c] = ac;
-                } else if constexpr (MODE == MV_RES) {
-                    y[base + c] = b[base + c] - ac;
-                } else if constexpr (MODE == MV_ADD) {
-                    y[base + c] += w * ac;
-                } else {
-                    const TY r = b[base + c] - ac;
-                    const TY xo = (TY)x[base + c];
-                    y[base + c] = RECIP ? xo + r * d[row] : xo + r / d[row];
+                for (int c = 0; c < NV; ++c) acc[u][c] += __shfl_down_sync(0xffffffffu, acc[u][c], o, LANES);
+            const int row = row0 + u * rpb;
+            if (row < n && sub == 0) {
+                const size_t base = (size_t)row * NV;
+#pragma unroll
+                for (int c = 0; c < NV; ++c) {
+                    const TY ac = (TY)acc[u][c];
+                    if constexpr (MODE == MV_AX) {
+                        y[base + c] = ac;
+                    } else if constexpr (MODE == MV_RES) {
+                        y[base + c] = b[base + c] - ac;
+                    } else if constexpr (MODE == MV_ADD) {
+                        y[base + c] += w * ac;
+                    } else {
+                        const TY r = b[base + c] - ac;
+                        const TY xo = (TY)x[base + c];
+                        y[base + c] = RECIP ? xo + r * d[row] : xo + r / d[row];
+                    }
                 }
             }
         }
@@ -813,10 +840,13 @@ struct DevCsr {
     int64_t nnz = 0;
     int lanes = 8;               // from the mean row length until tuned
     int tuned[4] = {0, 0, 0, 0}; // lanes chosen by timing for NV = 1, 2, 4, 8 (0 = not tuned)
+    int tuned_u[4] = {1, 1, 1, 1};  // rows per row group and pass chosen with them
+    static int nv_slot(int nv) { return nv == 1 ? 0 : nv == 2 ? 1 : nv == 4 ? 2 : 3; }
     int lanes_for(int nv) const {
-        const int i = nv == 1 ? 0 : nv == 2 ? 1 : nv == 4 ? 2 : 3;
+        const int i = nv_slot(nv);
         return tuned[i] ? tuned[i] : lanes;
     }
+    int unroll_for(int nv) const { return tuned[nv_slot(nv)] ? tuned_u[nv_slot(nv)] : 1; }
     DevBuf<int> rp, ci;
     DualVec v;
     void upload(const HostCsr& A, bool fp32, cudaStream_t s) {
@@ -902,28 +932,46 @@ static void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
     SSV_CUDA(cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...));
 }
 
+// the (lanes, rows per group and pass) shapes the tuner tries; U > 1 only where
+// the matrix is large enough to fill the GPU several times over
+constexpr int kShapeL[] = {2, 4, 8, 16, 32, 4, 8, 16, 8, 16};
+constexpr int kShapeU[] = {1, 1, 1, 1, 1, 2, 2, 2, 4, 4};
+constexpr int kShapes = 10;
+constexpr int kUnrollMinRows = 65536;
+
+template <typename TV, typename TX, typename TY, int NV, int MODE, bool RECIP>
+static void launch_mv(int lanes, int u, int grid, cudaStream_t s, int n, const int* rp, const int* ci, const TV* v,
+                      const TX* x, TY* y, const TY* b, const TY* d, TY w, const KState* st) {
+#define SSV_MV_CASE(L, UU)                                                                                          \
+    if (lanes == L && u == UU) {                                                                                   \
+        launch_k(k_mv_spmv<TV, TX, TY, NV, L, MODE, RECIP, UU>, grid, kBlock, s, n, rp, ci, v, x, y, b, d, w, st); \
+        return;                                                                                                    \
+    }
+    SSV_MV_CASE(2, 1)
+    SSV_MV_CASE(4, 1)
+    SSV_MV_CASE(8, 1)
+    SSV_MV_CASE(16, 1)
+    SSV_MV_CASE(4, 2)
+    SSV_MV_CASE(8, 2)
+    SSV_MV_CASE(16, 2)
+    SSV_MV_CASE(8, 4)
+    SSV_MV_CASE(16, 4)
+#undef SSV_MV_CASE
+    launch_k(k_mv_spmv<TV, TX, TY, NV, 32, MODE, RECIP, 1>, grid, kBlock, s, n, rp, ci, v, x, y, b, d, w, st);
+}
+
+static int mv_grid(int n, int lanes, int u) {
+    const int rpb = kBlock / lanes * u;
+    return std::max(1, std::min((n + rpb - 1) / rpb, sm_count() * 8));
+}
+
 template <typename TV, typename TX, typename TY, int NV, int MODE, bool RECIP>
 static void mv_spmv(const DevCsr& A, const TX* x, TY* y, const TY* b, const TY* d, TY w, const KState* st,
                     cudaStream_t s) {
     const int lanes = A.lanes_for(NV);
-    const int rpb = kBlock / lanes;
-    const int grid = std::max(1, std::min((A.n + rpb - 1) / rpb, sm_count() * 8));
-    const TV* v = A.val<TV>();
-#define SSV_MV_CASE(L)                                                                                   \
-    case L:                                                                                              \
-        launch_k(k_mv_spmv<TV, TX, TY, NV, L, MODE, RECIP>, grid, kBlock, s, A.n, A.rp.get(), A.ci.get(), v, x, \
-                                                                           y, b, d, w, st);              \
-        break;
-    switch (lanes) {
-        SSV_MV_CASE(2)
-        SSV_MV_CASE(4)
-        SSV_MV_CASE(8)
-        SSV_MV_CASE(16)
-        default:
-            launch_k(k_mv_spmv<TV, TX, TY, NV, 32, MODE, RECIP>, grid, kBlock, s, A.n, A.rp.get(), A.ci.get(), v, x,
-                                                                                y, b, d, w, st);
-    }
-#undef SSV_MV_CASE
+    const int u = A.unroll_for(NV);
+    launch_mv<TV, TX, TY, NV, MODE, RECIP>(lanes, u, mv_grid(A.n, lanes, u), s, A.n, A.rp.get(), A.ci.get(),
+                                           A.val<TV>(), x, y, b, d, w, st);
 }
 
 template <typename T, int NV, bool RECIP>
@@ -1241,9 +1289,11 @@ static void l2_flush(cudaStream_t s) {
 }
 
 // Device time of `reps` launches: back to back (warm), or each after an L2
-// flush and timed alone (cold).
+// flush and timed alone (cold; `median` returns reps x the median launch,
+// which ranks candidate shapes with less noise than the sum).
 template <typename F>
-static float time_launches(F&& launch, int reps, bool cold, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+static float time_launches(F&& launch, int reps, bool cold, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1,
+                           bool median = false) {
     float total = 0.f;
     if (!cold) {
         SSV_CUDA(cudaEventRecord(e0, s));
@@ -1254,6 +1304,7 @@ static float time_launches(F&& launch, int reps, bool cold, cudaStream_t s, cuda
         SSV_CUDA(cudaEventElapsedTime(&total, e0, e1));
         return total;
     }
+    float each[16];
     for (int k = 0; k < reps; ++k) {
         l2_flush(s);
         SSV_CUDA(cudaEventRecord(e0, s));
@@ -1264,53 +1315,76 @@ static float time_launches(F&& launch, int reps, bool cold, cudaStream_t s, cuda
         float ms = 0.f;
         SSV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         total += ms;
+        if (k < 16) each[k] = ms;
+    }
+    if (median && reps <= 16) {
+        std::sort(each, each + reps);
+        return each[reps / 2] * reps;
     }
     return total;
 }
 
+// largest rows-per-group the tuner may pick (SSV_AMS_MAX_UNROLL, default 4)
+static int max_unroll() {
+    static int v = 0;
+    if (v == 0) {
+        const char* e = std::getenv("SSV_AMS_MAX_UNROLL");
+        v = e ? std::max(1, std::atoi(e)) : 4;
+    }
+    return v;
+}
+
+// Shapes of square level matrices are timed as residuals r = b - A x (b given),
+// the form the cycle runs them in (smoothing reads the same streams); the
+// transfers as y = A x.
 template <typename TV, typename TX, typename TY, int NV>
-static void tune_csr(DevCsr& A, const TX* x, TY* y, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
     if (A.n == 0 || A.nnz == 0) return;
     const TV* v = A.val<TV>();
     // a matrix much larger than a quarter of L2 streams from HBM in the cycle: tune it cold
     const bool cold = (double)A.nnz * (4 + sizeof(TV)) > (double)(32 << 20);
     float best = 1e30f;
-    int pick = A.lanes;
-    const int cand[5] = {2, 4, 8, 16, 32};
-    for (int L : cand) {
-        const int rpb = kBlock / L;
-        const int grid = std::max(1, std::min((A.n + rpb - 1) / rpb, sm_count() * 8));
+    int pick = A.lanes, pick_u = 1;
+    for (int i = 0; i < kShapes; ++i) {
+        const int L = kShapeL[i], U = kShapeU[i];
+        if (U > 1 && (A.n < kUnrollMinRows || U > max_unroll())) continue;
+        const int grid = mv_grid(A.n, L, U);
         auto launch = [&] {
-            switch (L) {
-                case 2: k_mv_spmv<TV, TX, TY, NV, 2, MV_AX, false><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, nullptr, nullptr, TY(0), nullptr); break;
-                case 4: k_mv_spmv<TV, TX, TY, NV, 4, MV_AX, false><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, nullptr, nullptr, TY(0), nullptr); break;
-                case 8: k_mv_spmv<TV, TX, TY, NV, 8, MV_AX, false><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, nullptr, nullptr, TY(0), nullptr); break;
-                case 16: k_mv_spmv<TV, TX, TY, NV, 16, MV_AX, false><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, nullptr, nullptr, TY(0), nullptr); break;
-                default: k_mv_spmv<TV, TX, TY, NV, 32, MV_AX, false><<<grid, kBlock, 0, s>>>(A.n, A.rp.get(), A.ci.get(), v, x, y, nullptr, nullptr, TY(0), nullptr); break;
-            }
+            if (b)
+                launch_mv<TV, TX, TY, NV, MV_RES, false>(L, U, grid, s, A.n, A.rp.get(), A.ci.get(), v, x, y, b,
+                                                         nullptr, TY(0), nullptr);
+            else
+                launch_mv<TV, TX, TY, NV, MV_AX, false>(L, U, grid, s, A.n, A.rp.get(), A.ci.get(), v, x, y, nullptr,
+                                                        nullptr, TY(0), nullptr);
         };
         launch();
-        const float ms = time_launches(launch, cold ? 3 : 4, cold, s, e0, e1);
+        const float ms = time_launches(launch, cold ? 5 : 4, cold, s, e0, e1, true);
         if (ms < best) {
             best = ms;
             pick = L;
+            pick_u = U;
         }
     }
-    A.tuned[NV == 1 ? 0 : NV == 2 ? 1 : NV == 4 ? 2 : 3] = pick;
+    A.tuned[DevCsr::nv_slot(NV)] = pick;
+    A.tuned_u[DevCsr::nv_slot(NV)] = pick_u;
+    static const bool log = std::getenv("SSV_AMS_TUNE_LOG") != nullptr;
+    if (log)
+        std::fprintf(stderr, "ams tune: n=%d nnz=%lld nv=%d %s -> lanes %d rows/group %d (%.2f us)\n", A.n,
+                     (long long)A.nnz, NV, cold ? "cold" : "warm", pick, pick_u, 1e3 * best / (cold ? 5 : 4));
 }
 
 template <typename T, int NV>
 static void tune_all_nv(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
-    tune_csr<double, double, double, NV>(a.A_bc, a.xa.get(), a.xb.get(), s, e0, e1);
-    tune_csr<double, double, T, NV>(a.Gt, a.r.get(), a.rs[0].as<T>(), s, e0, e1);
-    tune_csr<double, T, double, NV>(a.G, a.rs[0].as<T>(), a.xb.get(), s, e0, e1);
+    tune_csr<double, double, double, NV>(a.A_bc, a.xa.get(), a.xb.get(), a.r.get(), s, e0, e1);
+    tune_csr<double, double, T, NV>(a.Gt, a.r.get(), a.rs[0].as<T>(), nullptr, s, e0, e1);
+    tune_csr<double, T, double, NV>(a.G, a.rs[0].as<T>(), a.xb.get(), nullptr, s, e0, e1);
     for (int sub = 0; sub < 4; ++sub) {
         auto& L = a.amg[sub];
         for (size_t l = 0; l < L.size(); ++l) {
-            tune_csr<T, T, T, NV>(L[l].A, L[l].xa.as<T>(), L[l].xb.as<T>(), s, e0, e1);
+            tune_csr<T, T, T, NV>(L[l].A, L[l].xa.as<T>(), L[l].xb.as<T>(), L[l].b.as<T>(), s, e0, e1);
             if (l + 1 < L.size()) {
-                tune_csr<T, T, T, NV>(L[l].P, L[l + 1].xa.as<T>(), L[l].r.as<T>(), s, e0, e1);
-                tune_csr<T, T, T, NV>(L[l].Pt, L[l].r.as<T>(), L[l + 1].b.as<T>(), s, e0, e1);
+                tune_csr<T, T, T, NV>(L[l].P, L[l + 1].xa.as<T>(), L[l].r.as<T>(), nullptr, s, e0, e1);
+                tune_csr<T, T, T, NV>(L[l].Pt, L[l].r.as<T>(), L[l + 1].b.as<T>(), nullptr, s, e0, e1);
             }
         }
     }

@@ -156,7 +156,7 @@ int ssv_matrix_create(int32_t rows, int32_t cols, const int32_t* row_ptr, const 
             A->ci.upload(A->h_ci.data(), A->h_ci.size(), s);
             const size_t words = (size_t)nnz * (dtype == SSV_F64 ? 1 : 2);
             A->val.upload(static_cast<const double*>(values), words, s);
-            A->lanes = ssv::pick_lanes(rows > 0 ? (double)nnz / rows : 1.0);
+            A->lanes = ssv::pick_shape(rows, rows > 0 ? (double)nnz / rows : 1.0);
             SSV_CUDA(cudaStreamSynchronize(s));
         } catch (...) {
             delete A;

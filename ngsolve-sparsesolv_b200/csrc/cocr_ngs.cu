@@ -214,7 +214,7 @@ static void run_cocr_ngs(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, int
         k_ngs_dot<S><<<g, kBlock, 0, s>>>(n, qt, q, dst, NGS_MU, red);
         k_ngs_update<S><<<g, kBlock, 0, s>>>(n, x, p, q, qt, r, rt, dst, red);
         {
-            const int L = A->lanes;
+            const int L = A->lanes & 0xff;
             const int rpb = kBlock / L;
             int gg = std::max(1, std::min((n + rpb - 1) / rpb, sm_count() * 8));
             switch (L) {

@@ -193,11 +193,13 @@ struct RedBuf {
 };
 
 // ---------------------------------------------------------------------------
-// SpMV family: a sub-warp of LANES threads per row, lanes stride the row.
+// SpMV family: a sub-warp of LANES threads per row, lanes stride the row; each
+// row group takes U rows per pass and issues all their loads before using
+// them (more HBM requests in flight; same per-row summation order for any U).
 // MODE 0: y = A x.  MODE 1: y = A x and reduce dot(x, y) (conj(x) if conj).
 // MODE 2: y = b - A x.  MODE 3: y = A x and reduce x^T y (unconjugated).
 // ---------------------------------------------------------------------------
-template <typename S, typename SV, int LANES, int MODE>
+template <typename S, typename SV, int LANES, int MODE, int U = 1>
 __global__ void __launch_bounds__(kBlock)
 k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const SV* __restrict__ v,
        const S* __restrict__ x, S* __restrict__ y, const S* __restrict__ b,
@@ -211,36 +213,68 @@ k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const SV* 
     const int lane_row = (threadIdx.x & 31) / LANES;
     double2 part = make_double2(0.0, 0.0);
     const bool conj = st ? (st->conj != 0) : false;
-    for (int row = blockIdx.x * rows_per_block + threadIdx.x / LANES; row - lane_row < n;
-         row += gridDim.x * rows_per_block) {
-        const bool valid = row < n;
-        S acc = ST<S>::zero();
-        if (valid) {
-            const int k0 = rp[row], k1 = rp[row + 1];
-            for (int k = k0 + sub; k < k1; k += LANES) acc = ST<S>::fma(hi_of_any(v[k]), x[ci[k]], acc);
+    for (int row0 = blockIdx.x * rows_per_block * U + threadIdx.x / LANES; row0 - lane_row < n;
+         row0 += gridDim.x * rows_per_block * U) {
+        int kk[U], ke[U];
+        S acc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int row = row0 + u * rows_per_block;
+            kk[u] = row < n ? rp[row] + sub : 0;
+            ke[u] = row < n ? rp[row + 1] : 0;
+            acc[u] = ST<S>::zero();
+        }
+        while (true) {
+            SV a[U];
+            int col[U];
+            bool any = false;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const bool on = kk[u] < ke[u];
+                if (on) {
+                    a[u] = v[kk[u]];
+                    col[u] = ci[kk[u]];
+                } else {
+                    col[u] = -1;
+                }
+                any |= on;
+            }
+            if (!any) break;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (col[u] >= 0) {
+                    acc[u] = ST<S>::fma(hi_of_any(a[u]), x[col[u]], acc[u]);
+                    kk[u] += LANES;
+                }
+            }
         }
 #pragma unroll
-        for (int o = LANES / 2; o > 0; o >>= 1) {
-            if constexpr (ST<S>::cplx) {
-                acc.x += __shfl_down_sync(0xffffffffu, acc.x, o, LANES);
-                acc.y += __shfl_down_sync(0xffffffffu, acc.y, o, LANES);
-            } else {
-                acc += __shfl_down_sync(0xffffffffu, acc, o, LANES);
+        for (int u = 0; u < U; ++u) {
+#pragma unroll
+            for (int o = LANES / 2; o > 0; o >>= 1) {
+                if constexpr (ST<S>::cplx) {
+                    acc[u].x += __shfl_down_sync(0xffffffffu, acc[u].x, o, LANES);
+                    acc[u].y += __shfl_down_sync(0xffffffffu, acc[u].y, o, LANES);
+                } else {
+                    acc[u] += __shfl_down_sync(0xffffffffu, acc[u], o, LANES);
+                }
             }
-        }
-        if (sub == 0 && valid) {
-            if (mask && !mask[row]) acc = ST<S>::zero();  // project() of the NGSolve COCR loop
-            if constexpr (MODE == 2) {
-                y[row] = b[row] - acc;
-            } else {
-                y[row] = acc;
-            }
-            if constexpr (MODE == 1) {
-                S xi = x[row];
-                S d = (conj ? ST<S>::conj(xi) : xi) * acc;
-                part = add2(part, s_to2<S>(d));
-            } else if constexpr (MODE == 3) {
-                part = add2(part, s_to2<S>(x[row] * acc));
+            const int row = row0 + u * rows_per_block;
+            if (sub == 0 && row < n) {
+                S r = acc[u];
+                if (mask && !mask[row]) r = ST<S>::zero();  // project() of the NGSolve COCR loop
+                if constexpr (MODE == 2) {
+                    y[row] = b[row] - r;
+                } else {
+                    y[row] = r;
+                }
+                if constexpr (MODE == 1) {
+                    S xi = x[row];
+                    S d = (conj ? ST<S>::conj(xi) : xi) * r;
+                    part = add2(part, s_to2<S>(d));
+                } else if constexpr (MODE == 3) {
+                    part = add2(part, s_to2<S>(x[row] * r));
+                }
             }
         }
     }

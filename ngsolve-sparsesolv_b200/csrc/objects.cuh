@@ -14,6 +14,8 @@ cudaStream_t stream();
 
 // Sub-warp width of the CSR kernels from the mean row length.
 int pick_lanes(double nnz_per_row);
+// SpMV launch shape: lanes | (rows per row group and pass) << 8
+int pick_shape(int n, double nnz_per_row);
 
 // Side streams for independent pieces of one stream's work: fork() makes k
 // side streams wait for the work queued so far on s, join() makes s wait for
@@ -155,7 +157,7 @@ struct ICDevice {
     std::vector<int> h_Arp;
     DevBuf<int> Arp, Aci, Asrc;
     DevBuf<S> Av;
-    int lanes = 8;
+    int lanes = 8;  // SpMV launch shape of the ABMC-ordered matrix (pick_shape)
     // factor L (diag last), U = L^T (diag first)
     std::vector<int> h_Lrp, h_Lci;
     DevBuf<int> Lrp, Lci, Lsrc, Urp, Uci, Usrc;
@@ -215,7 +217,7 @@ struct ssv_matrix {
     std::vector<int> h_rp, h_ci;
     ssv::DevBuf<int> rp, ci;
     ssv::DevBuf<double> val;  // nnz (F64) or 2*nnz (C128) doubles
-    int lanes = 8;
+    int lanes = 8;  // SpMV launch shape (pick_shape)
 };
 
 struct ssv_solver {

@@ -97,28 +97,45 @@ void run_graph_loop(GraphLoop& g, KState* d_st, int max_iters) {
     }
 }
 
+// `shape` = lanes per row | (rows per row group and pass) << 8
 template <typename S, typename SV, int MODE>
-void launch_spmv(int lanes, int n, const int* rp, const int* ci, const SV* v, const S* x, S* y,
+void launch_spmv(int shape, int n, const int* rp, const int* ci, const SV* v, const S* x, S* y,
                  const S* b, const uint8_t* mask, KState* st, int op, RedBuf red, double2* out,
                  cudaStream_t s) {
-    const int rows_per_block = kBlock / lanes;
+    const int lanes = shape & 0xff;
+    const int u = std::max(1, shape >> 8);
+    const int rows_per_block = kBlock / lanes * u;
     int grid = (n + rows_per_block - 1) / rows_per_block;
     grid = std::max(1, std::min(grid, sm_count() * 8));
-#define SSV_SPMV_CASE(L)                                                                       \
-    case L:                                                                                    \
-        k_spmv<S, SV, L, MODE><<<grid, kBlock, 0, s>>>(n, rp, ci, v, x, y, b, mask, st, op, red, \
-                                                       out);                                   \
-        break;
-    switch (lanes) {
-        SSV_SPMV_CASE(2)
-        SSV_SPMV_CASE(4)
-        SSV_SPMV_CASE(8)
-        SSV_SPMV_CASE(16)
-        default:
-            k_spmv<S, SV, 32, MODE><<<grid, kBlock, 0, s>>>(n, rp, ci, v, x, y, b, mask, st, op, red, out);
+#define SSV_SPMV_CASE(L, UU)                                                                          \
+    if (lanes == L && u == UU) {                                                                      \
+        k_spmv<S, SV, L, MODE, UU><<<grid, kBlock, 0, s>>>(n, rp, ci, v, x, y, b, mask, st, op, red, out); \
+        SSV_LAUNCH_CHECK();                                                                           \
+        return;                                                                                       \
     }
+    SSV_SPMV_CASE(2, 1)
+    SSV_SPMV_CASE(4, 1)
+    SSV_SPMV_CASE(8, 1)
+    SSV_SPMV_CASE(16, 1)
+    SSV_SPMV_CASE(4, 2)
+    SSV_SPMV_CASE(8, 2)
 #undef SSV_SPMV_CASE
+    k_spmv<S, SV, 32, MODE, 1><<<grid, kBlock, 0, s>>>(n, rp, ci, v, x, y, b, mask, st, op, red, out);
     SSV_LAUNCH_CHECK();
+}
+
+// lanes and rows per group for a matrix of n rows and nnz_per_row: a large
+// matrix takes two rows per group and half the lanes of the one-row shape
+// (SSV_SPMV_ROWS_PER_GROUP=1 keeps one row per group everywhere)
+int pick_shape(int n, double nnz_per_row) {
+    static int rows = -1;
+    if (rows < 0) {
+        const char* e = std::getenv("SSV_SPMV_ROWS_PER_GROUP");
+        rows = (e && e[0] == '1') ? 1 : 2;
+    }
+    const int lanes = pick_lanes(nnz_per_row);
+    if (rows == 2 && n >= 65536 && (lanes == 8 || lanes == 16)) return (lanes / 2) | (2 << 8);
+    return lanes;
 }
 
 template <typename S>
@@ -170,7 +187,7 @@ void ICDevice<S>::build_pattern(int n_, const std::vector<int>& rp, const std::v
         Aci.upload(pci.data(), pci.size(), s);
         Asrc.upload(psrc.data(), psrc.size(), s);
         Av.alloc(pci.size());
-        lanes = pick_lanes(n > 0 ? (double)pci.size() / n : 1.0);
+        lanes = pick_shape(n, n > 0 ? (double)pci.size() / n : 1.0);
         perm.upload(h_perm.data(), h_perm.size(), s);
         uoff.upload(sched.block_offsets.data(), sched.block_offsets.size(), s);
         h_boff = sched.block_offsets;
