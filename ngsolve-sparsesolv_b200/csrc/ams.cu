@@ -42,16 +42,6 @@ namespace ssv {
 // ---------------------------------------------------------------------------
 enum MvMode : int { MV_AX = 0, MV_RES = 1, MV_ADD = 2, MV_JAC = 3 };
 
-// Programmatic dependent launch: the cycle's kernels are launched so that the
-// next one in the stream may be scheduled before this one ends. Each waits
-// here for its predecessor's completion and memory (griddepcontrol.wait)
-// before touching any data, then lets its own successor start launching.
-// Launched without the attribute, both instructions have no effect.
-__device__ __forceinline__ void pdl_gate() {
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
 // One row of NV columns in the widest aligned accesses the row allows (work
 // vectors come from cudaMalloc, so row r starts at r * NV * sizeof(T)).
 template <int NV>
@@ -906,31 +896,6 @@ struct AmsState {
 };
 
 void ams_free(AmsState* a) { delete a; }
-
-// SSV_PDL=0 launches the cycle's kernels without programmatic dependence.
-static bool pdl_enabled() {
-    static int v = -1;
-    if (v < 0) {
-        const char* e = std::getenv("SSV_PDL");
-        v = (e && e[0] == '0') ? 0 : 1;
-    }
-    return v != 0;
-}
-
-template <typename... KArgs, typename... Args>
-static void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = pdl_enabled() ? 1 : 0;
-    SSV_CUDA(cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...));
-}
 
 // the (lanes, rows per group and pass) shapes the tuner tries; U > 1 only where
 // the matrix is large enough to fill the GPU several times over

@@ -35,6 +35,7 @@ __device__ inline void ngs_finish(double2 total, KState* st, int op) {
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
 k_ngs_dot(int n, const S* __restrict__ a, const S* __restrict__ b, KState* st, int op, RedBuf red) {
+    pdl_gate();
     if (st->done) return;
     double2 part = make_double2(0.0, 0.0);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -49,6 +50,7 @@ __global__ void __launch_bounds__(kBlock)
 k_ngs_spmv_dot(int n, const int* __restrict__ rp, const int* __restrict__ ci, const S* __restrict__ v,
                const S* __restrict__ x, S* __restrict__ y, const uint8_t* __restrict__ mask, KState* st,
                RedBuf red) {
+    pdl_gate();
     if (st->done) return;
     const int sub = threadIdx.x % LANES;
     const int rpb = kBlock / LANES;
@@ -83,6 +85,7 @@ template <typename S>
 __global__ void __launch_bounds__(kBlock)
 k_ngs_update(int n, S* __restrict__ x, const S* __restrict__ p, const S* __restrict__ q,
              const S* __restrict__ qt, S* __restrict__ r, S* __restrict__ rt, KState* st, RedBuf red) {
+    pdl_gate();
     if (st->done) return;
     const S alpha = s_from2<S>(st->alpha);
     double2 part = make_double2(0.0, 0.0);
@@ -141,7 +144,7 @@ template <> KrylovWork<zdouble>& cw_of<zdouble>(CocrCtx& c) { return c.w_z; }
 template <typename S>
 static void apply_pre(ssv_precond* pre, const S* x, S* y, const KState* st, int n, cudaStream_t s) {
     if (pre) precond_apply_any<S>(pre, x, y, st, s);
-    else k_copy<S><<<grid_for(n, kBlock), kBlock, 0, s>>>(n, x, y);
+    else launch_k(k_copy<S>, grid_for(n, kBlock), kBlock, s, n, x, y);
 }
 
 static std::string pre_key(const ssv_precond* pre) {
@@ -173,8 +176,8 @@ static void run_cocr_ngs(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, int
       *t = w.t.get();
     // sol = 0 ; r = rhs projected ; ||rhs|| (:274-299)
     SSV_CUDA(cudaMemsetAsync(x, 0, sizeof(S) * n, s));
-    k_gather_perm<S><<<g, kBlock, 0, s>>>(n, nullptr, d_b, r, fd, 1);
-    k_norm2<S><<<g, kBlock, 0, s>>>(n, r, red, w.scal.get());
+    launch_k(k_gather_perm<S>, g, kBlock, s, n, nullptr, d_b, r, fd, 1);
+    launch_k(k_norm2<S>, g, kBlock, s, n, r, red, w.scal.get());
     SSV_LAUNCH_CHECK();
     double2 nb;
     SSV_CUDA(cudaMemcpyAsync(&nb, w.scal.get(), sizeof(nb), cudaMemcpyDeviceToHost, s));
@@ -184,7 +187,7 @@ static void run_cocr_ngs(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, int
     // rt = M^{-1} r ; p = rt ; q = A p projected ; rho = rt^T q
     KState* dst = w.st.get();
     apply_pre<S>(pre, r, rt, nullptr, n, s);
-    k_copy<S><<<g, kBlock, 0, s>>>(n, rt, p);
+    launch_k(k_copy<S>, g, kBlock, s, n, rt, p);
     launch_spmv<S, S, 0>(A->lanes, n, A->rp.get(), A->ci.get(), v, p, q, nullptr, fd, nullptr, RED_STORE, red,
                          nullptr, s);
     SSV_LAUNCH_CHECK();
@@ -201,7 +204,7 @@ static void run_cocr_ngs(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, int
     {
         // state first, then rho = rt^T q into it
         SSV_CUDA(cudaMemcpyAsync(dst, &h, sizeof(h), cudaMemcpyHostToDevice, s));
-        k_dot<S><<<g, kBlock, 0, s>>>(n, rt, q, 0, nullptr, RED_STORE, red, &dst->rho);
+        launch_k(k_dot<S>, g, kBlock, s, n, rt, q, 0, nullptr, RED_STORE, red, &dst->rho);
         SSV_LAUNCH_CHECK();
     }
     std::string key = "ngs;" + std::to_string(n) + ";" + std::to_string((size_t)pre) + ";" +
@@ -211,21 +214,21 @@ static void run_cocr_ngs(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, int
     key += ";" + pre_key(pre);
     build_graph_loop(ctx.loop, key, [&](cudaGraphConditionalHandle hc, int use_cond) {
         apply_pre<S>(pre, q, qt, dst, n, s);
-        k_ngs_dot<S><<<g, kBlock, 0, s>>>(n, qt, q, dst, NGS_MU, red);
-        k_ngs_update<S><<<g, kBlock, 0, s>>>(n, x, p, q, qt, r, rt, dst, red);
+        launch_k(k_ngs_dot<S>, g, kBlock, s, n, qt, q, dst, NGS_MU, red);
+        launch_k(k_ngs_update<S>, g, kBlock, s, n, x, p, q, qt, r, rt, dst, red);
         {
             const int L = A->lanes & 0xff;
             const int rpb = kBlock / L;
             int gg = std::max(1, std::min((n + rpb - 1) / rpb, sm_count() * 8));
             switch (L) {
-                case 2: k_ngs_spmv_dot<S, 2><<<gg, kBlock, 0, s>>>(n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
-                case 4: k_ngs_spmv_dot<S, 4><<<gg, kBlock, 0, s>>>(n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
-                case 8: k_ngs_spmv_dot<S, 8><<<gg, kBlock, 0, s>>>(n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
-                case 16: k_ngs_spmv_dot<S, 16><<<gg, kBlock, 0, s>>>(n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
-                default: k_ngs_spmv_dot<S, 32><<<gg, kBlock, 0, s>>>(n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red);
+                case 2: launch_k(k_ngs_spmv_dot<S, 2>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
+                case 4: launch_k(k_ngs_spmv_dot<S, 4>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
+                case 8: launch_k(k_ngs_spmv_dot<S, 8>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
+                case 16: launch_k(k_ngs_spmv_dot<S, 16>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
+                default: launch_k(k_ngs_spmv_dot<S, 32>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red);
             }
         }
-        k_cocr_pq<S><<<g, kBlock, 0, s>>>(n, rt, t, p, q, dst);
+        launch_k(k_cocr_pq<S>, g, kBlock, s, n, rt, t, p, q, dst);
         k_ngs_loop_ctl<<<1, 32, 0, s>>>(dst, hc, use_cond);
         SSV_LAUNCH_CHECK();
     });
@@ -273,12 +276,12 @@ static void run_pcg(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, const ss
         v = reinterpret_cast<const S*>(ctx.vals_bc.get());
         ++nk;
     }
-    k_gather_perm<S><<<g, kBlock, 0, s>>>(n, nullptr, d_b, w.bw.get(), fd, 1);
-    k_gather_perm<S><<<g, kBlock, 0, s>>>(n, nullptr, d_x, w.xb[0].get(), fd, 1);
+    launch_k(k_gather_perm<S>, g, kBlock, s, n, nullptr, d_b, w.bw.get(), fd, 1);
+    launch_k(k_gather_perm<S>, g, kBlock, s, n, nullptr, d_x, w.xb[0].get(), fd, 1);
     launch_spmv<S, S, 2>(A->lanes, n, A->rp.get(), A->ci.get(), v, w.xb[0].get(), w.r.get(), w.bw.get(), nullptr,
                          nullptr, RED_STORE, red, nullptr, s);
-    k_norm2<S><<<g, kBlock, 0, s>>>(n, w.bw.get(), red, w.scal.get());
-    k_norm2<S><<<g, kBlock, 0, s>>>(n, w.r.get(), red, w.scal.get() + 1);
+    launch_k(k_norm2<S>, g, kBlock, s, n, w.bw.get(), red, w.scal.get());
+    launch_k(k_norm2<S>, g, kBlock, s, n, w.r.get(), red, w.scal.get() + 1);
     SSV_LAUNCH_CHECK();
     nk += 5;
     double2 nrm[2];
@@ -318,8 +321,8 @@ static void run_pcg(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, const ss
     SSV_CUDA(cudaMemcpyAsync(dst, &h, sizeof(h), cudaMemcpyHostToDevice, s));
     S* z = pre ? w.z.get() : w.r.get();
     if (pre) apply_pre<S>(pre, w.r.get(), w.z.get(), nullptr, n, s);
-    k_dot<S><<<g, kBlock, 0, s>>>(n, w.r.get(), z, cfg.conjugate, nullptr, RED_STORE, red, &dst->rho);
-    k_copy<S><<<g, kBlock, 0, s>>>(n, z, w.p.get());
+    launch_k(k_dot<S>, g, kBlock, s, n, w.r.get(), z, cfg.conjugate, nullptr, RED_STORE, red, &dst->rho);
+    launch_k(k_copy<S>, g, kBlock, s, n, z, w.p.get());
     SSV_LAUNCH_CHECK();
     const std::string key = "pcg;" + std::to_string(n) + ";" + std::to_string((size_t)v) + ";" +
                             std::to_string((size_t)dst) + ";" + std::to_string((size_t)red.partials) + ";" +
@@ -327,11 +330,11 @@ static void run_pcg(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, const ss
     build_graph_loop(ctx.pcg_loop, key, [&](cudaGraphConditionalHandle hc, int use_cond) {
         launch_spmv<S, S, 1>(A->lanes, n, A->rp.get(), A->ci.get(), v, w.p.get(), w.Ap.get(), nullptr, nullptr,
                              dst, RED_CG_ALPHA, red, nullptr, s);
-        k_cg_update<S><<<g, kBlock, 0, s>>>(n, w.xb[0].get(), w.xb[1].get(), w.xb[2].get(), w.p.get(), w.Ap.get(),
+        launch_k(k_cg_update<S>, g, kBlock, s, n, w.xb[0].get(), w.xb[1].get(), w.xb[2].get(), w.p.get(), w.Ap.get(),
                                            w.r.get(), dst, red);
         if (pre) apply_pre<S>(pre, w.r.get(), w.z.get(), dst, n, s);
-        k_dot<S><<<g, kBlock, 0, s>>>(n, w.r.get(), z, cfg.conjugate, dst, RED_CG_BETA, red, nullptr);
-        k_pupdate<S><<<g, kBlock, 0, s>>>(n, z, w.p.get(), dst);
+        launch_k(k_dot<S>, g, kBlock, s, n, w.r.get(), z, cfg.conjugate, dst, RED_CG_BETA, red, nullptr);
+        launch_k(k_pupdate<S>, g, kBlock, s, n, z, w.p.get(), dst);
         k_loop_ctl<<<1, 32, 0, s>>>(dst, hc, use_cond);
         SSV_LAUNCH_CHECK();
     });
@@ -353,7 +356,7 @@ static void run_pcg(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, const ss
     const S* xsrc;
     if (xbuf < 0) { w.t.zero(s); xsrc = w.t.get(); }
     else xsrc = w.xb[xbuf].get();
-    k_gather_perm<S><<<g, kBlock, 0, s>>>(n, nullptr, xsrc, d_x, fd, 0);
+    launch_k(k_gather_perm<S>, g, kBlock, s, n, nullptr, xsrc, d_x, fd, 0);
     SSV_LAUNCH_CHECK();
     res->kernel_launches = nk + 3 + (int64_t)ctx.pcg_loop.body_nodes * h.loops;
     res->history_total = cfg.save_residual_history ? h.hist_len : 0;

@@ -13,6 +13,17 @@ namespace ssv {
 
 constexpr int kBlock = 256;  // threads per block of the streaming kernels
 
+// Programmatic dependent launch: the iteration's kernels are launched so that the
+// next one in the stream may be scheduled before this one ends. Each waits
+// here for its predecessor's completion and memory (griddepcontrol.wait)
+// before touching any data, then lets its own successor start launching.
+// Launched without the attribute, both instructions have no effect.
+__device__ __forceinline__ void pdl_gate() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+
 // ---------------------------------------------------------------------------
 // Device-resident Krylov state. Scalars are double2 (real methods use .x).
 // ---------------------------------------------------------------------------
@@ -204,6 +215,7 @@ __global__ void __launch_bounds__(kBlock)
 k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const SV* __restrict__ v,
        const S* __restrict__ x, S* __restrict__ y, const S* __restrict__ b,
        const uint8_t* __restrict__ mask, KState* st, int op, RedBuf red, double2* out) {
+    pdl_gate();
     if (st && st->done) return;
     const int sub = threadIdx.x % LANES;
     const int rows_per_block = kBlock / LANES;
@@ -289,6 +301,7 @@ template <typename S>
 __global__ void __launch_bounds__(kBlock)
 k_dot(int n, const S* __restrict__ a, const S* __restrict__ b, int conj, KState* st, int op,
       RedBuf red, double2* out) {
+    pdl_gate();
     if (st && st->done && op != RED_STORE) return;
     double2 part = make_double2(0.0, 0.0);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -302,6 +315,7 @@ k_dot(int n, const S* __restrict__ a, const S* __restrict__ b, int conj, KState*
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
 k_norm2(int n, const S* __restrict__ a, RedBuf red, double2* out) {
+    pdl_gate();
     double2 part = make_double2(0.0, 0.0);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         part.x += ST<S>::norm2(a[i]);
@@ -316,6 +330,7 @@ template <typename S>
 __global__ void __launch_bounds__(kBlock)
 k_cg_update(int n, S* xb0, S* xb1, S* xb2, const S* __restrict__ p, const S* __restrict__ Ap,
             S* __restrict__ r, KState* st, RedBuf red) {
+    pdl_gate();
     if (st->done) return;
     const int brk = st->breakdown;
     const int cur = st->cur;
@@ -352,6 +367,7 @@ __global__ void __launch_bounds__(kBlock)
 k_cocr_update(int n, S* xb0, S* xb1, S* xb2, const S* __restrict__ p, const S* __restrict__ q,
               const S* __restrict__ qt, S* __restrict__ r, S* __restrict__ rt, KState* st,
               RedBuf red) {
+    pdl_gate();
     if (st->done) return;
     const int brk = st->breakdown;
     const int cur = st->cur;
@@ -386,6 +402,7 @@ k_cocr_update(int n, S* xb0, S* xb1, S* xb2, const S* __restrict__ p, const S* _
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
 k_pupdate(int n, const S* __restrict__ z, S* __restrict__ p, const KState* st) {
+    pdl_gate();
     if (st->done) return;
     const S beta = s_from2<S>(st->beta);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -397,6 +414,7 @@ template <typename S>
 __global__ void __launch_bounds__(kBlock)
 k_cocr_pq(int n, const S* __restrict__ rt, const S* __restrict__ t, S* __restrict__ p,
           S* __restrict__ q, const KState* st) {
+    pdl_gate();
     if (st->done) return;
     const S beta = s_from2<S>(st->beta);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -415,6 +433,7 @@ __global__ void k_loop_ctl(KState* st, cudaGraphConditionalHandle h, int use_con
 // ---------------------------------------------------------------------------
 template <typename S>
 __global__ void k_copy(int n, const S* __restrict__ a, S* __restrict__ b) {
+    pdl_gate();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
 }
 
@@ -422,6 +441,7 @@ __global__ void k_copy(int n, const S* __restrict__ a, S* __restrict__ b) {
 template <typename S>
 __global__ void k_scatter_perm(int n, const int* __restrict__ perm, const S* __restrict__ src,
                                S* __restrict__ dst, const uint8_t* __restrict__ mask) {
+    pdl_gate();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         S v = src[i];
         if (mask && !mask[i]) v = ST<S>::zero();
@@ -434,6 +454,7 @@ __global__ void k_scatter_perm(int n, const int* __restrict__ perm, const S* __r
 template <typename S>
 __global__ void k_gather_perm(int n, const int* __restrict__ perm, const S* __restrict__ src,
                               S* __restrict__ dst, const uint8_t* __restrict__ mask, int zero_masked) {
+    pdl_gate();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (mask && !mask[i]) {
             if (zero_masked) dst[i] = ST<S>::zero();
@@ -445,12 +466,14 @@ __global__ void k_gather_perm(int n, const int* __restrict__ perm, const S* __re
 
 template <typename S>
 __global__ void k_mask_zero(int n, S* __restrict__ a, const uint8_t* __restrict__ mask) {
+    pdl_gate();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         if (!mask[i]) a[i] = ST<S>::zero();
 }
 
 template <typename S>
 __global__ void k_scale_real(int n, S* __restrict__ a, const double* __restrict__ s) {
+    pdl_gate();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         a[i] = ST<S>::scale(s[i], a[i]);
 }
@@ -551,6 +574,7 @@ __global__ void __launch_bounds__(128)
 k_ic_fwd(int u0, int u1, const int* __restrict__ uoff, const int* __restrict__ rows,
          const int* __restrict__ Lrp, const int* __restrict__ Lci, const SL* __restrict__ Lv,
          const S* __restrict__ x, const double* __restrict__ sc, S* __restrict__ y, const KState* st) {
+    pdl_gate();
     if (st && st->done) return;
     const int u = u0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= u1) return;
@@ -572,6 +596,7 @@ __global__ void __launch_bounds__(128)
 k_ic_bwd(int u0, int u1, const int* __restrict__ uoff, const int* __restrict__ rows,
          const int* __restrict__ Urp, const int* __restrict__ Uci, const SL* __restrict__ Uv,
          const SL* __restrict__ inv_diag, const S* __restrict__ x, S* __restrict__ y, const KState* st) {
+    pdl_gate();
     if (st && st->done) return;
     const int u = u0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= u1) return;
@@ -609,6 +634,7 @@ k_ic_fwd_blk(int b0, int b1, const int* __restrict__ boff, const int* __restrict
              const int* __restrict__ eci, const SL* __restrict__ ev, const SL* __restrict__ iv, int tri,
              const SL* __restrict__ dv, const S* __restrict__ x, const double* __restrict__ sc,
              S* __restrict__ y, const KState* st) {
+    pdl_gate();
     if (st && st->done) return;
     const int lane = threadIdx.x % LANES;
     const int gw = (threadIdx.x & 31) / LANES;
@@ -644,6 +670,7 @@ __global__ void __launch_bounds__(128)
 k_ic_bwd_blk(int b0, int b1, const int* __restrict__ boff, const int* __restrict__ urp,
              const int* __restrict__ uci, const SL* __restrict__ uv, const SL* __restrict__ iv, int tri,
              const SL* __restrict__ inv, const S* __restrict__ x, S* __restrict__ y, const KState* st) {
+    pdl_gate();
     if (st && st->done) return;
     const int lane = threadIdx.x % LANES;
     const int gw = (threadIdx.x & 31) / LANES;
@@ -694,6 +721,7 @@ __global__ void __launch_bounds__(256)
 k_ic_fwd_cta(int nlev, const int* __restrict__ lev, const int* __restrict__ rows, const int* __restrict__ Lrp,
              const int* __restrict__ Lci, const SL* __restrict__ Lv, const S* __restrict__ x,
              const double* __restrict__ sc, S* y, const KState* st) {
+    pdl_gate();
     if (st && st->done) return;
     for (int l = 0; l < nlev; ++l) {
         const int q1 = lev[l + 1];
@@ -714,6 +742,7 @@ __global__ void __launch_bounds__(256)
 k_ic_bwd_cta(int nlev, const int* __restrict__ lev, const int* __restrict__ rows, const int* __restrict__ Urp,
              const int* __restrict__ Uci, const SL* __restrict__ Uv, const SL* __restrict__ inv_diag,
              const S* __restrict__ x, S* y, const KState* st) {
+    pdl_gate();
     if (st && st->done) return;
     for (int l = 0; l < nlev; ++l) {
         const int q1 = lev[l + 1];

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cstdlib>
 #include <memory>
 #include <string>
 
@@ -11,6 +12,32 @@
 namespace ssv {
 
 cudaStream_t stream();
+
+// Kernel launch with programmatic dependent launch allowed (the kernel must
+// start with pdl_gate()); SSV_PDL=0 launches without it.
+inline bool pdl_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("SSV_PDL");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v != 0;
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    SSV_CUDA(cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...));
+}
 
 // Sub-warp width of the CSR kernels from the mean row length.
 int pick_lanes(double nnz_per_row);

@@ -109,7 +109,7 @@ void launch_spmv(int shape, int n, const int* rp, const int* ci, const SV* v, co
     grid = std::max(1, std::min(grid, sm_count() * 8));
 #define SSV_SPMV_CASE(L, UU)                                                                          \
     if (lanes == L && u == UU) {                                                                      \
-        k_spmv<S, SV, L, MODE, UU><<<grid, kBlock, 0, s>>>(n, rp, ci, v, x, y, b, mask, st, op, red, out); \
+        launch_k(k_spmv<S, SV, L, MODE, UU>, grid, kBlock, s, n, rp, ci, v, x, y, b, mask, st, op, red, out); \
         SSV_LAUNCH_CHECK();                                                                           \
         return;                                                                                       \
     }
@@ -120,7 +120,7 @@ void launch_spmv(int shape, int n, const int* rp, const int* ci, const SV* v, co
     SSV_SPMV_CASE(4, 2)
     SSV_SPMV_CASE(8, 2)
 #undef SSV_SPMV_CASE
-    k_spmv<S, SV, 32, MODE, 1><<<grid, kBlock, 0, s>>>(n, rp, ci, v, x, y, b, mask, st, op, red, out);
+    launch_k(k_spmv<S, SV, 32, MODE, 1>, grid, kBlock, s, n, rp, ci, v, x, y, b, mask, st, op, red, out);
     SSV_LAUNCH_CHECK();
 }
 
@@ -490,10 +490,10 @@ static void launch_fwd_blk(const ICDevice<S>& ic, const SL* ev, const SL* iv, co
         const int units = g.b - g.a;
         if (units <= 0) continue;
         if (g.kind == 0)
-            k_ic_fwd_blk<S, SL, L><<<(units + per_cta - 1) / per_cta, 128, 0, s>>>(
+            launch_k(k_ic_fwd_blk<S, SL, L>, (units + per_cta - 1) / per_cta, 128, s, 
                 g.a, g.b, ic.uoff.get(), ic.erp.get(), ic.eci.get(), ev, iv, ic.tri, dv, x, sc, ic.tw.get(), st);
         else
-            k_ic_fwd_cta<S, SL><<<1, 256, 0, s>>>(units, ic.lev_f.get() + g.a, ic.rows_f.get(), ic.Lrp.get(),
+            launch_k(k_ic_fwd_cta<S, SL>, 1, 256, s, units, ic.lev_f.get() + g.a, ic.rows_f.get(), ic.Lrp.get(),
                                                   ic.Lci.get(), Lfull, x, sc, ic.tw.get(), st);
     }
 }
@@ -507,10 +507,10 @@ static void launch_bwd_blk(const ICDevice<S>& ic, const SL* uev, const SL* iv, c
         const int units = g.b - g.a;
         if (units <= 0) continue;
         if (g.kind == 0)
-            k_ic_bwd_blk<S, SL, L><<<(units + per_cta - 1) / per_cta, 128, 0, s>>>(
+            launch_k(k_ic_bwd_blk<S, SL, L>, (units + per_cta - 1) / per_cta, 128, s, 
                 g.a, g.b, ic.uoff.get(), ic.urpe.get(), ic.ucie.get(), uev, iv, ic.tri, inv, ic.tw.get(), y, st);
         else
-            k_ic_bwd_cta<S, SL><<<1, 256, 0, s>>>(units, ic.lev_b.get() + g.a, ic.rows_b.get(), ic.Urp.get(),
+            launch_k(k_ic_bwd_cta<S, SL>, 1, 256, s, units, ic.lev_b.get() + g.a, ic.rows_b.get(), ic.Urp.get(),
                                                   ic.Uci.get(), Ufull, inv, ic.tw.get(), y, st);
     }
 }
@@ -539,10 +539,10 @@ void ICDevice<S>::apply_fwd(const S* x, const KState* st, cudaStream_t s) const 
         const int units = g.second - g.first;
         if (units <= 0) continue;
         if (lo)
-            k_ic_fwd<S, SL><<<(units + 127) / 128, 128, 0, s>>>(g.first, g.second, uo, rows_f.get(), Lrp.get(),
+            launch_k(k_ic_fwd<S, SL>, (units + 127) / 128, 128, s, g.first, g.second, uo, rows_f.get(), Lrp.get(),
                                                                 Lci.get(), Lv_lo.get(), x, sc, tw.get(), st);
         else
-            k_ic_fwd<S, S><<<(units + 127) / 128, 128, 0, s>>>(g.first, g.second, uo, rows_f.get(), Lrp.get(),
+            launch_k(k_ic_fwd<S, S>, (units + 127) / 128, 128, s, g.first, g.second, uo, rows_f.get(), Lrp.get(),
                                                                Lci.get(), Lv.get(), x, sc, tw.get(), st);
     }
     SSV_LAUNCH_CHECK();
@@ -555,7 +555,7 @@ void ICDevice<S>::apply_bwd(S* y, const KState* st, cudaStream_t s) const {
     if (blk) {
         if (lo) { SSV_BLK_DISPATCH(launch_bwd_blk, SL, *this, uev_lo.get(), iv_lo.get(), inv_lo.get(), y, st, s) }
         else { SSV_BLK_DISPATCH(launch_bwd_blk, S, *this, uev.get(), iv.get(), inv.get(), y, st, s) }
-        if (sc) k_scale_real<S><<<grid_for(n, kBlock), kBlock, 0, s>>>(n, y, sc);
+        if (sc) launch_k(k_scale_real<S>, grid_for(n, kBlock), kBlock, s, n, y, sc);
         SSV_LAUNCH_CHECK();
         return;
     }
@@ -563,13 +563,13 @@ void ICDevice<S>::apply_bwd(S* y, const KState* st, cudaStream_t s) const {
         const int units = g.second - g.first;
         if (units <= 0) continue;
         if (lo)
-            k_ic_bwd<S, SL><<<(units + 127) / 128, 128, 0, s>>>(g.first, g.second, uo, rows_b.get(), Urp.get(),
+            launch_k(k_ic_bwd<S, SL>, (units + 127) / 128, 128, s, g.first, g.second, uo, rows_b.get(), Urp.get(),
                                                                 Uci.get(), Uv_lo.get(), inv_lo.get(), tw.get(), y, st);
         else
-            k_ic_bwd<S, S><<<(units + 127) / 128, 128, 0, s>>>(g.first, g.second, uo, rows_b.get(), Urp.get(),
+            launch_k(k_ic_bwd<S, S>, (units + 127) / 128, 128, s, g.first, g.second, uo, rows_b.get(), Urp.get(),
                                                                Uci.get(), Uv.get(), inv.get(), tw.get(), y, st);
     }
-    if (sc) k_scale_real<S><<<grid_for(n, kBlock), kBlock, 0, s>>>(n, y, sc);
+    if (sc) launch_k(k_scale_real<S>, grid_for(n, kBlock), kBlock, s, n, y, sc);
     SSV_LAUNCH_CHECK();
 }
 
@@ -663,18 +663,18 @@ static void run_krylov(ssv_solver* sv, int method, const ssv_config& cfg, const 
 
     // b and x into the working numbering, constrained entries zeroed
     if (perm) {
-        k_scatter_perm<S><<<g, kBlock, 0, s>>>(n, perm, d_b, w.bw.get(), fd);
-        k_scatter_perm<S><<<g, kBlock, 0, s>>>(n, perm, d_x, w.xb[0].get(), fd);
+        launch_k(k_scatter_perm<S>, g, kBlock, s, n, perm, d_b, w.bw.get(), fd);
+        launch_k(k_scatter_perm<S>, g, kBlock, s, n, perm, d_x, w.xb[0].get(), fd);
     } else {
-        k_gather_perm<S><<<g, kBlock, 0, s>>>(n, nullptr, d_b, w.bw.get(), fd, 1);
-        k_gather_perm<S><<<g, kBlock, 0, s>>>(n, nullptr, d_x, w.xb[0].get(), fd, 1);
+        launch_k(k_gather_perm<S>, g, kBlock, s, n, nullptr, d_b, w.bw.get(), fd, 1);
+        launch_k(k_gather_perm<S>, g, kBlock, s, n, nullptr, d_x, w.xb[0].get(), fd, 1);
     }
     SSV_LAUNCH_CHECK();
     // prepare_iteration (iterative_solver.hpp:135-180)
     launch_spmv<S, S, 2>(lanes, n, wrp, wci, wv, w.xb[0].get(), w.r.get(), w.bw.get(), nullptr, nullptr,
                          RED_STORE, red, nullptr, s);
-    k_norm2<S><<<g, kBlock, 0, s>>>(n, w.bw.get(), red, w.scal.get());
-    k_norm2<S><<<g, kBlock, 0, s>>>(n, w.r.get(), red, w.scal.get() + 1);
+    launch_k(k_norm2<S>, g, kBlock, s, n, w.bw.get(), red, w.scal.get());
+    launch_k(k_norm2<S>, g, kBlock, s, n, w.r.get(), red, w.scal.get() + 1);
     SSV_LAUNCH_CHECK();
     nk += 5;
     double2 nrm[2];
@@ -722,8 +722,8 @@ static void run_krylov(ssv_solver* sv, int method, const ssv_config& cfg, const 
     if (method == SSV_METHOD_CG || method == SSV_METHOD_ICCG) {
         // z = M^{-1} r, rho = (r, z), p = z (cg_solver.hpp:428-432)
         if (ic) ic->apply(w.r.get(), w.z.get(), nullptr, s);
-        k_dot<S><<<g, kBlock, 0, s>>>(n, w.r.get(), z, cfg.conjugate, nullptr, RED_STORE, red, &dst->rho);
-        k_copy<S><<<g, kBlock, 0, s>>>(n, z, w.p.get());
+        launch_k(k_dot<S>, g, kBlock, s, n, w.r.get(), z, cfg.conjugate, nullptr, RED_STORE, red, &dst->rho);
+        launch_k(k_copy<S>, g, kBlock, s, n, z, w.p.get());
         SSV_LAUNCH_CHECK();
         nk += 2 + (ic ? ic->kernels_per_apply() : 0);
         key = "cg" + std::to_string(method) + ";" + std::to_string(n) + ";" + std::to_string(lanes) + ";" +
@@ -735,34 +735,34 @@ static void run_krylov(ssv_solver* sv, int method, const ssv_config& cfg, const 
         build_graph_loop(sv->loop, key, [&](cudaGraphConditionalHandle hc, int use_cond) {
             launch_spmv<S, S, 1>(lanes, n, wrp, wci, wv, w.p.get(), w.Ap.get(), nullptr, nullptr, dst,
                                  RED_CG_ALPHA, red, nullptr, s);
-            k_cg_update<S><<<g, kBlock, 0, s>>>(n, w.xb[0].get(), w.xb[1].get(), w.xb[2].get(), w.p.get(),
+            launch_k(k_cg_update<S>, g, kBlock, s, n, w.xb[0].get(), w.xb[1].get(), w.xb[2].get(), w.p.get(),
                                                w.Ap.get(), w.r.get(), dst, red);
             if (ic) ic->apply(w.r.get(), w.z.get(), dst, s);
-            k_dot<S><<<g, kBlock, 0, s>>>(n, w.r.get(), z, cfg.conjugate, dst, RED_CG_BETA, red, nullptr);
-            k_pupdate<S><<<g, kBlock, 0, s>>>(n, z, w.p.get(), dst);
+            launch_k(k_dot<S>, g, kBlock, s, n, w.r.get(), z, cfg.conjugate, dst, RED_CG_BETA, red, nullptr);
+            launch_k(k_pupdate<S>, g, kBlock, s, n, z, w.p.get(), dst);
             k_loop_ctl<<<1, 32, 0, s>>>(dst, hc, use_cond);
             SSV_LAUNCH_CHECK();
         });
     } else {  // COCR without preconditioner (sparsesolv_solvers.hpp:120-123)
         S* rt = w.z.get();
         S* q = w.Ap.get();
-        k_copy<S><<<g, kBlock, 0, s>>>(n, w.r.get(), rt);
-        k_copy<S><<<g, kBlock, 0, s>>>(n, rt, w.p.get());
+        launch_k(k_copy<S>, g, kBlock, s, n, w.r.get(), rt);
+        launch_k(k_copy<S>, g, kBlock, s, n, rt, w.p.get());
         launch_spmv<S, S, 0>(lanes, n, wrp, wci, wv, w.p.get(), q, nullptr, nullptr, nullptr, RED_STORE, red,
                              nullptr, s);
- k_dot<S><<<g, kBlock, 0, s>>>(n, rt, q, 0, nullptr, RED_STORE, red, &dst->rho);
+ launch_k(k_dot<S>, g, kBlock, s, n, rt, q, 0, nullptr, RED_STORE, red, &dst->rho);
         SSV_LAUNCH_CHECK();
         nk += 4;
         key = "cocr;" + std::to_string(n) + ";" + std::to_string(lanes) + ";" + ptr_key(wrp) + ptr_key(wv) +
               ptr_key(w.r.get()) + ptr_key(dst) + ptr_key(red.partials);
         build_graph_loop(sv->loop, key, [&](cudaGraphConditionalHandle hc, int use_cond) {
             // qt = q (identity preconditioner); mu = qt^T q
-            k_dot<S><<<g, kBlock, 0, s>>>(n, q, q, 0, dst, RED_COCR_ALPHA, red, nullptr);
-            k_cocr_update<S><<<g, kBlock, 0, s>>>(n, w.xb[0].get(), w.xb[1].get(), w.xb[2].get(), w.p.get(), q,
+            launch_k(k_dot<S>, g, kBlock, s, n, q, q, 0, dst, RED_COCR_ALPHA, red, nullptr);
+            launch_k(k_cocr_update<S>, g, kBlock, s, n, w.xb[0].get(), w.xb[1].get(), w.xb[2].get(), w.p.get(), q,
                                                  q, w.r.get(), rt, dst, red);
             launch_spmv<S, S, 3>(lanes, n, wrp, wci, wv, rt, w.t.get(), nullptr, nullptr, dst, RED_COCR_BETA,
                                  red, nullptr, s);
-            k_cocr_pq<S><<<g, kBlock, 0, s>>>(n, rt, w.t.get(), w.p.get(), q, dst);
+            launch_k(k_cocr_pq<S>, g, kBlock, s, n, rt, w.t.get(), w.p.get(), q, dst);
             k_loop_ctl<<<1, 32, 0, s>>>(dst, hc, use_cond);
             SSV_LAUNCH_CHECK();
         });
@@ -788,7 +788,7 @@ static void run_krylov(ssv_solver* sv, int method, const ssv_config& cfg, const 
     } else {
         xsrc = w.xb[xbuf].get();
     }
-    k_gather_perm<S><<<g, kBlock, 0, s>>>(n, perm, xsrc, d_x, fd, 0);
+    launch_k(k_gather_perm<S>, g, kBlock, s, n, perm, xsrc, d_x, fd, 0);
     SSV_LAUNCH_CHECK();
     nk += 1;
     res->kernel_launches = nk + (int64_t)sv->loop.body_nodes * h.loops;
@@ -892,7 +892,7 @@ static void profile_krylov(ssv_solver* sv, int method, const ssv_config& cfg, in
                                  red, nullptr, s);
         });
         timed("axpy_norm", 6 * N * sb, 1, [&] {
-            k_cg_update<S><<<g, kBlock, 0, s>>>(n, w.xb[0].get(), w.xb[1].get(), w.xb[2].get(), w.p.get(), w.Ap.get(),
+            launch_k(k_cg_update<S>, g, kBlock, s, n, w.xb[0].get(), w.xb[1].get(), w.xb[2].get(), w.p.get(), w.Ap.get(),
                                                w.r.get(), dst, red);
         });
         if (ic) {
@@ -906,24 +906,24 @@ static void profile_krylov(ssv_solver* sv, int method, const ssv_config& cfg, in
                   kb + (ic->scaled_apply ? 1 : 0), [&] { ic->apply_bwd(w.z.get(), dst, s); });
         }
         timed("dot_beta", 2 * N * sb, 1, [&] {
-            k_dot<S><<<g, kBlock, 0, s>>>(n, w.r.get(), z, cfg.conjugate, dst, RED_CG_BETA, red, nullptr);
+            launch_k(k_dot<S>, g, kBlock, s, n, w.r.get(), z, cfg.conjugate, dst, RED_CG_BETA, red, nullptr);
         });
-        timed("p_update", 3 * N * sb, 1, [&] { k_pupdate<S><<<g, kBlock, 0, s>>>(n, z, w.p.get(), dst); });
+        timed("p_update", 3 * N * sb, 1, [&] { launch_k(k_pupdate<S>, g, kBlock, s, n, z, w.p.get(), dst); });
     } else if (method == SSV_METHOD_COCR) {
         S* rt = w.z.get();
         S* q = w.Ap.get();
         timed("dot_mu", 2 * N * sb, 1, [&] {
-            k_dot<S><<<g, kBlock, 0, s>>>(n, q, q, 0, dst, RED_COCR_ALPHA, red, nullptr);
+            launch_k(k_dot<S>, g, kBlock, s, n, q, q, 0, dst, RED_COCR_ALPHA, red, nullptr);
         });
         timed("update3_norm", 8 * N * sb, 1, [&] {
-            k_cocr_update<S><<<g, kBlock, 0, s>>>(n, w.xb[0].get(), w.xb[1].get(), w.xb[2].get(), w.p.get(), q, q,
+            launch_k(k_cocr_update<S>, g, kBlock, s, n, w.xb[0].get(), w.xb[1].get(), w.xb[2].get(), w.p.get(), q, q,
                                                  w.r.get(), rt, dst, red);
         });
         timed("spmv_dot", Z * (4 + sb) + (N + 1) * 4 + 2 * N * sb, 1, [&] {
             launch_spmv<S, S, 3>(lanes, n, wrp, wci, wv, rt, w.t.get(), nullptr, nullptr, dst, RED_COCR_BETA, red,
                                  nullptr, s);
         });
-        timed("pq_update", 6 * N * sb, 1, [&] { k_cocr_pq<S><<<g, kBlock, 0, s>>>(n, rt, w.t.get(), w.p.get(), q, dst); });
+        timed("pq_update", 6 * N * sb, 1, [&] { launch_k(k_cocr_pq<S>, g, kBlock, s, n, rt, w.t.get(), w.p.get(), q, dst); });
     } else {
         fail(SSV_ERR_INVALID_ARG, "ssv_solver_profile: method not profiled");
     }
@@ -986,12 +986,12 @@ void ic_apply_dev(ssv_precond* p, const S* x, S* y, const KState* st, cudaStream
     S* xw = reinterpret_cast<S*>(p->xw.get());
     S* yw = reinterpret_cast<S*>(p->yw.get());
     if (ic.abmc) {
-        k_scatter_perm<S><<<g, kBlock, 0, s>>>(n, ic.perm.get(), x, xw, nullptr);
+        launch_k(k_scatter_perm<S>, g, kBlock, s, n, ic.perm.get(), x, xw, nullptr);
         ic.apply(xw, yw, st, s);
-        k_gather_perm<S><<<g, kBlock, 0, s>>>(n, ic.perm.get(), yw, y, fd, 1);
+        launch_k(k_gather_perm<S>, g, kBlock, s, n, ic.perm.get(), yw, y, fd, 1);
     } else {
         ic.apply(x, y, st, s);
-        if (fd) k_mask_zero<S><<<g, kBlock, 0, s>>>(n, y, fd);
+        if (fd) launch_k(k_mask_zero<S>, g, kBlock, s, n, y, fd);
     }
     SSV_LAUNCH_CHECK();
 }
