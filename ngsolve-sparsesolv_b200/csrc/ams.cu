@@ -893,6 +893,7 @@ struct AmsState {
     ForkSet forks;  // the y and z nodal V-cycles run beside the x one
     TailSet tails[4];
     bool tri = true;  // nodal V-cycles in lockstep launches (SSV_AMS_TRI=0: three branches)
+    int pi_lanes[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};  // Pi restrict / prolong lanes by NV slot (0 = untuned)
 };
 
 void ams_free(AmsState* a) { delete a; }
@@ -1125,7 +1126,8 @@ static void pi_prolong_l(const AmsState& a, const T* gx, const T* gy, const T* g
 template <typename T, int NV>
 static void pi_restrict(const AmsState& a, const double* r, T* ox, T* oy, T* oz, const KState* st,
                         cudaStream_t s) {
-    switch (a.Gt.lanes_for(NV)) {
+    const int tuned = a.pi_lanes[0][DevCsr::nv_slot(NV)];
+    switch (tuned ? tuned : a.Gt.lanes) {
         case 2: pi_restrict_l<T, NV, 2>(a, r, ox, oy, oz, st, s); break;
         case 4: pi_restrict_l<T, NV, 4>(a, r, ox, oy, oz, st, s); break;
         case 8: pi_restrict_l<T, NV, 8>(a, r, ox, oy, oz, st, s); break;
@@ -1137,7 +1139,8 @@ static void pi_restrict(const AmsState& a, const double* r, T* ox, T* oy, T* oz,
 template <typename T, int NV>
 static void pi_prolong(const AmsState& a, const T* gx, const T* gy, const T* gz, double* x, const KState* st,
                        cudaStream_t s) {
-    switch (a.G.lanes_for(NV)) {
+    const int tuned = a.pi_lanes[1][DevCsr::nv_slot(NV)];
+    switch (tuned ? tuned : a.G.lanes) {
         case 2: pi_prolong_l<T, NV, 2>(a, gx, gy, gz, x, st, s); break;
         case 4: pi_prolong_l<T, NV, 4>(a, gx, gy, gz, x, st, s); break;
         case 8: pi_prolong_l<T, NV, 8>(a, gx, gy, gz, x, st, s); break;
@@ -1303,11 +1306,13 @@ static int max_unroll() {
 // the form the cycle runs them in (smoothing reads the same streams); the
 // transfers as y = A x.
 template <typename TV, typename TX, typename TY, int NV>
-static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1,
+                     bool force_cold = false) {
     if (A.n == 0 || A.nnz == 0) return;
     const TV* v = A.val<TV>();
-    // a matrix much larger than a quarter of L2 streams from HBM in the cycle: tune it cold
-    const bool cold = (double)A.nnz * (4 + sizeof(TV)) > (double)(32 << 20);
+    // a matrix much larger than a quarter of L2 streams from HBM in the cycle, and
+    // so do the fine-level transfers between the fine passes: tune those cold
+    const bool cold = force_cold || (double)A.nnz * (4 + sizeof(TV)) > (double)(32 << 20);
     float best = 1e30f;
     int pick = A.lanes, pick_u = 1;
     for (int i = 0; i < kShapes; ++i) {
@@ -1338,11 +1343,58 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
                      (long long)A.nnz, NV, cold ? "cold" : "warm", pick, pick_u, 1e3 * best / (cold ? 5 : 4));
 }
 
+// lanes of the Pi transfers (one pass over G's pattern, three coefficient
+// arrays), timed cold like the other fine-level transfers
+template <typename T, int NV>
+static void tune_pi(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+    const int slot = DevCsr::nv_slot(NV);
+    const int cand[5] = {2, 4, 8, 16, 32};
+    T* o1 = a.rs[1].as<T>();
+    T* o2 = a.rs[2].as<T>();
+    T* o3 = a.rs[3].as<T>();
+    for (int dir = 0; dir < 2; ++dir) {
+        float best = 1e30f;
+        int pick = 0;
+        for (int L : cand) {
+            auto launch = [&] {
+                if (dir == 0) {
+                    switch (L) {
+                        case 2: pi_restrict_l<T, NV, 2>(a, a.r.get(), o1, o2, o3, nullptr, s); break;
+                        case 4: pi_restrict_l<T, NV, 4>(a, a.r.get(), o1, o2, o3, nullptr, s); break;
+                        case 8: pi_restrict_l<T, NV, 8>(a, a.r.get(), o1, o2, o3, nullptr, s); break;
+                        case 16: pi_restrict_l<T, NV, 16>(a, a.r.get(), o1, o2, o3, nullptr, s); break;
+                        default: pi_restrict_l<T, NV, 32>(a, a.r.get(), o1, o2, o3, nullptr, s); break;
+                    }
+                } else {
+                    switch (L) {
+                        case 2: pi_prolong_l<T, NV, 2>(a, o1, o2, o3, a.xb.get(), nullptr, s); break;
+                        case 4: pi_prolong_l<T, NV, 4>(a, o1, o2, o3, a.xb.get(), nullptr, s); break;
+                        case 8: pi_prolong_l<T, NV, 8>(a, o1, o2, o3, a.xb.get(), nullptr, s); break;
+                        case 16: pi_prolong_l<T, NV, 16>(a, o1, o2, o3, a.xb.get(), nullptr, s); break;
+                        default: pi_prolong_l<T, NV, 32>(a, o1, o2, o3, a.xb.get(), nullptr, s); break;
+                    }
+                }
+            };
+            launch();
+            const float ms = time_launches(launch, 5, true, s, e0, e1, true);
+            if (ms < best) {
+                best = ms;
+                pick = L;
+            }
+        }
+        a.pi_lanes[dir][slot] = pick;
+        if (std::getenv("SSV_AMS_TUNE_LOG"))
+            std::fprintf(stderr, "ams tune: Pi %s nv=%d cold -> lanes %d (%.2f us)\n", dir ? "prolong" : "restrict", NV,
+                         pick, 1e3 * best / 5);
+    }
+}
+
 template <typename T, int NV>
 static void tune_all_nv(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
     tune_csr<double, double, double, NV>(a.A_bc, a.xa.get(), a.xb.get(), a.r.get(), s, e0, e1);
-    tune_csr<double, double, T, NV>(a.Gt, a.r.get(), a.rs[0].as<T>(), nullptr, s, e0, e1);
-    tune_csr<double, T, double, NV>(a.G, a.rs[0].as<T>(), a.xb.get(), nullptr, s, e0, e1);
+    tune_csr<double, double, T, NV>(a.Gt, a.r.get(), a.rs[0].as<T>(), nullptr, s, e0, e1, true);
+    tune_csr<double, T, double, NV>(a.G, a.rs[0].as<T>(), a.xb.get(), nullptr, s, e0, e1, true);
+    tune_pi<T, NV>(a, s, e0, e1);
     for (int sub = 0; sub < 4; ++sub) {
         auto& L = a.amg[sub];
         for (size_t l = 0; l < L.size(); ++l) {
