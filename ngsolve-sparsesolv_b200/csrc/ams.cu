@@ -1292,6 +1292,17 @@ static float time_launches(F&& launch, int reps, bool cold, cudaStream_t s, cuda
     return total;
 }
 
+// matrices larger than this are tuned cold (SSV_AMS_COLD_TUNE_MB, default 32;
+// 0.5 and 2 measured the same cycle time at 40^3)
+static double cold_tune_bytes() {
+    static double v = -1.0;
+    if (v < 0.0) {
+        const char* e = std::getenv("SSV_AMS_COLD_TUNE_MB");
+        v = (e ? std::max(0.0, std::atof(e)) : 32.0) * (1 << 20);
+    }
+    return v;
+}
+
 // largest rows-per-group the tuner may pick (SSV_AMS_MAX_UNROLL, default 4)
 static int max_unroll() {
     static int v = 0;
@@ -1310,9 +1321,9 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
                      bool force_cold = false) {
     if (A.n == 0 || A.nnz == 0) return;
     const TV* v = A.val<TV>();
-    // a matrix much larger than a quarter of L2 streams from HBM in the cycle, and
-    // so do the fine-level transfers between the fine passes: tune those cold
-    const bool cold = force_cold || (double)A.nnz * (4 + sizeof(TV)) > (double)(32 << 20);
+    // A matrix much larger than a quarter of L2 streams from HBM in the cycle:
+    // time it cold; the rest back to back.
+    const bool cold = force_cold || (double)A.nnz * (4 + sizeof(TV)) > (double)(cold_tune_bytes());
     float best = 1e30f;
     int pick = A.lanes, pick_u = 1;
     for (int i = 0; i < kShapes; ++i) {
