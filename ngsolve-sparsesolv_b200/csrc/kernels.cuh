@@ -757,4 +757,92 @@ k_ic_bwd_cta(int nlev, const int* __restrict__ lev, const int* __restrict__ rows
     }
 }
 
+// Oversized ABMC block, staged: the block's rows, their L (forward) or U
+// (backward) entries and the values of the couplings to other blocks (final
+// before the launch) are copied into shared memory first, so the chain of
+// level sets touches only shared memory. Same per-row arithmetic, in the same
+// order, as k_ic_fwd_cta / k_ic_bwd_cta. Per-row entry lists: srp (by position
+// in rows[]), value index ssrc, column scol, and sloc = the column's position
+// within the block (relative to lev[0]) or -1 for a coupling outside it.
+template <typename S, typename SL>
+struct StagedSmem {
+    S* ys;
+    S* xs;
+    S* eext;
+    SL* dg;
+    SL* ev;
+    int* eloc;
+    int* slev;
+    int* srow;
+};
+
+__host__ __device__ inline size_t staged_align(size_t b) { return (b + 15) & ~size_t(15); }
+
+template <typename S, typename SL>
+__host__ __device__ inline size_t staged_bytes(int nr, int ne, int nlev) {
+    return 2 * staged_align((size_t)nr * sizeof(S)) + staged_align((size_t)ne * sizeof(S)) +
+           staged_align((size_t)nr * sizeof(SL)) + staged_align((size_t)ne * sizeof(SL)) +
+           staged_align((size_t)ne * 4) + staged_align((size_t)(nlev + 1) * 4) + staged_align((size_t)(nr + 1) * 4);
+}
+
+template <typename S, typename SL, bool FWD>
+__global__ void __launch_bounds__(256)
+k_ic_sweep_staged(int nlev, const int* __restrict__ lev, const int* __restrict__ rows, const int* __restrict__ srp,
+                  const int* __restrict__ ssrc, const int* __restrict__ scol, const int* __restrict__ sloc,
+                  const int* __restrict__ Lrp, const SL* __restrict__ vals, const SL* __restrict__ inv_diag,
+                  const S* __restrict__ x, const double* __restrict__ sc, S* y, const KState* st) {
+    pdl_gate();
+    if (st && st->done) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int qa = lev[0], qb = lev[nlev];
+    const int nr = qb - qa;
+    const int ea = srp[qa], ne = srp[qb] - ea;
+    unsigned char* p = smem;
+    S* ys = reinterpret_cast<S*>(p);   p += staged_align((size_t)nr * sizeof(S));
+    S* xs = reinterpret_cast<S*>(p);   p += staged_align((size_t)nr * sizeof(S));
+    S* eext = reinterpret_cast<S*>(p); p += staged_align((size_t)ne * sizeof(S));
+    SL* dg = reinterpret_cast<SL*>(p); p += staged_align((size_t)nr * sizeof(SL));
+    SL* ev = reinterpret_cast<SL*>(p); p += staged_align((size_t)ne * sizeof(SL));
+    int* eloc = reinterpret_cast<int*>(p); p += staged_align((size_t)ne * 4);
+    int* slev = reinterpret_cast<int*>(p); p += staged_align((size_t)(nlev + 1) * 4);
+    int* srow = reinterpret_cast<int*>(p);
+    for (int l = threadIdx.x; l <= nlev; l += blockDim.x) slev[l] = lev[l] - qa;
+    for (int q = threadIdx.x; q <= nr; q += blockDim.x) srow[q] = srp[qa + q] - ea;
+    for (int q = threadIdx.x; q < nr; q += blockDim.x) {
+        const int i = rows[qa + q];
+        if constexpr (FWD) {
+            S v = x[i];
+            if (sc) v = ST<S>::scale(sc[i], v);
+            xs[q] = v;
+            dg[q] = vals[Lrp[i + 1] - 1];
+        } else {
+            xs[q] = x[i];
+            dg[q] = inv_diag[i];
+        }
+    }
+    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        const int loc = sloc[ea + e];
+        eloc[e] = loc;
+        ev[e] = vals[ssrc[ea + e]];
+        eext[e] = loc < 0 ? y[scol[ea + e]] : ST<S>::zero();
+    }
+    __syncthreads();
+    for (int l = 0; l < nlev; ++l) {
+        const int q1 = slev[l + 1];
+        for (int q = slev[l] + threadIdx.x; q < q1; q += blockDim.x) {
+            S s = FWD ? xs[q] : ST<S>::zero();
+            const int e1 = srow[q + 1];
+            for (int e = srow[q]; e < e1; ++e) {
+                const int loc = eloc[e];
+                const S yv = loc < 0 ? eext[e] : ys[loc];
+                s = s - hi_of_any(ev[e]) * yv;
+            }
+            if constexpr (FWD) ys[q] = ST<S>::div(s, hi_of_any(dg[q]));
+            else ys[q] = s * hi_of_any(dg[q]) + xs[q];
+        }
+        __syncthreads();
+    }
+    for (int q = threadIdx.x; q < nr; q += blockDim.x) y[rows[qa + q]] = ys[q];
+}
+
 }  // namespace ssv

@@ -205,9 +205,12 @@ struct ICDevice {
     // rows_f / rows_b lists (one level of an oversized block; factorisation),
     // kind 2 = an oversized block swept by one CTA over the level offsets
     // lev_f / lev_b [a, b] (apply)
-    struct Launch { int kind, a, b; };
+    struct Launch { int kind, a, b, smem = 0; };  // smem > 0: oversized block swept staged (bytes)
     std::vector<Launch> fwd_blk, bwd_blk, fwd_cta, bwd_cta;
     DevBuf<int> lev_f, lev_b;
+    // staged sweeps of oversized blocks: per position in rows_f / rows_b, the
+    // row's entries (value index, column, position in the block or -1)
+    DevBuf<int> sf_rp, sf_src, sf_col, sf_loc, sb_rp, sb_src, sb_col, sb_loc;
     DevBuf<int> erp, eci, esrc, urpe, ucie, usrce, isrc, dsrc;
     DevBuf<S> ev, uev, iv, dv;
     DevBuf<SL> ev_lo, uev_lo, iv_lo, dv_lo;

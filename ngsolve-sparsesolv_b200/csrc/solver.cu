@@ -261,6 +261,10 @@ void ICDevice<S>::build_pattern(int n_, const std::vector<int>& rp, const std::v
         std::vector<int> h_erp(n + 1, 0), h_eci, h_esrc, h_urp(n + 1, 0), h_uci, h_usrc, h_dsrc(n);
         std::vector<int> h_isrc((size_t)num_blocks * tri, -1);
         std::vector<int> h_rows_f, h_rows_b, h_lev_f, h_lev_b;
+        std::vector<int> h_sf_rp(1, 0), h_sf_src, h_sf_col, h_sf_loc, h_sb_rp(1, 0), h_sb_src, h_sb_col, h_sb_loc;
+        std::vector<int> pos;
+        int smem_optin = 0;
+        SSV_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, 0));
         h_eci.reserve(lci.size());
         h_esrc.reserve(lci.size());
         h_uci.reserve(uci.size());
@@ -313,6 +317,7 @@ void ICDevice<S>::build_pattern(int n_, const std::vector<int>& rp, const std::v
             std::vector<int>& lv = fwd ? h_lev_f : h_lev_b;
             const int p0 = (int)lv.size();
             lv.push_back((int)rows.size());
+            const int qa = (int)rows.size();
             for (int l = 0; l < nl; ++l) {
                 const int a = (int)rows.size();
                 for (int i = r0; i < r1; ++i)
@@ -320,7 +325,30 @@ void ICDevice<S>::build_pattern(int n_, const std::vector<int>& rp, const std::v
                 (fwd ? fwd_blk : bwd_blk).push_back({1, a, (int)rows.size()});
                 lv.push_back((int)rows.size());
             }
-            (fwd ? fwd_cta : bwd_cta).push_back({2, p0, p0 + nl});
+            // staged copy: each row's entries in sweep order, couplings inside
+            // the block by position, the others by column
+            const int qb = (int)rows.size();
+            pos.assign(m, -1);
+            for (int q = qa; q < qb; ++q) pos[rows[q] - r0] = q - qa;
+            std::vector<int>& srp = fwd ? h_sf_rp : h_sb_rp;
+            std::vector<int>& ssrc = fwd ? h_sf_src : h_sb_src;
+            std::vector<int>& scol = fwd ? h_sf_col : h_sb_col;
+            std::vector<int>& sloc = fwd ? h_sf_loc : h_sb_loc;
+            const int e0 = (int)ssrc.size();
+            for (int q = qa; q < qb; ++q) {
+                const int i = rows[q];
+                const int ka = fwd ? lrp[i] : urp[i] + 1, kb = fwd ? lrp[i + 1] - 1 : urp[i + 1];
+                for (int k = ka; k < kb; ++k) {
+                    const int c = fwd ? lci[k] : uci[k];
+                    ssrc.push_back(k);
+                    scol.push_back(c);
+                    sloc.push_back(c >= r0 && c < r1 ? pos[c - r0] : -1);
+                }
+                srp.push_back((int)ssrc.size());
+            }
+            const size_t bytes = staged_bytes<S, S>(qb - qa, (int)ssrc.size() - e0, nl);
+            const int smem = bytes <= (size_t)smem_optin ? (int)bytes : 0;
+            (fwd ? fwd_cta : bwd_cta).push_back({2, p0, p0 + nl, smem});
         };
         auto add_colour = [&](int c, bool fwd) {
             const int b0 = sched_color_offsets[c], b1 = sched_color_offsets[c + 1];
@@ -354,6 +382,18 @@ void ICDevice<S>::build_pattern(int n_, const std::vector<int>& rp, const std::v
         if (!h_rows_b.empty()) rows_b.upload(h_rows_b.data(), h_rows_b.size(), s);
         if (!h_lev_f.empty()) lev_f.upload(h_lev_f.data(), h_lev_f.size(), s);
         if (!h_lev_b.empty()) lev_b.upload(h_lev_b.data(), h_lev_b.size(), s);
+        auto up = [&](DevBuf<int>& d, const std::vector<int>& h) {
+            if (!h.empty()) d.upload(h.data(), h.size(), s);
+        };
+        up(sf_rp, h_sf_rp); up(sf_src, h_sf_src); up(sf_col, h_sf_col); up(sf_loc, h_sf_loc);
+        up(sb_rp, h_sb_rp); up(sb_src, h_sb_src); up(sb_col, h_sb_col); up(sb_loc, h_sb_loc);
+        if (smem_optin > 0) {
+            using SLo = typename ST<S>::lo;
+            SSV_CUDA(cudaFuncSetAttribute(k_ic_sweep_staged<S, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
+            SSV_CUDA(cudaFuncSetAttribute(k_ic_sweep_staged<S, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
+            SSV_CUDA(cudaFuncSetAttribute(k_ic_sweep_staged<S, SLo, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
+            SSV_CUDA(cudaFuncSetAttribute(k_ic_sweep_staged<S, SLo, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
+        }
         ev.alloc(h_eci.size()); uev.alloc(h_uci.size()); iv.alloc(h_isrc.size()); dv.alloc(n);
     }
     built = true;
@@ -481,6 +521,22 @@ int ICDevice<S>::factorize(const S* vals, const ssv_config& cfg) {
     return nk;
 }
 
+// one CTA of 256 threads with `smem` bytes of dynamic shared memory, PDL allowed
+template <typename... KArgs, typename... Args>
+static void launch_staged(void (*k)(KArgs...), int smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    SSV_CUDA(cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...));
+}
+
 template <typename S, typename SL, int L>
 static void launch_fwd_blk(const ICDevice<S>& ic, const SL* ev, const SL* iv, const SL* dv, const S* x,
                            const double* sc, const KState* st, cudaStream_t s) {
@@ -492,6 +548,10 @@ static void launch_fwd_blk(const ICDevice<S>& ic, const SL* ev, const SL* iv, co
         if (g.kind == 0)
             launch_k(k_ic_fwd_blk<S, SL, L>, (units + per_cta - 1) / per_cta, 128, s, 
                 g.a, g.b, ic.uoff.get(), ic.erp.get(), ic.eci.get(), ev, iv, ic.tri, dv, x, sc, ic.tw.get(), st);
+        else if (g.smem > 0)
+            launch_staged(k_ic_sweep_staged<S, SL, true>, g.smem, s, units, ic.lev_f.get() + g.a, ic.rows_f.get(),
+                          ic.sf_rp.get(), ic.sf_src.get(), ic.sf_col.get(), ic.sf_loc.get(), ic.Lrp.get(), Lfull,
+                          (const SL*)nullptr, x, sc, ic.tw.get(), st);
         else
             launch_k(k_ic_fwd_cta<S, SL>, 1, 256, s, units, ic.lev_f.get() + g.a, ic.rows_f.get(), ic.Lrp.get(),
                                                   ic.Lci.get(), Lfull, x, sc, ic.tw.get(), st);
@@ -509,6 +569,10 @@ static void launch_bwd_blk(const ICDevice<S>& ic, const SL* uev, const SL* iv, c
         if (g.kind == 0)
             launch_k(k_ic_bwd_blk<S, SL, L>, (units + per_cta - 1) / per_cta, 128, s, 
                 g.a, g.b, ic.uoff.get(), ic.urpe.get(), ic.ucie.get(), uev, iv, ic.tri, inv, ic.tw.get(), y, st);
+        else if (g.smem > 0)
+            launch_staged(k_ic_sweep_staged<S, SL, false>, g.smem, s, units, ic.lev_b.get() + g.a, ic.rows_b.get(),
+                          ic.sb_rp.get(), ic.sb_src.get(), ic.sb_col.get(), ic.sb_loc.get(), (const int*)nullptr,
+                          Ufull, inv, (const S*)ic.tw.get(), (const double*)nullptr, y, st);
         else
             launch_k(k_ic_bwd_cta<S, SL>, 1, 256, s, units, ic.lev_b.get() + g.a, ic.rows_b.get(), ic.Urp.get(),
                                                   ic.Uci.get(), Ufull, inv, ic.tw.get(), y, st);
