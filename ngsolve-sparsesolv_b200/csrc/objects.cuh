@@ -205,12 +205,19 @@ struct ICDevice {
     // rows_f / rows_b lists (one level of an oversized block; factorisation),
     // kind 2 = an oversized block swept by one CTA over the level offsets
     // lev_f / lev_b [a, b] (apply)
-    struct Launch { int kind, a, b, smem = 0; };  // smem > 0: oversized block swept staged (bytes)
+    struct Launch { int kind, a, b, smem = 0, color = -1; };  // smem > 0: oversized block swept staged (bytes)
     std::vector<Launch> fwd_blk, bwd_blk, fwd_cta, bwd_cta;
     DevBuf<int> lev_f, lev_b;
     // staged sweeps of oversized blocks: per position in rows_f / rows_b, the
     // row's entries (value index, column, position in the block or -1)
     DevBuf<int> sf_rp, sf_src, sf_col, sf_loc, sb_rp, sb_src, sb_col, sb_loc;
+    // one-launch sweeps (k_ic_sweep_all): work units in sweep order, units per
+    // colour stage, ticket / completion counters (zero between launches)
+    DevBuf<SweepUnit> swu[2];
+    DevBuf<int> swtot[2], swctr[2];
+    int swn[2] = {0, 0}, swsmem[2] = {0, 0};
+    bool swok[2] = {false, false};
+    bool sweep_one(int dir) const;
     DevBuf<int> erp, eci, esrc, urpe, ucie, usrce, isrc, dsrc;
     DevBuf<S> ev, uev, iv, dv;
     DevBuf<SL> ev_lo, uev_lo, iv_lo, dv_lo;
@@ -230,7 +237,9 @@ struct ICDevice {
     void apply_fwd(const S* x, const KState* st, cudaStream_t s) const;  // x -> tw
     void apply_bwd(S* y, const KState* st, cudaStream_t s) const;        // tw -> y
     int kernels_per_apply() const {
-        if (blk) return (int)(fwd_cta.size() + bwd_cta.size()) + (scaled_apply ? 1 : 0);
+        if (blk)
+            return (sweep_one(0) ? 1 : (int)fwd_cta.size()) + (sweep_one(1) ? 1 : (int)bwd_cta.size()) +
+                   (scaled_apply ? 1 : 0);
         return (int)(fwd_launch.size() + bwd_launch.size()) + (scaled_apply ? 1 : 0);
     }
 };
