@@ -483,7 +483,10 @@ def run_ams(args, rank, world, local):
             "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"], "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64 Krylov + f32 preconditioner hierarchy",
             "data": "synthetic", "config": config,
-            "e2e": {"value": statistics.mean(e2e_ms) / 1e3, "unit": UNIT, "h2d_bytes_per_step": int(2 * n * 8),
+            "e2e": {"value": statistics.mean(e2e_ms) / 1e3, "unit": UNIT,
+                    # b and x, the FreeDofs mask, and the matrix values, which Solve re-reads from the
+                    # host matrix every call (the matrix may have been modified in place)
+                    "h2d_bytes_per_step": int(2 * n * 8 + n + A.nnz * 8),
                     "d2h_bytes_per_step": int(n * 8 + 64)},
             "roofline": roofline, "gpu_launches": int(mixed["launches"]), "clocks": mixed["clocks"]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -664,7 +667,9 @@ def run_eddy(args, rank, world, local):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic", "config": config,
-            "e2e": {"value": statistics.mean(e2e_ms) / 1e3, "unit": UNIT, "h2d_bytes_per_step": int(2 * n * 16),
+            "e2e": {"value": statistics.mean(e2e_ms) / 1e3, "unit": UNIT,
+                    # b and x, the FreeDofs mask, and the complex matrix values re-read every call
+                    "h2d_bytes_per_step": int(2 * n * 16 + n + A.nnz * 16),
                     "d2h_bytes_per_step": int(n * 16)},
             "roofline": roofline, "gpu_launches": None, "clocks": clock_info}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -64,6 +64,7 @@ void check_mask(const uint8_t* fd, int n, std::vector<uint8_t>& h, ssv::DevBuf<u
 // Staging buffer for host-pointer calls.
 struct Stage {
     ssv::DevBuf<double> a, b;
+    ssv::DevBuf<uint8_t> fd;  // FreeDofs mask of the host-pointer solves (kept: stable address)
 };
 Stage& stage() {
     static Stage s;
@@ -170,7 +171,8 @@ int ssv_matrix_update_values(ssv_matrix* A, const void* values) {
     return guarded([&] {
         if (!A || !values) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_update_values: NULL argument");
         const size_t words = (size_t)A->nnz * (A->dtype == SSV_F64 ? 1 : 2);
-        A->val.upload(static_cast<const double*>(values), words, ssv::stream());
+        A->val.alloc(words);
+        ssv::h2d_staged(A->val.get(), values, words * sizeof(double), ssv::stream());
         SSV_CUDA(cudaStreamSynchronize(ssv::stream()));
     });
 }
@@ -521,15 +523,16 @@ int ssv_pcg_solve(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, cons
         Stage& st = stage();
         st.a.alloc(bytes / sizeof(double) + 1);
         st.b.alloc(bytes / sizeof(double) + 1);
-        ssv::DevBuf<uint8_t> dfd;
+        const uint8_t* dfd = nullptr;
         if (freedofs) {
             std::vector<uint8_t> h(freedofs, freedofs + n);
             for (auto& v : h) v = v ? 1 : 0;
-            dfd.upload(h.data(), h.size(), s);
+            st.fd.upload(h.data(), h.size(), s);
+            dfd = st.fd.get();
         }
         SSV_CUDA(cudaMemcpyAsync(st.a.get(), b, bytes, cudaMemcpyHostToDevice, s));
         SSV_CUDA(cudaMemcpyAsync(st.b.get(), x, bytes, cudaMemcpyHostToDevice, s));
-        ssv::pcg_solve_dev(A, pre, dfd.get(), *cfg, st.a.get(), st.b.get(), res, history, history_cap);
+        ssv::pcg_solve_dev(A, pre, dfd, *cfg, st.a.get(), st.b.get(), res, history, history_cap);
         SSV_CUDA(cudaMemcpyAsync(x, st.b.get(), bytes, cudaMemcpyDeviceToHost, s));
         SSV_CUDA(cudaStreamSynchronize(s));
     });
@@ -606,14 +609,15 @@ int ssv_cocr_solve(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, int
         Stage& st = stage();
         st.a.alloc(bytes / sizeof(double) + 1);
         st.b.alloc(bytes / sizeof(double) + 1);
-        ssv::DevBuf<uint8_t> dfd;
+        const uint8_t* dfd = nullptr;
         if (freedofs) {
             std::vector<uint8_t> h(freedofs, freedofs + n);
             for (auto& v : h) v = v ? 1 : 0;
-            dfd.upload(h.data(), h.size(), s);
+            st.fd.upload(h.data(), h.size(), s);
+            dfd = st.fd.get();
         }
         SSV_CUDA(cudaMemcpyAsync(st.a.get(), b, bytes, cudaMemcpyHostToDevice, s));
-        ssv::cocr_solve_dev(A, pre, dfd.get(), maxiter, tol, printrates, st.a.get(), st.b.get(), iterations);
+        ssv::cocr_solve_dev(A, pre, dfd, maxiter, tol, printrates, st.a.get(), st.b.get(), iterations);
         SSV_CUDA(cudaMemcpyAsync(x, st.b.get(), bytes, cudaMemcpyDeviceToHost, s));
         SSV_CUDA(cudaStreamSynchronize(s));
     });

@@ -39,6 +39,10 @@ inline void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
     SSV_CUDA(cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...));
 }
 
+// Host -> device copy of a large pageable array through threaded pinned staging
+// (small copies: one cudaMemcpyAsync); ordered after the work queued on s.
+void h2d_staged(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
 // Sub-warp width of the CSR kernels from the mean row length.
 int pick_lanes(double nnz_per_row);
 // SpMV launch shape: lanes | (rows per row group and pass) << 8
