@@ -91,3 +91,26 @@ def test_empty_rows_identity_freedofs():
     assert r.iterations == ro.iterations
     assert np.abs(x - xo).max() <= 1e-8 * np.abs(xo).max()
     assert np.all(x[[0, 13, 39]] == 7.0)  # constrained entries untouched
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_large_value_refresh_through_staging(cplx):
+    """Values above 16 MB are re-uploaded through the threaded pinned staging
+    (8 host threads, 4 MB chunks, ragged last chunks): after an in-place change
+    of the host matrix, refresh() must give exactly the new operator."""
+    import sparsesolv_ngsolve as ss
+    from sparsesolv_ngsolve import _capi
+    from sparsesolv_ngsolve import problems as P
+    A = P.laplacian_7pt(73, 71, 70).tocsr()  # 2.5M nnz: 20 MB of FP64 values, not a multiple of the chunk
+    if cplx:
+        A = P.complex_shifted(A, 0.3 + 0.7j).tocsr()
+    rng = np.random.default_rng(5)
+    m = ss._Matrix(A)
+    A.data *= rng.uniform(0.5, 2.0, A.nnz)  # in place: same arrays, new values
+    m.refresh()
+    n = A.shape[0]
+    x = rng.standard_normal(n) + (1j * rng.standard_normal(n) if cplx else 0)
+    y = np.zeros(n, dtype=x.dtype)
+    _capi.check(_capi.load().ssv_matrix_spmv(m.h, _capi.vptr(x), _capi.vptr(y)))
+    ref = A @ x
+    assert np.abs(y - ref).max() <= 1e-13 * np.abs(ref).max()
