@@ -427,7 +427,7 @@ def run_ams(args, rank, world, local):
     spmv_warm = phase(mixed, "fine_residual")
     achieved = gbps(spmv)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": 104.1e6,
+                "traffic": 102.9e6,
                 "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one launch of this kernel "
                                 "(ncu --set full, same workload), per launch",
                 "kernel": "k_mv_spmv fine residual (A_bc, 7.43M nnz, FP64), L2 flushed before each launch",
