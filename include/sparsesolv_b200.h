@@ -276,6 +276,11 @@ int ssv_abmc_build(int32_t n, const int32_t* row_ptr, const int32_t* col_idx,
  * upper-triangular pattern. */
 int ssv_level_schedule(int32_t n, const int32_t* row_ptr, const int32_t* col_idx,
                        int32_t upper, int32_t* level_of, int32_t* num_levels);
+/* compute_rcm_ordering (include/sparsesolv/core/rcm_ordering.hpp:38-140), the
+ * pre-ordering of the abmc_use_rcm path: ordering[old] = new,
+ * reverse_ordering[new] = old (n entries each). */
+int ssv_rcm_order(int32_t n, const int32_t* row_ptr, const int32_t* col_idx, int32_t* ordering,
+                  int32_t* reverse_ordering);
 
 /* ---- batched COCR over a frequency family (new: no reference counterpart) -
  * A_f = K + j*omega_f*M for num_freq frequencies (K, M real, square, one size;

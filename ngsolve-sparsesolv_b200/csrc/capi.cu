@@ -649,6 +649,19 @@ int ssv_level_schedule(int32_t n, const int32_t* row_ptr, const int32_t* col_idx
     });
 }
 
+int ssv_rcm_order(int32_t n, const int32_t* row_ptr, const int32_t* col_idx, int32_t* ordering,
+                  int32_t* reverse_ordering) {
+    return guarded([&] {
+        if (n < 0 || (n > 0 && (!row_ptr || !col_idx || !ordering || !reverse_ordering)))
+            ssv::fail(SSV_ERR_INVALID_ARG, "ssv_rcm_order: bad input");
+        std::vector<int> o, r;
+        ssv::rcm_order(n, row_ptr, col_idx, o, r);
+        if (n <= 0) return;
+        std::memcpy(ordering, o.data(), sizeof(int) * n);
+        std::memcpy(reverse_ordering, r.data(), sizeof(int) * n);
+    });
+}
+
 }  // extern "C"
 
 // Error text for ssv_spmv_dot_noalloc (noalloc.cu), which reports through the

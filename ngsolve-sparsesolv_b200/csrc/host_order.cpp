@@ -131,6 +131,75 @@ void build_abmc(int n, const int* rp, const int* ci, int block_size, int target_
     out.num_colors = static_cast<int>(out.color_offsets.size()) - 1;
 }
 
+void rcm_order(int n, const int* rp, const int* ci, std::vector<int>& ordering, std::vector<int>& reverse) {
+    ordering.assign(std::max(n, 0), 0);
+    reverse.assign(std::max(n, 0), 0);
+    if (n <= 0) return;
+    std::vector<int> deg(n);
+    for (int i = 0; i < n; ++i) deg[i] = rp[i + 1] - rp[i];
+    int root = 0;
+    for (int i = 1; i < n; ++i)
+        if (deg[i] < deg[root]) root = i;
+    // two sweeps toward a pseudo-peripheral row: the first row met at the
+    // largest distance becomes the next root
+    std::vector<int> dist(n);
+    std::vector<int> fifo;
+    fifo.reserve(n);
+    for (int sweep = 0; sweep < 2; ++sweep) {
+        std::fill(dist.begin(), dist.end(), -1);
+        fifo.clear();
+        fifo.push_back(root);
+        dist[root] = 0;
+        int far = root, far_d = 0;
+        for (size_t h = 0; h < fifo.size(); ++h) {
+            const int u = fifo[h];
+            for (int k = rp[u]; k < rp[u + 1]; ++k) {
+                const int v = ci[k];
+                if (dist[v] >= 0) continue;
+                dist[v] = dist[u] + 1;
+                fifo.push_back(v);
+                if (dist[v] > far_d) {
+                    far_d = dist[v];
+                    far = v;
+                }
+            }
+        }
+        root = far;
+    }
+    // Cuthill-McKee: breadth first, each row's unvisited neighbours by
+    // ascending degree (std::sort with the same comparison, so rows of equal
+    // degree land in the same order as the reference's)
+    std::vector<char> seen(n, 0);
+    std::vector<int> order;
+    order.reserve(n);
+    std::vector<int> nb;
+    for (int s0 = 0; s0 < n; ++s0) {
+        const int seed = s0 == 0 ? root : s0;
+        if (seen[seed]) continue;
+        seen[seed] = 1;
+        const size_t head0 = order.size();
+        order.push_back(seed);
+        for (size_t h = head0; h < order.size(); ++h) {
+            const int u = order[h];
+            nb.clear();
+            for (int k = rp[u]; k < rp[u + 1]; ++k) {
+                const int v = ci[k];
+                if (!seen[v]) {
+                    seen[v] = 1;
+                    nb.push_back(v);
+                }
+            }
+            std::sort(nb.begin(), nb.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+            for (int v : nb) order.push_back(v);
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        const int old = order[n - 1 - i];
+        reverse[i] = old;
+        ordering[old] = i;
+    }
+}
+
 int build_levels(int n, const int* rp, const int* ci, bool upper, std::vector<int>& level_of) {
     level_of.assign(std::max(n, 0), 0);
     if (n <= 0) return 0;

@@ -24,6 +24,13 @@ struct AbmcSchedule {
 void build_abmc(int n, const int* rp, const int* ci, int block_size, int target_colors,
                 AbmcSchedule& out);
 
+// Reverse Cuthill-McKee ordering (include/sparsesolv/core/rcm_ordering.hpp:
+// 38-140): start at the first row of least degree, move twice to the first
+// row at the largest BFS distance, then BFS from there with the unvisited
+// neighbours of each row sorted by degree, unreached rows seeding further
+// searches in index order, and reverse. ordering[old] = new, reverse[new] = old.
+void rcm_order(int n, const int* rp, const int* ci, std::vector<int>& ordering, std::vector<int>& reverse);
+
 // Level of every row for a forward (lower) or backward (upper) sweep
 // (include/sparsesolv/core/level_schedule.hpp:58-135). Returns #levels.
 int build_levels(int n, const int* rp, const int* ci, bool upper, std::vector<int>& level_of);

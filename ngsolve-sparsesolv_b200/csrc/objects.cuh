@@ -173,7 +173,7 @@ struct ICDevice {
     int n = 0;
     // pattern cache key (ICPreconditioner caches its ordering per pattern,
     // ic_preconditioner.hpp:74-81)
-    bool built = false, abmc = false;
+    bool built = false, abmc = false, rcm = false;
     int bs = 0, nct = 0;
     unsigned gen = 0;  // bumped on every pattern rebuild (part of graph keys)
     // schedule: launches in processing order, each a unit range

@@ -219,19 +219,34 @@ void ICDevice<S>::build_pattern(int n_, const std::vector<int>& rp, const std::v
     n = n_;
     ++gen;
     abmc = cfg.use_abmc != 0;
+    rcm = abmc && cfg.abmc_use_rcm != 0;
     bs = cfg.abmc_block_size;
     nct = cfg.abmc_num_colors;
     fwd_launch.clear();
     bwd_launch.clear();
     std::vector<int> lrp, lci, lsrc, urp, uci, usrc;
     if (abmc) {
+        // abmc_use_rcm (ic_preconditioner.hpp:97-104): the ABMC schedule is
+        // built on the RCM-reordered pattern, and the working numbering is the
+        // composite old -> RCM -> ABMC (build_composite_permutations, :584-596)
+        std::vector<int> rord, rrev, crp, cci, csrc;
+        const int* brp = rp.data();
+        const int* bci = ci.data();
+        if (rcm) {
+            rcm_order(n, rp.data(), ci.data(), rord, rrev);
+            permute_pattern(n, rp.data(), ci.data(), rord.data(), crp, cci, csrc);
+            brp = crp.data();
+            bci = cci.data();
+        }
         AbmcSchedule sched;
-        build_abmc(n, rp.data(), ci.data(), cfg.abmc_block_size, cfg.abmc_num_colors, sched);
+        build_abmc(n, brp, bci, cfg.abmc_block_size, cfg.abmc_num_colors, sched);
         num_colors = sched.num_colors;
         num_blocks = sched.num_blocks;
         h_perm = sched.ordering;
+        if (rcm)
+            for (int i = 0; i < n; ++i) h_perm[i] = sched.ordering[rord[i]];
         std::vector<int> prp, pci, psrc;
-        permute_pattern(n, rp.data(), ci.data(), sched.ordering.data(), prp, pci, psrc);
+        permute_pattern(n, rp.data(), ci.data(), h_perm.data(), prp, pci, psrc);
         lower_pattern(n, prp.data(), pci.data(), lrp, lci, lsrc);
         // L value sources as positions in the ORIGINAL value array
         for (auto& k : lsrc) k = psrc[k];
@@ -593,7 +608,10 @@ int ICDevice<S>::factorize(const S* vals, const ssv_config& cfg) {
         break;
     }
     actual_shift = shift;
-    scaled_apply = scale && (!abmc || cfg.abmc_reorder_spmv);
+    // the ABMC apply of the default path never scales (the scaling enters the
+    // factor only); the reordered-space applies of paths 1 and 2 do
+    // (ic_preconditioner.hpp:327-345)
+    scaled_apply = scale && (!abmc || cfg.abmc_reorder_spmv || cfg.abmc_use_rcm);
     const int64_t nu = (int64_t)Usrc.size();
     k_gather_values<S><<<grid_for(nu, kBlock), kBlock, 0, s>>>(nu, Usrc.get(), Lv.get(), Uv.get());
     SSV_LAUNCH_CHECK();
@@ -833,11 +851,10 @@ static void run_krylov(ssv_solver* sv, int method, const ssv_config& cfg, const 
     const int* perm = nullptr;
     ICDevice<S>* ic = nullptr;
     if (method == SSV_METHOD_ICCG) {
-        if (cfg.use_abmc && cfg.abmc_use_rcm)
-            fail(SSV_ERR_INVALID_ARG, "abmc_use_rcm (RCM pre-ordering) is not available on the B200 path yet");
         ic = &ic_of<S>(sv);
         const bool same = ic->built && ic->abmc == (cfg.use_abmc != 0) &&
-                          (!ic->abmc || (ic->bs == cfg.abmc_block_size && ic->nct == cfg.abmc_num_colors));
+                          (!ic->abmc || (ic->bs == cfg.abmc_block_size && ic->nct == cfg.abmc_num_colors &&
+                                         ic->rcm == (cfg.abmc_use_rcm != 0)));
         if (!same) ic->build_pattern(n, A->h_rp, A->h_ci, cfg);
         nk += ic->factorize(vals, cfg);
         res->actual_shift = ic->actual_shift;
@@ -1159,13 +1176,16 @@ static void ic_update(ssv_precond* p) {
     }
     ICDevice<S>& ic = pic_of<S>(p);
     const ssv_config& cfg = p->cfg;
-    if (cfg.use_abmc && cfg.abmc_use_rcm)
-        fail(SSV_ERR_INVALID_ARG, "abmc_use_rcm (RCM pre-ordering) is not available on the B200 path yet");
     // the pattern cache of ICPreconditioner::setup (ic_preconditioner.hpp:78-81)
     const bool same = ic.built && ic.abmc == (cfg.use_abmc != 0) &&
-                      (!ic.abmc || (ic.bs == cfg.abmc_block_size && ic.nct == cfg.abmc_num_colors));
+                      (!ic.abmc || (ic.bs == cfg.abmc_block_size && ic.nct == cfg.abmc_num_colors &&
+                                    ic.rcm == (cfg.abmc_use_rcm != 0)));
     if (!same) ic.build_pattern(n, A->h_rp, A->h_ci, cfg);
     ic.factorize(vals, cfg);
+    // Mult goes through ICPreconditioner::apply -> apply_abmc (:215-225,
+    // :655-700) in original numbering for every ABMC variant, which (single
+    // threaded) does not scale
+    if (ic.abmc) ic.scaled_apply = false;
     const size_t words = (size_t)n * (sizeof(S) / sizeof(double));
     p->xw.alloc(words);
     p->yw.alloc(words);

@@ -186,6 +186,7 @@ SIGNATURES = [
     ("ssv_cocr_solve_dev", I32, [P, P, PU8, I32, ctypes.c_double, I32, P, P, PI32]),
     ("ssv_abmc_build", I32, [I32, PI32, PI32, I32, I32, PI32, PI32, PI32, PI32, PI32, PI32]),
     ("ssv_level_schedule", I32, [I32, PI32, PI32, I32, PI32, PI32]),
+    ("ssv_rcm_order", I32, [I32, PI32, PI32, PI32, PI32]),
     ("ssv_spmv_dot_noalloc", I32, [I32, P, P, P, P, P, P]),
     ("ssv_ams_create", I32, [P, P, PU8, PD, PD, PD, I32, I32, ctypes.c_double, ctypes.c_double, I32, I32, PP]),
     ("ssv_ams_update", I32, [P, P]),

@@ -50,6 +50,7 @@ def _bind(lib, prefix):
     else:
         sig["set_threads"] = (None, [I32])
         sig["get_threads"] = (I32, [])
+        sig["rcm"] = (I32, [I32, PI32, PI32, PI32, PI32])
     for name, (res, args) in sig.items():
         fn = getattr(lib, prefix + name)
         fn.restype = res
@@ -151,6 +152,24 @@ def abmc(A, block_size=4, num_colors=4, which="port"):
     return {"num_colors": nc.value, "num_blocks": nb.value,
             "color_offsets": co[: nc.value + 1].copy(), "block_offsets": bo[: nb.value + 1].copy(),
             "ordering": od, "reverse": rv}
+
+
+def rcm(A, which="ref"):
+    """compute_rcm_ordering (rcm_ordering.hpp:38-140) of A's pattern, run by the
+    reference library (the C restatement has no RCM: its tie order among rows
+    of equal degree is the reference's std::sort, not restated in C).
+    Returns (ordering[old] = new, reverse[new] = old)."""
+    if which != "ref":
+        raise ValueError("rcm: only the reference library computes it")
+    lib = reference()
+    rp = np.ascontiguousarray(A.indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(A.indices, dtype=np.int32)
+    n = A.shape[0]
+    od = np.zeros(max(n, 1), np.int32)
+    rv = np.zeros(max(n, 1), np.int32)
+    if lib.ref_rcm(n, _p(rp), _p(ci), _p(od), _p(rv)) != 0:
+        raise RuntimeError("rcm failed")
+    return od[:n], rv[:n]
 
 
 def level_schedule(rp, ci, n, upper=False, which="port"):

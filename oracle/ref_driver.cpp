@@ -209,4 +209,13 @@ int ref_level_schedule(int n, const int* rp, const int* ci, int upper, int* leve
     return 0;
 }
 
+int ref_rcm(int n, const int* rp, const int* ci, int* ordering, int* reverse) {
+    std::vector<int> o, r;
+    sparsesolv::compute_rcm_ordering(rp, ci, n, o, r);
+    if (n <= 0) return 0;
+    std::memcpy(ordering, o.data(), sizeof(int) * n);
+    std::memcpy(reverse, r.data(), sizeof(int) * n);
+    return 0;
+}
+
 }  // extern "C"

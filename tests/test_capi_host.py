@@ -130,3 +130,45 @@ def test_config_default_matches_reference_defaults():
         assert getattr(c, f) == getattr(d, f), f
     assert c.tolerance == 1e-10 and c.max_iterations == 1000 and c.abs_tolerance == 1e-12
     assert c.divergence_threshold == 1000.0 and c.divergence_count == 100 and c.save_best_result == 1
+
+
+def _rcm(lib, rp, ci, n):
+    P = ctypes.POINTER(ctypes.c_int32)
+    rp = np.ascontiguousarray(rp, np.int32)
+    ci = np.ascontiguousarray(ci, np.int32)
+    od = np.zeros(max(n, 1), np.int32)
+    rv = np.zeros(max(n, 1), np.int32)
+    assert lib.ssv_rcm_order(n, rp.ctypes.data_as(P), ci.ctypes.data_as(P), od.ctypes.data_as(P),
+                             rv.ctypes.data_as(P)) == 0
+    return od[:n], rv[:n]
+
+
+@pytest.mark.parametrize("sysname", ["lap3d_6", "lap3d_8_fd", "lap2d_12", "cplx3d_6", "cplx3d_8_fd"])
+def test_rcm_host_equals_reference(golden, sysname):
+    """The abmc_use_rcm pre-ordering is bit-identical to compute_rcm_ordering."""
+    A, _, _ = golden_system(golden, sysname)
+    od, rv = _rcm(_lib(), A.indptr, A.indices, A.shape[0])
+    np.testing.assert_array_equal(od, golden[f"rcm/{sysname}/ordering"])
+    np.testing.assert_array_equal(rv, golden[f"rcm/{sysname}/reverse"])
+
+
+def test_rcm_permutation_and_edge_shapes():
+    import scipy.sparse as sp
+    lib = _lib()
+    # disconnected pattern (two blocks and an isolated row), ragged degrees
+    A = sp.block_diag([sp.random(9, 9, 0.4, random_state=1) + sp.eye(9), sp.eye(1),
+                       sp.random(6, 6, 0.5, random_state=2) + sp.eye(6)]).tocsr()
+    A = (A + A.T).tocsr()
+    A.sort_indices()
+    od, rv = _rcm(lib, A.indptr, A.indices, A.shape[0])
+    assert sorted(od.tolist()) == list(range(A.shape[0]))
+    assert (rv[od] == np.arange(A.shape[0])).all()
+    from oracle import oracle as O
+    if O.reference() is not None:
+        ro, rr = O.rcm(A)
+        np.testing.assert_array_equal(od, ro)
+        np.testing.assert_array_equal(rv, rr)
+    # empty and single-row patterns
+    assert _rcm(lib, np.zeros(1, np.int32), np.zeros(0, np.int32), 0)[0].size == 0
+    od1, rv1 = _rcm(lib, np.array([0, 1], np.int32), np.array([0], np.int32), 1)
+    assert od1.tolist() == [0] and rv1.tolist() == [0]

@@ -75,13 +75,19 @@ def items_dict(items):
 
 
 @pytest.mark.parametrize("sysname", ["lap3d_6", "lap3d_8_fd", "cplx3d_8_fd"])
-@pytest.mark.parametrize("kind", ["abmc", "level"])
+@pytest.mark.parametrize("kind", ["abmc", "level", "abmc_rcm"])
 def test_ic_preconditioner_mult(golden, sysname, kind):
     import sparsesolv_ngsolve as ss
     A, b, fd = golden_system(golden, sysname)
     p = ss.ICPreconditioner(A, freedofs=fd, shift=1.05)
     if kind == "abmc":
         p.use_abmc = True
+        p.Update()
+    elif kind == "abmc_rcm":
+        # the RCM pre-ordering has no ICPreconditioner keyword in the reference's
+        # Python API; the C ABI carries the whole SolverConfig
+        p.use_abmc = True
+        p._cfg.abmc_use_rcm = 1
         p.Update()
     y = p * b
     yr = golden[f"icmult/{sysname}/{kind}"]

@@ -19,6 +19,12 @@ def test_oracle_matches_reference_golden(golden):
     for case, sysname, method, items in golden_cases(golden):
         A, b, fd = golden_system(golden, sysname)
         cfg = _cfg_from(items)
+        if cfg.use_abmc and cfg.abmc_use_rcm:
+            # Path 2 is not restated in C (RCM's order among rows of equal degree is
+            # the reference's std::sort); those fixtures pin the GPU path directly
+            with pytest.raises(RuntimeError):
+                O.solve(A, b, method, cfg, freedofs=fd, which="port")
+            continue
         x, res, hist = O.solve(A, b, method, cfg, freedofs=fd, which="port")
         conv, iters, fres = golden[f"case/{case}/meta"]
         xr = golden[f"case/{case}/x"]
