@@ -24,7 +24,7 @@ def _solver(A, method, fd, items):
                             save_residual_history=bool(d["save_residual_history"]),
                             conjugate=bool(d["conjugate"]), use_abmc=bool(d["use_abmc"]),
                             abmc_block_size=d["abmc_block_size"], abmc_num_colors=d["abmc_num_colors"],
-                            abmc_reorder_spmv=bool(d["abmc_reorder_spmv"]))
+                            abmc_reorder_spmv=bool(d["abmc_reorder_spmv"]), abmc_use_rcm=bool(d["abmc_use_rcm"]))
     s.auto_shift = bool(d["auto_shift"])
     s.diagonal_scaling = bool(d["diagonal_scaling"])
     s.divergence_check = bool(d["divergence_check"])
