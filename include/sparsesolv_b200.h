@@ -182,6 +182,13 @@ int ssv_solver_profile(ssv_solver* s, const char* method, const ssv_config* cfg,
  * implicit Update(): call ssv_precond_update() to factorise. */
 int ssv_ic_create(ssv_matrix* A, const uint8_t* freedofs, double shift,
                   ssv_precond** out);
+/* SGSPreconditioner factory (sparsesolv_python_export.hpp:209-230) over
+ * SparseSolvSGSPreconditioner (ngsolve/sparsesolv_precond.hpp:230-250) and
+ * sparsesolv::SGSPreconditioner (preconditioners/sgs_preconditioner.hpp):
+ * M^{-1} = (D + U)^{-1} D (D + L)^{-1} on the FreeDofs view of A, output zero
+ * on constrained DOFs. ssv_precond_update computes it (the factory calls it
+ * once), ssv_precond_apply[_dev] applies it, ssv_precond_destroy frees it. */
+int ssv_sgs_create(ssv_matrix* A, const uint8_t* freedofs, ssv_precond** out);
 /* Options of SparseSolvICPreconditioner (sparsesolv_precond.hpp:200-223):
  * use_abmc, abmc_block_size, abmc_num_colors, diagonal_scaling, shift and the
  * auto-shift fields are read from cfg; they take effect at the next update. */

@@ -1867,6 +1867,7 @@ void ams_profile(AmsState* a, int nrhs, int reps, int flags, ssv_phase_profile* 
 template <>
 void precond_apply_any<double>(ssv_precond* p, const double* x, double* y, const KState* st, cudaStream_t s) {
     if (p->kind == 1) ic_apply_dev<double>(p, x, y, st, s);
+    else if (p->kind == 4) sgs_apply_dev<double>(p, x, y, st, s);
     else if (p->kind == 2) {
         if (p->ams->fp32) ams_cycle<float, 1, false>(*p->ams, x, y, st, s);
         else ams_cycle<double, 1, false>(*p->ams, x, y, st, s);
@@ -1876,6 +1877,7 @@ void precond_apply_any<double>(ssv_precond* p, const double* x, double* y, const
 template <>
 void precond_apply_any<zdouble>(ssv_precond* p, const zdouble* x, zdouble* y, const KState* st, cudaStream_t s) {
     if (p->kind == 1) ic_apply_dev<zdouble>(p, x, y, st, s);
+    else if (p->kind == 4) sgs_apply_dev<zdouble>(p, x, y, st, s);
     else if (p->kind == 3) {
         const double* xi = reinterpret_cast<const double*>(x);
         double* yo = reinterpret_cast<double*>(y);
@@ -1886,6 +1888,7 @@ void precond_apply_any<zdouble>(ssv_precond* p, const zdouble* x, zdouble* y, co
 
 unsigned precond_generation(const ssv_precond* p) {
     if (p->kind == 1) return p->A->dtype == SSV_F64 ? p->ic_d.gen : p->ic_z.gen;
+    if (p->kind == 4) return p->A->dtype == SSV_F64 ? p->sgs_d.gen : p->sgs_z.gen;
     return p->ams ? p->ams->gen : 0;
 }
 

@@ -304,6 +304,27 @@ int ssv_ic_create(ssv_matrix* A, const uint8_t* freedofs, double shift, ssv_prec
     });
 }
 
+int ssv_sgs_create(ssv_matrix* A, const uint8_t* freedofs, ssv_precond** out) {
+    return guarded([&] {
+        if (!A || !out) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_sgs_create: NULL argument");
+        if (A->rows != A->cols) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_sgs_create: matrix must be square");
+        auto* p = new ssv_precond();
+        p->kind = 4;
+        p->A = A;
+        p->vdtype = A->dtype;
+        p->n = A->rows;
+        ssv_config_default(&p->cfg);
+        try {
+            check_mask(freedofs, A->rows, p->h_fd, p->fd, p->has_fd);
+            SSV_CUDA(cudaStreamSynchronize(ssv::stream()));
+        } catch (...) {
+            delete p;
+            throw;
+        }
+        *out = p;
+    });
+}
+
 int ssv_ams_create(ssv_matrix* A, ssv_matrix* G, const uint8_t* freedofs, const double* coord_x,
                    const double* coord_y, const double* coord_z, int32_t cycle_type, int32_t num_smooth,
                    double theta, double correction_weight, int32_t complex_form, int32_t ndof_complex,

@@ -248,6 +248,18 @@ struct ICDevice {
     }
 };
 
+// Symmetric Gauss-Seidel preconditioner (sgs_preconditioner.hpp): level sets
+// of the forward (j < i) and backward (j > i) sweeps over the full pattern,
+// 1/a_ii, and the work vector between the sweeps.
+template <typename S>
+struct SgsDevice {
+    bool built = false;
+    unsigned gen = 0;
+    std::vector<std::pair<int, int>> fwd_lev, bwd_lev;  // row ranges of rows_f / rows_b per level
+    DevBuf<int> rows_f, rows_b;
+    DevBuf<S> inv, tmp;
+};
+
 }  // namespace ssv
 
 // ---------------------------------------------------------------------------
@@ -272,6 +284,8 @@ struct ssv_solver {
     ssv::DevBuf<double> io_b, io_x;  // staging for host-pointer solves
     ssv::ICDevice<double> ic_d;
     ssv::ICDevice<ssv::zdouble> ic_z;
+    ssv::SgsDevice<double> sgs_d;
+    ssv::SgsDevice<ssv::zdouble> sgs_z;
     ssv::KrylovWork<double> w_d;
     ssv::KrylovWork<ssv::zdouble> w_z;
     ssv::GraphLoop loop;
@@ -283,7 +297,7 @@ void ams_free(AmsState* a);
 }  // namespace ssv
 
 struct ssv_precond {
-    int kind = 0;    // 1 = IC, 2 = CompactAMS (real), 3 = ComplexCompactAMS
+    int kind = 0;    // 1 = IC, 2 = CompactAMS (real), 3 = ComplexCompactAMS, 4 = SGS
     int vdtype = 0;  // scalar type of the vectors it applies to
     int n = 0;       // vector length
     ssv_matrix* A = nullptr;
@@ -295,6 +309,8 @@ struct ssv_precond {
     bool ready = false;
     ssv::ICDevice<double> ic_d;
     ssv::ICDevice<ssv::zdouble> ic_z;
+    ssv::SgsDevice<double> sgs_d;
+    ssv::SgsDevice<ssv::zdouble> sgs_z;
     ssv::DevBuf<double> xw, yw, io_x, io_y;
     std::unique_ptr<ssv::AmsState, void (*)(ssv::AmsState*)> ams{nullptr, ssv::ams_free};
     virtual ~ssv_precond() = default;

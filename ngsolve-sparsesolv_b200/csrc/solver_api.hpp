@@ -22,6 +22,10 @@ void cocr_forget(const ssv_matrix* A);
 
 template <typename S>
 void ic_apply_dev(ssv_precond* p, const S* x, S* y, const KState* st, cudaStream_t s);
+// SGSPreconditioner (sgs.cu): Update() and Mult
+void sgs_update(ssv_precond* p);
+template <typename S>
+void sgs_apply_dev(ssv_precond* p, const S* x, S* y, const KState* st, cudaStream_t s);
 
 // y = M^{-1} x for any preconditioner handle, stream-ordered, no host sync
 // (so it can sit inside a captured iteration graph).

@@ -26,7 +26,7 @@ __all__ = [
     "COCRSolver", "COCRSolverD", "COCRSolverC", "has_compact_ams",
     "CompactAMSPreconditioner", "CompactAMSPreconditionerImpl",
     "ComplexCompactAMSPreconditioner", "ComplexCompactAMSPreconditionerImpl", "PCGSolver",
-    "BatchedCOCRSolver",
+    "BatchedCOCRSolver", "SGSPreconditioner", "SGSPreconditionerD", "SGSPreconditionerC",
 ]
 
 
@@ -420,6 +420,44 @@ def ICPreconditioner(mat, freedofs=None, shift=1.05):
     """Incomplete Cholesky (IC) preconditioner; calls Update() (factory :176-207)."""
     _, _, _, cplx, _ = _csr_arrays(mat)
     p = (ICPreconditionerC if cplx else ICPreconditionerD)(mat, freedofs, shift)
+    p.Update()
+    return p
+
+
+# ---------------------------------------------------------------------------
+# SGSPreconditioner (sparsesolv_python_export.hpp:82-89,209-240)
+# ---------------------------------------------------------------------------
+
+class _SGSPreconditionerBase(_PrecondBase):
+    def __init__(self, mat, freedofs=None):
+        self._mat = _Matrix(mat)
+        self._n = self._mat.n
+        self._dtype = self._mat.dtype
+        self._fd = _freedofs_array(freedofs, self._n)
+        lib = _capi.load()
+        h = ctypes.c_void_p()
+        check(lib.ssv_sgs_create(self._mat.h, _capi.u8ptr(self._fd), ctypes.byref(h)))
+        self._init_handle(h)
+
+    def Update(self):
+        """Re-read the matrix (FreeDofs view) and rebuild 1/a_ii
+        (SparseSolvSGSPreconditioner::Update)."""
+        self._mat.refresh()
+        check(self._lib.ssv_precond_update(self._h))
+
+
+class SGSPreconditionerD(_SGSPreconditionerBase):
+    _cplx = False
+
+
+class SGSPreconditionerC(_SGSPreconditionerBase):
+    _cplx = True
+
+
+def SGSPreconditioner(mat, freedofs=None):
+    """Symmetric Gauss-Seidel preconditioner (D+U)^{-1} D (D+L)^{-1}; calls Update() (factory :209-230)."""
+    _, _, _, cplx, _ = _csr_arrays(mat)
+    p = (SGSPreconditionerC if cplx else SGSPreconditionerD)(mat, freedofs)
     p.Update()
     return p
 

@@ -177,6 +177,7 @@ SIGNATURES = [
                                  ctypes.POINTER(ssv_phase_profile)]),
     ("ssv_ic_create", I32, [P, PU8, ctypes.c_double, PP]),
     ("ssv_ic_set_config", I32, [P, ctypes.POINTER(ssv_config)]),
+    ("ssv_sgs_create", I32, [P, PU8, PP]),
     ("ssv_precond_update", I32, [P]),
     ("ssv_precond_apply", I32, [P, P, P]),
     ("ssv_precond_apply_dev", I32, [P, P, P]),

@@ -41,6 +41,7 @@ def _bind(lib, prefix):
         "ic_mult": (I32, [I32, PI32, PI32, P, I32, PU8, ctypes.POINTER(ssv_config), P, P, PD]),
         "abmc_build": (I32, [I32, PI32, PI32, I32, I32, PI32, PI32, PI32, PI32, PI32, PI32]),
         "level_schedule": (I32, [I32, PI32, PI32, I32, PI32, PI32]),
+        "sgs_mult": (I32, [I32, PI32, PI32, P, I32, PU8, P, P]),
         "last_error": (ctypes.c_char_p, []),
     }
     if prefix == "orc_":
@@ -130,6 +131,22 @@ def ic_mult(A, x, config=None, freedofs=None, which="port"):
     if rc != 0:
         raise RuntimeError(getattr(lib, ("orc_" if which == "port" else "ref_") + "last_error")().decode())
     return y, sh.value
+
+
+def sgs_mult(A, x, freedofs=None, which="port"):
+    """SGSPreconditioner(A, freedofs) * x (factory, Update and Mult)."""
+    lib = port() if which == "port" else reference()
+    rp, ci, v, cplx = _csr_parts(A)
+    dt = np.complex128 if cplx else np.float64
+    xx = np.ascontiguousarray(x, dtype=dt)
+    y = np.zeros(A.shape[0], dtype=dt)
+    fd = None if freedofs is None else np.ascontiguousarray(freedofs, np.uint8)
+    rc = getattr(lib, ("orc_" if which == "port" else "ref_") + "sgs_mult")(
+        A.shape[0], _p(rp), _p(ci), v.ctypes.data_as(P), cplx, _p(fd, PU8), xx.ctypes.data_as(P),
+        y.ctypes.data_as(P))
+    if rc != 0:
+        raise RuntimeError("sgs_mult failed")
+    return y
 
 
 def abmc(A, block_size=4, num_colors=4, which="port"):

@@ -134,6 +134,29 @@ int ic_mult_impl(int n, const int* rp, const int* ci, const S* vals, const unsig
     return 0;
 }
 
+template <typename S>
+int sgs_mult_impl(int n, const int* rp, const int* ci, const S* vals, const unsigned char* fd, const S* x, S* y) {
+    using namespace sparsesolv;
+    const int nnz = rp[n];
+    std::vector<S> mv(vals, vals + nnz);
+    if (fd) {
+        for (int i = 0; i < n; ++i)
+            for (int k = rp[i]; k < rp[i + 1]; ++k) {
+                const int j = ci[k];
+                if (!fd[i]) mv[k] = (j == i) ? S(1) : S(0);
+                else if (!fd[j]) mv[k] = S(0);
+            }
+    }
+    SparseMatrixView<S> view(n, n, rp, ci, mv.data());
+    SGSPreconditioner<S> pre;
+    pre.setup(view);
+    pre.apply(x, y, n);
+    if (fd)
+        for (int i = 0; i < n; ++i)
+            if (!fd[i]) y[i] = S(0);
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -207,6 +230,21 @@ int ref_level_schedule(int n, const int* rp, const int* ci, int upper, int* leve
     for (int l = 0; l < ls.num_levels(); ++l)
         for (int r : ls.levels[l]) level_of[r] = l;
     return 0;
+}
+
+int ref_sgs_mult(int n, const int* rp, const int* ci, const void* vals, int dtype, const unsigned char* freedofs,
+                 const void* x, void* y) {
+    try {
+        if (dtype == SSV_F64)
+            return sgs_mult_impl<double>(n, rp, ci, static_cast<const double*>(vals), freedofs,
+                                         static_cast<const double*>(x), static_cast<double*>(y));
+        using Z = std::complex<double>;
+        return sgs_mult_impl<Z>(n, rp, ci, static_cast<const Z*>(vals), freedofs, static_cast<const Z*>(x),
+                                static_cast<Z*>(y));
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return SSV_ERR_RUNTIME;
+    }
 }
 
 int ref_rcm(int n, const int* rp, const int* ci, int* ordering, int* reverse) {

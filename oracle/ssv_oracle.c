@@ -294,6 +294,13 @@ int orc_solve(int n, const int* rp, const int* ci, const void* vals, int dtype,
                    hist, hist_cap, g_err, (int)sizeof(g_err));
 }
 
+int orc_sgs_mult(int n, const int* rp, const int* ci, const void* vals, int dtype, const unsigned char* freedofs,
+                 const void* x, void* y) {
+    if (dtype == SSV_F64)
+        return sgs_mult_d(n, rp, ci, (const double*)vals, freedofs, (const double*)x, (double*)y);
+    return sgs_mult_z(n, rp, ci, (const zc*)vals, freedofs, (const zc*)x, (zc*)y);
+}
+
 int orc_ic_mult(int n, const int* rp, const int* ci, const void* vals, int dtype,
                 const unsigned char* freedofs, const ssv_config* cfg, const void* x, void* y,
                 double* actual_shift) {

@@ -811,6 +811,51 @@ static int SFX(ic_mult)(int n, const int* rp, const int* ci, const T* vals, cons
     return rc;
 }
 
+/* SGSPreconditioner factory + Update() + Mult (sparsesolv_precond.hpp:123-136,
+ * 230-250; preconditioners/sgs_preconditioner.hpp:67-200): the forward sweep
+ * (D + L) t = x, t <- t / inv_diag, the backward sweep (D + U) y = t, on the
+ * FreeDofs view, constrained outputs zeroed. Rows of one level set do not
+ * depend on each other, so sweeping rows in index order (forward) and in
+ * reverse order (backward) gives every row the reference's operands. */
+static int SFX(sgs_mult)(int n, const int* rp, const int* ci, const T* vals, const unsigned char* fd,
+                         const T* x, T* y) {
+    int nnz = rp[n];
+    T* mv = (T*)malloc(sizeof(T) * (size_t)(nnz > 0 ? nnz : 1));
+    T* inv = (T*)malloc(sizeof(T) * (size_t)(n > 0 ? n : 1));
+    T* t = (T*)malloc(sizeof(T) * (size_t)(n > 0 ? n : 1));
+    memcpy(mv, vals, sizeof(T) * (size_t)nnz);
+    if (fd) {
+        for (int i = 0; i < n; ++i)
+            for (int k = rp[i]; k < rp[i + 1]; ++k) {
+                int j = ci[k];
+                if (!fd[i]) mv[k] = (j == i) ? FROM_REAL(1.0) : FROM_REAL(0.0);
+                else if (!fd[j]) mv[k] = FROM_REAL(0.0);
+            }
+    }
+    for (int i = 0; i < n; ++i) {
+        T d = FROM_REAL(0.0);
+        for (int k = rp[i]; k < rp[i + 1]; ++k)
+            if (ci[k] == i) { d = mv[k]; break; }
+        inv[i] = SABS(d) > 1e-15 ? FROM_REAL(1.0) / d : FROM_REAL(1.0);
+    }
+    for (int i = 0; i < n; ++i) {
+        T sum = x[i];
+        for (int k = rp[i]; k < rp[i + 1]; ++k)
+            if (ci[k] < i) sum -= mv[k] * t[ci[k]];
+        t[i] = sum * inv[i];
+    }
+    for (int i = 0; i < n; ++i) t[i] = t[i] / inv[i];
+    for (int i = n - 1; i >= 0; --i) {
+        T sum = t[i];
+        for (int k = rp[i]; k < rp[i + 1]; ++k)
+            if (ci[k] > i) sum -= mv[k] * y[ci[k]];
+        y[i] = sum * inv[i];
+    }
+    if (fd) for (int i = 0; i < n; ++i) if (!fd[i]) y[i] = FROM_REAL(0.0);
+    free(mv); free(inv); free(t);
+    return 0;
+}
+
 /* COCRSolverNGS::Mult, ngsolve/sparsesolv_solvers.hpp:273-369, with the
  * preconditioner given as a callback (identity when NULL). */
 static int SFX(cocr_ngs)(int n, const int* rp, const int* ci, const T* vals, const unsigned char* fd,

@@ -5,7 +5,8 @@ include/sparsesolv, compiled by oracle/build_oracle.py into
 oracle/_ref/libssv_ref.so) single-threaded on small synthetic systems and
 stores inputs and outputs in tests/golden/golden_small.npz:
 solutions, iteration counts, residual histories, ABMC schedules, RCM
-orderings, level schedules and one IC preconditioner application per case.
+orderings, level schedules and one IC and one SGS preconditioner application per
+system.
 
     python tests/golden/gen_golden.py [--rewrite]
 """
@@ -98,6 +99,7 @@ def main():
         out[f"icmult/{name}/level"] = y
         y, sh = O.ic_mult(A, b, O.default_config(use_abmc=1, abmc_use_rcm=1), freedofs=fd, which="ref")
         out[f"icmult/{name}/abmc_rcm"] = y
+        out[f"sgsmult/{name}"] = O.sgs_mult(A, b, freedofs=fd, which="ref")
     for case, sysname, method, over in CASES:
         A, b, fd = SYSTEMS[sysname]()
         cfg = O.default_config(save_residual_history=1, max_iterations=over.pop("max_iterations", 2000), **over)

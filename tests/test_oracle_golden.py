@@ -85,3 +85,15 @@ def test_oracle_live_reference_small():
     x2, r2, h2 = O.solve(A, b, "ICCG", cfg, which="ref")
     assert r1.iterations == r2.iterations
     assert np.abs(x1 - x2).max() < 1e-12 * np.abs(x2).max()
+
+
+@pytest.mark.parametrize("sysname", ["lap3d_6", "lap3d_8_fd", "lap2d_12", "cplx3d_6", "cplx3d_8_fd"])
+def test_oracle_sgs_mult_matches_reference(golden, sysname):
+    """SGSPreconditioner apply: bit-exact on real systems, complex to rounding
+    (C99 complex against std::complex arithmetic)."""
+    A, b, fd = golden_system(golden, sysname)
+    y = O.sgs_mult(A, b, freedofs=fd, which="port")
+    yr = golden[f"sgsmult/{sysname}"]
+    assert np.abs(y - yr).max() <= 1e-14 * np.abs(yr).max()
+    if not np.iscomplexobj(yr):
+        assert np.array_equal(y, yr)
