@@ -268,6 +268,16 @@ int ssv_pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, 
                       const void* d_b, void* d_x, ssv_result* res, double* history,
                       int32_t history_cap);
 
+/* GMRESSolver (GMRESSolverNGS, ngsolve/sparsesolv_solvers.hpp:409-584;
+ * factory sparsesolv_python_export.hpp:643-697): right-preconditioned GMRES
+ * with modified Gram-Schmidt and Givens rotations, x0 = 0, restart after
+ * `restart` steps (0 = maxiter), stop when |g_{j+1}| / ||P b|| < tol;
+ * iterations = total Arnoldi steps. pre may be NULL (identity). */
+int ssv_gmres_solve(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, int32_t maxiter, double tol,
+                    int32_t restart, const void* b, void* x, int32_t* iterations);
+int ssv_gmres_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, int32_t maxiter, double tol,
+                        int32_t restart, const void* d_b, void* d_x, int32_t* iterations);
+
 /* ---- host-side set-up logic exposed for parity checks (no device work) --- */
 /* ABMCSchedule::build (include/sparsesolv/core/abmc_ordering.hpp:83-121).
  * color_offsets needs room for n+1 entries, block_offsets n+1, ordering and

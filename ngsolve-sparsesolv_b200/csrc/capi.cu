@@ -644,6 +644,43 @@ int ssv_cocr_solve(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, int
     });
 }
 
+int ssv_gmres_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, int32_t maxiter, double tol,
+                        int32_t restart, const void* d_b, void* d_x, int32_t* iterations) {
+    return guarded([&] {
+        if (!A || !d_b || !d_x || !iterations) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_gmres_solve_dev: NULL argument");
+        if (A->rows != A->cols) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_gmres_solve_dev: matrix must be square");
+        require_device_ptr(d_b, "ssv_gmres_solve_dev b");
+        require_device_ptr(d_x, "ssv_gmres_solve_dev x");
+        require_device_ptr(freedofs, "ssv_gmres_solve_dev freedofs");
+        ssv::gmres_solve_dev(A, pre, freedofs, maxiter, tol, restart, d_b, d_x, iterations);
+    });
+}
+
+int ssv_gmres_solve(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, int32_t maxiter, double tol,
+                    int32_t restart, const void* b, void* x, int32_t* iterations) {
+    return guarded([&] {
+        if (!A || !b || !x || !iterations) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_gmres_solve: NULL argument");
+        if (A->rows != A->cols) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_gmres_solve: matrix must be square");
+        cudaStream_t s = ssv::stream();
+        const int n = A->rows;
+        const size_t bytes = (size_t)n * scalar_bytes(A->dtype);
+        Stage& st = stage();
+        st.a.alloc(bytes / sizeof(double) + 1);
+        st.b.alloc(bytes / sizeof(double) + 1);
+        const uint8_t* dfd = nullptr;
+        if (freedofs) {
+            std::vector<uint8_t> h(freedofs, freedofs + n);
+            for (auto& v : h) v = v ? 1 : 0;
+            st.fd.upload(h.data(), h.size(), s);
+            dfd = st.fd.get();
+        }
+        SSV_CUDA(cudaMemcpyAsync(st.a.get(), b, bytes, cudaMemcpyHostToDevice, s));
+        ssv::gmres_solve_dev(A, pre, dfd, maxiter, tol, restart, st.a.get(), st.b.get(), iterations);
+        SSV_CUDA(cudaMemcpyAsync(x, st.b.get(), bytes, cudaMemcpyDeviceToHost, s));
+        SSV_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 int ssv_abmc_build(int32_t n, const int32_t* row_ptr, const int32_t* col_idx, int32_t block_size,
                    int32_t target_colors, int32_t* num_colors, int32_t* num_blocks, int32_t* color_offsets,
                    int32_t* block_offsets, int32_t* ordering, int32_t* reverse_ordering) {

@@ -17,6 +17,8 @@ double precond_actual_shift(const ssv_precond* p);
 void matrix_spmv_dev(ssv_matrix* A, const void* d_x, void* d_y);
 void cocr_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, int maxiter, double tol,
                     int printrates, const void* d_b, void* d_x, int* iterations);
+void gmres_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, int maxiter, double tol, int restart,
+                     const void* d_b, void* d_x, int* iterations);
 void mrtr_forget(const ssv_solver* s);
 void cocr_forget(const ssv_matrix* A);
 

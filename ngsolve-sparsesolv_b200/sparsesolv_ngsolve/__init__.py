@@ -27,6 +27,7 @@ __all__ = [
     "CompactAMSPreconditioner", "CompactAMSPreconditionerImpl",
     "ComplexCompactAMSPreconditioner", "ComplexCompactAMSPreconditionerImpl", "PCGSolver",
     "BatchedCOCRSolver", "SGSPreconditioner", "SGSPreconditionerD", "SGSPreconditionerC",
+    "GMRESSolver", "GMRESSolverD", "GMRESSolverC",
 ]
 
 
@@ -513,6 +514,46 @@ class _COCRSolverBase:
 
     def IsComplex(self):
         return self._cplx
+
+
+# ---------------------------------------------------------------------------
+# GMRESSolver (ngsolve/sparsesolv_solvers.hpp:409-584, factory
+# sparsesolv_python_export.hpp:643-697)
+# ---------------------------------------------------------------------------
+
+class _GMRESSolverBase(_COCRSolverBase):
+    def __init__(self, mat, pre, freedofs=None, maxiter=500, tol=1e-8, restart=0, printrates=False):
+        super().__init__(mat, pre, freedofs, maxiter, tol, printrates)
+        self.restart = int(restart)
+
+    def Mult(self, rhs, sol):
+        b = np.ascontiguousarray(_vec_view(rhs), dtype=self._mat.dtype)
+        sv = _vec_view(sol)
+        x = np.zeros(self._mat.n, dtype=self._mat.dtype)
+        it = ctypes.c_int32(0)
+        pre_h = None if self._pre is None else self._pre._h
+        self._mat.refresh()
+        check(self._lib.ssv_gmres_solve(self._mat.h, pre_h, _capi.u8ptr(self._fd), self.maxiter, self.tol,
+                                        self.restart, _capi.vptr(b), _capi.vptr(x), ctypes.byref(it)))
+        self._iterations = it.value
+        if self.printrates:
+            print(f"GMRES: {it.value} iterations")
+        sv[...] = x
+
+
+class GMRESSolverD(_GMRESSolverBase):
+    _cplx = False
+
+
+class GMRESSolverC(_GMRESSolverBase):
+    _cplx = True
+
+
+def GMRESSolver(mat, pre, freedofs=None, maxiter=500, tol=1e-8, restart=0, printrates=False):
+    """Right-preconditioned restarted GMRES (modified Gram-Schmidt, Givens); `.iterations`."""
+    m = mat if isinstance(mat, _Matrix) else _Matrix(mat)
+    cls = GMRESSolverC if m.cplx else GMRESSolverD
+    return cls(m, pre, freedofs=freedofs, maxiter=maxiter, tol=tol, restart=restart, printrates=printrates)
 
 
 class COCRSolverD(_COCRSolverBase):

@@ -185,6 +185,8 @@ SIGNATURES = [
     ("ssv_precond_destroy", I32, [P]),
     ("ssv_cocr_solve", I32, [P, P, PU8, I32, ctypes.c_double, I32, P, P, PI32]),
     ("ssv_cocr_solve_dev", I32, [P, P, PU8, I32, ctypes.c_double, I32, P, P, PI32]),
+    ("ssv_gmres_solve", I32, [P, P, PU8, I32, ctypes.c_double, I32, P, P, PI32]),
+    ("ssv_gmres_solve_dev", I32, [P, P, PU8, I32, ctypes.c_double, I32, P, P, PI32]),
     ("ssv_abmc_build", I32, [I32, PI32, PI32, I32, I32, PI32, PI32, PI32, PI32, PI32, PI32]),
     ("ssv_level_schedule", I32, [I32, PI32, PI32, I32, PI32, PI32]),
     ("ssv_rcm_order", I32, [I32, PI32, PI32, PI32, PI32]),
