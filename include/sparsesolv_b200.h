@@ -189,6 +189,17 @@ int ssv_ic_create(ssv_matrix* A, const uint8_t* freedofs, double shift,
  * on constrained DOFs. ssv_precond_update computes it (the factory calls it
  * once), ssv_precond_apply[_dev] applies it, ssv_precond_destroy frees it. */
 int ssv_sgs_create(ssv_matrix* A, const uint8_t* freedofs, ssv_precond** out);
+/* CompactAMGPreconditioner factory (sparsesolv_python_export.hpp:359-404) over
+ * CompactAMG (preconditioners/compact_amg.hpp:49-183): PMIS coarsening, direct
+ * interpolation, Galerkin coarse matrices, l1-Jacobi smoothing, a direct
+ * coarsest solve below 10*min_coarse rows; set up on the FreeDofs view of the
+ * real matrix A (SSV_ERR_TYPE for complex); Mult = one V-cycle from x = 0 with
+ * constrained outputs zeroed (ssv_precond_apply[_dev]); ssv_precond_update
+ * rebuilds it from A's current values. */
+int ssv_amg_create(ssv_matrix* A, const uint8_t* freedofs, double theta, int32_t max_levels,
+                   int32_t min_coarse, int32_t num_smooth, ssv_precond** out);
+/* AMG hierarchy of a CompactAMG handle: sizes[2l] = rows, sizes[2l+1] = nnz. */
+int ssv_amg_levels(const ssv_precond* p, int32_t* sizes, int32_t cap, int32_t* num_levels);
 /* Options of SparseSolvICPreconditioner (sparsesolv_precond.hpp:200-223):
  * use_abmc, abmc_block_size, abmc_num_colors, diagonal_scaling, shift and the
  * auto-shift fields are read from cfg; they take effect at the next update. */

@@ -1863,11 +1863,130 @@ void ams_profile(AmsState* a, int nrhs, int reps, int flags, ssv_phase_profile* 
     else ams_profile_nrhs<double>(*a, nrhs, std::max(reps, 1), cold, out);
 }
 
+// ---------------------------------------------------------------------------
+// CompactAMGPreconditioner (compact_amg.hpp:49-183, factory
+// sparsesolv_python_export.hpp:359-404): one AMG hierarchy of a scalar H1
+// matrix (FreeDofs view), set up on the host like the AMS subspaces, and
+// Mult = x = 0, one V-cycle, constrained outputs zeroed, FP64 on the device.
+// ---------------------------------------------------------------------------
+struct AmgOnly {
+    AmgHost host;
+    std::vector<AmgDevLevel> lev;
+    TailSet tail;  // not used: the per-level launch chain
+    bool has_fd = false;
+    std::vector<uint8_t> h_fd;
+    DevBuf<uint8_t> fd;
+    int n = 0, num_smooth = 1;
+    unsigned gen = 0;
+};
+
+void amg_free(AmgOnly* g) { delete g; }
+
+static void amg_rebuild(AmgOnly& g, const ssv_matrix* A) {
+    cudaStream_t s = stream();
+    HostCsr H = host_csr_of(A);
+    if (g.has_fd)  // CreateBCModifiedMatrix (compact_amg.hpp:252-287)
+        for (int i = 0; i < H.n; ++i)
+            for (int k = H.rp[i]; k < H.rp[i + 1]; ++k) {
+                const int j = H.ci[k];
+                if (!g.h_fd[i]) H.v[k] = (j == i) ? 1.0 : 0.0;
+                else if (!g.h_fd[j]) H.v[k] = 0.0;
+            }
+    g.host.setup(H);
+    const auto& hl = g.host.levels;
+    g.lev.clear();
+    g.lev.resize(hl.size());
+    for (size_t l = 0; l < hl.size(); ++l) {
+        AmgDevLevel& dl = g.lev[l];
+        const int nl = hl[l].A.n;
+        dl.A.upload(hl[l].A, false, s);
+        dl.l1.set(hl[l].l1, false, s);
+        dl.il1.set(reciprocal(hl[l].l1), false, s);
+        if (l + 1 < hl.size()) {
+            dl.P.upload(hl[l].P, false, s);
+            dl.Pt.upload(hl[l].Pt, false, s);
+        }
+        dl.direct = hl[l].direct;
+        if (dl.direct) {
+            dl.Li.upload(hl[l].linv.data(), hl[l].linv.size(), s);
+            dl.LiT.upload(hl[l].linvt.data(), hl[l].linvt.size(), s);
+            dl.piv.upload(hl[l].piv.data(), hl[l].piv.size(), s);
+            dl.cz.alloc(nl);
+        }
+        dl.b.alloc(nl);
+        dl.xa.alloc(nl);
+        dl.xb.alloc(nl);
+        dl.r.alloc(nl);
+    }
+    g.tail.start = -1;
+    cudaEvent_t e0, e1;
+    SSV_CUDA(cudaEventCreate(&e0));
+    SSV_CUDA(cudaEventCreate(&e1));
+    for (size_t l = 0; l < g.lev.size(); ++l) {
+        AmgDevLevel& L = g.lev[l];
+        tune_csr<double, double, double, 1>(L.A, L.xa.as<double>(), L.xb.as<double>(), L.b.as<double>(), s, e0, e1);
+        if (l + 1 < g.lev.size()) {
+            tune_csr<double, double, double, 1>(L.P, g.lev[l + 1].xa.as<double>(), L.r.as<double>(), nullptr, s, e0,
+                                                e1);
+            tune_csr<double, double, double, 1>(L.Pt, L.r.as<double>(), g.lev[l + 1].b.as<double>(), nullptr, s, e0,
+                                                e1);
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ++g.gen;
+    SSV_CUDA(cudaStreamSynchronize(s));
+}
+
+AmgOnly* amg_create(const ssv_matrix* A, const uint8_t* fd, double theta, int max_levels, int min_coarse,
+                    int num_smooth) {
+    auto* g = new AmgOnly();
+    try {
+        g->n = A->rows;
+        g->num_smooth = std::max(1, num_smooth);
+        g->host.theta = theta;
+        g->host.max_levels = std::max(1, max_levels);
+        g->host.min_coarse = min_coarse;
+        g->host.num_smooth = g->num_smooth;
+        if (fd) {
+            g->has_fd = true;
+            g->h_fd.assign(fd, fd + g->n);
+            for (auto& v : g->h_fd) v = v ? 1 : 0;
+            g->fd.upload(g->h_fd.data(), g->h_fd.size(), stream());
+        }
+        amg_rebuild(*g, A);
+    } catch (...) {
+        delete g;
+        throw;
+    }
+    return g;
+}
+
+void amg_update(AmgOnly* g, const ssv_matrix* A) { amg_rebuild(*g, A); }
+
+int amg_levels(const AmgOnly* g, int* sizes, int cap) {
+    const auto& hl = g->host.levels;
+    for (size_t l = 0; l < hl.size() && 2 * (int)l + 1 < cap; ++l) {
+        sizes[2 * l] = hl[l].A.n;
+        sizes[2 * l + 1] = hl[l].A.nnz();
+    }
+    return (int)hl.size();
+}
+
+// Mult (compact_amg.hpp:166-183): x = 0, VCycle(0, b, x), constrained x = 0
+static void amg_apply(AmgOnly& g, const double* x, double* y, const KState* st, cudaStream_t s) {
+    const double* res = vcycle<double, 1, false>(g.lev, g.tail, 0, x, g.num_smooth, st, s);
+    launch_k(k_mv_mask_copy<double, double, 1>, grid_for(g.n, kBlock), kBlock, s, g.n, res,
+             (const uint8_t*)(g.has_fd ? g.fd.get() : nullptr), y, st);
+    SSV_LAUNCH_CHECK();
+}
+
 // y = M^{-1} x for the preconditioner p, stream-ordered and capturable.
 template <>
 void precond_apply_any<double>(ssv_precond* p, const double* x, double* y, const KState* st, cudaStream_t s) {
     if (p->kind == 1) ic_apply_dev<double>(p, x, y, st, s);
     else if (p->kind == 4) sgs_apply_dev<double>(p, x, y, st, s);
+    else if (p->kind == 5) amg_apply(*p->amg, x, y, st, s);
     else if (p->kind == 2) {
         if (p->ams->fp32) ams_cycle<float, 1, false>(*p->ams, x, y, st, s);
         else ams_cycle<double, 1, false>(*p->ams, x, y, st, s);
@@ -1889,6 +2008,7 @@ void precond_apply_any<zdouble>(ssv_precond* p, const zdouble* x, zdouble* y, co
 unsigned precond_generation(const ssv_precond* p) {
     if (p->kind == 1) return p->A->dtype == SSV_F64 ? p->ic_d.gen : p->ic_z.gen;
     if (p->kind == 4) return p->A->dtype == SSV_F64 ? p->sgs_d.gen : p->sgs_z.gen;
+    if (p->kind == 5) return p->amg ? p->amg->gen : 0;
     return p->ams ? p->ams->gen : 0;
 }
 

@@ -325,6 +325,39 @@ int ssv_sgs_create(ssv_matrix* A, const uint8_t* freedofs, ssv_precond** out) {
     });
 }
 
+int ssv_amg_create(ssv_matrix* A, const uint8_t* freedofs, double theta, int32_t max_levels, int32_t min_coarse,
+                   int32_t num_smooth, ssv_precond** out) {
+    return guarded([&] {
+        if (!A || !out) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_amg_create: NULL argument");
+        if (A->dtype != SSV_F64)
+            ssv::fail(SSV_ERR_TYPE, "CompactAMGPreconditioner: expected real SparseMatrix<double>");
+        if (A->rows != A->cols) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_amg_create: matrix must be square");
+        auto* p = new ssv_precond();
+        p->kind = 5;
+        p->A = A;
+        p->vdtype = SSV_F64;
+        p->n = A->rows;
+        ssv_config_default(&p->cfg);
+        try {
+            check_mask(freedofs, A->rows, p->h_fd, p->fd, p->has_fd);
+            p->amg.reset(ssv::amg_create(A, p->has_fd ? p->h_fd.data() : nullptr, theta, max_levels, min_coarse,
+                                         num_smooth));
+            p->ready = true;
+        } catch (...) {
+            delete p;
+            throw;
+        }
+        *out = p;
+    });
+}
+
+int ssv_amg_levels(const ssv_precond* p, int32_t* sizes, int32_t cap, int32_t* num_levels) {
+    return guarded([&] {
+        if (!p || !p->amg || !sizes || !num_levels) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_amg_levels: bad argument");
+        *num_levels = ssv::amg_levels(p->amg.get(), sizes, cap);
+    });
+}
+
 int ssv_ams_create(ssv_matrix* A, ssv_matrix* G, const uint8_t* freedofs, const double* coord_x,
                    const double* coord_y, const double* coord_z, int32_t cycle_type, int32_t num_smooth,
                    double theta, double correction_weight, int32_t complex_form, int32_t ndof_complex,

@@ -294,10 +294,12 @@ struct ssv_solver {
 namespace ssv {
 struct AmsState;
 void ams_free(AmsState* a);
+struct AmgOnly;
+void amg_free(AmgOnly* g);
 }  // namespace ssv
 
 struct ssv_precond {
-    int kind = 0;    // 1 = IC, 2 = CompactAMS (real), 3 = ComplexCompactAMS, 4 = SGS
+    int kind = 0;    // 1 = IC, 2 = CompactAMS (real), 3 = ComplexCompactAMS, 4 = SGS, 5 = CompactAMG
     int vdtype = 0;  // scalar type of the vectors it applies to
     int n = 0;       // vector length
     ssv_matrix* A = nullptr;
@@ -313,5 +315,6 @@ struct ssv_precond {
     ssv::SgsDevice<ssv::zdouble> sgs_z;
     ssv::DevBuf<double> xw, yw, io_x, io_y;
     std::unique_ptr<ssv::AmsState, void (*)(ssv::AmsState*)> ams{nullptr, ssv::ams_free};
+    std::unique_ptr<ssv::AmgOnly, void (*)(ssv::AmgOnly*)> amg{nullptr, ssv::amg_free};
     virtual ~ssv_precond() = default;
 };

@@ -1214,15 +1214,17 @@ void ic_apply_dev(ssv_precond* p, const S* x, S* y, const KState* st, cudaStream
 }
 
 void precond_update(ssv_precond* p) {
-    if (p->kind == 4) sgs_update(p);
+    if (p->kind == 5) amg_update(p->amg.get(), p->A);
+    else if (p->kind == 4) sgs_update(p);
     else if (p->A->dtype == SSV_F64) ic_update<double>(p);
     else ic_update<zdouble>(p);
 }
 
 void precond_apply_dev(ssv_precond* p, const void* d_x, void* d_y) {
     if (!p->ready)
-        fail(SSV_ERR_RUNTIME, p->kind == 4 ? "SGSPreconditioner::apply called before setup"
-                                           : "ICPreconditioner::apply called before setup");
+        fail(SSV_ERR_RUNTIME, p->kind == 4   ? "SGSPreconditioner::apply called before setup"
+                              : p->kind == 5 ? "CompactAMG::Mult called before Setup"
+                                             : "ICPreconditioner::apply called before setup");
     if (p->vdtype == SSV_F64)
         precond_apply_any<double>(p, static_cast<const double*>(d_x), static_cast<double*>(d_y), nullptr, stream());
     else

@@ -45,6 +45,11 @@ AmsState* ams_create(const ssv_matrix* A, const ssv_matrix* G, const uint8_t* fd
                      const double* cy, const double* cz, int cycle_type, int num_smooth, double theta, double w,
                      int complex_form, int ndof_complex);
 void ams_update(AmsState* a, const ssv_matrix* A);
+// CompactAMGPreconditioner (ams.cu): host set-up, FP64 V-cycle on the device
+AmgOnly* amg_create(const ssv_matrix* A, const uint8_t* fd, double theta, int max_levels, int min_coarse,
+                    int num_smooth);
+void amg_update(AmgOnly* g, const ssv_matrix* A);
+int amg_levels(const AmgOnly* g, int* sizes, int cap);
 int ams_levels(const AmsState* a, int sub, int* sizes, int cap);
 void ams_set_precision(AmsState* a, int precision);
 int ams_precision(const AmsState* a);

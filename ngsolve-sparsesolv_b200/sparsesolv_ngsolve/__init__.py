@@ -27,7 +27,7 @@ __all__ = [
     "CompactAMSPreconditioner", "CompactAMSPreconditionerImpl",
     "ComplexCompactAMSPreconditioner", "ComplexCompactAMSPreconditionerImpl", "PCGSolver",
     "BatchedCOCRSolver", "SGSPreconditioner", "SGSPreconditionerD", "SGSPreconditionerC",
-    "GMRESSolver", "GMRESSolverD", "GMRESSolverC",
+    "GMRESSolver", "GMRESSolverD", "GMRESSolverC", "CompactAMGPreconditioner", "CompactAMGPreconditionerImpl",
 ]
 
 
@@ -461,6 +461,46 @@ def SGSPreconditioner(mat, freedofs=None):
     p = (SGSPreconditionerC if cplx else SGSPreconditionerD)(mat, freedofs)
     p.Update()
     return p
+
+
+# ---------------------------------------------------------------------------
+# CompactAMGPreconditioner (sparsesolv_python_export.hpp:339-404)
+# ---------------------------------------------------------------------------
+
+class CompactAMGPreconditionerImpl(_PrecondBase):
+    """CompactAMG (compact_amg.hpp:49-183): V-cycle preconditioner of a real H1 matrix."""
+
+    _cplx = False
+
+    def __init__(self, mat, freedofs=None, theta=0.25, max_levels=25, min_coarse=50, num_smooth=1,
+                 print_level=0):
+        self._mat = mat if isinstance(mat, _Matrix) else _Matrix(mat)
+        if self._mat.cplx:
+            raise TypeError("CompactAMGPreconditioner: expected real SparseMatrix<double>")
+        self._n = self._mat.n
+        self._dtype = np.float64
+        self._fd = _freedofs_array(freedofs, self._n)
+        lib = _capi.load()
+        h = ctypes.c_void_p()
+        check(lib.ssv_amg_create(self._mat.h, _capi.u8ptr(self._fd), float(theta), int(max_levels),
+                                 int(min_coarse), int(num_smooth), ctypes.byref(h)))
+        self._init_handle(h)
+        if print_level > 0:
+            lv = self.levels()
+            print(f"  CompactAMG: {len(lv)} levels, coarsest = {lv[-1][0]} DOFs")
+
+    def levels(self):
+        """[(rows, nnz), ...] of the AMG hierarchy."""
+        buf = np.zeros(256, np.int32)
+        nl = ctypes.c_int32()
+        check(self._lib.ssv_amg_levels(self._h, _capi.i32ptr(buf), 256, ctypes.byref(nl)))
+        return [(int(buf[2 * l]), int(buf[2 * l + 1])) for l in range(nl.value)]
+
+
+def CompactAMGPreconditioner(mat, freedofs=None, theta=0.25, max_levels=25, min_coarse=50, num_smooth=1,
+                             print_level=0):
+    """Compact algebraic multigrid (PMIS, direct interpolation, l1-Jacobi) for scalar H1 problems."""
+    return CompactAMGPreconditionerImpl(mat, freedofs, theta, max_levels, min_coarse, num_smooth, print_level)
 
 
 # ---------------------------------------------------------------------------

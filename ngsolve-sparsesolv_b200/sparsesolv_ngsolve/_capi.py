@@ -178,6 +178,8 @@ SIGNATURES = [
     ("ssv_ic_create", I32, [P, PU8, ctypes.c_double, PP]),
     ("ssv_ic_set_config", I32, [P, ctypes.POINTER(ssv_config)]),
     ("ssv_sgs_create", I32, [P, PU8, PP]),
+    ("ssv_amg_create", I32, [P, PU8, ctypes.c_double, I32, I32, I32, PP]),
+    ("ssv_amg_levels", I32, [P, PI32, I32, PI32]),
     ("ssv_precond_update", I32, [P]),
     ("ssv_precond_apply", I32, [P, P, P]),
     ("ssv_precond_apply_dev", I32, [P, P, P]),

@@ -745,6 +745,50 @@ void ams_oracle_apply_complex(void* h, const double* f, double* u) {
                                         reinterpret_cast<std::complex<double>*>(u));
 }
 
+// CompactAMGPreconditioner (compact_amg.hpp:49-183): Setup on the FreeDofs
+// view (CreateBCModifiedMatrix, :72-79) and Mult = x = 0, VCycle, constrained
+// outputs zeroed (:166-183).
+struct AmgOnly {
+    Amg amg;
+    std::vector<unsigned char> fd;
+};
+
+void* ams_oracle_amg_create(int n, const int* rp, const int* ci, const double* v, const unsigned char* fd,
+                            double theta, int max_levels, int min_coarse, int num_smooth) {
+    AmgOnly* g = new AmgOnly();
+    Csr A = make_csr(n, n, rp, ci, v);
+    if (fd) {
+        g->fd.assign(fd, fd + n);
+        A = bc_modified(A, fd);
+    }
+    g->amg.theta = theta;
+    g->amg.max_levels = max_levels;
+    g->amg.min_coarse = min_coarse;
+    g->amg.num_smooth = num_smooth;
+    g->amg.setup(A);
+    return g;
+}
+
+void ams_oracle_amg_apply(void* h, const double* b, double* x) {
+    AmgOnly* g = static_cast<AmgOnly*>(h);
+    g->amg.apply(b, x);
+    if (!g->fd.empty())
+        for (size_t i = 0; i < g->fd.size(); ++i)
+            if (!g->fd[i]) x[i] = 0.0;
+}
+
+int ams_oracle_amg_levels(void* h, int* sizes, int cap) {
+    const Amg& m = static_cast<AmgOnly*>(h)->amg;
+    const int nl = (int)m.lv.size();
+    for (int l = 0; l < nl && 2 * l + 1 < cap; ++l) {
+        sizes[2 * l] = m.lv[l].A.n;
+        sizes[2 * l + 1] = m.lv[l].A.nnz();
+    }
+    return nl;
+}
+
+void ams_oracle_amg_destroy(void* h) { delete static_cast<AmgOnly*>(h); }
+
 // Hierarchy shape: for subspace s (0 = G, 1..3 = Pi x,y,z) the number of
 // levels, and per level (rows, nnz) into sizes[2*l], sizes[2*l+1].
 int ams_oracle_levels(void* h, int s, int* sizes, int cap) {

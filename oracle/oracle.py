@@ -200,6 +200,39 @@ def level_schedule(rp, ci, n, upper=False, which="port"):
     return lev[:n], nl.value
 
 
+class AmgOracle:
+    """CPU restatement of CompactAMGPreconditioner (compact_amg.hpp:49-183)."""
+
+    def __init__(self, A, freedofs=None, theta=0.25, max_levels=25, min_coarse=50, num_smooth=1):
+        lib = AmsOracle.lib()
+        D = ctypes.POINTER(ctypes.c_double)
+        rp = np.ascontiguousarray(A.indptr, np.int32)
+        ci = np.ascontiguousarray(A.indices, np.int32)
+        v = np.ascontiguousarray(A.data, np.float64)
+        fd = None if freedofs is None else np.ascontiguousarray(freedofs, np.uint8)
+        self.n = A.shape[0]
+        self.h = lib.ams_oracle_amg_create(self.n, _p(rp), _p(ci), v.ctypes.data_as(D), _p(fd, PU8), float(theta),
+                                           int(max_levels), int(min_coarse), int(num_smooth))
+
+    def apply(self, b):
+        D = ctypes.POINTER(ctypes.c_double)
+        bb = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.n)
+        AmsOracle.lib().ams_oracle_amg_apply(self.h, bb.ctypes.data_as(D), x.ctypes.data_as(D))
+        return x
+
+    def levels(self):
+        buf = np.zeros(256, np.int32)
+        nl = AmsOracle.lib().ams_oracle_amg_levels(self.h, _p(buf), 256)
+        return [(int(buf[2 * l]), int(buf[2 * l + 1])) for l in range(nl)]
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            AmsOracle.lib().ams_oracle_amg_destroy(h)
+            self.h = None
+
+
 class AmsOracle:
     """CPU restatement of CompactAMS / ComplexCompactAMS (oracle/ams_oracle.cpp)."""
 
@@ -226,6 +259,12 @@ class AmsOracle:
             lib.ams_oracle_cocr.restype = I32
             lib.ams_oracle_cocr.argtypes = [P, I32, PI32, PI32, D, PU8, I32, ctypes.c_double, D, D, PI32, D, I32,
                                             PI32]
+            lib.ams_oracle_amg_create.restype = ctypes.c_void_p
+            lib.ams_oracle_amg_create.argtypes = [I32, PI32, PI32, D, PU8, ctypes.c_double, I32, I32, I32]
+            lib.ams_oracle_amg_apply.argtypes = [P, D, D]
+            lib.ams_oracle_amg_levels.restype = I32
+            lib.ams_oracle_amg_levels.argtypes = [P, PI32, I32]
+            lib.ams_oracle_amg_destroy.argtypes = [P]
             lib.ams_oracle_set_threads.restype = None
             lib.ams_oracle_set_threads.argtypes = [I32]
             lib.ams_oracle_set_threads(1)
