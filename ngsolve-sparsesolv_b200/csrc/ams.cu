@@ -402,28 +402,29 @@ k_mv_coarse_bwd(int n, const double* __restrict__ LiT, const double* __restrict_
 }
 
 // ---------------------------------------------------------------------------
-// The three nodal V-cycles in lockstep: one launch carries the same step of
-// the x, y and z hierarchies (blockIdx.y picks the subspace), so the three
-// chains of small per-level launches become one chain with three times the
-// work per launch. Same arithmetic per subspace as the single-hierarchy
-// kernels above.
+// V-cycles in lockstep: one launch carries the same step of up to K
+// hierarchies (blockIdx.y picks the hierarchy) -- the x, y and z nodal
+// hierarchies of one AMS (K = 3), or the hierarchies of several AMS
+// preconditioners applied together -- so K chains of small per-level
+// launches become one chain with K times the work per launch. Same
+// arithmetic per hierarchy as the single-hierarchy kernels above.
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, int K = 3>
 struct Tri {
-    int n[3];
-    const int* rp[3];
-    const int* ci[3];
-    const T* v[3];
-    const T* x[3];
-    T* y[3];
-    const T* b[3];
-    const T* d[3];
-    T* r[3];
+    int n[K];
+    const int* rp[K];
+    const int* ci[K];
+    const T* v[K];
+    const T* x[K];
+    T* y[K];
+    const T* b[K];
+    const T* d[K];
+    T* r[K];
 };
 
-template <typename T, int NV, int LANES, int MODE, bool RECIP>
+template <typename T, int NV, int LANES, int MODE, bool RECIP, int K = 3>
 __global__ void __launch_bounds__(kBlock)
-k_mv3_spmv(Tri<T> t, T w, const KState* st) {
+k_mv3_spmv(Tri<T, K> t, T w, const KState* st) {
     pdl_gate();
     if (st && st->done) return;
     const int q = blockIdx.y;
@@ -475,9 +476,9 @@ k_mv3_spmv(Tri<T> t, T w, const KState* st) {
     }
 }
 
-template <typename T, int NV, int LANES, bool RECIP>
+template <typename T, int NV, int LANES, bool RECIP, int K = 3>
 __global__ void __launch_bounds__(kBlock)
-k_mv3_first_res(Tri<T> t, const KState* st) {
+k_mv3_first_res(Tri<T, K> t, const KState* st) {
     pdl_gate();
     if (st && st->done) return;
     const int q = blockIdx.y;
@@ -527,17 +528,18 @@ k_mv3_first_res(Tri<T> t, const KState* st) {
 }
 
 // coarsest LDL^T solves of the three hierarchies: Li/LiT/piv/cz per subspace
+template <int K = 3>
 struct TriCoarse {
-    int n[3];
-    const double* M[3];    // L^{-1} (forward) or its transpose (backward)
-    const double* piv[3];
-    double* cz[3];
-    const void* io[3];     // forward: b (hierarchy type); backward: x output
+    int n[K];
+    const double* M[K];    // L^{-1} (forward) or its transpose (backward)
+    const double* piv[K];
+    double* cz[K];
+    const void* io[K];     // forward: b (hierarchy type); backward: x output
 };
 
-template <typename T, int NV, bool FWD>
+template <typename T, int NV, bool FWD, int K = 3>
 __global__ void __launch_bounds__(kBlock)
-k_mv3_coarse(TriCoarse t, const KState* st) {
+k_mv3_coarse(TriCoarse<K> t, const KState* st) {
     pdl_gate();
     if (st && st->done) return;
     const int q = blockIdx.y;
@@ -1015,94 +1017,123 @@ static T* vcycle(std::vector<AmgDevLevel>& L, const TailSet& tail, int l, const 
 // ---- the three nodal V-cycles in lockstep --------------------------------
 static bool tri_ok(const AmsState& a) {
     if (!a.tri) return false;
-    const size_t L = a.amg[1].size();
-    if (L < 1 || a.amg[2].size() != L || a.amg[3].size() != L) return false;
     for (int k = 1; k < 4; ++k) {
-        if (a.tails[k].start >= 0) return false;
-        if (a.amg[k].back().direct != a.amg[1].back().direct || !a.amg[k].back().direct) return false;
+        if (a.amg[k].empty() || a.tails[k].start >= 0 || !a.amg[k].back().direct) return false;
     }
     return true;
 }
 
-template <typename T, int NV, int MODE, bool RECIP>
-static void spmv3(const Tri<T>& t, int lanes, T w, const KState* st, cudaStream_t s) {
-    const int nmax = std::max(t.n[0], std::max(t.n[1], t.n[2]));
+template <typename T, int K>
+static int parts_nmax(const Tri<T, K>& t, int parts) {
+    int m = 0;
+    for (int k = 0; k < parts; ++k) m = std::max(m, t.n[k]);
+    return m;
+}
+
+template <typename T, int NV, int MODE, bool RECIP, int K>
+static void spmv3(const Tri<T, K>& t, int parts, int lanes, T w, const KState* st, cudaStream_t s) {
     const int rpb = kBlock / lanes;
-    const dim3 grid(std::max(1, std::min((nmax + rpb - 1) / rpb, sm_count() * 8 / 3)), 3);
+    const dim3 grid(std::max(1, std::min((parts_nmax(t, parts) + rpb - 1) / rpb, sm_count() * 8 / parts)), parts);
     switch (lanes) {
-        case 2: launch_k(k_mv3_spmv<T, NV, 2, MODE, RECIP>, grid, kBlock, s, t, w, st); break;
-        case 4: launch_k(k_mv3_spmv<T, NV, 4, MODE, RECIP>, grid, kBlock, s, t, w, st); break;
-        case 8: launch_k(k_mv3_spmv<T, NV, 8, MODE, RECIP>, grid, kBlock, s, t, w, st); break;
-        case 16: launch_k(k_mv3_spmv<T, NV, 16, MODE, RECIP>, grid, kBlock, s, t, w, st); break;
-        default: launch_k(k_mv3_spmv<T, NV, 32, MODE, RECIP>, grid, kBlock, s, t, w, st); break;
+        case 2: launch_k(k_mv3_spmv<T, NV, 2, MODE, RECIP, K>, grid, kBlock, s, t, w, st); break;
+        case 4: launch_k(k_mv3_spmv<T, NV, 4, MODE, RECIP, K>, grid, kBlock, s, t, w, st); break;
+        case 8: launch_k(k_mv3_spmv<T, NV, 8, MODE, RECIP, K>, grid, kBlock, s, t, w, st); break;
+        case 16: launch_k(k_mv3_spmv<T, NV, 16, MODE, RECIP, K>, grid, kBlock, s, t, w, st); break;
+        default: launch_k(k_mv3_spmv<T, NV, 32, MODE, RECIP, K>, grid, kBlock, s, t, w, st); break;
     }
 }
 
-template <typename T, int NV, bool RECIP>
-static void first_res3(const Tri<T>& t, int lanes, const KState* st, cudaStream_t s) {
-    const int nmax = std::max(t.n[0], std::max(t.n[1], t.n[2]));
+template <typename T, int NV, bool RECIP, int K>
+static void first_res3(const Tri<T, K>& t, int parts, int lanes, const KState* st, cudaStream_t s) {
     const int rpb = kBlock / lanes;
-    const dim3 grid(std::max(1, std::min((nmax + rpb - 1) / rpb, sm_count() * 8 / 3)), 3);
+    const dim3 grid(std::max(1, std::min((parts_nmax(t, parts) + rpb - 1) / rpb, sm_count() * 8 / parts)), parts);
     switch (lanes) {
-        case 2: launch_k(k_mv3_first_res<T, NV, 2, RECIP>, grid, kBlock, s, t, st); break;
-        case 4: launch_k(k_mv3_first_res<T, NV, 4, RECIP>, grid, kBlock, s, t, st); break;
-        case 8: launch_k(k_mv3_first_res<T, NV, 8, RECIP>, grid, kBlock, s, t, st); break;
-        case 16: launch_k(k_mv3_first_res<T, NV, 16, RECIP>, grid, kBlock, s, t, st); break;
-        default: launch_k(k_mv3_first_res<T, NV, 32, RECIP>, grid, kBlock, s, t, st); break;
+        case 2: launch_k(k_mv3_first_res<T, NV, 2, RECIP, K>, grid, kBlock, s, t, st); break;
+        case 4: launch_k(k_mv3_first_res<T, NV, 4, RECIP, K>, grid, kBlock, s, t, st); break;
+        case 8: launch_k(k_mv3_first_res<T, NV, 8, RECIP, K>, grid, kBlock, s, t, st); break;
+        case 16: launch_k(k_mv3_first_res<T, NV, 16, RECIP, K>, grid, kBlock, s, t, st); break;
+        default: launch_k(k_mv3_first_res<T, NV, 32, RECIP, K>, grid, kBlock, s, t, st); break;
     }
 }
 
-// V-cycles of subspaces 1..3 from their right-hand sides a.rs[1..3]; returns
-// the result buffers (each level 0's post-sweep buffer).
-template <typename T, int NV, bool RECIP>
-static void vcycle3(AmsState& a, const KState* st, cudaStream_t s, T* out[3]) {
-    const int L = (int)a.amg[1].size();
-    auto rhs = [&](int k, int l) -> const T* { return l == 0 ? a.rs[k + 1].as<T>() : a.amg[k + 1][l].b.as<T>(); };
-    auto lv = [&](int k, int l) -> AmgDevLevel& { return a.amg[k + 1][l]; };
-    for (int l = 0; l < L - 1; ++l) {
-        Tri<T> fr{}, rs{};
-        for (int k = 0; k < 3; ++k) {
+// Hierarchies H[0..parts) (direct coarsest, num_smooth 1, level counts may
+// differ) in lockstep from right-hand sides rhs0[k]; out[k] = each level 0's
+// result. Every hierarchy keeps its own order of steps -- its down levels,
+// its coarsest solve, its up levels -- and a launch carries the hierarchies
+// that have a step at that level: the down sweep of level l those with more
+// than l+1 levels, then one pair of launches for all coarsest solves, then
+// the up sweep of level l those with more than l+1 levels.
+template <typename T, int NV, bool RECIP, int K>
+static void vcycleM(std::vector<AmgDevLevel>* const* H, const T* const* rhs0, int parts, const KState* st,
+                    cudaStream_t s, T** out) {
+    int Lmax = 0;
+    for (int k = 0; k < parts; ++k) Lmax = std::max(Lmax, (int)H[k]->size());
+    auto L = [&](int k) { return (int)H[k]->size(); };
+    auto rhs = [&](int k, int l) -> const T* { return l == 0 ? rhs0[k] : (*H[k])[l].b.template as<T>(); };
+    auto lv = [&](int k, int l) -> AmgDevLevel& { return (*H[k])[l]; };
+    for (int l = 0; l < Lmax - 1; ++l) {
+        Tri<T, K> fr{}, rs{};
+        int q = 0, k0 = -1;
+        for (int k = 0; k < parts; ++k) {
+            if (l >= L(k) - 1) continue;
+            if (k0 < 0) k0 = k;
             AmgDevLevel& v = lv(k, l);
-            fr.n[k] = v.A.n; fr.rp[k] = v.A.rp.get(); fr.ci[k] = v.A.ci.get(); fr.v[k] = v.A.val<T>();
-            fr.b[k] = rhs(k, l); fr.d[k] = l1_of<T, RECIP>(v); fr.y[k] = v.xa.as<T>(); fr.r[k] = v.r.as<T>();
-            rs.n[k] = v.Pt.n; rs.rp[k] = v.Pt.rp.get(); rs.ci[k] = v.Pt.ci.get(); rs.v[k] = v.Pt.val<T>();
-            rs.x[k] = v.r.as<T>(); rs.y[k] = lv(k, l + 1).b.template as<T>();
+            fr.n[q] = v.A.n; fr.rp[q] = v.A.rp.get(); fr.ci[q] = v.A.ci.get(); fr.v[q] = v.A.val<T>();
+            fr.b[q] = rhs(k, l); fr.d[q] = l1_of<T, RECIP>(v); fr.y[q] = v.xa.as<T>(); fr.r[q] = v.r.as<T>();
+            rs.n[q] = v.Pt.n; rs.rp[q] = v.Pt.rp.get(); rs.ci[q] = v.Pt.ci.get(); rs.v[q] = v.Pt.val<T>();
+            rs.x[q] = v.r.as<T>(); rs.y[q] = lv(k, l + 1).b.template as<T>();
+            ++q;
         }
-        first_res3<T, NV, RECIP>(fr, lv(0, l).A.lanes_for(NV), st, s);
-        spmv3<T, NV, MV_AX, RECIP>(rs, lv(0, l).Pt.lanes_for(NV), T(0), st, s);
+        if (q == 0) continue;
+        first_res3<T, NV, RECIP, K>(fr, q, lv(k0, l).A.lanes_for(NV), st, s);
+        spmv3<T, NV, MV_AX, RECIP, K>(rs, q, lv(k0, l).Pt.lanes_for(NV), T(0), st, s);
     }
-    {   // coarsest: LDL^T pseudo-inverse, FP64
-        TriCoarse f{}, b{};
+    {   // coarsest levels: LDL^T pseudo-inverse, FP64
+        TriCoarse<K> f{}, b{};
         int nmax = 0;
-        for (int k = 0; k < 3; ++k) {
-            AmgDevLevel& v = lv(k, L - 1);
+        for (int k = 0; k < parts; ++k) {
+            AmgDevLevel& v = lv(k, L(k) - 1);
             nmax = std::max(nmax, v.A.n);
             f.n[k] = b.n[k] = v.A.n;
             f.M[k] = v.Li.get(); b.M[k] = v.LiT.get();
             f.piv[k] = b.piv[k] = v.piv.get();
             f.cz[k] = b.cz[k] = v.cz.get();
-            f.io[k] = rhs(k, L - 1);
+            f.io[k] = rhs(k, L(k) - 1);
             b.io[k] = v.xa.raw.get();
         }
-        const dim3 grid(std::max(1, std::min((nmax + 7) / 8, sm_count() * 4 / 3)), 3);
-        launch_k(k_mv3_coarse<T, NV, true>, grid, kBlock, s, f, st);
-        launch_k(k_mv3_coarse<T, NV, false>, grid, kBlock, s, b, st);
+        const dim3 grid(std::max(1, std::min((nmax + 7) / 8, std::max(1, sm_count() * 4 / parts))), parts);
+        launch_k(k_mv3_coarse<T, NV, true, K>, grid, kBlock, s, f, st);
+        launch_k(k_mv3_coarse<T, NV, false, K>, grid, kBlock, s, b, st);
     }
-    for (int l = L - 2; l >= 0; --l) {
-        Tri<T> pa{}, js{};
-        for (int k = 0; k < 3; ++k) {
+    for (int l = Lmax - 2; l >= 0; --l) {
+        Tri<T, K> pa{}, js{};
+        int q = 0, k0 = -1;
+        for (int k = 0; k < parts; ++k) {
+            if (l > L(k) - 2) continue;
+            if (k0 < 0) k0 = k;
             AmgDevLevel& v = lv(k, l);
             AmgDevLevel& nx = lv(k, l + 1);
-            const T* e = (l + 1 == L - 1) ? nx.xa.as<T>() : nx.xb.as<T>();
-            pa.n[k] = v.P.n; pa.rp[k] = v.P.rp.get(); pa.ci[k] = v.P.ci.get(); pa.v[k] = v.P.val<T>();
-            pa.x[k] = e; pa.y[k] = v.xa.as<T>();
-            js.n[k] = v.A.n; js.rp[k] = v.A.rp.get(); js.ci[k] = v.A.ci.get(); js.v[k] = v.A.val<T>();
-            js.x[k] = v.xa.as<T>(); js.y[k] = v.xb.as<T>(); js.b[k] = rhs(k, l); js.d[k] = l1_of<T, RECIP>(v);
+            const T* e = (l + 1 == L(k) - 1) ? nx.xa.as<T>() : nx.xb.as<T>();
+            pa.n[q] = v.P.n; pa.rp[q] = v.P.rp.get(); pa.ci[q] = v.P.ci.get(); pa.v[q] = v.P.val<T>();
+            pa.x[q] = e; pa.y[q] = v.xa.as<T>();
+            js.n[q] = v.A.n; js.rp[q] = v.A.rp.get(); js.ci[q] = v.A.ci.get(); js.v[q] = v.A.val<T>();
+            js.x[q] = v.xa.as<T>(); js.y[q] = v.xb.as<T>(); js.b[q] = rhs(k, l); js.d[q] = l1_of<T, RECIP>(v);
+            ++q;
         }
-        spmv3<T, NV, MV_ADD, RECIP>(pa, lv(0, l).P.lanes_for(NV), T(1), st, s);
-        spmv3<T, NV, MV_JAC, RECIP>(js, lv(0, l).A.lanes_for(NV), T(0), st, s);
+        if (q == 0) continue;
+        spmv3<T, NV, MV_ADD, RECIP, K>(pa, q, lv(k0, l).P.lanes_for(NV), T(1), st, s);
+        spmv3<T, NV, MV_JAC, RECIP, K>(js, q, lv(k0, l).A.lanes_for(NV), T(0), st, s);
     }
-    for (int k = 0; k < 3; ++k) out[k] = (L == 1) ? lv(k, 0).xa.template as<T>() : lv(k, 0).xb.template as<T>();
+    for (int k = 0; k < parts; ++k)
+        out[k] = (L(k) == 1) ? lv(k, 0).xa.template as<T>() : lv(k, 0).xb.template as<T>();
+}
+
+// V-cycles of subspaces 1..3 from their right-hand sides a.rs[1..3]
+template <typename T, int NV, bool RECIP>
+static void vcycle3(AmsState& a, const KState* st, cudaStream_t s, T* out[3]) {
+    std::vector<AmgDevLevel>* H[3] = {&a.amg[1], &a.amg[2], &a.amg[3]};
+    const T* rhs0[3] = {a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>()};
+    vcycleM<T, NV, RECIP, 3>(H, rhs0, 3, st, s, out);
 }
 
 template <typename T, int NV, int LANES>
@@ -1226,6 +1257,149 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
     }
     ensure_x();
     launch_k(k_mv_mask_copy<double, double, NV>, gm, kBlock, s, n, cur, fd, out, st);
+    SSV_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// Several AMS preconditioners applied together (the frequencies of a batched
+// solve): every step of the cycle string is issued for all of them before the
+// next step, the fine-level and transfer passes one launch per preconditioner,
+// the gradient and nodal V-cycles as single lockstep chains over all their
+// hierarchies (vcycleM). Each preconditioner's arithmetic is that of
+// ams_cycle. Requires direct coarsest solves in every hierarchy.
+//
+// Opt-in (SSV_AMS_MULTI=1). It issues 2.5-3.7x fewer launches than parallel
+// graph branches (one per preconditioner) but runs them as one serial chain,
+// and on B200 the branches win at every size measured: 8 frequencies x 4
+// right-hand sides of the eddy-current family, 0.57 / 1.29 / 2.50 / 4.35 /
+// 9.88 ms per COCR iteration at 12^3 / 18^3 / 24^3 / 30^3 / 40^3 as branches
+// against 1.00 / 1.80 / 3.25 / 5.33 / 11.32 ms in lockstep. The branches
+// overlap the frequencies' fine-level passes, which the lockstep chain
+// issues one preconditioner after another.
+// ---------------------------------------------------------------------------
+constexpr int kMultiParts = 32;
+
+// SSV_AMS_MULTI=1: the batched solver applies its preconditioners in lockstep
+// instead of as parallel graph branches
+static bool multi_lockstep_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("SSV_AMS_MULTI");
+        v = (e && e[0] == '1') ? 1 : 0;
+    }
+    return v != 0;
+}
+
+template <typename T, int NV, bool RECIP>
+struct CycleCtx {
+    AmsState* a;
+    const double* d;
+    double *b0, *cur, *alt, *r;
+    const uint8_t* fd;
+    int n;
+    bool fresh = true;
+    void init(AmsState* as) {
+        a = as;
+        n = as->nhc;
+        fd = as->has_fd ? as->fd.get() : nullptr;
+        d = RECIP ? as->fine_il1.get() : as->fine_l1.get();
+        b0 = as->b0.get();
+        cur = as->xa.get();
+        alt = as->xb.get();
+        r = as->r.get();
+        fresh = true;
+    }
+    void smooth(const KState* st, cudaStream_t s) {
+        for (int k = 0; k < a->num_smooth; ++k) {
+            if (fresh) {
+                first_sweep<double, NV, RECIP>(n, b0, d, cur, st, s);
+                fresh = false;
+            } else {
+                mv_spmv<double, double, double, NV, MV_JAC, RECIP>(a->A_bc, cur, alt, b0, d, 0.0, st, s);
+                std::swap(cur, alt);
+            }
+        }
+    }
+    void ensure_x(cudaStream_t s) {
+        if (fresh) {
+            SSV_CUDA(cudaMemsetAsync(cur, 0, sizeof(double) * (size_t)n * NV, s));
+            fresh = false;
+        }
+    }
+    void residual(const KState* st, cudaStream_t s) {
+        ensure_x(s);
+        mv_spmv<double, double, double, NV, MV_RES, RECIP>(a->A_bc, cur, r, b0, nullptr, 0.0, st, s);
+    }
+};
+
+static bool multi_ok(AmsState* const* A, int F) {
+    if (F < 2 || 3 * F > kMultiParts) return false;
+    const AmsState& a0 = *A[0];
+    for (int f = 0; f < F; ++f) {
+        const AmsState& a = *A[f];
+        if (a.fp32 != a0.fp32 || a.complex_form != a0.complex_form || a.cycle_type != a0.cycle_type) return false;
+        for (int k = 0; k < 4; ++k)
+            if (a.tails[k].start >= 0 || a.amg[k].empty() || !a.amg[k].back().direct) return false;
+    }
+    return true;
+}
+
+template <typename T, int NV, bool RECIP>
+static void ams_cycle_multi(AmsState* const* A, int F, const double* const* in, double* const* out, const KState* st,
+                            cudaStream_t s) {
+    std::vector<CycleCtx<T, NV, RECIP>> c(F);
+    for (int f = 0; f < F; ++f) {
+        c[f].init(A[f]);
+        launch_k(k_mv_mask_copy<double, double, NV>, grid_for((int64_t)c[f].n * NV, kBlock), kBlock, s, c[f].n,
+                 in[f], c[f].fd, c[f].b0, st);
+    }
+    auto smooth = [&]() {
+        for (auto& x : c) x.smooth(st, s);
+    };
+    auto gradient = [&]() {
+        std::vector<AmgDevLevel>* H[kMultiParts];
+        const T* rhs0[kMultiParts];
+        T* g[kMultiParts];
+        for (int f = 0; f < F; ++f) {
+            AmsState& a = *c[f].a;
+            c[f].residual(st, s);
+            mv_spmv<double, double, T, NV, MV_AX, RECIP>(a.Gt, c[f].r, a.rs[0].as<T>(), nullptr, nullptr, T(0), st, s);
+            H[f] = &a.amg[0];
+            rhs0[f] = a.rs[0].as<T>();
+        }
+        vcycleM<T, NV, RECIP, kMultiParts>(H, rhs0, F, st, s, g);
+        for (int f = 0; f < F; ++f) {
+            AmsState& a = *c[f].a;
+            mv_spmv<double, T, double, NV, MV_ADD, RECIP>(a.G, g[f], c[f].cur, nullptr, nullptr, a.w, st, s);
+        }
+    };
+    auto nodal = [&]() {
+        std::vector<AmgDevLevel>* H[kMultiParts];
+        const T* rhs0[kMultiParts];
+        T* g[kMultiParts];
+        for (int f = 0; f < F; ++f) {
+            AmsState& a = *c[f].a;
+            c[f].residual(st, s);
+            pi_restrict<T, NV>(a, c[f].r, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), st, s);
+            for (int k = 0; k < 3; ++k) {
+                H[3 * f + k] = &a.amg[k + 1];
+                rhs0[3 * f + k] = a.rs[k + 1].as<T>();
+            }
+        }
+        vcycleM<T, NV, RECIP, kMultiParts>(H, rhs0, 3 * F, st, s, g);
+        for (int f = 0; f < F; ++f)
+            pi_prolong<T, NV>(*c[f].a, g[3 * f], g[3 * f + 1], g[3 * f + 2], c[f].cur, st, s);
+    };
+    if (A[0]->cycle_type == 7) {
+        smooth(); gradient(); smooth(); nodal(); smooth(); gradient(); smooth();
+    } else {
+        smooth(); gradient(); nodal(); gradient(); smooth();
+    }
+    for (int f = 0; f < F; ++f) {
+        c[f].ensure_x(s);
+        launch_k(k_mv_mask_copy<double, double, NV>, grid_for((int64_t)c[f].n * NV, kBlock), kBlock, s, c[f].n,
+                 (const double*)c[f].cur, c[f].fd, out[f], st);
+    }
     SSV_LAUNCH_CHECK();
 }
 
@@ -1739,6 +1913,34 @@ static void ams_block_t(AmsState& a, const double* in, double* out, int nrhs, co
         }
     }
     fail(SSV_ERR_INVALID_ARG, "AMS block apply: nrhs must be 1 or 4");
+}
+
+template <typename T>
+static bool ams_multi_t(AmsState* const* A, int F, const double* const* in, double* const* out, int nrhs,
+                        const KState* st, cudaStream_t s) {
+    if (A[0]->complex_form) {
+        switch (nrhs) {
+            case 1: ams_cycle_multi<T, 2, true>(A, F, in, out, st, s); return true;
+            case 4: ams_cycle_multi<T, 8, true>(A, F, in, out, st, s); return true;
+        }
+    } else {
+        switch (nrhs) {
+            case 1: ams_cycle_multi<T, 1, false>(A, F, in, out, st, s); return true;
+            case 4: ams_cycle_multi<T, 4, false>(A, F, in, out, st, s); return true;
+        }
+    }
+    return false;
+}
+
+bool ams_apply_block_multi(AmsState* const* A, int F, const double* const* in, double* const* out, int nrhs,
+                           const KState* st, cudaStream_t s) {
+    if (!multi_lockstep_enabled() || !multi_ok(A, F)) return false;
+    for (int f = 0; f < F; ++f) {
+        if (nrhs * (A[f]->complex_form ? 2 : 1) > A[f]->nv_alloc) return false;
+        for (int g = 0; g < f; ++g)
+            if (A[g] == A[f]) return false;  // one preconditioner's work vectors serve one column block at a time
+    }
+    return A[0]->fp32 ? ams_multi_t<float>(A, F, in, out, nrhs, st, s) : ams_multi_t<double>(A, F, in, out, nrhs, st, s);
 }
 
 // nrhs right-hand sides, row-interleaved ([row][rhs], complex as Re/Im pairs).
