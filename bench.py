@@ -427,10 +427,13 @@ def run_ams(args, rank, world, local):
     spmv_warm = phase(mixed, "fine_residual")
     achieved = gbps(spmv)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": 102.9e6,
+                "traffic": 105.2e6,
                 "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one launch of this kernel "
-                                "(ncu --set full, same workload), per launch",
-                "kernel": "k_mv_spmv fine residual (A_bc, 7.43M nnz, FP64), L2 flushed before each launch",
+                                "(ncu --set full, same workload, mean of 2 launches), per launch; the sliced-ELL "
+                                "copy's padding (2.9% of the entries) and row map add 3% to the algorithmic bytes",
+                "kernel": "k_sell_spmv fine residual (A_bc in 32-row sliced-ELL, 7.43M nnz, FP64; the shape tuner "
+                          "keeps it where it times faster than the CSR shapes, on every B200 run so far), "
+                          "L2 flushed before each launch",
                 "peak_kind": peak_kind, "algorithmic_bytes_per_launch": spmv["bytes"], "launch_ms": spmv["ms"],
                 "warm_GBps": gbps(spmv_warm),
                 "phases_mixed_cold": [{**p, "GBps": gbps(p)} for p in mixed["phases_cold"]],
@@ -638,8 +641,8 @@ def run_eddy(args, rank, world, local):
     spmv_warm = next(p for p in prof if p["name"] == "fine_residual")
     roofline = {"bound": "hbm", "achieved": gbps(spmv), "peak": peak, "unit": "GB/s", "frac": gbps(spmv) / peak,
                 "traffic": None,
-                "kernel": "k_mv_spmv fine residual (A_bc real, Re/Im columns, 30.3M nnz, FP64), L2 flushed before "
-                          "each launch",
+                "kernel": "k_sell_spmv fine residual (A_bc real in 32-row sliced-ELL, Re/Im columns, 30.3M nnz, "
+                          "FP64; tuner-chosen over the CSR shapes), L2 flushed before each launch",
                 "peak_kind": peak_kind, "algorithmic_bytes_per_launch": spmv["bytes"], "launch_ms": spmv["ms"],
                 "warm_GBps": gbps(spmv_warm),
                 "phases_cold": [{**p, "GBps": gbps(p)} for p in prof_cold],

@@ -165,6 +165,85 @@ k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T
     }
 }
 
+// Sliced-ELL form of the same product (FP64 values): one warp per slice of 32
+// rows, slice entries stored column-major, so step k of the slice's 32 rows
+// is one coalesced load of 32 values and one of 32 column indices, with no
+// row-pointer load in front of them. Padding entries carry column -1 and are
+// skipped. The steps go in rounds of R: the values and columns of round j+1
+// are loaded before the gathers of round j are issued, so each warp keeps two
+// rounds of requests in flight. Each row is summed in its CSR column order.
+template <typename TX, typename TY, int NV, int MODE, bool RECIP, int R>
+__global__ void __launch_bounds__(kBlock)
+k_sell_spmv(int slices, const int* __restrict__ off, const int* __restrict__ rows, const int* __restrict__ ci,
+            const double* __restrict__ v, const TX* __restrict__ x, TY* __restrict__ y, const TY* __restrict__ b,
+            const TY* __restrict__ d, TY w, const KState* st) {
+    using TA = wider_t<double, TX>;
+    pdl_gate();
+    if (st && st->done) return;
+    const int lane = threadIdx.x & 31;
+    const int wpb = kBlock / 32;
+    for (int sl = blockIdx.x * wpb + threadIdx.x / 32; sl < slices; sl += gridDim.x * wpb) {
+        const int e1 = off[sl + 1];
+        int e = off[sl] + lane;
+        const int row = rows[(size_t)sl * 32 + lane];
+        TA acc[NV];
+#pragma unroll
+        for (int c = 0; c < NV; ++c) acc[c] = TA(0);
+        double a[R];
+        int col[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            const int k = e + 32 * u;
+            a[u] = k < e1 ? v[k] : 0.0;
+            col[u] = k < e1 ? ci[k] : -1;
+        }
+        while (e < e1) {
+            const int en = e + 32 * R;
+            double an[R];
+            int cn[R];
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                const int k = en + 32 * u;
+                an[u] = k < e1 ? v[k] : 0.0;
+                cn[u] = k < e1 ? ci[k] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                if (col[u] >= 0) {
+                    TX xv[NV];
+                    load_row<NV>(x + (size_t)col[u] * NV, xv);
+#pragma unroll
+                    for (int c = 0; c < NV; ++c) acc[c] += (TA)a[u] * (TA)xv[c];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                a[u] = an[u];
+                col[u] = cn[u];
+            }
+            e = en;
+        }
+        if (row >= 0) {
+            const size_t base = (size_t)row * NV;
+#pragma unroll
+            for (int c = 0; c < NV; ++c) {
+                const TY ac = (TY)acc[c];
+                if constexpr (MODE == MV_AX) {
+                    y[base + c] = ac;
+                } else if constexpr (MODE == MV_RES) {
+                    y[base + c] = b[base + c] - ac;
+                } else if constexpr (MODE == MV_ADD) {
+                    y[base + c] += w * ac;
+                } else {
+                    const TY r = b[base + c] - ac;
+                    const TY xo = (TY)x[base + c];
+                    y[base + c] = RECIP ? xo + r * d[row] : xo + r / d[row];
+                }
+            }
+        }
+    }
+}
+
 // rx/ry/rz = Pi_{x,y,z}^T r over the shared pattern of G^T (one pass over r);
 // FP64 values and accumulation, outputs in the hierarchy type TO
 template <typename TO, int NV, int LANES>
@@ -827,6 +906,65 @@ struct DualVec {
 template <> inline const double* DualVec::get<double>() const { return d.get(); }
 template <> inline const float* DualVec::get<float>() const { return f.get(); }
 
+// Sliced-ELL copy of a CSR matrix for k_sell_spmv: rows sorted by length
+// (longest first, ties in row order) inside windows of kSellWindow rows, cut
+// into slices of 32 rows, each slice padded to its longest row. Entry k of
+// slice row t sits at off[slice] + 32 k + t. (Storing the slices widest
+// first, so that the last partial wave of a launch holds the shortest ones,
+// measured no faster at 40^3 and 8% slower at 64^3: neighbouring slices then
+// no longer run side by side and share fewer x rows in L1.)
+constexpr int kSellWindow = 256;
+
+struct DevSell {
+    int slices = 0;
+    int64_t entries = 0;
+    DevBuf<int> off, rows, ci;
+    DevBuf<double> v;
+    void build(const HostCsr& A, cudaStream_t s) {
+        const int n = A.n;
+        slices = (n + 31) / 32;
+        std::vector<int> order(n);
+        for (int i = 0; i < n; ++i) order[i] = i;
+        auto len = [&](int r) { return A.rp[r + 1] - A.rp[r]; };
+        for (int w0 = 0; w0 < n; w0 += kSellWindow) {
+            const int w1 = std::min(n, w0 + kSellWindow);
+            std::stable_sort(order.begin() + w0, order.begin() + w1, [&](int p, int q) { return len(p) > len(q); });
+        }
+        std::vector<int> h_off(slices + 1, 0), h_rows((size_t)slices * 32, -1);
+        for (int sl = 0; sl < slices; ++sl) {
+            int wmax = 0;
+            for (int t = 0; t < 32 && sl * 32 + t < n; ++t) {
+                const int r = order[sl * 32 + t];
+                h_rows[(size_t)sl * 32 + t] = r;
+                wmax = std::max(wmax, len(r));
+            }
+            if ((int64_t)h_off[sl] + 32 * (int64_t)wmax > (int64_t)INT32_MAX - 4096) {  // int offsets: no copy
+                slices = 0;
+                entries = 0;
+                return;
+            }
+            h_off[sl + 1] = h_off[sl] + 32 * wmax;
+        }
+        entries = h_off[slices];
+        std::vector<int> h_ci((size_t)entries, -1);
+        std::vector<double> h_v((size_t)entries, 0.0);
+        for (int sl = 0; sl < slices; ++sl)
+            for (int t = 0; t < 32; ++t) {
+                const int r = h_rows[(size_t)sl * 32 + t];
+                if (r < 0) continue;
+                for (int k = 0; k < len(r); ++k) {
+                    const size_t e = (size_t)h_off[sl] + 32 * (size_t)k + t;
+                    h_ci[e] = A.ci[A.rp[r] + k];
+                    h_v[e] = A.v[A.rp[r] + k];
+                }
+            }
+        off.upload(h_off.data(), h_off.size(), s);
+        rows.upload(h_rows.data(), h_rows.size(), s);
+        ci.upload(h_ci.data(), h_ci.size(), s);
+        v.upload(h_v.data(), h_v.size(), s);
+    }
+};
+
 struct DevCsr {
     int n = 0, m = 0;
     int64_t nnz = 0;
@@ -839,8 +977,11 @@ struct DevCsr {
         return tuned[i] ? tuned[i] : lanes;
     }
     int unroll_for(int nv) const { return tuned[nv_slot(nv)] ? tuned_u[nv_slot(nv)] : 1; }
+    bool sell_for(int nv) const { return sell.slices > 0 && tuned_sell[nv_slot(nv)] > 0; }
+    int tuned_sell[4] = {0, 0, 0, 0};  // steps per round of the sliced-ELL copy when it timed fastest (0 = CSR)
     DevBuf<int> rp, ci;
     DualVec v;
+    DevSell sell;  // built for the fine matrix only (FP64 values)
     void upload(const HostCsr& A, bool fp32, cudaStream_t s) {
         n = A.n;
         m = A.m;
@@ -933,9 +1074,26 @@ static int mv_grid(int n, int lanes, int u) {
     return std::max(1, std::min((n + rpb - 1) / rpb, sm_count() * 8));
 }
 
+template <typename TX, typename TY, int NV, int MODE, bool RECIP>
+static void launch_sell(const DevSell& S, int steps, cudaStream_t s, const TX* x, TY* y, const TY* b, const TY* d,
+                        TY w, const KState* st) {
+    const int grid = std::max(1, (S.slices + kBlock / 32 - 1) / (kBlock / 32));
+#define SSV_SELL_ARGS grid, kBlock, s, S.slices, S.off.get(), S.rows.get(), S.ci.get(), S.v.get(), x, y, b, d, w, st
+    if (steps == 2) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 2>, SSV_SELL_ARGS);
+    else if (steps == 4) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 4>, SSV_SELL_ARGS);
+    else launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 8>, SSV_SELL_ARGS);
+#undef SSV_SELL_ARGS
+}
+
 template <typename TV, typename TX, typename TY, int NV, int MODE, bool RECIP>
 static void mv_spmv(const DevCsr& A, const TX* x, TY* y, const TY* b, const TY* d, TY w, const KState* st,
                     cudaStream_t s) {
+    if constexpr (std::is_same_v<TV, double>) {
+        if (A.sell_for(NV)) {
+            launch_sell<TX, TY, NV, MODE, RECIP>(A.sell, A.tuned_sell[DevCsr::nv_slot(NV)], s, x, y, b, d, w, st);
+            return;
+        }
+    }
     const int lanes = A.lanes_for(NV);
     const int u = A.unroll_for(NV);
     launch_mv<TV, TX, TY, NV, MODE, RECIP>(lanes, u, mv_grid(A.n, lanes, u), s, A.n, A.rp.get(), A.ci.get(),
@@ -1477,6 +1635,19 @@ static double cold_tune_bytes() {
     return v;
 }
 
+// The fine matrix's sliced-ELL copy (SSV_AMS_SELL): 1 (default) = a tuner
+// candidate beside the CSR shapes on matrices of at least kUnrollMinRows rows,
+// 0 = off, 2 = always used, on any size
+static int sell_mode() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("SSV_AMS_SELL");
+        v = (e && (e[0] == '0' || e[0] == '2')) ? e[0] - '0' : 1;
+    }
+    return v;
+}
+static bool sell_enabled() { return sell_mode() != 0; }
+
 // largest rows-per-group the tuner may pick (SSV_AMS_MAX_UNROLL, default 4)
 static int max_unroll() {
     static int v = 0;
@@ -1522,10 +1693,38 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
     }
     A.tuned[DevCsr::nv_slot(NV)] = pick;
     A.tuned_u[DevCsr::nv_slot(NV)] = pick_u;
+    const int slot = DevCsr::nv_slot(NV);
+    A.tuned_sell[slot] = 0;
+    float sell_best = 1e30f;
+    int sell_pick = 0;
+    if constexpr (std::is_same_v<TV, double>) {
+        if (A.sell.slices > 0 && sell_enabled()) {
+            for (int R : {2, 4, 8}) {
+                auto launch = [&] {
+                    if (b)
+                        launch_sell<TX, TY, NV, MV_RES, false>(A.sell, R, s, x, y, b, nullptr, TY(0), nullptr);
+                    else
+                        launch_sell<TX, TY, NV, MV_AX, false>(A.sell, R, s, x, y, nullptr, nullptr, TY(0), nullptr);
+                };
+                launch();
+                const float ms = time_launches(launch, cold ? 5 : 4, cold, s, e0, e1, true);
+                if (ms < sell_best) {
+                    sell_best = ms;
+                    sell_pick = R;
+                }
+            }
+            if (sell_best < best || sell_mode() == 2) A.tuned_sell[slot] = sell_pick;
+        }
+    }
     static const bool log = std::getenv("SSV_AMS_TUNE_LOG") != nullptr;
-    if (log)
-        std::fprintf(stderr, "ams tune: n=%d nnz=%lld nv=%d %s -> lanes %d rows/group %d (%.2f us)\n", A.n,
+    if (log) {
+        std::fprintf(stderr, "ams tune: n=%d nnz=%lld nv=%d %s -> lanes %d rows/group %d (%.2f us)", A.n,
                      (long long)A.nnz, NV, cold ? "cold" : "warm", pick, pick_u, 1e3 * best / (cold ? 5 : 4));
+        if (sell_pick)
+            std::fprintf(stderr, "; sliced-ELL %d steps/round %.2f us%s", sell_pick, 1e3 * sell_best / (cold ? 5 : 4),
+                         A.tuned_sell[slot] ? " -> sliced-ELL" : "");
+        std::fprintf(stderr, "\n");
+    }
 }
 
 // lanes of the Pi transfers (one pass over G's pattern, three coefficient
@@ -1765,6 +1964,7 @@ static std::vector<double> inverted(const std::vector<double>& v) {
 static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
     const int nv = std::max(a.nv_alloc, a.complex_form ? 2 : 1);
     a.A_bc.upload(a.host.A_bc, false, s);
+    if (sell_mode() == 2 || (sell_mode() == 1 && a.A_bc.n >= kUnrollMinRows)) a.A_bc.sell.build(a.host.A_bc, s);
     a.fine_l1.upload(a.host.fine_l1.data(), a.host.fine_l1.size(), s);
     const std::vector<double> il1 = reciprocal(a.host.fine_l1);
     a.fine_il1.upload(il1.data(), il1.size(), s);
