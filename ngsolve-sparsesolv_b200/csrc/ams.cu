@@ -981,7 +981,7 @@ struct DevCsr {
     int tuned_sell[4] = {0, 0, 0, 0};  // steps per round of the sliced-ELL copy when it timed fastest (0 = CSR)
     DevBuf<int> rp, ci;
     DualVec v;
-    DevSell sell;  // built for the fine matrix only (FP64 values)
+    DevSell sell;  // built for the fine-level FP64 matrices only (A_bc, G, G^T)
     void upload(const HostCsr& A, bool fp32, cudaStream_t s) {
         n = A.n;
         m = A.m;
@@ -1635,9 +1635,9 @@ static double cold_tune_bytes() {
     return v;
 }
 
-// The fine matrix's sliced-ELL copy (SSV_AMS_SELL): 1 (default) = a tuner
-// candidate beside the CSR shapes on matrices of at least kUnrollMinRows rows,
-// 0 = off, 2 = always used, on any size
+// The fine-level matrices' sliced-ELL copies (A_bc, G, G^T; SSV_AMS_SELL):
+// 1 (default) = a tuner candidate beside the CSR shapes on matrices of at
+// least kUnrollMinRows rows, 0 = off, 2 = always used, on any size
 static int sell_mode() {
     static int v = -1;
     if (v < 0) {
@@ -1908,11 +1908,18 @@ static std::vector<double> reciprocal(const std::vector<double>& v) {
     return r;
 }
 
+// Uploads a fine-level FP64 matrix (A_bc, G, G^T) and, where the shape tuner
+// may use it, its sliced-ELL copy.
+static void upload_fine(DevCsr& M, const HostCsr& H, cudaStream_t s) {
+    M.upload(H, false, s);
+    if (sell_mode() == 2 || (sell_mode() == 1 && M.n >= kUnrollMinRows)) M.sell.build(H, s);
+}
+
 // Geometry part (G, G^T, Pi): FP64 in both forms. (The FP32 form replaces
 // the values by scaled ones in ams_upload_matrix.)
 static void ams_upload_geometry(AmsState& a, cudaStream_t s) {
-    a.G.upload(a.host.G, false, s);
-    a.Gt.upload(a.host.Gt, false, s);
+    upload_fine(a.G, a.host.G, s);
+    upload_fine(a.Gt, a.host.Gt, s);
     for (int d = 0; d < 3; ++d) {
         a.Piv[d].upload(a.host.Pi[d].v.data(), a.host.Pi[d].v.size(), s);
         a.Pitv[d].upload(a.host.Pit[d].v.data(), a.host.Pit[d].v.size(), s);
@@ -1963,8 +1970,7 @@ static std::vector<double> inverted(const std::vector<double>& v) {
 // transfer values.
 static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
     const int nv = std::max(a.nv_alloc, a.complex_form ? 2 : 1);
-    a.A_bc.upload(a.host.A_bc, false, s);
-    if (sell_mode() == 2 || (sell_mode() == 1 && a.A_bc.n >= kUnrollMinRows)) a.A_bc.sell.build(a.host.A_bc, s);
+    upload_fine(a.A_bc, a.host.A_bc, s);
     a.fine_l1.upload(a.host.fine_l1.data(), a.host.fine_l1.size(), s);
     const std::vector<double> il1 = reciprocal(a.host.fine_l1);
     a.fine_il1.upload(il1.data(), il1.size(), s);
@@ -2021,8 +2027,8 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
         }
         // level-0 scaling folded into this subspace's transfers
         if (sub == 0) {
-            a.G.upload(a.fp32 ? scaled_csr(a.host.G, nullptr, &isc[0]) : a.host.G, false, s);
-            a.Gt.upload(a.fp32 ? scaled_csr(a.host.Gt, &isc[0], nullptr) : a.host.Gt, false, s);
+            upload_fine(a.G, a.fp32 ? scaled_csr(a.host.G, nullptr, &isc[0]) : a.host.G, s);
+            upload_fine(a.Gt, a.fp32 ? scaled_csr(a.host.Gt, &isc[0], nullptr) : a.host.Gt, s);
         } else {
             const int d = sub - 1;
             const HostCsr pi = a.fp32 ? scaled_csr(a.host.Pi[d], nullptr, &isc[0]) : a.host.Pi[d];

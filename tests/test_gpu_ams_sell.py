@@ -1,8 +1,9 @@
-"""The fine matrix's sliced-ELL copy (32-row slices, rows sorted by length
-inside 256-row windows, column-major entries) gives the same AMS applies and
-solves as the CSR shapes. By default the tuner only offers it on fine
-matrices of at least 65,536 rows; SSV_AMS_SELL=2 forces it on any size, so
-these small systems run it. The switch is read once per process: the cases
+"""The fine-level matrices' sliced-ELL copies (A_bc, G, G^T: 32-row slices,
+rows sorted by length inside 256-row windows, column-major entries) give the
+same AMS applies and solves as the CSR shapes, in the FP64 and the FP32 form
+(where G and G^T carry mixed input/output types). By default the tuner only
+offers them on matrices of at least 65,536 rows; SSV_AMS_SELL=2 forces them
+on any size, so these small systems run them. The switch is read once per process: the cases
 run in a child process, whose tuner log shows the sliced-ELL kernel chosen
 for the fine matrix."""
 from __future__ import annotations
@@ -41,6 +42,19 @@ for name, d in [("mag_well", H.magnetostatic(8, nu_iron=1.0, mass_eps=1.0)), ("m
     xo, ro, _ = o.pcg(d["f"], config=O.default_config(tolerance=1e-10, max_iterations=500))
     out[name + "_its"] = [int(r.iterations), int(ro.iterations)]
     out[name + "_x"] = float(np.abs(x - xo).max() / np.abs(xo).max())
+d = H.magnetostatic(8, nu_iron=1.0, mass_eps=1.0)
+p = ss.CompactAMSPreconditioner(d["A"], d["G"], freedofs=d["freedofs"], coord_x=d["coords"][0],
+                                coord_y=d["coords"][1], coord_z=d["coords"][2], precision="fp32")
+o = O.AmsOracle(d["A"], d["G"], d["freedofs"], *d["coords"])
+b = rng.standard_normal(d["A"].shape[0])
+yo = o.apply(b)
+out["fp32_apply"] = float(np.linalg.norm(p * b - yo) / np.linalg.norm(yo))
+inv = ss.PCGSolver(d["A"], p, freedofs=d["freedofs"], maxiter=500, tol=1e-10)
+x = np.zeros(d["A"].shape[0])
+r = inv.Solve(d["f"], x)
+fd = d["freedofs"].astype(bool)
+out["fp32_cg"] = [bool(r.converged), int(r.iterations), int(out["mag_well_its"][1]),
+                  float(np.linalg.norm((d["f"] - d["A"] @ np.where(fd, x, 0))[fd]) / np.linalg.norm(d["f"]))]
 d = H.eddy_current(8, nu_r_core=1.0, mass_eps=1.0, sigma=1e5, freq=1e3)
 p = ss.ComplexCompactAMSPreconditioner(d["a_real"], d["G"], freedofs=d["freedofs"], coord_x=d["coords"][0],
                                        coord_y=d["coords"][1], coord_z=d["coords"][2])
@@ -73,6 +87,14 @@ def test_sell_applies_match_oracle(sell_run):
     assert out["mag_well_apply"] <= 1e-11, out
     assert out["eddy_well_apply"] <= 1e-11, out
     assert out["mag_si_apply"] <= 1e-7, out  # cond ~ 1e10: the bar of the CSR applies on these systems
+
+
+def test_sell_fp32_form(sell_run):
+    out, _ = sell_run
+    assert out["fp32_apply"] <= 1e-4, out  # FP32 storage and arithmetic through ~20 passes (stated)
+    conv, its, its64, res = out["fp32_cg"]
+    assert conv and res <= 1e-10 * 1.01, out
+    assert its <= 1.5 * its64 + 2, out
 
 
 def test_sell_cg_matches_oracle(sell_run):
