@@ -883,6 +883,283 @@ k_vcycle_tail(const TailLevel* __restrict__ lv, int l0, int L, const T* __restri
 }
 
 // ---------------------------------------------------------------------------
+// Whole V-cycles as one cooperative launch (SSV_AMS_GRID=1): up to K
+// hierarchies (the three nodal ones in lockstep, or the gradient one), from
+// the finest level down to the coarsest LDL^T solves and back up, every CTA on
+// every step and a grid-wide barrier wherever the launch chain has a kernel
+// boundary. The launch is cooperative, so all CTAs are resident together.
+// Each barrier wait is bounded: a wait that gives up fails the solve
+// (SSV_ERR_TIMEOUT, done) and the CTAs then run through the remaining steps
+// without waiting. Vectors written inside the launch are read through L2
+// (ld.global.cg), never through a possibly stale L1 line of another SM. The
+// arithmetic per row is the chain's (num_smooth = 1, direct coarsest solves).
+//
+// Opt-in: measured slower than the per-level launch chain on B200. On the 40^3
+// magnetostatic hierarchies (FP32) one launch takes 148 us for the gradient
+// V-cycle (18 barrier steps) and 391 us for the three nodal ones (34 steps),
+// against 64 and 172 us for the chains, whose launches overlap through
+// programmatic dependent launch at ~3.6-5 us a step. Here each step costs
+// ~8-11 us: the fixed 4 lanes per row are slow on the long rows of the coarse
+// Galerkin levels (the chain's tuner picks up to 32 lanes there), gathers go
+// through L2 only, and the barrier itself costs microseconds.
+// ---------------------------------------------------------------------------
+constexpr int kGridBlock = 1024;
+constexpr int kGridPerSm = 1;   // CTAs per SM, guaranteed by the launch bounds (no shared memory)
+constexpr int kBarGroups = 8;   // first-level arrival counters of the grid barrier
+
+// Barrier state, every counter on its own 128-byte line: CTAs arrive on the
+// counter of their group (blockIdx % kBarGroups), the last of a group on the
+// root, the last at the root advances the generation.
+struct GridBar {
+    unsigned group[kBarGroups][32];
+    unsigned root, r1[31];
+    unsigned gen, r2[31];
+    unsigned exit, r3[31];
+    int err, r4[31];
+};
+
+template <int K>
+struct GridCycle {
+    const TailLevel* lv[K];  // each hierarchy's level descriptors, finest first (device)
+    const void* b0[K];       // level-0 right-hand sides (hierarchy type)
+    int L[K];                // level counts (may differ)
+    int parts;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
+    unsigned o;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(o) : "l"(p), "r"(v) : "memory");
+    return o;
+}
+__device__ __forceinline__ void red_add_release(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_u32(unsigned* p, unsigned v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_relaxed_s32(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// CTA leaders arrive on their group's counter, the last of each group on the
+// root, the last at the root advances the generation; everyone else waits for
+// the generation to move (bounded). The arrivals are acquire-release
+// read-modify-writes and the generation step a release, so every write made
+// before the barrier by any CTA (ordered before its leader's arrival by the
+// CTA barrier) is visible to every CTA after it. Each last arrival resets the
+// counter it completed before passing on.
+__device__ __forceinline__ void grid_barrier(GridBar* gb, KState* st) {
+    __syncthreads();
+    if (threadIdx.x == 0 && ld_relaxed_s32(&gb->err) == 0) {
+        const unsigned g = ld_acquire_u32(&gb->gen);
+        const unsigned ng = min((unsigned)kBarGroups, gridDim.x);
+        const unsigned grp = blockIdx.x % ng;
+        const unsigned members = (gridDim.x - grp + ng - 1) / ng;
+        bool last = false;
+        if (atom_add_acq_rel(&gb->group[grp][0], 1u) == members - 1) {
+            st_relaxed_u32(&gb->group[grp][0], 0u);
+            if (atom_add_acq_rel(&gb->root, 1u) == ng - 1) {
+                st_relaxed_u32(&gb->root, 0u);
+                red_add_release(&gb->gen, 1u);
+                last = true;
+            }
+        }
+        if (!last) {
+            int spins = 0;
+            while (ld_acquire_u32(&gb->gen) == g) {
+                if (++spins > (1 << 24)) {  // never expected: fail the solve, finish the launch
+                    atomicExch(&gb->err, 1);
+                    if (st) {
+                        st->status = SSV_ERR_TIMEOUT;
+                        st->done = 1;
+                    }
+                    break;
+                }
+                if (spins > 256) __nanosleep(32);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// the last CTA out resets the barrier state for the next launch
+__device__ __forceinline__ void grid_exit(GridBar* gb) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&gb->exit, 1u) == gridDim.x - 1) {
+            for (int i = 0; i < kBarGroups; ++i) atomicExch(&gb->group[i][0], 0u);
+            atomicExch(&gb->root, 0u);
+            atomicExch(&gb->gen, 0u);
+            atomicExch(&gb->err, 0);
+            __threadfence();
+            atomicExch(&gb->exit, 0u);
+        }
+    }
+}
+
+template <typename T, int NV>
+__device__ __forceinline__ void ldcg_row(const T* p, T (&o)[NV]) {
+#pragma unroll
+    for (int c = 0; c < NV; ++c) o[c] = __ldcg(p + c);
+}
+
+template <typename T, int NV, bool RECIP, int K>
+__global__ void __launch_bounds__(kGridBlock, kGridPerSm)
+k_vcycle_grid(GridCycle<K> g, GridBar* gb, KState* st) {
+    const bool skip = st && st->done;  // every CTA still takes part in the exit count
+    if (!skip) {
+        int Lmax = 0;
+        for (int q = 0; q < g.parts; ++q) Lmax = max(Lmax, g.L[q]);
+        auto sync = [&]() { grid_barrier(gb, st); };
+        auto dv = [&](const TailLevel& Lv) { return (const T*)(RECIP ? Lv.il1 : Lv.l1); };
+        auto rhs = [&](int q, int l) { return l == 0 ? (const T*)g.b0[q] : (const T*)g.lv[q][l].b; };
+        auto upd = [&](T xo, T r, T d) { return RECIP ? xo + r * d : xo + r / d; };
+        const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+        const int lane = threadIdx.x & 31;
+        const int gw = gt >> 5, GW = (gridDim.x * blockDim.x) >> 5;
+        // down: fused first sweep + residual, then restriction
+        for (int l = 0; l < Lmax - 1; ++l) {
+            for (int q = 0; q < g.parts; ++q) {
+                if (l >= g.L[q] - 1) continue;
+                const TailLevel& Lv = g.lv[q][l];
+                const T* b = rhs(q, l);
+                const T* d = dv(Lv);
+                T* x = (T*)Lv.x;
+                T* r = (T*)Lv.r;
+                tail_rows<T, NV>(Lv.n, Lv.Arp, Lv.Aci, (const T*)Lv.Av,
+                                 [&](int j, T (&o)[NV]) {
+                                     const T dj = d[j];
+                                     ldcg_row<T, NV>(b + (size_t)j * NV, o);
+#pragma unroll
+                                     for (int c = 0; c < NV; ++c) o[c] = RECIP ? o[c] * dj : o[c] / dj;
+                                 },
+                                 [&](int row, T (&acc)[NV]) {
+                                     const T di = d[row];
+#pragma unroll
+                                     for (int c = 0; c < NV; ++c) {
+                                         const T bi = __ldcg(b + (size_t)row * NV + c);
+                                         x[(size_t)row * NV + c] = RECIP ? bi * di : bi / di;
+                                         r[(size_t)row * NV + c] = bi - acc[c];
+                                     }
+                                 });
+            }
+            sync();
+            for (int q = 0; q < g.parts; ++q) {
+                if (l >= g.L[q] - 1) continue;
+                const TailLevel& Lv = g.lv[q][l];
+                const T* r = (const T*)Lv.r;
+                T* bn = (T*)g.lv[q][l + 1].b;
+                tail_rows<T, NV>(g.lv[q][l + 1].n, Lv.Trp, Lv.Tci, (const T*)Lv.Tv,
+                                 [&](int j, T (&o)[NV]) { ldcg_row<T, NV>(r + (size_t)j * NV, o); },
+                                 [&](int row, T (&acc)[NV]) {
+#pragma unroll
+                                     for (int c = 0; c < NV; ++c) bn[(size_t)row * NV + c] = acc[c];
+                                 });
+            }
+            sync();
+        }
+        // coarsest levels: z = (L^{-1} b) / d, then x = L^{-T} z (FP64), warp per row
+        for (int q = 0; q < g.parts; ++q) {
+            const TailLevel& C = g.lv[q][g.L[q] - 1];
+            const T* bc = rhs(q, g.L[q] - 1);
+            const int n = C.n;
+            for (int row = gw; row < n; row += GW) {
+                double acc[NV];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) acc[c] = 0.0;
+                const double* lr = C.Li + (size_t)row * n;
+                for (int k = lane; k <= row; k += 32) {
+                    const double a = lr[k];
+#pragma unroll
+                    for (int c = 0; c < NV; ++c) acc[c] += a * (double)__ldcg(bc + (size_t)k * NV + c);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                    for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
+                if (lane == 0) {
+                    const double dd = C.piv[row];
+#pragma unroll
+                    for (int c = 0; c < NV; ++c) C.cz[(size_t)row * NV + c] = dd != 0.0 ? acc[c] / dd : 0.0;
+                }
+            }
+        }
+        sync();
+        for (int q = 0; q < g.parts; ++q) {
+            const TailLevel& C = g.lv[q][g.L[q] - 1];
+            const int n = C.n;
+            T* x = (T*)C.x;
+            for (int row = gw; row < n; row += GW) {
+                double acc[NV];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) acc[c] = 0.0;
+                const double* lr = C.LiT + (size_t)row * n;
+                for (int k = row + lane; k < n; k += 32) {
+                    const double a = lr[k];
+#pragma unroll
+                    for (int c = 0; c < NV; ++c) acc[c] += a * __ldcg(C.cz + (size_t)k * NV + c);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                    for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
+                if (lane == 0)
+#pragma unroll
+                    for (int c = 0; c < NV; ++c) x[(size_t)row * NV + c] = (T)acc[c];
+            }
+        }
+        sync();
+        // up: prolongation, then the post sweep into the level's second buffer
+        for (int l = Lmax - 2; l >= 0; --l) {
+            for (int q = 0; q < g.parts; ++q) {
+                if (l > g.L[q] - 2) continue;
+                const TailLevel& Lv = g.lv[q][l];
+                const TailLevel& Nx = g.lv[q][l + 1];
+                const T* e = (const T*)((l + 1 == g.L[q] - 1) ? Nx.x : Nx.xalt);
+                T* x = (T*)Lv.x;
+                tail_rows<T, NV>(Lv.n, Lv.Prp, Lv.Pci, (const T*)Lv.Pv,
+                                 [&](int j, T (&o)[NV]) { ldcg_row<T, NV>(e + (size_t)j * NV, o); },
+                                 [&](int row, T (&acc)[NV]) {
+#pragma unroll
+                                     for (int c = 0; c < NV; ++c) {
+                                         const size_t i = (size_t)row * NV + c;
+                                         x[i] = __ldcg(x + i) + T(1) * acc[c];
+                                     }
+                                 });
+            }
+            sync();
+            for (int q = 0; q < g.parts; ++q) {
+                if (l > g.L[q] - 2) continue;
+                const TailLevel& Lv = g.lv[q][l];
+                const T* b = rhs(q, l);
+                const T* d = dv(Lv);
+                const T* x = (const T*)Lv.x;
+                T* xa = (T*)Lv.xalt;
+                tail_rows<T, NV>(Lv.n, Lv.Arp, Lv.Aci, (const T*)Lv.Av,
+                                 [&](int j, T (&o)[NV]) { ldcg_row<T, NV>(x + (size_t)j * NV, o); },
+                                 [&](int row, T (&acc)[NV]) {
+#pragma unroll
+                                     for (int c = 0; c < NV; ++c) {
+                                         const size_t i = (size_t)row * NV + c;
+                                         xa[i] = upd(__ldcg(x + i), __ldcg(b + i) - acc[c], d[row]);
+                                     }
+                                 });
+            }
+            sync();
+        }
+    }
+    grid_exit(gb);
+}
+
+// ---------------------------------------------------------------------------
 // Device hierarchy
 // ---------------------------------------------------------------------------
 static std::vector<float> to_float(const std::vector<double>& h) { return std::vector<float>(h.begin(), h.end()); }
@@ -1036,6 +1313,9 @@ struct AmsState {
     ForkSet forks;  // the y and z nodal V-cycles run beside the x one
     TailSet tails[4];
     bool tri = true;  // nodal V-cycles in lockstep launches (SSV_AMS_TRI=0: three branches)
+    bool grid = false;              // whole V-cycles as cooperative launches (SSV_AMS_GRID=1)
+    DevBuf<TailLevel> gdesc[4];     // every level of each hierarchy, for k_vcycle_grid
+    DevBuf<GridBar> gbar;           // its barrier state (zero between launches)
     int pi_lanes[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};  // Pi restrict / prolong lanes by NV slot (0 = untuned)
 };
 
@@ -1294,6 +1574,42 @@ static void vcycle3(AmsState& a, const KState* st, cudaStream_t s, T* out[3]) {
     vcycleM<T, NV, RECIP, 3>(H, rhs0, 3, st, s, out);
 }
 
+// The batched solver applies several preconditioners on concurrent graph
+// branches; whole-V-cycle launches need the whole GPU, so they are used only
+// outside such branches.
+static bool g_grid_suspended = false;
+void ams_grid_suspend(bool on) { g_grid_suspended = on; }
+
+static bool grid_ok(const AmsState& a, const KState* st) { return a.grid && st && !g_grid_suspended; }
+
+// One cooperative launch of k_vcycle_grid over hierarchies subs[0..parts) with
+// right-hand sides rhs0; out[k] = each hierarchy's level-0 result.
+template <typename T, int NV, bool RECIP, int K>
+static void vcycle_grid(AmsState& a, const int* subs, const T* const* rhs0, int parts, const KState* st,
+                        cudaStream_t s, T** out) {
+    const int grid = sm_count() * kGridPerSm;  // co-resident: the launch bounds fit kGridPerSm CTAs per SM
+    GridCycle<K> g{};
+    g.parts = parts;
+    for (int k = 0; k < parts; ++k) {
+        const auto& L = a.amg[subs[k]];
+        g.lv[k] = a.gdesc[subs[k]].get();
+        g.b0[k] = rhs0[k];
+        g.L[k] = (int)L.size();
+        out[k] = (L.size() == 1) ? L[0].xa.template as<T>() : L[0].xb.template as<T>();
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kGridBlock);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    SSV_CUDA(cudaLaunchKernelEx(&cfg, k_vcycle_grid<T, NV, RECIP, K>, g, a.gbar.get(), const_cast<KState*>(st)));
+}
+
 template <typename T, int NV, int LANES>
 static void pi_restrict_l(const AmsState& a, const double* r, T* ox, T* oy, T* oz, const KState* st,
                           cudaStream_t s) {
@@ -1390,14 +1706,25 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
     auto gradient = [&]() {
         residual();
         mv_spmv<double, double, T, NV, MV_AX, RECIP>(a.Gt, r, a.rs[0].as<T>(), nullptr, nullptr, T(0), st, s);
-        T* g = vcycle<T, NV, RECIP>(a.amg[0], a.tails[0], 0, a.rs[0].as<T>(), 1, st, s);
+        T* g;
+        if (grid_ok(a, st)) {
+            const int subs[1] = {0};
+            const T* rhs0[1] = {a.rs[0].as<T>()};
+            vcycle_grid<T, NV, RECIP, 1>(a, subs, rhs0, 1, st, s, &g);
+        } else {
+            g = vcycle<T, NV, RECIP>(a.amg[0], a.tails[0], 0, a.rs[0].as<T>(), 1, st, s);
+        }
         mv_spmv<double, T, double, NV, MV_ADD, RECIP>(a.G, g, cur, nullptr, nullptr, a.w, st, s);
     };
     auto nodal = [&]() {
         residual();
         pi_restrict<T, NV>(a, r, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), st, s);
         T* g3[3];
-        if (tri_ok(a)) {  // one chain of launches carrying all three hierarchies
+        if (grid_ok(a, st)) {  // one cooperative launch for all three V-cycles
+            const int subs[3] = {1, 2, 3};
+            const T* rhs0[3] = {a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>()};
+            vcycle_grid<T, NV, RECIP, 3>(a, subs, rhs0, 3, st, s, g3);
+        } else if (tri_ok(a)) {  // one chain of launches carrying all three hierarchies
             vcycle3<T, NV, RECIP>(a, st, s, g3);
         } else {  // the three V-cycles are independent (own hierarchies and vectors)
             a.forks.fork(s, 2);
@@ -1873,6 +2200,61 @@ static void build_tails(AmsState& a) {
     SSV_CUDA(cudaStreamSynchronize(stream()));
 }
 
+// Level descriptors of every hierarchy for the whole-V-cycle launch, rebuilt
+// with the work vectors. Used only where every hierarchy ends in a direct
+// coarsest solve and no cluster tail is active.
+static void build_grid(AmsState& a) {
+    const char* env = std::getenv("SSV_AMS_GRID");
+    a.grid = env && env[0] == '1';
+    for (int sub = 0; sub < 4 && a.grid; ++sub)
+        if (a.amg[sub].empty() || !a.amg[sub].back().direct || a.tails[sub].start >= 0) a.grid = false;
+    if (!a.grid) return;
+    auto vals = [&](const DevCsr& M) -> const void* {
+        return a.fp32 ? (const void*)M.val<float>() : (const void*)M.val<double>();
+    };
+    auto dual = [&](const DualVec& v) -> const void* {
+        return a.fp32 ? (const void*)v.get<float>() : (const void*)v.get<double>();
+    };
+    for (int sub = 0; sub < 4; ++sub) {
+        auto& L = a.amg[sub];
+        std::vector<TailLevel> h(L.size());
+        std::memset(h.data(), 0, sizeof(TailLevel) * h.size());
+        for (size_t l = 0; l < L.size(); ++l) {
+            AmgDevLevel& lv = L[l];
+            TailLevel& d = h[l];
+            d.n = lv.A.n;
+            d.direct = lv.direct ? 1 : 0;
+            d.Arp = lv.A.rp.get();
+            d.Aci = lv.A.ci.get();
+            d.Av = vals(lv.A);
+            if (l + 1 < L.size()) {
+                d.Prp = lv.P.rp.get();
+                d.Pci = lv.P.ci.get();
+                d.Pv = vals(lv.P);
+                d.Trp = lv.Pt.rp.get();
+                d.Tci = lv.Pt.ci.get();
+                d.Tv = vals(lv.Pt);
+            }
+            d.l1 = dual(lv.l1);
+            d.il1 = dual(lv.il1);
+            d.b = lv.b.raw.get();
+            d.x = lv.xa.raw.get();
+            d.xalt = lv.xb.raw.get();
+            d.r = lv.r.raw.get();
+            d.Li = lv.Li.get();
+            d.LiT = lv.LiT.get();
+            d.piv = lv.piv.get();
+            d.cz = lv.cz.get();
+        }
+        a.gdesc[sub].upload(h.data(), h.size(), stream());
+    }
+    if (!a.gbar.get()) {
+        a.gbar.alloc(1);
+        a.gbar.zero(stream());
+    }
+    SSV_CUDA(cudaStreamSynchronize(stream()));
+}
+
 // Work vectors for blocks of up to nv real columns (allocation only, so the
 // cycle itself never allocates and can be captured).
 static void ams_reserve(AmsState& a, int nv) {
@@ -1896,6 +2278,7 @@ static void ams_reserve(AmsState& a, int nv) {
     ++a.gen;  // new work buffers: graphs that captured the old ones must be rebuilt
     tune_lanes(a);
     build_tails(a);
+    build_grid(a);
     {
         const char* e = std::getenv("SSV_AMS_TRI");
         a.tri = !(e && e[0] == '0');
