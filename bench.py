@@ -433,7 +433,9 @@ def run_ams(args, rank, world, local):
                                 "copy's padding (2.9% of the entries) and row map add 3% to the algorithmic bytes",
                 "kernel": "k_sell_spmv fine residual (A_bc in 32-row sliced-ELL, 7.43M nnz, FP64; the shape tuner "
                           "keeps it where it times faster than the CSR shapes, on every B200 run so far), "
-                          "L2 flushed before each launch",
+                          "each launch timed alone after evicting L2 by reading a 256 MB buffer (a write-based "
+                          "flush leaves dirty lines whose write-back the launch would pay for: "
+                          "SSV_PROFILE_FLUSH=write measures that form)",
                 "peak_kind": peak_kind, "algorithmic_bytes_per_launch": spmv["bytes"], "launch_ms": spmv["ms"],
                 "warm_GBps": gbps(spmv_warm),
                 "phases_mixed_cold": [{**p, "GBps": gbps(p)} for p in mixed["phases_cold"]],

@@ -1905,14 +1905,41 @@ static HostCsr host_csr_of(const ssv_matrix* M) {
 // operands) and keep the fastest. Runs when work vectors are (re)allocated,
 // outside any capture.
 // ---------------------------------------------------------------------------
-// Evicts the 126 MB L2 by writing a 256 MiB buffer (allocated on first use,
-// kept until exit): the measurements below that stand for HBM-bound passes
-// time each launch after a flush.
+// Evicts the 126 MB L2 by reading a 256 MiB buffer (allocated and zeroed on
+// first use, kept until exit), which leaves L2 holding clean lines of that
+// buffer: the measurements below that stand for HBM-bound passes time each
+// launch after an eviction. (Writing the buffer instead leaves up to 126 MB of
+// dirty lines, whose write-back the timed launch would then pay for while it
+// streams its own data -- which no pass of the cycle meets in a solve, where
+// the preceding passes write only vectors. SSV_PROFILE_FLUSH=write selects
+// that form, for comparison.)
+__global__ void k_l2_evict(const uint4* __restrict__ p, size_t n, unsigned* sink) {
+    unsigned acc = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint4 v = p[i];
+        acc ^= v.x ^ v.y ^ v.z ^ v.w;
+    }
+    if (acc == 0x9e3779b9u) sink[0] = acc;  // the buffer is zero: never taken, keeps the loads
+}
+
 static void l2_flush(cudaStream_t s) {
     static DevBuf<uint8_t> buf;
-    static int k = 0;
-    if (!buf.get()) buf.alloc((size_t)256 << 20);
-    SSV_CUDA(cudaMemsetAsync(buf.get(), ++k & 0xff, buf.size(), s));
+    static DevBuf<unsigned> sink;
+    static const bool write_form = [] {
+        const char* e = std::getenv("SSV_PROFILE_FLUSH");
+        return e && std::strcmp(e, "write") == 0;
+    }();
+    if (!buf.get()) {
+        buf.alloc((size_t)256 << 20);
+        sink.alloc(1);
+        buf.zero(s);
+    }
+    if (write_form) {
+        SSV_CUDA(cudaMemsetAsync(buf.get(), 0, buf.size(), s));
+        return;
+    }
+    k_l2_evict<<<sm_count() * 8, 256, 0, s>>>(reinterpret_cast<const uint4*>(buf.get()), buf.size() / 16, sink.get());
+    SSV_LAUNCH_CHECK();
 }
 
 // Device time of `reps` launches: back to back (warm), or each after an L2
@@ -1985,6 +2012,60 @@ static int max_unroll() {
     return v;
 }
 
+// Tuner record and replay. SSV_AMS_TUNE_SAVE=<file> appends every choice of
+// the tuners below, in call order, one line each ("csr n nnz nv lanes rows
+// sliced" / "pi dir nv lanes"); SSV_AMS_TUNE_LOAD=<file> replays such a file
+// instead of timing, as long as each line names the matrix (size, nonzeros,
+// columns) the tuner is at -- on the first mismatch it says so on stderr and
+// times from there on. A tuning cache for repeated runs, and what keeps a
+// profiled run (where every launch is serialised and the timings say nothing)
+// on the shapes of the plain run it profiles.
+struct TuneReplay {
+    std::vector<std::vector<long long>> rows;
+    size_t next = 0;
+    bool live = false;
+    FILE* save = nullptr;
+    TuneReplay() {
+        if (const char* f = std::getenv("SSV_AMS_TUNE_LOAD")) {
+            if (FILE* in = std::fopen(f, "r")) {
+                char kind[8];
+                while (std::fscanf(in, "%7s", kind) == 1) {
+                    std::vector<long long> r(1, kind[0] == 'c' ? 0 : 1);
+                    const int cnt = kind[0] == 'c' ? 6 : 3;
+                    long long v;
+                    for (int i = 0; i < cnt && std::fscanf(in, "%lld", &v) == 1; ++i) r.push_back(v);
+                    if ((int)r.size() == cnt + 1) rows.push_back(r);
+                }
+                std::fclose(in);
+                live = !rows.empty();
+            } else {
+                std::fprintf(stderr, "ams tune: cannot read %s, timing instead\n", f);
+            }
+        }
+        if (const char* f = std::getenv("SSV_AMS_TUNE_SAVE")) save = std::fopen(f, "a");
+    }
+    // the next recorded row if it matches `want` (kind and key fields), else stop replaying
+    const std::vector<long long>* take(const std::vector<long long>& want) {
+        if (!live) return nullptr;
+        if (next < rows.size() && rows[next].size() >= want.size() &&
+            std::equal(want.begin(), want.end(), rows[next].begin()))
+            return &rows[next++];
+        std::fprintf(stderr, "ams tune: replay stops at entry %zu (matrix differs), timing from here on\n", next);
+        live = false;
+        return nullptr;
+    }
+    void record(const char* line) {
+        if (save) {
+            std::fputs(line, save);
+            std::fflush(save);
+        }
+    }
+};
+static TuneReplay& tune_replay() {
+    static TuneReplay r;
+    return r;
+}
+
 // Shapes of square level matrices are timed as residuals r = b - A x (b given),
 // the form the cycle runs them in (smoothing reads the same streams); the
 // transfers as y = A x.
@@ -1992,6 +2073,13 @@ template <typename TV, typename TX, typename TY, int NV>
 static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1,
                      bool force_cold = false) {
     if (A.n == 0 || A.nnz == 0) return;
+    if (const auto* r = tune_replay().take({0, A.n, A.nnz, NV})) {
+        const int slot = DevCsr::nv_slot(NV);
+        A.tuned[slot] = (int)(*r)[4];
+        A.tuned_u[slot] = (int)(*r)[5];
+        A.tuned_sell[slot] = (A.sell.slices > 0 && std::is_same_v<TV, double>) ? (int)(*r)[6] : 0;
+        return;
+    }
     const TV* v = A.val<TV>();
     // A matrix much larger than a quarter of L2 streams from HBM in the cycle:
     // time it cold; the rest back to back.
@@ -2043,6 +2131,12 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
             if (sell_best < best || sell_mode() == 2) A.tuned_sell[slot] = sell_pick;
         }
     }
+    {
+        char line[128];
+        std::snprintf(line, sizeof(line), "csr %d %lld %d %d %d %d\n", A.n, (long long)A.nnz, NV, pick, pick_u,
+                      A.tuned_sell[slot]);
+        tune_replay().record(line);
+    }
     static const bool log = std::getenv("SSV_AMS_TUNE_LOG") != nullptr;
     if (log) {
         std::fprintf(stderr, "ams tune: n=%d nnz=%lld nv=%d %s -> lanes %d rows/group %d (%.2f us)", A.n,
@@ -2064,6 +2158,10 @@ static void tune_pi(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1)
     T* o2 = a.rs[2].as<T>();
     T* o3 = a.rs[3].as<T>();
     for (int dir = 0; dir < 2; ++dir) {
+        if (const auto* r = tune_replay().take({1, dir, NV})) {
+            a.pi_lanes[dir][slot] = (int)(*r)[3];
+            continue;
+        }
         float best = 1e30f;
         int pick = 0;
         for (int L : cand) {
@@ -2094,6 +2192,11 @@ static void tune_pi(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1)
             }
         }
         a.pi_lanes[dir][slot] = pick;
+        {
+            char line[64];
+            std::snprintf(line, sizeof(line), "pi %d %d %d\n", dir, NV, pick);
+            tune_replay().record(line);
+        }
         if (std::getenv("SSV_AMS_TUNE_LOG"))
             std::fprintf(stderr, "ams tune: Pi %s nv=%d cold -> lanes %d (%.2f us)\n", dir ? "prolong" : "restrict", NV,
                          pick, 1e3 * best / 5);
