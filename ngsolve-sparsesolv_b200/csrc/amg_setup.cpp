@@ -10,6 +10,7 @@
 #include <cmath>
 #include <random>
 #include <thread>
+#include <utility>
 
 namespace ssv {
 
@@ -31,6 +32,102 @@ HostCsr csr_transpose(const HostCsr& A) {
             T.v[p] = A.v[k];
         }
     return T;
+}
+
+HostCsr csr_mul(const HostCsr& A, const HostCsr& B) {
+    HostCsr C;
+    C.n = A.n;
+    C.m = B.m;
+    C.rp.assign(A.n + 1, 0);
+    std::vector<double> acc(B.m, 0.0);
+    std::vector<int> mark(B.m, -1), cols;
+    for (int i = 0; i < A.n; ++i) {
+        cols.clear();
+        for (int a = A.rp[i]; a < A.rp[i + 1]; ++a) {
+            const int j = A.ci[a];
+            const double av = A.v[a];
+            for (int b = B.rp[j]; b < B.rp[j + 1]; ++b) {
+                const int l = B.ci[b];
+                if (mark[l] != i) {
+                    mark[l] = i;
+                    acc[l] = 0.0;
+                    cols.push_back(l);
+                }
+                acc[l] += av * B.v[b];
+            }
+        }
+        std::sort(cols.begin(), cols.end());
+        for (int l : cols) {
+            C.ci.push_back(l);
+            C.v.push_back(acc[l]);
+        }
+        C.rp[i + 1] = (int)C.ci.size();
+    }
+    return C;
+}
+
+HostCsr csr_add(const HostCsr& A, double a, const HostCsr& B, double b) {
+    HostCsr C;
+    C.n = A.n;
+    C.m = std::max(A.m, B.m);
+    C.rp.assign(A.n + 1, 0);
+    std::vector<std::pair<int, double>> row;
+    for (int i = 0; i < A.n; ++i) {
+        row.clear();
+        for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) row.push_back({A.ci[k], a * A.v[k]});
+        for (int k = B.rp[i]; k < B.rp[i + 1]; ++k) row.push_back({B.ci[k], b * B.v[k]});
+        std::stable_sort(row.begin(), row.end(),
+                         [](const std::pair<int, double>& p, const std::pair<int, double>& q) { return p.first < q.first; });
+        for (size_t k = 0; k < row.size();) {
+            size_t e = k;
+            double sum = 0.0;
+            while (e < row.size() && row[e].first == row[k].first) sum += row[e++].second;
+            C.ci.push_back(row[k].first);
+            C.v.push_back(sum);
+            k = e;
+        }
+        C.rp[i + 1] = (int)C.ci.size();
+    }
+    return C;
+}
+
+FusedLevel fused_level(const HostCsr& A, const HostCsr& P, const HostCsr& Pt, const std::vector<double>& d) {
+    const int n = A.n;
+    HostCsr AD = A;  // A D^{-1}
+    for (int i = 0; i < n; ++i)
+        for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) AD.v[k] = A.v[k] / d[A.ci[k]];
+    FusedLevel F;
+    F.R = csr_add(Pt, 1.0, csr_mul(Pt, AD), -1.0);
+    HostCsr I2;  // 2 I
+    I2.n = I2.m = n;
+    I2.rp.resize(n + 1);
+    I2.ci.resize(n);
+    I2.v.assign(n, 2.0);
+    for (int i = 0; i <= n; ++i) I2.rp[i] = i;
+    for (int i = 0; i < n; ++i) I2.ci[i] = i;
+    HostCsr S = csr_add(I2, 1.0, AD, -1.0);  // then rows by D^{-1}
+    for (int i = 0; i < n; ++i)
+        for (int k = S.rp[i]; k < S.rp[i + 1]; ++k) S.v[k] /= d[i];
+    HostCsr DAP = csr_mul(A, P);  // then rows by D^{-1}
+    for (int i = 0; i < n; ++i)
+        for (int k = DAP.rp[i]; k < DAP.rp[i + 1]; ++k) DAP.v[k] /= d[i];
+    const HostCsr Q = csr_add(P, 1.0, DAP, -1.0);
+    HostCsr& U = F.U;
+    U.n = n;
+    U.m = n + P.m;
+    U.rp.assign(n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        for (int k = S.rp[i]; k < S.rp[i + 1]; ++k) {
+            U.ci.push_back(S.ci[k]);
+            U.v.push_back(S.v[k]);
+        }
+        for (int k = Q.rp[i]; k < Q.rp[i + 1]; ++k) {
+            U.ci.push_back(n + Q.ci[k]);
+            U.v.push_back(Q.v[k]);
+        }
+        U.rp[i + 1] = (int)U.ci.size();
+    }
+    return F;
 }
 
 HostCsr csr_rap(const HostCsr& A, const HostCsr& P) {

@@ -21,6 +21,23 @@ HostCsr csr_transpose(const HostCsr& A);
 // sorted) -- the semantics of NGSolve's SparseMatrix::Restrict.
 HostCsr csr_rap(const HostCsr& A, const HostCsr& P);
 
+// C = A B (columns of each row sorted)
+HostCsr csr_mul(const HostCsr& A, const HostCsr& B);
+// C = a A + b B on the union pattern (columns sorted)
+HostCsr csr_add(const HostCsr& A, double a, const HostCsr& B, double b);
+
+// One level's V-cycle steps (num_smooth = 1, l1-Jacobi with l1 = d) folded
+// into two matrices, from the level's A, P, P^T and d:
+//   down: b_next = R b,  R = P^T (I - A D^{-1})        (first sweep x = D^{-1} b,
+//         residual b - A x and restriction in one product)
+//   up:   x = U [b; e],  U = [D^{-1}(2I - A D^{-1}) | (I - D^{-1} A) P]
+//         (prolongation x + P e and the post sweep in one product; columns
+//         n.. of U address the coarse correction e)
+struct FusedLevel {
+    HostCsr R, U;
+};
+FusedLevel fused_level(const HostCsr& A, const HostCsr& P, const HostCsr& Pt, const std::vector<double>& d);
+
 struct AmgHostLevel {
     HostCsr A, P, Pt;
     std::vector<double> l1;

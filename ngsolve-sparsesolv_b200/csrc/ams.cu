@@ -40,7 +40,11 @@ namespace ssv {
 // ---------------------------------------------------------------------------
 // Multi-vector kernels
 // ---------------------------------------------------------------------------
-enum MvMode : int { MV_AX = 0, MV_RES = 1, MV_ADD = 2, MV_JAC = 3 };
+// MV_TWO: y = A [x; z] with z passed in the b slot -- columns below the row
+// count read x, the rest read z at (column - rows) (the fused up-sweep
+// matrix of a V-cycle level: its own right-hand side and the coarse
+// correction)
+enum MvMode : int { MV_AX = 0, MV_RES = 1, MV_ADD = 2, MV_JAC = 3, MV_TWO = 4 };
 
 // One row of NV columns in the widest aligned accesses the row allows (work
 // vectors come from cudaMalloc, so row r starts at r * NV * sizeof(T)).
@@ -129,7 +133,12 @@ k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T
             for (int u = 0; u < U; ++u) {
                 if (col[u] >= 0) {
                     TX xv[NV];
-                    load_row<NV>(x + (size_t)col[u] * NV, xv);
+                    if constexpr (MODE == MV_TWO)
+                        load_row<NV>(col[u] < n ? x + (size_t)col[u] * NV
+                                                : reinterpret_cast<const TX*>(b) + (size_t)(col[u] - n) * NV,
+                                     xv);
+                    else
+                        load_row<NV>(x + (size_t)col[u] * NV, xv);
 #pragma unroll
                     for (int c = 0; c < NV; ++c) acc[u][c] += a[u] * (TA)xv[c];
                     kk[u] += LANES;
@@ -148,7 +157,7 @@ k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T
 #pragma unroll
                 for (int c = 0; c < NV; ++c) {
                     const TY ac = (TY)acc[u][c];
-                    if constexpr (MODE == MV_AX) {
+                    if constexpr (MODE == MV_AX || MODE == MV_TWO) {
                         y[base + c] = ac;
                     } else if constexpr (MODE == MV_RES) {
                         y[base + c] = b[base + c] - ac;
@@ -527,8 +536,12 @@ k_mv3_spmv(Tri<T, K> t, T w, const KState* st) {
             const int k1 = rp[row + 1];
             for (int k = rp[row] + sub; k < k1; k += LANES) {
                 const T a = v[k];
+                const int j = ci[k];
                 T xv[NV];
-                load_row<NV>(x + (size_t)ci[k] * NV, xv);
+                if constexpr (MODE == MV_TWO)
+                    load_row<NV>(j < n ? x + (size_t)j * NV : b + (size_t)(j - n) * NV, xv);
+                else
+                    load_row<NV>(x + (size_t)j * NV, xv);
 #pragma unroll
                 for (int c = 0; c < NV; ++c) acc[c] += a * xv[c];
             }
@@ -541,7 +554,7 @@ k_mv3_spmv(Tri<T, K> t, T w, const KState* st) {
             const size_t base = (size_t)row * NV;
 #pragma unroll
             for (int c = 0; c < NV; ++c) {
-                if constexpr (MODE == MV_AX) {
+                if constexpr (MODE == MV_AX || MODE == MV_TWO) {
                     y[base + c] = acc[c];
                 } else if constexpr (MODE == MV_ADD) {
                     y[base + c] += w * acc[c];
@@ -1280,6 +1293,7 @@ struct WorkVec {
 
 struct AmgDevLevel {
     DevCsr A, P, Pt;
+    DevCsr R, U;  // fused down / up matrices (fused_level; non-coarsest levels, SSV_AMS_FUSED)
     DualVec l1, il1;
     bool direct = false;
     DevBuf<double> Li, LiT, piv;  // coarsest: LDL^T factors (FP64 in both forms)
@@ -1368,7 +1382,7 @@ static void launch_sell(const DevSell& S, int steps, cudaStream_t s, const TX* x
 template <typename TV, typename TX, typename TY, int NV, int MODE, bool RECIP>
 static void mv_spmv(const DevCsr& A, const TX* x, TY* y, const TY* b, const TY* d, TY w, const KState* st,
                     cudaStream_t s) {
-    if constexpr (std::is_same_v<TV, double>) {
+    if constexpr (std::is_same_v<TV, double> && MODE != MV_TWO) {
         if (A.sell_for(NV)) {
             launch_sell<TX, TY, NV, MODE, RECIP>(A.sell, A.tuned_sell[DevCsr::nv_slot(NV)], s, x, y, b, d, w, st);
             return;
@@ -1405,11 +1419,59 @@ static const T* l1_of(const AmgDevLevel& lv) {
     return RECIP ? lv.il1.get<T>() : lv.l1.get<T>();
 }
 
+// SSV_AMS_FUSED=0: V-cycles run the four per-level passes (fused first sweep +
+// residual, restriction, prolongation, post sweep) instead of the two fused
+// products R and U
+static bool fused_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("SSV_AMS_FUSED");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v != 0;
+}
+
+// a hierarchy the fused V-cycle can run: R and U on every non-coarsest level,
+// a direct coarsest solve
+static bool fused_ready(const std::vector<AmgDevLevel>& L) {
+    if (L.empty() || !L.back().direct) return false;
+    for (size_t l = 0; l + 1 < L.size(); ++l)
+        if (L[l].U.n == 0 || L[l].R.n == 0) return false;
+    return true;
+}
+
+template <typename T, int NV, bool RECIP>
+static void coarse_direct(AmgDevLevel& lv, const T* b, T* x, const KState* st, cudaStream_t s) {
+    const int g = std::max(1, std::min((lv.A.n + 7) / 8, sm_count() * 4));
+    launch_k(k_mv_coarse_fwd<T, NV>, g, kBlock, s, lv.A.n, lv.Li.get(), lv.piv.get(), b, lv.cz.get(), st);
+    launch_k(k_mv_coarse_bwd<T, NV>, g, kBlock, s, lv.A.n, lv.LiT.get(), lv.cz.get(), x, st);
+}
+
+// The V-cycle of `vcycle` (num_smooth = 1, direct coarsest) through the fused
+// level matrices: the down sweep is one product b_{l+1} = R_l b_l per level,
+// the up sweep one product x_l = U_l [b_l; e_{l+1}] per level -- two launches
+// per level instead of four. Same arithmetic up to rounding.
+template <typename T, int NV, bool RECIP>
+static T* vcycle_fused(std::vector<AmgDevLevel>& L, const T* b0, const KState* st, cudaStream_t s) {
+    const int n = (int)L.size();
+    auto rhs = [&](int l) -> const T* { return l == 0 ? b0 : L[l].b.template as<T>(); };
+    for (int l = 0; l + 1 < n; ++l)
+        mv_spmv<T, T, T, NV, MV_AX, RECIP>(L[l].R, rhs(l), L[l + 1].b.template as<T>(), nullptr, nullptr, T(0), st,
+                                           s);
+    coarse_direct<T, NV, RECIP>(L[n - 1], rhs(n - 1), L[n - 1].xa.template as<T>(), st, s);
+    for (int l = n - 2; l >= 0; --l) {
+        const T* e = (l + 1 == n - 1) ? L[l + 1].xa.template as<T>() : L[l + 1].xb.template as<T>();
+        mv_spmv<T, T, T, NV, MV_TWO, RECIP>(L[l].U, rhs(l), L[l].xb.template as<T>(), e, nullptr, T(0), st, s);
+    }
+    return n == 1 ? L[0].xa.template as<T>() : L[0].xb.template as<T>();
+}
+
 // One AMG V-cycle (VCycle / DualVCycle, compact_amg.hpp:662-706,801-841) on
 // level l: b -> x (x starts at zero). Returns the buffer holding x.
 template <typename T, int NV, bool RECIP>
 static T* vcycle(std::vector<AmgDevLevel>& L, const TailSet& tail, int l, const T* b, int num_smooth,
                  const KState* st, cudaStream_t s) {
+    if (l == 0 && num_smooth == 1 && tail.start < 0 && fused_ready(L)) return vcycle_fused<T, NV, RECIP>(L, b, st, s);
     AmgDevLevel& lv = L[l];
     if (num_smooth == 1 && tail.start >= 0 && l == tail.start) {
         k_vcycle_tail<T, NV, RECIP><<<kTailCluster, kTailBlock, 0, s>>>(tail.desc.get(), l, (int)L.size(), b, st);
@@ -1509,6 +1571,60 @@ static void vcycleM(std::vector<AmgDevLevel>* const* H, const T* const* rhs0, in
     auto L = [&](int k) { return (int)H[k]->size(); };
     auto rhs = [&](int k, int l) -> const T* { return l == 0 ? rhs0[k] : (*H[k])[l].b.template as<T>(); };
     auto lv = [&](int k, int l) -> AmgDevLevel& { return (*H[k])[l]; };
+    bool fused = true;
+    for (int k = 0; k < parts; ++k) fused = fused && fused_ready(*H[k]);
+    auto coarse = [&]() {  // coarsest levels: LDL^T pseudo-inverse, FP64
+        TriCoarse<K> f{}, b{};
+        int nmax = 0;
+        for (int k = 0; k < parts; ++k) {
+            AmgDevLevel& v = lv(k, L(k) - 1);
+            nmax = std::max(nmax, v.A.n);
+            f.n[k] = b.n[k] = v.A.n;
+            f.M[k] = v.Li.get(); b.M[k] = v.LiT.get();
+            f.piv[k] = b.piv[k] = v.piv.get();
+            f.cz[k] = b.cz[k] = v.cz.get();
+            f.io[k] = rhs(k, L(k) - 1);
+            b.io[k] = v.xa.raw.get();
+        }
+        const dim3 grid(std::max(1, std::min((nmax + 7) / 8, std::max(1, sm_count() * 4 / parts))), parts);
+        launch_k(k_mv3_coarse<T, NV, true, K>, grid, kBlock, s, f, st);
+        launch_k(k_mv3_coarse<T, NV, false, K>, grid, kBlock, s, b, st);
+    };
+    if (fused) {  // two fused products per level (vcycle_fused), all hierarchies in each launch
+        for (int l = 0; l < Lmax - 1; ++l) {
+            Tri<T, K> rs{};
+            int q = 0, k0 = -1;
+            for (int k = 0; k < parts; ++k) {
+                if (l >= L(k) - 1) continue;
+                if (k0 < 0) k0 = k;
+                const DevCsr& R = lv(k, l).R;
+                rs.n[q] = R.n; rs.rp[q] = R.rp.get(); rs.ci[q] = R.ci.get(); rs.v[q] = R.val<T>();
+                rs.x[q] = rhs(k, l); rs.y[q] = lv(k, l + 1).b.template as<T>();
+                ++q;
+            }
+            if (q) spmv3<T, NV, MV_AX, RECIP, K>(rs, q, lv(k0, l).R.lanes_for(NV), T(0), st, s);
+        }
+        coarse();
+        for (int l = Lmax - 2; l >= 0; --l) {
+            Tri<T, K> up{};
+            int q = 0, k0 = -1;
+            for (int k = 0; k < parts; ++k) {
+                if (l > L(k) - 2) continue;
+                if (k0 < 0) k0 = k;
+                AmgDevLevel& v = lv(k, l);
+                AmgDevLevel& nx = lv(k, l + 1);
+                up.n[q] = v.U.n; up.rp[q] = v.U.rp.get(); up.ci[q] = v.U.ci.get(); up.v[q] = v.U.val<T>();
+                up.x[q] = rhs(k, l);
+                up.b[q] = (l + 1 == L(k) - 1) ? nx.xa.template as<T>() : nx.xb.template as<T>();
+                up.y[q] = v.xb.template as<T>();
+                ++q;
+            }
+            if (q) spmv3<T, NV, MV_TWO, RECIP, K>(up, q, lv(k0, l).U.lanes_for(NV), T(0), st, s);
+        }
+        for (int k = 0; k < parts; ++k)
+            out[k] = (L(k) == 1) ? lv(k, 0).xa.template as<T>() : lv(k, 0).xb.template as<T>();
+        return;
+    }
     for (int l = 0; l < Lmax - 1; ++l) {
         Tri<T, K> fr{}, rs{};
         int q = 0, k0 = -1;
@@ -2071,7 +2187,7 @@ static TuneReplay& tune_replay() {
 // transfers as y = A x.
 template <typename TV, typename TX, typename TY, int NV>
 static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1,
-                     bool force_cold = false) {
+                     bool force_cold = false, bool two = false) {
     if (A.n == 0 || A.nnz == 0) return;
     if (const auto* r = tune_replay().take({0, A.n, A.nnz, NV})) {
         const int slot = DevCsr::nv_slot(NV);
@@ -2091,7 +2207,10 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
         if (U > 1 && (A.n < kUnrollMinRows || U > max_unroll())) continue;
         const int grid = mv_grid(A.n, L, U);
         auto launch = [&] {
-            if (b)
+            if (two)
+                launch_mv<TV, TX, TY, NV, MV_TWO, false>(L, U, grid, s, A.n, A.rp.get(), A.ci.get(), v, x, y, b,
+                                                         nullptr, TY(0), nullptr);
+            else if (b)
                 launch_mv<TV, TX, TY, NV, MV_RES, false>(L, U, grid, s, A.n, A.rp.get(), A.ci.get(), v, x, y, b,
                                                          nullptr, TY(0), nullptr);
             else
@@ -2216,6 +2335,11 @@ static void tune_all_nv(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t
             if (l + 1 < L.size()) {
                 tune_csr<T, T, T, NV>(L[l].P, L[l + 1].xa.as<T>(), L[l].r.as<T>(), nullptr, s, e0, e1);
                 tune_csr<T, T, T, NV>(L[l].Pt, L[l].r.as<T>(), L[l + 1].b.as<T>(), nullptr, s, e0, e1);
+                if (L[l].R.n) {  // fused down: b_{l+1} = R b_l; fused up: x_l = U [b_l; e]
+                    tune_csr<T, T, T, NV>(L[l].R, L[l].b.as<T>(), L[l + 1].b.as<T>(), nullptr, s, e0, e1);
+                    tune_csr<T, T, T, NV>(L[l].U, L[l].b.as<T>(), L[l].xb.as<T>(), L[l + 1].xa.as<T>(), s, e0, e1,
+                                          false, true);
+                }
             }
         }
     }
@@ -2511,6 +2635,17 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
                 }
             }
         }
+        // fused down / up matrices of every non-coarsest level (FP64
+        // hierarchies only: rounded to FP32, the merged matrices cost the
+        // preconditioner its quality -- 207 instead of 34 PCG iterations on the
+        // 40^3 magnetostatic system -- so the FP32 form keeps the four passes)
+        if (fused_enabled() && !a.fp32)
+            for (size_t l = 0; l + 1 < hl.size(); ++l) {
+                AmgDevLevel& dl = a.amg[sub][l];
+                const FusedLevel F = fused_level(hl[l].A, hl[l].P, hl[l].Pt, hl[l].l1);
+                dl.R.upload(F.R, false, s);
+                dl.U.upload(F.U, false, s);
+            }
         // level-0 scaling folded into this subspace's transfers
         if (sub == 0) {
             upload_fine(a.G, a.fp32 ? scaled_csr(a.host.G, nullptr, &isc[0]) : a.host.G, s);
