@@ -29,6 +29,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <type_traits>
 
 #include "amg_setup.hpp"
@@ -2584,6 +2585,23 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
     a.fine_l1.upload(a.host.fine_l1.data(), a.host.fine_l1.size(), s);
     const std::vector<double> il1 = reciprocal(a.host.fine_l1);
     a.fine_il1.upload(il1.data(), il1.size(), s);
+    // fused down / up matrices of every non-coarsest level (FP64 hierarchies
+    // only: rounded to FP32, the merged matrices cost the preconditioner its
+    // quality -- 207 instead of 34 PCG iterations on the 40^3 magnetostatic
+    // system -- so the FP32 form keeps the four passes); the four subspaces on
+    // their own host threads
+    std::vector<FusedLevel> fused[4];
+    if (fused_enabled() && !a.fp32) {
+        std::vector<std::thread> th;
+        for (int sub = 0; sub < 4; ++sub)
+            th.emplace_back([&a, &fused, sub] {
+                const auto& hl = a.host.amg[sub].levels;
+                fused[sub].resize(hl.empty() ? 0 : hl.size() - 1);
+                for (size_t l = 0; l + 1 < hl.size(); ++l)
+                    fused[sub][l] = fused_level(hl[l].A, hl[l].P, hl[l].Pt, hl[l].l1);
+            });
+        for (auto& t : th) t.join();
+    }
     for (int sub = 0; sub < 4; ++sub) {
         const auto& hl = a.host.amg[sub].levels;
         a.amg[sub].clear();
@@ -2635,17 +2653,10 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
                 }
             }
         }
-        // fused down / up matrices of every non-coarsest level (FP64
-        // hierarchies only: rounded to FP32, the merged matrices cost the
-        // preconditioner its quality -- 207 instead of 34 PCG iterations on the
-        // 40^3 magnetostatic system -- so the FP32 form keeps the four passes)
-        if (fused_enabled() && !a.fp32)
-            for (size_t l = 0; l + 1 < hl.size(); ++l) {
-                AmgDevLevel& dl = a.amg[sub][l];
-                const FusedLevel F = fused_level(hl[l].A, hl[l].P, hl[l].Pt, hl[l].l1);
-                dl.R.upload(F.R, false, s);
-                dl.U.upload(F.U, false, s);
-            }
+        for (size_t l = 0; l < fused[sub].size(); ++l) {
+            a.amg[sub][l].R.upload(fused[sub][l].R, false, s);
+            a.amg[sub][l].U.upload(fused[sub][l].U, false, s);
+        }
         // level-0 scaling folded into this subspace's transfers
         if (sub == 0) {
             upload_fine(a.G, a.fp32 ? scaled_csr(a.host.G, nullptr, &isc[0]) : a.host.G, s);
