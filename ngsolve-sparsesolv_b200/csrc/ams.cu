@@ -2945,6 +2945,11 @@ static void amg_rebuild(AmgOnly& g, const ssv_matrix* A) {
         if (l + 1 < hl.size()) {
             dl.P.upload(hl[l].P, false, s);
             dl.Pt.upload(hl[l].Pt, false, s);
+            if (fused_enabled() && g.num_smooth == 1) {  // the two fused level products (vcycle_fused)
+                const FusedLevel F = fused_level(hl[l].A, hl[l].P, hl[l].Pt, hl[l].l1);
+                dl.R.upload(F.R, false, s);
+                dl.U.upload(F.U, false, s);
+            }
         }
         dl.direct = hl[l].direct;
         if (dl.direct) {
@@ -2970,6 +2975,12 @@ static void amg_rebuild(AmgOnly& g, const ssv_matrix* A) {
                                                 e1);
             tune_csr<double, double, double, 1>(L.Pt, L.r.as<double>(), g.lev[l + 1].b.as<double>(), nullptr, s, e0,
                                                 e1);
+            if (L.R.n) {
+                tune_csr<double, double, double, 1>(L.R, L.b.as<double>(), g.lev[l + 1].b.as<double>(), nullptr, s,
+                                                    e0, e1);
+                tune_csr<double, double, double, 1>(L.U, L.b.as<double>(), L.xb.as<double>(),
+                                                    g.lev[l + 1].xa.as<double>(), s, e0, e1, false, true);
+            }
         }
     }
     cudaEventDestroy(e0);

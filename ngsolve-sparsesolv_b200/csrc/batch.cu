@@ -486,7 +486,10 @@ static void bt_precond(ssv_batch& B, const zdouble* in, zdouble* out, const KSta
         if ((int)A.size() == B.F && ams_apply_block_multi(A.data(), B.F, ins.data(), outs.data(), B.R, st, s)) return;
     }
     B.forks.fork(s, B.branches);
-    ams_grid_suspend(true);
+    struct GridSuspend {  // whole-V-cycle launches off while the branches are issued, also on a throw
+        GridSuspend() { ams_grid_suspend(true); }
+        ~GridSuspend() { ams_grid_suspend(false); }
+    } suspend;
     for (int f = 0; f < B.F; ++f) {
         const zdouble* i = in + f * blk;
         zdouble* o = out + f * blk;
@@ -497,7 +500,6 @@ static void bt_precond(ssv_batch& B, const zdouble* in, zdouble* out, const KSta
         else
             SSV_CUDA(cudaMemcpyAsync(o, i, sizeof(zdouble) * blk, cudaMemcpyDeviceToDevice, fs));
     }
-    ams_grid_suspend(false);
     B.forks.join(s, B.branches);
 }
 
