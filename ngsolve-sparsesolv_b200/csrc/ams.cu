@@ -2585,20 +2585,37 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
     a.fine_l1.upload(a.host.fine_l1.data(), a.host.fine_l1.size(), s);
     const std::vector<double> il1 = reciprocal(a.host.fine_l1);
     a.fine_il1.upload(il1.data(), il1.size(), s);
-    // fused down / up matrices of every non-coarsest level (FP64 hierarchies
-    // only: rounded to FP32, the merged matrices cost the preconditioner its
-    // quality -- 207 instead of 34 PCG iterations on the 40^3 magnetostatic
-    // system -- so the FP32 form keeps the four passes); the four subspaces on
-    // their own host threads
+    // fused down / up matrices of every non-coarsest level, from the matrices in
+    // the form the device holds them (diagonally scaled in the FP32 form); the
+    // subspaces on their own host threads. In the FP32 form only the three
+    // nodal hierarchies take them: fused in FP32, the gradient hierarchy costs
+    // the preconditioner its quality (144 instead of 34 PCG iterations on the
+    // 40^3 magnetostatic system; with every hierarchy fused, no convergence in
+    // 500), while the fused nodal ones change nothing (34).
     std::vector<FusedLevel> fused[4];
-    if (fused_enabled() && !a.fp32) {
+    if (fused_enabled()) {
         std::vector<std::thread> th;
-        for (int sub = 0; sub < 4; ++sub)
+        for (int sub = a.fp32 ? 1 : 0; sub < 4; ++sub)
             th.emplace_back([&a, &fused, sub] {
                 const auto& hl = a.host.amg[sub].levels;
                 fused[sub].resize(hl.empty() ? 0 : hl.size() - 1);
-                for (size_t l = 0; l + 1 < hl.size(); ++l)
-                    fused[sub][l] = fused_level(hl[l].A, hl[l].P, hl[l].Pt, hl[l].l1);
+                std::vector<std::vector<double>> sc(hl.size()), isc(hl.size());
+                if (a.fp32)
+                    for (size_t l = 0; l < hl.size(); ++l) {
+                        sc[l] = diag_scale(hl[l].A);
+                        isc[l] = inverted(sc[l]);
+                    }
+                for (size_t l = 0; l + 1 < hl.size(); ++l) {
+                    if (!a.fp32) {
+                        fused[sub][l] = fused_level(hl[l].A, hl[l].P, hl[l].Pt, hl[l].l1);
+                        continue;
+                    }
+                    std::vector<double> l1s(hl[l].A.n);
+                    for (int i = 0; i < hl[l].A.n; ++i) l1s[i] = hl[l].l1[i] * isc[l][i] * isc[l][i];
+                    fused[sub][l] =
+                        fused_level(scaled_csr(hl[l].A, &isc[l], &isc[l]), scaled_csr(hl[l].P, &sc[l], &isc[l + 1]),
+                                    scaled_csr(hl[l].Pt, &isc[l + 1], &sc[l]), l1s);
+                }
             });
         for (auto& t : th) t.join();
     }
@@ -2654,8 +2671,8 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
             }
         }
         for (size_t l = 0; l < fused[sub].size(); ++l) {
-            a.amg[sub][l].R.upload(fused[sub][l].R, false, s);
-            a.amg[sub][l].U.upload(fused[sub][l].U, false, s);
+            a.amg[sub][l].R.upload(fused[sub][l].R, a.fp32, s);
+            a.amg[sub][l].U.upload(fused[sub][l].U, a.fp32, s);
         }
         // level-0 scaling folded into this subspace's transfers
         if (sub == 0) {
