@@ -132,6 +132,13 @@ typedef struct ssv_batch_tune_entry {
 /* ---- library ----------------------------------------------------------- */
 void ssv_version(int* major, int* minor, int* patch);
 const char* ssv_last_error(void);
+/* Watchdog of the device-looped solves (new: no reference counterpart). Every
+ * iterative solve loops its iteration graph on the device and stops after
+ * maxiter + 4 loop bodies at most (a state that never reports done: the
+ * solve fails with SSV_ERR_TIMEOUT and the context stays usable).
+ * max_loops > 0 sets that cap for every later solve of the process; 0
+ * restores the default. */
+void ssv_set_loop_guard(int32_t max_loops);
 /* Number of CUDA devices and the name of device 0 (no allocation). */
 int ssv_device_info(int* count, char* name, int name_cap);
 /* Reference defaults of SolverConfig (solver_config.hpp:39-157). */
@@ -224,6 +231,38 @@ int ssv_cocr_solve(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs,
 int ssv_cocr_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs,
                        int32_t maxiter, double tol, int32_t printrates,
                        const void* d_b, void* d_x, int32_t* iterations);
+
+/* ---- refined COCR: the mixed-precision form's Krylov driver (new: no
+ *      reference counterpart; each cycle is the COCRSolverNGS recurrence) ----
+ * FP64 defect correction around COCR: cycles of the recurrence of
+ * ssv_cocr_solve, each started from the FP64 true residual r = P(b - A x) of
+ * the current x (rt = M^{-1} r, p = rt, q = P A p) and ended once its
+ * recurrence residual has dropped by restart_drop (0 < restart_drop < 1)
+ * from the residual it started from (or on tol, a breakdown, maxiter). The
+ * solve ends when the true relative residual ||P(b - A x)|| / ||P b|| <= tol.
+ * This is what keeps an FP32-form preconditioner usable under COCR: the
+ * plain recurrence (rt -= alpha M^{-1} q) assumes an exactly linear M^{-1}
+ * and stalls near M^{-1}'s rounding level. The breakdown thresholds (1e-30 on
+ * |mu|, |rho|) scale with (||r_start|| / ||P b||)^2. x is zeroed on entry.
+ * info: iterations = recurrence steps over all cycles, cycles, converged
+ * (true residual <= tol), true_residual (relative, FP64). */
+typedef struct ssv_refine_info {
+    int32_t iterations;
+    int32_t cycles;
+    int32_t converged;
+    int32_t pad_;
+    double true_residual;
+} ssv_refine_info;
+int ssv_cocr_refined_solve(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, int32_t maxiter,
+                           double tol, double restart_drop, int32_t printrates, const void* b, void* x,
+                           ssv_refine_info* info);
+int ssv_cocr_refined_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, int32_t maxiter,
+                               double tol, double restart_drop, int32_t printrates, const void* d_b,
+                               void* d_x, ssv_refine_info* info);
+/* Measurement hook (no reference counterpart): kernels launched by the last
+ * ssv_cocr_solve[_dev] / ssv_cocr_refined_solve[_dev] of the calling thread
+ * (graph kernel nodes times executed loop bodies, plus the set-up launches). */
+int ssv_cocr_last_launches(int64_t* launches);
 
 /* ---- Compact AMS (include/sparsesolv/preconditioners/compact_ams.hpp,
  *      complex_compact_ams.hpp; factories sparsesolv_python_export.hpp:410-530) */
@@ -340,6 +379,17 @@ int ssv_batch_cocr_solve_dev(ssv_batch* b, int32_t maxiter, double tol, const vo
  * every 10th step when a preconditioner is in the FP32 form, whose rounding
  * makes it not exactly linear, so the recurrence drifts; never otherwise). */
 int ssv_batch_set_replacement(ssv_batch* b, int32_t every);
+/* Refined form (new: no reference counterpart; the per-column form of
+ * ssv_cocr_refined_solve): restart_drop in (0, 1) makes every column run
+ * cycles of the recurrence, each started from its FP64 true residual and
+ * ended once its residual has dropped by restart_drop; a column is done when
+ * its true relative residual is <= tol (converged) or it is out of
+ * iterations. residuals then hold the true relative residuals, iterations the
+ * recurrence steps over all cycles. 0 (the default) = the plain recurrence.
+ * Residual replacement is off in the refined form. */
+int ssv_batch_set_refinement(ssv_batch* b, double restart_drop);
+/* Cycles (graph loops) of the last solve (1 for the plain form). */
+int ssv_batch_last_cycles(const ssv_batch* b, int32_t* cycles);
 /* Autotuner record: up to cap entries, *count = entries measured, *chosen =
  * index of the shape in use. */
 int ssv_batch_tuning(const ssv_batch* b, ssv_batch_tune_entry* entries, int32_t cap, int32_t* count,

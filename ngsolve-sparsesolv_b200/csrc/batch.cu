@@ -20,6 +20,14 @@
 // ||r|| / ||b|| <= tol (Hermitian norm), iterations = j + 1 on convergence and
 // maxiter otherwise. A finished column is frozen (no further updates) while
 // the others continue.
+//
+// Refined form (restart_drop > 0; the single-system ssv_cocr_refined_solve per
+// column): every column runs cycles of that recurrence, each started from its
+// FP64 true residual and ended once its residual has dropped by restart_drop
+// (or on tol, a breakdown, maxiter); a column is finished when its true
+// residual is <= tol. The graph loop runs one cycle of every live column; the
+// host then computes the true residuals of all columns (one SpMM pass) and
+// restarts the columns that need another cycle.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -34,15 +42,21 @@ namespace ssv {
 struct BCol {
     double2 alpha, beta, rho;
     double normalizer, res;
-    int done, converged, iters, pad_;
+    double brk_thr;      // |mu|, |rho| breakdown threshold (1e-30, scaled in refined cycles)
+    double restart_abs;  // refined form: ||r|| that ends this column's cycle (0 = never)
+    double tres;         // refined form: ||P(b - A x)|| after the last cycle
+    int done, converged, iters;
+    int work;            // x updates performed (all cycles)
 };
 
 struct BState {
     KState ks;  // ks.done: every column finished (set only by the loop control)
     int ncols, ndone;
+    double drop;  // refined form's restart_drop (0 = the reference's recurrence only)
+    int refined, pad_;
 };
 
-enum BtOp : int { BT_TIME = 0, BT_RHO_INIT, BT_RHO, BT_MU, BT_NORM0, BT_UPDATE };
+enum BtOp : int { BT_TIME = 0, BT_RHO_INIT, BT_RHO, BT_MU, BT_NORM0, BT_UPDATE, BT_TRUE };
 
 __device__ inline void bcol_done(BState* bs, BCol& c, int conv, int iters) {
     c.done = 1;
@@ -54,26 +68,35 @@ __device__ inline void bcol_done(BState* bs, BCol& c, int conv, int iters) {
 __device__ inline void bt_finish(BState* bs, BCol* cols, int c, double2 total, int op) {
     if (op == BT_TIME) return;
     BCol& col = cols[c];
+    if (op == BT_TRUE) {  // between refined cycles (every column is stopped then)
+        col.tres = std::sqrt(std::fabs(total.x));
+        return;
+    }
     if (col.done) return;
     if (op == BT_RHO_INIT) {
         col.rho = total;
     } else if (op == BT_RHO) {  // :354-359
         const zdouble rho{col.rho.x, col.rho.y};
-        if (ST<zdouble>::abs(rho) < 1e-30) { bcol_done(bs, col, 0, bs->ks.it); return; }
+        if (ST<zdouble>::abs(rho) < col.brk_thr) { bcol_done(bs, col, 0, bs->ks.it); return; }
         const zdouble b = zdiv(zdouble{total.x, total.y}, rho);
         col.beta = make_double2(b.x, b.y);
         col.rho = total;
     } else if (op == BT_MU) {  // :323-327
         const zdouble mu{total.x, total.y};
-        if (ST<zdouble>::abs(mu) < 1e-30) { bcol_done(bs, col, 0, bs->ks.it); return; }
+        if (ST<zdouble>::abs(mu) < col.brk_thr) { bcol_done(bs, col, 0, bs->ks.it); return; }
         const zdouble a = zdiv(zdouble{col.rho.x, col.rho.y}, mu);
         col.alpha = make_double2(a.x, a.y);
     } else if (op == BT_NORM0) {  // :298-301
         col.normalizer = std::sqrt(std::fabs(total.x));
+        col.brk_thr = 1e-30;
+        col.restart_abs = bs->drop * col.normalizer;
         if (col.normalizer < 1e-30) bcol_done(bs, col, 0, 0);
     } else {  // BT_UPDATE, :338-347
         col.res = std::sqrt(std::fabs(total.x));
+        col.work++;
         if (col.res / col.normalizer <= bs->ks.tol) bcol_done(bs, col, 1, bs->ks.it + 1);
+        else if (col.res <= col.restart_abs) bcol_done(bs, col, 0, bs->ks.it + 1);
+        else if (bs->refined && col.work >= bs->ks.maxiter) bcol_done(bs, col, 0, bs->ks.it + 1);
     }
 }
 
@@ -222,6 +245,33 @@ k_bt_dot(int n, const zdouble* __restrict__ a, const zdouble* __restrict__ b, BS
         for (int q = threadIdx.x; q < R; q += blockDim.x) bt_finish(bs, cols, f * R + q, tot[q], op);
 }
 
+// r = P(b - t) with t = A x, and ||r||^2 per column (refined form, between
+// cycles; every column is stopped, so no skip test)
+template <int R>
+__global__ void __launch_bounds__(kBlock)
+k_bt_resid(int n, const zdouble* __restrict__ b, const zdouble* __restrict__ t, zdouble* __restrict__ r,
+           const uint8_t* __restrict__ mask, BState* bs, BCol* cols, double2* partials, unsigned* tickets,
+           int gx_cap) {
+    __shared__ double2 tot[R];
+    const int f = blockIdx.y;
+    const size_t base = (size_t)f * n * R;
+    double2 part[R];
+#pragma unroll
+    for (int c = 0; c < R; ++c) part[c] = make_double2(0.0, 0.0);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const bool keep = !mask || mask[i];
+#pragma unroll
+        for (int c = 0; c < R; ++c) {
+            const size_t idx = base + (size_t)i * R + c;
+            const zdouble v = keep ? b[idx] - t[idx] : zdouble{0.0, 0.0};
+            r[idx] = v;
+            part[c].x += ST<zdouble>::norm2(v);
+        }
+    }
+    if (grid_reduce_cols<R>(part, partials + (size_t)f * gx_cap * R, tickets + f, tot))
+        for (int c = threadIdx.x; c < R; c += blockDim.x) bt_finish(bs, cols, f * R + c, tot[c], BT_TRUE);
+}
+
 // sol += alpha p ; r -= alpha q ; rt -= alpha qt (unless the step replaces
 // rt by M^{-1} r afterwards) ; ||r||^2 per live column
 template <int R, bool UPD_RT>
@@ -353,7 +403,7 @@ struct ssv_batch {
     std::vector<ssv_precond*> pre;
     bool has_fd = false;
     DevBuf<uint8_t> fd;
-    DevBuf<zdouble> x, r, rt, p, q, qt, t, io_b, io_x;
+    DevBuf<zdouble> x, r, rt, p, q, qt, t, bw, io_b, io_x;
     DevBuf<BState> bs;
     DevBuf<BCol> cols;
     DevBuf<double2> partials;
@@ -366,6 +416,9 @@ struct ssv_batch {
     // preconditioner is in the FP32 form, whose rounding makes M^{-1} not
     // exactly linear so the recurrence drifts from M^{-1} r)
     int replace_every = -1;
+    // refined form (defect correction, true-residual restarts): restart_drop
+    // > 0; 0 = the reference's recurrence alone
+    double restart_drop = 0.0;
     std::vector<ssv_batch_tune_entry> table;
     ssv::GraphLoop loop;
     // frequencies' preconditioner cycles run as parallel branches; frequencies
@@ -376,7 +429,7 @@ struct ssv_batch {
     // last solve
     double last_ms = 0.0, last_loop_ms = 0.0;
     int64_t last_launches = 0;
-    int last_loops = 0;
+    int last_loops = 0, last_cycles = 0;
 };
 
 namespace ssv {
@@ -649,7 +702,7 @@ ssv_batch* batch_create(ssv_matrix* K, ssv_matrix* M, int F, const double* omega
         }
         B->forks.ensure(B->branches);
         const size_t len = (size_t)F * B->n * R;
-        for (DevBuf<zdouble>* v : {&B->x, &B->r, &B->rt, &B->p, &B->q, &B->qt, &B->t}) v->alloc(len);
+        for (DevBuf<zdouble>* v : {&B->x, &B->r, &B->rt, &B->p, &B->q, &B->qt, &B->t, &B->bw}) v->alloc(len);
         B->bs.alloc(1);
         B->cols.alloc(B->C);
         B->gx_cap = sm_count() * 8;
@@ -669,6 +722,7 @@ ssv_batch* batch_create(ssv_matrix* K, ssv_matrix* M, int F, const double* omega
 void batch_destroy(ssv_batch* B) { delete B; }
 
 static int replace_period(const ssv_batch& B) {
+    if (B.restart_drop > 0.0) return 0;  // the refined cycles restart from the true residual instead
     if (B.replace_every >= 0) return B.replace_every;
     for (const ssv_precond* p : B.pre)
         if (p && ams_precision(p->ams.get()) == SSV_PREC_FP32) return 10;
@@ -683,6 +737,18 @@ static std::string batch_key(const ssv_batch& B) {
     return k;
 }
 
+static void bt_resid(ssv_batch& B, cudaStream_t s) {
+    dim3 grid(B.gx_elem, B.F);
+    const uint8_t* fdp = B.has_fd ? B.fd.get() : nullptr;
+    if (B.R == 1)
+        k_bt_resid<1><<<grid, kBlock, 0, s>>>(B.n, B.bw.get(), B.t.get(), B.r.get(), fdp, B.bs.get(), B.cols.get(),
+                                              B.partials.get(), B.tickets.get(), B.gx_cap);
+    else
+        k_bt_resid<4><<<grid, kBlock, 0, s>>>(B.n, B.bw.get(), B.t.get(), B.r.get(), fdp, B.bs.get(), B.cols.get(),
+                                              B.partials.get(), B.tickets.get(), B.gx_cap);
+    SSV_LAUNCH_CHECK();
+}
+
 void batch_cocr_solve_dev(ssv_batch* Bp, int maxiter, double tol, const void* d_b, void* d_x, int* iters,
                           int* conv, double* res) {
     ssv_batch& B = *Bp;
@@ -690,6 +756,7 @@ void batch_cocr_solve_dev(ssv_batch* Bp, int maxiter, double tol, const void* d_
         if (p && !p->ready) fail(SSV_ERR_RUNTIME, "batch: preconditioner is not set up (call Update())");
     cudaStream_t s = stream();
     KState* kst = &B.bs.get()->ks;
+    const bool refined = B.restart_drop > 0.0;
     // the iteration graph first (capture only), so the events below time device work alone
     const int period = replace_period(B);
     build_graph_loop(B.loop, batch_key(B), [&](cudaGraphConditionalHandle hc, int use_cond) {
@@ -716,7 +783,9 @@ void batch_cocr_solve_dev(ssv_batch* Bp, int maxiter, double tol, const void* d_
     h.ncols = B.C;
     h.ks.tol = tol;
     h.ks.maxiter = maxiter;
-    h.ks.max_loops = std::max(maxiter, 0) + 4;
+    h.ks.max_loops = loop_guard(maxiter);
+    h.drop = refined ? B.restart_drop : 0.0;
+    h.refined = refined ? 1 : 0;
     if (maxiter <= 0) {
         h.ks.done = 1;
         h.ndone = B.C;
@@ -733,17 +802,70 @@ void batch_cocr_solve_dev(ssv_batch* Bp, int maxiter, double tol, const void* d_
     if (B.R == 1) k_bt_gather<1><<<ge, kBlock, 0, s>>>(B.n, B.F, ub, B.r.get(), fdp);
     else k_bt_gather<4><<<ge, kBlock, 0, s>>>(B.n, B.F, ub, B.r.get(), fdp);
     SSV_LAUNCH_CHECK();
+    if (refined) SSV_CUDA(cudaMemcpyAsync(B.bw.get(), B.r.get(), sizeof(zdouble) * len, cudaMemcpyDeviceToDevice, s));
     bt_dot(B, B.r.get(), B.r.get(), BT_NORM0, true, s);
-    // rt = M^{-1} r ; p = rt ; q = A p ; rho = rt^T q
-    bt_precond(B, B.r.get(), B.rt.get(), kst, s);
-    SSV_CUDA(cudaMemcpyAsync(B.p.get(), B.rt.get(), sizeof(zdouble) * len, cudaMemcpyDeviceToDevice, s));
-    spmm(B, B.p.get(), B.q.get(), BT_RHO_INIT, s);
-    nk += 4;
-    SSV_CUDA(cudaEventRecord(e1, s));
-    if (maxiter > 0) run_graph_loop(B.loop, kst, maxiter);
-    SSV_CUDA(cudaMemcpyAsync(&h, B.bs.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
     std::vector<BCol> hc(B.C);
-    SSV_CUDA(cudaMemcpyAsync(hc.data(), B.cols.get(), sizeof(BCol) * B.C, cudaMemcpyDeviceToHost, s));
+    std::vector<char> fin(B.C, 0);
+    std::vector<int> work_prev(B.C, 0);
+    int cycles = 0, loops = 0;
+    while (true) {
+        // rt = M^{-1} r ; p = rt ; q = A p ; rho = rt^T q (live columns)
+        bt_precond(B, B.r.get(), B.rt.get(), kst, s);
+        SSV_CUDA(cudaMemcpyAsync(B.p.get(), B.rt.get(), sizeof(zdouble) * len, cudaMemcpyDeviceToDevice, s));
+        spmm(B, B.p.get(), B.q.get(), BT_RHO_INIT, s);
+        nk += 4;
+        if (cycles == 0) SSV_CUDA(cudaEventRecord(e1, s));
+        if (maxiter > 0) run_graph_loop(B.loop, kst, maxiter);
+        SSV_CUDA(cudaMemcpyAsync(&h, B.bs.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+        SSV_CUDA(cudaStreamSynchronize(s));
+        if (h.ks.status == SSV_ERR_TIMEOUT) fail(SSV_ERR_TIMEOUT, "batched COCR loop guard fired");
+        ++cycles;
+        loops += h.ks.loops;
+        if (!refined) {
+            SSV_CUDA(cudaMemcpyAsync(hc.data(), B.cols.get(), sizeof(BCol) * B.C, cudaMemcpyDeviceToHost, s));
+            break;
+        }
+        // FP64 true residuals of every column: t = A x, r = P(b - t)
+        h.ks.done = 0;  // lets the SpMM run; nothing is live while the host decides
+        SSV_CUDA(cudaMemcpyAsync(B.bs.get(), &h, sizeof(h), cudaMemcpyHostToDevice, s));
+        spmm(B, B.x.get(), B.t.get(), BT_TIME, s);
+        bt_resid(B, s);
+        nk += 2;
+        SSV_CUDA(cudaMemcpyAsync(hc.data(), B.cols.get(), sizeof(BCol) * B.C, cudaMemcpyDeviceToHost, s));
+        SSV_CUDA(cudaStreamSynchronize(s));
+        int restart = 0, ndone = 0;
+        for (int c = 0; c < B.C; ++c) {
+            BCol& col = hc[c];
+            if (!fin[c]) {
+                const double tr = col.normalizer > 0 ? col.tres / col.normalizer : 0.0;
+                if (col.normalizer < 1e-30 || tr <= tol) {
+                    fin[c] = 1;
+                    col.converged = 1;
+                } else if (col.work >= maxiter || col.work == work_prev[c] || col.tres < 1e-300) {
+                    fin[c] = 1;  // out of iterations, or a cycle that could not take a step
+                    col.converged = 0;
+                } else {  // another cycle from the true residual
+                    const double sc = col.tres / col.normalizer;
+                    col.done = 0;
+                    col.converged = 0;
+                    col.restart_abs = B.restart_drop * col.tres;
+                    col.brk_thr = 1e-30 * sc * sc;
+                    ++restart;
+                }
+                col.iters = col.work;
+                col.res = tr;
+                work_prev[c] = col.work;
+            }
+            ndone += fin[c] ? 1 : 0;
+        }
+        if (!restart) break;
+        h.ks.done = 0;
+        h.ks.it = 0;
+        h.ks.loops = 0;
+        h.ndone = ndone;
+        SSV_CUDA(cudaMemcpyAsync(B.cols.get(), hc.data(), sizeof(BCol) * B.C, cudaMemcpyHostToDevice, s));
+        SSV_CUDA(cudaMemcpyAsync(B.bs.get(), &h, sizeof(h), cudaMemcpyHostToDevice, s));
+    }
     zdouble* ux = static_cast<zdouble*>(d_x);
     if (B.R == 1) k_bt_scatter<1><<<ge, kBlock, 0, s>>>(B.n, B.F, B.x.get(), ux);
     else k_bt_scatter<4><<<ge, kBlock, 0, s>>>(B.n, B.F, B.x.get(), ux);
@@ -756,16 +878,19 @@ void batch_cocr_solve_dev(ssv_batch* Bp, int maxiter, double tol, const void* d_
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaEventDestroy(e2);
-    if (h.ks.status == SSV_ERR_TIMEOUT) fail(SSV_ERR_TIMEOUT, "batched COCR loop guard fired");
     for (int c = 0; c < B.C; ++c) {
         if (iters) iters[c] = hc[c].iters;
         if (conv) conv[c] = hc[c].converged;
-        if (res) res[c] = hc[c].normalizer > 0 ? hc[c].res / hc[c].normalizer : 0.0;
+        if (res) {
+            if (refined) res[c] = hc[c].res;
+            else res[c] = hc[c].normalizer > 0 ? hc[c].res / hc[c].normalizer : 0.0;
+        }
     }
     B.last_ms = ms_all;
     B.last_loop_ms = ms_loop;
-    B.last_loops = h.ks.loops;
-    B.last_launches = nk + 2 + (int64_t)B.loop.body_nodes * h.ks.loops / std::max(period, 1);
+    B.last_loops = loops;
+    B.last_cycles = cycles;
+    B.last_launches = nk + 2 + (int64_t)B.loop.body_nodes * loops / std::max(period, 1);
 }
 
 void batch_cocr_solve_host(ssv_batch* B, int maxiter, double tol, const void* b, void* x, int* iters, int* conv,
@@ -788,7 +913,15 @@ int batch_tuning(const ssv_batch* B, ssv_batch_tune_entry* e, int cap, int* chos
 
 void batch_set_replacement(ssv_batch* B, int every) { B->replace_every = every < 0 ? -1 : every; }
 
-void batch_last_timing(const ssv_batch* B, double* ms, double* loop_ms, int* loops, int64_t* launches) {
+void batch_set_refinement(ssv_batch* B, double restart_drop) {
+    if (!(restart_drop >= 0.0 && restart_drop < 1.0))
+        fail(SSV_ERR_INVALID_ARG, "batch: restart_drop must lie in [0, 1)");
+    B->restart_drop = restart_drop;
+}
+
+void batch_last_timing(const ssv_batch* B, double* ms, double* loop_ms, int* loops, int64_t* launches,
+                       int* cycles) {
+    if (cycles) *cycles = B->last_cycles;
     if (ms) *ms = B->last_ms;
     if (loop_ms) *loop_ms = B->last_loop_ms;
     if (loops) *loops = B->last_loops;

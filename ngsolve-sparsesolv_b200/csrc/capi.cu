@@ -83,6 +83,8 @@ void ssv_version(int* major, int* minor, int* patch) {
 
 const char* ssv_last_error(void) { return g_last_error.c_str(); }
 
+void ssv_set_loop_guard(int32_t max_loops) { ssv::set_loop_guard(max_loops); }
+
 int ssv_device_info(int* count, char* name, int name_cap) {
     return guarded([&] {
         int c = 0;
@@ -487,13 +489,29 @@ int ssv_batch_set_replacement(ssv_batch* b, int32_t every) {
     });
 }
 
+int ssv_batch_set_refinement(ssv_batch* b, double restart_drop) {
+    return guarded([&] {
+        if (!b) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_batch_set_refinement: NULL batch");
+        ssv::batch_set_refinement(b, restart_drop);
+    });
+}
+
 int ssv_batch_last_timing(const ssv_batch* b, double* device_ms, double* loop_ms, int32_t* loops,
                           int64_t* kernel_launches) {
     return guarded([&] {
         if (!b) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_batch_last_timing: NULL batch");
         int lp = 0;
-        ssv::batch_last_timing(b, device_ms, loop_ms, &lp, kernel_launches);
+        ssv::batch_last_timing(b, device_ms, loop_ms, &lp, kernel_launches, nullptr);
         if (loops) *loops = lp;
+    });
+}
+
+int ssv_batch_last_cycles(const ssv_batch* b, int32_t* cycles) {
+    return guarded([&] {
+        if (!b || !cycles) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_batch_last_cycles: NULL argument");
+        int c = 0;
+        ssv::batch_last_timing(b, nullptr, nullptr, nullptr, nullptr, &c);
+        *cycles = c;
     });
 }
 
@@ -672,6 +690,51 @@ int ssv_cocr_solve(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, int
         }
         SSV_CUDA(cudaMemcpyAsync(st.a.get(), b, bytes, cudaMemcpyHostToDevice, s));
         ssv::cocr_solve_dev(A, pre, dfd, maxiter, tol, printrates, st.a.get(), st.b.get(), iterations);
+        SSV_CUDA(cudaMemcpyAsync(x, st.b.get(), bytes, cudaMemcpyDeviceToHost, s));
+        SSV_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int ssv_cocr_last_launches(int64_t* launches) {
+    return guarded([&] {
+        if (!launches) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_cocr_last_launches: NULL argument");
+        *launches = ssv::cocr_last_launches();
+    });
+}
+
+int ssv_cocr_refined_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, int32_t maxiter,
+                               double tol, double restart_drop, int32_t printrates, const void* d_b,
+                               void* d_x, ssv_refine_info* info) {
+    return guarded([&] {
+        if (!A || !d_b || !d_x) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_cocr_refined_solve_dev: NULL argument");
+        require_device_ptr(d_b, "ssv_cocr_refined_solve_dev b");
+        require_device_ptr(d_x, "ssv_cocr_refined_solve_dev x");
+        require_device_ptr(freedofs, "ssv_cocr_refined_solve_dev freedofs");
+        ssv::cocr_refined_solve_dev(A, pre, freedofs, maxiter, tol, restart_drop, printrates, d_b, d_x, info);
+    });
+}
+
+int ssv_cocr_refined_solve(ssv_matrix* A, ssv_precond* pre, const uint8_t* freedofs, int32_t maxiter, double tol,
+                           double restart_drop, int32_t printrates, const void* b, void* x,
+                           ssv_refine_info* info) {
+    return guarded([&] {
+        if (!A || !b || !x) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_cocr_refined_solve: NULL argument");
+        cudaStream_t s = ssv::stream();
+        const int n = A->rows;
+        const size_t bytes = (size_t)n * scalar_bytes(A->dtype);
+        Stage& st = stage();
+        st.a.alloc(bytes / sizeof(double) + 1);
+        st.b.alloc(bytes / sizeof(double) + 1);
+        const uint8_t* dfd = nullptr;
+        if (freedofs) {
+            std::vector<uint8_t> h(freedofs, freedofs + n);
+            for (auto& v : h) v = v ? 1 : 0;
+            st.fd.upload(h.data(), h.size(), s);
+            dfd = st.fd.get();
+        }
+        SSV_CUDA(cudaMemcpyAsync(st.a.get(), b, bytes, cudaMemcpyHostToDevice, s));
+        ssv::cocr_refined_solve_dev(A, pre, dfd, maxiter, tol, restart_drop, printrates, st.a.get(), st.b.get(),
+                                    info);
         SSV_CUDA(cudaMemcpyAsync(x, st.b.get(), bytes, cudaMemcpyDeviceToHost, s));
         SSV_CUDA(cudaStreamSynchronize(s));
     });

@@ -19,13 +19,13 @@ enum NgsOp : int { NGS_MU = 100, NGS_RHO = 101 };
 
 template <typename S>
 __device__ inline void ngs_finish(double2 total, KState* st, int op) {
-    if (op == NGS_MU) {  // :323-327
+    if (op == NGS_MU) {  // :323-327 (brk_thr = 1e-30 in the reference's form)
         const S mu = s_from2<S>(total);
-        if (ST<S>::abs(mu) < 1e-30) { st->done = 1; st->iters = st->it; return; }
+        if (ST<S>::abs(mu) < st->brk_thr) { st->done = 1; st->iters = st->it; return; }
         st->alpha = s_to2<S>(ST<S>::div(s_from2<S>(st->rho), mu));
     } else if (op == NGS_RHO) {  // :354-359
         const S rho = s_from2<S>(st->rho);
-        if (ST<S>::abs(rho) < 1e-30) { st->done = 1; st->iters = st->it; return; }
+        if (ST<S>::abs(rho) < st->brk_thr) { st->done = 1; st->iters = st->it; return; }
         st->beta = s_to2<S>(ST<S>::div(s_from2<S>(total), rho));
         st->rho = total;
     }
@@ -100,6 +100,7 @@ k_ngs_update(int n, S* __restrict__ x, const S* __restrict__ p, const S* __restr
     if (grid_reduce2(part, red.partials, red.ticket, total)) {
         const double res = std::sqrt(std::fabs(total.x));
         st->norm_r = res;
+        st->updates++;
         if (st->save_hist) {
             if (st->hist_len < st->hist_cap) st->hist[st->hist_len] = res / st->normalizer;
             st->hist_len++;
@@ -107,6 +108,9 @@ k_ngs_update(int n, S* __restrict__ x, const S* __restrict__ p, const S* __restr
         if (res / st->normalizer <= st->tol) {  // :344-347
             st->done = 1;
             st->converged = 1;
+            st->iters = st->it + 1;
+        } else if (res <= st->restart_abs) {  // refined form: this cycle has done its part
+            st->done = 1;
             st->iters = st->it + 1;
         }
     }
@@ -158,9 +162,30 @@ static std::string pre_key(const ssv_precond* pre) {
     return k;
 }
 
+// One COCRSolverNGS solve (refine == nullptr), or the refined form: cycles of
+// that recurrence, each started from the FP64 true residual r = P(b - A x) of
+// the current x (rt = M^{-1} r, p = rt, q = P A p, rho = rt^T q) and ended when
+// its residual has dropped by `drop` from its start (or on tol, a breakdown,
+// maxiter); the solve stops once the true residual is <= tol. Continuing the
+// same x is defect correction: each cycle solves A d = r for the correction.
+// Restarting makes the recurrence consistent again with an M^{-1} that is
+// not exactly linear (an FP32-form preconditioner: rt -= alpha M^{-1} q then
+// drifts from M^{-1} r, which stalls the plain recurrence near the rounding
+// level of M^{-1}). The reference's absolute breakdown tests (|mu|, |rho| <
+// 1e-30) are scaled by (||r_start|| / ||b||)^2 in later cycles: mu and rho
+// scale with the square of the residual the cycle starts from.
+struct RefineOpt {
+    double drop;
+};
+
+// kernels launched by the last COCR solve of this thread (measurement hook)
+thread_local int64_t g_cocr_launches = 0;
+int64_t cocr_last_launches() { return g_cocr_launches; }
+
 template <typename S>
 static void run_cocr_ngs(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, int maxiter, double tol,
-                         int printrates, const S* d_b, S* d_x, int* iterations) {
+                         int printrates, const S* d_b, S* d_x, int* iterations, const RefineOpt* refine,
+                         ssv_refine_info* info) {
     cudaStream_t s = stream();
     const int n = A->rows;
     auto& ctx_ptr = cocr_table()[A];
@@ -174,6 +199,8 @@ static void run_cocr_ngs(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, int
     const S* v = reinterpret_cast<const S*>(A->val.get());
     S *x = d_x, *r = w.r.get(), *rt = w.z.get(), *p = w.p.get(), *q = w.Ap.get(), *qt = w.qt.get(),
       *t = w.t.get();
+    if (info) std::memset(info, 0, sizeof(*info));
+    g_cocr_launches = 2;
     // sol = 0 ; r = rhs projected ; ||rhs|| (:274-299)
     SSV_CUDA(cudaMemsetAsync(x, 0, sizeof(S) * n, s));
     launch_k(k_gather_perm<S>, g, kBlock, s, n, nullptr, d_b, r, fd, 1);
@@ -183,64 +210,118 @@ static void run_cocr_ngs(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, int
     SSV_CUDA(cudaMemcpyAsync(&nb, w.scal.get(), sizeof(nb), cudaMemcpyDeviceToHost, s));
     SSV_CUDA(cudaStreamSynchronize(s));
     const double rhs_norm = std::sqrt(std::fabs(nb.x));
-    if (rhs_norm < 1e-30) { *iterations = 0; return; }
-    // rt = M^{-1} r ; p = rt ; q = A p projected ; rho = rt^T q
-    KState* dst = w.st.get();
-    apply_pre<S>(pre, r, rt, nullptr, n, s);
-    launch_k(k_copy<S>, g, kBlock, s, n, rt, p);
-    launch_spmv<S, S, 0>(A->lanes, n, A->rp.get(), A->ci.get(), v, p, q, nullptr, fd, nullptr, RED_STORE, red,
-                         nullptr, s);
-    SSV_LAUNCH_CHECK();
-    KState h;
-    std::memset(&h, 0, sizeof(h));
-    h.normalizer = rhs_norm;
-    h.tol = tol;
-    h.maxiter = maxiter;
-    h.save_hist = printrates ? 1 : 0;
-    h.hist_cap = dev_hist;
-    h.hist = w.hist.get();
-    h.max_loops = std::max(maxiter, 0) + 4;
-    if (maxiter <= 0) { h.done = 1; h.iters = 0; }
-    {
-        // state first, then rho = rt^T q into it
-        SSV_CUDA(cudaMemcpyAsync(dst, &h, sizeof(h), cudaMemcpyHostToDevice, s));
-        launch_k(k_dot<S>, g, kBlock, s, n, rt, q, 0, nullptr, RED_STORE, red, &dst->rho);
-        SSV_LAUNCH_CHECK();
+    if (rhs_norm < 1e-30) {
+        *iterations = 0;
+        if (info) info->converged = 1;
+        return;
     }
+    KState* dst = w.st.get();
     std::string key = "ngs;" + std::to_string(n) + ";" + std::to_string((size_t)pre) + ";" +
                       std::to_string((size_t)fd) + ";" + std::to_string((size_t)x) + ";" +
                       std::to_string((size_t)dst) + ";" + std::to_string(A->lanes) + ";" +
                       std::to_string((size_t)red.partials);
     key += ";" + pre_key(pre);
-    build_graph_loop(ctx.loop, key, [&](cudaGraphConditionalHandle hc, int use_cond) {
-        apply_pre<S>(pre, q, qt, dst, n, s);
-        launch_k(k_ngs_dot<S>, g, kBlock, s, n, qt, q, dst, NGS_MU, red);
-        launch_k(k_ngs_update<S>, g, kBlock, s, n, x, p, q, qt, r, rt, dst, red);
-        {
-            const int L = A->lanes & 0xff;
-            const int rpb = kBlock / L;
-            int gg = std::max(1, std::min((n + rpb - 1) / rpb, sm_count() * 8));
-            switch (L) {
-                case 2: launch_k(k_ngs_spmv_dot<S, 2>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
-                case 4: launch_k(k_ngs_spmv_dot<S, 4>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
-                case 8: launch_k(k_ngs_spmv_dot<S, 8>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
-                case 16: launch_k(k_ngs_spmv_dot<S, 16>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
-                default: launch_k(k_ngs_spmv_dot<S, 32>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red);
+    // the iteration graph; captured after the first preconditioner application, which
+    // allocates and tunes on first use
+    auto build = [&] {
+        build_graph_loop(ctx.loop, key, [&](cudaGraphConditionalHandle hc, int use_cond) {
+            apply_pre<S>(pre, q, qt, dst, n, s);
+            launch_k(k_ngs_dot<S>, g, kBlock, s, n, qt, q, dst, NGS_MU, red);
+            launch_k(k_ngs_update<S>, g, kBlock, s, n, x, p, q, qt, r, rt, dst, red);
+            {
+                const int L = A->lanes & 0xff;
+                const int rpb = kBlock / L;
+                int gg = std::max(1, std::min((n + rpb - 1) / rpb, sm_count() * 8));
+                switch (L) {
+                    case 2: launch_k(k_ngs_spmv_dot<S, 2>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
+                    case 4: launch_k(k_ngs_spmv_dot<S, 4>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
+                    case 8: launch_k(k_ngs_spmv_dot<S, 8>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
+                    case 16: launch_k(k_ngs_spmv_dot<S, 16>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red); break;
+                    default: launch_k(k_ngs_spmv_dot<S, 32>, gg, kBlock, s, n, A->rp.get(), A->ci.get(), v, rt, t, fd, dst, red);
+                }
             }
-        }
-        launch_k(k_cocr_pq<S>, g, kBlock, s, n, rt, t, p, q, dst);
-        k_ngs_loop_ctl<<<1, 32, 0, s>>>(dst, hc, use_cond);
+            launch_k(k_cocr_pq<S>, g, kBlock, s, n, rt, t, p, q, dst);
+            k_ngs_loop_ctl<<<1, 32, 0, s>>>(dst, hc, use_cond);
+            SSV_LAUNCH_CHECK();
+        });
+    };
+    std::vector<double> hs;  // printrates: the residual history over every cycle
+    int used = 0, cycles = 0;
+    double rs = rhs_norm;  // norm of the residual the cycle starts from
+    double true_rel = 1.0;
+    bool conv = false;
+    KState h;
+    while (true) {
+        // rt = M^{-1} r ; p = rt ; q = A p projected ; rho = rt^T q
+        apply_pre<S>(pre, r, rt, nullptr, n, s);
+        launch_k(k_copy<S>, g, kBlock, s, n, rt, p);
+        launch_spmv<S, S, 0>(A->lanes, n, A->rp.get(), A->ci.get(), v, p, q, nullptr, fd, nullptr, RED_STORE, red,
+                             nullptr, s);
         SSV_LAUNCH_CHECK();
-    });
-    if (maxiter > 0) run_graph_loop(ctx.loop, dst, maxiter);
-    SSV_CUDA(cudaMemcpyAsync(&h, dst, sizeof(h), cudaMemcpyDeviceToHost, s));
-    SSV_CUDA(cudaStreamSynchronize(s));
-    if (h.status == SSV_ERR_TIMEOUT) fail(SSV_ERR_TIMEOUT, "COCR loop guard fired");
-    *iterations = h.iters;
+        const int left = maxiter - used;
+        std::memset(&h, 0, sizeof(h));
+        h.normalizer = rhs_norm;
+        h.tol = tol;
+        h.maxiter = left;
+        h.save_hist = printrates ? 1 : 0;
+        h.hist_cap = dev_hist;
+        h.hist = w.hist.get();
+        h.max_loops = loop_guard(left);
+        h.brk_thr = 1e-30 * (rs / rhs_norm) * (rs / rhs_norm);
+        h.restart_abs = refine ? refine->drop * rs : 0.0;
+        if (left <= 0) { h.done = 1; h.iters = 0; }
+        // state first, then rho = rt^T q into it
+        SSV_CUDA(cudaMemcpyAsync(dst, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+        launch_k(k_dot<S>, g, kBlock, s, n, rt, q, 0, nullptr, RED_STORE, red, &dst->rho);
+        SSV_LAUNCH_CHECK();
+        if (cycles == 0) build();
+        if (left > 0) run_graph_loop(ctx.loop, dst, left);
+        SSV_CUDA(cudaMemcpyAsync(&h, dst, sizeof(h), cudaMemcpyDeviceToHost, s));
+        SSV_CUDA(cudaStreamSynchronize(s));
+        if (h.status == SSV_ERR_TIMEOUT) fail(SSV_ERR_TIMEOUT, "COCR loop guard fired");
+        ++cycles;
+        g_cocr_launches += 4 + (pre ? 0 : 1) + (int64_t)ctx.loop.body_nodes * h.loops;
+        if (printrates && h.hist_len > 0) {
+            const size_t k0 = hs.size();
+            hs.resize(k0 + std::min(h.hist_len, dev_hist));
+            SSV_CUDA(cudaMemcpy(hs.data() + k0, w.hist.get(), sizeof(double) * (hs.size() - k0),
+                                cudaMemcpyDeviceToHost));
+        }
+        if (!refine) {
+            *iterations = h.iters;
+            break;
+        }
+        used += h.updates;
+        // FP64 true residual of the current x: r = P(b - A x) (t, free between cycles, holds P b)
+        launch_k(k_gather_perm<S>, g, kBlock, s, n, nullptr, d_b, t, fd, 1);
+        launch_spmv<S, S, 2>(A->lanes, n, A->rp.get(), A->ci.get(), v, x, r, t, fd, nullptr, RED_STORE, red,
+                             nullptr, s);
+        launch_k(k_norm2<S>, g, kBlock, s, n, r, red, w.scal.get());
+        SSV_LAUNCH_CHECK();
+        g_cocr_launches += 3;
+        double2 nr;
+        SSV_CUDA(cudaMemcpyAsync(&nr, w.scal.get(), sizeof(nr), cudaMemcpyDeviceToHost, s));
+        SSV_CUDA(cudaStreamSynchronize(s));
+        rs = std::sqrt(std::fabs(nr.x));
+        true_rel = rs / rhs_norm;
+        if (printrates) {
+            std::printf("COCR cycle %d: %d iterations, true residual = %g\n", cycles, h.updates, true_rel);
+            std::fflush(stdout);
+        }
+        if (true_rel <= tol) { conv = true; break; }
+        // out of iterations, or a cycle that could not take a single step
+        if (used >= maxiter || h.updates == 0 || rs < 1e-300) break;
+    }
+    if (refine) {
+        *iterations = used;
+        if (info) {
+            info->iterations = used;
+            info->cycles = cycles;
+            info->converged = conv ? 1 : 0;
+            info->true_residual = true_rel;
+        }
+    }
     if (printrates) {
-        std::vector<double> hs(std::min(h.hist_len, dev_hist));
-        if (!hs.empty())
-            SSV_CUDA(cudaMemcpy(hs.data(), w.hist.get(), sizeof(double) * hs.size(), cudaMemcpyDeviceToHost));
         std::printf("COCR iter 0: res = 1\n");
         for (size_t k = 0; k < hs.size(); ++k) std::printf("COCR iter %zu: res = %g\n", k + 1, hs[k]);
         std::fflush(stdout);
@@ -310,7 +391,7 @@ static void run_pcg(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, const ss
     h.conj = cfg.conjugate;
     h.hist_cap = dev_hist;
     h.hist = w.hist.get();
-    h.max_loops = std::max(cfg.max_iterations, 0) + 4;
+    h.max_loops = loop_guard(cfg.max_iterations);
     if (cfg.save_residual_history) {
         const double h0 = r0 / normalizer;
         SSV_CUDA(cudaMemcpyAsync(w.hist.get(), &h0, sizeof(double), cudaMemcpyHostToDevice, s));
@@ -382,18 +463,35 @@ void pcg_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, const s
                          hist, hist_cap);
 }
 
-void cocr_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, int maxiter, double tol,
-                    int printrates, const void* d_b, void* d_x, int* iterations) {
+static void cocr_any(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, int maxiter, double tol,
+                     int printrates, const void* d_b, void* d_x, int* iterations, const RefineOpt* ro,
+                     ssv_refine_info* info) {
     if (pre && !pre->ready) fail(SSV_ERR_RUNTIME, "COCRSolver: preconditioner is not set up (call Update())");
     if (pre && pre->vdtype != A->dtype)
         fail(SSV_ERR_TYPE, "COCRSolver: preconditioner scalar type differs from the matrix");
     if (pre && pre->n != A->rows) fail(SSV_ERR_INVALID_ARG, "COCRSolver: preconditioner size differs from the matrix");
+    if (A->rows != A->cols) fail(SSV_ERR_INVALID_ARG, "COCRSolver: matrix must be square");
     if (A->dtype == SSV_F64)
         run_cocr_ngs<double>(A, pre, d_fd, maxiter, tol, printrates, static_cast<const double*>(d_b),
-                             static_cast<double*>(d_x), iterations);
+                             static_cast<double*>(d_x), iterations, ro, info);
     else
         run_cocr_ngs<zdouble>(A, pre, d_fd, maxiter, tol, printrates, static_cast<const zdouble*>(d_b),
-                              static_cast<zdouble*>(d_x), iterations);
+                              static_cast<zdouble*>(d_x), iterations, ro, info);
+}
+
+void cocr_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, int maxiter, double tol,
+                    int printrates, const void* d_b, void* d_x, int* iterations) {
+    cocr_any(A, pre, d_fd, maxiter, tol, printrates, d_b, d_x, iterations, nullptr, nullptr);
+}
+
+void cocr_refined_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, int maxiter, double tol,
+                            double restart_drop, int printrates, const void* d_b, void* d_x,
+                            ssv_refine_info* info) {
+    if (!(restart_drop > 0.0 && restart_drop < 1.0))
+        fail(SSV_ERR_INVALID_ARG, "refined COCR: restart_drop must lie in (0, 1)");
+    RefineOpt ro{restart_drop};
+    int its = 0;
+    cocr_any(A, pre, d_fd, maxiter, tol, printrates, d_b, d_x, &its, &ro, info);
 }
 
 }  // namespace ssv

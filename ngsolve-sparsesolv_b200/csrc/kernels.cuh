@@ -47,6 +47,12 @@ struct KState {
     double tol, abs_tol, div_threshold;
     int maxiter, div_check, div_count, save_best, save_hist, conj, hist_cap, max_loops;
     double* hist;      // device history buffer (hist_cap entries)
+    // COCR with an external preconditioner: breakdown threshold on |mu| and
+    // |rho| (the reference's 1e-30), and the residual norm at which a cycle
+    // of the refined (defect-correction) form ends (0 = never)
+    double brk_thr, restart_abs;
+    int updates;       // x updates performed in this cycle
+    int pad2_;
 };
 
 // Reduction epilogues run by the last block of a reduction kernel.

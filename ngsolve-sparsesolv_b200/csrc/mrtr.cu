@@ -354,7 +354,7 @@ void run_mrtr(ssv_solver* sv, const ssv_config& cfg, const S* d_b, S* d_x, ssv_r
     h.conj = cfg.conjugate;
     h.hist_cap = dev_hist;
     h.hist = w.hist.get();
-    h.max_loops = std::max(cfg.max_iterations, 0) + 4;
+    h.max_loops = loop_guard(cfg.max_iterations);
     h.rho = make_double2(1.0, 0.0);      // zeta_old
     h.rho_new = make_double2(1.0, 0.0);  // nu
     if (cfg.save_residual_history) {

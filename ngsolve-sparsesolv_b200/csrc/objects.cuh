@@ -163,6 +163,9 @@ void build_graph_loop(GraphLoop& g, const std::string& key_in, F&& body) {
 
 // Runs the loop until the device state reports done (bounded).
 void run_graph_loop(GraphLoop& g, KState* d_st, int max_iters);
+// Loop-body cap of a device-looped solve of maxiter iterations (see solver.cu).
+int loop_guard(int maxiter);
+void set_loop_guard(int loops);
 
 // ---------------------------------------------------------------------------
 // IC(0) preconditioner on the device (ic_preconditioner.hpp)

@@ -78,6 +78,14 @@ __global__ void k_loop_ctl(KState* st, cudaGraphConditionalHandle h, int use_con
     if (use_cond) cudaGraphSetConditional(h, st->done ? 0u : 1u);
 }
 
+// Cap on the executed loop bodies of every device-looped solve: maxiter + 4
+// (a loop that outruns its own iteration count means a stuck state), or the
+// process-wide override of ssv_set_loop_guard (> 0). A solve that reaches it
+// stops on the device and fails with SSV_ERR_TIMEOUT.
+static int g_loop_guard = 0;
+void set_loop_guard(int loops) { g_loop_guard = loops > 0 ? loops : 0; }
+int loop_guard(int maxiter) { return g_loop_guard > 0 ? g_loop_guard : std::max(maxiter, 0) + 4; }
+
 void run_graph_loop(GraphLoop& g, KState* d_st, int max_iters) {
     cudaStream_t s = stream();
     if (g.cond) {
@@ -918,7 +926,7 @@ static void run_krylov(ssv_solver* sv, int method, const ssv_config& cfg, const 
     h.conj = cfg.conjugate;
     h.hist_cap = dev_hist;
     h.hist = w.hist.get();
-    h.max_loops = std::max(cfg.max_iterations, 0) + 4;
+    h.max_loops = loop_guard(cfg.max_iterations);
     if (cfg.save_residual_history) {
         const double h0 = init_norm_r / normalizer;
         SSV_CUDA(cudaMemcpyAsync(w.hist.get(), &h0, sizeof(double), cudaMemcpyHostToDevice, s));

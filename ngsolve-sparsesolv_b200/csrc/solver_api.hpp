@@ -17,6 +17,10 @@ double precond_actual_shift(const ssv_precond* p);
 void matrix_spmv_dev(ssv_matrix* A, const void* d_x, void* d_y);
 void cocr_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, int maxiter, double tol,
                     int printrates, const void* d_b, void* d_x, int* iterations);
+void cocr_refined_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, int maxiter, double tol,
+                            double restart_drop, int printrates, const void* d_b, void* d_x,
+                            ssv_refine_info* info);
+int64_t cocr_last_launches();
 void gmres_solve_dev(ssv_matrix* A, ssv_precond* pre, const uint8_t* d_fd, int maxiter, double tol, int restart,
                      const void* d_b, void* d_x, int* iterations);
 void mrtr_forget(const ssv_solver* s);
@@ -75,8 +79,10 @@ void batch_cocr_solve_dev(ssv_batch* B, int maxiter, double tol, const void* d_b
 void batch_cocr_solve_host(ssv_batch* B, int maxiter, double tol, const void* b, void* x, int* iters, int* conv,
                            double* res);
 int batch_tuning(const ssv_batch* B, ssv_batch_tune_entry* e, int cap, int* chosen);
-void batch_last_timing(const ssv_batch* B, double* ms, double* loop_ms, int* loops, int64_t* launches);
+void batch_last_timing(const ssv_batch* B, double* ms, double* loop_ms, int* loops, int64_t* launches,
+                       int* cycles);
 void batch_set_replacement(ssv_batch* B, int every);
+void batch_set_refinement(ssv_batch* B, double restart_drop);
 
 // Learned initial-guess MLP (mlp.cu)
 ssv_mlp* mlp_create(int D, int H, uint64_t seed);

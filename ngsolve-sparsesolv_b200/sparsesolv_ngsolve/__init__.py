@@ -24,6 +24,7 @@ __all__ = [
     "SparseSolvResult", "SparseSolvSolver", "SparseSolvSolverD", "SparseSolvSolverC",
     "ICPreconditioner", "ICPreconditionerD", "ICPreconditionerC",
     "COCRSolver", "COCRSolverD", "COCRSolverC", "has_compact_ams",
+    "MixedCOCRSolver", "MixedCOCRSolverD", "MixedCOCRSolverC",
     "CompactAMSPreconditioner", "CompactAMSPreconditionerImpl",
     "ComplexCompactAMSPreconditioner", "ComplexCompactAMSPreconditionerImpl", "PCGSolver",
     "BatchedCOCRSolver", "SGSPreconditioner", "SGSPreconditionerD", "SGSPreconditionerC",
@@ -69,6 +70,13 @@ def _freedofs_array(freedofs, n):
     if fd.shape[0] != n:
         raise ValueError(f"freedofs has {fd.shape[0]} entries, matrix has {n} rows")
     return np.ascontiguousarray(fd)
+
+
+def _note_applies(pre, count):
+    """Tells a preconditioner how many times a solve applied it (print_level diagnostics)."""
+    f = getattr(pre, "_note_applies", None)
+    if f is not None and count > 0:
+        f(int(count))
 
 
 def _vec_view(v):
@@ -537,6 +545,7 @@ class _COCRSolverBase:
                                        1 if self.printrates else 0, _capi.vptr(b), _capi.vptr(x),
                                        ctypes.byref(it)))
         self._iterations = it.value
+        _note_applies(self._pre, it.value + 1)
         sv[...] = x
 
     def __mul__(self, vec):
@@ -609,6 +618,69 @@ def COCRSolver(mat, pre, freedofs=None, maxiter=500, tol=1e-8, printrates=False)
     m = mat if isinstance(mat, _Matrix) else _Matrix(mat)
     cls = COCRSolverC if m.cplx else COCRSolverD
     return cls(m, pre, freedofs, maxiter, tol, printrates)
+
+
+class _MixedCOCRSolverBase(_COCRSolverBase):
+    def __init__(self, mat, pre, freedofs=None, maxiter=500, tol=1e-8, restart_drop=1e-5, printrates=False):
+        super().__init__(mat, pre, freedofs, maxiter, tol, printrates)
+        self.restart_drop = float(restart_drop)
+        self._info = _capi.ssv_refine_info()
+
+    @property
+    def cycles(self):
+        return self._info.cycles
+
+    @property
+    def converged(self):
+        return bool(self._info.converged)
+
+    @property
+    def true_residual(self):
+        return self._info.true_residual
+
+    def Mult(self, rhs, sol):
+        b = np.ascontiguousarray(_vec_view(rhs), dtype=self._mat.dtype)
+        sv = _vec_view(sol)
+        x = np.zeros(self._mat.n, dtype=self._mat.dtype)
+        pre_h = None if self._pre is None else self._pre._h
+        self._mat.refresh()
+        check(self._lib.ssv_cocr_refined_solve(self._mat.h, pre_h, _capi.u8ptr(self._fd), self.maxiter, self.tol,
+                                               self.restart_drop, 1 if self.printrates else 0, _capi.vptr(b),
+                                               _capi.vptr(x), ctypes.byref(self._info)))
+        self._iterations = self._info.iterations
+        _note_applies(self._pre, self._info.iterations + self._info.cycles)
+        sv[...] = x
+
+    def solve_dev(self, d_b, d_x, d_freedofs=None):
+        """Device-pointer form (integers: addresses of n-vectors in HBM; d_freedofs a uint8 mask or None)."""
+        pre_h = None if self._pre is None else self._pre._h
+        check(self._lib.ssv_cocr_refined_solve_dev(self._mat.h, pre_h, ctypes.cast(d_freedofs or 0, _capi.PU8),
+                                                   self.maxiter, self.tol, self.restart_drop,
+                                                   1 if self.printrates else 0, ctypes.c_void_p(d_b),
+                                                   ctypes.c_void_p(d_x), ctypes.byref(self._info)))
+        self._iterations = self._info.iterations
+
+
+class MixedCOCRSolverD(_MixedCOCRSolverBase):
+    _cplx = False
+
+
+class MixedCOCRSolverC(_MixedCOCRSolverBase):
+    _cplx = True
+
+
+def MixedCOCRSolver(mat, pre, freedofs=None, maxiter=500, tol=1e-8, restart_drop=1e-5, printrates=False):
+    """COCR with FP64 defect correction (new: no reference counterpart): the
+    Krylov driver of the mixed-precision form. Cycles of the COCRSolver
+    recurrence, each restarted from the FP64 true residual once its residual
+    has dropped by ``restart_drop``; it stops when the true relative residual
+    is <= tol. Use it with a preconditioner in the FP32 form
+    (``precision="fp32"``), which the plain COCR recurrence cannot drive to
+    1e-10. ``.iterations`` (over all cycles), ``.cycles``, ``.converged``,
+    ``.true_residual``."""
+    m = mat if isinstance(mat, _Matrix) else _Matrix(mat)
+    cls = MixedCOCRSolverC if m.cplx else MixedCOCRSolverD
+    return cls(m, pre, freedofs, maxiter, tol, restart_drop, printrates)
 
 
 def has_compact_ams():
@@ -822,11 +894,15 @@ class BatchedCOCRSolver:
     (F, nrhs) arrays with the COCRSolver meaning per column. The SpMM launch
     shape is autotuned at construction (``tuning``). ``residual_replacement``:
     every k-th step recomputes the preconditioned residual (None = automatic,
-    k = 10 with FP32 preconditioners; 0 = never).
+    k = 10 with FP32 preconditioners; 0 = never). ``restart_drop`` (new, the
+    mixed-precision form's driver): each column runs cycles restarted from its
+    FP64 true residual once its residual has dropped by this factor, and is
+    done when its true relative residual is <= tol (``residuals`` then hold
+    true residuals); None keeps the plain recurrence.
     """
 
     def __init__(self, K, M, omegas, pres, nrhs=1, freedofs=None, maxiter=500, tol=1e-8,
-                 residual_replacement=None):
+                 residual_replacement=None, restart_drop=None):
         self._K = K if isinstance(K, _Matrix) else _Matrix(K)
         self._M = M if isinstance(M, _Matrix) else _Matrix(M)
         if self._K.cplx or self._M.cplx:
@@ -851,6 +927,9 @@ class BatchedCOCRSolver:
         self._h = h
         if residual_replacement is not None:
             check(self._lib.ssv_batch_set_replacement(self._h, int(residual_replacement)))
+        self.restart_drop = None if restart_drop is None else float(restart_drop)
+        if self.restart_drop:
+            check(self._lib.ssv_batch_set_refinement(self._h, self.restart_drop))
         shape = (self.F, self.nrhs)
         self.iterations = np.zeros(shape, np.int32)
         self.converged = np.zeros(shape, np.int32)
@@ -899,4 +978,7 @@ class BatchedCOCRSolver:
         loops, nk = ctypes.c_int32(), ctypes.c_int64()
         check(self._lib.ssv_batch_last_timing(self._h, ctypes.byref(ms), ctypes.byref(lms), ctypes.byref(loops),
                                               ctypes.byref(nk)))
-        return {"device_ms": ms.value, "loop_ms": lms.value, "loops": loops.value, "kernel_launches": nk.value}
+        cyc = ctypes.c_int32()
+        check(self._lib.ssv_batch_last_cycles(self._h, ctypes.byref(cyc)))
+        return {"device_ms": ms.value, "loop_ms": lms.value, "loops": loops.value, "kernel_launches": nk.value,
+                "cycles": cyc.value}

@@ -89,6 +89,16 @@ class ssv_batch_tune_entry(ctypes.Structure):
     ]
 
 
+class ssv_refine_info(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int32),
+        ("cycles", ctypes.c_int32),
+        ("converged", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
+        ("true_residual", ctypes.c_double),
+    ]
+
+
 SSV_MAX_PHASES = 8
 
 
@@ -187,6 +197,12 @@ SIGNATURES = [
     ("ssv_precond_destroy", I32, [P]),
     ("ssv_cocr_solve", I32, [P, P, PU8, I32, ctypes.c_double, I32, P, P, PI32]),
     ("ssv_cocr_solve_dev", I32, [P, P, PU8, I32, ctypes.c_double, I32, P, P, PI32]),
+    ("ssv_cocr_refined_solve", I32, [P, P, PU8, I32, ctypes.c_double, ctypes.c_double, I32, P, P,
+                                     ctypes.POINTER(ssv_refine_info)]),
+    ("ssv_cocr_refined_solve_dev", I32, [P, P, PU8, I32, ctypes.c_double, ctypes.c_double, I32, P, P,
+                                         ctypes.POINTER(ssv_refine_info)]),
+    ("ssv_set_loop_guard", None, [I32]),
+    ("ssv_cocr_last_launches", I32, [ctypes.POINTER(ctypes.c_int64)]),
     ("ssv_gmres_solve", I32, [P, P, PU8, I32, ctypes.c_double, I32, P, P, PI32]),
     ("ssv_gmres_solve_dev", I32, [P, P, PU8, I32, ctypes.c_double, I32, P, P, PI32]),
     ("ssv_abmc_build", I32, [I32, PI32, PI32, I32, I32, PI32, PI32, PI32, PI32, PI32, PI32]),
@@ -203,6 +219,8 @@ SIGNATURES = [
     ("ssv_batch_cocr_solve_dev", I32, [P, I32, ctypes.c_double, P, P, PI32, PI32, PD]),
     ("ssv_batch_tuning", I32, [P, ctypes.POINTER(ssv_batch_tune_entry), I32, PI32, PI32]),
     ("ssv_batch_set_replacement", I32, [P, I32]),
+    ("ssv_batch_set_refinement", I32, [P, ctypes.c_double]),
+    ("ssv_batch_last_cycles", I32, [P, PI32]),
     ("ssv_batch_last_timing", I32, [P, PD, PD, PI32, ctypes.POINTER(ctypes.c_int64)]),
     ("ssv_ams_get_precision", I32, [P, PI32]),
     ("ssv_ams_profile", I32, [P, I32, I32, I32, ctypes.POINTER(ssv_phase_profile)]),

@@ -390,3 +390,68 @@ def cocr_solve(A, b, precond=None, freedofs=None, maxiter=500, tol=1e-8):
     if rc != 0:
         raise RuntimeError("oracle cocr failed")
     return x, it.value
+
+
+def refined_cocr(A, f, precond, freedofs=None, maxiter=500, tol=1e-10, restart_drop=1e-5):
+    """FP64 defect correction around COCRSolverNGS::Mult
+    (ngsolve/sparsesolv_solvers.hpp:273-369), the mixed-precision form's
+    driver (new: the reference has no counterpart). Cycles of the COCR
+    recurrence, each started from the true residual r = P(b - A x) of the
+    current x (rt = M^{-1} r, p = rt, q = P A p, rho = rt^T q) and ended when
+    its residual ||r|| has dropped to restart_drop times the residual it
+    started from, or is <= tol ||P b||, or on a breakdown (|mu|, |rho| below
+    1e-30 (||r_start|| / ||P b||)^2), or out of iterations; the solve ends
+    when the true relative residual is <= tol. precond: y = M^{-1} x.
+    Returns (x, iterations over all cycles, cycles, true relative residual).
+    Plain numpy loops over whole vectors: for the small systems of the tests."""
+    fd = None if freedofs is None else np.asarray(freedofs).astype(bool)
+
+    def proj(v):
+        if fd is not None:
+            v[~fd] = 0
+        return v
+
+    n = A.shape[0]
+    x = np.zeros(n, dtype=np.result_type(A.dtype, f.dtype))
+    r = proj(np.array(f, dtype=x.dtype))
+    nb = float(np.linalg.norm(r))
+    if nb < 1e-30:
+        return x, 0, 0, 0.0
+    used, cycles, rs = 0, 0, nb
+    tr = 1.0
+    while True:
+        thr = 1e-30 * (rs / nb) ** 2
+        stop = restart_drop * rs
+        rt = precond(r.copy())
+        p = rt.copy()
+        q = proj(A @ p)
+        rho = rt @ q
+        steps = 0
+        while used + steps < maxiter:
+            qt = precond(q.copy())
+            mu = qt @ q
+            if abs(mu) < thr:
+                break
+            alpha = rho / mu
+            x += alpha * p
+            r -= alpha * q
+            rt -= alpha * qt
+            steps += 1
+            res = float(np.linalg.norm(r))
+            if res / nb <= tol or res <= stop:
+                break
+            t = proj(A @ rt)
+            rho_new = rt @ t
+            if abs(rho) < thr:
+                break
+            beta = rho_new / rho
+            rho = rho_new
+            p = rt + beta * p
+            q = t + beta * q
+        used += steps
+        cycles += 1
+        r = proj(np.array(f, dtype=x.dtype) - A @ x)
+        rs = float(np.linalg.norm(r))
+        tr = rs / nb
+        if tr <= tol or used >= maxiter or steps == 0 or rs < 1e-300:
+            return x, used, cycles, tr
