@@ -430,8 +430,12 @@ int ssv_mlp_predict_dev(ssv_mlp* m, const float* d_X, int64_t n, float* d_out);
  * array inside the library, held by every GPU that loads it until exit.
  * Limit: rows <= 2,097,152 (larger sizes fail with SSV_ERR_INVALID_ARG).
  * The first call on a device looks up the array's device address (make it
- * before any stream capture); calls that overlap on the GPU share the array
- * and race. Runs on the default stream and is synchronous on return. */
+ * before any stream capture) and keeps it for the process: calls must not
+ * span a cudaDeviceReset. Calls that overlap on the GPU share the array and
+ * race. Every pointer must be device memory (host pointers are refused with
+ * SSV_ERR_INVALID_ARG). Runs on the legacy default stream and is synchronous
+ * on return; callers that produced the inputs on a non-blocking stream must
+ * synchronise that stream first. */
 int ssv_spmv_dot_noalloc(int32_t rows, const int32_t* d_row_ptr, const int32_t* d_col_idx,
                          const double* d_values, const double* d_x, double* d_y, double* d_dot);
 

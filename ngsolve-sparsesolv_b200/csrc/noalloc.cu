@@ -21,7 +21,19 @@
 // it names a host-side stand-in, not device memory. Its device address is
 // looked up with cudaGetSymbolAddress once per device, on the first call made
 // with that device current (that first call should therefore come before any
-// stream capture that includes this entry point).
+// stream capture that includes this entry point). The address is kept for the
+// life of the process: calls must not span a cudaDeviceReset (or any other
+// teardown of the device's primary context), after which the module is
+// reloaded elsewhere and the kept address is stale.
+//
+// Every pointer argument is checked to be device (or managed) memory with
+// cudaPointerGetAttributes before anything is launched, as in the library's
+// other _dev calls: a host pointer is refused with SSV_ERR_INVALID_ARG
+// instead of reaching the kernel.
+//
+// The kernel runs on the legacy default stream and the call synchronises it
+// before returning. A caller whose inputs were produced on a non-blocking
+// stream must synchronise that stream (or the device) before the call.
 #include <mutex>
 
 #include "kernels.cuh"
@@ -86,6 +98,19 @@ namespace ssv {
 const char* noalloc_set_error(const std::string& m);
 }
 
+namespace {
+// true when p is device or managed memory (cudaPointerGetAttributes
+// allocates nothing)
+bool is_device_ptr(const void* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+}  // namespace
+
 extern "C" int ssv_spmv_dot_noalloc(int32_t rows, const int32_t* d_row_ptr, const int32_t* d_col_idx,
                                     const double* d_values, const double* d_x, double* d_y, double* d_dot) {
     if (rows < 0 || !d_row_ptr || !d_x || !d_y || !d_dot || (rows > 0 && (!d_col_idx || !d_values))) {
@@ -103,6 +128,18 @@ extern "C" int ssv_spmv_dot_noalloc(int32_t rows, const int32_t* d_row_ptr, cons
     if (e != cudaSuccess || dev < 0 || dev >= 64) {
         ssv::noalloc_set_error(std::string("ssv_spmv_dot_noalloc: no usable CUDA device: ") + cudaGetErrorString(e));
         return SSV_ERR_NO_DEVICE;
+    }
+    {
+        const void* ptrs[6] = {d_row_ptr, d_col_idx, d_values, d_x, d_y, d_dot};
+        const char* names[6] = {"d_row_ptr", "d_col_idx", "d_values", "d_x", "d_y", "d_dot"};
+        for (int k = 0; k < 6; ++k) {
+            if (!ptrs[k]) continue;  // NULL col_idx / values are allowed for rows == 0
+            if (!is_device_ptr(ptrs[k])) {
+                ssv::noalloc_set_error(std::string("ssv_spmv_dot_noalloc: ") + names[k] +
+                                       " is not device memory (every pointer must be a device address)");
+                return SSV_ERR_INVALID_ARG;
+            }
+        }
     }
     double* scratch = nullptr;
     {

@@ -46,8 +46,10 @@ def test_noalloc_matches_existing_spmv_two_calls_in_a_row():
         torch.cuda.synchronize()
         y = dy.cpu().numpy()
         yref = dref.cpu().numpy()
+        ys = A @ x  # scipy, FP64 on the host
         np.testing.assert_allclose(y, yref, rtol=1e-14, atol=1e-14)
-        np.testing.assert_allclose(ddot.item(), float(x @ yref), rtol=1e-12)
+        np.testing.assert_allclose(y, ys, rtol=1e-13, atol=1e-13 * np.abs(ys).max())
+        np.testing.assert_allclose(ddot.item(), float(x @ ys), rtol=1e-12)
 
 
 def test_noalloc_rejects_too_many_rows():
@@ -60,3 +62,22 @@ def test_noalloc_rejects_too_many_rows():
     rc = lib.ssv_spmv_dot_noalloc(2097152 + 1, p, p, q, q, q, q)
     assert rc == _capi.SSV_ERR_INVALID_ARG
     assert b"exceed the maximum of 2097152" in lib.ssv_last_error()
+
+
+def test_noalloc_refuses_host_pointers():
+    """A host array where device memory is required is refused before any
+    launch (it would otherwise reach the kernel as an invalid address)."""
+    from sparsesolv_ngsolve import _capi
+    from sparsesolv_ngsolve import problems as P
+    lib = _capi.load()
+    A = P.laplacian_7pt(6)
+    n = A.shape[0]
+    rp, ci, val = _dev(A.indptr.astype(np.int32)), _dev(A.indices.astype(np.int32)), _dev(A.data)
+    hx = np.ones(n)
+    dy = _dev(np.zeros(n))
+    ddot = _dev(np.zeros(1))
+    rc = lib.ssv_spmv_dot_noalloc(n, ctypes.c_void_p(rp.data_ptr()), ctypes.c_void_p(ci.data_ptr()),
+                                  ctypes.c_void_p(val.data_ptr()), ctypes.c_void_p(hx.ctypes.data),
+                                  ctypes.c_void_p(dy.data_ptr()), ctypes.c_void_p(ddot.data_ptr()))
+    assert rc == _capi.SSV_ERR_INVALID_ARG
+    assert b"d_x is not device memory" in lib.ssv_last_error()
