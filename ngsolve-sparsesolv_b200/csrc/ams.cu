@@ -677,503 +677,6 @@ k_mv3_coarse(TriCoarse<K> t, const KState* st) {
 }
 
 // ---------------------------------------------------------------------------
-// V-cycle tail on one thread-block cluster: every level from the first small
-// one down to the coarsest solve and back up, in one launch. The cluster's 8
-// CTAs split each step's rows and meet at cluster barriers, which replace the
-// kernel boundaries of the per-level launch chain (latency-bound on small
-// levels). The arithmetic per level is the chain's (num_smooth = 1): fused
-// first sweep + residual, restriction, coarsest LDL^T solve (FP64) or 10
-// l1-Jacobi sweeps, prolongation, post sweep.
-// ---------------------------------------------------------------------------
-constexpr int kTailCluster = 8;
-constexpr int kTailBlock = 512;
-constexpr int kTailLanes = 4;
-
-// One level as the tail kernel sees it (values and vectors in the hierarchy type).
-struct TailLevel {
-    int n, direct;
-    const int *Arp, *Aci;
-    const void* Av;
-    const int *Prp, *Pci;
-    const void* Pv;  // n x n_next (not at the coarsest level)
-    const int *Trp, *Tci;
-    const void* Tv;  // P^T
-    const void *l1, *il1;
-    void *b, *x, *xalt, *r;
-    const double *Li, *LiT, *piv;
-    double* cz;
-};
-
-// rows of a CSR pass split over the cluster, kTailLanes threads per row;
-// acc = sum_k a_k * xval(col_k), then out(row, acc)
-template <typename T, int NV, typename FX, typename FO>
-__device__ __forceinline__ void tail_rows(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                                          const T* __restrict__ v, FX xval, FO out) {
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int G = gridDim.x * blockDim.x / kTailLanes;
-    const int sub = threadIdx.x % kTailLanes;
-    const int lane_row = (threadIdx.x & 31) / kTailLanes;  // warp-uniform trip count
-    for (int row = gt / kTailLanes; row - lane_row < n; row += G) {
-        const bool valid = row < n;
-        T acc[NV];
-#pragma unroll
-        for (int c = 0; c < NV; ++c) acc[c] = T(0);
-        if (valid)
-            for (int k = rp[row] + sub; k < rp[row + 1]; k += kTailLanes) {
-                const T a = v[k];
-                T xj[NV];
-                xval(ci[k], xj);
-#pragma unroll
-                for (int c = 0; c < NV; ++c) acc[c] += a * xj[c];
-            }
-#pragma unroll
-        for (int o = kTailLanes / 2; o > 0; o >>= 1)
-#pragma unroll
-            for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o, kTailLanes);
-        if (valid && sub == 0) out(row, acc);
-    }
-}
-
-template <typename T, int NV, bool RECIP>
-__global__ void __cluster_dims__(kTailCluster, 1, 1) __launch_bounds__(kTailBlock)
-k_vcycle_tail(const TailLevel* __restrict__ lv, int l0, int L, const T* __restrict__ b0, const KState* st) {
-    if (st && st->done) return;  // uniform: the state does not change while this runs
-    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
-    auto sync = [&]() {
-        __threadfence();
-        cl.sync();
-    };
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31;
-    const int gw = gt >> 5, GW = (gridDim.x * blockDim.x) >> 5;
-    auto dv = [&](int l) { return (const T*)(RECIP ? lv[l].il1 : lv[l].l1); };
-    auto rhs = [&](int l) { return l == l0 ? b0 : (const T*)lv[l].b; };
-    auto upd = [&](T xo, T r, T d) { return RECIP ? xo + r * d : xo + r / d; };
-    // down: fused first sweep + residual, then restriction
-    for (int l = l0; l < L - 1; ++l) {
-        const TailLevel& Lv = lv[l];
-        const T* b = rhs(l);
-        const T* d = dv(l);
-        T* x = (T*)Lv.x;
-        T* r = (T*)Lv.r;
-        tail_rows<T, NV>(Lv.n, Lv.Arp, Lv.Aci, (const T*)Lv.Av,
-                         [&](int j, T (&o)[NV]) {
-                             const T dj = d[j];
-#pragma unroll
-                             for (int c = 0; c < NV; ++c) o[c] = RECIP ? b[(size_t)j * NV + c] * dj : b[(size_t)j * NV + c] / dj;
-                         },
-                         [&](int row, T (&acc)[NV]) {
-                             const T di = d[row];
-#pragma unroll
-                             for (int c = 0; c < NV; ++c) {
-                                 const T bi = b[(size_t)row * NV + c];
-                                 x[(size_t)row * NV + c] = RECIP ? bi * di : bi / di;
-                                 r[(size_t)row * NV + c] = bi - acc[c];
-                             }
-                         });
-        sync();
-        T* bn = (T*)lv[l + 1].b;
-        tail_rows<T, NV>(lv[l + 1].n, Lv.Trp, Lv.Tci, (const T*)Lv.Tv,
-                         [&](int j, T (&o)[NV]) {
-#pragma unroll
-                             for (int c = 0; c < NV; ++c) o[c] = r[(size_t)j * NV + c];
-                         },
-                         [&](int row, T (&acc)[NV]) {
-#pragma unroll
-                             for (int c = 0; c < NV; ++c) bn[(size_t)row * NV + c] = acc[c];
-                         });
-        sync();
-    }
-    // coarsest
-    const TailLevel& C = lv[L - 1];
-    const T* bc = rhs(L - 1);
-    const T* res;
-    if (C.direct) {
-        const int n = C.n;
-        for (int row = gw; row < n; row += GW) {  // z = (L^{-1} b) / d, warp per row
-            double acc[NV];
-#pragma unroll
-            for (int c = 0; c < NV; ++c) acc[c] = 0.0;
-            const double* lr = C.Li + (size_t)row * n;
-            for (int k = lane; k <= row; k += 32) {
-                const double a = lr[k];
-#pragma unroll
-                for (int c = 0; c < NV; ++c) acc[c] += a * (double)bc[(size_t)k * NV + c];
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-                for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
-            if (lane == 0) {
-                const double dd = C.piv[row];
-#pragma unroll
-                for (int c = 0; c < NV; ++c) C.cz[(size_t)row * NV + c] = dd != 0.0 ? acc[c] / dd : 0.0;
-            }
-        }
-        sync();
-        T* x = (T*)C.x;
-        for (int row = gw; row < n; row += GW) {  // x = L^{-T} z
-            double acc[NV];
-#pragma unroll
-            for (int c = 0; c < NV; ++c) acc[c] = 0.0;
-            const double* lr = C.LiT + (size_t)row * n;
-            for (int k = row + lane; k < n; k += 32) {
-                const double a = lr[k];
-#pragma unroll
-                for (int c = 0; c < NV; ++c) acc[c] += a * C.cz[(size_t)k * NV + c];
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-                for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
-            if (lane == 0)
-#pragma unroll
-                for (int c = 0; c < NV; ++c) x[(size_t)row * NV + c] = (T)acc[c];
-        }
-        sync();
-        res = x;
-    } else {  // 10 l1-Jacobi sweeps from x = 0
-        const T* d = dv(L - 1);
-        T* cur = (T*)C.x;
-        T* alt = (T*)C.xalt;
-        for (int q = gt; q < C.n * NV; q += gridDim.x * blockDim.x) {
-            const int i = q / NV;
-            cur[q] = RECIP ? bc[q] * d[i] : bc[q] / d[i];
-        }
-        sync();
-        for (int k = 0; k < 9; ++k) {
-            tail_rows<T, NV>(C.n, C.Arp, C.Aci, (const T*)C.Av,
-                             [&](int j, T (&o)[NV]) {
-#pragma unroll
-                                 for (int c = 0; c < NV; ++c) o[c] = cur[(size_t)j * NV + c];
-                             },
-                             [&](int row, T (&acc)[NV]) {
-#pragma unroll
-                                 for (int c = 0; c < NV; ++c) {
-                                     const size_t q = (size_t)row * NV + c;
-                                     alt[q] = upd(cur[q], bc[q] - acc[c], d[row]);
-                                 }
-                             });
-            sync();
-            T* t = cur;
-            cur = alt;
-            alt = t;
-        }
-        res = cur;
-    }
-    // up: prolongation, then the post sweep into the level's second buffer
-    for (int l = L - 2; l >= l0; --l) {
-        const TailLevel& Lv = lv[l];
-        const T* b = rhs(l);
-        const T* d = dv(l);
-        T* x = (T*)Lv.x;
-        T* xa = (T*)Lv.xalt;
-        const T* e = res;
-        tail_rows<T, NV>(Lv.n, Lv.Prp, Lv.Pci, (const T*)Lv.Pv,
-                         [&](int j, T (&o)[NV]) {
-#pragma unroll
-                             for (int c = 0; c < NV; ++c) o[c] = e[(size_t)j * NV + c];
-                         },
-                         [&](int row, T (&acc)[NV]) {
-#pragma unroll
-                             for (int c = 0; c < NV; ++c) x[(size_t)row * NV + c] += T(1) * acc[c];
-                         });
-        sync();
-        tail_rows<T, NV>(Lv.n, Lv.Arp, Lv.Aci, (const T*)Lv.Av,
-                         [&](int j, T (&o)[NV]) {
-#pragma unroll
-                             for (int c = 0; c < NV; ++c) o[c] = x[(size_t)j * NV + c];
-                         },
-                         [&](int row, T (&acc)[NV]) {
-#pragma unroll
-                             for (int c = 0; c < NV; ++c) {
-                                 const size_t q = (size_t)row * NV + c;
-                                 xa[q] = upd(x[q], b[q] - acc[c], d[row]);
-                             }
-                         });
-        sync();
-        res = xa;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Whole V-cycles as one cooperative launch (SSV_AMS_GRID=1): up to K
-// hierarchies (the three nodal ones in lockstep, or the gradient one), from
-// the finest level down to the coarsest LDL^T solves and back up, every CTA on
-// every step and a grid-wide barrier wherever the launch chain has a kernel
-// boundary. The launch is cooperative, so all CTAs are resident together.
-// Each barrier wait is bounded: a wait that gives up fails the solve
-// (SSV_ERR_TIMEOUT, done) and the CTAs then run through the remaining steps
-// without waiting. Vectors written inside the launch are read through L2
-// (ld.global.cg), never through a possibly stale L1 line of another SM. The
-// arithmetic per row is the chain's (num_smooth = 1, direct coarsest solves).
-//
-// Opt-in: measured slower than the per-level launch chain on B200. On the 40^3
-// magnetostatic hierarchies (FP32) one launch takes 148 us for the gradient
-// V-cycle (18 barrier steps) and 391 us for the three nodal ones (34 steps),
-// against 64 and 172 us for the chains, whose launches overlap through
-// programmatic dependent launch at ~3.6-5 us a step. Here each step costs
-// ~8-11 us: the fixed 4 lanes per row are slow on the long rows of the coarse
-// Galerkin levels (the chain's tuner picks up to 32 lanes there), gathers go
-// through L2 only, and the barrier itself costs microseconds.
-// ---------------------------------------------------------------------------
-constexpr int kGridBlock = 1024;
-constexpr int kGridPerSm = 1;   // CTAs per SM, guaranteed by the launch bounds (no shared memory)
-constexpr int kBarGroups = 8;   // first-level arrival counters of the grid barrier
-
-// Barrier state, every counter on its own 128-byte line: CTAs arrive on the
-// counter of their group (blockIdx % kBarGroups), the last of a group on the
-// root, the last at the root advances the generation.
-struct GridBar {
-    unsigned group[kBarGroups][32];
-    unsigned root, r1[31];
-    unsigned gen, r2[31];
-    unsigned exit, r3[31];
-    int err, r4[31];
-};
-
-template <int K>
-struct GridCycle {
-    const TailLevel* lv[K];  // each hierarchy's level descriptors, finest first (device)
-    const void* b0[K];       // level-0 right-hand sides (hierarchy type)
-    int L[K];                // level counts (may differ)
-    int parts;
-};
-
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
-    unsigned o;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(o) : "l"(p), "r"(v) : "memory");
-    return o;
-}
-__device__ __forceinline__ void red_add_release(unsigned* p, unsigned v) {
-    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ void st_relaxed_u32(unsigned* p, unsigned v) {
-    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ int ld_relaxed_s32(const int* p) {
-    int v;
-    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// CTA leaders arrive on their group's counter, the last of each group on the
-// root, the last at the root advances the generation; everyone else waits for
-// the generation to move (bounded). The arrivals are acquire-release
-// read-modify-writes and the generation step a release, so every write made
-// before the barrier by any CTA (ordered before its leader's arrival by the
-// CTA barrier) is visible to every CTA after it. Each last arrival resets the
-// counter it completed before passing on.
-__device__ __forceinline__ void grid_barrier(GridBar* gb, KState* st) {
-    __syncthreads();
-    if (threadIdx.x == 0 && ld_relaxed_s32(&gb->err) == 0) {
-        const unsigned g = ld_acquire_u32(&gb->gen);
-        const unsigned ng = min((unsigned)kBarGroups, gridDim.x);
-        const unsigned grp = blockIdx.x % ng;
-        const unsigned members = (gridDim.x - grp + ng - 1) / ng;
-        bool last = false;
-        if (atom_add_acq_rel(&gb->group[grp][0], 1u) == members - 1) {
-            st_relaxed_u32(&gb->group[grp][0], 0u);
-            if (atom_add_acq_rel(&gb->root, 1u) == ng - 1) {
-                st_relaxed_u32(&gb->root, 0u);
-                red_add_release(&gb->gen, 1u);
-                last = true;
-            }
-        }
-        if (!last) {
-            int spins = 0;
-            while (ld_acquire_u32(&gb->gen) == g) {
-                if (++spins > (1 << 24)) {  // never expected: fail the solve, finish the launch
-                    atomicExch(&gb->err, 1);
-                    if (st) {
-                        st->status = SSV_ERR_TIMEOUT;
-                        st->done = 1;
-                    }
-                    break;
-                }
-                if (spins > 256) __nanosleep(32);
-            }
-        }
-    }
-    __syncthreads();
-}
-
-// the last CTA out resets the barrier state for the next launch
-__device__ __forceinline__ void grid_exit(GridBar* gb) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        if (atomicAdd(&gb->exit, 1u) == gridDim.x - 1) {
-            for (int i = 0; i < kBarGroups; ++i) atomicExch(&gb->group[i][0], 0u);
-            atomicExch(&gb->root, 0u);
-            atomicExch(&gb->gen, 0u);
-            atomicExch(&gb->err, 0);
-            __threadfence();
-            atomicExch(&gb->exit, 0u);
-        }
-    }
-}
-
-template <typename T, int NV>
-__device__ __forceinline__ void ldcg_row(const T* p, T (&o)[NV]) {
-#pragma unroll
-    for (int c = 0; c < NV; ++c) o[c] = __ldcg(p + c);
-}
-
-template <typename T, int NV, bool RECIP, int K>
-__global__ void __launch_bounds__(kGridBlock, kGridPerSm)
-k_vcycle_grid(GridCycle<K> g, GridBar* gb, KState* st) {
-    const bool skip = st && st->done;  // every CTA still takes part in the exit count
-    if (!skip) {
-        int Lmax = 0;
-        for (int q = 0; q < g.parts; ++q) Lmax = max(Lmax, g.L[q]);
-        auto sync = [&]() { grid_barrier(gb, st); };
-        auto dv = [&](const TailLevel& Lv) { return (const T*)(RECIP ? Lv.il1 : Lv.l1); };
-        auto rhs = [&](int q, int l) { return l == 0 ? (const T*)g.b0[q] : (const T*)g.lv[q][l].b; };
-        auto upd = [&](T xo, T r, T d) { return RECIP ? xo + r * d : xo + r / d; };
-        const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-        const int lane = threadIdx.x & 31;
-        const int gw = gt >> 5, GW = (gridDim.x * blockDim.x) >> 5;
-        // down: fused first sweep + residual, then restriction
-        for (int l = 0; l < Lmax - 1; ++l) {
-            for (int q = 0; q < g.parts; ++q) {
-                if (l >= g.L[q] - 1) continue;
-                const TailLevel& Lv = g.lv[q][l];
-                const T* b = rhs(q, l);
-                const T* d = dv(Lv);
-                T* x = (T*)Lv.x;
-                T* r = (T*)Lv.r;
-                tail_rows<T, NV>(Lv.n, Lv.Arp, Lv.Aci, (const T*)Lv.Av,
-                                 [&](int j, T (&o)[NV]) {
-                                     const T dj = d[j];
-                                     ldcg_row<T, NV>(b + (size_t)j * NV, o);
-#pragma unroll
-                                     for (int c = 0; c < NV; ++c) o[c] = RECIP ? o[c] * dj : o[c] / dj;
-                                 },
-                                 [&](int row, T (&acc)[NV]) {
-                                     const T di = d[row];
-#pragma unroll
-                                     for (int c = 0; c < NV; ++c) {
-                                         const T bi = __ldcg(b + (size_t)row * NV + c);
-                                         x[(size_t)row * NV + c] = RECIP ? bi * di : bi / di;
-                                         r[(size_t)row * NV + c] = bi - acc[c];
-                                     }
-                                 });
-            }
-            sync();
-            for (int q = 0; q < g.parts; ++q) {
-                if (l >= g.L[q] - 1) continue;
-                const TailLevel& Lv = g.lv[q][l];
-                const T* r = (const T*)Lv.r;
-                T* bn = (T*)g.lv[q][l + 1].b;
-                tail_rows<T, NV>(g.lv[q][l + 1].n, Lv.Trp, Lv.Tci, (const T*)Lv.Tv,
-                                 [&](int j, T (&o)[NV]) { ldcg_row<T, NV>(r + (size_t)j * NV, o); },
-                                 [&](int row, T (&acc)[NV]) {
-#pragma unroll
-                                     for (int c = 0; c < NV; ++c) bn[(size_t)row * NV + c] = acc[c];
-                                 });
-            }
-            sync();
-        }
-        // coarsest levels: z = (L^{-1} b) / d, then x = L^{-T} z (FP64), warp per row
-        for (int q = 0; q < g.parts; ++q) {
-            const TailLevel& C = g.lv[q][g.L[q] - 1];
-            const T* bc = rhs(q, g.L[q] - 1);
-            const int n = C.n;
-            for (int row = gw; row < n; row += GW) {
-                double acc[NV];
-#pragma unroll
-                for (int c = 0; c < NV; ++c) acc[c] = 0.0;
-                const double* lr = C.Li + (size_t)row * n;
-                for (int k = lane; k <= row; k += 32) {
-                    const double a = lr[k];
-#pragma unroll
-                    for (int c = 0; c < NV; ++c) acc[c] += a * (double)__ldcg(bc + (size_t)k * NV + c);
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-                    for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
-                if (lane == 0) {
-                    const double dd = C.piv[row];
-#pragma unroll
-                    for (int c = 0; c < NV; ++c) C.cz[(size_t)row * NV + c] = dd != 0.0 ? acc[c] / dd : 0.0;
-                }
-            }
-        }
-        sync();
-        for (int q = 0; q < g.parts; ++q) {
-            const TailLevel& C = g.lv[q][g.L[q] - 1];
-            const int n = C.n;
-            T* x = (T*)C.x;
-            for (int row = gw; row < n; row += GW) {
-                double acc[NV];
-#pragma unroll
-                for (int c = 0; c < NV; ++c) acc[c] = 0.0;
-                const double* lr = C.LiT + (size_t)row * n;
-                for (int k = row + lane; k < n; k += 32) {
-                    const double a = lr[k];
-#pragma unroll
-                    for (int c = 0; c < NV; ++c) acc[c] += a * __ldcg(C.cz + (size_t)k * NV + c);
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-                    for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
-                if (lane == 0)
-#pragma unroll
-                    for (int c = 0; c < NV; ++c) x[(size_t)row * NV + c] = (T)acc[c];
-            }
-        }
-        sync();
-        // up: prolongation, then the post sweep into the level's second buffer
-        for (int l = Lmax - 2; l >= 0; --l) {
-            for (int q = 0; q < g.parts; ++q) {
-                if (l > g.L[q] - 2) continue;
-                const TailLevel& Lv = g.lv[q][l];
-                const TailLevel& Nx = g.lv[q][l + 1];
-                const T* e = (const T*)((l + 1 == g.L[q] - 1) ? Nx.x : Nx.xalt);
-                T* x = (T*)Lv.x;
-                tail_rows<T, NV>(Lv.n, Lv.Prp, Lv.Pci, (const T*)Lv.Pv,
-                                 [&](int j, T (&o)[NV]) { ldcg_row<T, NV>(e + (size_t)j * NV, o); },
-                                 [&](int row, T (&acc)[NV]) {
-#pragma unroll
-                                     for (int c = 0; c < NV; ++c) {
-                                         const size_t i = (size_t)row * NV + c;
-                                         x[i] = __ldcg(x + i) + T(1) * acc[c];
-                                     }
-                                 });
-            }
-            sync();
-            for (int q = 0; q < g.parts; ++q) {
-                if (l > g.L[q] - 2) continue;
-                const TailLevel& Lv = g.lv[q][l];
-                const T* b = rhs(q, l);
-                const T* d = dv(Lv);
-                const T* x = (const T*)Lv.x;
-                T* xa = (T*)Lv.xalt;
-                tail_rows<T, NV>(Lv.n, Lv.Arp, Lv.Aci, (const T*)Lv.Av,
-                                 [&](int j, T (&o)[NV]) { ldcg_row<T, NV>(x + (size_t)j * NV, o); },
-                                 [&](int row, T (&acc)[NV]) {
-#pragma unroll
-                                     for (int c = 0; c < NV; ++c) {
-                                         const size_t i = (size_t)row * NV + c;
-                                         xa[i] = upd(__ldcg(x + i), __ldcg(b + i) - acc[c], d[row]);
-                                     }
-                                 });
-            }
-            sync();
-        }
-    }
-    grid_exit(gb);
-}
-
-// ---------------------------------------------------------------------------
 // Device hierarchy
 // ---------------------------------------------------------------------------
 static std::vector<float> to_float(const std::vector<double>& h) { return std::vector<float>(h.begin(), h.end()); }
@@ -1302,13 +805,6 @@ struct AmgDevLevel {
     WorkVec b, xa, xb, r;  // NV-column work vectors of this level
 };
 
-// Levels of one hierarchy run by the cluster tail kernel (start = first such
-// level, -1 = none) and their descriptors on the device.
-struct TailSet {
-    int start = -1;
-    DevBuf<TailLevel> desc;
-};
-
 struct AmsState {
     int nhc = 0, nh1 = 0, cycle_type = 1, num_smooth = 1, nv_alloc = 0;
     double w = 1.0;
@@ -1326,11 +822,7 @@ struct AmsState {
     std::vector<uint8_t> h_fd;
     unsigned gen = 0;
     ForkSet forks;  // the y and z nodal V-cycles run beside the x one
-    TailSet tails[4];
     bool tri = true;  // nodal V-cycles in lockstep launches (SSV_AMS_TRI=0: three branches)
-    bool grid = false;              // whole V-cycles as cooperative launches (SSV_AMS_GRID=1)
-    DevBuf<TailLevel> gdesc[4];     // every level of each hierarchy, for k_vcycle_grid
-    DevBuf<GridBar> gbar;           // its barrier state (zero between launches)
     int pi_lanes[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};  // Pi restrict / prolong lanes by NV slot (0 = untuned)
 };
 
@@ -1470,14 +962,9 @@ static T* vcycle_fused(std::vector<AmgDevLevel>& L, const T* b0, const KState* s
 // One AMG V-cycle (VCycle / DualVCycle, compact_amg.hpp:662-706,801-841) on
 // level l: b -> x (x starts at zero). Returns the buffer holding x.
 template <typename T, int NV, bool RECIP>
-static T* vcycle(std::vector<AmgDevLevel>& L, const TailSet& tail, int l, const T* b, int num_smooth,
-                 const KState* st, cudaStream_t s) {
-    if (l == 0 && num_smooth == 1 && tail.start < 0 && fused_ready(L)) return vcycle_fused<T, NV, RECIP>(L, b, st, s);
+static T* vcycle(std::vector<AmgDevLevel>& L, int l, const T* b, int num_smooth, const KState* st, cudaStream_t s) {
+    if (l == 0 && num_smooth == 1 && fused_ready(L)) return vcycle_fused<T, NV, RECIP>(L, b, st, s);
     AmgDevLevel& lv = L[l];
-    if (num_smooth == 1 && tail.start >= 0 && l == tail.start) {
-        k_vcycle_tail<T, NV, RECIP><<<kTailCluster, kTailBlock, 0, s>>>(tail.desc.get(), l, (int)L.size(), b, st);
-        return lv.xb.as<T>();  // the post sweep's buffer (the tail spans at least two levels)
-    }
     const T* d = l1_of<T, RECIP>(lv);
     T* cur = lv.xa.as<T>();
     T* alt = lv.xb.as<T>();
@@ -1509,7 +996,7 @@ static T* vcycle(std::vector<AmgDevLevel>& L, const TailSet& tail, int l, const 
     }
     AmgDevLevel& nx = L[l + 1];
     mv_spmv<T, T, T, NV, MV_AX, RECIP>(lv.Pt, lv.r.as<T>(), nx.b.as<T>(), nullptr, nullptr, T(0), st, s);
-    T* ec = vcycle<T, NV, RECIP>(L, tail, l + 1, nx.b.as<T>(), num_smooth, st, s);
+    T* ec = vcycle<T, NV, RECIP>(L, l + 1, nx.b.as<T>(), num_smooth, st, s);
     mv_spmv<T, T, T, NV, MV_ADD, RECIP>(lv.P, ec, cur, nullptr, nullptr, T(1), st, s);
     sweep(num_smooth);
     return cur;
@@ -1519,7 +1006,7 @@ static T* vcycle(std::vector<AmgDevLevel>& L, const TailSet& tail, int l, const 
 static bool tri_ok(const AmsState& a) {
     if (!a.tri) return false;
     for (int k = 1; k < 4; ++k) {
-        if (a.amg[k].empty() || a.tails[k].start >= 0 || !a.amg[k].back().direct) return false;
+        if (a.amg[k].empty() || !a.amg[k].back().direct) return false;
     }
     return true;
 }
@@ -1691,42 +1178,6 @@ static void vcycle3(AmsState& a, const KState* st, cudaStream_t s, T* out[3]) {
     vcycleM<T, NV, RECIP, 3>(H, rhs0, 3, st, s, out);
 }
 
-// The batched solver applies several preconditioners on concurrent graph
-// branches; whole-V-cycle launches need the whole GPU, so they are used only
-// outside such branches.
-static bool g_grid_suspended = false;
-void ams_grid_suspend(bool on) { g_grid_suspended = on; }
-
-static bool grid_ok(const AmsState& a, const KState* st) { return a.grid && st && !g_grid_suspended; }
-
-// One cooperative launch of k_vcycle_grid over hierarchies subs[0..parts) with
-// right-hand sides rhs0; out[k] = each hierarchy's level-0 result.
-template <typename T, int NV, bool RECIP, int K>
-static void vcycle_grid(AmsState& a, const int* subs, const T* const* rhs0, int parts, const KState* st,
-                        cudaStream_t s, T** out) {
-    const int grid = sm_count() * kGridPerSm;  // co-resident: the launch bounds fit kGridPerSm CTAs per SM
-    GridCycle<K> g{};
-    g.parts = parts;
-    for (int k = 0; k < parts; ++k) {
-        const auto& L = a.amg[subs[k]];
-        g.lv[k] = a.gdesc[subs[k]].get();
-        g.b0[k] = rhs0[k];
-        g.L[k] = (int)L.size();
-        out[k] = (L.size() == 1) ? L[0].xa.template as<T>() : L[0].xb.template as<T>();
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(kGridBlock);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeCooperative;
-    at[0].val.cooperative = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    SSV_CUDA(cudaLaunchKernelEx(&cfg, k_vcycle_grid<T, NV, RECIP, K>, g, a.gbar.get(), const_cast<KState*>(st)));
-}
-
 template <typename T, int NV, int LANES>
 static void pi_restrict_l(const AmsState& a, const double* r, T* ox, T* oy, T* oz, const KState* st,
                           cudaStream_t s) {
@@ -1823,31 +1274,20 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
     auto gradient = [&]() {
         residual();
         mv_spmv<double, double, T, NV, MV_AX, RECIP>(a.Gt, r, a.rs[0].as<T>(), nullptr, nullptr, T(0), st, s);
-        T* g;
-        if (grid_ok(a, st)) {
-            const int subs[1] = {0};
-            const T* rhs0[1] = {a.rs[0].as<T>()};
-            vcycle_grid<T, NV, RECIP, 1>(a, subs, rhs0, 1, st, s, &g);
-        } else {
-            g = vcycle<T, NV, RECIP>(a.amg[0], a.tails[0], 0, a.rs[0].as<T>(), 1, st, s);
-        }
+        T* g = vcycle<T, NV, RECIP>(a.amg[0], 0, a.rs[0].as<T>(), 1, st, s);
         mv_spmv<double, T, double, NV, MV_ADD, RECIP>(a.G, g, cur, nullptr, nullptr, a.w, st, s);
     };
     auto nodal = [&]() {
         residual();
         pi_restrict<T, NV>(a, r, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), st, s);
         T* g3[3];
-        if (grid_ok(a, st)) {  // one cooperative launch for all three V-cycles
-            const int subs[3] = {1, 2, 3};
-            const T* rhs0[3] = {a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>()};
-            vcycle_grid<T, NV, RECIP, 3>(a, subs, rhs0, 3, st, s, g3);
-        } else if (tri_ok(a)) {  // one chain of launches carrying all three hierarchies
+        if (tri_ok(a)) {  // one chain of launches carrying all three hierarchies
             vcycle3<T, NV, RECIP>(a, st, s, g3);
         } else {  // the three V-cycles are independent (own hierarchies and vectors)
             a.forks.fork(s, 2);
-            g3[0] = vcycle<T, NV, RECIP>(a.amg[1], a.tails[1], 0, a.rs[1].as<T>(), 1, st, s);
-            g3[1] = vcycle<T, NV, RECIP>(a.amg[2], a.tails[2], 0, a.rs[2].as<T>(), 1, st, a.forks.side[0]);
-            g3[2] = vcycle<T, NV, RECIP>(a.amg[3], a.tails[3], 0, a.rs[3].as<T>(), 1, st, a.forks.side[1]);
+            g3[0] = vcycle<T, NV, RECIP>(a.amg[1], 0, a.rs[1].as<T>(), 1, st, s);
+            g3[1] = vcycle<T, NV, RECIP>(a.amg[2], 0, a.rs[2].as<T>(), 1, st, a.forks.side[0]);
+            g3[2] = vcycle<T, NV, RECIP>(a.amg[3], 0, a.rs[3].as<T>(), 1, st, a.forks.side[1]);
             a.forks.join(s, 2);
         }
         pi_prolong<T, NV>(a, g3[0], g3[1], g3[2], cur, st, s);
@@ -1859,149 +1299,6 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
     }
     ensure_x();
     launch_k(k_mv_mask_copy<double, double, NV>, gm, kBlock, s, n, cur, fd, out, st);
-    SSV_LAUNCH_CHECK();
-}
-
-// ---------------------------------------------------------------------------
-// Several AMS preconditioners applied together (the frequencies of a batched
-// solve): every step of the cycle string is issued for all of them before the
-// next step, the fine-level and transfer passes one launch per preconditioner,
-// the gradient and nodal V-cycles as single lockstep chains over all their
-// hierarchies (vcycleM). Each preconditioner's arithmetic is that of
-// ams_cycle. Requires direct coarsest solves in every hierarchy.
-//
-// Opt-in (SSV_AMS_MULTI=1). It issues 2.5-3.7x fewer launches than parallel
-// graph branches (one per preconditioner) but runs them as one serial chain,
-// and on B200 the branches win at every size measured: 8 frequencies x 4
-// right-hand sides of the eddy-current family, 0.57 / 1.29 / 2.50 / 4.35 /
-// 9.88 ms per COCR iteration at 12^3 / 18^3 / 24^3 / 30^3 / 40^3 as branches
-// against 1.00 / 1.80 / 3.25 / 5.33 / 11.32 ms in lockstep. The branches
-// overlap the frequencies' fine-level passes, which the lockstep chain
-// issues one preconditioner after another.
-// ---------------------------------------------------------------------------
-constexpr int kMultiParts = 32;
-
-// SSV_AMS_MULTI=1: the batched solver applies its preconditioners in lockstep
-// instead of as parallel graph branches
-static bool multi_lockstep_enabled() {
-    static int v = -1;
-    if (v < 0) {
-        const char* e = std::getenv("SSV_AMS_MULTI");
-        v = (e && e[0] == '1') ? 1 : 0;
-    }
-    return v != 0;
-}
-
-template <typename T, int NV, bool RECIP>
-struct CycleCtx {
-    AmsState* a;
-    const double* d;
-    double *b0, *cur, *alt, *r;
-    const uint8_t* fd;
-    int n;
-    bool fresh = true;
-    void init(AmsState* as) {
-        a = as;
-        n = as->nhc;
-        fd = as->has_fd ? as->fd.get() : nullptr;
-        d = RECIP ? as->fine_il1.get() : as->fine_l1.get();
-        b0 = as->b0.get();
-        cur = as->xa.get();
-        alt = as->xb.get();
-        r = as->r.get();
-        fresh = true;
-    }
-    void smooth(const KState* st, cudaStream_t s) {
-        for (int k = 0; k < a->num_smooth; ++k) {
-            if (fresh) {
-                first_sweep<double, NV, RECIP>(n, b0, d, cur, st, s);
-                fresh = false;
-            } else {
-                mv_spmv<double, double, double, NV, MV_JAC, RECIP>(a->A_bc, cur, alt, b0, d, 0.0, st, s);
-                std::swap(cur, alt);
-            }
-        }
-    }
-    void ensure_x(cudaStream_t s) {
-        if (fresh) {
-            SSV_CUDA(cudaMemsetAsync(cur, 0, sizeof(double) * (size_t)n * NV, s));
-            fresh = false;
-        }
-    }
-    void residual(const KState* st, cudaStream_t s) {
-        ensure_x(s);
-        mv_spmv<double, double, double, NV, MV_RES, RECIP>(a->A_bc, cur, r, b0, nullptr, 0.0, st, s);
-    }
-};
-
-static bool multi_ok(AmsState* const* A, int F) {
-    if (F < 2 || 3 * F > kMultiParts) return false;
-    const AmsState& a0 = *A[0];
-    for (int f = 0; f < F; ++f) {
-        const AmsState& a = *A[f];
-        if (a.fp32 != a0.fp32 || a.complex_form != a0.complex_form || a.cycle_type != a0.cycle_type) return false;
-        for (int k = 0; k < 4; ++k)
-            if (a.tails[k].start >= 0 || a.amg[k].empty() || !a.amg[k].back().direct) return false;
-    }
-    return true;
-}
-
-template <typename T, int NV, bool RECIP>
-static void ams_cycle_multi(AmsState* const* A, int F, const double* const* in, double* const* out, const KState* st,
-                            cudaStream_t s) {
-    std::vector<CycleCtx<T, NV, RECIP>> c(F);
-    for (int f = 0; f < F; ++f) {
-        c[f].init(A[f]);
-        launch_k(k_mv_mask_copy<double, double, NV>, grid_for((int64_t)c[f].n * NV, kBlock), kBlock, s, c[f].n,
-                 in[f], c[f].fd, c[f].b0, st);
-    }
-    auto smooth = [&]() {
-        for (auto& x : c) x.smooth(st, s);
-    };
-    auto gradient = [&]() {
-        std::vector<AmgDevLevel>* H[kMultiParts];
-        const T* rhs0[kMultiParts];
-        T* g[kMultiParts];
-        for (int f = 0; f < F; ++f) {
-            AmsState& a = *c[f].a;
-            c[f].residual(st, s);
-            mv_spmv<double, double, T, NV, MV_AX, RECIP>(a.Gt, c[f].r, a.rs[0].as<T>(), nullptr, nullptr, T(0), st, s);
-            H[f] = &a.amg[0];
-            rhs0[f] = a.rs[0].as<T>();
-        }
-        vcycleM<T, NV, RECIP, kMultiParts>(H, rhs0, F, st, s, g);
-        for (int f = 0; f < F; ++f) {
-            AmsState& a = *c[f].a;
-            mv_spmv<double, T, double, NV, MV_ADD, RECIP>(a.G, g[f], c[f].cur, nullptr, nullptr, a.w, st, s);
-        }
-    };
-    auto nodal = [&]() {
-        std::vector<AmgDevLevel>* H[kMultiParts];
-        const T* rhs0[kMultiParts];
-        T* g[kMultiParts];
-        for (int f = 0; f < F; ++f) {
-            AmsState& a = *c[f].a;
-            c[f].residual(st, s);
-            pi_restrict<T, NV>(a, c[f].r, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), st, s);
-            for (int k = 0; k < 3; ++k) {
-                H[3 * f + k] = &a.amg[k + 1];
-                rhs0[3 * f + k] = a.rs[k + 1].as<T>();
-            }
-        }
-        vcycleM<T, NV, RECIP, kMultiParts>(H, rhs0, 3 * F, st, s, g);
-        for (int f = 0; f < F; ++f)
-            pi_prolong<T, NV>(*c[f].a, g[3 * f], g[3 * f + 1], g[3 * f + 2], c[f].cur, st, s);
-    };
-    if (A[0]->cycle_type == 7) {
-        smooth(); gradient(); smooth(); nodal(); smooth(); gradient(); smooth();
-    } else {
-        smooth(); gradient(); nodal(); gradient(); smooth();
-    }
-    for (int f = 0; f < F; ++f) {
-        c[f].ensure_x(s);
-        launch_k(k_mv_mask_copy<double, double, NV>, grid_for((int64_t)c[f].n * NV, kBlock), kBlock, s, c[f].n,
-                 (const double*)c[f].cur, c[f].fd, out[f], st);
-    }
     SSV_LAUNCH_CHECK();
 }
 
@@ -2368,121 +1665,6 @@ static void tune_lanes(AmsState& a) {
     cudaEventDestroy(e1);
 }
 
-// Which levels the cluster tail runs: the suffix of levels with at most 8192
-// rows and at most SSV_AMS_TAIL_NNZ nonzeros, when it spans at least two
-// levels. Off by default (0): on the 40^3 benchmark hierarchies it measured no
-// faster than the per-level launches (8 SMs stream the larger tail levels no
-// faster than the launch latency it saves). Descriptors are rebuilt whenever
-// the work vectors are.
-static void build_tails(AmsState& a) {
-    const char* env = std::getenv("SSV_AMS_TAIL_NNZ");
-    const long lim = env ? std::atol(env) : 0L;
-    for (int sub = 0; sub < 4; ++sub) {
-        auto& L = a.amg[sub];
-        TailSet& t = a.tails[sub];
-        t.start = -1;
-        if (lim <= 0 || a.num_smooth != 1) continue;
-        for (int l = (int)L.size() - 1; l >= 0; --l) {
-            if (L[l].A.n <= 8192 && L[l].A.nnz <= lim) t.start = l;
-            else break;
-        }
-        if (t.start >= 0 && (int)L.size() - t.start < 2) t.start = -1;
-        if (t.start < 0) continue;
-        std::vector<TailLevel> h(L.size());
-        std::memset(h.data(), 0, sizeof(TailLevel) * h.size());
-        auto vals = [&](const DevCsr& M) -> const void* {
-            return a.fp32 ? (const void*)M.val<float>() : (const void*)M.val<double>();
-        };
-        auto dual = [&](const DualVec& v) -> const void* {
-            return a.fp32 ? (const void*)v.get<float>() : (const void*)v.get<double>();
-        };
-        for (size_t l = t.start; l < L.size(); ++l) {
-            AmgDevLevel& lv = L[l];
-            TailLevel& d = h[l];
-            d.n = lv.A.n;
-            d.direct = lv.direct ? 1 : 0;
-            d.Arp = lv.A.rp.get();
-            d.Aci = lv.A.ci.get();
-            d.Av = vals(lv.A);
-            if (l + 1 < L.size()) {
-                d.Prp = lv.P.rp.get();
-                d.Pci = lv.P.ci.get();
-                d.Pv = vals(lv.P);
-                d.Trp = lv.Pt.rp.get();
-                d.Tci = lv.Pt.ci.get();
-                d.Tv = vals(lv.Pt);
-            }
-            d.l1 = dual(lv.l1);
-            d.il1 = dual(lv.il1);
-            d.b = lv.b.raw.get();
-            d.x = lv.xa.raw.get();
-            d.xalt = lv.xb.raw.get();
-            d.r = lv.r.raw.get();
-            d.Li = lv.Li.get();
-            d.LiT = lv.LiT.get();
-            d.piv = lv.piv.get();
-            d.cz = lv.cz.get();
-        }
-        t.desc.upload(h.data(), h.size(), stream());
-    }
-    SSV_CUDA(cudaStreamSynchronize(stream()));
-}
-
-// Level descriptors of every hierarchy for the whole-V-cycle launch, rebuilt
-// with the work vectors. Used only where every hierarchy ends in a direct
-// coarsest solve and no cluster tail is active.
-static void build_grid(AmsState& a) {
-    const char* env = std::getenv("SSV_AMS_GRID");
-    a.grid = env && env[0] == '1';
-    for (int sub = 0; sub < 4 && a.grid; ++sub)
-        if (a.amg[sub].empty() || !a.amg[sub].back().direct || a.tails[sub].start >= 0) a.grid = false;
-    if (!a.grid) return;
-    auto vals = [&](const DevCsr& M) -> const void* {
-        return a.fp32 ? (const void*)M.val<float>() : (const void*)M.val<double>();
-    };
-    auto dual = [&](const DualVec& v) -> const void* {
-        return a.fp32 ? (const void*)v.get<float>() : (const void*)v.get<double>();
-    };
-    for (int sub = 0; sub < 4; ++sub) {
-        auto& L = a.amg[sub];
-        std::vector<TailLevel> h(L.size());
-        std::memset(h.data(), 0, sizeof(TailLevel) * h.size());
-        for (size_t l = 0; l < L.size(); ++l) {
-            AmgDevLevel& lv = L[l];
-            TailLevel& d = h[l];
-            d.n = lv.A.n;
-            d.direct = lv.direct ? 1 : 0;
-            d.Arp = lv.A.rp.get();
-            d.Aci = lv.A.ci.get();
-            d.Av = vals(lv.A);
-            if (l + 1 < L.size()) {
-                d.Prp = lv.P.rp.get();
-                d.Pci = lv.P.ci.get();
-                d.Pv = vals(lv.P);
-                d.Trp = lv.Pt.rp.get();
-                d.Tci = lv.Pt.ci.get();
-                d.Tv = vals(lv.Pt);
-            }
-            d.l1 = dual(lv.l1);
-            d.il1 = dual(lv.il1);
-            d.b = lv.b.raw.get();
-            d.x = lv.xa.raw.get();
-            d.xalt = lv.xb.raw.get();
-            d.r = lv.r.raw.get();
-            d.Li = lv.Li.get();
-            d.LiT = lv.LiT.get();
-            d.piv = lv.piv.get();
-            d.cz = lv.cz.get();
-        }
-        a.gdesc[sub].upload(h.data(), h.size(), stream());
-    }
-    if (!a.gbar.get()) {
-        a.gbar.alloc(1);
-        a.gbar.zero(stream());
-    }
-    SSV_CUDA(cudaStreamSynchronize(stream()));
-}
-
 // Work vectors for blocks of up to nv real columns (allocation only, so the
 // cycle itself never allocates and can be captured).
 static void ams_reserve(AmsState& a, int nv) {
@@ -2505,8 +1687,6 @@ static void ams_reserve(AmsState& a, int nv) {
     a.nv_alloc = nv;
     ++a.gen;  // new work buffers: graphs that captured the old ones must be rebuilt
     tune_lanes(a);
-    build_tails(a);
-    build_grid(a);
     {
         const char* e = std::getenv("SSV_AMS_TRI");
         a.tri = !(e && e[0] == '0');
@@ -2770,34 +1950,6 @@ static void ams_block_t(AmsState& a, const double* in, double* out, int nrhs, co
     fail(SSV_ERR_INVALID_ARG, "AMS block apply: nrhs must be 1 or 4");
 }
 
-template <typename T>
-static bool ams_multi_t(AmsState* const* A, int F, const double* const* in, double* const* out, int nrhs,
-                        const KState* st, cudaStream_t s) {
-    if (A[0]->complex_form) {
-        switch (nrhs) {
-            case 1: ams_cycle_multi<T, 2, true>(A, F, in, out, st, s); return true;
-            case 4: ams_cycle_multi<T, 8, true>(A, F, in, out, st, s); return true;
-        }
-    } else {
-        switch (nrhs) {
-            case 1: ams_cycle_multi<T, 1, false>(A, F, in, out, st, s); return true;
-            case 4: ams_cycle_multi<T, 4, false>(A, F, in, out, st, s); return true;
-        }
-    }
-    return false;
-}
-
-bool ams_apply_block_multi(AmsState* const* A, int F, const double* const* in, double* const* out, int nrhs,
-                           const KState* st, cudaStream_t s) {
-    if (!multi_lockstep_enabled() || !multi_ok(A, F)) return false;
-    for (int f = 0; f < F; ++f) {
-        if (nrhs * (A[f]->complex_form ? 2 : 1) > A[f]->nv_alloc) return false;
-        for (int g = 0; g < f; ++g)
-            if (A[g] == A[f]) return false;  // one preconditioner's work vectors serve one column block at a time
-    }
-    return A[0]->fp32 ? ams_multi_t<float>(A, F, in, out, nrhs, st, s) : ams_multi_t<double>(A, F, in, out, nrhs, st, s);
-}
-
 // nrhs right-hand sides, row-interleaved ([row][rhs], complex as Re/Im pairs).
 void ams_apply_block(AmsState* a, const double* in, double* out, int nrhs, const KState* st, cudaStream_t s) {
     if (nrhs * (a->complex_form ? 2 : 1) > a->nv_alloc) fail(SSV_ERR_INVALID_ARG, "AMS block apply: reserve first");
@@ -2875,7 +2027,7 @@ static void ams_profile_t(AmsState& a, int reps, bool cold, ssv_phase_profile* o
     timed("fine_smooth", fine_jac, 1, [&] {
         mv_spmv<double, double, double, NV, MV_JAC, RECIP>(a.A_bc, cur, alt, a.b0.get(), d, 0.0, nullptr, s);
     });
-    timed("grad_vcycle", grad_vc, 0, [&] { vcycle<T, NV, RECIP>(a.amg[0], a.tails[0], 0, a.rs[0].as<T>(), 1, nullptr, s); });
+    timed("grad_vcycle", grad_vc, 0, [&] { vcycle<T, NV, RECIP>(a.amg[0], 0, a.rs[0].as<T>(), 1, nullptr, s); });
     timed("nodal_vcycles", nod_vc, 0, [&] {
         if (tri_ok(a)) {
             T* g3[3];
@@ -2883,9 +2035,9 @@ static void ams_profile_t(AmsState& a, int reps, bool cold, ssv_phase_profile* o
             return;
         }
         a.forks.fork(s, 2);
-        vcycle<T, NV, RECIP>(a.amg[1], a.tails[1], 0, a.rs[1].as<T>(), 1, nullptr, s);
-        vcycle<T, NV, RECIP>(a.amg[2], a.tails[2], 0, a.rs[2].as<T>(), 1, nullptr, a.forks.side[0]);
-        vcycle<T, NV, RECIP>(a.amg[3], a.tails[3], 0, a.rs[3].as<T>(), 1, nullptr, a.forks.side[1]);
+        vcycle<T, NV, RECIP>(a.amg[1], 0, a.rs[1].as<T>(), 1, nullptr, s);
+        vcycle<T, NV, RECIP>(a.amg[2], 0, a.rs[2].as<T>(), 1, nullptr, a.forks.side[0]);
+        vcycle<T, NV, RECIP>(a.amg[3], 0, a.rs[3].as<T>(), 1, nullptr, a.forks.side[1]);
         a.forks.join(s, 2);
     });
     timed("grad_transfers", g_tr, 2, [&] {
@@ -2929,7 +2081,6 @@ void ams_profile(AmsState* a, int nrhs, int reps, int flags, ssv_phase_profile* 
 struct AmgOnly {
     AmgHost host;
     std::vector<AmgDevLevel> lev;
-    TailSet tail;  // not used: the per-level launch chain
     bool has_fd = false;
     std::vector<uint8_t> h_fd;
     DevBuf<uint8_t> fd;
@@ -2980,7 +2131,6 @@ static void amg_rebuild(AmgOnly& g, const ssv_matrix* A) {
         dl.xb.alloc(nl);
         dl.r.alloc(nl);
     }
-    g.tail.start = -1;
     cudaEvent_t e0, e1;
     SSV_CUDA(cudaEventCreate(&e0));
     SSV_CUDA(cudaEventCreate(&e1));
@@ -3043,7 +2193,7 @@ int amg_levels(const AmgOnly* g, int* sizes, int cap) {
 
 // Mult (compact_amg.hpp:166-183): x = 0, VCycle(0, b, x), constrained x = 0
 static void amg_apply(AmgOnly& g, const double* x, double* y, const KState* st, cudaStream_t s) {
-    const double* res = vcycle<double, 1, false>(g.lev, g.tail, 0, x, g.num_smooth, st, s);
+    const double* res = vcycle<double, 1, false>(g.lev, 0, x, g.num_smooth, st, s);
     launch_k(k_mv_mask_copy<double, double, 1>, grid_for(g.n, kBlock), kBlock, s, g.n, res,
              (const uint8_t*)(g.has_fd ? g.fd.get() : nullptr), y, st);
     SSV_LAUNCH_CHECK();

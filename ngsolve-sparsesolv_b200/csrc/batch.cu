@@ -527,22 +527,7 @@ static void bt_pq(ssv_batch& B, cudaStream_t s) {
 // the frequencies are independent and run as parallel branches
 static void bt_precond(ssv_batch& B, const zdouble* in, zdouble* out, const KState* st, cudaStream_t s) {
     const size_t blk = (size_t)B.n * B.R;
-    {  // all frequencies' AMS cycles in lockstep (opt-in, SSV_AMS_MULTI=1)
-        std::vector<AmsState*> A;
-        std::vector<const double*> ins;
-        std::vector<double*> outs;
-        for (int f = 0; f < B.F && B.pre[f]; ++f) {
-            A.push_back(B.pre[f]->ams.get());
-            ins.push_back(reinterpret_cast<const double*>(in + f * blk));
-            outs.push_back(reinterpret_cast<double*>(out + f * blk));
-        }
-        if ((int)A.size() == B.F && ams_apply_block_multi(A.data(), B.F, ins.data(), outs.data(), B.R, st, s)) return;
-    }
     B.forks.fork(s, B.branches);
-    struct GridSuspend {  // whole-V-cycle launches off while the branches are issued, also on a throw
-        GridSuspend() { ams_grid_suspend(true); }
-        ~GridSuspend() { ams_grid_suspend(false); }
-    } suspend;
     for (int f = 0; f < B.F; ++f) {
         const zdouble* i = in + f * blk;
         zdouble* o = out + f * blk;

@@ -798,11 +798,6 @@ __device__ __forceinline__ zdouble ld_cg(const zdouble* p) {
     const double2 v = __ldcg(reinterpret_cast<const double2*>(p));
     return {v.x, v.y};
 }
-__device__ __forceinline__ int ld_acquire(const int* p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
 
 template <typename S, typename SL, bool FWD>
 __device__ __forceinline__ void staged_sweep(unsigned char* smem, int nlev, const int* __restrict__ lev,
@@ -872,119 +867,6 @@ k_ic_sweep_staged(int nlev, const int* __restrict__ lev, const int* __restrict__
     if (st && st->done) return;
     extern __shared__ __align__(16) unsigned char smem[];
     staged_sweep<S, SL, FWD>(smem, nlev, lev, rows, srp, ssrc, scol, sloc, Lrp, vals, inv_diag, x, sc, y);
-}
-
-// ---------------------------------------------------------------------------
-// All colours of one IC sweep in one launch. Work units (a run of ordinary
-// ABMC blocks of one colour, blockDim/LANES blocks per unit, or one oversized
-// block, swept staged) are handed out by a ticket counter in sweep order; a
-// unit of colour stage k waits until every unit of stage k-1 has signalled,
-// which by induction means all earlier stages are done. A unit only waits for
-// units with earlier tickets, which CTAs already running hold, so the launch
-// needs no co-residency: it makes progress with any number of resident CTAs.
-// The wait is bounded (a timeout marks the solve failed and lets the launch
-// finish). The last CTA to leave resets the counters for the next launch.
-// ctr: [0] tickets, [1] CTAs done, [2 + k] units of stage k done.
-// ---------------------------------------------------------------------------
-struct SweepUnit {
-    int kind;   // 0: ordinary blocks [a, b); 2: oversized block, level offsets lev[a..b]
-    int a, b;
-    int stage;  // position of the unit's colour in the sweep order
-};
-
-template <typename S, typename SL, int LANES, bool FWD>
-__global__ void __launch_bounds__(256)
-k_ic_sweep_all(int nunits, const SweepUnit* __restrict__ units, const int* __restrict__ stage_total, int* ctr,
-               const int* __restrict__ boff, const int* __restrict__ xrp, const int* __restrict__ xci,
-               const SL* __restrict__ xv, const SL* __restrict__ iv, int tri, const SL* __restrict__ dv,
-               const int* __restrict__ lev, const int* __restrict__ rows, const int* __restrict__ srp,
-               const int* __restrict__ ssrc, const int* __restrict__ scol, const int* __restrict__ sloc,
-               const int* __restrict__ Lrp, const SL* __restrict__ full, const S* __restrict__ x,
-               const double* __restrict__ sc, S* y, KState* st) {
-    pdl_gate();
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_unit;
-    const int tid = threadIdx.x;
-    // a finished solve skips the work, but every CTA still takes part in the
-    // exit count so that the counters are reset
-    const bool skip = st && st->done;
-    while (!skip) {
-        if (tid == 0) s_unit = atomicAdd(&ctr[0], 1);
-        __syncthreads();
-        const int u = s_unit;
-        if (u >= nunits) break;
-        const SweepUnit U = units[u];
-        if (tid == 0 && U.stage > 0) {
-            const int need = stage_total[U.stage - 1];
-            int spins = 0;
-            while (ld_acquire(&ctr[2 + U.stage - 1]) < need) {
-                if (++spins > (1 << 22)) {  // never expected: fail the solve, finish the launch
-                    if (st) {
-                        st->status = SSV_ERR_TIMEOUT;
-                        st->done = 1;
-                    }
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __syncthreads();
-        if (U.kind == 0) {
-            const int lane = tid % LANES;
-            const int b = U.a + tid / LANES;
-            const bool vb = b < U.b;
-            int r0 = 0, nr = 0;
-            if (vb) {
-                r0 = boff[b];
-                nr = boff[b + 1] - r0;
-            }
-            const bool act = vb && lane < nr;
-            const int i = r0 + lane;
-            S s = ST<S>::zero();
-            if (act) {
-                if constexpr (FWD) {
-                    s = x[i];
-                    if (sc) s = ST<S>::scale(sc[i], s);
-                }
-                const int k1 = xrp[i + 1];
-                for (int k = xrp[i]; k < k1; ++k) s = s - hi_of_any(xv[k]) * ld_cg(y + xci[k]);
-            }
-            S yi = ST<S>::zero();
-            const SL* ib = iv + (size_t)(vb ? b : 0) * tri;
-            if constexpr (FWD) {
-#pragma unroll
-                for (int t = 0; t < LANES; ++t) {
-                    if (act && lane == t) yi = ST<S>::div(s, hi_of_any(dv[i]));
-                    const S yt = shfl_s(yi, t, LANES);
-                    if (act && t < lane) s = s - hi_of_any(ib[lane * (lane - 1) / 2 + t]) * yt;
-                }
-            } else {
-#pragma unroll
-                for (int t = LANES - 1; t >= 0; --t) {
-                    if (act && lane == t) yi = s * hi_of_any(dv[i]) + x[i];
-                    const S yt = shfl_s(yi, t, LANES);
-                    if (act && lane < t && t < nr) s = s - hi_of_any(ib[t * (t - 1) / 2 + lane]) * yt;
-                }
-            }
-            if (act) y[i] = yi;
-        } else {
-            staged_sweep<S, SL, FWD>(smem, U.b - U.a, lev + U.a, rows, srp, ssrc, scol, sloc, Lrp, full, dv, x,
-                                     sc, y);
-        }
-        __syncthreads();  // the unit's stores, then one release by thread 0
-        if (tid == 0) {
-            __threadfence();
-            atomicAdd(&ctr[2 + U.stage], 1);
-        }
-    }
-    if (tid == 0) {
-        __threadfence();
-        if (atomicAdd(&ctr[1], 1) == (int)gridDim.x - 1) {
-            const int nst = units[nunits - 1].stage + 1;
-            for (int k = 0; k < 2 + nst; ++k) ctr[k] = 0;
-            __threadfence();
-        }
-    }
 }
 
 }  // namespace ssv

@@ -218,13 +218,6 @@ struct ICDevice {
     // staged sweeps of oversized blocks: per position in rows_f / rows_b, the
     // row's entries (value index, column, position in the block or -1)
     DevBuf<int> sf_rp, sf_src, sf_col, sf_loc, sb_rp, sb_src, sb_col, sb_loc;
-    // one-launch sweeps (k_ic_sweep_all): work units in sweep order, units per
-    // colour stage, ticket / completion counters (zero between launches)
-    DevBuf<SweepUnit> swu[2];
-    DevBuf<int> swtot[2], swctr[2];
-    int swn[2] = {0, 0}, swsmem[2] = {0, 0};
-    bool swok[2] = {false, false};
-    bool sweep_one(int dir) const;
     DevBuf<int> erp, eci, esrc, urpe, ucie, usrce, isrc, dsrc;
     DevBuf<S> ev, uev, iv, dv;
     DevBuf<SL> ev_lo, uev_lo, iv_lo, dv_lo;
@@ -245,7 +238,7 @@ struct ICDevice {
     void apply_bwd(S* y, const KState* st, cudaStream_t s) const;        // tw -> y
     int kernels_per_apply() const {
         if (blk)
-            return (sweep_one(0) ? 1 : (int)fwd_cta.size()) + (sweep_one(1) ? 1 : (int)bwd_cta.size()) +
+            return (int)fwd_cta.size() + (int)bwd_cta.size() +
                    (scaled_apply ? 1 : 0);
         return (int)(fwd_launch.size() + bwd_launch.size()) + (scaled_apply ? 1 : 0);
     }

@@ -167,58 +167,6 @@ void KrylovWork<S>::ensure(int n_, int hist_cap) {
 // ---------------------------------------------------------------------------
 // IC(0)
 // ---------------------------------------------------------------------------
-// One launch per sweep (SSV_IC_SWEEP=one) instead of one launch per colour
-// (the default): correct (tested), but measured slower on the 64^3 ICCG
-// (forward sweep 69.7 vs 63.9 us) - the completion counters cost as much as
-// the launches they replace, which programmatic dependent launch already
-// overlaps.
-static bool sweep_one_enabled() {
-    static int v = -1;
-    if (v < 0) {
-        const char* e = std::getenv("SSV_IC_SWEEP");
-        v = (e && std::strcmp(e, "one") == 0) ? 1 : 0;
-    }
-    return v != 0;
-}
-
-template <typename S>
-bool ICDevice<S>::sweep_one(int dir) const {
-    return blk && swok[dir] && sweep_one_enabled();
-}
-
-template <typename S, typename SL, int L, bool FWD>
-static void launch_sweep_all(const ICDevice<S>& ic, const SL* xv, const SL* iv, const SL* dv, const SL* full,
-                             const S* x, const double* sc, S* y, const KState* st, cudaStream_t s) {
-    const int dir = FWD ? 0 : 1;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(std::max(1, std::min(ic.swn[dir], sm_count() * 2)));
-    cfg.blockDim = dim3(256);
-    cfg.dynamicSmemBytes = (size_t)ic.swsmem[dir];
-    cfg.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = pdl_enabled() ? 1 : 0;
-    SSV_CUDA(cudaLaunchKernelEx(&cfg, k_ic_sweep_all<S, SL, L, FWD>, ic.swn[dir],
-                                (const SweepUnit*)ic.swu[dir].get(), (const int*)ic.swtot[dir].get(),
-                                ic.swctr[dir].get(), (const int*)ic.uoff.get(),
-                                (const int*)(FWD ? ic.erp.get() : ic.urpe.get()),
-                                (const int*)(FWD ? ic.eci.get() : ic.ucie.get()), xv, iv, ic.tri, dv,
-                                (const int*)(FWD ? ic.lev_f.get() : ic.lev_b.get()),
-                                (const int*)(FWD ? ic.rows_f.get() : ic.rows_b.get()),
-                                (const int*)(FWD ? ic.sf_rp.get() : ic.sb_rp.get()),
-                                (const int*)(FWD ? ic.sf_src.get() : ic.sb_src.get()),
-                                (const int*)(FWD ? ic.sf_col.get() : ic.sb_col.get()),
-                                (const int*)(FWD ? ic.sf_loc.get() : ic.sb_loc.get()), (const int*)ic.Lrp.get(),
-                                full, x, sc, y, const_cast<KState*>(st)));
-}
-
-template <typename S, typename SL, int L>
-static void set_sweep_attr(int smem) {
-    SSV_CUDA(cudaFuncSetAttribute(k_ic_sweep_all<S, SL, L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    SSV_CUDA(cudaFuncSetAttribute(k_ic_sweep_all<S, SL, L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-}
 
 template <typename S>
 void ICDevice<S>::build_pattern(int n_, const std::vector<int>& rp, const std::vector<int>& ci,
@@ -467,54 +415,9 @@ void ICDevice<S>::build_pattern(int n_, const std::vector<int>& rp, const std::v
         };
         up(sf_rp, h_sf_rp); up(sf_src, h_sf_src); up(sf_col, h_sf_col); up(sf_loc, h_sf_loc);
         up(sb_rp, h_sb_rp); up(sb_src, h_sb_src); up(sb_col, h_sb_col); up(sb_loc, h_sb_loc);
-        // one-launch sweeps: units of blockDim / blk_lanes ordinary blocks, or one
-        // oversized block; stages = colours in sweep order
-        for (int dir = 0; dir < 2; ++dir) {
-            const std::vector<Launch>& L = dir == 0 ? fwd_cta : bwd_cta;
-            std::vector<SweepUnit> U;
-            std::vector<int> tot;
-            const int G = 256 / blk_lanes;
-            int stage = -1, last = -2, smax = 0;
-            bool ok = !L.empty();
-            for (const auto& g : L) {
-                if (g.color != last) {
-                    ++stage;
-                    last = g.color;
-                    tot.push_back(0);
-                }
-                if (g.kind == 0) {
-                    for (int a = g.a; a < g.b; a += G) {
-                        U.push_back({0, a, std::min(g.b, a + G), stage});
-                        ++tot[stage];
-                    }
-                } else {
-                    if (g.smem <= 0) ok = false;
-                    smax = std::max(smax, g.smem);
-                    U.push_back({2, g.a, g.b, stage});
-                    ++tot[stage];
-                }
-            }
-            swok[dir] = ok && !U.empty();
-            swn[dir] = (int)U.size();
-            swsmem[dir] = smax;
-            if (swok[dir]) {
-                swu[dir].upload(U.data(), U.size(), s);
-                swtot[dir].upload(tot.data(), tot.size(), s);
-                std::vector<int> zero(2 + tot.size(), 0);
-                swctr[dir].upload(zero.data(), zero.size(), s);
-            }
-        }
         if (staged_max > 0) {  // dynamic shared memory of the staged sweeps (<= optin - 1 KB)
             using SLo = typename ST<S>::lo;
             const int sm = staged_max;
-            switch (blk_lanes) {
-                case 1: set_sweep_attr<S, S, 1>(sm); set_sweep_attr<S, SLo, 1>(sm); break;
-                case 2: set_sweep_attr<S, S, 2>(sm); set_sweep_attr<S, SLo, 2>(sm); break;
-                case 4: set_sweep_attr<S, S, 4>(sm); set_sweep_attr<S, SLo, 4>(sm); break;
-                case 8: set_sweep_attr<S, S, 8>(sm); set_sweep_attr<S, SLo, 8>(sm); break;
-                case 16: set_sweep_attr<S, S, 16>(sm); set_sweep_attr<S, SLo, 16>(sm); break;
-                default: set_sweep_attr<S, S, 32>(sm); set_sweep_attr<S, SLo, 32>(sm); break;
-            }
             SSV_CUDA(cudaFuncSetAttribute(k_ic_sweep_staged<S, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
             SSV_CUDA(cudaFuncSetAttribute(k_ic_sweep_staged<S, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
             SSV_CUDA(cudaFuncSetAttribute(k_ic_sweep_staged<S, SLo, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
@@ -708,16 +611,6 @@ static void launch_bwd_blk(const ICDevice<S>& ic, const SL* uev, const SL* iv, c
     }
 }
 
-#define SSV_SWEEP_DISPATCH(SLT, FWD, ...)                                       \
-    switch (blk_lanes) {                                                         \
-        case 1: launch_sweep_all<S, SLT, 1, FWD>(*this, __VA_ARGS__); break;     \
-        case 2: launch_sweep_all<S, SLT, 2, FWD>(*this, __VA_ARGS__); break;     \
-        case 4: launch_sweep_all<S, SLT, 4, FWD>(*this, __VA_ARGS__); break;     \
-        case 8: launch_sweep_all<S, SLT, 8, FWD>(*this, __VA_ARGS__); break;     \
-        case 16: launch_sweep_all<S, SLT, 16, FWD>(*this, __VA_ARGS__); break;   \
-        default: launch_sweep_all<S, SLT, 32, FWD>(*this, __VA_ARGS__); break;   \
-    }
-
 #define SSV_BLK_DISPATCH(FN, SLT, ...)                         \
     switch (blk_lanes) {                                      \
         case 1: FN<S, SLT, 1>(__VA_ARGS__); break;            \
@@ -733,13 +626,7 @@ void ICDevice<S>::apply_fwd(const S* x, const KState* st, cudaStream_t s) const 
     const int* uo = abmc ? uoff.get() : nullptr;
     const double* sc = scaled_apply ? scaling.get() : nullptr;
     if (blk) {
-        if (sweep_one(0)) {
-            if (lo) {
-                SSV_SWEEP_DISPATCH(SL, true, ev_lo.get(), iv_lo.get(), dv_lo.get(), Lv_lo.get(), x, sc, tw.get(), st, s)
-            } else {
-                SSV_SWEEP_DISPATCH(S, true, ev.get(), iv.get(), dv.get(), Lv.get(), x, sc, tw.get(), st, s)
-            }
-        } else if (lo) {
+        if (lo) {
             SSV_BLK_DISPATCH(launch_fwd_blk, SL, *this, ev_lo.get(), iv_lo.get(), dv_lo.get(), x, sc, st, s)
         } else {
             SSV_BLK_DISPATCH(launch_fwd_blk, S, *this, ev.get(), iv.get(), dv.get(), x, sc, st, s)
@@ -765,15 +652,7 @@ void ICDevice<S>::apply_bwd(S* y, const KState* st, cudaStream_t s) const {
     const int* uo = abmc ? uoff.get() : nullptr;
     const double* sc = scaled_apply ? scaling.get() : nullptr;
     if (blk) {
-        if (sweep_one(1)) {
-            if (lo) {
-                SSV_SWEEP_DISPATCH(SL, false, uev_lo.get(), iv_lo.get(), inv_lo.get(), Uv_lo.get(), tw.get(),
-                                   (const double*)nullptr, y, st, s)
-            } else {
-                SSV_SWEEP_DISPATCH(S, false, uev.get(), iv.get(), inv.get(), Uv.get(), tw.get(), (const double*)nullptr,
-                                   y, st, s)
-            }
-        } else if (lo) {
+        if (lo) {
             SSV_BLK_DISPATCH(launch_bwd_blk, SL, *this, uev_lo.get(), iv_lo.get(), inv_lo.get(), y, st, s)
         } else {
             SSV_BLK_DISPATCH(launch_bwd_blk, S, *this, uev.get(), iv.get(), inv.get(), y, st, s)

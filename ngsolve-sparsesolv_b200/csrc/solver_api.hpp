@@ -62,13 +62,6 @@ int ams_precision(const AmsState* a);
 void ams_reserve_block(AmsState* a, int nrhs);
 void ams_profile(AmsState* a, int nrhs, int reps, int flags, ssv_phase_profile* out);
 void ams_apply_block(AmsState* a, const double* in, double* out, int nrhs, const KState* st, cudaStream_t s);
-// The same for F distinct preconditioners at once, their cycles in lockstep;
-// false (nothing launched) when their hierarchies do not line up.
-// Whole-V-cycle cooperative launches off (on = true) while the batched solver
-// captures its concurrent per-frequency branches.
-void ams_grid_suspend(bool on);
-bool ams_apply_block_multi(AmsState* const* A, int F, const double* const* in, double* const* out, int nrhs,
-                           const KState* st, cudaStream_t s);
 
 // Batched COCR over a frequency family (batch.cu)
 ssv_batch* batch_create(ssv_matrix* K, ssv_matrix* M, int F, const double* omegas, ssv_precond* const* pre, int R,

@@ -302,24 +302,6 @@ def test_fp32_complex_apply_well_conditioned(eddy_well):
 
 
 @pytest.mark.parametrize("complex_form", [False, True])
-def test_cluster_tail_and_launch_chain_agree(mag_well, eddy_well, monkeypatch, complex_form):
-    # SSV_AMS_TAIL_NNZ=200000 runs whole V-cycles of these small hierarchies in
-    # the cluster tail kernel; 0 (the default) keeps the per-level launch chain
-    d = eddy_well if complex_form else mag_well
-    rng = np.random.default_rng(11)
-    n = d["A"].shape[0]
-    b = rng.standard_normal(n) + (1j * rng.standard_normal(n) if complex_form else 0)
-    monkeypatch.setenv("SSV_AMS_TAIL_NNZ", "200000")
-    y_tail = _ams(d, complex_form=complex_form) * b
-    monkeypatch.setenv("SSV_AMS_TAIL_NNZ", "0")
-    y_chain = _ams(d, complex_form=complex_form) * b
-    assert np.abs(y_tail - y_chain).max() <= APPLY_RTOL_WELL * np.abs(y_chain).max()
-    o = O.AmsOracle(d["a_real"] if complex_form else d["A"], d["G"], d["freedofs"], *d["coords"])
-    yo = o.apply_complex(b) if complex_form else o.apply(b)
-    assert np.abs(y_tail - yo).max() <= APPLY_RTOL_WELL * np.abs(yo).max()
-
-
-@pytest.mark.parametrize("complex_form", [False, True])
 def test_lockstep_nodal_cycles_and_branches_agree(mag_well, eddy_well, monkeypatch, complex_form):
     # by default the three nodal V-cycles run as one chain of launches over
     # all three hierarchies; SSV_AMS_TRI=0 runs them as three graph branches
