@@ -38,12 +38,16 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "ngsolve-sparsesolv_b200"))
 
 METRIC = "time-to-solution @1e-10 (s), ms/iter, SpMV HBM GB/s: mixed/batched vs plain FP64 GPU"
 UNIT = "s"
+# dram__bytes_read.sum + dram__bytes_write.sum of one eddy64 fine-residual launch (ncu; None until captured)
+EDDY_FINE_RESIDUAL_TRAFFIC = None
 
 
 def _peaks():
@@ -282,53 +286,6 @@ def run_reference_ams(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def batched_family_extra(ss, nc=40):
-    """Batched COCR (8 frequencies x 4 right-hand sides, FP64 preconditioners) vs 32 sequential solves."""
-    import numpy as np
-    from sparsesolv_ngsolve import hcurl as H
-    d = H.eddy_family(nc, nrhs=4)
-    fd = d["freedofs"].astype(bool)
-    pres = [ss.ComplexCompactAMSPreconditioner(a, d["G"], freedofs=d["freedofs"], coord_x=d["coords"][0],
-                                               coord_y=d["coords"][1], coord_z=d["coords"][2])
-            for a in d["a_real"]]
-    bs = ss.BatchedCOCRSolver(d["K"], d["M"], d["omegas"], pres, nrhs=4, freedofs=d["freedofs"], maxiter=1000,
-                              tol=1e-10)
-    bs.Solve(d["B"])
-    walls = []
-    for _ in range(2):
-        t0 = time.perf_counter()
-        X = bs.Solve(d["B"])
-        walls.append(time.perf_counter() - t0)
-    tm = bs.last_timing
-    its_b = bs.iterations.copy()
-
-    def tres(f, x, b):
-        return float(np.linalg.norm((b - d["A"][f] @ np.where(fd, x, 0))[fd]) / np.linalg.norm(b[fd]))
-
-    tr_b = max(tres(f, X[f, r], d["B"][f, r]) for f in range(8) for r in range(4))
-    seq, its_s, tr_s = 0.0, [], 0.0
-    for f in range(8):
-        inv = ss.COCRSolver(d["A"][f], pres[f], freedofs=d["freedofs"], maxiter=1000, tol=1e-10)
-        inv * d["B"][f, 0]
-        for r in range(4):
-            t0 = time.perf_counter()
-            x = inv * d["B"][f, r]
-            seq += time.perf_counter() - t0
-            its_s.append(inv.iterations)
-            tr_s = max(tr_s, tres(f, x, d["B"][f, r]))
-    return {"family": f"complex eddy current on the {nc}^3 Kuhn mesh ({d['K'].shape[0]} edges), 8 frequencies "
-                      f"1 kHz..100 kHz x 4 loop sources (default_rng(1)), ComplexCompactAMS per frequency (FP64) "
-                      f"+ COCR, tol 1e-10",
-            "batched_s": min(walls), "batched_device_ms": tm["device_ms"], "batched_loops": tm["loops"],
-            "batched_kernel_launches": tm["kernel_launches"], "sequential_fp64_s": seq,
-            "speedup": seq / min(walls), "iterations_batched": its_b.ravel().tolist(), "iterations_sequential": its_s,
-            "max_true_residual_batched": tr_b, "max_true_residual_sequential": tr_s,
-            "autotuned_spmm": bs.tuning["chosen"],
-            "fp32_preconditioner": "not used: COCR with an FP32-rounded preconditioner stops at a true residual of "
-                                   "~1e-7 on these systems (the FP64 oracle with only its output rounded to FP32 "
-                                   "does the same), above the 1e-10 target"}
-
-
 def run_ams(args, rank, world, local):
     import numpy as np
     import torch
@@ -353,7 +310,7 @@ def run_ams(args, rank, world, local):
     d_b = torch.from_numpy(np.ascontiguousarray(d["f"])).to(dev)
     d_x = torch.zeros(n, dtype=torch.float64, device=dev)
     cfg = _capi.default_config(tolerance=1e-10, max_iterations=500)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev).fill_(1.0)  # > 126 MB L2
     t0 = time.perf_counter()
     pre = _ams_pre(ss, d, "fp64")
     setup_s = time.perf_counter() - t0
@@ -369,8 +326,7 @@ def run_ams(args, rank, world, local):
     def timed_steps(k):
         ms, launches, iters, conv = [], 0, 0, True
         for _ in range(k):
-            flush.fill_(1.0)
-            torch.cuda.synchronize()
+            _l2_evict(flush)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
@@ -460,8 +416,7 @@ def run_ams(args, rank, world, local):
         solver.Solve(d["f"], xh)
     e2e_ms = []
     for _ in range(max(3, args.steps // 2)):
-        flush.fill_(1.0)
-        torch.cuda.synchronize()
+        _l2_evict(flush)
         xh[:] = 0
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -471,7 +426,7 @@ def run_ams(args, rank, world, local):
         torch.cuda.synchronize()
         e2e_ms.append(e0.elapsed_time(e1))
     value = head["ms_per_step"] / 1e3
-    config = dict(AMS_DESC, parallelism=f"replicas{world}", l2="flushed between timed steps (256 MB write)",
+    config = dict(AMS_DESC, parallelism=f"replicas{world}", l2="evicted between timed steps (256 MB read)",
                   form="mixed: FP32 subspace AMG hierarchies (diagonally scaled); the three nodal V-cycles "
                        "through the fused level products (down b' = R b, up x = U [b; e]: two launches per level), "
                        "the gradient V-cycle in four passes (fused, it loses too much in FP32); FP64 fine level in "
@@ -487,11 +442,6 @@ def run_ams(args, rank, world, local):
                               "true_rel_residual": plain["true_rel_residual"]},
                   speedup_mixed_vs_plain=plain["ms_per_step"] / mixed["ms_per_step"],
                   ams_setup_s=setup_s)
-    if not args.no_extras and rank == 0:
-        try:
-            config["batched_family"] = batched_family_extra(ss)
-        except Exception as exc:  # reported, not hidden
-            config["batched_family"] = {"error": repr(exc)}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64 Krylov + f32 preconditioner hierarchy",
@@ -513,14 +463,15 @@ def run_ams(args, rank, world, local):
 
 
 # ---------------------------------------------------------------------------
-# Complex eddy current at 64^3 (ComplexCompactAMS + COCR)
+# Complex eddy current at 64^3 (ComplexCompactAMS + COCR): the default workload
 # ---------------------------------------------------------------------------
 EDDY_DESC = {"workload": "eddy64: complex eddy current A = K + j omega sigma M_cond, Kuhn 6-tet mesh of a 64^3 cube "
-                         "(1,872,064 edges, complex<double>), omega = 2 pi 3e4, sigma = 5.8e7 in a copper annulus, "
-                         "nu_r = 1e-3 core, auxiliary K + |omega| sigma M + 1e-6 nu M, ComplexCompactAMS (cycle 1) + "
-                         "COCR, tol 1e-10",
+                         "(1,872,064 edges, 30,331,072 nnz, complex<double>), omega = 2 pi 3e4, sigma = 5.8e7 in a "
+                         "copper annulus, nu_r = 1e-3 core, auxiliary K + |omega| sigma M + 1e-6 nu M, "
+                         "ComplexCompactAMS (cycle 1) + COCR, tol 1e-10",
              "tol": 1e-10, "rhs": "square loop currents at mid-height (discretely divergence-free)"}
-EDDY_CPU_ITERS = 30
+REFINE_DROP = 1e-5
+EDDY_MAXITER = 3000
 
 
 def _eddy_system():
@@ -528,9 +479,19 @@ def _eddy_system():
     return H.eddy_current(64)
 
 
-def cpu_eddy_sample(d, gpu_iters):
-    """ComplexCompactAMS restatement + COCRSolverNGS on all host cores, EDDY_CPU_ITERS
-    iterations (a bounded sample), extrapolated to the GPU's iteration count."""
+def _rel_err(x, xref):
+    return float(np.linalg.norm(x - xref) / max(np.linalg.norm(xref), 1e-300))
+
+
+def _eddy_true_res(d, x):
+    fdm = d["freedofs"].astype(bool)
+    return float(np.linalg.norm((d["f"] - d["A"] @ np.where(fdm, x, 0))[fdm]) / np.linalg.norm(d["f"][fdm]))
+
+
+def cpu_eddy_full(d):
+    """One full solve of the workload with the ComplexCompactAMS restatement +
+    COCRSolverNGS on all host cores (NGSolve, which the reference's AMS needs,
+    is absent); returns the baseline record and the solution."""
     from oracle import oracle as O
     cores = os.cpu_count() or 1
     O.AmsOracle.set_threads(cores)
@@ -538,13 +499,14 @@ def cpu_eddy_sample(d, gpu_iters):
     o = O.AmsOracle(d["a_real"], d["G"], d["freedofs"], *d["coords"])
     setup = time.perf_counter() - t0
     t0 = time.perf_counter()
-    _, its = o.cocr(d["A"], d["f"], freedofs=d["freedofs"], maxiter=EDDY_CPU_ITERS, tol=1e-10)[:2]
+    x, its, _ = o.cocr(d["A"], d["f"], freedofs=d["freedofs"], maxiter=EDDY_MAXITER, tol=1e-10)
     wall = time.perf_counter() - t0
-    per_it = wall / max(int(its), 1)
-    return {"value": per_it * gpu_iters, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{int(its)} COCR iterations of the workload with the ComplexCompactAMS restatement on {cores} "
-                      f"OpenMP threads ({per_it * 1e3:.1f} ms per iteration, preconditioner set-up {setup:.1f} s), "
-                      f"extrapolated to the {gpu_iters} iterations of the full solve"}
+    rec = {"value": wall, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"1 full COCR solve of the workload ({int(its)} iterations, {wall / max(int(its), 1) * 1e3:.1f} "
+                     f"ms per iteration) with the ComplexCompactAMS restatement on {cores} OpenMP threads, "
+                     f"preconditioner built (its set-up took {setup:.1f} s)",
+           "iterations": int(its), "true_rel_residual": _eddy_true_res(d, x), "setup_s": setup}
+    return rec, x
 
 
 def run_reference_eddy(args, rank, world):
@@ -555,28 +517,141 @@ def run_reference_eddy(args, rank, world):
     cores = os.cpu_count() or 1
     O.AmsOracle.set_threads(cores)
     o = O.AmsOracle(d["a_real"], d["G"], d["freedofs"], *d["coords"])
-    # one full solve for the iteration count (about a minute), then bounded samples
-    full_iters = int(o.cocr(d["A"], d["f"], freedofs=d["freedofs"], maxiter=3000, tol=1e-10)[1])
-    per_it = []
-    for _ in range(args.steps):
+    for _ in range(args.warmup):  # warm-up: bounded samples (5 COCR iterations), untimed
+        o.cocr(d["A"], d["f"], freedofs=d["freedofs"], maxiter=5, tol=1e-10)
+    times, iters, x = [], 0, None
+    for _ in range(args.steps):  # every timed step is one full solve to tolerance
         t0 = time.perf_counter()
-        _, its = o.cocr(d["A"], d["f"], freedofs=d["freedofs"], maxiter=EDDY_CPU_ITERS, tol=1e-10)[:2]
-        per_it.append((time.perf_counter() - t0) / max(int(its), 1))
-    v = statistics.mean(per_it) * full_iters
+        x, its, _ = o.cocr(d["A"], d["f"], freedofs=d["freedofs"], maxiter=EDDY_MAXITER, tol=1e-10)
+        times.append(time.perf_counter() - t0)
+        iters = int(its)
+    v = statistics.mean(times)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": dict(EDDY_DESC, iterations=full_iters, ms_per_iter=statistics.mean(per_it) * 1e3),
+            "config": dict(EDDY_DESC, iterations=iters, ms_per_iter=v * 1e3 / max(iters, 1),
+                           true_rel_residual=_eddy_true_res(d, x)),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{args.steps} samples of {EDDY_CPU_ITERS} COCR iterations with the "
-                                       f"ComplexCompactAMS restatement on {cores} OpenMP threads, scaled to the "
-                                       f"{full_iters} iterations of its full solve"},
+                             "sample": f"{args.steps} full COCR solves ({iters} iterations each) with the "
+                                       f"ComplexCompactAMS restatement on {cores} OpenMP threads; warm-up steps are "
+                                       f"5-iteration samples"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
+def _l2_evict(buf):
+    """Evicts L2 by reading a buffer larger than it (a read leaves clean lines:
+    no write-back for the next kernel to pay)."""
+    import torch
+    buf.sum()
+    torch.cuda.synchronize()
+
+
+def batched_family_extra(ss, nc=40):
+    """Config 4: the 40^3 eddy-current family, 8 frequencies x 4 sources (32
+    systems). The mixed batched form (FP32-form ComplexCompactAMS per
+    frequency, refined COCR cycles to a true residual of 1e-10, one launch
+    graph with the autotuned SpMM) against 32 sequential plain FP64 GPU solves
+    (COCRSolver, FP64 ComplexCompactAMS); the FP64 batched form beside it.
+    Device time (CUDA events), inputs resident in HBM."""
+    import torch
+
+    from oracle import oracle as O
+    from sparsesolv_ngsolve import _capi
+    from sparsesolv_ngsolve import hcurl as H
+    lib = _capi.load()
+    dev = torch.device("cuda:0")
+    d = H.eddy_family(nc, nrhs=4)
+    F, R, n = len(d["omegas"]), 4, d["K"].shape[0]
+    fdm = d["freedofs"].astype(bool)
+    pres = [ss.ComplexCompactAMSPreconditioner(a, d["G"], freedofs=d["freedofs"], coord_x=d["coords"][0],
+                                               coord_y=d["coords"][1], coord_z=d["coords"][2])
+            for a in d["a_real"]]
+    d_B = torch.from_numpy(np.ascontiguousarray(d["B"]).view(np.float64).reshape(-1)).to(dev)
+    d_X = torch.zeros_like(d_B)
+
+    def tres(f, x, b):
+        return float(np.linalg.norm((b - d["A"][f] @ np.where(fdm, x, 0))[fdm]) / np.linalg.norm(b[fdm]))
+
+    def timed(fn, reps=2):
+        fn()
+        out = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1) / 1e3)
+        return min(out)
+
+    # 32 sequential plain FP64 solves (the drop-in, one system at a time)
+    mats = [ss._Matrix(a) for a in d["A"]]
+    d_fd = torch.from_numpy(np.ascontiguousarray(d["freedofs"].astype(np.uint8))).to(dev)
+    d_b1 = torch.zeros(2 * n, dtype=torch.float64, device=dev)
+    d_x1 = torch.zeros(2 * n, dtype=torch.float64, device=dev)
+    seq_x = np.zeros_like(d["B"])
+    its_seq = np.zeros((F, R), np.int32)
+
+    def seq_all(keep=False):
+        it = ctypes.c_int32()
+        for f in range(F):
+            for r in range(R):
+                d_b1.copy_(d_B.view(F, R, 2 * n)[f, r])
+                _capi.check(lib.ssv_cocr_solve_dev(mats[f].h, pres[f]._h, ctypes.cast(d_fd.data_ptr(), _capi.PU8),
+                                                   1000, 1e-10, 0, ctypes.c_void_p(d_b1.data_ptr()),
+                                                   ctypes.c_void_p(d_x1.data_ptr()), ctypes.byref(it)))
+                if keep:
+                    seq_x[f, r] = d_x1.cpu().numpy().view(np.complex128)
+                    its_seq[f, r] = it.value
+    seq_all(keep=True)
+    t_seq = timed(seq_all, reps=1)
+    out = {"family": f"complex eddy current on the {nc}^3 Kuhn mesh ({n} edges), 8 frequencies 1 kHz..100 kHz x 4 "
+                     f"loop sources (default_rng(1)), ComplexCompactAMS per frequency + COCR, tol 1e-10",
+           "sequential_fp64_s": t_seq, "iterations_sequential": its_seq.ravel().tolist(),
+           "max_true_residual_sequential": max(tres(f, seq_x[f, r], d["B"][f, r]) for f in range(F) for r in range(R))}
+    # batched, FP64 preconditioners, the reference recurrence per column
+    bs = ss.BatchedCOCRSolver(d["K"], d["M"], d["omegas"], pres, nrhs=4, freedofs=d["freedofs"], maxiter=1000,
+                              tol=1e-10)
+    out["batched_fp64_s"] = timed(lambda: bs.solve_dev(d_B.data_ptr(), d_X.data_ptr()))
+    X = d_X.cpu().numpy().view(np.complex128).reshape(F, R, n)
+    out["iterations_batched_fp64"] = bs.iterations.ravel().tolist()
+    out["max_true_residual_batched_fp64"] = max(tres(f, X[f, r], d["B"][f, r]) for f in range(F) for r in range(R))
+    del bs
+    # the mixed batched form
+    for p in pres:
+        p.precision = "fp32"
+    bm = ss.BatchedCOCRSolver(d["K"], d["M"], d["omegas"], pres, nrhs=4, freedofs=d["freedofs"], maxiter=1500,
+                              tol=1e-10, restart_drop=REFINE_DROP)
+    out["batched_mixed_s"] = timed(lambda: bm.solve_dev(d_B.data_ptr(), d_X.data_ptr()))
+    tm = bm.last_timing
+    X = d_X.cpu().numpy().view(np.complex128).reshape(F, R, n)
+    out.update({"iterations_batched_mixed": bm.iterations.ravel().tolist(), "batched_mixed_cycles": tm["cycles"],
+                "batched_mixed_kernel_launches": tm["kernel_launches"],
+                "max_true_residual_batched_mixed": max(tres(f, X[f, r], d["B"][f, r])
+                                                       for f in range(F) for r in range(R)),
+                "batched_mixed_all_converged": bool(bm.converged.all()),
+                "max_error_mixed_vs_sequential_fp64": max(_rel_err(X[f, r], seq_x[f, r])
+                                                          for f in range(F) for r in range(R)),
+                "autotuned_spmm": bm.tuning["chosen"]})
+    out["speedup_batched_mixed_vs_sequential_fp64"] = t_seq / out["batched_mixed_s"]
+    out["speedup_batched_fp64_vs_sequential_fp64"] = t_seq / out["batched_fp64_s"]
+    # two columns against the FP64 restatement (the lowest and highest frequency)
+    O.AmsOracle.set_threads(os.cpu_count() or 1)
+    errs = []
+    for f in (0, F - 1):
+        o = O.AmsOracle(d["a_real"][f], d["G"], d["freedofs"], *d["coords"])
+        xo, _, _ = o.cocr(d["A"][f], d["B"][f, 0], freedofs=d["freedofs"], maxiter=1000, tol=1e-10)
+        errs.append(_rel_err(X[f, 0], xo))
+    out["error_mixed_vs_reference_f0_f7"] = errs
+    del bm
+    for p in pres:
+        p.precision = "fp64"
+    return out
+
+
 def run_eddy(args, rank, world, local):
-    import numpy as np
     import torch
 
     import sparsesolv_ngsolve as ss
@@ -598,50 +673,85 @@ def run_eddy(args, rank, world, local):
     d_fd = torch.from_numpy(np.ascontiguousarray(d["freedofs"].astype(np.uint8))).to(dev)
     d_b = torch.from_numpy(np.ascontiguousarray(d["f"]).view(np.float64)).to(dev)
     d_x = torch.zeros(2 * n, dtype=torch.float64, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev).fill_(1.0)  # > 126 MB L2
     t0 = time.perf_counter()
     pre = ss.ComplexCompactAMSPreconditioner(d["a_real"], d["G"], freedofs=d["freedofs"], coord_x=d["coords"][0],
                                              coord_y=d["coords"][1], coord_z=d["coords"][2])
     setup_s = time.perf_counter() - t0
-    maxiter = 3000
+    setup_times = pre.setup_times
+    fdp = ctypes.cast(d_fd.data_ptr(), _capi.PU8)
+    info = _capi.ssv_refine_info()
+    nl = ctypes.c_int64()
 
-    def solve_dev():
-        d_x.zero_()
+    def solve_plain():
         its = ctypes.c_int32()
-        _capi.check(lib.ssv_cocr_solve_dev(mat.h, pre._h, ctypes.cast(d_fd.data_ptr(), _capi.PU8), maxiter,
-                                           1e-10, 0, ctypes.c_void_p(d_b.data_ptr()), ctypes.c_void_p(d_x.data_ptr()),
-                                           ctypes.byref(its)))
-        return its.value
+        _capi.check(lib.ssv_cocr_solve_dev(mat.h, pre._h, fdp, EDDY_MAXITER, 1e-10, 0, ctypes.c_void_p(d_b.data_ptr()),
+                                           ctypes.c_void_p(d_x.data_ptr()), ctypes.byref(its)))
+        return its.value, 1
 
-    for _ in range(args.warmup):
-        solve_dev()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
-    ms, iters = [], 0
-    for _ in range(args.steps):
-        flush.fill_(1.0)
+    def solve_mixed():
+        _capi.check(lib.ssv_cocr_refined_solve_dev(mat.h, pre._h, fdp, EDDY_MAXITER, 1e-10, REFINE_DROP, 0,
+                                                   ctypes.c_void_p(d_b.data_ptr()), ctypes.c_void_p(d_x.data_ptr()),
+                                                   ctypes.byref(info)))
+        return info.iterations, info.cycles
+
+    def timed_form(fn, sample_clocks):
+        for _ in range(args.warmup):
+            fn()
         torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        iters = solve_dev()
-        e1.record()
-        torch.cuda.synchronize()
-        ms.append(e0.elapsed_time(e1))
-    clock_info = clocks.stop()
-    total_ms = sum(ms)
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    x = d_x.cpu().numpy().view(np.complex128)
-    fdm = d["freedofs"].astype(bool)
-    tres = float(np.linalg.norm((d["f"] - A @ np.where(fdm, x, 0))[fdm]) / np.linalg.norm(d["f"][fdm]))
+        if dist:
+            dist.barrier()
+        clocks = ClockSampler(local) if sample_clocks else None
+        if clocks:
+            clocks.start()
+        ms, iters, cycles, launches = [], 0, 0, 0
+        for _ in range(args.steps):
+            _l2_evict(flush)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            iters, cycles = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            _capi.check(lib.ssv_cocr_last_launches(ctypes.byref(nl)))
+            launches += nl.value
+        clock_info = clocks.stop() if clocks else None
+        total_ms = sum(ms)
+        if dist:
+            t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        x = d_x.cpu().numpy().view(np.complex128).copy()
+        return {"s": total_ms / args.steps / 1e3, "iterations": iters, "cycles": cycles, "launches": launches,
+                "clocks": clock_info, "x": x, "true_rel_residual": _eddy_true_res(d, x)}
+
+    plain = timed_form(solve_plain, True)
     prof = pre.profile(nrhs=1, reps=10)
     prof_cold = pre.profile(nrhs=1, reps=5, cold=True)
+    # end to end through the public API with host buffers (the drop-in COCRSolver)
+    inv = ss.COCRSolver(A, pre, freedofs=d["freedofs"], maxiter=EDDY_MAXITER, tol=1e-10)
+
+    def e2e(solver, reps):
+        solver * d["f"]
+        out = []
+        for _ in range(reps):
+            _l2_evict(flush)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            solver * d["f"]
+            e1.record()
+            torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1) / 1e3)
+        return statistics.mean(out)
+
+    e2e_plain = e2e(inv, max(2, args.steps // 4))
+    pre.precision = "fp32"
+    mixed = timed_form(solve_mixed, False)
+    invm = ss.MixedCOCRSolver(A, pre, freedofs=d["freedofs"], maxiter=EDDY_MAXITER, tol=1e-10,
+                              restart_drop=REFINE_DROP)
+    e2e_mixed = e2e(invm, max(2, args.steps // 4))
+    prof_mixed = pre.profile(nrhs=1, reps=10)
+    pre.precision = "fp64"
     peak, peak_kind = _peaks()
 
     def gbps(p):
@@ -650,46 +760,62 @@ def run_eddy(args, rank, world, local):
     spmv = next(p for p in prof_cold if p["name"] == "fine_residual")
     spmv_warm = next(p for p in prof if p["name"] == "fine_residual")
     roofline = {"bound": "hbm", "achieved": gbps(spmv), "peak": peak, "unit": "GB/s", "frac": gbps(spmv) / peak,
-                "traffic": None,
-                "kernel": "k_sell_spmv fine residual (A_bc real in 32-row sliced-ELL, Re/Im columns, 30.3M nnz, "
-                          "FP64; tuner-chosen over the CSR shapes), L2 flushed before each launch",
+                "traffic": EDDY_FINE_RESIDUAL_TRAFFIC,
+                "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one launch of this kernel (ncu, same "
+                                "workload), per launch",
+                "kernel": "k_sell_spmv fine residual (A_bc real in 32-row sliced-ELL, Re/Im columns, 30.3M nnz, FP64; "
+                          "tuner-chosen over the CSR shapes), each launch timed alone after evicting L2 by reading a "
+                          "256 MB buffer",
                 "peak_kind": peak_kind, "algorithmic_bytes_per_launch": spmv["bytes"], "launch_ms": spmv["ms"],
                 "warm_GBps": gbps(spmv_warm),
                 "phases_cold": [{**p, "GBps": gbps(p)} for p in prof_cold],
-                "phases": [{**p, "GBps": gbps(p)} for p in prof]}
-    # end to end through the public API with host buffers
-    inv = ss.COCRSolver(A, pre, freedofs=d["freedofs"], maxiter=maxiter, tol=1e-10)
-    inv * d["f"]
-    e2e_ms = []
-    for _ in range(max(2, args.steps // 2)):
-        flush.fill_(1.0)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        inv * d["f"]
-        e1.record()
-        torch.cuda.synchronize()
-        e2e_ms.append(e0.elapsed_time(e1))
-    value = total_ms / args.steps / 1e3
-    config = dict(EDDY_DESC, parallelism=f"replicas{world}", l2="flushed between timed steps (256 MB write)",
-                  form="plain FP64 (COCR carries M^-1 r by recurrence, so an FP32-rounded preconditioner stops it "
-                       "near a true residual of 1e-7, above the 1e-10 target: the mixed form serves CG only)",
-                  iterations=iters, ms_per_iter=value * 1e3 / max(iters, 1), spmv_GBps=gbps(spmv),
-                  true_rel_residual=tres, ams_setup_s=setup_s)
+                "phases": [{**p, "GBps": gbps(p)} for p in prof],
+                "phases_mixed": [{**p, "GBps": gbps(p)} for p in prof_mixed]}
+    value = plain["s"]
+    config = dict(EDDY_DESC, parallelism=f"replicas{world}",
+                  l2="evicted between timed steps (256 MB read)",
+                  form="plain FP64 (the drop-in: COCRSolverNGS recurrence, FP64 ComplexCompactAMS)",
+                  iterations=plain["iterations"], ms_per_iter=value * 1e3 / max(plain["iterations"], 1),
+                  spmv_GBps=gbps(spmv), true_rel_residual=plain["true_rel_residual"], ams_setup_s=setup_s,
+                  ams_setup_breakdown_s=setup_times,
+                  mixed_form="FP32-form ComplexCompactAMS (subspace hierarchies FP32, diagonally scaled; fine level, "
+                             "transfers, coarsest solves FP64) under refined COCR: cycles restarted from the FP64 true "
+                             f"residual after a {REFINE_DROP:g} drop, stop on the true residual",
+                  mixed_time_to_solution_s=mixed["s"], mixed_iterations=mixed["iterations"],
+                  mixed_cycles=mixed["cycles"], mixed_true_rel_residual=mixed["true_rel_residual"],
+                  mixed_ms_per_iter=mixed["s"] * 1e3 / max(mixed["iterations"], 1),
+                  speedup_mixed_vs_plain=value / mixed["s"],
+                  error_mixed_vs_plain=_rel_err(mixed["x"], plain["x"]),
+                  e2e_mixed_s=e2e_mixed)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic", "config": config,
-            "e2e": {"value": statistics.mean(e2e_ms) / 1e3, "unit": UNIT,
+            "e2e": {"value": e2e_plain, "unit": UNIT,
                     # b and x, the FreeDofs mask, and the complex matrix values re-read every call
                     "h2d_bytes_per_step": int(2 * n * 16 + n + A.nnz * 16),
                     "d2h_bytes_per_step": int(n * 16)},
-            "roofline": roofline, "gpu_launches": None, "clocks": clock_info}
+            "roofline": roofline, "gpu_launches": int(plain["launches"]), "clocks": plain["clocks"]}
+    if rank == 0 and not args.no_extras:
+        try:
+            bf = batched_family_extra(ss)
+            config["batched_family"] = bf
+            for k in ("batched_mixed_s", "sequential_fp64_s", "batched_fp64_s",
+                      "speedup_batched_mixed_vs_sequential_fp64", "speedup_batched_fp64_vs_sequential_fp64",
+                      "max_true_residual_batched_mixed", "max_error_mixed_vs_sequential_fp64"):
+                config[k] = bf[k]
+        except Exception as exc:  # reported, not hidden
+            config["batched_family"] = {"error": repr(exc)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_eddy_sample(d, iters)
+        cb, xref = cpu_eddy_full(d)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        config["reference_iterations"] = cb["iterations"]
+        config["reference_true_rel_residual"] = cb["true_rel_residual"]
+        config["reference_setup_s"] = cb["setup_s"]
+        config["error_vs_reference"] = _rel_err(plain["x"], xref)
+        config["mixed_error_vs_reference"] = _rel_err(mixed["x"], xref)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    del inv
+    del inv, invm
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -701,7 +827,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="ams40", choices=["ams40", "iccg64", "eddy64"])
+    ap.add_argument("--workload", default="eddy64", choices=["eddy64", "ams40", "iccg64"])
     ap.add_argument("--no-extras", action="store_true", help="skip the batched-family measurement")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"], help="AMS form of --ncu-case")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -755,7 +881,7 @@ def main():
     c = _capi.default_config(tolerance=cfg["tol"], max_iterations=cfg["maxiter"], shift_parameter=cfg["shift"],
                              use_abmc=cfg["use_abmc"], abmc_block_size=cfg["abmc_block_size"],
                              abmc_num_colors=cfg["abmc_num_colors"])
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev).fill_(1.0)  # > 126 MB L2
 
     def solve_dev(keep=None):
         h = ctypes.c_void_p()
@@ -781,8 +907,7 @@ def main():
     step_ms, launches, iters, conv = [], 0, 0, True
     setup_s, solve_s = [], []
     for _ in range(args.steps):
-        flush.fill_(1.0)
-        torch.cuda.synchronize()
+        _l2_evict(flush)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -813,8 +938,7 @@ def main():
     hwarm = keep[0]
     warm_ms = []
     for _ in range(max(3, args.steps // 2)):
-        flush.fill_(1.0)
-        torch.cuda.synchronize()
+        _l2_evict(flush)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         d_x.zero_()
@@ -851,8 +975,7 @@ def main():
         solver.Solve(b, xh)
     e2e_ms = []
     for _ in range(max(3, args.steps // 2)):
-        flush.fill_(1.0)
-        torch.cuda.synchronize()
+        _l2_evict(flush)
         xh[:] = 0
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -869,7 +992,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(desc, iterations=iters, converged=conv, parallelism=f"replicas{world}",
-                           l2="flushed between timed steps (256 MB write)",
+                           l2="evicted between timed steps (256 MB read)",
                            cold_setup_s=statistics.mean(setup_s), cold_iterate_s=statistics.mean(solve_s),
                            warm_time_to_solution_s=statistics.mean(warm_ms) / 1e3,
                            ms_per_iter_warm=statistics.mean(warm_ms) / max(iters, 1),

@@ -305,6 +305,12 @@ int ssv_ams_get_precision(const ssv_precond* p, int32_t* precision);
  * launches back to back (operands that fit in L2 stay there). */
 #define SSV_PROFILE_COLD 1
 int ssv_ams_profile(ssv_precond* p, int32_t nrhs, int32_t reps, int32_t flags, ssv_phase_profile* out);
+/* Measurement hook (no reference counterpart): wall seconds of the last
+ * set-up of p (create, Update() or a precision switch) into times[0..3]:
+ * total, host hierarchy (BC matrix, Galerkin products, coarsening,
+ * interpolation, coarse operators, coarsest factors), fused level products,
+ * launch-shape tuner; the rest of the total is device uploads. */
+int ssv_ams_setup_times(const ssv_precond* p, double* times);
 
 /* ---- CG with an external preconditioner (new: the reference's AMS scripts
  *      drive it with NGSolve's krylovspace.CGSolver) ---------------------------

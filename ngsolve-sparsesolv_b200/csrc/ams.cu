@@ -824,6 +824,9 @@ struct AmsState {
     ForkSet forks;  // the y and z nodal V-cycles run beside the x one
     bool tri = true;  // nodal V-cycles in lockstep launches (SSV_AMS_TRI=0: three branches)
     int pi_lanes[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};  // Pi restrict / prolong lanes by NV slot (0 = untuned)
+    // wall seconds of the last set-up (create, Update or precision switch):
+    // total, host hierarchy, fused level products, shape tuner (the rest is uploads)
+    double t_total = 0, t_host = 0, t_fused = 0, t_tune = 0;
 };
 
 void ams_free(AmsState* a) { delete a; }
@@ -1686,7 +1689,9 @@ static void ams_reserve(AmsState& a, int nv) {
     for (int s = 0; s < 4; ++s) a.rs[s].alloc(m1);
     a.nv_alloc = nv;
     ++a.gen;  // new work buffers: graphs that captured the old ones must be rebuilt
+    const double t0 = wall_seconds();
     tune_lanes(a);
+    a.t_tune += wall_seconds() - t0;
     {
         const char* e = std::getenv("SSV_AMS_TRI");
         a.tri = !(e && e[0] == '0');
@@ -1773,6 +1778,7 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
     // 40^3 magnetostatic system; with every hierarchy fused, no convergence in
     // 500), while the fused nodal ones change nothing (34).
     std::vector<FusedLevel> fused[4];
+    const double tf0 = wall_seconds();
     if (fused_enabled()) {
         std::vector<std::thread> th;
         for (int sub = a.fp32 ? 1 : 0; sub < 4; ++sub)
@@ -1799,6 +1805,7 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
             });
         for (auto& t : th) t.join();
     }
+    a.t_fused = wall_seconds() - tf0;
     for (int sub = 0; sub < 4; ++sub) {
         const auto& hl = a.host.amg[sub].levels;
         a.amg[sub].clear();
@@ -1873,11 +1880,22 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
 // Rebuild the matrix-dependent part (RebuildMatrix) and upload it.
 static void ams_rebuild(AmsState& a, const ssv_matrix* A) {
     cudaStream_t s = stream();
+    const double t0 = wall_seconds();
+    a.t_tune = 0;
     HostCsr H = host_csr_of(A);
     a.host.rebuild(H, a.has_fd ? a.h_fd.data() : nullptr);
+    a.t_host = wall_seconds() - t0;
     ams_upload_matrix(a, s);
     ++a.gen;
     SSV_CUDA(cudaStreamSynchronize(s));
+    a.t_total = wall_seconds() - t0;
+}
+
+void ams_setup_times(const AmsState* a, double* t) {
+    t[0] = a->t_total;
+    t[1] = a->t_host;
+    t[2] = a->t_fused;
+    t[3] = a->t_tune;
 }
 
 AmsState* ams_create(const ssv_matrix* A, const ssv_matrix* G, const uint8_t* fd, const double* cx,
@@ -1921,10 +1939,14 @@ void ams_set_precision(AmsState* a, int precision) {
     const bool lo = precision == SSV_PREC_FP32;
     if (lo == a->fp32) return;
     cudaStream_t s = stream();
+    const double t0 = wall_seconds();
     a->fp32 = lo;
+    a->t_tune = 0;
+    a->t_host = 0;
     ams_upload_matrix(*a, s);
     ++a->gen;
     SSV_CUDA(cudaStreamSynchronize(s));
+    a->t_total = wall_seconds() - t0;
 }
 
 int ams_precision(const AmsState* a) { return a->fp32 ? SSV_PREC_FP32 : SSV_PREC_FP64; }

@@ -427,6 +427,13 @@ int ssv_ams_set_precision(ssv_precond* p, int32_t precision) {
     });
 }
 
+int ssv_ams_setup_times(const ssv_precond* p, double* times) {
+    return guarded([&] {
+        if (!p || !p->ams || !times) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_setup_times: bad argument");
+        ssv::ams_setup_times(p->ams.get(), times);
+    });
+}
+
 int ssv_ams_profile(ssv_precond* p, int32_t nrhs, int32_t reps, int32_t flags, ssv_phase_profile* out) {
     return guarded([&] {
         if (!p || !p->ams || !out) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_profile: bad argument");

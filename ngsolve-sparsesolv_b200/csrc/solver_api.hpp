@@ -56,6 +56,8 @@ void amg_update(AmgOnly* g, const ssv_matrix* A);
 int amg_levels(const AmgOnly* g, int* sizes, int cap);
 int ams_levels(const AmsState* a, int sub, int* sizes, int cap);
 void ams_set_precision(AmsState* a, int precision);
+// wall seconds of the last set-up: total, host hierarchy, fused products, shape tuner
+void ams_setup_times(const AmsState* a, double* t);
 int ams_precision(const AmsState* a);
 // Block application to nrhs right-hand sides ([row][rhs] interleaved; complex
 // form: Re/Im pairs), after ams_reserve_block(a, nrhs).

@@ -703,7 +703,13 @@ class _AmsBase(_PrecondBase):
     _complex_form = 0
 
     def __init__(self, mat, grad_mat, freedofs, coord_x, coord_y, coord_z, cycle_type, num_smooth,
-                 correction_weight, ndof_complex=0):
+                 correction_weight, ndof_complex=0, print_level=0):
+        import time
+        t0 = time.perf_counter()
+        self.print_level = int(print_level)
+        self._cycle_type = int(cycle_type)
+        self._mult_count = 0
+        self._breakdown_done = False
         ip, ix, data, cplx, shape = _csr_arrays(mat)
         if cplx:
             raise TypeError("CompactAMSPreconditioner: expected real SparseMatrix<double>")
@@ -725,6 +731,47 @@ class _AmsBase(_PrecondBase):
                                  int(cycle_type), int(num_smooth), 0.25, float(correction_weight),
                                  self._complex_form, int(ndof_complex), ctypes.byref(h)))
         self._init_handle(h)
+        if self.print_level > 0:
+            self._print_setup(nh1, int(ndof_complex) or self._n, time.perf_counter() - t0)
+
+    def _print_setup(self, nh1, ndof_complex, seconds):
+        """The set-up report of print_level >= 1 (compact_ams.hpp:247-271, 325-329;
+        compact_amg.hpp:119-155; complex_compact_ams.hpp:86-88): sizes, each
+        subspace hierarchy's coarsening, its coarsest level, the set-up time."""
+        names = ("G", "Pix", "Piy", "Piz")
+        print(f"CompactAMS setup: HC={self._n} H1={nh1}", end="")
+        for sub in range(4):
+            lv = self.levels(sub)
+            print(f"\n  subspace {names[sub]}: A={lv[0][0]}x{lv[0][0]} nnz={lv[0][1]}")
+            for l in range(len(lv) - 1):
+                print(f"  CompactAMG level {l}: {lv[l][0]} -> {lv[l + 1][0]} (ratio {lv[l + 1][0] / lv[l][0]:g})")
+            print(f"\n  CompactAMG: {len(lv)} levels, coarsest = {lv[-1][0]} DOFs", end="")
+        print(f"\n  CompactAMS setup complete: {seconds:g}s total")
+        if self._complex_form:
+            print(f"  ComplexCompactAMS: fused Re/Im SpMV (ndof={ndof_complex})")
+
+    def _note_applies(self, count):
+        """print_level >= 1: after the 25th application, the per-phase breakdown of
+        compact_ams.hpp:185-194. The phases run inside captured device graphs, so
+        their times come from one profiled cycle (CUDA events), times 25."""
+        self._mult_count += count
+        if self.print_level < 1 or self._breakdown_done or self._mult_count < 25:
+            return
+        self._breakdown_done = True
+        ph = {q["name"]: q["ms"] * 1e-3 for q in self.profile(nrhs=1, reps=5)}
+        k = 25
+        n_smooth = 3 if self._cycle_type == 7 else 1  # full fine sweeps (the first starts from x = 0)
+        smooth = n_smooth * ph["fine_smooth"]
+        grad = 2 * (ph["fine_residual"] + ph["grad_transfers"] + ph["grad_vcycle"])
+        nodal = ph["fine_residual"] + ph["pi_transfers"] + ph["nodal_vcycles"]
+        total = ph["ams_cycle"]
+        bc = max(total - smooth - grad - nodal, 0.0)
+        print(f"\n  AMS Mult x{k} breakdown: smooth={k * smooth:g}s grad={k * grad:g}s nodal={k * nodal:g}s "
+              f"bc={k * bc:g}s total={k * total:g}s (device time: one profiled cycle x {k})")
+
+    def Mult(self, x, y):
+        super().Mult(x, y)
+        self._note_applies(1)
 
     def Update(self, new_mat=None):
         """Rebuild with the current matrix values, or with new_mat (geometry kept)."""
@@ -760,6 +807,15 @@ class _AmsBase(_PrecondBase):
                                         ctypes.byref(prof)))
         return prof.as_list()
 
+    @property
+    def setup_times(self):
+        """Wall seconds of the last set-up (construction, Update() or precision switch): total,
+        host hierarchy, fused level products, launch-shape tuner, uploads (the rest)."""
+        t = np.zeros(4)
+        check(self._lib.ssv_ams_setup_times(self._h, t.ctypes.data_as(_capi.PD)))
+        return {"total": t[0], "host_hierarchy": t[1], "fused_products": t[2], "tuner": t[3],
+                "uploads": max(t[0] - t[1] - t[2] - t[3], 0.0)}
+
     def levels(self, subspace):
         """AMG hierarchy of a subspace (0 gradient, 1..3 Nedelec x/y/z): [(rows, nnz), ...]."""
         buf = np.zeros(256, np.int32)
@@ -786,7 +842,7 @@ def CompactAMSPreconditioner(mat, grad_mat, freedofs=None, coord_x=(), coord_y=(
     if subspace_solver != 0:
         raise ValueError("subspace_solver=1 (sparse Cholesky subspace solves, diagnostic) is not provided")
     p = CompactAMSPreconditionerImpl(mat, grad_mat, freedofs, coord_x, coord_y, coord_z, cycle_type,
-                                     num_smooth, 1.0)
+                                     num_smooth, 1.0, print_level=print_level)
     if str(precision).lower() != "fp64":
         p.precision = precision
     return p
@@ -800,7 +856,8 @@ def ComplexCompactAMSPreconditioner(a_real_mat, grad_mat, freedofs=None, coord_x
     if subspace_solver != 0:
         raise ValueError("subspace_solver=1 (sparse Cholesky subspace solves, diagnostic) is not provided")
     p = ComplexCompactAMSPreconditionerImpl(a_real_mat, grad_mat, freedofs, coord_x, coord_y, coord_z,
-                                            cycle_type, num_smooth, correction_weight, ndof_complex)
+                                            cycle_type, num_smooth, correction_weight, ndof_complex,
+                                            print_level=print_level)
     if str(precision).lower() != "fp64":
         p.precision = precision
     return p
@@ -865,6 +922,7 @@ class PCGSolver:
             for i, v in enumerate(r.residual_history):
                 print(f"CG iteration {i}, residual = {v}")
         self._last = r
+        _note_applies(self._pre, res.iterations + 1)
         return r
 
     def Mult(self, rhs, sol):
@@ -952,6 +1010,9 @@ class BatchedCOCRSolver:
         check(self._lib.ssv_batch_cocr_solve(self._h, self.maxiter, self.tol, _capi.vptr(b), _capi.vptr(x),
                                              _capi.i32ptr(self.iterations), _capi.i32ptr(self.converged),
                                              self.residuals.ctypes.data_as(_capi.PD)))
+        its = int(self.iterations.max()) if self.iterations.size else 0
+        for p in {id(p): p for p in self._pres if p is not None}.values():
+            _note_applies(p, its + 1)
         return x
 
     def solve_dev(self, d_b, d_x):

@@ -1,7 +1,9 @@
 """bench.py's reference arm runs on the host cores (no GPU): one JSON line
 with the GPU arm's metric, unit and direction, "impl": "reference", a
 cpu_baseline describing the run (kind, cores, sample; value = the line's),
-and an e2e block with the line's value and no host<->device bytes."""
+and an e2e block with the line's value and no host<->device bytes. Run on
+the ams40 workload (a 40^3 PCG solve of the restatement takes about a second
+here; the default eddy64 workload's full 64^3 COCR solve takes minutes)."""
 from __future__ import annotations
 
 import json
@@ -13,8 +15,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def test_reference_arm_line():
-    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "0"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload", "ams40",
+                        "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
     sys.path.insert(0, ROOT)
