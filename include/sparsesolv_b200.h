@@ -311,6 +311,14 @@ int ssv_ams_profile(ssv_precond* p, int32_t nrhs, int32_t reps, int32_t flags, s
  * interpolation, coarse operators, coarsest factors), fused level products,
  * launch-shape tuner; the rest of the total is device uploads. */
 int ssv_ams_setup_times(const ssv_precond* p, double* times);
+/* Parity hook (no reference counterpart): level `level` of subspace s
+ * (0 gradient, 1..3 Nedelec x, y, z) of the hierarchy as set up, FP64 and
+ * unscaled: what = 0 the level matrix A_l (CompactAMG Level::A), 1 the
+ * interpolation P_l. *nnz receives its nonzeros; row_ptr (rows + 1),
+ * col_idx and values are filled when cap >= *nnz. *on_device (may be NULL)
+ * = 1 when the hierarchy was set up on the device. */
+int ssv_ams_level_matrix(const ssv_precond* p, int32_t subspace, int32_t level, int32_t what, int32_t* row_ptr,
+                         int32_t* col_idx, double* values, int32_t cap, int32_t* nnz, int32_t* on_device);
 
 /* ---- CG with an external preconditioner (new: the reference's AMS scripts
  *      drive it with NGSolve's krylovspace.CGSolver) ---------------------------

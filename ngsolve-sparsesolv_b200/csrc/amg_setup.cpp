@@ -329,6 +329,8 @@ void l1_norms(const HostCsr& A, std::vector<double>& out) {
     }
 }
 
+}  // namespace
+
 // Pseudo-inverse of the small coarsest matrix through LDL^T: pivots below
 // 1e-13 of the row's diagonal count as zero and drop their component (the
 // gradient-space matrix is singular, constants being in the kernel of G).
@@ -389,8 +391,6 @@ void dense_ldlt_pseudo(const HostCsr& A, std::vector<double>& linv, std::vector<
         for (auto& x : th) x.join();
     }
 }
-
-}  // namespace
 
 // CompactAMG::Setup (:66-156) for freedofs = nullptr (the AMS subspaces)
 void AmgHost::setup(const HostCsr& A0) {

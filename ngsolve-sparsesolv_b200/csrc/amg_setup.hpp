@@ -38,6 +38,12 @@ struct FusedLevel {
 };
 FusedLevel fused_level(const HostCsr& A, const HostCsr& P, const HostCsr& Pt, const std::vector<double>& d);
 
+// Pseudo-inverse of the small coarsest matrix through LDL^T (pivots below
+// 1e-13 of their row's diagonal dropped): linv = L^{-1} row-major, linvt its
+// transpose, piv the pivots (0 where dropped).
+void dense_ldlt_pseudo(const HostCsr& A, std::vector<double>& linv, std::vector<double>& linvt,
+                       std::vector<double>& piv);
+
 struct AmgHostLevel {
     HostCsr A, P, Pt;
     std::vector<double> l1;

@@ -25,13 +25,17 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <thread>
 #include <type_traits>
 
+#include "amg_device.hpp"
 #include "amg_setup.hpp"
 #include "objects.cuh"
 #include "solver_api.hpp"
@@ -695,6 +699,18 @@ struct DualVec {
             d.upload(h.data(), h.size(), s);
         }
     }
+    // the same from a device FP64 array
+    void set_dev(const double* src, size_t n, bool fp32, cudaStream_t s) {
+        if (fp32) {
+            d.release();
+            f.alloc(std::max<size_t>(n, 1));
+            d_to_float((int64_t)n, src, f.get(), s);
+        } else {
+            f.release();
+            d.alloc(std::max<size_t>(n, 1));
+            if (n) SSV_CUDA(cudaMemcpyAsync(d.get(), src, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        }
+    }
     template <typename T> const T* get() const;
 };
 template <> inline const double* DualVec::get<double>() const { return d.get(); }
@@ -709,12 +725,29 @@ template <> inline const float* DualVec::get<float>() const { return f.get(); }
 // no longer run side by side and share fewer x rows in L1.)
 constexpr int kSellWindow = 256;
 
+__global__ void k_sell_refresh(int64_t entries, const int* __restrict__ src, const double* __restrict__ csr_v,
+                               double* __restrict__ v) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < entries; e += (int64_t)gridDim.x * blockDim.x)
+        v[e] = src[e] >= 0 ? csr_v[src[e]] : 0.0;
+}
+
 struct DevSell {
     int slices = 0;
     int64_t entries = 0;
+    int pat_n = -1;
+    int64_t pat_nnz = -1;  // the pattern the layout was built for
     DevBuf<int> off, rows, ci;
+    DevBuf<int> src;  // slot -> CSR entry index (-1 = padding), for value refreshes
     DevBuf<double> v;
+    // the same values on the same pattern: v from the CSR values (device)
+    void refresh(const double* csr_v, cudaStream_t s) {
+        if (slices > 0 && entries > 0)
+            k_sell_refresh<<<grid_for(entries, 256), 256, 0, s>>>(entries, src.get(), csr_v, v.get());
+        SSV_LAUNCH_CHECK();
+    }
     void build(const HostCsr& A, cudaStream_t s) {
+        pat_n = A.n;
+        pat_nnz = A.nnz();
         const int n = A.n;
         slices = (n + 31) / 32;
         std::vector<int> order(n);
@@ -740,7 +773,7 @@ struct DevSell {
             h_off[sl + 1] = h_off[sl] + 32 * wmax;
         }
         entries = h_off[slices];
-        std::vector<int> h_ci((size_t)entries, -1);
+        std::vector<int> h_ci((size_t)entries, -1), h_src((size_t)entries, -1);
         std::vector<double> h_v((size_t)entries, 0.0);
         for (int sl = 0; sl < slices; ++sl)
             for (int t = 0; t < 32; ++t) {
@@ -750,12 +783,15 @@ struct DevSell {
                     const size_t e = (size_t)h_off[sl] + 32 * (size_t)k + t;
                     h_ci[e] = A.ci[A.rp[r] + k];
                     h_v[e] = A.v[A.rp[r] + k];
+                    h_src[e] = A.rp[r] + k;
                 }
             }
         off.upload(h_off.data(), h_off.size(), s);
         rows.upload(h_rows.data(), h_rows.size(), s);
         ci.upload(h_ci.data(), h_ci.size(), s);
+        src.upload(h_src.data(), h_src.size(), s);
         v.upload(h_v.data(), h_v.size(), s);
+        SSV_CUDA(cudaStreamSynchronize(s));  // pageable sources
     }
 };
 
@@ -805,6 +841,17 @@ struct AmgDevLevel {
     WorkVec b, xa, xb, r;  // NV-column work vectors of this level
 };
 
+// The hierarchy as the device set-up builds it (FP64, unscaled): the input of
+// the cycle's arrays in either form, kept so that a precision switch needs no
+// new set-up.
+struct AmsDev {
+    bool on = false;                 // this state was set up on the device
+    const ssv_matrix* src = nullptr;  // the HCurl matrix the fine layouts were built for
+    DCsr A_bc, G, Gt, Pi[3], Pit[3];
+    DevBuf<double> fine_l1;
+    std::vector<DAmgLevel> amg[4];
+};
+
 struct AmsState {
     int nhc = 0, nh1 = 0, cycle_type = 1, num_smooth = 1, nv_alloc = 0;
     double w = 1.0;
@@ -825,8 +872,9 @@ struct AmsState {
     bool tri = true;  // nodal V-cycles in lockstep launches (SSV_AMS_TRI=0: three branches)
     int pi_lanes[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};  // Pi restrict / prolong lanes by NV slot (0 = untuned)
     // wall seconds of the last set-up (create, Update or precision switch):
-    // total, host hierarchy, fused level products, shape tuner (the rest is uploads)
+    // total, hierarchy, fused level products, shape tuner (the rest is uploads)
     double t_total = 0, t_host = 0, t_fused = 0, t_tune = 0;
+    AmsDev dev;
 };
 
 void ams_free(AmsState* a) { delete a; }
@@ -1483,6 +1531,27 @@ static TuneReplay& tune_replay() {
     return r;
 }
 
+// Shapes already timed in this process, by matrix (rows, nonzeros, columns
+// per pass, value type, kind): a later Update() of the same preconditioner,
+// whose fine level and often several coarse levels keep their sizes, and the
+// other preconditioners of a frequency family reuse them instead of timing
+// again (SSV_AMS_TUNE_MEMO=0 times every matrix).
+struct TuneMemo {
+    std::mutex mu;
+    std::map<std::array<long long, 6>, std::array<int, 3>> m;
+    static bool on() {
+        static const bool v = [] {
+            const char* e = std::getenv("SSV_AMS_TUNE_MEMO");
+            return !(e && e[0] == '0');
+        }();
+        return v;
+    }
+};
+static TuneMemo& tune_memo() {
+    static TuneMemo t;
+    return t;
+}
+
 // Shapes of square level matrices are timed as residuals r = b - A x (b given),
 // the form the cycle runs them in (smoothing reads the same streams); the
 // transfers as y = A x.
@@ -1496,6 +1565,20 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
         A.tuned_u[slot] = (int)(*r)[5];
         A.tuned_sell[slot] = (A.sell.slices > 0 && std::is_same_v<TV, double>) ? (int)(*r)[6] : 0;
         return;
+    }
+    const std::array<long long, 6> memo_key = {A.n, A.nnz, NV, (long long)sizeof(TV),
+                                               (two ? 2 : 0) + (b ? 1 : 0) + (force_cold ? 4 : 0),
+                                               A.sell.slices > 0 ? 1 : 0};
+    if (TuneMemo::on()) {
+        std::lock_guard<std::mutex> lk(tune_memo().mu);
+        auto it = tune_memo().m.find(memo_key);
+        if (it != tune_memo().m.end()) {
+            const int slot = DevCsr::nv_slot(NV);
+            A.tuned[slot] = it->second[0];
+            A.tuned_u[slot] = it->second[1];
+            A.tuned_sell[slot] = it->second[2];
+            return;
+        }
     }
     const TV* v = A.val<TV>();
     // A matrix much larger than a quarter of L2 streams from HBM in the cycle:
@@ -1557,6 +1640,10 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
                       A.tuned_sell[slot]);
         tune_replay().record(line);
     }
+    if (TuneMemo::on()) {
+        std::lock_guard<std::mutex> lk(tune_memo().mu);
+        tune_memo().m[memo_key] = {pick, pick_u, A.tuned_sell[slot]};
+    }
     static const bool log = std::getenv("SSV_AMS_TUNE_LOG") != nullptr;
     if (log) {
         std::fprintf(stderr, "ams tune: n=%d nnz=%lld nv=%d %s -> lanes %d rows/group %d (%.2f us)", A.n,
@@ -1581,6 +1668,15 @@ static void tune_pi(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1)
         if (const auto* r = tune_replay().take({1, dir, NV})) {
             a.pi_lanes[dir][slot] = (int)(*r)[3];
             continue;
+        }
+        const std::array<long long, 6> memo_key = {-1, a.G.n, a.G.nnz, NV, (long long)sizeof(T), dir};
+        if (TuneMemo::on()) {
+            std::lock_guard<std::mutex> lk(tune_memo().mu);
+            auto it = tune_memo().m.find(memo_key);
+            if (it != tune_memo().m.end()) {
+                a.pi_lanes[dir][slot] = it->second[0];
+                continue;
+            }
         }
         float best = 1e30f;
         int pick = 0;
@@ -1612,6 +1708,10 @@ static void tune_pi(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1)
             }
         }
         a.pi_lanes[dir][slot] = pick;
+        if (TuneMemo::on()) {
+            std::lock_guard<std::mutex> lk(tune_memo().mu);
+            tune_memo().m[memo_key] = {pick, 0, 0};
+        }
         {
             char line[64];
             std::snprintf(line, sizeof(line), "pi %d %d %d\n", dir, NV, pick);
@@ -1877,15 +1977,220 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
     ams_reserve(a, nv);
 }
 
+// ---------------------------------------------------------------------------
+// Set-up on the device (the default; SSV_AMS_SETUP=host runs the host set-up
+// of amg_setup.cpp instead, which gives the same hierarchy bit for bit): the
+// BC matrix, the four Galerkin products and the four AMG hierarchies come
+// from amg_device.cu; the cycle's arrays (FP64, or diagonally scaled FP32) and
+// the fused level products are derived from them on the device.
+// ---------------------------------------------------------------------------
+static bool device_setup_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("SSV_AMS_SETUP");
+        v = (e && std::strcmp(e, "host") == 0) ? 0 : 1;
+    }
+    return v != 0;
+}
+
+// the cycle's CSR from a device FP64 CSR: an FP64 copy, or FP32 values
+static void devcsr_from(DevCsr& M, const DCsr& D, bool fp32, cudaStream_t s) {
+    M.n = D.n;
+    M.m = D.m;
+    M.nnz = D.nnz;
+    M.rp.alloc(D.n + 1);
+    M.ci.alloc(std::max<int64_t>(D.nnz, 1));
+    SSV_CUDA(cudaMemcpyAsync(M.rp.get(), D.rp.get(), sizeof(int) * (D.n + 1), cudaMemcpyDeviceToDevice, s));
+    if (D.nnz) SSV_CUDA(cudaMemcpyAsync(M.ci.get(), D.ci.get(), sizeof(int) * D.nnz, cudaMemcpyDeviceToDevice, s));
+    M.v.set_dev(D.v.get(), (size_t)D.nnz, fp32, s);
+    M.lanes = pick_lanes(D.n > 0 ? (double)D.nnz / D.n : 1.0);
+}
+
+// a fine-level FP64 matrix and its sliced-ELL copy: the layout (a function of
+// the pattern) is kept while the pattern is the same, and only its values
+// are gathered again
+static void fine_from(DevCsr& M, const DCsr& D, bool layout_valid, cudaStream_t s) {
+    devcsr_from(M, D, false, s);
+    const bool want = sell_mode() == 2 || (sell_mode() == 1 && M.n >= kUnrollMinRows);
+    if (!want) return;
+    if (layout_valid && M.sell.slices > 0 && M.sell.pat_n == D.n && M.sell.pat_nnz == D.nnz)
+        M.sell.refresh(D.v.get(), s);
+    else
+        M.sell.build(D.to_host(s), s);
+}
+
+// BC matrix, Galerkin products (FixZeroRows) and AMG hierarchies of the four
+// subspaces, fine l1 norms; false (nothing replaced) if a product row is too
+// long for the device symbolic step
+static bool ams_device_setup(AmsState& a, const ssv_matrix* A, cudaStream_t s) {
+    AmsDev& D = a.dev;
+    DCsr Abc;
+    d_bc_matrix(A->rows, A->cols, A->nnz, A->rp.get(), A->ci.get(), A->val.get(), a.has_fd ? a.fd.get() : nullptr,
+                Abc, s);
+    std::vector<DAmgLevel> amg[4];
+    for (int sub = 0; sub < 4; ++sub) {
+        const DCsr& P0 = sub == 0 ? D.G : D.Pi[sub - 1];
+        const DCsr& P0t = sub == 0 ? D.Gt : D.Pit[sub - 1];
+        DCsr A0;
+        if (!d_rap(Abc, P0, P0t, A0, s)) return false;
+        d_fix_zero_rows(A0, s);
+        if (!d_amg_setup(A0, a.host.theta, 25, 500, amg[sub], s)) return false;
+    }
+    D.A_bc = std::move(Abc);
+    for (int sub = 0; sub < 4; ++sub) D.amg[sub] = std::move(amg[sub]);
+    d_fine_l1(D.A_bc, D.fine_l1, s);
+    SSV_CUDA(cudaStreamSynchronize(s));
+    return true;
+}
+
+// The cycle's arrays from the device hierarchy (ams_upload_matrix's device
+// counterpart, the same values): fine level FP64, every subspace level in the
+// current form, the fused level products, the coarsest factors, the scaled
+// transfers of the FP32 form.
+static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
+    AmsDev& D = a.dev;
+    const int nv = std::max(a.nv_alloc, a.complex_form ? 2 : 1);
+    fine_from(a.A_bc, D.A_bc, layout_valid, s);
+    a.fine_l1.alloc(std::max(a.nhc, 1));
+    SSV_CUDA(cudaMemcpyAsync(a.fine_l1.get(), D.fine_l1.get(), sizeof(double) * a.nhc, cudaMemcpyDeviceToDevice, s));
+    a.fine_il1.alloc(std::max(a.nhc, 1));
+    d_reciprocal(a.nhc, a.fine_l1.get(), a.fine_il1.get(), s);
+    double t_fused = 0;
+    for (int sub = 0; sub < 4; ++sub) {
+        const auto& hl = D.amg[sub];
+        const size_t L = hl.size();
+        a.amg[sub].clear();
+        a.amg[sub].resize(L);
+        std::vector<DevBuf<double>> sc(L), isc(L);
+        if (a.fp32)
+            for (size_t l = 0; l < L; ++l) d_diag_scale(hl[l].A, sc[l], isc[l], s);
+        // in the FP32 form only the three nodal hierarchies take the fused products
+        const bool fuse = fused_enabled() && (!a.fp32 || sub >= 1);
+        for (size_t l = 0; l < L; ++l) {
+            AmgDevLevel& dl = a.amg[sub][l];
+            const int nl = hl[l].A.n;
+            const bool last = l + 1 == L;
+            DCsr As, Ps, Pts;
+            DevBuf<double> l1s, il1(std::max(nl, 1));
+            const DCsr* Al = &hl[l].A;
+            const DCsr* Pl = last ? nullptr : &hl[l].P;
+            const DCsr* Ptl = last ? nullptr : &hl[l].Pt;
+            const double* l1p = hl[l].l1.get();
+            if (a.fp32) {
+                d_scaled(hl[l].A, isc[l].get(), isc[l].get(), As, s);
+                Al = &As;
+                l1s.alloc(std::max(nl, 1));
+                d_scale_vec(nl, hl[l].l1.get(), isc[l].get(), isc[l].get(), l1s.get(), s);
+                l1p = l1s.get();
+                if (!last) {
+                    d_scaled(hl[l].P, sc[l].get(), isc[l + 1].get(), Ps, s);
+                    d_scaled(hl[l].Pt, isc[l + 1].get(), sc[l].get(), Pts, s);
+                    Pl = &Ps;
+                    Ptl = &Pts;
+                }
+            }
+            devcsr_from(dl.A, *Al, a.fp32, s);
+            dl.l1.set_dev(l1p, nl, a.fp32, s);
+            d_reciprocal(nl, l1p, il1.get(), s);
+            dl.il1.set_dev(il1.get(), nl, a.fp32, s);
+            if (!last) {
+                devcsr_from(dl.P, *Pl, a.fp32, s);
+                devcsr_from(dl.Pt, *Ptl, a.fp32, s);
+            }
+            dl.direct = hl[l].direct;
+            if (dl.direct) {  // FP64 in both forms; in the FP32 form scaled like the level
+                if (a.fp32) {
+                    std::vector<double> hs(nl), his(nl);
+                    SSV_CUDA(cudaMemcpyAsync(hs.data(), sc[l].get(), sizeof(double) * nl, cudaMemcpyDeviceToHost, s));
+                    SSV_CUDA(cudaMemcpyAsync(his.data(), isc[l].get(), sizeof(double) * nl, cudaMemcpyDeviceToHost, s));
+                    SSV_CUDA(cudaStreamSynchronize(s));
+                    std::vector<double> li = hl[l].linv, lt = hl[l].linvt, pv = hl[l].piv;
+                    for (int i = 0; i < nl; ++i)
+                        for (int k = 0; k < nl; ++k) {
+                            li[(size_t)i * nl + k] *= his[i] * hs[k];
+                            lt[(size_t)i * nl + k] *= hs[i] * his[k];
+                        }
+                    for (int i = 0; i < nl; ++i) pv[i] *= his[i] * his[i];
+                    dl.Li.upload(li.data(), li.size(), s);
+                    dl.LiT.upload(lt.data(), lt.size(), s);
+                    dl.piv.upload(pv.data(), pv.size(), s);
+                    SSV_CUDA(cudaStreamSynchronize(s));
+                } else {
+                    dl.Li.upload(hl[l].linv.data(), hl[l].linv.size(), s);
+                    dl.LiT.upload(hl[l].linvt.data(), hl[l].linvt.size(), s);
+                    dl.piv.upload(hl[l].piv.data(), hl[l].piv.size(), s);
+                }
+            }
+            if (fuse && !last) {
+                const double tf0 = wall_seconds();
+                DCsr R, U;
+                if (d_fused_level(*Al, *Pl, *Ptl, l1p, R, U, s)) {
+                    devcsr_from(dl.R, R, a.fp32, s);
+                    devcsr_from(dl.U, U, a.fp32, s);
+                }
+                SSV_CUDA(cudaStreamSynchronize(s));
+                t_fused += wall_seconds() - tf0;
+            }
+            SSV_CUDA(cudaStreamSynchronize(s));  // this level's temporaries go out of scope
+        }
+        // level-0 scaling folded into this subspace's transfers
+        if (sub == 0) {
+            if (a.fp32) {
+                DCsr Gs, Gts;
+                d_scaled(D.G, nullptr, isc[0].get(), Gs, s);
+                d_scaled(D.Gt, isc[0].get(), nullptr, Gts, s);
+                fine_from(a.G, Gs, true, s);
+                fine_from(a.Gt, Gts, true, s);
+                SSV_CUDA(cudaStreamSynchronize(s));
+            } else {
+                fine_from(a.G, D.G, true, s);
+                fine_from(a.Gt, D.Gt, true, s);
+            }
+        } else {
+            const int d = sub - 1;
+            const int64_t nz = D.Pi[d].nnz;
+            a.Piv[d].alloc(std::max<int64_t>(nz, 1));
+            a.Pitv[d].alloc(std::max<int64_t>(nz, 1));
+            if (a.fp32) {
+                DCsr pi, pit;
+                d_scaled(D.Pi[d], nullptr, isc[0].get(), pi, s);
+                d_scaled(D.Pit[d], isc[0].get(), nullptr, pit, s);
+                SSV_CUDA(cudaMemcpyAsync(a.Piv[d].get(), pi.v.get(), sizeof(double) * nz, cudaMemcpyDeviceToDevice, s));
+                SSV_CUDA(cudaMemcpyAsync(a.Pitv[d].get(), pit.v.get(), sizeof(double) * nz, cudaMemcpyDeviceToDevice, s));
+                SSV_CUDA(cudaStreamSynchronize(s));
+            } else {
+                SSV_CUDA(cudaMemcpyAsync(a.Piv[d].get(), D.Pi[d].v.get(), sizeof(double) * nz, cudaMemcpyDeviceToDevice,
+                                         s));
+                SSV_CUDA(cudaMemcpyAsync(a.Pitv[d].get(), D.Pit[d].v.get(), sizeof(double) * nz,
+                                         cudaMemcpyDeviceToDevice, s));
+            }
+        }
+    }
+    a.t_fused = t_fused;
+    a.nv_alloc = 0;
+    ams_reserve(a, nv);
+}
+
 // Rebuild the matrix-dependent part (RebuildMatrix) and upload it.
 static void ams_rebuild(AmsState& a, const ssv_matrix* A) {
     cudaStream_t s = stream();
     const double t0 = wall_seconds();
     a.t_tune = 0;
-    HostCsr H = host_csr_of(A);
-    a.host.rebuild(H, a.has_fd ? a.h_fd.data() : nullptr);
-    a.t_host = wall_seconds() - t0;
-    ams_upload_matrix(a, s);
+    a.t_fused = 0;
+    if (A->dtype != SSV_F64) fail(SSV_ERR_TYPE, "CompactAMS: the HCurl matrix must be real");
+    if (device_setup_enabled() && ams_device_setup(a, A, stream())) {
+        a.t_host = wall_seconds() - t0;
+        const bool same = a.dev.on && a.dev.src == A;
+        a.dev.on = true;
+        a.dev.src = A;
+        ams_build_cycle(a, same, s);
+    } else {
+        a.dev.on = false;
+        HostCsr H = host_csr_of(A);
+        a.host.rebuild(H, a.has_fd ? a.h_fd.data() : nullptr);
+        a.t_host = wall_seconds() - t0;
+        ams_upload_matrix(a, s);
+    }
     ++a.gen;
     SSV_CUDA(cudaStreamSynchronize(s));
     a.t_total = wall_seconds() - t0;
@@ -1922,6 +2227,15 @@ AmsState* ams_create(const ssv_matrix* A, const ssv_matrix* G, const uint8_t* fd
         HostCsr Gh = host_csr_of(G);
         a->host.setup_geometry(Gh, cx, cy, cz);
         ams_upload_geometry(*a, s);
+        if (device_setup_enabled()) {  // the geometry in FP64 for the device set-up (kept)
+            a->dev.G.from_host(a->host.G, s);
+            a->dev.Gt.from_host(a->host.Gt, s);
+            for (int d = 0; d < 3; ++d) {
+                a->dev.Pi[d].from_host(a->host.Pi[d], s);
+                a->dev.Pit[d].from_host(a->host.Pit[d], s);
+            }
+            SSV_CUDA(cudaStreamSynchronize(s));
+        }
         ams_rebuild(*a, A);
         if (a->w <= 0.0) a->w = 1.0;  // Setup (:260-262)
     } catch (...) {
@@ -1943,7 +2257,8 @@ void ams_set_precision(AmsState* a, int precision) {
     a->fp32 = lo;
     a->t_tune = 0;
     a->t_host = 0;
-    ams_upload_matrix(*a, s);
+    if (a->dev.on) ams_build_cycle(*a, true, s);
+    else ams_upload_matrix(*a, s);
     ++a->gen;
     SSV_CUDA(cudaStreamSynchronize(s));
     a->t_total = wall_seconds() - t0;
@@ -2252,7 +2567,42 @@ unsigned precond_generation(const ssv_precond* p) {
     return p->ams ? p->ams->gen : 0;
 }
 
+// Level matrix of the hierarchy as set up (FP64, unscaled): what = 0 A_l,
+// 1 P_l; returns nnz (arrays filled only when cap >= nnz)
+int ams_level_matrix(const AmsState* a, int sub, int l, int what, int* rp, int* ci, double* v, int cap) {
+    if (sub < 0 || sub > 3) fail(SSV_ERR_INVALID_ARG, "ssv_ams_level_matrix: subspace must be 0..3");
+    HostCsr H;
+    if (a->dev.on) {
+        const auto& dl = a->dev.amg[sub];
+        if (l < 0 || l >= (int)dl.size() || (what == 1 && l + 1 >= (int)dl.size()))
+            fail(SSV_ERR_INVALID_ARG, "ssv_ams_level_matrix: no such level");
+        H = (what == 0 ? dl[l].A : dl[l].P).to_host(stream());
+    } else {
+        const auto& hl = a->host.amg[sub].levels;
+        if (l < 0 || l >= (int)hl.size() || (what == 1 && l + 1 >= (int)hl.size()))
+            fail(SSV_ERR_INVALID_ARG, "ssv_ams_level_matrix: no such level");
+        H = what == 0 ? hl[l].A : hl[l].P;
+    }
+    const int nnz = H.nnz();
+    if (cap >= nnz && rp && ci && v) {
+        std::copy(H.rp.begin(), H.rp.end(), rp);
+        std::copy(H.ci.begin(), H.ci.begin() + nnz, ci);
+        std::copy(H.v.begin(), H.v.begin() + nnz, v);
+    }
+    return nnz;
+}
+
+bool ams_on_device(const AmsState* a) { return a->dev.on; }
+
 int ams_levels(const AmsState* a, int sub, int* sizes, int cap) {
+    if (a->dev.on) {
+        const auto& dl = a->dev.amg[sub];
+        for (size_t l = 0; l < dl.size() && 2 * (int)l + 1 < cap; ++l) {
+            sizes[2 * l] = dl[l].A.n;
+            sizes[2 * l + 1] = (int)dl[l].A.nnz;
+        }
+        return (int)dl.size();
+    }
     const auto& hl = a->host.amg[sub].levels;
     for (size_t l = 0; l < hl.size() && 2 * (int)l + 1 < cap; ++l) {
         sizes[2 * l] = hl[l].A.n;

@@ -427,6 +427,15 @@ int ssv_ams_set_precision(ssv_precond* p, int32_t precision) {
     });
 }
 
+int ssv_ams_level_matrix(const ssv_precond* p, int32_t subspace, int32_t level, int32_t what, int32_t* row_ptr,
+                         int32_t* col_idx, double* values, int32_t cap, int32_t* nnz, int32_t* on_device) {
+    return guarded([&] {
+        if (!p || !p->ams || !nnz) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_level_matrix: bad argument");
+        *nnz = ssv::ams_level_matrix(p->ams.get(), subspace, level, what, row_ptr, col_idx, values, cap);
+        if (on_device) *on_device = ssv::ams_on_device(p->ams.get()) ? 1 : 0;
+    });
+}
+
 int ssv_ams_setup_times(const ssv_precond* p, double* times) {
     return guarded([&] {
         if (!p || !p->ams || !times) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_setup_times: bad argument");

@@ -55,6 +55,8 @@ AmgOnly* amg_create(const ssv_matrix* A, const uint8_t* fd, double theta, int ma
 void amg_update(AmgOnly* g, const ssv_matrix* A);
 int amg_levels(const AmgOnly* g, int* sizes, int cap);
 int ams_levels(const AmsState* a, int sub, int* sizes, int cap);
+int ams_level_matrix(const AmsState* a, int sub, int l, int what, int* rp, int* ci, double* v, int cap);
+bool ams_on_device(const AmsState* a);
 void ams_set_precision(AmsState* a, int precision);
 // wall seconds of the last set-up: total, host hierarchy, fused products, shape tuner
 void ams_setup_times(const AmsState* a, double* t);

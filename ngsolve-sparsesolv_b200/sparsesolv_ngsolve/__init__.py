@@ -816,6 +816,24 @@ class _AmsBase(_PrecondBase):
         return {"total": t[0], "host_hierarchy": t[1], "fused_products": t[2], "tuner": t[3],
                 "uploads": max(t[0] - t[1] - t[2] - t[3], 0.0)}
 
+    def level_matrix(self, subspace, level, what=0):
+        """Level matrix (what=0) or interpolation (what=1) of a subspace hierarchy as set up
+        (FP64, unscaled), as scipy CSR; ``.on_device`` tells whether the set-up ran on the GPU."""
+        import scipy.sparse as sp
+        nnz, dev = ctypes.c_int32(), ctypes.c_int32()
+        check(self._lib.ssv_ams_level_matrix(self._h, subspace, level, what, None, None, None, 0, ctypes.byref(nnz),
+                                             ctypes.byref(dev)))
+        sizes = self.levels(subspace)
+        n = sizes[level][0]
+        m = n if what == 0 else sizes[level + 1][0]
+        rp = np.zeros(n + 1, np.int32)
+        ci = np.zeros(max(nnz.value, 1), np.int32)
+        v = np.zeros(max(nnz.value, 1))
+        check(self._lib.ssv_ams_level_matrix(self._h, subspace, level, what, _capi.i32ptr(rp), _capi.i32ptr(ci),
+                                             v.ctypes.data_as(_capi.PD), nnz.value, ctypes.byref(nnz), None))
+        self.on_device = bool(dev.value)
+        return sp.csr_matrix((v[: nnz.value], ci[: nnz.value], rp), shape=(n, m))
+
     def levels(self, subspace):
         """AMG hierarchy of a subspace (0 gradient, 1..3 Nedelec x/y/z): [(rows, nnz), ...]."""
         buf = np.zeros(256, np.int32)

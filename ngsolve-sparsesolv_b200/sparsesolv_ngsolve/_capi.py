@@ -224,6 +224,7 @@ SIGNATURES = [
     ("ssv_batch_last_timing", I32, [P, PD, PD, PI32, ctypes.POINTER(ctypes.c_int64)]),
     ("ssv_ams_get_precision", I32, [P, PI32]),
     ("ssv_ams_setup_times", I32, [P, PD]),
+    ("ssv_ams_level_matrix", I32, [P, I32, I32, I32, PI32, PI32, PD, I32, PI32, PI32]),
     ("ssv_ams_profile", I32, [P, I32, I32, I32, ctypes.POINTER(ssv_phase_profile)]),
     ("ssv_mlp_create", I32, [I32, I32, ctypes.c_uint64, PP]),
     ("ssv_mlp_destroy", I32, [P]),
