@@ -549,8 +549,8 @@ def _l2_evict(buf):
 
 def batched_family_extra(ss, nc=40):
     """Config 4: the 40^3 eddy-current family, 8 frequencies x 4 sources (32
-    systems). The mixed batched form (FP32-form ComplexCompactAMS per
-    frequency, refined COCR cycles to a true residual of 1e-10, one launch
+    systems). The mixed batched form (ComplexCompactAMS per frequency with its
+    nodal hierarchies in FP32, refined COCR cycles to a true residual of 1e-10, one launch
     graph with the autotuned SpMM) against 32 sequential plain FP64 GPU solves
     (COCRSolver, FP64 ComplexCompactAMS); the FP64 batched form beside it.
     Device time (CUDA events), inputs resident in HBM."""
@@ -621,7 +621,7 @@ def batched_family_extra(ss, nc=40):
     del bs
     # the mixed batched form
     for p in pres:
-        p.precision = "fp32"
+        p.precision = "fp32_nodal"
     bm = ss.BatchedCOCRSolver(d["K"], d["M"], d["omegas"], pres, nrhs=4, freedofs=d["freedofs"], maxiter=1500,
                               tol=1e-10, restart_drop=REFINE_DROP)
     out["batched_mixed_s"] = timed(lambda: bm.solve_dev(d_B.data_ptr(), d_X.data_ptr()))
@@ -745,7 +745,7 @@ def run_eddy(args, rank, world, local):
         return statistics.mean(out)
 
     e2e_plain = e2e(inv, max(2, args.steps // 4))
-    pre.precision = "fp32"
+    pre.precision = "fp32_nodal"
     mixed = timed_form(solve_mixed, False)
     invm = ss.MixedCOCRSolver(A, pre, freedofs=d["freedofs"], maxiter=EDDY_MAXITER, tol=1e-10,
                               restart_drop=REFINE_DROP)
@@ -778,9 +778,10 @@ def run_eddy(args, rank, world, local):
                   iterations=plain["iterations"], ms_per_iter=value * 1e3 / max(plain["iterations"], 1),
                   spmv_GBps=gbps(spmv), true_rel_residual=plain["true_rel_residual"], ams_setup_s=setup_s,
                   ams_setup_breakdown_s=setup_times,
-                  mixed_form="FP32-form ComplexCompactAMS (subspace hierarchies FP32, diagonally scaled; fine level, "
-                             "transfers, coarsest solves FP64) under refined COCR: cycles restarted from the FP64 true "
-                             f"residual after a {REFINE_DROP:g} drop, stop on the true residual",
+                  mixed_form="ComplexCompactAMS with the three nodal hierarchies in FP32 (diagonally scaled) and the "
+                             "gradient hierarchy, fine level, transfers and coarsest solves FP64, under refined COCR: "
+                             f"cycles restarted from the FP64 true residual after a {REFINE_DROP:g} drop, stop on the "
+                             "true residual",
                   mixed_time_to_solution_s=mixed["s"], mixed_iterations=mixed["iterations"],
                   mixed_cycles=mixed["cycles"], mixed_true_rel_residual=mixed["true_rel_residual"],
                   mixed_ms_per_iter=mixed["s"] * 1e3 / max(mixed["iterations"], 1),

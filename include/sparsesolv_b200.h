@@ -54,7 +54,7 @@ enum ssv_method { SSV_METHOD_ICCG = 0, SSV_METHOD_SGSMRTR = 1, SSV_METHOD_CG = 2
 /* Precision of a preconditioner application (new: no reference counterpart).
  * FP64 is the drop-in; FP32 stores L / auxiliary matrices in float and applies
  * in float while the outer Krylov recurrence stays in double. */
-enum ssv_precision { SSV_PREC_FP64 = 0, SSV_PREC_FP32 = 1 };
+enum ssv_precision { SSV_PREC_FP64 = 0, SSV_PREC_FP32 = 1, SSV_PREC_FP32_NODAL = 2 };
 
 /*
  * Field-for-field mirror of sparsesolv::SolverConfig
@@ -289,6 +289,10 @@ int ssv_ams_update(ssv_precond* p, ssv_matrix* new_A);
 int ssv_ams_levels(const ssv_precond* p, int32_t subspace, int32_t* sizes, int32_t cap,
                    int32_t* num_levels);
 /* New (no reference counterpart): the FP32-preconditioner form. With
+ * SSV_PREC_FP32_NODAL (AMS only) the gradient hierarchy stays FP64 and the
+ * three nodal hierarchies take the FP32 form (the split that keeps COCR
+ * convergent on mass-dominated eddy-current systems, whose gradient-space
+ * matrices span many decades). With
  * SSV_PREC_FP32 every matrix of the AMS hierarchy, the l1 norms and the work
  * vectors of the cycle are FP32; the coarsest solve and the cycle's FP64
  * input/output stay FP64. Switching re-uploads the hierarchy (no new set-up);

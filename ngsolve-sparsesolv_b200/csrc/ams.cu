@@ -856,7 +856,8 @@ struct AmsState {
     int nhc = 0, nh1 = 0, cycle_type = 1, num_smooth = 1, nv_alloc = 0;
     double w = 1.0;
     bool complex_form = false;
-    bool fp32 = false;
+    bool fp32 = false;    // some subspace hierarchy in FP32
+    bool grad64 = false;  // with fp32: the gradient hierarchy stays FP64, the three nodal ones FP32
     int ndof_complex = 0;
     AmsHost host;
     DevCsr A_bc, G, Gt;                          // FP64 in both forms
@@ -1276,7 +1277,7 @@ static void pi_prolong(const AmsState& a, const T* gx, const T* gy, const T* gz,
 // One AMS cycle (CompactAMS::Mult, compact_ams.hpp:136-195, or the fused
 // ComplexCompactAMS::Mult, complex_compact_ams.hpp:112-154): in -> out, both
 // FP64 with NV columns.
-template <typename T, int NV, bool RECIP>
+template <typename TG, typename TN, int NV, bool RECIP>
 static void ams_cycle(AmsState& a, const double* in, double* out, const KState* st, cudaStream_t s) {
     const int n = a.nhc;
     const uint8_t* fd = a.has_fd ? a.fd.get() : nullptr;
@@ -1324,24 +1325,24 @@ static void ams_cycle(AmsState& a, const double* in, double* out, const KState* 
     };
     auto gradient = [&]() {
         residual();
-        mv_spmv<double, double, T, NV, MV_AX, RECIP>(a.Gt, r, a.rs[0].as<T>(), nullptr, nullptr, T(0), st, s);
-        T* g = vcycle<T, NV, RECIP>(a.amg[0], 0, a.rs[0].as<T>(), 1, st, s);
-        mv_spmv<double, T, double, NV, MV_ADD, RECIP>(a.G, g, cur, nullptr, nullptr, a.w, st, s);
+        mv_spmv<double, double, TG, NV, MV_AX, RECIP>(a.Gt, r, a.rs[0].as<TG>(), nullptr, nullptr, TG(0), st, s);
+        TG* g = vcycle<TG, NV, RECIP>(a.amg[0], 0, a.rs[0].as<TG>(), 1, st, s);
+        mv_spmv<double, TG, double, NV, MV_ADD, RECIP>(a.G, g, cur, nullptr, nullptr, a.w, st, s);
     };
     auto nodal = [&]() {
         residual();
-        pi_restrict<T, NV>(a, r, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), st, s);
-        T* g3[3];
+        pi_restrict<TN, NV>(a, r, a.rs[1].as<TN>(), a.rs[2].as<TN>(), a.rs[3].as<TN>(), st, s);
+        TN* g3[3];
         if (tri_ok(a)) {  // one chain of launches carrying all three hierarchies
-            vcycle3<T, NV, RECIP>(a, st, s, g3);
+            vcycle3<TN, NV, RECIP>(a, st, s, g3);
         } else {  // the three V-cycles are independent (own hierarchies and vectors)
             a.forks.fork(s, 2);
-            g3[0] = vcycle<T, NV, RECIP>(a.amg[1], 0, a.rs[1].as<T>(), 1, st, s);
-            g3[1] = vcycle<T, NV, RECIP>(a.amg[2], 0, a.rs[2].as<T>(), 1, st, a.forks.side[0]);
-            g3[2] = vcycle<T, NV, RECIP>(a.amg[3], 0, a.rs[3].as<T>(), 1, st, a.forks.side[1]);
+            g3[0] = vcycle<TN, NV, RECIP>(a.amg[1], 0, a.rs[1].as<TN>(), 1, st, s);
+            g3[1] = vcycle<TN, NV, RECIP>(a.amg[2], 0, a.rs[2].as<TN>(), 1, st, a.forks.side[0]);
+            g3[2] = vcycle<TN, NV, RECIP>(a.amg[3], 0, a.rs[3].as<TN>(), 1, st, a.forks.side[1]);
             a.forks.join(s, 2);
         }
-        pi_prolong<T, NV>(a, g3[0], g3[1], g3[2], cur, st, s);
+        pi_prolong<TN, NV>(a, g3[0], g3[1], g3[2], cur, st, s);
     };
     if (a.cycle_type == 7) {
         fine_smooth(); gradient(); fine_smooth(); nodal(); fine_smooth(); gradient(); fine_smooth();
@@ -1723,37 +1724,49 @@ static void tune_pi(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1)
     }
 }
 
+// The hierarchy types of the current form: FP64 for every subspace, FP32 for
+// every subspace, or the gradient hierarchy FP64 with the nodal ones FP32.
+template <typename F>
+static void with_forms(const AmsState& a, F&& fn) {
+    if (!a.fp32) fn(double{}, double{});
+    else if (a.grad64) fn(double{}, float{});
+    else fn(float{}, float{});
+}
+
 template <typename T, int NV>
-static void tune_all_nv(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
-    tune_csr<double, double, double, NV>(a.A_bc, a.xa.get(), a.xb.get(), a.r.get(), s, e0, e1);
-    tune_csr<double, double, T, NV>(a.Gt, a.r.get(), a.rs[0].as<T>(), nullptr, s, e0, e1, true);
-    tune_csr<double, T, double, NV>(a.G, a.rs[0].as<T>(), a.xb.get(), nullptr, s, e0, e1, true);
-    tune_pi<T, NV>(a, s, e0, e1);
-    for (int sub = 0; sub < 4; ++sub) {
-        auto& L = a.amg[sub];
-        for (size_t l = 0; l < L.size(); ++l) {
-            tune_csr<T, T, T, NV>(L[l].A, L[l].xa.as<T>(), L[l].xb.as<T>(), L[l].b.as<T>(), s, e0, e1);
-            if (l + 1 < L.size()) {
-                tune_csr<T, T, T, NV>(L[l].P, L[l + 1].xa.as<T>(), L[l].r.as<T>(), nullptr, s, e0, e1);
-                tune_csr<T, T, T, NV>(L[l].Pt, L[l].r.as<T>(), L[l + 1].b.as<T>(), nullptr, s, e0, e1);
-                if (L[l].R.n) {  // fused down: b_{l+1} = R b_l; fused up: x_l = U [b_l; e]
-                    tune_csr<T, T, T, NV>(L[l].R, L[l].b.as<T>(), L[l + 1].b.as<T>(), nullptr, s, e0, e1);
-                    tune_csr<T, T, T, NV>(L[l].U, L[l].b.as<T>(), L[l].xb.as<T>(), L[l + 1].xa.as<T>(), s, e0, e1,
-                                          false, true);
-                }
+static void tune_levels(std::vector<AmgDevLevel>& L, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+    for (size_t l = 0; l < L.size(); ++l) {
+        tune_csr<T, T, T, NV>(L[l].A, L[l].xa.as<T>(), L[l].xb.as<T>(), L[l].b.as<T>(), s, e0, e1);
+        if (l + 1 < L.size()) {
+            tune_csr<T, T, T, NV>(L[l].P, L[l + 1].xa.as<T>(), L[l].r.as<T>(), nullptr, s, e0, e1);
+            tune_csr<T, T, T, NV>(L[l].Pt, L[l].r.as<T>(), L[l + 1].b.as<T>(), nullptr, s, e0, e1);
+            if (L[l].R.n) {  // fused down: b_{l+1} = R b_l; fused up: x_l = U [b_l; e]
+                tune_csr<T, T, T, NV>(L[l].R, L[l].b.as<T>(), L[l + 1].b.as<T>(), nullptr, s, e0, e1);
+                tune_csr<T, T, T, NV>(L[l].U, L[l].b.as<T>(), L[l].xb.as<T>(), L[l + 1].xa.as<T>(), s, e0, e1,
+                                      false, true);
             }
         }
     }
 }
 
-template <typename T>
+template <typename TG, typename TN, int NV>
+static void tune_all_nv(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+    tune_csr<double, double, double, NV>(a.A_bc, a.xa.get(), a.xb.get(), a.r.get(), s, e0, e1);
+    tune_csr<double, double, TG, NV>(a.Gt, a.r.get(), a.rs[0].as<TG>(), nullptr, s, e0, e1, true);
+    tune_csr<double, TG, double, NV>(a.G, a.rs[0].as<TG>(), a.xb.get(), nullptr, s, e0, e1, true);
+    tune_pi<TN, NV>(a, s, e0, e1);
+    tune_levels<TG, NV>(a.amg[0], s, e0, e1);
+    for (int sub = 1; sub < 4; ++sub) tune_levels<TN, NV>(a.amg[sub], s, e0, e1);
+}
+
+template <typename TG, typename TN>
 static void tune_lanes_t(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
     if (a.complex_form) {
-        tune_all_nv<T, 2>(a, s, e0, e1);
-        if (a.nv_alloc >= 8) tune_all_nv<T, 8>(a, s, e0, e1);
+        tune_all_nv<TG, TN, 2>(a, s, e0, e1);
+        if (a.nv_alloc >= 8) tune_all_nv<TG, TN, 8>(a, s, e0, e1);
     } else {
-        tune_all_nv<T, 1>(a, s, e0, e1);
-        if (a.nv_alloc >= 4) tune_all_nv<T, 4>(a, s, e0, e1);
+        tune_all_nv<TG, TN, 1>(a, s, e0, e1);
+        if (a.nv_alloc >= 4) tune_all_nv<TG, TN, 4>(a, s, e0, e1);
     }
 }
 
@@ -1762,8 +1775,7 @@ static void tune_lanes(AmsState& a) {
     cudaEvent_t e0, e1;
     SSV_CUDA(cudaEventCreate(&e0));
     SSV_CUDA(cudaEventCreate(&e1));
-    if (a.fp32) tune_lanes_t<float>(a, s, e0, e1);
-    else tune_lanes_t<double>(a, s, e0, e1);
+    with_forms(a, [&](auto g, auto n) { tune_lanes_t<decltype(g), decltype(n)>(a, s, e0, e1); });
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
 }
@@ -1861,6 +1873,9 @@ static std::vector<double> inverted(const std::vector<double>& v) {
     return r;
 }
 
+// whether subspace sub's hierarchy is held in FP32 (diagonally scaled)
+static bool sub_lo(const AmsState& a, int sub) { return a.fp32 && !(a.grad64 && sub == 0); }
+
 // Matrix part: A_bc and its l1 norms (FP64), the four AMG hierarchies (in the
 // chosen form; the coarsest factors FP64), and in the FP32 form the scaled
 // transfer values.
@@ -1881,18 +1896,20 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
     const double tf0 = wall_seconds();
     if (fused_enabled()) {
         std::vector<std::thread> th;
-        for (int sub = a.fp32 ? 1 : 0; sub < 4; ++sub)
+        for (int sub = 0; sub < 4; ++sub) {
+            if (sub_lo(a, sub) && sub == 0) continue;  // FP32 gradient hierarchies keep the four passes
             th.emplace_back([&a, &fused, sub] {
+                const bool lo = sub_lo(a, sub);
                 const auto& hl = a.host.amg[sub].levels;
                 fused[sub].resize(hl.empty() ? 0 : hl.size() - 1);
                 std::vector<std::vector<double>> sc(hl.size()), isc(hl.size());
-                if (a.fp32)
+                if (lo)
                     for (size_t l = 0; l < hl.size(); ++l) {
                         sc[l] = diag_scale(hl[l].A);
                         isc[l] = inverted(sc[l]);
                     }
                 for (size_t l = 0; l + 1 < hl.size(); ++l) {
-                    if (!a.fp32) {
+                    if (!lo) {
                         fused[sub][l] = fused_level(hl[l].A, hl[l].P, hl[l].Pt, hl[l].l1);
                         continue;
                     }
@@ -1903,22 +1920,24 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
                                     scaled_csr(hl[l].Pt, &isc[l + 1], &sc[l]), l1s);
                 }
             });
+        }
         for (auto& t : th) t.join();
     }
     a.t_fused = wall_seconds() - tf0;
     for (int sub = 0; sub < 4; ++sub) {
+        const bool lo = sub_lo(a, sub);
         const auto& hl = a.host.amg[sub].levels;
         a.amg[sub].clear();
         a.amg[sub].resize(hl.size());
         std::vector<std::vector<double>> sc(hl.size()), isc(hl.size());
         for (size_t l = 0; l < hl.size(); ++l) {
-            sc[l] = a.fp32 ? diag_scale(hl[l].A) : std::vector<double>(hl[l].A.n, 1.0);
+            sc[l] = lo ? diag_scale(hl[l].A) : std::vector<double>(hl[l].A.n, 1.0);
             isc[l] = inverted(sc[l]);
         }
         for (size_t l = 0; l < hl.size(); ++l) {
             AmgDevLevel& dl = a.amg[sub][l];
             const int nl = hl[l].A.n;
-            if (a.fp32) {
+            if (lo) {
                 dl.A.upload(scaled_csr(hl[l].A, &isc[l], &isc[l]), true, s);
                 std::vector<double> l1s(nl);
                 for (int i = 0; i < nl; ++i) l1s[i] = hl[l].l1[i] * isc[l][i] * isc[l][i];
@@ -1939,7 +1958,7 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
             }
             dl.direct = hl[l].direct;
             if (dl.direct) {  // FP64 in both forms
-                if (a.fp32) {
+                if (lo) {
                     std::vector<double> li = hl[l].linv, lt = hl[l].linvt, pv = hl[l].piv;
                     for (int i = 0; i < nl; ++i)
                         for (int k = 0; k < nl; ++k) {
@@ -1958,17 +1977,17 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
             }
         }
         for (size_t l = 0; l < fused[sub].size(); ++l) {
-            a.amg[sub][l].R.upload(fused[sub][l].R, a.fp32, s);
-            a.amg[sub][l].U.upload(fused[sub][l].U, a.fp32, s);
+            a.amg[sub][l].R.upload(fused[sub][l].R, lo, s);
+            a.amg[sub][l].U.upload(fused[sub][l].U, lo, s);
         }
         // level-0 scaling folded into this subspace's transfers
         if (sub == 0) {
-            upload_fine(a.G, a.fp32 ? scaled_csr(a.host.G, nullptr, &isc[0]) : a.host.G, s);
-            upload_fine(a.Gt, a.fp32 ? scaled_csr(a.host.Gt, &isc[0], nullptr) : a.host.Gt, s);
+            upload_fine(a.G, lo ? scaled_csr(a.host.G, nullptr, &isc[0]) : a.host.G, s);
+            upload_fine(a.Gt, lo ? scaled_csr(a.host.Gt, &isc[0], nullptr) : a.host.Gt, s);
         } else {
             const int d = sub - 1;
-            const HostCsr pi = a.fp32 ? scaled_csr(a.host.Pi[d], nullptr, &isc[0]) : a.host.Pi[d];
-            const HostCsr pit = a.fp32 ? scaled_csr(a.host.Pit[d], &isc[0], nullptr) : a.host.Pit[d];
+            const HostCsr pi = lo ? scaled_csr(a.host.Pi[d], nullptr, &isc[0]) : a.host.Pi[d];
+            const HostCsr pit = lo ? scaled_csr(a.host.Pit[d], &isc[0], nullptr) : a.host.Pit[d];
             a.Piv[d].upload(pi.v.data(), pi.v.size(), s);
             a.Pitv[d].upload(pit.v.data(), pit.v.size(), s);
         }
@@ -2061,11 +2080,12 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
         const size_t L = hl.size();
         a.amg[sub].clear();
         a.amg[sub].resize(L);
+        const bool lo = sub_lo(a, sub);
         std::vector<DevBuf<double>> sc(L), isc(L);
-        if (a.fp32)
+        if (lo)
             for (size_t l = 0; l < L; ++l) d_diag_scale(hl[l].A, sc[l], isc[l], s);
-        // in the FP32 form only the three nodal hierarchies take the fused products
-        const bool fuse = fused_enabled() && (!a.fp32 || sub >= 1);
+        // FP32 gradient hierarchies keep the four passes (fused, they lose too much)
+        const bool fuse = fused_enabled() && !(lo && sub == 0);
         for (size_t l = 0; l < L; ++l) {
             AmgDevLevel& dl = a.amg[sub][l];
             const int nl = hl[l].A.n;
@@ -2076,7 +2096,7 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
             const DCsr* Pl = last ? nullptr : &hl[l].P;
             const DCsr* Ptl = last ? nullptr : &hl[l].Pt;
             const double* l1p = hl[l].l1.get();
-            if (a.fp32) {
+            if (lo) {
                 d_scaled(hl[l].A, isc[l].get(), isc[l].get(), As, s);
                 Al = &As;
                 l1s.alloc(std::max(nl, 1));
@@ -2089,17 +2109,17 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
                     Ptl = &Pts;
                 }
             }
-            devcsr_from(dl.A, *Al, a.fp32, s);
-            dl.l1.set_dev(l1p, nl, a.fp32, s);
+            devcsr_from(dl.A, *Al, lo, s);
+            dl.l1.set_dev(l1p, nl, lo, s);
             d_reciprocal(nl, l1p, il1.get(), s);
-            dl.il1.set_dev(il1.get(), nl, a.fp32, s);
+            dl.il1.set_dev(il1.get(), nl, lo, s);
             if (!last) {
-                devcsr_from(dl.P, *Pl, a.fp32, s);
-                devcsr_from(dl.Pt, *Ptl, a.fp32, s);
+                devcsr_from(dl.P, *Pl, lo, s);
+                devcsr_from(dl.Pt, *Ptl, lo, s);
             }
             dl.direct = hl[l].direct;
             if (dl.direct) {  // FP64 in both forms; in the FP32 form scaled like the level
-                if (a.fp32) {
+                if (lo) {
                     std::vector<double> hs(nl), his(nl);
                     SSV_CUDA(cudaMemcpyAsync(hs.data(), sc[l].get(), sizeof(double) * nl, cudaMemcpyDeviceToHost, s));
                     SSV_CUDA(cudaMemcpyAsync(his.data(), isc[l].get(), sizeof(double) * nl, cudaMemcpyDeviceToHost, s));
@@ -2125,8 +2145,8 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
                 const double tf0 = wall_seconds();
                 DCsr R, U;
                 if (d_fused_level(*Al, *Pl, *Ptl, l1p, R, U, s)) {
-                    devcsr_from(dl.R, R, a.fp32, s);
-                    devcsr_from(dl.U, U, a.fp32, s);
+                    devcsr_from(dl.R, R, lo, s);
+                    devcsr_from(dl.U, U, lo, s);
                 }
                 SSV_CUDA(cudaStreamSynchronize(s));
                 t_fused += wall_seconds() - tf0;
@@ -2135,7 +2155,7 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
         }
         // level-0 scaling folded into this subspace's transfers
         if (sub == 0) {
-            if (a.fp32) {
+            if (lo) {
                 DCsr Gs, Gts;
                 d_scaled(D.G, nullptr, isc[0].get(), Gs, s);
                 d_scaled(D.Gt, isc[0].get(), nullptr, Gts, s);
@@ -2151,7 +2171,7 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
             const int64_t nz = D.Pi[d].nnz;
             a.Piv[d].alloc(std::max<int64_t>(nz, 1));
             a.Pitv[d].alloc(std::max<int64_t>(nz, 1));
-            if (a.fp32) {
+            if (lo) {
                 DCsr pi, pit;
                 d_scaled(D.Pi[d], nullptr, isc[0].get(), pi, s);
                 d_scaled(D.Pit[d], isc[0].get(), nullptr, pit, s);
@@ -2250,11 +2270,13 @@ void ams_update(AmsState* a, const ssv_matrix* A) { ams_rebuild(*a, A); }
 // Switch between the FP64 and FP32 forms: the host keeps the hierarchy, so
 // this is a re-upload, no new set-up.
 void ams_set_precision(AmsState* a, int precision) {
-    const bool lo = precision == SSV_PREC_FP32;
-    if (lo == a->fp32) return;
+    const bool lo = precision == SSV_PREC_FP32 || precision == SSV_PREC_FP32_NODAL;
+    const bool g64 = precision == SSV_PREC_FP32_NODAL;
+    if (lo == a->fp32 && g64 == a->grad64) return;
     cudaStream_t s = stream();
     const double t0 = wall_seconds();
     a->fp32 = lo;
+    a->grad64 = g64;
     a->t_tune = 0;
     a->t_host = 0;
     if (a->dev.on) ams_build_cycle(*a, true, s);
@@ -2264,24 +2286,26 @@ void ams_set_precision(AmsState* a, int precision) {
     a->t_total = wall_seconds() - t0;
 }
 
-int ams_precision(const AmsState* a) { return a->fp32 ? SSV_PREC_FP32 : SSV_PREC_FP64; }
+int ams_precision(const AmsState* a) {
+    return !a->fp32 ? SSV_PREC_FP64 : a->grad64 ? SSV_PREC_FP32_NODAL : SSV_PREC_FP32;
+}
 
 void ams_reserve_block(AmsState* a, int nrhs) {
     ams_reserve(*a, nrhs * (a->complex_form ? 2 : 1));
     SSV_CUDA(cudaStreamSynchronize(stream()));
 }
 
-template <typename T>
+template <typename TG, typename TN>
 static void ams_block_t(AmsState& a, const double* in, double* out, int nrhs, const KState* st, cudaStream_t s) {
     if (a.complex_form) {
         switch (nrhs) {
-            case 1: ams_cycle<T, 2, true>(a, in, out, st, s); return;
-            case 4: ams_cycle<T, 8, true>(a, in, out, st, s); return;
+            case 1: ams_cycle<TG, TN, 2, true>(a, in, out, st, s); return;
+            case 4: ams_cycle<TG, TN, 8, true>(a, in, out, st, s); return;
         }
     } else {
         switch (nrhs) {
-            case 1: ams_cycle<T, 1, false>(a, in, out, st, s); return;
-            case 4: ams_cycle<T, 4, false>(a, in, out, st, s); return;
+            case 1: ams_cycle<TG, TN, 1, false>(a, in, out, st, s); return;
+            case 4: ams_cycle<TG, TN, 4, false>(a, in, out, st, s); return;
         }
     }
     fail(SSV_ERR_INVALID_ARG, "AMS block apply: nrhs must be 1 or 4");
@@ -2290,8 +2314,7 @@ static void ams_block_t(AmsState& a, const double* in, double* out, int nrhs, co
 // nrhs right-hand sides, row-interleaved ([row][rhs], complex as Re/Im pairs).
 void ams_apply_block(AmsState* a, const double* in, double* out, int nrhs, const KState* st, cudaStream_t s) {
     if (nrhs * (a->complex_form ? 2 : 1) > a->nv_alloc) fail(SSV_ERR_INVALID_ARG, "AMS block apply: reserve first");
-    if (a->fp32) ams_block_t<float>(*a, in, out, nrhs, st, s);
-    else ams_block_t<double>(*a, in, out, nrhs, st, s);
+    with_forms(*a, [&](auto g, auto n) { ams_block_t<decltype(g), decltype(n)>(*a, in, out, nrhs, st, s); });
 }
 
 // ---------------------------------------------------------------------------
@@ -2321,11 +2344,11 @@ static double vcycle_bytes(const std::vector<AmgDevLevel>& L, int l, int NV, int
     return b;
 }
 
-template <typename T, int NV, bool RECIP>
+template <typename TG, typename TN, int NV, bool RECIP>
 static void ams_profile_t(AmsState& a, int reps, bool cold, ssv_phase_profile* out) {
     cudaStream_t s = stream();
     const int n = a.nhc, n1 = a.nh1;
-    const int tb = (int)sizeof(T);
+    const int tg = (int)sizeof(TG), tn = (int)sizeof(TN);
     DevBuf<double> pin((size_t)n * NV), pout((size_t)n * NV);
     pin.zero(s);
     double* cur = a.xa.get();
@@ -2345,59 +2368,59 @@ static void ams_profile_t(AmsState& a, int reps, bool cold, ssv_phase_profile* o
         out->bytes[i] = bytes;
         out->kernels[i] = kernels;
     };
-    const double N = n, N1 = n1, V = 8.0 * NV, Vt = (double)tb * NV;
+    const double N = n, N1 = n1, V = 8.0 * NV, Vg = (double)tg * NV, Vn = (double)tn * NV;
     const double fine_res = csr_pass_bytes(a.A_bc, 8) + 3 * N * V;
     const double fine_jac = csr_pass_bytes(a.A_bc, 8) + N * (3 * V + 8);
-    const double grad_vc = vcycle_bytes(a.amg[0], 0, NV, tb);
+    const double grad_vc = vcycle_bytes(a.amg[0], 0, NV, tg);
     double nod_vc = 0;
-    for (int k = 1; k < 4; ++k) nod_vc += vcycle_bytes(a.amg[k], 0, NV, tb);
-    const double g_tr = csr_pass_bytes(a.Gt, 8) + N * V + N1 * Vt + csr_pass_bytes(a.G, 8) + N1 * Vt + 2 * N * V;
-    const double pi_tr = (double)a.Gt.nnz * (4 + 24) + 4.0 * (n1 + 1) + N * V + 3 * N1 * Vt +
-                         (double)a.G.nnz * (4 + 24) + 4.0 * (n + 1) + 3 * N1 * Vt + 2 * N * V;
+    for (int k = 1; k < 4; ++k) nod_vc += vcycle_bytes(a.amg[k], 0, NV, tn);
+    const double g_tr = csr_pass_bytes(a.Gt, 8) + N * V + N1 * Vg + csr_pass_bytes(a.G, 8) + N1 * Vg + 2 * N * V;
+    const double pi_tr = (double)a.Gt.nnz * (4 + 24) + 4.0 * (n1 + 1) + N * V + 3 * N1 * Vn +
+                         (double)a.G.nnz * (4 + 24) + 4.0 * (n + 1) + 3 * N1 * Vn + 2 * N * V;
     // cycle 1 (01210): 2 masks, first sweep, 3 residuals, 2 + 1 corrections, one final sweep
     const double cyc = 2 * (2 * N * V + N) + N * (2 * V + 8) + 3 * fine_res + 2 * grad_vc + nod_vc + 2 * g_tr + pi_tr +
                        fine_jac;
-    timed("ams_cycle", cyc, 0, [&] { ams_cycle<T, NV, RECIP>(a, pin.get(), pout.get(), nullptr, s); });
+    timed("ams_cycle", cyc, 0, [&] { ams_cycle<TG, TN, NV, RECIP>(a, pin.get(), pout.get(), nullptr, s); });
     timed("fine_residual", fine_res, 1, [&] {
         mv_spmv<double, double, double, NV, MV_RES, RECIP>(a.A_bc, cur, r, a.b0.get(), nullptr, 0.0, nullptr, s);
     });
     timed("fine_smooth", fine_jac, 1, [&] {
         mv_spmv<double, double, double, NV, MV_JAC, RECIP>(a.A_bc, cur, alt, a.b0.get(), d, 0.0, nullptr, s);
     });
-    timed("grad_vcycle", grad_vc, 0, [&] { vcycle<T, NV, RECIP>(a.amg[0], 0, a.rs[0].as<T>(), 1, nullptr, s); });
+    timed("grad_vcycle", grad_vc, 0, [&] { vcycle<TG, NV, RECIP>(a.amg[0], 0, a.rs[0].as<TG>(), 1, nullptr, s); });
     timed("nodal_vcycles", nod_vc, 0, [&] {
         if (tri_ok(a)) {
-            T* g3[3];
-            vcycle3<T, NV, RECIP>(a, nullptr, s, g3);
+            TN* g3[3];
+            vcycle3<TN, NV, RECIP>(a, nullptr, s, g3);
             return;
         }
         a.forks.fork(s, 2);
-        vcycle<T, NV, RECIP>(a.amg[1], 0, a.rs[1].as<T>(), 1, nullptr, s);
-        vcycle<T, NV, RECIP>(a.amg[2], 0, a.rs[2].as<T>(), 1, nullptr, a.forks.side[0]);
-        vcycle<T, NV, RECIP>(a.amg[3], 0, a.rs[3].as<T>(), 1, nullptr, a.forks.side[1]);
+        vcycle<TN, NV, RECIP>(a.amg[1], 0, a.rs[1].as<TN>(), 1, nullptr, s);
+        vcycle<TN, NV, RECIP>(a.amg[2], 0, a.rs[2].as<TN>(), 1, nullptr, a.forks.side[0]);
+        vcycle<TN, NV, RECIP>(a.amg[3], 0, a.rs[3].as<TN>(), 1, nullptr, a.forks.side[1]);
         a.forks.join(s, 2);
     });
     timed("grad_transfers", g_tr, 2, [&] {
-        mv_spmv<double, double, T, NV, MV_AX, RECIP>(a.Gt, r, a.rs[0].as<T>(), nullptr, nullptr, T(0), nullptr, s);
-        mv_spmv<double, T, double, NV, MV_ADD, RECIP>(a.G, a.rs[0].as<T>(), alt, nullptr, nullptr, a.w, nullptr, s);
+        mv_spmv<double, double, TG, NV, MV_AX, RECIP>(a.Gt, r, a.rs[0].as<TG>(), nullptr, nullptr, TG(0), nullptr, s);
+        mv_spmv<double, TG, double, NV, MV_ADD, RECIP>(a.G, a.rs[0].as<TG>(), alt, nullptr, nullptr, a.w, nullptr, s);
     });
     timed("pi_transfers", pi_tr, 2, [&] {
-        pi_restrict<T, NV>(a, r, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), nullptr, s);
-        pi_prolong<T, NV>(a, a.rs[1].as<T>(), a.rs[2].as<T>(), a.rs[3].as<T>(), alt, nullptr, s);
+        pi_restrict<TN, NV>(a, r, a.rs[1].as<TN>(), a.rs[2].as<TN>(), a.rs[3].as<TN>(), nullptr, s);
+        pi_prolong<TN, NV>(a, a.rs[1].as<TN>(), a.rs[2].as<TN>(), a.rs[3].as<TN>(), alt, nullptr, s);
     });
     SSV_CUDA(cudaEventDestroy(e0));
     SSV_CUDA(cudaEventDestroy(e1));
     SSV_CUDA(cudaStreamSynchronize(s));
 }
 
-template <typename T>
+template <typename TG, typename TN>
 static void ams_profile_nrhs(AmsState& a, int nrhs, int reps, bool cold, ssv_phase_profile* out) {
     if (a.complex_form) {
-        if (nrhs == 1) ams_profile_t<T, 2, true>(a, reps, cold, out);
-        else ams_profile_t<T, 8, true>(a, reps, cold, out);
+        if (nrhs == 1) ams_profile_t<TG, TN, 2, true>(a, reps, cold, out);
+        else ams_profile_t<TG, TN, 8, true>(a, reps, cold, out);
     } else {
-        if (nrhs == 1) ams_profile_t<T, 1, false>(a, reps, cold, out);
-        else ams_profile_t<T, 4, false>(a, reps, cold, out);
+        if (nrhs == 1) ams_profile_t<TG, TN, 1, false>(a, reps, cold, out);
+        else ams_profile_t<TG, TN, 4, false>(a, reps, cold, out);
     }
 }
 
@@ -2405,8 +2428,9 @@ void ams_profile(AmsState* a, int nrhs, int reps, int flags, ssv_phase_profile* 
     if (nrhs != 1 && nrhs != 4) fail(SSV_ERR_INVALID_ARG, "ssv_ams_profile: nrhs must be 1 or 4");
     ams_reserve(*a, nrhs * (a->complex_form ? 2 : 1));
     const bool cold = (flags & SSV_PROFILE_COLD) != 0;
-    if (a->fp32) ams_profile_nrhs<float>(*a, nrhs, std::max(reps, 1), cold, out);
-    else ams_profile_nrhs<double>(*a, nrhs, std::max(reps, 1), cold, out);
+    with_forms(*a, [&](auto g, auto n) {
+        ams_profile_nrhs<decltype(g), decltype(n)>(*a, nrhs, std::max(reps, 1), cold, out);
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -2543,8 +2567,7 @@ void precond_apply_any<double>(ssv_precond* p, const double* x, double* y, const
     else if (p->kind == 4) sgs_apply_dev<double>(p, x, y, st, s);
     else if (p->kind == 5) amg_apply(*p->amg, x, y, st, s);
     else if (p->kind == 2) {
-        if (p->ams->fp32) ams_cycle<float, 1, false>(*p->ams, x, y, st, s);
-        else ams_cycle<double, 1, false>(*p->ams, x, y, st, s);
+        with_forms(*p->ams, [&](auto g, auto n) { ams_cycle<decltype(g), decltype(n), 1, false>(*p->ams, x, y, st, s); });
     } else fail(SSV_ERR_TYPE, "preconditioner is complex; the matrix is real");
 }
 
@@ -2555,8 +2578,7 @@ void precond_apply_any<zdouble>(ssv_precond* p, const zdouble* x, zdouble* y, co
     else if (p->kind == 3) {
         const double* xi = reinterpret_cast<const double*>(x);
         double* yo = reinterpret_cast<double*>(y);
-        if (p->ams->fp32) ams_cycle<float, 2, true>(*p->ams, xi, yo, st, s);
-        else ams_cycle<double, 2, true>(*p->ams, xi, yo, st, s);
+        with_forms(*p->ams, [&](auto g, auto n) { ams_cycle<decltype(g), decltype(n), 2, true>(*p->ams, xi, yo, st, s); });
     } else fail(SSV_ERR_TYPE, "preconditioner is real; the matrix is complex");
 }
 

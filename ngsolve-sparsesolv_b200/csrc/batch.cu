@@ -710,7 +710,7 @@ static int replace_period(const ssv_batch& B) {
     if (B.restart_drop > 0.0) return 0;  // the refined cycles restart from the true residual instead
     if (B.replace_every >= 0) return B.replace_every;
     for (const ssv_precond* p : B.pre)
-        if (p && ams_precision(p->ams.get()) == SSV_PREC_FP32) return 10;
+        if (p && ams_precision(p->ams.get()) != SSV_PREC_FP64) return 10;
     return 0;
 }
 

@@ -421,8 +421,9 @@ int ssv_ams_levels(const ssv_precond* p, int32_t subspace, int32_t* sizes, int32
 int ssv_ams_set_precision(ssv_precond* p, int32_t precision) {
     return guarded([&] {
         if (!p || !p->ams) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_set_precision: not an AMS preconditioner");
-        if (precision != SSV_PREC_FP64 && precision != SSV_PREC_FP32)
-            ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_set_precision: precision must be SSV_PREC_FP64 or SSV_PREC_FP32");
+        if (precision != SSV_PREC_FP64 && precision != SSV_PREC_FP32 && precision != SSV_PREC_FP32_NODAL)
+            ssv::fail(SSV_ERR_INVALID_ARG,
+                      "ssv_ams_set_precision: precision must be SSV_PREC_FP64, SSV_PREC_FP32 or SSV_PREC_FP32_NODAL");
         ssv::ams_set_precision(p->ams.get(), precision);
     });
 }

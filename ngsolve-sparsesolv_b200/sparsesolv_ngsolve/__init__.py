@@ -787,17 +787,20 @@ class _AmsBase(_PrecondBase):
 
     @property
     def precision(self):
-        """"fp64" (drop-in) or "fp32" (new: FP32 hierarchy and cycle, FP64 coarsest solve and in/out)."""
+        """"fp64" (drop-in), "fp32" (new: FP32 hierarchies and cycle, FP64 coarsest solve and in/out) or
+        "fp32_nodal" (new: the gradient hierarchy FP64, the three nodal ones FP32 -- the mixed form for
+        COCR on eddy-current systems)."""
         v = ctypes.c_int32()
         check(self._lib.ssv_ams_get_precision(self._h, ctypes.byref(v)))
-        return "fp32" if v.value == _capi.SSV_PREC_FP32 else "fp64"
+        return {_capi.SSV_PREC_FP32: "fp32", _capi.SSV_PREC_FP32_NODAL: "fp32_nodal"}.get(v.value, "fp64")
 
     @precision.setter
     def precision(self, value):
         v = str(value).lower()
-        if v not in ("fp32", "fp64"):
-            raise ValueError("precision must be 'fp64' or 'fp32'")
-        check(self._lib.ssv_ams_set_precision(self._h, _capi.SSV_PREC_FP32 if v == "fp32" else _capi.SSV_PREC_FP64))
+        if v not in ("fp32", "fp64", "fp32_nodal"):
+            raise ValueError("precision must be 'fp64', 'fp32' or 'fp32_nodal'")
+        check(self._lib.ssv_ams_set_precision(self._h, {"fp32": _capi.SSV_PREC_FP32,
+                                                        "fp32_nodal": _capi.SSV_PREC_FP32_NODAL}.get(v, _capi.SSV_PREC_FP64)))
 
     def profile(self, nrhs=1, reps=20, cold=False):
         """Per-phase device time (ms) and algorithmic bytes of one cycle (measurement hook);

@@ -28,6 +28,7 @@ SSV_C128 = 1
 
 SSV_PREC_FP64 = 0
 SSV_PREC_FP32 = 1
+SSV_PREC_FP32_NODAL = 2
 
 SSV_PROFILE_COLD = 1
 

@@ -5,7 +5,7 @@ the bench measures:
 * config 2: real magnetostatic curl-curl on the 40^3 Kuhn mesh (462,520
   edges), Compact AMS + CG, FP64 and the FP32-preconditioner form;
 * config 3: complex eddy current on the 64^3 Kuhn mesh (1,872,064 edges),
-  ComplexCompactAMS + COCR to 1e-10, FP64 and the mixed form (FP32
+  ComplexCompactAMS + COCR to 1e-10, FP64 and the mixed form (fp32_nodal
   preconditioner under refined COCR);
 * config 4: one column of the 40^3 eddy-current family (8 frequencies x 4
   sources), the single FP64 solve and the batched mixed form.
@@ -97,7 +97,7 @@ def test_config3_eddy_cocr_64():
     x = inv * d["f"]
     tr = _true_res(d["A"], d["freedofs"], x, d["f"])
     e = _rel(x, xo)
-    pre.precision = "fp32"
+    pre.precision = "fp32_nodal"
     invm = ss.MixedCOCRSolver(d["A"], pre, freedofs=d["freedofs"], maxiter=3000, tol=TOL, restart_drop=1e-5)
     xm = invm * d["f"]
     trm = _true_res(d["A"], d["freedofs"], xm, d["f"])
@@ -128,7 +128,7 @@ def test_config4_family_column_40():
     x = inv * d["B"][f, r]
     e = _rel(x, xo)
     for p in pres:
-        p.precision = "fp32"
+        p.precision = "fp32_nodal"
     bs = ss.BatchedCOCRSolver(d["K"], d["M"], d["omegas"], pres, nrhs=4, freedofs=d["freedofs"], maxiter=1500,
                               tol=TOL, restart_drop=1e-5)
     X = bs.Solve(d["B"])
