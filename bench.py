@@ -822,13 +822,91 @@ def run_eddy(args, rank, world, local):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# Nonlinear magnetostatic Newton sequence at 40^3 with the learned initial guess
+# ---------------------------------------------------------------------------
+NEWTON_DESC = {"workload": "newton40: nonlinear magnetostatics on the 40^3 Kuhn mesh (462,520 edges), iron nu(|B|) = "
+                           "nu0 (k1 + k2 |B|^2), k1 = 1e-3, k2 = 5e-3, 20 Newton steps per load x 50 loads "
+                           "(amplitudes U[0.5, 2], default_rng(2)), each step Update() + Compact AMS + CG to 1e-10; "
+                           "per-edge MLP guess (12 features, 64 hidden, FP32, the library's own train/infer kernels) "
+                           "trained on loads 0-29, judged on loads 30-49 against the previous-step guesses",
+               "tol": 1e-10}
+
+
+def run_newton(args, rank, world, local):
+    import torch
+
+    import sparsesolv_ngsolve as ss
+    from sparsesolv_ngsolve import newton as NW
+    if rank != 0:
+        return
+    torch.cuda.set_device(0)
+    prob = NW.NonlinearMagnetostatic(40)
+    amps = np.random.default_rng(2).uniform(0.5, 2.0, 50)
+    nsteps = 20
+    tm = {"update_s": 0.0, "solve_s": 0.0, "updates": 0, "solves": 0}
+
+    class TimedPre:
+        """the AMS preconditioner, its Update() timed"""
+        def __init__(self, J):
+            t0 = time.perf_counter()
+            self.p = ss.CompactAMSPreconditioner(J, prob.G, freedofs=prob.freedofs, coord_x=prob.coords[0],
+                                                 coord_y=prob.coords[1], coord_z=prob.coords[2])
+            self.create_s = time.perf_counter() - t0
+            self._h = self.p._h
+
+        def Update(self, J):
+            t0 = time.perf_counter()
+            self.p.Update(J)
+            tm["update_s"] += time.perf_counter() - t0
+            tm["updates"] += 1
+            self._h = self.p._h
+
+    class TimedSolver:
+        def __init__(self, J, pre):
+            self.inv = ss.PCGSolver(J, pre.p, freedofs=prob.freedofs, maxiter=500, tol=1e-10)
+
+        def Solve(self, rhs, x):
+            t0 = time.perf_counter()
+            r = self.inv.Solve(rhs, x)
+            tm["solve_s"] += time.perf_counter() - t0
+            tm["solves"] += 1
+            return r
+
+    t0 = time.perf_counter()
+    tr = NW.run_loads(prob, amps[:30], nsteps, TimedPre, TimedSolver, collect=True)
+    t_train_loads = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    net, ys, loss = NW.train_predictor(tr)
+    t_train = time.perf_counter() - t0
+    ev = NW.run_loads(prob, amps[29:], nsteps, TimedPre, TimedSolver, predictor=net, scale=tr["scale"], yscale=ys)
+    prev = int(sum(sum(x) for x in ev["iters_prev"][1:]))
+    mlp = int(sum(sum(x) for x in ev["iters_mlp"][1:]))
+    first = [int(x[0]) for x in ev["iters_prev"][1:]], [int(x[0]) for x in ev["iters_mlp"][1:]]
+    per_step = (tm["update_s"] + tm["solve_s"]) / max(tm["solves"], 1)
+    line = {"metric": METRIC, "value": per_step, "unit": UNIT, "n_gpus": world, "steps": tm["solves"], "warmup": 0,
+            "ms_per_step": per_step * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (MLP f32)", "data": "synthetic",
+            "config": dict(NEWTON_DESC, value_is="mean wall time of one Newton linear step: Update() + PCG solve",
+                           update_s_mean=tm["update_s"] / max(tm["updates"], 1),
+                           solve_s_mean=tm["solve_s"] / max(tm["solves"], 1), newton_steps=tm["solves"],
+                           training_loads_wall_s=t_train_loads, mlp_training_s=t_train, mlp_last_loss=loss,
+                           cg_iterations_eval_previous_step_guess=prev, cg_iterations_eval_learned_guess=mlp,
+                           iteration_cut=1.0 - mlp / max(prev, 1),
+                           first_step_iterations_previous=first[0], first_step_iterations_learned=first[1],
+                           start_error_previous_mean=float(np.mean(ev["start_err_prev"])),
+                           start_error_learned_mean=float(np.mean(ev["start_err_mlp"]))),
+            "gpu_launches": None}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="eddy64", choices=["eddy64", "ams40", "iccg64"])
+    ap.add_argument("--workload", default="eddy64", choices=["eddy64", "ams40", "iccg64", "newton40"])
     ap.add_argument("--no-extras", action="store_true", help="skip the batched-family measurement")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"], help="AMS form of --ncu-case")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -857,6 +935,8 @@ def main():
         return run_ams(args, rank, world, local)
     if args.workload == "eddy64":
         return run_eddy(args, rank, world, local)
+    if args.workload == "newton40":
+        return run_newton(args, rank, world, local)
 
     import numpy as np
     import torch

@@ -779,9 +779,18 @@ class _AmsBase(_PrecondBase):
             self._mat.refresh()
             check(self._lib.ssv_ams_update(self._h, None))
             return
-        m = _Matrix(new_mat)
-        if m.cplx:
+        ip, ix, _, cplx, shape = _csr_arrays(new_mat)
+        if cplx:
             raise TypeError("CompactAMS::Update: expected a real SparseMatrix<double>")
+        oip, oix, _, _, oshape = _csr_arrays(self._mat.src)
+        if tuple(shape) == tuple(oshape) and np.array_equal(ip, oip) and np.array_equal(ix, oix):
+            # same pattern (a Newton step's Jacobian): new values into the same device matrix, so
+            # the set-up keeps the layouts that depend only on the pattern
+            self._mat.src = new_mat
+            self._mat.refresh()
+            check(self._lib.ssv_ams_update(self._h, None))
+            return
+        m = _Matrix(new_mat)
         check(self._lib.ssv_ams_update(self._h, m.h))
         self._mat = m  # the handle now refers to the new matrix
 

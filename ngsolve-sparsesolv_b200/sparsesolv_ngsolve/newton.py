@@ -16,7 +16,9 @@ The learned guess: between loads, a per-edge MLP (``EdgeMLP``, 64 hidden
 units, FP32, trained and run by the library's own kernels) predicts the next
 load's solution u*_l from the previous one. Its features per edge are the
 midpoint, the direction, u*_{l-1}[e] / (a_{l-1} S), log10 nu(u*_{l-1}) on the
-edge, a_l, a_{l-1} and a_l / a_{l-1} - 1; its target is the change of the
+edge, a_l, a_{l-1}, a_l / a_{l-1} - 1 and the nonlinear residual of the
+previous solution under the new load, F(u*_{l-1}; a_l f)[e] / (a_l |f|_inf);
+its target is the change of the
 solution per unit amplitude, (u*_l / a_l - u*_{l-1} / a_{l-1})[e] / (S Ys), S a
 fixed solution scale and Ys the training targets' standard deviation. The
 Newton trajectory is the baseline's (each load starts from the previous
@@ -103,12 +105,14 @@ class NonlinearMagnetostatic:
         return s / self.tets_per_edge
 
 
-N_FEATURES = 11
+N_FEATURES = 12
 
 
 def load_features(prob, u_prev, a_prev, a, scale):
-    """Per-edge features (ne x 11, float32) for predicting load a from the solution of load a_prev."""
+    """Per-edge features (ne x 12, float32) for predicting load a from the solution of load a_prev."""
     _, nu = prob.fields(u_prev)
+    f = a * prob.f_unit
+    res = prob.residual(u_prev, f) / max(float(np.abs(f).max()), 1e-300)
     X = np.empty((prob.m.ne, N_FEATURES), np.float32)
     X[:, 0:3] = prob.edge_mid
     X[:, 3:6] = prob.edge_dir
@@ -117,6 +121,7 @@ def load_features(prob, u_prev, a_prev, a, scale):
     X[:, 8] = a / 2.0
     X[:, 9] = a_prev / 2.0
     X[:, 10] = a / a_prev - 1.0
+    X[:, 11] = res
     return X
 
 
