@@ -157,3 +157,24 @@ def test_batch_si_family_converges():
     for f in range(2):
         for r in range(4):
             assert _true_res(d, f, X[f, r], d["B"][f, r]) <= 1e-6
+
+
+def test_batch_columns_match_oracle(fam_well):
+    """Every column of the plain batched solve against the restatement's
+    COCRSolverNGS with the FP64 AMS oracle of its frequency: iterations within
+    2%, solutions to 1e-8 relative (well-conditioned family)."""
+    import sparsesolv_ngsolve as ss
+
+    from oracle import oracle as O
+    d = fam_well
+    pres = _pres(d)
+    bs = ss.BatchedCOCRSolver(d["K"], d["M"], d["omegas"], pres, nrhs=4, freedofs=d["freedofs"], maxiter=500,
+                              tol=1e-10)
+    X = bs.Solve(d["B"])
+    for f in range(len(d["omegas"])):
+        o = O.AmsOracle(d["a_real"][f], d["G"], d["freedofs"], *d["coords"])
+        for r in range(4):
+            xo, ito, _ = o.cocr(d["A"][f], d["B"][f, r], freedofs=d["freedofs"], maxiter=500, tol=1e-10)
+            it = int(bs.iterations[f, r])
+            assert abs(it - ito) <= max(1, int(0.02 * ito)), (f, r, it, ito)
+            assert np.abs(X[f, r] - xo).max() <= 1e-8 * np.abs(xo).max(), (f, r)
