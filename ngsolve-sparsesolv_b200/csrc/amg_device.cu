@@ -18,7 +18,7 @@ constexpr int kT = 256;
 constexpr int kHashBits = 11;
 constexpr int kHash = 1 << kHashBits;  // per-warp slots of the symbolic hash set
 constexpr int kSymWarps = 4;           // warps per block of the symbolic kernels
-constexpr int kSymSmem = 2 * kSymWarps * kHash * (int)sizeof(int);  // table + list, 64 KB
+constexpr int kSymSmem = kSymWarps * kHash * (int)(sizeof(unsigned long long) + sizeof(int));  // 96 KB
 
 inline int blocks_for(int64_t n, int t = kT) {
     return (int)std::max<int64_t>(1, std::min<int64_t>((n + t - 1) / t, (int64_t)sm_count() * 16));
@@ -129,30 +129,47 @@ void graph_transpose(int n, int m, const int* rp, const int* ci, int64_t nnz, De
 // ---- symbolic products --------------------------------------------------------
 // Row `row` of X Y (Z): the distinct columns, counted (Cci == null) or written
 // sorted at Crp[row]. X's entries in order, Y's strided over the lanes, Z's in
-// order; a warp's hash set holds up to kHash distinct columns (more: overflow).
+// order. A warp's hash set (kHash slots) holds the columns of one row; a slot
+// stores (row + 1) << 32 | column, so the slots of earlier rows count as free
+// and the table is cleared only once per block. Each column is appended to
+// the warp's list as it is first inserted; more than kHash distinct columns
+// in a row is an overflow.
 template <bool THREE>
 __global__ void __launch_bounds__(kSymWarps * 32)
 k_sym(int rows, const int* __restrict__ Xrp, const int* __restrict__ Xci, const int* __restrict__ Yrp,
       const int* __restrict__ Yci, const int* __restrict__ Zrp, const int* __restrict__ Zci, int* __restrict__ cnt,
       const int* __restrict__ Crp, int* __restrict__ Cci, int* overflow) {
-    extern __shared__ int smem[];
+    extern __shared__ unsigned long long smem64[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int* tab = smem + warp * kHash;
-    int* lst = smem + (kSymWarps + warp) * kHash;
+    unsigned long long* tab = smem64 + warp * kHash;
+    int* lst = reinterpret_cast<int*>(smem64 + kSymWarps * kHash) + warp * kHash;
     __shared__ int fillc[kSymWarps];
+    for (int t = threadIdx.x; t < kSymWarps * kHash; t += blockDim.x) smem64[t] = 0ull;
+    __syncthreads();
     for (int row = blockIdx.x * kSymWarps + warp; row < rows; row += gridDim.x * kSymWarps) {
-        for (int t = lane; t < kHash; t += 32) tab[t] = -1;
+        const unsigned long long tag = (unsigned long long)(row + 1) << 32;
         if (lane == 0) fillc[warp] = 0;
         __syncwarp();
         int mine = 0;
         bool ovf = false;
         auto insert = [&](int key) {
+            const unsigned long long mark = tag | (unsigned)key;
             unsigned h = ((unsigned)key * 2654435761u) >> (32 - kHashBits);
-            for (int probe = 0; probe < kHash; ++probe) {
-                const int prev = atomicCAS(&tab[h], -1, key);
-                if (prev == -1) { ++mine; return; }
-                if (prev == key) return;
-                h = (h + 1) & (kHash - 1);
+            volatile unsigned long long* vt = tab;  // other lanes write through atomics
+            for (int probe = 0; probe < 2 * kHash; ++probe) {
+                const unsigned long long cur = vt[h];
+                if ((cur & 0xffffffff00000000ull) == tag) {  // a column of this row
+                    if (cur == mark) return;
+                    h = (h + 1) & (kHash - 1);
+                    continue;
+                }
+                if (atomicCAS(&tab[h], cur, mark) == cur) {  // claimed a free slot
+                    const int pos = atomicAdd(&fillc[warp], 1);
+                    if (pos < kHash) lst[pos] = key;
+                    ++mine;
+                    return;
+                }
+                // another lane took this slot first: look at it again
             }
             ovf = true;
         };
@@ -174,9 +191,6 @@ k_sym(int rows, const int* __restrict__ Xrp, const int* __restrict__ Xci, const 
         if (!Cci) {
             if (lane == 0) cnt[row] = mine;
         } else {
-            for (int t = lane; t < kHash; t += 32)
-                if (tab[t] >= 0) lst[atomicAdd(&fillc[warp], 1)] = tab[t];
-            __syncwarp();
             const int m = min(mine, kHash);
             int* out = Cci + Crp[row];
             for (int e = lane; e < m; e += 32) {
@@ -647,6 +661,45 @@ void d_l1(const DCsr& A, DevBuf<double>& out, cudaStream_t s) {
 }
 
 }  // namespace
+
+// sliced-ELL offsets: off[s] = sum width[0..s), off[slices] = total; -1 when the
+// total exceeds the int range (the caller then keeps no sliced-ELL copy)
+__global__ void __launch_bounds__(1024) k_scan64(int n, const int* __restrict__ cnt, int* __restrict__ out,
+                                                 long long* __restrict__ total) {
+    __shared__ long long sh[1024];
+    const int T = blockDim.x, t = threadIdx.x;
+    const int chunk = (n + T - 1) / T;
+    const int a = min(n, t * chunk), b = min(n, a + chunk);
+    long long s = 0;
+    for (int i = a; i < b; ++i) s += cnt[i];
+    sh[t] = s;
+    __syncthreads();
+    for (int off = 1; off < T; off <<= 1) {
+        const long long v = t >= off ? sh[t - off] : 0;
+        __syncthreads();
+        sh[t] += v;
+        __syncthreads();
+    }
+    long long base = t ? sh[t - 1] : 0;
+    for (int i = a; i < b; ++i) {
+        out[i] = (int)min(base, (long long)INT32_MAX);
+        base += cnt[i];
+    }
+    if (t == T - 1) {
+        *total = sh[T - 1];
+        out[n] = (int)min(sh[T - 1], (long long)INT32_MAX);
+    }
+}
+
+int sell_offsets(int slices, const int* width, int* off, cudaStream_t s) {
+    DevBuf<long long> tot(1);
+    k_scan64<<<1, 1024, 0, s>>>(slices, width, off, tot.get());
+    SSV_LAUNCH_CHECK();
+    long long h = 0;
+    SSV_CUDA(cudaMemcpyAsync(&h, tot.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    SSV_CUDA(cudaStreamSynchronize(s));
+    return h > (long long)INT32_MAX - 4096 ? -1 : (int)h;
+}
 
 // ---- DCsr --------------------------------------------------------------------------
 void DCsr::from_host(const HostCsr& H, cudaStream_t s) {

@@ -725,6 +725,57 @@ template <> inline const float* DualVec::get<float>() const { return f.get(); }
 // no longer run side by side and share fewer x rows in L1.)
 constexpr int kSellWindow = 256;
 
+// Sliced-ELL layout on the device (DevSell::build's order): in each window of
+// kSellWindow rows the rows sorted by length, longest first, ties in row
+// order (a stable rank per row); then slices of 32 consecutive sorted rows,
+// each padded to its longest row; entry k of slice row t at off[slice] + 32 k + t.
+__global__ void __launch_bounds__(256) k_sell_order(int n, int window, const int* __restrict__ rp, int* __restrict__ order) {
+    __shared__ int len[256];
+    const int w0 = blockIdx.x * window, t = threadIdx.x;
+    const int m = min(window, n - w0);
+    if (t < m) len[t] = rp[w0 + t + 1] - rp[w0 + t];
+    __syncthreads();
+    if (t < m) {
+        int r = 0;
+        for (int j = 0; j < m; ++j) r += (len[j] > len[t]) || (len[j] == len[t] && j < t);
+        order[w0 + r] = w0 + t;
+    }
+}
+
+__global__ void k_sell_width(int n, int slices, const int* __restrict__ rp, const int* __restrict__ order,
+                             int* __restrict__ rows, int* __restrict__ width) {
+    for (int sl = blockIdx.x * blockDim.x + threadIdx.x; sl < slices; sl += gridDim.x * blockDim.x) {
+        int w = 0;
+        for (int t = 0; t < 32; ++t) {
+            const int q = sl * 32 + t;
+            const int r = q < n ? order[q] : -1;
+            rows[q] = r;
+            if (r >= 0) w = max(w, rp[r + 1] - rp[r]);
+        }
+        width[sl] = 32 * w;
+    }
+}
+
+__global__ void k_sell_fill(int slices, const int* __restrict__ rp, const int* __restrict__ ci,
+                            const double* __restrict__ v, const int* __restrict__ rows, const int* __restrict__ off,
+                            int* __restrict__ sci, double* __restrict__ sv, int* __restrict__ src) {
+    const int64_t total = (int64_t)slices * 32;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int r = rows[q];
+        if (r < 0) continue;
+        const int sl = (int)(q / 32), t = (int)(q % 32);
+        const int k0 = rp[r], len = rp[r + 1] - k0;
+        for (int k = 0; k < len; ++k) {
+            const size_t e = (size_t)off[sl] + 32 * (size_t)k + t;
+            sci[e] = ci[k0 + k];
+            sv[e] = v[k0 + k];
+            src[e] = k0 + k;
+        }
+    }
+}
+
+int sell_offsets(int slices, const int* width, int* off, cudaStream_t s);  // exclusive scan (amg_device.cu)
+
 __global__ void k_sell_refresh(int64_t entries, const int* __restrict__ src, const double* __restrict__ csr_v,
                                double* __restrict__ v) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < entries; e += (int64_t)gridDim.x * blockDim.x)
@@ -744,6 +795,39 @@ struct DevSell {
         if (slices > 0 && entries > 0)
             k_sell_refresh<<<grid_for(entries, 256), 256, 0, s>>>(entries, src.get(), csr_v, v.get());
         SSV_LAUNCH_CHECK();
+    }
+    // the same layout built on the device from a device CSR (a_rp, a_ci, a_v)
+    void build_dev(int n, int64_t nnz, const int* a_rp, const int* a_ci, const double* a_v, cudaStream_t s) {
+        pat_n = n;
+        pat_nnz = nnz;
+        slices = (n + 31) / 32;
+        DevBuf<int> order(std::max(n, 1)), width(std::max(slices, 1));
+        off.alloc(slices + 1);
+        rows.alloc((size_t)std::max(slices, 1) * 32);
+        if (n) {
+            k_sell_order<<<(n + kSellWindow - 1) / kSellWindow, kSellWindow, 0, s>>>(n, kSellWindow, a_rp, order.get());
+            k_sell_width<<<grid_for(slices, 128), 128, 0, s>>>(n, slices, a_rp, order.get(), rows.get(), width.get());
+            SSV_LAUNCH_CHECK();
+        }
+        const int total = sell_offsets(slices, width.get(), off.get(), s);
+        if (total < 0) {  // int offsets would overflow: no copy
+            slices = 0;
+            entries = 0;
+            return;
+        }
+        entries = total;
+        const size_t cap = (size_t)std::max<int64_t>(entries, 1);
+        ci.alloc(cap);
+        src.alloc(cap);
+        v.alloc(cap);
+        SSV_CUDA(cudaMemsetAsync(ci.get(), 0xff, sizeof(int) * cap, s));  // -1: padding
+        SSV_CUDA(cudaMemsetAsync(src.get(), 0xff, sizeof(int) * cap, s));
+        SSV_CUDA(cudaMemsetAsync(v.get(), 0, sizeof(double) * cap, s));
+        if (slices)
+            k_sell_fill<<<grid_for((int64_t)slices * 32, 256), 256, 0, s>>>(slices, a_rp, a_ci, a_v, rows.get(),
+                                                                             off.get(), ci.get(), v.get(), src.get());
+        SSV_LAUNCH_CHECK();
+        SSV_CUDA(cudaStreamSynchronize(s));  // the temporaries go out of scope
     }
     void build(const HostCsr& A, cudaStream_t s) {
         pat_n = A.n;
@@ -1578,6 +1662,10 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
             A.tuned[slot] = it->second[0];
             A.tuned_u[slot] = it->second[1];
             A.tuned_sell[slot] = it->second[2];
+            char line[128];  // the record lists every choice in call order, memo hits included
+            std::snprintf(line, sizeof(line), "csr %d %lld %d %d %d %d\n", A.n, (long long)A.nnz, NV, A.tuned[slot],
+                          A.tuned_u[slot], A.tuned_sell[slot]);
+            tune_replay().record(line);
             return;
         }
     }
@@ -1676,6 +1764,9 @@ static void tune_pi(AmsState& a, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1)
             auto it = tune_memo().m.find(memo_key);
             if (it != tune_memo().m.end()) {
                 a.pi_lanes[dir][slot] = it->second[0];
+                char line[64];
+                std::snprintf(line, sizeof(line), "pi %d %d %d\n", dir, NV, a.pi_lanes[dir][slot]);
+                tune_replay().record(line);
                 continue;
             }
         }
@@ -2035,7 +2126,7 @@ static void fine_from(DevCsr& M, const DCsr& D, bool layout_valid, cudaStream_t 
     if (layout_valid && M.sell.slices > 0 && M.sell.pat_n == D.n && M.sell.pat_nnz == D.nnz)
         M.sell.refresh(D.v.get(), s);
     else
-        M.sell.build(D.to_host(s), s);
+        M.sell.build_dev(D.n, D.nnz, D.rp.get(), D.ci.get(), D.v.get(), s);
 }
 
 // BC matrix, Galerkin products (FixZeroRows) and AMG hierarchies of the four

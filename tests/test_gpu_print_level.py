@@ -23,7 +23,7 @@ def _make(d, complex_form, print_level):
 
 
 def test_setup_report_and_breakdown_after_25_mults(capsys):
-    d = H.magnetostatic(6)
+    d = H.magnetostatic(10)  # 1,331 vertices: more than one AMG level
     p = _make(d, False, 1)
     out = capsys.readouterr().out
     assert f"CompactAMS setup: HC={d['A'].shape[0]} H1={d['G'].shape[1]}" in out
