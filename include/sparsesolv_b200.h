@@ -217,6 +217,13 @@ int ssv_precond_update(ssv_precond* p);
 /* Mult (sparsesolv_precond.hpp:123-136): y = M^{-1} x, constrained DOFs 0. */
 int ssv_precond_apply(ssv_precond* p, const void* x, void* y);
 int ssv_precond_apply_dev(ssv_precond* p, const void* d_x, void* d_y);
+/* Block form of Mult for the CompactAMS / ComplexCompactAMS handles (new, no
+ * reference counterpart; the batched COCR driver's per-frequency apply):
+ * nrhs right-hand sides (1 or 4) in one cycle, row-interleaved: x[i*nrhs + c]
+ * is row i of column c (complex: Re/Im pairs). Each column gets the result of
+ * ssv_precond_apply up to reduction order. Host buffers; SSV_ERR_TYPE for
+ * other preconditioners, SSV_ERR_INVALID_ARG for another nrhs. */
+int ssv_precond_apply_block(ssv_precond* p, int32_t nrhs, const void* x, void* y);
 /* Actual IC shift after auto-shift (ICPreconditioner::actual_shift). */
 int ssv_ic_actual_shift(const ssv_precond* p, double* shift);
 int ssv_precond_destroy(ssv_precond* p);

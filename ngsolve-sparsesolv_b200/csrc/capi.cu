@@ -666,6 +666,25 @@ int ssv_precond_apply(ssv_precond* p, const void* x, void* y) {
     });
 }
 
+int ssv_precond_apply_block(ssv_precond* p, int32_t nrhs, const void* x, void* y) {
+    return guarded([&] {
+        if (!p || !x || !y) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_precond_apply_block: NULL argument");
+        if ((p->kind != 2 && p->kind != 3) || !p->ams)
+            ssv::fail(SSV_ERR_TYPE, "ssv_precond_apply_block: CompactAMS / ComplexCompactAMS handles only");
+        if (nrhs != 1 && nrhs != 4) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_precond_apply_block: nrhs must be 1 or 4");
+        if (!p->ready) ssv::fail(SSV_ERR_RUNTIME, "CompactAMS::Mult called before Setup");
+        cudaStream_t s = ssv::stream();
+        const size_t bytes = (size_t)p->n * nrhs * scalar_bytes(p->vdtype);
+        p->io_x.alloc(bytes / sizeof(double) + 1);
+        p->io_y.alloc(bytes / sizeof(double) + 1);
+        SSV_CUDA(cudaMemcpyAsync(p->io_x.get(), x, bytes, cudaMemcpyHostToDevice, s));
+        ssv::ams_reserve_block(p->ams.get(), nrhs);
+        ssv::ams_apply_block(p->ams.get(), p->io_x.get(), p->io_y.get(), nrhs, nullptr, s);
+        SSV_CUDA(cudaMemcpyAsync(y, p->io_y.get(), bytes, cudaMemcpyDeviceToHost, s));
+        SSV_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 int ssv_ic_actual_shift(const ssv_precond* p, double* shift) {
     return guarded([&] {
         if (!p || !shift) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ic_actual_shift: NULL argument");

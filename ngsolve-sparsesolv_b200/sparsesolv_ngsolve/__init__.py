@@ -811,6 +811,19 @@ class _AmsBase(_PrecondBase):
         check(self._lib.ssv_ams_set_precision(self._h, {"fp32": _capi.SSV_PREC_FP32,
                                                         "fp32_nodal": _capi.SSV_PREC_FP32_NODAL}.get(v, _capi.SSV_PREC_FP64)))
 
+    def MultBlock(self, X):
+        """M^{-1} applied to the rows of X (shape (nrhs, n), nrhs 1 or 4) in one block
+        cycle (new: the batched driver's apply); returns an array of X's shape."""
+        X = np.asarray(X, dtype=self._dtype)
+        if X.ndim != 2 or X.shape[1] != self._n or X.shape[0] not in (1, 4):
+            raise ValueError(f"MultBlock: X must have shape (1 or 4, {self._n})")
+        k = X.shape[0]
+        xi = np.ascontiguousarray(X.T)  # [row][rhs]
+        out = np.empty_like(xi)
+        check(self._lib.ssv_precond_apply_block(self._h, k, _capi.vptr(xi), _capi.vptr(out)))
+        self._note_applies(1)
+        return np.ascontiguousarray(out.T)
+
     def profile(self, nrhs=1, reps=20, cold=False):
         """Per-phase device time (ms) and algorithmic bytes of one cycle (measurement hook);
         cold=True times each launch alone after evicting the L2."""
