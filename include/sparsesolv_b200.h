@@ -330,6 +330,15 @@ int ssv_ams_setup_times(const ssv_precond* p, double* times);
  * = 1 when the hierarchy was set up on the device. */
 int ssv_ams_level_matrix(const ssv_precond* p, int32_t subspace, int32_t level, int32_t what, int32_t* row_ptr,
                          int32_t* col_idx, double* values, int32_t cap, int32_t* nnz, int32_t* on_device);
+/* Parity hook (no reference counterpart): one subspace correction of the
+ * cycle on its own, in the current form. From the residual r (rows x nv host
+ * doubles, nv = 2 for ComplexCompactAMS: Re/Im pairs): b_s = the restricted
+ * residual (G^T r, or Pi_s^T r), x_s = the subspace V-cycle's result (both
+ * h1_rows x nv, in the hierarchy's coordinates: diagonally scaled where the
+ * hierarchy is FP32), corr = w P_s x_s (rows x nv). subspace: 0 gradient,
+ * 1..3 Nedelec x, y, z. */
+int ssv_ams_subspace_apply(ssv_precond* p, int32_t subspace, const double* r, double* b_s, double* x_s,
+                           double* corr);
 
 /* ---- CG with an external preconditioner (new: the reference's AMS scripts
  *      drive it with NGSolve's krylovspace.CGSolver) ---------------------------

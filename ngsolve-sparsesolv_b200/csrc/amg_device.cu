@@ -5,6 +5,9 @@
 // patterns (which columns a product row holds) come from a per-warp hash set
 // in shared memory, sorted afterwards; their order never enters a sum.
 #include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <random>
@@ -701,6 +704,28 @@ int sell_offsets(int slices, const int* width, int* off, cudaStream_t s) {
     return h > (long long)INT32_MAX - 4096 ? -1 : (int)h;
 }
 
+SetupLog::SetupLog(cudaStream_t st) : s(st) {
+    static const bool env = std::getenv("SSV_AMS_SETUP_LOG") != nullptr;
+    on = env;
+    if (on) {
+        SSV_CUDA(cudaStreamSynchronize(s));
+        t = wall_seconds();
+    }
+}
+
+void SetupLog::mark(const char* fmt, ...) {
+    if (!on) return;
+    SSV_CUDA(cudaStreamSynchronize(s));
+    const double now = wall_seconds();
+    std::fprintf(stderr, "ams setup: %8.3f ms  ", 1e3 * (now - t));
+    va_list ap;
+    va_start(ap, fmt);
+    std::vfprintf(stderr, fmt, ap);
+    va_end(ap);
+    std::fprintf(stderr, "\n");
+    t = now;
+}
+
 // ---- DCsr --------------------------------------------------------------------------
 void DCsr::from_host(const HostCsr& H, cudaStream_t s) {
     n = H.n;
@@ -871,6 +896,7 @@ bool d_fused_level(const DCsr& A, const DCsr& P, const DCsr& Pt, const double* d
 
 bool d_amg_setup(const DCsr& A0, double theta, int max_levels, int min_coarse, std::vector<DAmgLevel>& out,
                  cudaStream_t s) {
+    SetupLog log(s);
     out.clear();
     out.emplace_back();
     out[0].A.copy_from(A0, s);
@@ -878,6 +904,7 @@ bool d_amg_setup(const DCsr& A0, double theta, int max_levels, int min_coarse, s
     for (int l = 0; l < max_levels - 1; ++l) {
         const int n = out[l].A.n;
         if (n <= min_coarse) break;
+        log.mark("  level %d (%d rows, %lld nnz): start", l, n, (long long)out[l].A.nnz);
         const DCsr& A = out[l].A;
         // strength (ComputeStrength, compact_amg.hpp:292-372)
         DevBuf<int> cnt(n), Srp(n + 1), Sci;
@@ -890,14 +917,18 @@ bool d_amg_setup(const DCsr& A0, double theta, int max_levels, int min_coarse, s
         SSV_LAUNCH_CHECK();
         DevBuf<int> Trp, Tci;
         graph_transpose(n, n, Srp.get(), Sci.get(), snnz, Trp, Tci, s);
+        log.mark("    strength + transpose (%d strong)", snnz);
+        int passes = 0, rounds = 0;
         // PMIS
         DevBuf<double> measure(n);
         DevBuf<int> cf(n), state(n), flags(2);
         k_pmis_measure<<<blocks_for(n), kT, 0, s>>>(n, Trp.get(), pmis_random(n, s), measure.get(), cf.get());
         SSV_LAUNCH_CHECK();
         for (int round = 0; round < 100; ++round) {
+            ++rounds;
             k_pmis_init<<<blocks_for(n), kT, 0, s>>>(n, cf.get(), state.get());
             for (int pass = 0; pass <= n; ++pass) {  // each pass decides at least one row
+                ++passes;
                 flags.zero(s);
                 k_pmis_resolve<<<blocks_for(n), kT, 0, s>>>(n, Srp.get(), Sci.get(), Trp.get(), Tci.get(), cf.get(),
                                                             measure.get(), state.get(), flags.get());
@@ -920,6 +951,7 @@ bool d_amg_setup(const DCsr& A0, double theta, int max_levels, int min_coarse, s
         DevBuf<int> isc(n), cidx(n + 1);
         k_pmis_finish<<<blocks_for(n), kT, 0, s>>>(n, cf.get(), isc.get());
         const int nc = scan(n, isc.get(), cidx.get(), s);
+        log.mark("    PMIS: %d coarse, %d rounds, %d passes", nc, rounds, passes);
         if (nc == 0 || nc >= n) break;
         // interpolation
         DevBuf<uint8_t> strong(std::max<int64_t>(A.nnz, 1));
@@ -936,9 +968,12 @@ bool d_amg_setup(const DCsr& A0, double theta, int max_levels, int min_coarse, s
         k_interp_fill<<<blocks_for(n), kT, 0, s>>>(n, A.rp.get(), A.ci.get(), A.v.get(), strong.get(), cf.get(),
                                                    cidx.get(), P.rp.get(), P.ci.get(), P.v.get());
         SSV_LAUNCH_CHECK();
+        log.mark("    interpolation (%lld nnz)", (long long)P.nnz);
         DCsr Pt, Ac;
         d_transpose(P, Pt, s);
+        log.mark("    P transpose");
         if (!d_rap(A, P, Pt, Ac, s)) return false;
+        log.mark("    RAP (%lld nnz)", (long long)Ac.nnz);
         SSV_CUDA(cudaStreamSynchronize(s));  // this level's temporaries go out of scope
         out[l].P = std::move(P);
         out[l].Pt = std::move(Pt);
@@ -949,7 +984,8 @@ bool d_amg_setup(const DCsr& A0, double theta, int max_levels, int min_coarse, s
     DAmgLevel& co = out.back();
     if (co.A.n <= min_coarse * 10) {
         co.direct = true;
-        dense_ldlt_pseudo(co.A.to_host(s), co.linv, co.linvt, co.piv);
+        co.piv_min = dense_ldlt_pseudo(co.A.to_host(s), co.linv, co.linvt, co.piv);
+        log.mark("  coarsest LDL^T (%d rows, host)", co.A.n);
     }
     SSV_CUDA(cudaStreamSynchronize(s));
     return true;

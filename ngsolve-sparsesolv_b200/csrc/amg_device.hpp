@@ -16,6 +16,16 @@
 
 namespace ssv {
 
+// SSV_AMS_SETUP_LOG=1: the wall time of every set-up stage on stderr (the
+// stream is synchronised at each mark; off, a mark costs nothing)
+struct SetupLog {
+    bool on = false;
+    cudaStream_t s = nullptr;
+    double t = 0;
+    explicit SetupLog(cudaStream_t st);
+    void mark(const char* fmt, ...);
+};
+
 // FP64 CSR in device memory (columns sorted per row where the producer says so)
 struct DCsr {
     int n = 0, m = 0;
@@ -32,6 +42,7 @@ struct DAmgLevel {
     DevBuf<double> l1;
     bool direct = false;
     std::vector<double> linv, linvt, piv;  // coarsest LDL^T pseudo-inverse factors (host, FP64)
+    double piv_min = 1.0;                  // smallest kept |pivot| / |diagonal|
 };
 
 // A_bc (CreateBCModifiedMatrix, compact_amg.hpp:252-287): identity rows on

@@ -341,8 +341,8 @@ void l1_norms(const HostCsr& A, std::vector<double>& out) {
 // next to the 1e-6 mass weight of air gives ~1e13) X's entries are dominated
 // by the smallest pivots and X b loses the other components, enough to stall
 // COCR on the eddy-current systems.
-void dense_ldlt_pseudo(const HostCsr& A, std::vector<double>& linv, std::vector<double>& linvt,
-                       std::vector<double>& piv) {
+double dense_ldlt_pseudo(const HostCsr& A, std::vector<double>& linv, std::vector<double>& linvt,
+                         std::vector<double>& piv, double tau) {
     const int n = A.n;
     std::vector<double> L((size_t)n * n, 0.0), w(n), diag0(n);
     piv.assign(n, 0.0);
@@ -350,12 +350,14 @@ void dense_ldlt_pseudo(const HostCsr& A, std::vector<double>& linv, std::vector<
     for (int i = 0; i < n; ++i)
         for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) L[(size_t)i * n + A.ci[k]] += A.v[k];
     for (int i = 0; i < n; ++i) diag0[i] = std::abs(L[(size_t)i * n + i]);
+    double kept_min = 1.0;
     for (int j = 0; j < n; ++j) {
         for (int k = 0; k < j; ++k) w[k] = L[(size_t)j * n + k] * d[k];
         double dj = L[(size_t)j * n + j];
         for (int k = 0; k < j; ++k) dj -= L[(size_t)j * n + k] * w[k];
-        const bool zero = !(std::abs(dj) > 1e-13 * diag0[j]);
+        const bool zero = !(std::abs(dj) > tau * diag0[j]);
         d[j] = zero ? 0.0 : dj;
+        if (!zero) kept_min = std::min(kept_min, std::abs(dj) / diag0[j]);
         L[(size_t)j * n + j] = 1.0;
         for (int i = j + 1; i < n; ++i) {
             double s = L[(size_t)i * n + j];
@@ -390,6 +392,7 @@ void dense_ldlt_pseudo(const HostCsr& A, std::vector<double>& linv, std::vector<
         for (int t = 0; t < nt; ++t) th.emplace_back(columns, n * t / nt, n * (t + 1) / nt);
         for (auto& x : th) x.join();
     }
+    return kept_min;
 }
 
 // CompactAMG::Setup (:66-156) for freedofs = nullptr (the AMS subspaces)
@@ -418,7 +421,7 @@ void AmgHost::setup(const HostCsr& A0) {
     AmgHostLevel& co = levels.back();
     if (co.A.n <= min_coarse * 10) {
         co.direct = true;
-        dense_ldlt_pseudo(co.A, co.linv, co.linvt, co.piv);
+        co.piv_min = dense_ldlt_pseudo(co.A, co.linv, co.linvt, co.piv);
     }
 }
 

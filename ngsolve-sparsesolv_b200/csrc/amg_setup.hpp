@@ -38,11 +38,13 @@ struct FusedLevel {
 };
 FusedLevel fused_level(const HostCsr& A, const HostCsr& P, const HostCsr& Pt, const std::vector<double>& d);
 
-// Pseudo-inverse of the small coarsest matrix through LDL^T (pivots below
-// 1e-13 of their row's diagonal dropped): linv = L^{-1} row-major, linvt its
-// transpose, piv the pivots (0 where dropped).
-void dense_ldlt_pseudo(const HostCsr& A, std::vector<double>& linv, std::vector<double>& linvt,
-                       std::vector<double>& piv);
+// Pseudo-inverse of the small coarsest matrix through LDL^T (pivots at or
+// below tau of their row's diagonal dropped; the reference's tau is 1e-13):
+// linv = L^{-1} row-major, linvt its transpose, piv the pivots (0 where
+// dropped). Returns the smallest |pivot| / |diagonal| among the kept pivots
+// (1 when none is kept).
+double dense_ldlt_pseudo(const HostCsr& A, std::vector<double>& linv, std::vector<double>& linvt,
+                         std::vector<double>& piv, double tau = 1e-13);
 
 struct AmgHostLevel {
     HostCsr A, P, Pt;
@@ -51,6 +53,7 @@ struct AmgHostLevel {
     std::vector<double> linv;     // n x n row-major L^{-1} (unit lower; direct only)
     std::vector<double> linvt;    // its transpose
     std::vector<double> piv;      // D, dropped pivots as 0
+    double piv_min = 1.0;         // smallest kept |pivot| / |diagonal| (direct only)
 };
 
 struct AmgHost {

@@ -1967,6 +1967,31 @@ static std::vector<double> inverted(const std::vector<double>& v) {
 // whether subspace sub's hierarchy is held in FP32 (diagonally scaled)
 static bool sub_lo(const AmsState& a, int sub) { return a.fp32 && !(a.grad64 && sub == 0); }
 
+// Coarsest factors of an FP32 hierarchy. Its solve reads FP32 right-hand
+// sides, whose rounding (6e-8 relative) a kept pivot of relative size rho =
+// |d_j| / |a_jj| amplifies by 1/rho along that pivot's direction. The
+// reference's factorization keeps every pivot above 1e-13 of its diagonal, so
+// a near-null mode (rho 1e-13..1e-9: the nodal hierarchies that are one level
+// deep, whose coarsest matrix is the subspace's fine Galerkin matrix) turns
+// one FP32 rounding into an O(1) error of the correction, and COCR diverges
+// (the FP64 form is unaffected: its inputs round at 1e-16). Such a matrix is
+// factored again with pivots at or below kLoPivotDrop of their diagonal
+// dropped (their direction is left to the other subspaces, as a dropped
+// pivot of the reference's). Out: the factors of the FP32 form, unscaled.
+constexpr double kLoPivotDrop = 1e-6;
+
+static void lo_coarse_factors(const HostCsr& A, double piv_min, const std::vector<double>& linv,
+                              const std::vector<double>& linvt, const std::vector<double>& piv,
+                              std::vector<double>& li, std::vector<double>& lt, std::vector<double>& pv) {
+    if (piv_min > kLoPivotDrop) {
+        li = linv;
+        lt = linvt;
+        pv = piv;
+        return;
+    }
+    dense_ldlt_pseudo(A, li, lt, pv, kLoPivotDrop);
+}
+
 // Matrix part: A_bc and its l1 norms (FP64), the four AMG hierarchies (in the
 // chosen form; the coarsest factors FP64), and in the FP32 form the scaled
 // transfer values.
@@ -2050,7 +2075,8 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
             dl.direct = hl[l].direct;
             if (dl.direct) {  // FP64 in both forms
                 if (lo) {
-                    std::vector<double> li = hl[l].linv, lt = hl[l].linvt, pv = hl[l].piv;
+                    std::vector<double> li, lt, pv;
+                    lo_coarse_factors(hl[l].A, hl[l].piv_min, hl[l].linv, hl[l].linvt, hl[l].piv, li, lt, pv);
                     for (int i = 0; i < nl; ++i)
                         for (int k = 0; k < nl; ++k) {
                             li[(size_t)i * nl + k] *= isc[l][i] * sc[l][k];
@@ -2134,9 +2160,11 @@ static void fine_from(DevCsr& M, const DCsr& D, bool layout_valid, cudaStream_t 
 // long for the device symbolic step
 static bool ams_device_setup(AmsState& a, const ssv_matrix* A, cudaStream_t s) {
     AmsDev& D = a.dev;
+    SetupLog log(s);
     DCsr Abc;
     d_bc_matrix(A->rows, A->cols, A->nnz, A->rp.get(), A->ci.get(), A->val.get(), a.has_fd ? a.fd.get() : nullptr,
                 Abc, s);
+    log.mark("BC matrix");
     std::vector<DAmgLevel> amg[4];
     for (int sub = 0; sub < 4; ++sub) {
         const DCsr& P0 = sub == 0 ? D.G : D.Pi[sub - 1];
@@ -2144,7 +2172,9 @@ static bool ams_device_setup(AmsState& a, const ssv_matrix* A, cudaStream_t s) {
         DCsr A0;
         if (!d_rap(Abc, P0, P0t, A0, s)) return false;
         d_fix_zero_rows(A0, s);
+        log.mark("subspace %d Galerkin product (%d rows, %lld nnz)", sub, A0.n, (long long)A0.nnz);
         if (!d_amg_setup(A0, a.host.theta, 25, 500, amg[sub], s)) return false;
+        log.mark("subspace %d hierarchy (%zu levels)", sub, amg[sub].size());
     }
     D.A_bc = std::move(Abc);
     for (int sub = 0; sub < 4; ++sub) D.amg[sub] = std::move(amg[sub]);
@@ -2160,7 +2190,9 @@ static bool ams_device_setup(AmsState& a, const ssv_matrix* A, cudaStream_t s) {
 static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
     AmsDev& D = a.dev;
     const int nv = std::max(a.nv_alloc, a.complex_form ? 2 : 1);
+    SetupLog log(s);
     fine_from(a.A_bc, D.A_bc, layout_valid, s);
+    log.mark("fine A_bc and its sliced-ELL copy");
     a.fine_l1.alloc(std::max(a.nhc, 1));
     SSV_CUDA(cudaMemcpyAsync(a.fine_l1.get(), D.fine_l1.get(), sizeof(double) * a.nhc, cudaMemcpyDeviceToDevice, s));
     a.fine_il1.alloc(std::max(a.nhc, 1));
@@ -2215,7 +2247,15 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
                     SSV_CUDA(cudaMemcpyAsync(hs.data(), sc[l].get(), sizeof(double) * nl, cudaMemcpyDeviceToHost, s));
                     SSV_CUDA(cudaMemcpyAsync(his.data(), isc[l].get(), sizeof(double) * nl, cudaMemcpyDeviceToHost, s));
                     SSV_CUDA(cudaStreamSynchronize(s));
-                    std::vector<double> li = hl[l].linv, lt = hl[l].linvt, pv = hl[l].piv;
+                    std::vector<double> li, lt, pv;
+                    if (hl[l].piv_min > kLoPivotDrop) {
+                        li = hl[l].linv;
+                        lt = hl[l].linvt;
+                        pv = hl[l].piv;
+                    } else {
+                        lo_coarse_factors(hl[l].A.to_host(s), hl[l].piv_min, hl[l].linv, hl[l].linvt, hl[l].piv, li,
+                                          lt, pv);
+                    }
                     for (int i = 0; i < nl; ++i)
                         for (int k = 0; k < nl; ++k) {
                             li[(size_t)i * nl + k] *= his[i] * hs[k];
@@ -2244,6 +2284,7 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
             }
             SSV_CUDA(cudaStreamSynchronize(s));  // this level's temporaries go out of scope
         }
+        log.mark("subspace %d cycle arrays (%s%s)", sub, lo ? "FP32" : "FP64", fuse ? ", fused products" : "");
         // level-0 scaling folded into this subspace's transfers
         if (sub == 0) {
             if (lo) {
@@ -2277,9 +2318,11 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
             }
         }
     }
+    log.mark("transfers");
     a.t_fused = t_fused;
     a.nv_alloc = 0;
     ams_reserve(a, nv);
+    log.mark("work vectors + shape tuner");
 }
 
 // Rebuild the matrix-dependent part (RebuildMatrix) and upload it.
@@ -2400,6 +2443,68 @@ static void ams_block_t(AmsState& a, const double* in, double* out, int nrhs, co
         }
     }
     fail(SSV_ERR_INVALID_ARG, "AMS block apply: nrhs must be 1 or 4");
+}
+
+// One subspace correction of the cycle on its own (parity hook): the
+// restriction b_s = P_s^T r (G^T for the gradient subspace, the scaled Pi_s^T
+// for a nodal one), the subspace V-cycle x_s, and the prolonged correction
+// c = w P_s x_s -- each in the types of the current form, returned as FP64
+// (b_s and x_s in the hierarchy's own, diagonally scaled in the FP32 forms,
+// coordinates).
+__global__ void k_widen(int64_t n, const float* __restrict__ in, double* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = in[i];
+}
+
+template <typename T>
+static void widen_to(const T* in, int64_t n, double* out, cudaStream_t s) {
+    if constexpr (std::is_same_v<T, double>) {
+        if (n) SSV_CUDA(cudaMemcpyAsync(out, in, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    } else {
+        if (n) k_widen<<<grid_for(n, 256), 256, 0, s>>>(n, in, out);
+        SSV_LAUNCH_CHECK();
+    }
+}
+
+template <typename TG, typename TN, int NV>
+static void ams_subspace_t(AmsState& a, int sub, const double* r, double* bs, double* xs, double* corr,
+                           cudaStream_t s) {
+    const int64_t m1 = (int64_t)a.nh1 * NV;
+    SSV_CUDA(cudaMemsetAsync(corr, 0, sizeof(double) * (size_t)a.nhc * NV, s));
+    if (sub == 0) {
+        mv_spmv<double, double, TG, NV, MV_AX, true>(a.Gt, r, a.rs[0].as<TG>(), nullptr, nullptr, TG(0), nullptr, s);
+        widen_to<TG>(a.rs[0].as<TG>(), m1, bs, s);
+        TG* g = vcycle<TG, NV, true>(a.amg[0], 0, a.rs[0].as<TG>(), 1, nullptr, s);
+        widen_to<TG>(g, m1, xs, s);
+        mv_spmv<double, TG, double, NV, MV_ADD, true>(a.G, g, corr, nullptr, nullptr, a.w, nullptr, s);
+    } else {
+        pi_restrict<TN, NV>(a, r, a.rs[1].as<TN>(), a.rs[2].as<TN>(), a.rs[3].as<TN>(), nullptr, s);
+        widen_to<TN>(a.rs[sub].as<TN>(), m1, bs, s);
+        TN* g = vcycle<TN, NV, true>(a.amg[sub], 0, a.rs[sub].as<TN>(), 1, nullptr, s);
+        widen_to<TN>(g, m1, xs, s);
+        DevBuf<TN> zero((size_t)std::max<int64_t>(m1, 1));
+        zero.zero(s);
+        pi_prolong<TN, NV>(a, sub == 1 ? g : zero.get(), sub == 2 ? g : zero.get(), sub == 3 ? g : zero.get(), corr,
+                           nullptr, s);
+        SSV_CUDA(cudaStreamSynchronize(s));
+    }
+}
+
+void ams_subspace_apply(AmsState* a, int sub, const double* r, double* bs, double* xs, double* corr) {
+    if (sub < 0 || sub > 3) fail(SSV_ERR_INVALID_ARG, "ssv_ams_subspace_apply: subspace must be 0..3");
+    cudaStream_t s = stream();
+    const int nv = a->complex_form ? 2 : 1;
+    const size_t nh = (size_t)a->nhc * nv, n1 = (size_t)a->nh1 * nv;
+    DevBuf<double> dr(nh), db(n1), dx(n1), dc(nh);
+    SSV_CUDA(cudaMemcpyAsync(dr.get(), r, sizeof(double) * nh, cudaMemcpyHostToDevice, s));
+    with_forms(*a, [&](auto g, auto n) {
+        if (nv == 2) ams_subspace_t<decltype(g), decltype(n), 2>(*a, sub, dr.get(), db.get(), dx.get(), dc.get(), s);
+        else ams_subspace_t<decltype(g), decltype(n), 1>(*a, sub, dr.get(), db.get(), dx.get(), dc.get(), s);
+    });
+    SSV_CUDA(cudaMemcpyAsync(bs, db.get(), sizeof(double) * n1, cudaMemcpyDeviceToHost, s));
+    SSV_CUDA(cudaMemcpyAsync(xs, dx.get(), sizeof(double) * n1, cudaMemcpyDeviceToHost, s));
+    SSV_CUDA(cudaMemcpyAsync(corr, dc.get(), sizeof(double) * nh, cudaMemcpyDeviceToHost, s));
+    SSV_CUDA(cudaStreamSynchronize(s));
 }
 
 // nrhs right-hand sides, row-interleaved ([row][rhs], complex as Re/Im pairs).

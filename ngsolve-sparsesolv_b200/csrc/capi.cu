@@ -437,6 +437,16 @@ int ssv_ams_level_matrix(const ssv_precond* p, int32_t subspace, int32_t level, 
     });
 }
 
+int ssv_ams_subspace_apply(ssv_precond* p, int32_t subspace, const double* r, double* b_s, double* x_s,
+                           double* corr) {
+    return guarded([&] {
+        if (!p || !p->ams || !r || !b_s || !x_s || !corr)
+            ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_subspace_apply: bad argument");
+        if (!p->ready) ssv::fail(SSV_ERR_RUNTIME, "CompactAMS::Mult called before Setup");
+        ssv::ams_subspace_apply(p->ams.get(), subspace, r, b_s, x_s, corr);
+    });
+}
+
 int ssv_ams_setup_times(const ssv_precond* p, double* times) {
     return guarded([&] {
         if (!p || !p->ams || !times) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_setup_times: bad argument");

@@ -66,6 +66,8 @@ int ams_precision(const AmsState* a);
 void ams_reserve_block(AmsState* a, int nrhs);
 void ams_profile(AmsState* a, int nrhs, int reps, int flags, ssv_phase_profile* out);
 void ams_apply_block(AmsState* a, const double* in, double* out, int nrhs, const KState* st, cudaStream_t s);
+// one subspace correction on its own (host arrays; parity hook)
+void ams_subspace_apply(AmsState* a, int sub, const double* r, double* bs, double* xs, double* corr);
 
 // Batched COCR over a frequency family (batch.cu)
 ssv_batch* batch_create(ssv_matrix* K, ssv_matrix* M, int F, const double* omegas, ssv_precond* const* pre, int R,

@@ -811,6 +811,23 @@ class _AmsBase(_PrecondBase):
         check(self._lib.ssv_ams_set_precision(self._h, {"fp32": _capi.SSV_PREC_FP32,
                                                         "fp32_nodal": _capi.SSV_PREC_FP32_NODAL}.get(v, _capi.SSV_PREC_FP64)))
 
+    def subspace_apply(self, sub, r):
+        """Parity hook: one subspace correction on its own from the residual r
+        (sub 0 gradient, 1..3 Nedelec x, y, z): returns (b_s, x_s, corr) -- the
+        restricted residual and the subspace V-cycle's result in the hierarchy's
+        coordinates (diagonally scaled where it is FP32), and the prolonged
+        correction w P_s x_s."""
+        nv = 2 if self._cplx else 1
+        rr = np.ascontiguousarray(np.asarray(r, dtype=self._dtype)).view(np.float64)
+        n1 = self._grad.m * nv
+        bs, xs = np.empty(n1), np.empty(n1)
+        corr = np.empty(self._n * nv)
+        check(self._lib.ssv_ams_subspace_apply(self._h, int(sub), _capi.vptr(rr), _capi.vptr(bs), _capi.vptr(xs),
+                                               _capi.vptr(corr)))
+        if nv == 2:
+            return bs.view(np.complex128), xs.view(np.complex128), corr.view(np.complex128)
+        return bs, xs, corr
+
     def MultBlock(self, X):
         """M^{-1} applied to the rows of X (shape (nrhs, n), nrhs 1 or 4) in one block
         cycle (new: the batched driver's apply); returns an array of X's shape."""

@@ -3,10 +3,14 @@ right-hand sides in one cycle against four single applies of the same
 preconditioner (ssv_precond_apply), and the FP64 form against the AMS oracle.
 
 Bars: the FP64 form gives each column the single apply's result up to the
-reduction order of the shape tuner's picks (1e-10 relative); the FP32 forms
-agree with their own single applies to 1e-5 relative (one FP32 cycle's
-rounding, taken twice). The hierarchies at 6^3 are one level deep (a direct
-coarsest solve at level 0); at 10^3 they have two or more levels."""
+reduction order of the shape tuner's picks: 1e-10 relative (of max|y|) on
+the well-conditioned family (cond ~ 3e3), 1e-7 on the SI family (iron
+nu_r 1e-3, mass weight 1e-6: cond 1e8..1e11, where a 1e-16 difference in a
+sum grows to ~1e-8 of max|y| in one apply; the oracle comparison uses the
+same two bars). The FP32 forms agree with their own single applies to 1e-5
+relative (one FP32 cycle's rounding, taken twice). The hierarchies at 6^3
+are one level deep (a direct coarsest solve at level 0); at 10^3 they have
+two or more levels."""
 from __future__ import annotations
 
 import numpy as np
@@ -44,7 +48,7 @@ def _rhs(d, seed):
 def test_block_equals_single(nc, precision, si):
     d = _family(nc, si)
     X = _rhs(d, 3)
-    tol = 1e-10 if precision == "fp64" else 1e-5
+    tol = (1e-7 if si else 1e-10) if precision == "fp64" else 1e-5
     for f in range(2):
         p = _pre(d, f, precision)
         Y1 = np.stack([p * X[c] for c in range(4)])
@@ -57,9 +61,11 @@ def test_block_equals_single(nc, precision, si):
 
 
 @pytest.mark.parametrize("nc", [6, 10])
-def test_block_fp64_matches_oracle(nc):
-    d = _family(nc, True)
+@pytest.mark.parametrize("si", [False, True])
+def test_block_fp64_matches_oracle(nc, si):
+    d = _family(nc, si)
     X = _rhs(d, 5)
+    tol = 1e-7 if si else 1e-11
     for f in range(2):
         p = _pre(d, f, "fp64")
         o = O.AmsOracle(d["a_real"][f], d["G"], d["freedofs"], *d["coords"])
@@ -67,7 +73,7 @@ def test_block_fp64_matches_oracle(nc):
         for c in range(4):
             yo = o.apply_complex(X[c])
             err = np.abs(Y4[c] - yo).max() / np.abs(yo).max()
-            assert err <= 1e-8, (f, c, err)
+            assert err <= tol, (f, c, err)
 
 
 def test_block_rejects_bad_nrhs_and_kind():
