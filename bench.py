@@ -199,7 +199,7 @@ def run_ncu_case(args):
     if args.workload == "eddy64":
         # one warm solve first (tuner, graph capture), then the profiled one inside the NVTX
         # range "solve" (capture with ncu --nvtx --nvtx-include "solve/"; SSV_GRAPH_MODE=chunk)
-        d = _eddy_system()
+        d = _eddy_system(args.eddy_nc)
         pre = ss.ComplexCompactAMSPreconditioner(d["a_real"], d["G"], freedofs=d["freedofs"],
                                                  coord_x=d["coords"][0], coord_y=d["coords"][1],
                                                  coord_z=d["coords"][2], precision=args.precision_eddy)
@@ -212,7 +212,7 @@ def run_ncu_case(args):
         inv * d["f"]
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
-        print(json.dumps({"ncu_case": args.workload, "precision": args.precision_eddy,
+        print(json.dumps({"ncu_case": args.workload, "mesh": f"{args.eddy_nc}^3", "precision": args.precision_eddy,
                           "iterations": inv.iterations}))
         return
     if args.workload == "ams40":
@@ -494,9 +494,9 @@ REFINE_DROP = 1e-5
 EDDY_MAXITER = 3000
 
 
-def _eddy_system():
+def _eddy_system(nc=64):
     from sparsesolv_ngsolve import hcurl as H
-    return H.eddy_current(64)
+    return H.eddy_current(nc)
 
 
 def _rel_err(x, xref):
@@ -929,8 +929,10 @@ def main():
     ap.add_argument("--workload", default="eddy64", choices=["eddy64", "ams40", "iccg64", "newton40"])
     ap.add_argument("--no-extras", action="store_true", help="skip the batched-family measurement")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"], help="AMS form of --ncu-case")
-    ap.add_argument("--precision-eddy", default="fp64", choices=["fp64", "fp32_nodal"],
+    ap.add_argument("--precision-eddy", default="fp64", choices=["fp64", "fp32_nodal", "fp32"],
                     help="AMS form of the eddy64 --ncu-case")
+    ap.add_argument("--eddy-nc", type=int, default=64,
+                    help="mesh size of the eddy64 --ncu-case (a smaller mesh for multi-pass ncu sections)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ncu-case", action="store_true",
                     help="run exactly one solve of the workload and exit (for ncu captures)")

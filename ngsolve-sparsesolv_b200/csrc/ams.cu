@@ -681,6 +681,142 @@ k_mv3_coarse(TriCoarse<K> t, const KState* st) {
 }
 
 // ---------------------------------------------------------------------------
+// Dense V-cycle tails. Below a level of at most tail_rows() rows, the fused
+// V-cycle from x = 0 is one fixed linear map b_l -> x_l: T = L^{-T} D^+ L^{-1}
+// on the coarsest level and T_l = M_l + Q_l T_{l+1} R_l above it, where
+// U_l = [M_l | Q_l] and R_l are the level's two fused products. The set-up
+// forms T (FP64, dense) at the first level with at most tail_rows() rows, and
+// the cycle applies it as one dense product in place of the two launches per
+// level below: the same operator up to the order of the roundings, for the
+// small levels where launch latency, not bytes, sets the time.
+// ---------------------------------------------------------------------------
+template <typename T, int K>
+struct TailSet {
+    int n[K];
+    const double* M[K];
+    const T* b[K];
+    T* y[K];
+};
+
+// y = T b for K hierarchies (blockIdx.y), warp per row, FP64 accumulation
+template <typename T, int NV, int K>
+__global__ void __launch_bounds__(kBlock) k_tail_apply(TailSet<T, K> t, const KState* st) {
+    pdl_gate();
+    if (st && st->done) return;
+    const int q = blockIdx.y;
+    const int n = t.n[q];
+    const double* __restrict__ M = t.M[q];
+    const T* __restrict__ b = t.b[q];
+    const int lane = threadIdx.x & 31;
+    for (int row = blockIdx.x * (kBlock / 32) + threadIdx.x / 32; row < n; row += gridDim.x * (kBlock / 32)) {
+        double acc[NV];
+#pragma unroll
+        for (int c = 0; c < NV; ++c) acc[c] = 0.0;
+        const double* mr = M + (size_t)row * n;
+        for (int j = lane; j < n; j += 32) {
+            const double a = mr[j];
+            T bv[NV];
+            load_row<NV>(b + (size_t)j * NV, bv);
+#pragma unroll
+            for (int c = 0; c < NV; ++c) acc[c] += a * (double)bv[c];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int c = 0; c < NV; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
+        if (lane == 0)
+#pragma unroll
+            for (int c = 0; c < NV; ++c) t.y[q][(size_t)row * NV + c] = (T)acc[c];
+    }
+}
+
+template <typename T, int NV, int K>
+static void tail_apply(const TailSet<T, K>& t, int parts, const KState* st, cudaStream_t s) {
+    int nmax = 0;
+    for (int k = 0; k < parts; ++k) nmax = std::max(nmax, t.n[k]);
+    const dim3 grid(std::max(1, std::min((nmax + 7) / 8, std::max(1, sm_count() * 4 / parts))), parts);
+    launch_k(k_tail_apply<T, NV, K>, grid, kBlock, s, t, st);
+}
+
+// set-up: T[i][j] = sum_{k >= max(i,j)} LiT[i][k] Li[k][j] / piv_k (0 for a
+// dropped pivot), one block per row i
+__global__ void k_tail_coarsest(int n, const double* __restrict__ Li, const double* __restrict__ LiT,
+                                const double* __restrict__ piv, double* __restrict__ T) {
+    extern __shared__ double arow[];
+    const int i = blockIdx.x;
+    for (int k = threadIdx.x; k < n; k += blockDim.x)
+        arow[k] = (k >= i && piv[k] != 0.0) ? LiT[(size_t)i * n + k] / piv[k] : 0.0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double acc = 0.0;
+        for (int k = max(i, j); k < n; ++k) acc += arow[k] * Li[(size_t)k * n + j];
+        T[(size_t)i * n + j] = acc;
+    }
+}
+
+// set-up: W = T R (T n1 x n1, R n1 x n0 given as its transpose Rt, n0 rows),
+// one block per row i of T
+__global__ void k_tail_w(int n1, int n0, const double* __restrict__ T, const int* __restrict__ rtp,
+                         const int* __restrict__ rti, const double* __restrict__ rtv, double* __restrict__ W) {
+    extern __shared__ double trow[];
+    const int i = blockIdx.x;
+    for (int k = threadIdx.x; k < n1; k += blockDim.x) trow[k] = T[(size_t)i * n1 + k];
+    __syncthreads();
+    for (int j = threadIdx.x; j < n0; j += blockDim.x) {
+        double acc = 0.0;
+        for (int e = rtp[j]; e < rtp[j + 1]; ++e) acc += trow[rti[e]] * rtv[e];
+        W[(size_t)i * n0 + j] = acc;
+    }
+}
+
+// set-up: T0 = M + Q W with U = [M | Q] (rows n0, columns n0 + n1), one
+// block per row i
+template <typename TV>
+__global__ void k_tail_t(int n0, const int* __restrict__ up, const int* __restrict__ uci, const TV* __restrict__ uv,
+                         const double* __restrict__ W, double* __restrict__ T0) {
+    const int i = blockIdx.x;
+    const int e0 = up[i], e1 = up[i + 1];
+    for (int j = threadIdx.x; j < n0; j += blockDim.x) {
+        double acc = 0.0;
+        for (int e = e0; e < e1; ++e) {
+            const int c = uci[e];
+            const double v = (double)uv[e];
+            if (c < n0) {
+                if (c == j) acc += v;
+            } else {
+                acc += v * W[(size_t)(c - n0) * n0 + j];
+            }
+        }
+        T0[(size_t)i * n0 + j] = acc;
+    }
+}
+
+__global__ void k_widen(int64_t n, const float* __restrict__ in, double* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = in[i];
+}
+
+template <typename T>
+static void widen_to(const T* in, int64_t n, double* out, cudaStream_t s) {
+    if constexpr (std::is_same_v<T, double>) {
+        if (n) SSV_CUDA(cudaMemcpyAsync(out, in, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    } else {
+        if (n) k_widen<<<grid_for(n, 256), 256, 0, s>>>(n, in, out);
+        SSV_LAUNCH_CHECK();
+    }
+}
+
+// rows of the largest level a tail may start at (SSV_AMS_TAIL=<rows>; 0: no tails)
+static int tail_rows() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("SSV_AMS_TAIL");
+        v = e ? std::max(0, std::atoi(e)) : 2048;
+    }
+    return v;
+}
+
+// ---------------------------------------------------------------------------
 // Device hierarchy
 // ---------------------------------------------------------------------------
 static std::vector<float> to_float(const std::vector<double>& h) { return std::vector<float>(h.begin(), h.end()); }
@@ -922,8 +1058,17 @@ struct AmgDevLevel {
     bool direct = false;
     DevBuf<double> Li, LiT, piv;  // coarsest: LDL^T factors (FP64 in both forms)
     DevBuf<double> cz;            // coarsest: FP64 scratch between the two triangular products
+    DevBuf<double> tail;          // tail level: the V-cycle from here down as one dense FP64 map x = T b
+    double piv_min = 1.0;         // coarsest: smallest kept |pivot| / |diagonal| of the factors held
     WorkVec b, xa, xb, r;  // NV-column work vectors of this level
 };
+
+// the level holding the hierarchy's dense tail, or -1
+static int tail_level(const std::vector<AmgDevLevel>& L) {
+    for (size_t l = 0; l < L.size(); ++l)
+        if (L[l].tail.get()) return (int)l;
+    return -1;
+}
 
 // The hierarchy as the device set-up builds it (FP64, unscaled): the input of
 // the cycle's arrays in either form, kept so that a precision switch needs no
@@ -1082,12 +1227,22 @@ static void coarse_direct(AmgDevLevel& lv, const T* b, T* x, const KState* st, c
 // per level instead of four. Same arithmetic up to rounding.
 template <typename T, int NV, bool RECIP>
 static T* vcycle_fused(std::vector<AmgDevLevel>& L, const T* b0, const KState* st, cudaStream_t s) {
-    const int n = (int)L.size();
+    const int tl = tail_level(L);
+    const int n = tl >= 0 ? tl + 1 : (int)L.size();  // levels run one by one (the last: coarsest or tail)
     auto rhs = [&](int l) -> const T* { return l == 0 ? b0 : L[l].b.template as<T>(); };
     for (int l = 0; l + 1 < n; ++l)
         mv_spmv<T, T, T, NV, MV_AX, RECIP>(L[l].R, rhs(l), L[l + 1].b.template as<T>(), nullptr, nullptr, T(0), st,
                                            s);
-    coarse_direct<T, NV, RECIP>(L[n - 1], rhs(n - 1), L[n - 1].xa.template as<T>(), st, s);
+    if (tl >= 0) {
+        TailSet<T, 1> t{};
+        t.n[0] = L[tl].A.n;
+        t.M[0] = L[tl].tail.get();
+        t.b[0] = rhs(tl);
+        t.y[0] = L[tl].xa.template as<T>();
+        tail_apply<T, NV, 1>(t, 1, st, s);
+    } else {
+        coarse_direct<T, NV, RECIP>(L[n - 1], rhs(n - 1), L[n - 1].xa.template as<T>(), st, s);
+    }
     for (int l = n - 2; l >= 0; --l) {
         const T* e = (l + 1 == n - 1) ? L[l + 1].xa.template as<T>() : L[l + 1].xb.template as<T>();
         mv_spmv<T, T, T, NV, MV_TWO, RECIP>(L[l].U, rhs(l), L[l].xb.template as<T>(), e, nullptr, T(0), st, s);
@@ -1197,29 +1352,17 @@ static void vcycleM(std::vector<AmgDevLevel>* const* H, const T* const* rhs0, in
     auto lv = [&](int k, int l) -> AmgDevLevel& { return (*H[k])[l]; };
     bool fused = true;
     for (int k = 0; k < parts; ++k) fused = fused && fused_ready(*H[k]);
-    auto coarse = [&]() {  // coarsest levels: LDL^T pseudo-inverse, FP64
-        TriCoarse<K> f{}, b{};
-        int nmax = 0;
-        for (int k = 0; k < parts; ++k) {
-            AmgDevLevel& v = lv(k, L(k) - 1);
-            nmax = std::max(nmax, v.A.n);
-            f.n[k] = b.n[k] = v.A.n;
-            f.M[k] = v.Li.get(); b.M[k] = v.LiT.get();
-            f.piv[k] = b.piv[k] = v.piv.get();
-            f.cz[k] = b.cz[k] = v.cz.get();
-            f.io[k] = rhs(k, L(k) - 1);
-            b.io[k] = v.xa.raw.get();
-        }
-        const dim3 grid(std::max(1, std::min((nmax + 7) / 8, std::max(1, sm_count() * 4 / parts))), parts);
-        launch_k(k_mv3_coarse<T, NV, true, K>, grid, kBlock, s, f, st);
-        launch_k(k_mv3_coarse<T, NV, false, K>, grid, kBlock, s, b, st);
-    };
-    if (fused) {  // two fused products per level (vcycle_fused), all hierarchies in each launch
+    if (fused) {  // the dense tails end the level-by-level part (vcycle_fused)
+        int lt[K];
+        for (int k = 0; k < parts; ++k) lt[k] = tail_level(*H[k]);
+        auto Lt = [&](int k) { return lt[k] >= 0 ? lt[k] + 1 : L(k); };
+        Lmax = 0;
+        for (int k = 0; k < parts; ++k) Lmax = std::max(Lmax, Lt(k));
         for (int l = 0; l < Lmax - 1; ++l) {
             Tri<T, K> rs{};
             int q = 0, k0 = -1;
             for (int k = 0; k < parts; ++k) {
-                if (l >= L(k) - 1) continue;
+                if (l >= Lt(k) - 1) continue;
                 if (k0 < 0) k0 = k;
                 const DevCsr& R = lv(k, l).R;
                 rs.n[q] = R.n; rs.rp[q] = R.rp.get(); rs.ci[q] = R.ci.get(); rs.v[q] = R.val<T>();
@@ -1228,25 +1371,52 @@ static void vcycleM(std::vector<AmgDevLevel>* const* H, const T* const* rhs0, in
             }
             if (q) spmv3<T, NV, MV_AX, RECIP, K>(rs, q, lv(k0, l).R.lanes_for(NV), T(0), st, s);
         }
-        coarse();
+        {  // the last level of each: its dense tail, or the LDL^T solve of the coarsest
+            TailSet<T, K> ts{};
+            TriCoarse<K> f{}, b{};
+            int qt = 0, qc = 0, nmax = 0;
+            for (int k = 0; k < parts; ++k) {
+                AmgDevLevel& v = lv(k, Lt(k) - 1);
+                if (lt[k] >= 0) {
+                    ts.n[qt] = v.A.n; ts.M[qt] = v.tail.get();
+                    ts.b[qt] = rhs(k, Lt(k) - 1); ts.y[qt] = v.xa.template as<T>();
+                    ++qt;
+                } else {
+                    nmax = std::max(nmax, v.A.n);
+                    f.n[qc] = b.n[qc] = v.A.n;
+                    f.M[qc] = v.Li.get(); b.M[qc] = v.LiT.get();
+                    f.piv[qc] = b.piv[qc] = v.piv.get();
+                    f.cz[qc] = b.cz[qc] = v.cz.get();
+                    f.io[qc] = rhs(k, Lt(k) - 1);
+                    b.io[qc] = v.xa.raw.get();
+                    ++qc;
+                }
+            }
+            if (qt) tail_apply<T, NV, K>(ts, qt, st, s);
+            if (qc) {
+                const dim3 grid(std::max(1, std::min((nmax + 7) / 8, std::max(1, sm_count() * 4 / qc))), qc);
+                launch_k(k_mv3_coarse<T, NV, true, K>, grid, kBlock, s, f, st);
+                launch_k(k_mv3_coarse<T, NV, false, K>, grid, kBlock, s, b, st);
+            }
+        }
         for (int l = Lmax - 2; l >= 0; --l) {
             Tri<T, K> up{};
             int q = 0, k0 = -1;
             for (int k = 0; k < parts; ++k) {
-                if (l > L(k) - 2) continue;
+                if (l > Lt(k) - 2) continue;
                 if (k0 < 0) k0 = k;
                 AmgDevLevel& v = lv(k, l);
                 AmgDevLevel& nx = lv(k, l + 1);
                 up.n[q] = v.U.n; up.rp[q] = v.U.rp.get(); up.ci[q] = v.U.ci.get(); up.v[q] = v.U.val<T>();
                 up.x[q] = rhs(k, l);
-                up.b[q] = (l + 1 == L(k) - 1) ? nx.xa.template as<T>() : nx.xb.template as<T>();
+                up.b[q] = (l + 1 == Lt(k) - 1) ? nx.xa.template as<T>() : nx.xb.template as<T>();
                 up.y[q] = v.xb.template as<T>();
                 ++q;
             }
             if (q) spmv3<T, NV, MV_TWO, RECIP, K>(up, q, lv(k0, l).U.lanes_for(NV), T(0), st, s);
         }
         for (int k = 0; k < parts; ++k)
-            out[k] = (L(k) == 1) ? lv(k, 0).xa.template as<T>() : lv(k, 0).xb.template as<T>();
+            out[k] = (Lt(k) == 1) ? lv(k, 0).xa.template as<T>() : lv(k, 0).xb.template as<T>();
         return;
     }
     for (int l = 0; l < Lmax - 1; ++l) {
@@ -1980,16 +2150,91 @@ static bool sub_lo(const AmsState& a, int sub) { return a.fp32 && !(a.grad64 && 
 // pivot of the reference's). Out: the factors of the FP32 form, unscaled.
 constexpr double kLoPivotDrop = 1e-6;
 
-static void lo_coarse_factors(const HostCsr& A, double piv_min, const std::vector<double>& linv,
-                              const std::vector<double>& linvt, const std::vector<double>& piv,
-                              std::vector<double>& li, std::vector<double>& lt, std::vector<double>& pv) {
+static double lo_coarse_factors(const HostCsr& A, double piv_min, const std::vector<double>& linv,
+                                const std::vector<double>& linvt, const std::vector<double>& piv,
+                                std::vector<double>& li, std::vector<double>& lt, std::vector<double>& pv) {
     if (piv_min > kLoPivotDrop) {
         li = linv;
         lt = linvt;
         pv = piv;
-        return;
+        return piv_min;
     }
-    dense_ldlt_pseudo(A, li, lt, pv, kLoPivotDrop);
+    return dense_ldlt_pseudo(A, li, lt, pv, kLoPivotDrop);
+}
+
+// The dense tail of one hierarchy (see k_tail_apply) from its fused level
+// products (values TV, as the cycle holds them) and its coarsest factors: none
+// unless every level above the coarsest has R and U and some level has at
+// most tail_rows() rows.
+constexpr double kTailPivot = 1e-6;
+
+template <typename TV>
+static void build_tail(std::vector<AmgDevLevel>& L, cudaStream_t s) {
+    for (auto& lv : L) lv.tail.release();
+    const int rows = tail_rows();
+    // an explicit inverse of a coarsest matrix with a kept pivot of relative size
+    // rho carries entries of size 1/rho, whose rounding (1e-16 / rho relative)
+    // the factored solve does not have: no tail below kTailPivot
+    if (rows <= 0 || !fused_ready(L) || L.back().piv_min < kTailPivot) return;
+    const int nl = (int)L.size();
+    int cut = -1;
+    for (int l = 0; l < nl; ++l)
+        if (L[l].A.n <= rows) {
+            cut = l;
+            break;
+        }
+    if (cut < 0) return;
+    const AmgDevLevel& co = L[nl - 1];
+    const int nc = co.A.n;
+    DevBuf<double> T((size_t)std::max(nc, 1) * std::max(nc, 1));
+    if (nc)
+        k_tail_coarsest<<<nc, 256, sizeof(double) * nc, s>>>(nc, co.Li.get(), co.LiT.get(), co.piv.get(), T.get());
+    SSV_LAUNCH_CHECK();
+    for (int l = nl - 2; l >= cut; --l) {
+        const int n0 = L[l].A.n, n1 = L[l + 1].A.n;
+        const DevCsr& R = L[l].R;
+        DCsr Rd, Rt;
+        Rd.n = R.n;
+        Rd.m = R.m;
+        Rd.nnz = R.nnz;
+        Rd.rp.alloc(R.n + 1);
+        Rd.ci.alloc(std::max<int64_t>(R.nnz, 1));
+        Rd.v.alloc(std::max<int64_t>(R.nnz, 1));
+        SSV_CUDA(cudaMemcpyAsync(Rd.rp.get(), R.rp.get(), sizeof(int) * (R.n + 1), cudaMemcpyDeviceToDevice, s));
+        if (R.nnz) SSV_CUDA(cudaMemcpyAsync(Rd.ci.get(), R.ci.get(), sizeof(int) * R.nnz, cudaMemcpyDeviceToDevice, s));
+        widen_to<TV>(R.val<TV>(), R.nnz, Rd.v.get(), s);
+        d_transpose(Rd, Rt, s);
+        DevBuf<double> W((size_t)std::max(n1, 1) * std::max(n0, 1)), T0((size_t)std::max(n0, 1) * std::max(n0, 1));
+        if (n1 && n0)
+            k_tail_w<<<n1, 256, sizeof(double) * n1, s>>>(n1, n0, T.get(), Rt.rp.get(), Rt.ci.get(), Rt.v.get(),
+                                                           W.get());
+        if (n0)
+            k_tail_t<TV><<<n0, 256, 0, s>>>(n0, L[l].U.rp.get(), L[l].U.ci.get(), L[l].U.val<TV>(), W.get(), T0.get());
+        SSV_LAUNCH_CHECK();
+        SSV_CUDA(cudaStreamSynchronize(s));  // this level's temporaries go out of scope
+        T = std::move(T0);
+    }
+    SSV_CUDA(cudaStreamSynchronize(s));
+    L[cut].tail = std::move(T);
+}
+
+static void build_tails(AmsState& a, cudaStream_t s) {
+    SetupLog log(s);
+    for (int sub = 0; sub < 4; ++sub) {
+        if (a.num_smooth != 1) {
+            for (auto& lv : a.amg[sub]) lv.tail.release();
+            continue;
+        }
+        if (sub_lo(a, sub)) build_tail<float>(a.amg[sub], s);
+        else build_tail<double>(a.amg[sub], s);
+        const int tl = tail_level(a.amg[sub]);
+        if (tl >= 0)
+            log.mark("  subspace %d: dense tail at level %d (%d rows, %zu levels below)", sub, tl, a.amg[sub][tl].A.n,
+                     a.amg[sub].size() - 1 - tl);
+        else
+            log.mark("  subspace %d: no dense tail (coarsest pivot ratio %.1e)", sub,
+                     a.amg[sub].empty() ? 0.0 : a.amg[sub].back().piv_min);
+    }
 }
 
 // Matrix part: A_bc and its l1 norms (FP64), the four AMG hierarchies (in the
@@ -2076,7 +2321,8 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
             if (dl.direct) {  // FP64 in both forms
                 if (lo) {
                     std::vector<double> li, lt, pv;
-                    lo_coarse_factors(hl[l].A, hl[l].piv_min, hl[l].linv, hl[l].linvt, hl[l].piv, li, lt, pv);
+                    dl.piv_min =
+                        lo_coarse_factors(hl[l].A, hl[l].piv_min, hl[l].linv, hl[l].linvt, hl[l].piv, li, lt, pv);
                     for (int i = 0; i < nl; ++i)
                         for (int k = 0; k < nl; ++k) {
                             li[(size_t)i * nl + k] *= isc[l][i] * sc[l][k];
@@ -2090,6 +2336,7 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
                     dl.Li.upload(hl[l].linv.data(), hl[l].linv.size(), s);
                     dl.LiT.upload(hl[l].linvt.data(), hl[l].linvt.size(), s);
                     dl.piv.upload(hl[l].piv.data(), hl[l].piv.size(), s);
+                    dl.piv_min = hl[l].piv_min;
                 }
             }
         }
@@ -2109,6 +2356,7 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
             a.Pitv[d].upload(pit.v.data(), pit.v.size(), s);
         }
     }
+    build_tails(a, s);
     a.nv_alloc = 0;
     ams_reserve(a, nv);
 }
@@ -2252,9 +2500,10 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
                         li = hl[l].linv;
                         lt = hl[l].linvt;
                         pv = hl[l].piv;
+                        dl.piv_min = hl[l].piv_min;
                     } else {
-                        lo_coarse_factors(hl[l].A.to_host(s), hl[l].piv_min, hl[l].linv, hl[l].linvt, hl[l].piv, li,
-                                          lt, pv);
+                        dl.piv_min = lo_coarse_factors(hl[l].A.to_host(s), hl[l].piv_min, hl[l].linv, hl[l].linvt,
+                                                       hl[l].piv, li, lt, pv);
                     }
                     for (int i = 0; i < nl; ++i)
                         for (int k = 0; k < nl; ++k) {
@@ -2270,6 +2519,7 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
                     dl.Li.upload(hl[l].linv.data(), hl[l].linv.size(), s);
                     dl.LiT.upload(hl[l].linvt.data(), hl[l].linvt.size(), s);
                     dl.piv.upload(hl[l].piv.data(), hl[l].piv.size(), s);
+                    dl.piv_min = hl[l].piv_min;
                 }
             }
             if (fuse && !last) {
@@ -2319,6 +2569,8 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
         }
     }
     log.mark("transfers");
+    build_tails(a, s);
+    log.mark("dense V-cycle tails");
     a.t_fused = t_fused;
     a.nv_alloc = 0;
     ams_reserve(a, nv);
@@ -2451,21 +2703,6 @@ static void ams_block_t(AmsState& a, const double* in, double* out, int nrhs, co
 // c = w P_s x_s -- each in the types of the current form, returned as FP64
 // (b_s and x_s in the hierarchy's own, diagonally scaled in the FP32 forms,
 // coordinates).
-__global__ void k_widen(int64_t n, const float* __restrict__ in, double* __restrict__ out) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = in[i];
-}
-
-template <typename T>
-static void widen_to(const T* in, int64_t n, double* out, cudaStream_t s) {
-    if constexpr (std::is_same_v<T, double>) {
-        if (n) SSV_CUDA(cudaMemcpyAsync(out, in, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-    } else {
-        if (n) k_widen<<<grid_for(n, 256), 256, 0, s>>>(n, in, out);
-        SSV_LAUNCH_CHECK();
-    }
-}
-
 template <typename TG, typename TN, int NV>
 static void ams_subspace_t(AmsState& a, int sub, const double* r, double* bs, double* xs, double* corr,
                            cudaStream_t s) {
