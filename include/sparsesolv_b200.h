@@ -316,6 +316,16 @@ int ssv_ams_get_precision(const ssv_precond* p, int32_t* precision);
  * launches back to back (operands that fit in L2 stay there). */
 #define SSV_PROFILE_COLD 1
 int ssv_ams_profile(ssv_precond* p, int32_t nrhs, int32_t reps, int32_t flags, ssv_phase_profile* out);
+/* Measurement hook (no reference counterpart): per-level device time (ms,
+ * warm, mean of reps back-to-back launches) of one subspace's V-cycle on one
+ * right-hand side: the down product R_l into ms_r[l] and the up product U_l
+ * into ms_u[l] for every level run one by one (cap entries at most), their
+ * launch shapes (lanes * 10 + rows per group) in shape_r / shape_u, and the
+ * last step (the dense tail, or the coarsest solve's two launches) in
+ * *last_ms. *levels receives the number of levels run one by one, the last
+ * included. */
+int ssv_ams_profile_levels(ssv_precond* p, int32_t subspace, int32_t reps, double* ms_r, double* ms_u,
+                           int32_t* shape_r, int32_t* shape_u, int32_t cap, double* last_ms, int32_t* levels);
 /* Measurement hook (no reference counterpart): wall seconds of the last
  * set-up of p (create, Update() or a precision switch) into times[0..3]:
  * total, host hierarchy (BC matrix, Galerkin products, coarsening,

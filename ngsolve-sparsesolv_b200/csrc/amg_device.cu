@@ -895,7 +895,7 @@ bool d_fused_level(const DCsr& A, const DCsr& P, const DCsr& Pt, const double* d
 }
 
 bool d_amg_setup(const DCsr& A0, double theta, int max_levels, int min_coarse, std::vector<DAmgLevel>& out,
-                 cudaStream_t s) {
+                 cudaStream_t s, std::thread* coarse) {
     SetupLog log(s);
     out.clear();
     out.emplace_back();
@@ -984,8 +984,14 @@ bool d_amg_setup(const DCsr& A0, double theta, int max_levels, int min_coarse, s
     DAmgLevel& co = out.back();
     if (co.A.n <= min_coarse * 10) {
         co.direct = true;
-        co.piv_min = dense_ldlt_pseudo(co.A.to_host(s), co.linv, co.linvt, co.piv);
-        log.mark("  coarsest LDL^T (%d rows, host)", co.A.n);
+        if (coarse) {  // the level object stays where it is: out is not resized again
+            *coarse = std::thread([&co, H = co.A.to_host(s)] {
+                co.piv_min = dense_ldlt_pseudo(H, co.linv, co.linvt, co.piv);
+            });
+        } else {
+            co.piv_min = dense_ldlt_pseudo(co.A.to_host(s), co.linv, co.linvt, co.piv);
+            log.mark("  coarsest LDL^T (%d rows, host)", co.A.n);
+        }
     }
     SSV_CUDA(cudaStreamSynchronize(s));
     return true;

@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <thread>
 #include <vector>
 
 #include "amg_setup.hpp"
@@ -59,9 +60,12 @@ void d_fix_zero_rows(DCsr& A, cudaStream_t s);
 // truncated l1 of the fine smoother (compact_ams.hpp:395-413)
 void d_fine_l1(const DCsr& A, DevBuf<double>& out, cudaStream_t s);
 // CompactAMG::Setup for freedofs = nullptr on the device; false when a row is
-// too long for the device symbolic products (the caller then uses the host)
+// too long for the device symbolic products (the caller then uses the host).
+// The coarsest LDL^T factorisation runs on the host: inline, or, when
+// `coarse` is given, on a host thread stored there (the caller joins it
+// before the factors are read), so it overlaps the device work that follows.
 bool d_amg_setup(const DCsr& A0, double theta, int max_levels, int min_coarse, std::vector<DAmgLevel>& out,
-                 cudaStream_t s);
+                 cudaStream_t s, std::thread* coarse = nullptr);
 // fused_level (amg_setup.hpp) on the device: R = P^T (I - A D^{-1}),
 // U = [D^{-1}(2I - A D^{-1}) | (I - D^{-1} A) P]
 bool d_fused_level(const DCsr& A, const DCsr& P, const DCsr& Pt, const double* d, DCsr& R, DCsr& U,

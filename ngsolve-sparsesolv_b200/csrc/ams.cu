@@ -38,6 +38,7 @@
 #include "amg_device.hpp"
 #include "amg_setup.hpp"
 #include "objects.cuh"
+#include "sell.cuh"
 #include "solver_api.hpp"
 
 namespace ssv {
@@ -852,118 +853,17 @@ struct DualVec {
 template <> inline const double* DualVec::get<double>() const { return d.get(); }
 template <> inline const float* DualVec::get<float>() const { return f.get(); }
 
-// Sliced-ELL copy of a CSR matrix for k_sell_spmv: rows sorted by length
-// (longest first, ties in row order) inside windows of kSellWindow rows, cut
-// into slices of 32 rows, each slice padded to its longest row. Entry k of
-// slice row t sits at off[slice] + 32 k + t. (Storing the slices widest
-// first, so that the last partial wave of a launch holds the shortest ones,
-// measured no faster at 40^3 and 8% slower at 64^3: neighbouring slices then
-// no longer run side by side and share fewer x rows in L1.)
-constexpr int kSellWindow = 256;
-
-// Sliced-ELL layout on the device (DevSell::build's order): in each window of
-// kSellWindow rows the rows sorted by length, longest first, ties in row
-// order (a stable rank per row); then slices of 32 consecutive sorted rows,
-// each padded to its longest row; entry k of slice row t at off[slice] + 32 k + t.
-__global__ void __launch_bounds__(256) k_sell_order(int n, int window, const int* __restrict__ rp, int* __restrict__ order) {
-    __shared__ int len[256];
-    const int w0 = blockIdx.x * window, t = threadIdx.x;
-    const int m = min(window, n - w0);
-    if (t < m) len[t] = rp[w0 + t + 1] - rp[w0 + t];
-    __syncthreads();
-    if (t < m) {
-        int r = 0;
-        for (int j = 0; j < m; ++j) r += (len[j] > len[t]) || (len[j] == len[t] && j < t);
-        order[w0 + r] = w0 + t;
-    }
-}
-
-__global__ void k_sell_width(int n, int slices, const int* __restrict__ rp, const int* __restrict__ order,
-                             int* __restrict__ rows, int* __restrict__ width) {
-    for (int sl = blockIdx.x * blockDim.x + threadIdx.x; sl < slices; sl += gridDim.x * blockDim.x) {
-        int w = 0;
-        for (int t = 0; t < 32; ++t) {
-            const int q = sl * 32 + t;
-            const int r = q < n ? order[q] : -1;
-            rows[q] = r;
-            if (r >= 0) w = max(w, rp[r + 1] - rp[r]);
-        }
-        width[sl] = 32 * w;
-    }
-}
-
-__global__ void k_sell_fill(int slices, const int* __restrict__ rp, const int* __restrict__ ci,
-                            const double* __restrict__ v, const int* __restrict__ rows, const int* __restrict__ off,
-                            int* __restrict__ sci, double* __restrict__ sv, int* __restrict__ src) {
-    const int64_t total = (int64_t)slices * 32;
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
-        const int r = rows[q];
-        if (r < 0) continue;
-        const int sl = (int)(q / 32), t = (int)(q % 32);
-        const int k0 = rp[r], len = rp[r + 1] - k0;
-        for (int k = 0; k < len; ++k) {
-            const size_t e = (size_t)off[sl] + 32 * (size_t)k + t;
-            sci[e] = ci[k0 + k];
-            sv[e] = v[k0 + k];
-            src[e] = k0 + k;
-        }
-    }
-}
-
-int sell_offsets(int slices, const int* width, int* off, cudaStream_t s);  // exclusive scan (amg_device.cu)
-
-__global__ void k_sell_refresh(int64_t entries, const int* __restrict__ src, const double* __restrict__ csr_v,
-                               double* __restrict__ v) {
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < entries; e += (int64_t)gridDim.x * blockDim.x)
-        v[e] = src[e] >= 0 ? csr_v[src[e]] : 0.0;
-}
-
-struct DevSell {
-    int slices = 0;
-    int64_t entries = 0;
-    int pat_n = -1;
-    int64_t pat_nnz = -1;  // the pattern the layout was built for
-    DevBuf<int> off, rows, ci;
-    DevBuf<int> src;  // slot -> CSR entry index (-1 = padding), for value refreshes
+// Sliced-ELL copy (sell.cuh) of a fine-level FP64 matrix for k_sell_spmv.
+struct DevSell : SellPattern {
     DevBuf<double> v;
     // the same values on the same pattern: v from the CSR values (device)
-    void refresh(const double* csr_v, cudaStream_t s) {
-        if (slices > 0 && entries > 0)
-            k_sell_refresh<<<grid_for(entries, 256), 256, 0, s>>>(entries, src.get(), csr_v, v.get());
-        SSV_LAUNCH_CHECK();
-    }
-    // the same layout built on the device from a device CSR (a_rp, a_ci, a_v)
+    void refresh(const double* csr_v, cudaStream_t s) { sell_gather(*this, csr_v, 1, v.get(), s); }
+    // the layout built on the device from a device CSR (a_rp, a_ci, a_v)
     void build_dev(int n, int64_t nnz, const int* a_rp, const int* a_ci, const double* a_v, cudaStream_t s) {
-        pat_n = n;
-        pat_nnz = nnz;
-        slices = (n + 31) / 32;
-        DevBuf<int> order(std::max(n, 1)), width(std::max(slices, 1));
-        off.alloc(slices + 1);
-        rows.alloc((size_t)std::max(slices, 1) * 32);
-        if (n) {
-            k_sell_order<<<(n + kSellWindow - 1) / kSellWindow, kSellWindow, 0, s>>>(n, kSellWindow, a_rp, order.get());
-            k_sell_width<<<grid_for(slices, 128), 128, 0, s>>>(n, slices, a_rp, order.get(), rows.get(), width.get());
-            SSV_LAUNCH_CHECK();
-        }
-        const int total = sell_offsets(slices, width.get(), off.get(), s);
-        if (total < 0) {  // int offsets would overflow: no copy
-            slices = 0;
-            entries = 0;
-            return;
-        }
-        entries = total;
-        const size_t cap = (size_t)std::max<int64_t>(entries, 1);
-        ci.alloc(cap);
-        src.alloc(cap);
-        v.alloc(cap);
-        SSV_CUDA(cudaMemsetAsync(ci.get(), 0xff, sizeof(int) * cap, s));  // -1: padding
-        SSV_CUDA(cudaMemsetAsync(src.get(), 0xff, sizeof(int) * cap, s));
-        SSV_CUDA(cudaMemsetAsync(v.get(), 0, sizeof(double) * cap, s));
-        if (slices)
-            k_sell_fill<<<grid_for((int64_t)slices * 32, 256), 256, 0, s>>>(slices, a_rp, a_ci, a_v, rows.get(),
-                                                                             off.get(), ci.get(), v.get(), src.get());
-        SSV_LAUNCH_CHECK();
-        SSV_CUDA(cudaStreamSynchronize(s));  // the temporaries go out of scope
+        if (!build_pattern(n, nnz, a_rp, a_ci, s)) return;
+        v.alloc((size_t)std::max<int64_t>(entries, 1));
+        sell_gather(*this, a_v, 1, v.get(), s);
+        SSV_CUDA(cudaStreamSynchronize(s));
     }
     void build(const HostCsr& A, cudaStream_t s) {
         pat_n = A.n;
@@ -2414,16 +2314,34 @@ static bool ams_device_setup(AmsState& a, const ssv_matrix* A, cudaStream_t s) {
                 Abc, s);
     log.mark("BC matrix");
     std::vector<DAmgLevel> amg[4];
-    for (int sub = 0; sub < 4; ++sub) {
-        const DCsr& P0 = sub == 0 ? D.G : D.Pi[sub - 1];
-        const DCsr& P0t = sub == 0 ? D.Gt : D.Pit[sub - 1];
-        DCsr A0;
-        if (!d_rap(Abc, P0, P0t, A0, s)) return false;
-        d_fix_zero_rows(A0, s);
-        log.mark("subspace %d Galerkin product (%d rows, %lld nnz)", sub, A0.n, (long long)A0.nnz);
-        if (!d_amg_setup(A0, a.host.theta, 25, 500, amg[sub], s)) return false;
-        log.mark("subspace %d hierarchy (%zu levels)", sub, amg[sub].size());
+    std::thread coarse[4];  // the coarsest factorisations, on host threads while the device goes on
+    auto join = [&] {
+        for (auto& t : coarse)
+            if (t.joinable()) t.join();
+    };
+    try {
+        for (int sub = 0; sub < 4; ++sub) {
+            const DCsr& P0 = sub == 0 ? D.G : D.Pi[sub - 1];
+            const DCsr& P0t = sub == 0 ? D.Gt : D.Pit[sub - 1];
+            DCsr A0;
+            if (!d_rap(Abc, P0, P0t, A0, s)) {
+                join();
+                return false;
+            }
+            d_fix_zero_rows(A0, s);
+            log.mark("subspace %d Galerkin product (%d rows, %lld nnz)", sub, A0.n, (long long)A0.nnz);
+            if (!d_amg_setup(A0, a.host.theta, 25, 500, amg[sub], s, &coarse[sub])) {
+                join();
+                return false;
+            }
+            log.mark("subspace %d hierarchy (%zu levels)", sub, amg[sub].size());
+        }
+    } catch (...) {
+        join();
+        throw;
     }
+    join();
+    log.mark("coarsest factorisations joined");
     D.A_bc = std::move(Abc);
     for (int sub = 0; sub < 4; ++sub) D.amg[sub] = std::move(amg[sub]);
     d_fine_l1(D.A_bc, D.fine_l1, s);
@@ -2844,6 +2762,78 @@ static void ams_profile_t(AmsState& a, int reps, bool cold, ssv_phase_profile* o
     SSV_CUDA(cudaEventDestroy(e0));
     SSV_CUDA(cudaEventDestroy(e1));
     SSV_CUDA(cudaStreamSynchronize(s));
+}
+
+// Per-level device time of one subspace V-cycle (measurement hook): the down
+// product R_l and the up product U_l of every level run one by one (warm,
+// back to back, reps times), then the last step (the dense tail or the
+// coarsest solve); shape = lanes * 10 + rows per group, as the tuner chose.
+template <typename T, int NV>
+static int profile_levels_t(std::vector<AmgDevLevel>& L, int reps, double* ms_r, double* ms_u, int* shape_r,
+                            int* shape_u, int cap, double* last_ms, cudaStream_t s) {
+    cudaEvent_t e0, e1;
+    SSV_CUDA(cudaEventCreate(&e0));
+    SSV_CUDA(cudaEventCreate(&e1));
+    const int tl = tail_level(L);
+    const int n = tl >= 0 ? tl + 1 : (int)L.size();
+    auto time = [&](auto&& launch) {
+        launch();
+        return (double)time_launches(launch, reps, false, s, e0, e1) / reps;
+    };
+    for (int l = 0; l + 1 < n && l < cap; ++l) {
+        if (!L[l].R.n) {
+            ms_r[l] = ms_u[l] = 0;
+            shape_r[l] = shape_u[l] = 0;
+            continue;
+        }
+        const T* e = (l + 1 == n - 1) ? L[l + 1].xa.template as<T>() : L[l + 1].xb.template as<T>();
+        ms_r[l] = time([&] {
+            mv_spmv<T, T, T, NV, MV_AX, true>(L[l].R, L[l].b.template as<T>(), L[l + 1].b.template as<T>(), nullptr,
+                                              nullptr, T(0), nullptr, s);
+        });
+        ms_u[l] = time([&] {
+            mv_spmv<T, T, T, NV, MV_TWO, true>(L[l].U, L[l].b.template as<T>(), L[l].xb.template as<T>(), e, nullptr,
+                                               T(0), nullptr, s);
+        });
+        shape_r[l] = L[l].R.lanes_for(NV) * 10 + L[l].R.unroll_for(NV);
+        shape_u[l] = L[l].U.lanes_for(NV) * 10 + L[l].U.unroll_for(NV);
+    }
+    *last_ms = time([&] {
+        if (tl >= 0) {
+            TailSet<T, 1> t{};
+            t.n[0] = L[tl].A.n;
+            t.M[0] = L[tl].tail.get();
+            t.b[0] = L[tl].b.template as<T>();
+            t.y[0] = L[tl].xa.template as<T>();
+            tail_apply<T, NV, 1>(t, 1, nullptr, s);
+        } else {
+            coarse_direct<T, NV, true>(L[n - 1], L[n - 1].b.template as<T>(), L[n - 1].xa.template as<T>(), nullptr,
+                                       s);
+        }
+    });
+    SSV_CUDA(cudaEventDestroy(e0));
+    SSV_CUDA(cudaEventDestroy(e1));
+    return n;
+}
+
+int ams_profile_levels(AmsState* a, int sub, int reps, double* ms_r, double* ms_u, int* shape_r, int* shape_u,
+                       int cap, double* last_ms) {
+    if (sub < 0 || sub > 3) fail(SSV_ERR_INVALID_ARG, "ssv_ams_profile_levels: subspace must be 0..3");
+    const int nv = a->complex_form ? 2 : 1;
+    ams_reserve(*a, nv);
+    cudaStream_t s = stream();
+    int n = 0;
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        if (nv == 2)
+            n = profile_levels_t<T, 2>(a->amg[sub], std::max(reps, 1), ms_r, ms_u, shape_r, shape_u, cap, last_ms, s);
+        else
+            n = profile_levels_t<T, 1>(a->amg[sub], std::max(reps, 1), ms_r, ms_u, shape_r, shape_u, cap, last_ms, s);
+    };
+    if (sub_lo(*a, sub)) run(float{});
+    else run(double{});
+    SSV_CUDA(cudaStreamSynchronize(s));
+    return n;
 }
 
 template <typename TG, typename TN>

@@ -175,6 +175,7 @@ int ssv_matrix_update_values(ssv_matrix* A, const void* values) {
         const size_t words = (size_t)A->nnz * (A->dtype == SSV_F64 ? 1 : 2);
         A->val.alloc(words);
         ssv::h2d_staged(A->val.get(), values, words * sizeof(double), ssv::stream());
+        ++A->vgen;
         SSV_CUDA(cudaStreamSynchronize(ssv::stream()));
     });
 }
@@ -444,6 +445,16 @@ int ssv_ams_subspace_apply(ssv_precond* p, int32_t subspace, const double* r, do
             ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_subspace_apply: bad argument");
         if (!p->ready) ssv::fail(SSV_ERR_RUNTIME, "CompactAMS::Mult called before Setup");
         ssv::ams_subspace_apply(p->ams.get(), subspace, r, b_s, x_s, corr);
+    });
+}
+
+int ssv_ams_profile_levels(ssv_precond* p, int32_t subspace, int32_t reps, double* ms_r, double* ms_u,
+                           int32_t* shape_r, int32_t* shape_u, int32_t cap, double* last_ms, int32_t* levels) {
+    return guarded([&] {
+        if (!p || !p->ams || !ms_r || !ms_u || !shape_r || !shape_u || !last_ms || !levels || cap < 0)
+            ssv::fail(SSV_ERR_INVALID_ARG, "ssv_ams_profile_levels: bad argument");
+        if (!p->ready) ssv::fail(SSV_ERR_RUNTIME, "CompactAMS::Mult called before Setup");
+        *levels = ssv::ams_profile_levels(p->ams.get(), subspace, reps, ms_r, ms_u, shape_r, shape_u, cap, last_ms);
     });
 }
 

@@ -80,6 +80,92 @@ k_ngs_spmv_dot(int n, const int* __restrict__ rp, const int* __restrict__ ci, co
     if (grid_reduce2(part, red.partials, red.ticket, total)) ngs_finish<S>(total, st, NGS_RHO);
 }
 
+// The same through the matrix's sliced-ELL copy (sell.cuh): one warp per
+// slice of 32 rows, a lane per row, R steps per round with the next round's
+// values and columns loaded before this round's gathers; each row is summed
+// in its CSR column order.
+template <typename S, int R>
+__global__ void __launch_bounds__(kBlock)
+k_ngs_sell_dot(int slices, const int* __restrict__ off, const int* __restrict__ rows, const int* __restrict__ ci,
+               const S* __restrict__ v, const S* __restrict__ x, S* __restrict__ y, const uint8_t* __restrict__ mask,
+               KState* st, RedBuf red) {
+    pdl_gate();
+    if (st->done) return;
+    const int lane = threadIdx.x & 31;
+    const int wpb = kBlock / 32;
+    double2 part = make_double2(0.0, 0.0);
+    for (int sl = blockIdx.x * wpb + threadIdx.x / 32; sl < slices; sl += gridDim.x * wpb) {
+        const int e1 = off[sl + 1];
+        int e = off[sl] + lane;
+        const int row = rows[(size_t)sl * 32 + lane];
+        S acc = ST<S>::zero();
+        S a[R];
+        int col[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            const int k = e + 32 * u;
+            a[u] = k < e1 ? v[k] : ST<S>::zero();
+            col[u] = k < e1 ? ci[k] : -1;
+        }
+        while (e < e1) {
+            const int en = e + 32 * R;
+            S an[R];
+            int cn[R];
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                const int k = en + 32 * u;
+                an[u] = k < e1 ? v[k] : ST<S>::zero();
+                cn[u] = k < e1 ? ci[k] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < R; ++u)
+                if (col[u] >= 0) acc = ST<S>::fma(a[u], x[col[u]], acc);
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                a[u] = an[u];
+                col[u] = cn[u];
+            }
+            e = en;
+        }
+        if (row >= 0) {
+            if (mask && !mask[row]) acc = ST<S>::zero();
+            y[row] = acc;
+            part = add2(part, s_to2<S>(x[row] * acc));
+        }
+    }
+    double2 total;
+    if (grid_reduce2(part, red.partials, red.ticket, total)) ngs_finish<S>(total, st, NGS_RHO);
+}
+
+// SSV_KRYLOV_SELL=0: the COCR iteration's SpMV stays on the CSR arrays
+static bool krylov_sell_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("SSV_KRYLOV_SELL");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v != 0;
+}
+
+// The matrix's sliced-ELL values for the iteration's SpMV, or null (small
+// matrices, switched off, or a layout past the int range): the layout is built
+// once per matrix, the values gathered again whenever they changed. Called
+// outside any capture.
+static const double* krylov_sell(ssv_matrix* A, cudaStream_t s) {
+    if (!krylov_sell_enabled() || A->rows < 65536) return nullptr;
+    if (!A->sell_tried) {
+        A->sell_tried = true;
+        if (!A->sell.build_pattern(A->rows, A->nnz, A->rp.get(), A->ci.get(), s)) return nullptr;
+        A->sell_v.alloc((size_t)std::max<int64_t>(A->sell.entries, 1) * (A->dtype == SSV_F64 ? 1 : 2));
+    }
+    if (A->sell.slices <= 0) return nullptr;
+    if (A->sell_vgen != A->vgen) {
+        sell_gather(A->sell, A->val.get(), A->dtype == SSV_F64 ? 1 : 2, A->sell_v.get(), s);
+        A->sell_vgen = A->vgen;
+    }
+    return A->sell_v.get();
+}
+
 // sol += alpha p ; r -= alpha q ; rt -= alpha qt ; res = sqrt(|r^H r|)
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
@@ -220,7 +306,8 @@ static void run_cocr_ngs(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, int
                       std::to_string((size_t)fd) + ";" + std::to_string((size_t)x) + ";" +
                       std::to_string((size_t)dst) + ";" + std::to_string(A->lanes) + ";" +
                       std::to_string((size_t)red.partials);
-    key += ";" + pre_key(pre);
+    const double* sv = krylov_sell(A, s);  // before any capture
+    key += ";" + pre_key(pre) + ";sell:" + std::to_string((size_t)sv);
     // the iteration graph; captured after the first preconditioner application, which
     // allocates and tunes on first use
     auto build = [&] {
@@ -228,7 +315,11 @@ static void run_cocr_ngs(ssv_matrix* A, ssv_precond* pre, const uint8_t* fd, int
             apply_pre<S>(pre, q, qt, dst, n, s);
             launch_k(k_ngs_dot<S>, g, kBlock, s, n, qt, q, dst, NGS_MU, red);
             launch_k(k_ngs_update<S>, g, kBlock, s, n, x, p, q, qt, r, rt, dst, red);
-            {
+            if (sv) {
+                const int gs = std::max(1, std::min((A->sell.slices + kBlock / 32 - 1) / (kBlock / 32), sm_count() * 8));
+                launch_k(k_ngs_sell_dot<S, 4>, gs, kBlock, s, A->sell.slices, A->sell.off.get(), A->sell.rows.get(),
+                         A->sell.ci.get(), reinterpret_cast<const S*>(sv), rt, t, fd, dst, red);
+            } else {
                 const int L = A->lanes & 0xff;
                 const int rpb = kBlock / L;
                 int gg = std::max(1, std::min((n + rpb - 1) / rpb, sm_count() * 8));

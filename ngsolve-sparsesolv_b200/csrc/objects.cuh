@@ -8,6 +8,7 @@
 
 #include "host_order.hpp"
 #include "kernels.cuh"
+#include "sell.cuh"
 
 namespace ssv {
 
@@ -269,6 +270,13 @@ struct ssv_matrix {
     ssv::DevBuf<int> rp, ci;
     ssv::DevBuf<double> val;  // nnz (F64) or 2*nnz (C128) doubles
     int lanes = 8;  // SpMV launch shape (pick_shape)
+    unsigned vgen = 0;  // bumped whenever the values change
+    // sliced-ELL copy for the COCR iteration's SpMV of a large matrix (built on
+    // first use, values gathered again after a value change)
+    ssv::SellPattern sell;
+    ssv::DevBuf<double> sell_v;
+    unsigned sell_vgen = ~0u;
+    bool sell_tried = false;
 };
 
 struct ssv_solver {

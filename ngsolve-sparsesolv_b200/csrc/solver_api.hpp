@@ -65,6 +65,8 @@ int ams_precision(const AmsState* a);
 // form: Re/Im pairs), after ams_reserve_block(a, nrhs).
 void ams_reserve_block(AmsState* a, int nrhs);
 void ams_profile(AmsState* a, int nrhs, int reps, int flags, ssv_phase_profile* out);
+int ams_profile_levels(AmsState* a, int sub, int reps, double* ms_r, double* ms_u, int* shape_r, int* shape_u,
+                       int cap, double* last_ms);
 void ams_apply_block(AmsState* a, const double* in, double* out, int nrhs, const KState* st, cudaStream_t s);
 // one subspace correction on its own (host arrays; parity hook)
 void ams_subspace_apply(AmsState* a, int sub, const double* r, double* bs, double* xs, double* corr);

@@ -849,6 +849,21 @@ class _AmsBase(_PrecondBase):
                                         ctypes.byref(prof)))
         return prof.as_list()
 
+    def profile_levels(self, sub, reps=20):
+        """Per-level device time (ms) of subspace sub's V-cycle (measurement hook): a list of
+        (level, R ms, U ms, R shape, U shape) for the levels run one by one, and the last step's ms
+        (dense tail or coarsest solve)."""
+        cap = 32
+        mr, mu = np.zeros(cap), np.zeros(cap)
+        sr, su = np.zeros(cap, np.int32), np.zeros(cap, np.int32)
+        last = ctypes.c_double()
+        nl = ctypes.c_int32()
+        check(self._lib.ssv_ams_profile_levels(self._h, int(sub), int(reps), _capi.vptr(mr), _capi.vptr(mu),
+                                               _capi.vptr(sr), _capi.vptr(su), cap, ctypes.byref(last),
+                                               ctypes.byref(nl)))
+        rows = [(l, float(mr[l]), float(mu[l]), int(sr[l]), int(su[l])) for l in range(max(nl.value - 1, 0))]
+        return rows, last.value
+
     @property
     def setup_times(self):
         """Wall seconds of the last set-up (construction, Update() or precision switch): total,

@@ -195,6 +195,7 @@ SIGNATURES = [
     ("ssv_precond_apply", I32, [P, P, P]),
     ("ssv_precond_apply_block", I32, [P, I32, P, P]),
     ("ssv_ams_subspace_apply", I32, [P, I32, P, P, P, P]),
+    ("ssv_ams_profile_levels", I32, [P, I32, I32, P, P, P, P, I32, P, P]),
     ("ssv_precond_apply_dev", I32, [P, P, P]),
     ("ssv_ic_actual_shift", I32, [P, PD]),
     ("ssv_precond_destroy", I32, [P]),
