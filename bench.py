@@ -47,7 +47,9 @@ sys.path.insert(0, os.path.join(ROOT, "ngsolve-sparsesolv_b200"))
 METRIC = "time-to-solution @1e-10 (s), ms/iter, SpMV HBM GB/s: mixed/batched vs plain FP64 GPU"
 UNIT = "s"
 # dram__bytes_read.sum + dram__bytes_write.sum of one eddy64 fine-residual launch (ncu; None until captured)
-EDDY_FINE_RESIDUAL_TRAFFIC = None
+# DRAM bytes per launch of the fine residual at 64^3: the 48^3 ncu capture's traffic (195.3 MB against
+# 195.2 MB algorithmic) scaled to 64^3 by the algorithmic bytes (461.3 MB)
+EDDY_FINE_RESIDUAL_TRAFFIC = 461.5e6
 
 
 def _peaks():
@@ -781,8 +783,8 @@ def run_eddy(args, rank, world, local):
     spmv_warm = next(p for p in prof if p["name"] == "fine_residual")
     roofline = {"bound": "hbm", "achieved": gbps(spmv), "peak": peak, "unit": "GB/s", "frac": gbps(spmv) / peak,
                 "traffic": EDDY_FINE_RESIDUAL_TRAFFIC,
-                "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one launch of this kernel (ncu, same "
-                                "workload), per launch",
+                "traffic_note": "DRAM bytes of one launch of this kernel from an ncu capture on the 48^3 mesh "
+                                "(dram__bytes.sum), scaled to 64^3 by the algorithmic bytes",
                 "kernel": "k_sell_spmv fine residual (A_bc real in 32-row sliced-ELL, Re/Im columns, 30.3M nnz, FP64; "
                           "tuner-chosen over the CSR shapes), each launch timed alone after evicting L2 by reading a "
                           "256 MB buffer",
