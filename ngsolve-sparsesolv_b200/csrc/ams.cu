@@ -191,7 +191,7 @@ template <typename TX, typename TY, int NV, int MODE, bool RECIP, int R>
 __global__ void __launch_bounds__(kBlock)
 k_sell_spmv(int slices, const int* __restrict__ off, const int* __restrict__ rows, const int* __restrict__ ci,
             const double* __restrict__ v, const TX* __restrict__ x, TY* __restrict__ y, const TY* __restrict__ b,
-            const TY* __restrict__ d, TY w, const KState* st) {
+            const TY* __restrict__ d, TY w, const KState* st, int n) {
     using TA = wider_t<double, TX>;
     pdl_gate();
     if (st && st->done) return;
@@ -226,7 +226,12 @@ k_sell_spmv(int slices, const int* __restrict__ off, const int* __restrict__ row
             for (int u = 0; u < R; ++u) {
                 if (col[u] >= 0) {
                     TX xv[NV];
-                    load_row<NV>(x + (size_t)col[u] * NV, xv);
+                    if constexpr (MODE == MV_TWO)  // columns past the row count read the b slot
+                        load_row<NV>(col[u] < n ? x + (size_t)col[u] * NV
+                                                : reinterpret_cast<const TX*>(b) + (size_t)(col[u] - n) * NV,
+                                     xv);
+                    else
+                        load_row<NV>(x + (size_t)col[u] * NV, xv);
 #pragma unroll
                     for (int c = 0; c < NV; ++c) acc[c] += (TA)a[u] * (TA)xv[c];
                 }
@@ -243,7 +248,7 @@ k_sell_spmv(int slices, const int* __restrict__ off, const int* __restrict__ row
 #pragma unroll
             for (int c = 0; c < NV; ++c) {
                 const TY ac = (TY)acc[c];
-                if constexpr (MODE == MV_AX) {
+                if constexpr (MODE == MV_AX || MODE == MV_TWO) {
                     y[base + c] = ac;
                 } else if constexpr (MODE == MV_RES) {
                     y[base + c] = b[base + c] - ac;
@@ -1046,7 +1051,8 @@ template <typename TX, typename TY, int NV, int MODE, bool RECIP>
 static void launch_sell(const DevSell& S, int steps, cudaStream_t s, const TX* x, TY* y, const TY* b, const TY* d,
                         TY w, const KState* st) {
     const int grid = std::max(1, (S.slices + kBlock / 32 - 1) / (kBlock / 32));
-#define SSV_SELL_ARGS grid, kBlock, s, S.slices, S.off.get(), S.rows.get(), S.ci.get(), S.v.get(), x, y, b, d, w, st
+#define SSV_SELL_ARGS grid, kBlock, s, S.slices, S.off.get(), S.rows.get(), S.ci.get(), S.v.get(), x, y, b, d, w, st, \
+                      S.pat_n
     if (steps == 2) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 2>, SSV_SELL_ARGS);
     else if (steps == 4) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 4>, SSV_SELL_ARGS);
     else launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 8>, SSV_SELL_ARGS);
@@ -1056,7 +1062,7 @@ static void launch_sell(const DevSell& S, int steps, cudaStream_t s, const TX* x
 template <typename TV, typename TX, typename TY, int NV, int MODE, bool RECIP>
 static void mv_spmv(const DevCsr& A, const TX* x, TY* y, const TY* b, const TY* d, TY w, const KState* st,
                     cudaStream_t s) {
-    if constexpr (std::is_same_v<TV, double> && MODE != MV_TWO) {
+    if constexpr (std::is_same_v<TV, double>) {
         if (A.sell_for(NV)) {
             launch_sell<TX, TY, NV, MODE, RECIP>(A.sell, A.tuned_sell[DevCsr::nv_slot(NV)], s, x, y, b, d, w, st);
             return;
@@ -1258,7 +1264,26 @@ static void vcycleM(std::vector<AmgDevLevel>* const* H, const T* const* rhs0, in
         auto Lt = [&](int k) { return lt[k] >= 0 ? lt[k] + 1 : L(k); };
         Lmax = 0;
         for (int k = 0; k < parts; ++k) Lmax = std::max(Lmax, Lt(k));
+        // a level whose products all have a chosen sliced-ELL copy (the large FP64 levels) runs
+        // them one by one on it; the rest in one lockstep launch
+        auto all_sell = [&](int l, bool up) {
+            bool any = false;
+            for (int k = 0; k < parts; ++k) {
+                if (l >= Lt(k) - 1) continue;
+                const DevCsr& M = up ? lv(k, l).U : lv(k, l).R;
+                if (!M.sell_for(NV)) return false;
+                any = true;
+            }
+            return any;
+        };
         for (int l = 0; l < Lmax - 1; ++l) {
+            if (all_sell(l, false)) {
+                for (int k = 0; k < parts; ++k)
+                    if (l < Lt(k) - 1)
+                        mv_spmv<T, T, T, NV, MV_AX, RECIP>(lv(k, l).R, rhs(k, l), lv(k, l + 1).b.template as<T>(),
+                                                           nullptr, nullptr, T(0), st, s);
+                continue;
+            }
             Tri<T, K> rs{};
             int q = 0, k0 = -1;
             for (int k = 0; k < parts; ++k) {
@@ -1300,6 +1325,16 @@ static void vcycleM(std::vector<AmgDevLevel>* const* H, const T* const* rhs0, in
             }
         }
         for (int l = Lmax - 2; l >= 0; --l) {
+            if (all_sell(l, true)) {
+                for (int k = 0; k < parts; ++k) {
+                    if (l > Lt(k) - 2) continue;
+                    AmgDevLevel& nx = lv(k, l + 1);
+                    const T* e = (l + 1 == Lt(k) - 1) ? nx.xa.template as<T>() : nx.xb.template as<T>();
+                    mv_spmv<T, T, T, NV, MV_TWO, RECIP>(lv(k, l).U, rhs(k, l), lv(k, l).xb.template as<T>(), e,
+                                                        nullptr, T(0), st, s);
+                }
+                continue;
+            }
             Tri<T, K> up{};
             int q = 0, k0 = -1;
             for (int k = 0; k < parts; ++k) {
@@ -1778,7 +1813,9 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
         if (A.sell.slices > 0 && sell_enabled()) {
             for (int R : {2, 4, 8}) {
                 auto launch = [&] {
-                    if (b)
+                    if (two)
+                        launch_sell<TX, TY, NV, MV_TWO, false>(A.sell, R, s, x, y, b, nullptr, TY(0), nullptr);
+                    else if (b)
                         launch_sell<TX, TY, NV, MV_RES, false>(A.sell, R, s, x, y, b, nullptr, TY(0), nullptr);
                     else
                         launch_sell<TX, TY, NV, MV_AX, false>(A.sell, R, s, x, y, nullptr, nullptr, TY(0), nullptr);
@@ -2243,6 +2280,11 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
         for (size_t l = 0; l < fused[sub].size(); ++l) {
             a.amg[sub][l].R.upload(fused[sub][l].R, lo, s);
             a.amg[sub][l].U.upload(fused[sub][l].U, lo, s);
+            // sliced-ELL copies of the large FP64 level products (timed by the tuner against CSR)
+            if (!lo && sell_enabled() && fused[sub][l].R.n >= kUnrollMinRows)
+                a.amg[sub][l].R.sell.build(fused[sub][l].R, s);
+            if (!lo && sell_enabled() && fused[sub][l].U.n >= kUnrollMinRows)
+                a.amg[sub][l].U.sell.build(fused[sub][l].U, s);
         }
         // level-0 scaling folded into this subspace's transfers
         if (sub == 0) {
@@ -2446,6 +2488,10 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
                 if (d_fused_level(*Al, *Pl, *Ptl, l1p, R, U, s)) {
                     devcsr_from(dl.R, R, lo, s);
                     devcsr_from(dl.U, U, lo, s);
+                    if (!lo && sell_enabled() && R.n >= kUnrollMinRows)
+                        dl.R.sell.build_dev(R.n, R.nnz, R.rp.get(), R.ci.get(), R.v.get(), s);
+                    if (!lo && sell_enabled() && U.n >= kUnrollMinRows)
+                        dl.U.sell.build_dev(U.n, U.nnz, U.rp.get(), U.ci.get(), U.v.get(), s);
                 }
                 SSV_CUDA(cudaStreamSynchronize(s));
                 t_fused += wall_seconds() - tf0;
