@@ -471,19 +471,24 @@ __global__ void k_pmis_finish(int n, int* __restrict__ cf, int* __restrict__ isc
 // std::mt19937(42), as the host's PMIS takes them (one per row, in row order);
 // kept for the longest n asked so far (a prefix serves any shorter n).
 const double* pmis_random(int n, cudaStream_t s) {
+    // shared by concurrent set-ups: a grown table never frees the one that kernels
+    // on other streams may still read, and it is allocated outside any
+    // stream-ordered scope
     static std::mutex mu;
     static std::vector<double> host;
-    static DevBuf<double> dev;
+    static std::vector<DevBuf<double>> dev;
     std::lock_guard<std::mutex> lk(mu);
     if ((int)host.size() < n) {
         host.resize(n);
         std::mt19937 rng(42);
         std::uniform_real_distribution<double> dist(0.0, 1.0);
         for (int i = 0; i < n; ++i) host[i] = dist(rng);
-        dev.upload(host.data(), host.size(), s);
+        AllocScope plain(nullptr);
+        dev.emplace_back();
+        dev.back().upload(host.data(), host.size(), s);
         SSV_CUDA(cudaStreamSynchronize(s));
     }
-    return dev.get();
+    return dev.back().get();
 }
 
 // ---- direct interpolation (BuildClassicalInterp, compact_amg.hpp:488-612) ----------

@@ -32,6 +32,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <thread>
 #include <type_traits>
 
@@ -2345,6 +2346,72 @@ static void fine_from(DevCsr& M, const DCsr& D, bool layout_valid, cudaStream_t 
         M.sell.build_dev(D.n, D.nnz, D.rp.get(), D.ci.get(), D.v.get(), s);
 }
 
+// The four subspaces' set-up steps on host threads, each on its own stream with
+// stream-ordered temporaries (AllocScope), so their latency-bound launch chains
+// and host syncs overlap. The caller's stream s is drained first (buffers a job
+// frees may have been in use there) and each job's stream before its thread
+// ends; errors are rethrown on the calling thread. SSV_AMS_SETUP_THREADS=0
+// runs the jobs in turn on s.
+static bool setup_threads_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("SSV_AMS_SETUP_THREADS");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v != 0;
+}
+
+static cudaStream_t setup_stream(int k) {
+    static cudaStream_t st[4] = {};
+    static std::once_flag once;
+    std::call_once(once, [] {
+        for (auto& x : st) SSV_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+        // the pool keeps up to 4 GB of freed temporaries for the next set-up
+        int dev = 0;
+        cudaMemPool_t pool;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = 4ull << 30;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    });
+    return st[k];
+}
+
+template <typename F>
+static void for_subspaces(cudaStream_t s, F&& job) {
+    if (!setup_threads_enabled()) {
+        for (int sub = 0; sub < 4; ++sub) job(sub, s);
+        return;
+    }
+    SSV_CUDA(cudaStreamSynchronize(s));
+    int dev = 0;
+    SSV_CUDA(cudaGetDevice(&dev));
+    std::exception_ptr err[4];
+    std::vector<std::thread> th;
+    for (int sub = 0; sub < 4; ++sub) {
+        try {
+            th.emplace_back([&, sub] {
+                try {
+                    SSV_CUDA(cudaSetDevice(dev));
+                    cudaStream_t ss = setup_stream(sub);
+                    {
+                        AllocScope scope(ss);
+                        job(sub, ss);
+                    }
+                    SSV_CUDA(cudaStreamSynchronize(ss));
+                } catch (...) {
+                    err[sub] = std::current_exception();
+                }
+            });
+        } catch (...) {
+            err[sub] = std::current_exception();
+        }
+    }
+    for (auto& t : th) t.join();
+    for (auto& e : err)
+        if (e) std::rethrow_exception(e);
+}
+
 // BC matrix, Galerkin products (FixZeroRows) and AMG hierarchies of the four
 // subspaces, fine l1 norms; false (nothing replaced) if a product row is too
 // long for the device symbolic step
@@ -2357,33 +2424,34 @@ static bool ams_device_setup(AmsState& a, const ssv_matrix* A, cudaStream_t s) {
     log.mark("BC matrix");
     std::vector<DAmgLevel> amg[4];
     std::thread coarse[4];  // the coarsest factorisations, on host threads while the device goes on
+    bool ok[4] = {true, true, true, true};
     auto join = [&] {
         for (auto& t : coarse)
             if (t.joinable()) t.join();
     };
     try {
-        for (int sub = 0; sub < 4; ++sub) {
+        for_subspaces(s, [&](int sub, cudaStream_t ss) {
+            SetupLog slog(ss);
             const DCsr& P0 = sub == 0 ? D.G : D.Pi[sub - 1];
             const DCsr& P0t = sub == 0 ? D.Gt : D.Pit[sub - 1];
             DCsr A0;
-            if (!d_rap(Abc, P0, P0t, A0, s)) {
-                join();
-                return false;
+            if (!d_rap(Abc, P0, P0t, A0, ss)) {
+                ok[sub] = false;
+                return;
             }
-            d_fix_zero_rows(A0, s);
-            log.mark("subspace %d Galerkin product (%d rows, %lld nnz)", sub, A0.n, (long long)A0.nnz);
-            if (!d_amg_setup(A0, a.host.theta, 25, 500, amg[sub], s, &coarse[sub])) {
-                join();
-                return false;
-            }
-            log.mark("subspace %d hierarchy (%zu levels)", sub, amg[sub].size());
-        }
+            d_fix_zero_rows(A0, ss);
+            slog.mark("subspace %d Galerkin product (%d rows, %lld nnz)", sub, A0.n, (long long)A0.nnz);
+            ok[sub] = d_amg_setup(A0, a.host.theta, 25, 500, amg[sub], ss, &coarse[sub]);
+            slog.mark("subspace %d hierarchy (%zu levels)", sub, amg[sub].size());
+        });
     } catch (...) {
         join();
         throw;
     }
     join();
-    log.mark("coarsest factorisations joined");
+    log.mark("subspace hierarchies and coarsest factorisations");
+    for (bool o : ok)
+        if (!o) return false;
     D.A_bc = std::move(Abc);
     for (int sub = 0; sub < 4; ++sub) D.amg[sub] = std::move(amg[sub]);
     d_fine_l1(D.A_bc, D.fine_l1, s);
@@ -2405,8 +2473,13 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
     SSV_CUDA(cudaMemcpyAsync(a.fine_l1.get(), D.fine_l1.get(), sizeof(double) * a.nhc, cudaMemcpyDeviceToDevice, s));
     a.fine_il1.alloc(std::max(a.nhc, 1));
     d_reciprocal(a.nhc, a.fine_l1.get(), a.fine_il1.get(), s);
-    double t_fused = 0;
-    for (int sub = 0; sub < 4; ++sub) {
+    (void)fused_enabled();  // the switches are read once, before the jobs' threads
+    (void)sell_enabled();
+    (void)tail_rows();
+    double t_fused_sub[4] = {0, 0, 0, 0};
+    auto job = [&](int sub, cudaStream_t s) {
+        SetupLog log(s);
+        double& t_fused = t_fused_sub[sub];
         const auto& hl = D.amg[sub];
         const size_t L = hl.size();
         a.amg[sub].clear();
@@ -2531,11 +2604,18 @@ static void ams_build_cycle(AmsState& a, bool layout_valid, cudaStream_t s) {
                                          cudaMemcpyDeviceToDevice, s));
             }
         }
-    }
-    log.mark("transfers");
-    build_tails(a, s);
-    log.mark("dense V-cycle tails");
-    a.t_fused = t_fused;
+        if (a.num_smooth == 1) {
+            if (lo) build_tail<float>(a.amg[sub], s);
+            else build_tail<double>(a.amg[sub], s);
+        } else {
+            for (auto& lv : a.amg[sub]) lv.tail.release();
+        }
+        const int tl = tail_level(a.amg[sub]);
+        log.mark("subspace %d transfers and %s", sub, tl >= 0 ? "dense tail" : "no dense tail");
+    };
+    for_subspaces(s, job);
+    log.mark("subspace cycle arrays, transfers, dense tails");
+    a.t_fused = t_fused_sub[0] + t_fused_sub[1] + t_fused_sub[2] + t_fused_sub[3];
     a.nv_alloc = 0;
     ams_reserve(a, nv);
     log.mark("work vectors + shape tuner");

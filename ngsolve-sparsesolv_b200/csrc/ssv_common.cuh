@@ -122,17 +122,40 @@ __host__ __device__ inline zdouble hi_of_any(zfloat a) { return {(double)a.x, (d
 // ---------------------------------------------------------------------------
 // Device memory
 // ---------------------------------------------------------------------------
+// While a thread has an allocation stream set (AllocScope), its DevBuf
+// allocations are stream-ordered on it (cudaMallocAsync / cudaFreeAsync from
+// the device's default pool): no device-wide synchronisation per free, so
+// host threads that each build one part of a set-up on their own stream do
+// not serialise on their temporaries. A buffer allocated that way and freed
+// outside such a scope is freed by cudaFree (which waits for the device).
+inline cudaStream_t& alloc_stream() {
+    thread_local cudaStream_t s = nullptr;
+    return s;
+}
+struct AllocScope {
+    cudaStream_t prev;
+    explicit AllocScope(cudaStream_t s) : prev(alloc_stream()) { alloc_stream() = s; }
+    ~AllocScope() { alloc_stream() = prev; }
+    AllocScope(const AllocScope&) = delete;
+    AllocScope& operator=(const AllocScope&) = delete;
+};
+
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
+    bool pooled = false;  // from cudaMallocAsync
     DevBuf() = default;
     explicit DevBuf(size_t count) { alloc(count); }
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), pooled(o.pooled) { o.p = nullptr; o.n = 0; o.pooled = false; }
     DevBuf& operator=(DevBuf&& o) noexcept {
-        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        if (this != &o) {
+            release();
+            p = o.p; n = o.n; pooled = o.pooled;
+            o.p = nullptr; o.n = 0; o.pooled = false;
+        }
         return *this;
     }
     ~DevBuf() { release(); }
@@ -140,12 +163,22 @@ struct DevBuf {
         if (count == n && p) return;
         release();
         n = count;
-        if (count) SSV_CUDA(cudaMalloc(&p, sizeof(T) * count));
+        if (!count) return;
+        if (cudaStream_t as = alloc_stream()) {
+            SSV_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p), sizeof(T) * count, as));
+            pooled = true;
+        } else {
+            SSV_CUDA(cudaMalloc(&p, sizeof(T) * count));
+        }
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (pooled && alloc_stream()) cudaFreeAsync(p, alloc_stream());
+            else cudaFree(p);
+        }
         p = nullptr;
         n = 0;
+        pooled = false;
     }
     void upload(const T* h, size_t count, cudaStream_t s) {
         alloc(count);
