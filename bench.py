@@ -798,14 +798,19 @@ def run_eddy(args, rank, world, local):
                   l2="evicted between timed steps (256 MB read)",
                   form="plain FP64 (the drop-in: COCRSolverNGS recurrence, FP64 ComplexCompactAMS)",
                   iterations=plain["iterations"], ms_per_iter=value * 1e3 / max(plain["iterations"], 1),
-                  spmv_GBps=gbps(spmv), true_rel_residual=plain["true_rel_residual"], ams_setup_s=setup_s,
-                  ams_setup_breakdown_s=setup_times,
+                  spmv_GBps=gbps(spmv), true_rel_residual=plain["true_rel_residual"],
+                  true_rel_residual_meets_tol=bool(plain["true_rel_residual"] <= 1e-10),
+                  stop_rule="plain form: the recurrence residual ||r_j|| / ||b|| <= tol (COCRSolverNGS, "
+                            "sparsesolv_solvers.hpp:338-344), so its true residual can end above tol; mixed form: "
+                            "the FP64 true residual <= tol",
+                  ams_setup_s=setup_s, ams_setup_breakdown_s=setup_times,
                   mixed_form="ComplexCompactAMS with the three nodal hierarchies in FP32 (diagonally scaled) and the "
                              "gradient hierarchy, fine level, transfers and coarsest solves FP64, under refined COCR: "
                              f"cycles restarted from the FP64 true residual after a {REFINE_DROP:g} drop, stop on the "
                              "true residual",
                   mixed_time_to_solution_s=mixed["s"], mixed_iterations=mixed["iterations"],
                   mixed_cycles=mixed["cycles"], mixed_true_rel_residual=mixed["true_rel_residual"],
+                  mixed_true_rel_residual_meets_tol=bool(mixed["true_rel_residual"] <= 1e-10),
                   mixed_ms_per_iter=mixed["s"] * 1e3 / max(mixed["iterations"], 1),
                   speedup_mixed_vs_plain=value / mixed["s"],
                   error_mixed_vs_plain=_rel_err(mixed["x"], plain["x"]),
