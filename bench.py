@@ -218,6 +218,13 @@ def run_ncu_case(args):
         torch.cuda.nvtx.range_pop()
         print(json.dumps({"ncu_case": args.workload, "mesh": f"{args.eddy_nc}^3", "precision": args.precision_eddy,
                           "iterations": inv.iterations}))
+        if args.profile_levels:  # per-level V-cycle times (warm, back to back) of every subspace
+            for sub in range(4):
+                rows, last = pre.profile_levels(sub, reps=20)
+                print(json.dumps({"subspace": sub, "levels": [{"level": l, "R_us": r * 1e3, "U_us": u * 1e3,
+                                                               "R_shape": sr, "U_shape": su}
+                                                              for l, r, u, sr, su in rows],
+                                  "last_step_us": last * 1e3}))
         return
     if args.workload == "ams40":
         d = _ams_system()
@@ -882,7 +889,7 @@ def run_newton(args, rank, world, local):
     prob = NW.NonlinearMagnetostatic(40)
     amps = np.random.default_rng(2).uniform(0.5, 2.0, 50)
     nsteps = 20
-    tm = {"update_s": 0.0, "solve_s": 0.0, "updates": 0, "solves": 0}
+    tm = {"update_s": 0.0, "solve_s": 0.0, "updates": 0, "solves": 0, "launches": 0}
 
     class TimedPre:
         """the AMS preconditioner, its Update() timed"""
@@ -909,6 +916,7 @@ def run_newton(args, rank, world, local):
             r = self.inv.Solve(rhs, x)
             tm["solve_s"] += time.perf_counter() - t0
             tm["solves"] += 1
+            tm["launches"] += int(r.kernel_launches)
             return r
 
     t0 = time.perf_counter()
@@ -934,7 +942,8 @@ def run_newton(args, rank, world, local):
                            first_step_iterations_previous=first[0], first_step_iterations_learned=first[1],
                            start_error_previous_mean=float(np.mean(ev["start_err_prev"])),
                            start_error_learned_mean=float(np.mean(ev["start_err_mlp"]))),
-            "gpu_launches": None}
+            "gpu_launches": tm["launches"],
+            "gpu_launches_note": "kernels of the PCG solves (the set-up kernels of Update() are not counted)"}
     print(json.dumps(line), flush=True)
 
 
@@ -949,6 +958,8 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"], help="AMS form of --ncu-case")
     ap.add_argument("--precision-eddy", default="fp64", choices=["fp64", "fp32_nodal", "fp32"],
                     help="AMS form of the eddy64 --ncu-case")
+    ap.add_argument("--profile-levels", action="store_true",
+                    help="with the eddy64 --ncu-case: print each subspace's per-level V-cycle times")
     ap.add_argument("--eddy-nc", type=int, default=64,
                     help="mesh size of the eddy64 --ncu-case (a smaller mesh for multi-pass ncu sections)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
