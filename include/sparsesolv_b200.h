@@ -160,6 +160,25 @@ int ssv_matrix_info(const ssv_matrix* A, int32_t* rows, int32_t* cols,
                     int64_t* nnz, int32_t* dtype);
 /* y = A x (SparseMatrixView::multiply, sparse_matrix_view.hpp:139-147). */
 int ssv_matrix_spmv(ssv_matrix* A, const void* x, void* y);
+/* Copies A's CSR arrays to host buffers (row_ptr rows + 1, col_idx and values
+ * nnz entries; values as doubles, two per entry for complex). New, no
+ * reference counterpart: reads back matrices assembled on the device. */
+int ssv_matrix_export(const ssv_matrix* A, int32_t* row_ptr, int32_t* col_idx, void* values);
+
+/* On-device assembly (new, no reference counterpart: NGSolve assembles the
+ * reference's matrices) of a tetrahedral mesh's lowest-order Nedelec system:
+ * K = sum_t nu_t Ke_t (curl-curl), M = sum_t kappa_t Me_t (mass; nu or kappa
+ * NULL = 1), on the pattern of the edges sharing an element (columns sorted,
+ * every entry summed in element order), and the discrete gradient G (ne x nv,
+ * -1 at an edge's first vertex, +1 at its second). Host inputs: coords (nv x 3),
+ * tets (nt x 4 vertex ids), tet_edges (nt x 6 edge ids of the local edges
+ * (0,1),(0,2),(0,3),(1,2),(1,3),(2,3)), signs (nt x 6, +1 where the local edge
+ * runs as the global one, else -1), edge_verts (ne x 2). Outputs: three new
+ * F64 matrix handles. */
+int ssv_hcurl_assemble(int32_t nv, const double* coords, int32_t nt, const int32_t* tets,
+                       const int32_t* tet_edges, const int8_t* signs, int32_t ne,
+                       const int32_t* edge_verts, const double* nu, const double* kappa,
+                       ssv_matrix** K, ssv_matrix** M, ssv_matrix** G);
 int ssv_matrix_spmv_dev(ssv_matrix* A, const void* d_x, void* d_y);
 
 /* ---- SparseSolvSolver (ngsolve/sparsesolv_solvers.hpp:33-239) ---------- */

@@ -180,6 +180,46 @@ int ssv_matrix_update_values(ssv_matrix* A, const void* values) {
     });
 }
 
+int ssv_matrix_export(const ssv_matrix* A, int32_t* row_ptr, int32_t* col_idx, void* values) {
+    return guarded([&] {
+        if (!A || !row_ptr || (!col_idx && A->nnz) || (!values && A->nnz))
+            ssv::fail(SSV_ERR_INVALID_ARG, "ssv_matrix_export: NULL argument");
+        cudaStream_t s = ssv::stream();
+        const size_t words = (size_t)A->nnz * (A->dtype == SSV_F64 ? 1 : 2);
+        SSV_CUDA(cudaMemcpyAsync(row_ptr, A->rp.get(), sizeof(int32_t) * (A->rows + 1), cudaMemcpyDeviceToHost, s));
+        if (A->nnz) {
+            SSV_CUDA(cudaMemcpyAsync(col_idx, A->ci.get(), sizeof(int32_t) * A->nnz, cudaMemcpyDeviceToHost, s));
+            SSV_CUDA(cudaMemcpyAsync(values, A->val.get(), sizeof(double) * words, cudaMemcpyDeviceToHost, s));
+        }
+        SSV_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int ssv_hcurl_assemble(int32_t nv, const double* coords, int32_t nt, const int32_t* tets,
+                       const int32_t* tet_edges, const int8_t* signs, int32_t ne,
+                       const int32_t* edge_verts, const double* nu, const double* kappa,
+                       ssv_matrix** K, ssv_matrix** M, ssv_matrix** G) {
+    return guarded([&] {
+        if (!K || !M || !G) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_hcurl_assemble: NULL output");
+        *K = *M = *G = nullptr;
+        if (nv < 0 || nt < 0 || ne < 0) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_hcurl_assemble: negative size");
+        if ((nv && !coords) || (nt && (!tets || !tet_edges || !signs)) || (ne && !edge_verts))
+            ssv::fail(SSV_ERR_INVALID_ARG, "ssv_hcurl_assemble: NULL array");
+        for (int64_t q = 0; q < (int64_t)nt * 4; ++q)
+            if (tets[q] < 0 || tets[q] >= nv) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_hcurl_assemble: vertex id out of range");
+        for (int64_t q = 0; q < (int64_t)nt * 6; ++q) {
+            if (tet_edges[q] < 0 || tet_edges[q] >= ne)
+                ssv::fail(SSV_ERR_INVALID_ARG, "ssv_hcurl_assemble: edge id out of range");
+            if (signs[q] != 1 && signs[q] != -1) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_hcurl_assemble: signs must be +1 or -1");
+        }
+        for (int64_t q = 0; q < (int64_t)ne; ++q)
+            if (edge_verts[2 * q] < 0 || edge_verts[2 * q] >= edge_verts[2 * q + 1] || edge_verts[2 * q + 1] >= nv)
+                ssv::fail(SSV_ERR_INVALID_ARG, "ssv_hcurl_assemble: an edge must list its vertices low, high");
+        require_device();
+        ssv::hcurl_assemble(nv, coords, nt, tets, tet_edges, signs, ne, edge_verts, nu, kappa, K, M, G);
+    });
+}
+
 int ssv_matrix_destroy(ssv_matrix* A) {
     return guarded([&] {
         if (!A) return;

@@ -44,6 +44,11 @@ void precond_apply_any<zdouble>(ssv_precond* p, const zdouble* x, zdouble* y, co
 // Changes whenever the preconditioner's device structures are rebuilt.
 unsigned precond_generation(const ssv_precond* p);
 
+// on-device assembly of a tetrahedral mesh's Nedelec K, M and gradient G (assembly.cu)
+void hcurl_assemble(int nv, const double* xyz, int nt, const int* tets, const int* tet_edges, const int8_t* signs,
+                    int ne, const int* edge_verts, const double* nu, const double* kappa, ssv_matrix** K,
+                    ssv_matrix** M, ssv_matrix** G);
+
 // Compact AMS (ams.cu)
 AmsState* ams_create(const ssv_matrix* A, const ssv_matrix* G, const uint8_t* fd, const double* cx,
                      const double* cy, const double* cz, int cycle_type, int num_smooth, double theta, double w,

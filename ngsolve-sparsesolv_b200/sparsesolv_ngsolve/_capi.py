@@ -194,6 +194,8 @@ SIGNATURES = [
     ("ssv_precond_update", I32, [P]),
     ("ssv_precond_apply", I32, [P, P, P]),
     ("ssv_precond_apply_block", I32, [P, I32, P, P]),
+    ("ssv_matrix_export", I32, [P, P, P, P]),
+    ("ssv_hcurl_assemble", I32, [I32, P, I32, P, P, P, I32, P, P, P, P, P, P]),
     ("ssv_ams_subspace_apply", I32, [P, I32, P, P, P, P]),
     ("ssv_ams_profile_levels", I32, [P, I32, I32, P, P, P, P, I32, P, P]),
     ("ssv_precond_apply_dev", I32, [P, P, P]),

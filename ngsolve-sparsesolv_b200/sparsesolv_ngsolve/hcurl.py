@@ -133,6 +133,44 @@ def gradient_matrix(m: KuhnMesh):
     return G
 
 
+def assemble_on_device(m: KuhnMesh, nu_e=None, kappa_e=None):
+    """K = sum_t nu_t Ke_t, M = sum_t kappa_t Me_t and G assembled on the GPU
+    (ssv_hcurl_assemble; nu_e / kappa_e None = 1), returned as scipy CSR
+    matrices with the same patterns as assemble() and gradient_matrix()."""
+    import ctypes
+
+    from . import _capi
+    lib = _capi.load()
+    xyz = np.ascontiguousarray(m.coords, dtype=np.float64)
+    tets = np.ascontiguousarray(m.tets, dtype=np.int32)
+    te = np.ascontiguousarray(m.tet_edges, dtype=np.int32)
+    sg = np.ascontiguousarray(m.tet_signs, dtype=np.int8)
+    ev = np.ascontiguousarray(m.edges, dtype=np.int32)
+    nu = None if nu_e is None else np.ascontiguousarray(nu_e, dtype=np.float64)
+    ka = None if kappa_e is None else np.ascontiguousarray(kappa_e, dtype=np.float64)
+    hs = [ctypes.c_void_p() for _ in range(3)]
+    _capi.check(lib.ssv_hcurl_assemble(m.nv, _capi.vptr(xyz), tets.shape[0], _capi.vptr(tets), _capi.vptr(te),
+                                       _capi.vptr(sg), m.ne, _capi.vptr(ev),
+                                       None if nu is None else _capi.vptr(nu), None if ka is None else _capi.vptr(ka),
+                                       ctypes.byref(hs[0]), ctypes.byref(hs[1]), ctypes.byref(hs[2])))
+    out = []
+    try:
+        for h, ncols in zip(hs, (m.ne, m.ne, m.nv)):
+            rows, cols, nnz, dt = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int32()
+            _capi.check(lib.ssv_matrix_info(h, ctypes.byref(rows), ctypes.byref(cols), ctypes.byref(nnz),
+                                            ctypes.byref(dt)))
+            ip = np.empty(rows.value + 1, dtype=np.int32)
+            ix = np.empty(nnz.value, dtype=np.int32)
+            v = np.empty(nnz.value, dtype=np.float64)
+            _capi.check(lib.ssv_matrix_export(h, _capi.vptr(ip), _capi.vptr(ix), _capi.vptr(v)))
+            out.append(sp.csr_matrix((v, ix, ip), shape=(rows.value, ncols)))
+    finally:
+        for h in hs:
+            if h.value:
+                lib.ssv_matrix_destroy(h)
+    return tuple(out)
+
+
 def boundary_freedofs(m: KuhnMesh):
     """1 for free edges, 0 for edges lying in the boundary surface."""
     c = m.coords
