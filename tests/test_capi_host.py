@@ -172,3 +172,47 @@ def test_rcm_permutation_and_edge_shapes():
     assert _rcm(lib, np.zeros(1, np.int32), np.zeros(0, np.int32), 0)[0].size == 0
     od1, rv1 = _rcm(lib, np.array([0, 1], np.int32), np.array([0], np.int32), 1)
     assert od1.tolist() == [0] and rv1.tolist() == [0]
+
+
+def test_hcurl_assemble_validates_inputs_before_the_device():
+    """ssv_hcurl_assemble checks its mesh arrays on the host first: out-of-range
+    ids, signs other than +-1 and edges not listed low -> high are refused with
+    SSV_ERR_INVALID_ARG (on a machine without a device too); a valid mesh then
+    reaches the device check."""
+    from sparsesolv_ngsolve import _capi
+    from sparsesolv_ngsolve import hcurl as H
+    lib = _lib()
+    m = H.kuhn_mesh(2)
+    xyz = np.ascontiguousarray(m.coords, dtype=np.float64)
+    tets = np.ascontiguousarray(m.tets, dtype=np.int32)
+    te = np.ascontiguousarray(m.tet_edges, dtype=np.int32)
+    sg = np.ascontiguousarray(m.tet_signs, dtype=np.int8)
+    ev = np.ascontiguousarray(m.edges, dtype=np.int32)
+
+    def call(tets=tets, te=te, sg=sg, ev=ev):
+        hs = [ctypes.c_void_p() for _ in range(3)]
+        rc = lib.ssv_hcurl_assemble(m.nv, _capi.vptr(xyz), tets.shape[0], _capi.vptr(tets), _capi.vptr(te),
+                                    _capi.vptr(sg), m.ne, _capi.vptr(ev), None, None, ctypes.byref(hs[0]),
+                                    ctypes.byref(hs[1]), ctypes.byref(hs[2]))
+        for h in hs:
+            if h.value:
+                lib.ssv_matrix_destroy(h)
+        return rc
+
+    bad = tets.copy()
+    bad[0, 0] = m.nv
+    assert call(tets=bad) == _capi.SSV_ERR_INVALID_ARG
+    bad = te.copy()
+    bad[1, 2] = -1
+    assert call(te=bad) == _capi.SSV_ERR_INVALID_ARG
+    bad = sg.copy()
+    bad[0, 0] = 0
+    assert call(sg=bad) == _capi.SSV_ERR_INVALID_ARG
+    bad = ev.copy()
+    bad[3] = bad[3][::-1]
+    assert call(ev=bad) == _capi.SSV_ERR_INVALID_ARG
+    cnt = ctypes.c_int32(-1)
+    name = ctypes.create_string_buffer(128)
+    assert lib.ssv_device_info(ctypes.byref(cnt), name, 128) == 0
+    if cnt.value == 0:
+        assert call() == _capi.SSV_ERR_NO_DEVICE
