@@ -63,6 +63,29 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+
+def _init_dist(world, backend="nccl"):
+    """One process group for the replicas (None on one rank); a short timeout, so ranks
+    that wait for a missing peer end with an error."""
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def _max_over_ranks(value, dist, device):
+    """The job's time: the maximum of the ranks' values (every rank calls this once)."""
+    if not dist:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _workload(name):
     import numpy as np
     from sparsesolv_ngsolve import problems as P
@@ -324,12 +347,7 @@ def run_ams(args, rank, world, local):
     import sparsesolv_ngsolve as ss
     from sparsesolv_ngsolve import _capi
 
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = _init_dist(world)
     torch.cuda.set_device(0)
     dev = torch.device("cuda:0")
     lib = _capi.load()
@@ -388,10 +406,7 @@ def run_ams(args, rank, world, local):
         ms, launches, iters, conv = timed_steps(args.steps)
         clock_info = clocks.stop()
         total_ms = sum(ms)
-        if dist:
-            t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
+        total_ms = _max_over_ranks(total_ms, dist, dev)
         prof = pre.profile(nrhs=1, reps=20)
         prof_cold = pre.profile(nrhs=1, reps=10, cold=True)
         forms[prec] = {"ms_per_step": total_ms / args.steps, "launches": launches, "iterations": iters,
@@ -697,12 +712,7 @@ def run_eddy(args, rank, world, local):
     import sparsesolv_ngsolve as ss
     from sparsesolv_ngsolve import _capi
 
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = _init_dist(world)
     torch.cuda.set_device(0)
     dev = torch.device("cuda:0")
     lib = _capi.load()
@@ -757,10 +767,7 @@ def run_eddy(args, rank, world, local):
             launches += nl.value
         clock_info = clocks.stop() if clocks else None
         total_ms = sum(ms)
-        if dist:
-            t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
+        total_ms = _max_over_ranks(total_ms, dist, dev)
         x = d_x.cpu().numpy().view(np.complex128).copy()
         return {"s": total_ms / args.steps / 1e3, "iterations": iters, "cycles": cycles, "launches": launches,
                 "clocks": clock_info, "x": x, "true_rel_residual": _eddy_true_res(d, x)}
@@ -997,12 +1004,7 @@ def main():
     import sparsesolv_ngsolve as ss
     from sparsesolv_ngsolve import _capi
 
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = _init_dist(world)
     torch.cuda.set_device(0)
     dev = torch.device("cuda:0")
 
@@ -1059,10 +1061,7 @@ def main():
         dist.barrier()
     clock_info = clocks.stop()
     total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = _max_over_ranks(total_ms, dist, dev)
     ms_per_step = total_ms / args.steps
     value = ms_per_step / 1e3
 
