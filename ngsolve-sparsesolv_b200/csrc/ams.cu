@@ -187,8 +187,13 @@ k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T
 // row-pointer load in front of them. Padding entries carry column -1 and are
 // skipped. The steps go in rounds of R: the values and columns of round j+1
 // are loaded before the gathers of round j are issued, so each warp keeps two
-// rounds of requests in flight. Each row is summed in its CSR column order.
-template <typename TX, typename TY, int NV, int MODE, bool RECIP, int R>
+// rounds of requests in flight. With P = 2 a warp walks two neighbouring
+// slices side by side (a lane per row of each), which doubles the requests a
+// warp keeps in flight and halves the warp count, so a matrix of about 1.5
+// waves of slices runs in one. Each row is summed in its CSR column order for
+// every R and P. A slice's entry count is a multiple of 32, so the loop
+// conditions are warp-uniform.
+template <typename TX, typename TY, int NV, int MODE, bool RECIP, int R, int P = 1>
 __global__ void __launch_bounds__(kBlock)
 k_sell_spmv(int slices, const int* __restrict__ off, const int* __restrict__ rows, const int* __restrict__ ci,
             const double* __restrict__ v, const TX* __restrict__ x, TY* __restrict__ y, const TY* __restrict__ b,
@@ -198,57 +203,75 @@ k_sell_spmv(int slices, const int* __restrict__ off, const int* __restrict__ row
     if (st && st->done) return;
     const int lane = threadIdx.x & 31;
     const int wpb = kBlock / 32;
-    for (int sl = blockIdx.x * wpb + threadIdx.x / 32; sl < slices; sl += gridDim.x * wpb) {
-        const int e1 = off[sl + 1];
-        int e = off[sl] + lane;
-        const int row = rows[(size_t)sl * 32 + lane];
-        TA acc[NV];
+    for (int sl0 = (blockIdx.x * wpb + threadIdx.x / 32) * P; sl0 < slices; sl0 += gridDim.x * wpb * P) {
+        int e[P], e1[P], row[P];
+        TA acc[P][NV];
+        double a[P][R];
+        int col[P][R];
 #pragma unroll
-        for (int c = 0; c < NV; ++c) acc[c] = TA(0);
-        double a[R];
-        int col[R];
+        for (int q = 0; q < P; ++q) {
+            const int sl = sl0 + q;
+            const bool on = sl < slices;
+            e1[q] = on ? off[sl + 1] : 0;
+            e[q] = on ? off[sl] + lane : 32;  // past e1 = 0: no steps
+            row[q] = on ? rows[(size_t)sl * 32 + lane] : -1;
 #pragma unroll
-        for (int u = 0; u < R; ++u) {
-            const int k = e + 32 * u;
-            a[u] = k < e1 ? v[k] : 0.0;
-            col[u] = k < e1 ? ci[k] : -1;
-        }
-        while (e < e1) {
-            const int en = e + 32 * R;
-            double an[R];
-            int cn[R];
+            for (int c = 0; c < NV; ++c) acc[q][c] = TA(0);
 #pragma unroll
             for (int u = 0; u < R; ++u) {
-                const int k = en + 32 * u;
-                an[u] = k < e1 ? v[k] : 0.0;
-                cn[u] = k < e1 ? ci[k] : -1;
+                const int k = e[q] + 32 * u;
+                a[q][u] = k < e1[q] ? v[k] : 0.0;
+                col[q][u] = k < e1[q] ? ci[k] : -1;
             }
+        }
+        while (true) {
+            bool any = false;
 #pragma unroll
-            for (int u = 0; u < R; ++u) {
-                if (col[u] >= 0) {
-                    TX xv[NV];
-                    if constexpr (MODE == MV_TWO)  // columns past the row count read the b slot
-                        load_row<NV>(col[u] < n ? x + (size_t)col[u] * NV
-                                                : reinterpret_cast<const TX*>(b) + (size_t)(col[u] - n) * NV,
-                                     xv);
-                    else
-                        load_row<NV>(x + (size_t)col[u] * NV, xv);
+            for (int q = 0; q < P; ++q) any |= e[q] < e1[q];
+            if (!any) break;
+            double an[P][R];
+            int cn[P][R];
 #pragma unroll
-                    for (int c = 0; c < NV; ++c) acc[c] += (TA)a[u] * (TA)xv[c];
+            for (int q = 0; q < P; ++q)
+#pragma unroll
+                for (int u = 0; u < R; ++u) {
+                    const int k = e[q] + 32 * R + 32 * u;
+                    an[q][u] = k < e1[q] ? v[k] : 0.0;
+                    cn[q][u] = k < e1[q] ? ci[k] : -1;
                 }
-            }
 #pragma unroll
-            for (int u = 0; u < R; ++u) {
-                a[u] = an[u];
-                col[u] = cn[u];
+            for (int q = 0; q < P; ++q)
+#pragma unroll
+                for (int u = 0; u < R; ++u) {
+                    if (col[q][u] >= 0) {
+                        TX xv[NV];
+                        if constexpr (MODE == MV_TWO)  // columns past the row count read the b slot
+                            load_row<NV>(col[q][u] < n ? x + (size_t)col[q][u] * NV
+                                                       : reinterpret_cast<const TX*>(b) + (size_t)(col[q][u] - n) * NV,
+                                         xv);
+                        else
+                            load_row<NV>(x + (size_t)col[q][u] * NV, xv);
+#pragma unroll
+                        for (int c = 0; c < NV; ++c) acc[q][c] += (TA)a[q][u] * (TA)xv[c];
+                    }
+                }
+#pragma unroll
+            for (int q = 0; q < P; ++q) {
+#pragma unroll
+                for (int u = 0; u < R; ++u) {
+                    a[q][u] = an[q][u];
+                    col[q][u] = cn[q][u];
+                }
+                e[q] += 32 * R;
             }
-            e = en;
         }
-        if (row >= 0) {
-            const size_t base = (size_t)row * NV;
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+            if (row[q] < 0) continue;
+            const size_t base = (size_t)row[q] * NV;
 #pragma unroll
             for (int c = 0; c < NV; ++c) {
-                const TY ac = (TY)acc[c];
+                const TY ac = (TY)acc[q][c];
                 if constexpr (MODE == MV_AX || MODE == MV_TWO) {
                     y[base + c] = ac;
                 } else if constexpr (MODE == MV_RES) {
@@ -258,7 +281,7 @@ k_sell_spmv(int slices, const int* __restrict__ off, const int* __restrict__ row
                 } else {
                     const TY r = b[base + c] - ac;
                     const TY xo = (TY)x[base + c];
-                    y[base + c] = RECIP ? xo + r * d[row] : xo + r / d[row];
+                    y[base + c] = RECIP ? xo + r * d[row[q]] : xo + r / d[row[q]];
                 }
             }
         }
@@ -949,7 +972,7 @@ struct DevCsr {
     }
     int unroll_for(int nv) const { return tuned[nv_slot(nv)] ? tuned_u[nv_slot(nv)] : 1; }
     bool sell_for(int nv) const { return sell.slices > 0 && tuned_sell[nv_slot(nv)] > 0; }
-    int tuned_sell[4] = {0, 0, 0, 0};  // steps per round of the sliced-ELL copy when it timed fastest (0 = CSR)
+    int tuned_sell[4] = {0, 0, 0, 0};  // launch shape of the sliced-ELL copy when it timed fastest (0 = CSR)
     DevBuf<int> rp, ci;
     DualVec v;
     DevSell sell;  // built for the fine-level FP64 matrices only (A_bc, G, G^T)
@@ -1036,6 +1059,10 @@ constexpr int kShapeL[] = {2, 4, 8, 16, 32, 4, 8, 16, 8, 16};
 constexpr int kShapeU[] = {1, 1, 1, 1, 1, 2, 2, 2, 4, 4};
 constexpr int kShapes = 10;
 constexpr int kUnrollMinRows = 65536;
+// sliced-ELL launch shapes: steps per round R (2, 4, 8), | kSellPair for two
+// slices per warp (R = 2, 4)
+constexpr int kSellPair = 16;
+constexpr int kSellShapes[] = {2, 4, 8, kSellPair | 2, kSellPair | 4};
 
 template <typename TV, typename TX, typename TY, int NV, int MODE, bool RECIP>
 static void launch_mv(int lanes, int u, int grid, cudaStream_t s, int n, const int* rp, const int* ci, const TV* v,
@@ -1064,13 +1091,17 @@ static int mv_grid(int n, int lanes, int u) {
 }
 
 template <typename TX, typename TY, int NV, int MODE, bool RECIP>
-static void launch_sell(const DevSell& S, int steps, cudaStream_t s, const TX* x, TY* y, const TY* b, const TY* d,
+static void launch_sell(const DevSell& S, int shape, cudaStream_t s, const TX* x, TY* y, const TY* b, const TY* d,
                         TY w, const KState* st) {
-    const int grid = std::max(1, (S.slices + kBlock / 32 - 1) / (kBlock / 32));
+    const int pairs = shape & kSellPair;  // two slices per warp
+    const int per_block = (kBlock / 32) * (pairs ? 2 : 1);
+    const int grid = std::max(1, (S.slices + per_block - 1) / per_block);
 #define SSV_SELL_ARGS grid, kBlock, s, S.slices, S.off.get(), S.rows.get(), S.ci.get(), S.v.get(), x, y, b, d, w, st, \
                       S.pat_n
-    if (steps == 2) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 2>, SSV_SELL_ARGS);
-    else if (steps == 4) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 4>, SSV_SELL_ARGS);
+    if (shape == (kSellPair | 2)) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 2, 2>, SSV_SELL_ARGS);
+    else if (shape == (kSellPair | 4)) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 4, 2>, SSV_SELL_ARGS);
+    else if (shape == 2) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 2>, SSV_SELL_ARGS);
+    else if (shape == 4) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 4>, SSV_SELL_ARGS);
     else launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 8>, SSV_SELL_ARGS);
 #undef SSV_SELL_ARGS
 }
@@ -1672,6 +1703,20 @@ static int sell_mode() {
     return v;
 }
 static bool sell_enabled() { return sell_mode() != 0; }
+// SSV_AMS_SELL_SHAPE=<shape> (one of kSellShapes): the tuner offers that
+// sliced-ELL launch shape alone
+static int sell_shape_forced() {
+    static int v = -1;
+    if (v < 0) {
+        v = 0;
+        if (const char* e = std::getenv("SSV_AMS_SELL_SHAPE")) {
+            const int k = std::atoi(e);
+            for (int c : kSellShapes)
+                if (c == k) v = k;
+        }
+    }
+    return v;
+}
 
 // largest rows-per-group the tuner may pick (SSV_AMS_MAX_UNROLL, default 4)
 static int max_unroll() {
@@ -1827,7 +1872,8 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
     int sell_pick = 0;
     if constexpr (std::is_same_v<TV, double>) {
         if (A.sell.slices > 0 && sell_enabled()) {
-            for (int R : {2, 4, 8}) {
+            for (int R : kSellShapes) {
+                if (sell_shape_forced() && R != sell_shape_forced()) continue;
                 auto launch = [&] {
                     if (two)
                         launch_sell<TX, TY, NV, MV_TWO, false>(A.sell, R, s, x, y, b, nullptr, TY(0), nullptr);
@@ -1861,7 +1907,8 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
         std::fprintf(stderr, "ams tune: n=%d nnz=%lld nv=%d %s -> lanes %d rows/group %d (%.2f us)", A.n,
                      (long long)A.nnz, NV, cold ? "cold" : "warm", pick, pick_u, 1e3 * best / (cold ? 5 : 4));
         if (sell_pick)
-            std::fprintf(stderr, "; sliced-ELL %d steps/round %.2f us%s", sell_pick, 1e3 * sell_best / (cold ? 5 : 4),
+            std::fprintf(stderr, "; sliced-ELL %d steps/round%s %.2f us%s", sell_pick & ~kSellPair,
+                         (sell_pick & kSellPair) ? " two slices/warp" : "", 1e3 * sell_best / (cold ? 5 : 4),
                          A.tuned_sell[slot] ? " -> sliced-ELL" : "");
         std::fprintf(stderr, "\n");
     }

@@ -5,7 +5,8 @@ same AMS applies and solves as the CSR shapes, in the FP64 and the FP32 form
 offers them on matrices of at least 65,536 rows; SSV_AMS_SELL=2 forces them
 on any size, so these small systems run them. The switch is read once per process: the cases
 run in a child process, whose tuner log shows the sliced-ELL kernel chosen
-for the fine matrix."""
+for the fine matrix. Every sliced-ELL launch shape gives bitwise the same
+results."""
 from __future__ import annotations
 
 import json
@@ -75,6 +76,62 @@ def sell_run():
     r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=900, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-3000:]
     return json.loads(r.stdout.strip().splitlines()[-1]), r.stderr
+
+
+SHAPES_CHILD = r"""
+import sys
+import numpy as np
+sys.path.insert(0, {root!r}); sys.path.insert(0, {pkg!r})
+import sparsesolv_ngsolve as ss
+from sparsesolv_ngsolve import hcurl as H
+rng = np.random.default_rng(5)
+out = {{}}
+d = H.magnetostatic(8)
+for prec in ("fp64", "fp32"):
+    p = ss.CompactAMSPreconditioner(d["A"], d["G"], freedofs=d["freedofs"], coord_x=d["coords"][0],
+                                    coord_y=d["coords"][1], coord_z=d["coords"][2], precision=prec)
+    out["mag_" + prec] = p * rng.standard_normal(d["A"].shape[0])
+inv = ss.PCGSolver(d["A"], p, freedofs=d["freedofs"], maxiter=500, tol=1e-10)
+x = np.zeros(d["A"].shape[0])
+inv.Solve(d["f"], x)
+out["mag_fp32_cg"] = x
+e = H.eddy_current(8)
+p = ss.ComplexCompactAMSPreconditioner(e["a_real"], e["G"], freedofs=e["freedofs"], coord_x=e["coords"][0],
+                                       coord_y=e["coords"][1], coord_z=e["coords"][2])
+n = e["A"].shape[0]
+out["eddy"] = p * (rng.standard_normal(n) + 1j * rng.standard_normal(n))
+np.savez(sys.argv[1], **out)
+"""
+
+
+def test_sell_shapes_bitwise_equal(tmp_path):
+    """Every sliced-ELL launch shape (2, 4 or 8 steps per round; two slices
+    per warp at 2 and 4 steps) sums each row in its CSR column order, so the
+    applies and a PCG solve are bitwise the same whichever shape runs. The
+    first child records the tuner's choices; the others replay them with every
+    sliced-ELL choice replaced by one shape."""
+    code = SHAPES_CHILD.format(root=ROOT, pkg=os.path.join(ROOT, "ngsolve-sparsesolv_b200"))
+    rec = tmp_path / "tune.txt"
+
+    def run(out, **extra):
+        env = dict(os.environ, SSV_AMS_SELL="2", **extra)
+        r = subprocess.run([sys.executable, "-c", code, str(out)], env=env, capture_output=True, text=True,
+                           timeout=600, cwd=ROOT)
+        assert r.returncode == 0, r.stderr[-3000:]
+        assert "replay stops" not in r.stderr, r.stderr[-2000:]
+        return np.load(out)
+
+    base = run(tmp_path / "base.npz", SSV_AMS_TUNE_SAVE=str(rec))
+    lines = rec.read_text().splitlines()
+    assert any(ln.startswith("csr") and ln.split()[6] != "0" for ln in lines), lines
+    for shape in (2, 8, 16 | 2, 16 | 4):
+        forced = tmp_path / f"tune_{shape}.txt"
+        forced.write_text("\n".join(
+            " ".join(f[:6] + [str(shape)]) if f[0] == "csr" and f[6] != "0" else " ".join(f)
+            for f in (ln.split() for ln in lines)) + "\n")
+        got = run(tmp_path / f"x_{shape}.npz", SSV_AMS_TUNE_LOAD=str(forced))
+        for k in base.files:
+            assert np.array_equal(got[k], base[k]), (shape, k, float(np.abs(got[k] - base[k]).max()))
 
 
 def test_sell_chosen_for_fine_matrix(sell_run):
