@@ -193,6 +193,28 @@ k_mv_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T
 // waves of slices runs in one. Each row is summed in its CSR column order for
 // every R and P. A slice's entry count is a multiple of 32, so the loop
 // conditions are warp-uniform.
+// the output of one row of a sliced-ELL product, by mode
+template <typename TX, typename TY, int NV, int MODE, bool RECIP, typename TA>
+__device__ __forceinline__ void sell_store(int row, const TA (&acc)[NV], const TX* __restrict__ x, TY* __restrict__ y,
+                                           const TY* __restrict__ b, const TY* __restrict__ d, TY w) {
+    const size_t base = (size_t)row * NV;
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+        const TY ac = (TY)acc[c];
+        if constexpr (MODE == MV_AX || MODE == MV_TWO) {
+            y[base + c] = ac;
+        } else if constexpr (MODE == MV_RES) {
+            y[base + c] = b[base + c] - ac;
+        } else if constexpr (MODE == MV_ADD) {
+            y[base + c] += w * ac;
+        } else {
+            const TY r = b[base + c] - ac;
+            const TY xo = (TY)x[base + c];
+            y[base + c] = RECIP ? xo + r * d[row] : xo + r / d[row];
+        }
+    }
+}
+
 template <typename TX, typename TY, int NV, int MODE, bool RECIP, int R, int P = 1>
 __global__ void __launch_bounds__(kBlock)
 k_sell_spmv(int slices, const int* __restrict__ off, const int* __restrict__ rows, const int* __restrict__ ci,
@@ -266,25 +288,88 @@ k_sell_spmv(int slices, const int* __restrict__ off, const int* __restrict__ row
             }
         }
 #pragma unroll
-        for (int q = 0; q < P; ++q) {
-            if (row[q] < 0) continue;
-            const size_t base = (size_t)row[q] * NV;
+        for (int q = 0; q < P; ++q)
+            if (row[q] >= 0) sell_store<TX, TY, NV, MODE, RECIP>(row[q], acc[q], x, y, b, d, w);
+    }
+}
+
+// Three-stage form of the one-slice product (NV <= 2): in each round the
+// values and columns of round j+2 are loaded and the x entries of round j+1
+// gathered before the products of round j are summed, so the gather no longer
+// waits behind the column load of its own round: a warp has one HBM round
+// trip per round on its critical path instead of two. Same summation order
+// as k_sell_spmv.
+template <typename TX, typename TY, int NV, int MODE, bool RECIP, int R>
+__global__ void __launch_bounds__(kBlock)
+k_sell_spmv_deep(int slices, const int* __restrict__ off, const int* __restrict__ rows, const int* __restrict__ ci,
+                 const double* __restrict__ v, const TX* __restrict__ x, TY* __restrict__ y, const TY* __restrict__ b,
+                 const TY* __restrict__ d, TY w, const KState* st, int n) {
+    using TA = wider_t<double, TX>;
+    pdl_gate();
+    if (st && st->done) return;
+    const int lane = threadIdx.x & 31;
+    const int wpb = kBlock / 32;
+    auto gather = [&](int c, TX (&o)[NV]) {
+        if constexpr (MODE == MV_TWO)  // columns past the row count read the b slot
+            load_row<NV>(c < n ? x + (size_t)c * NV : reinterpret_cast<const TX*>(b) + (size_t)(c - n) * NV, o);
+        else
+            load_row<NV>(x + (size_t)c * NV, o);
+    };
+    for (int sl = blockIdx.x * wpb + threadIdx.x / 32; sl < slices; sl += gridDim.x * wpb) {
+        const int e1 = off[sl + 1];
+        int e = off[sl] + lane;
+        const int row = rows[(size_t)sl * 32 + lane];
+        TA acc[NV];
 #pragma unroll
-            for (int c = 0; c < NV; ++c) {
-                const TY ac = (TY)acc[q][c];
-                if constexpr (MODE == MV_AX || MODE == MV_TWO) {
-                    y[base + c] = ac;
-                } else if constexpr (MODE == MV_RES) {
-                    y[base + c] = b[base + c] - ac;
-                } else if constexpr (MODE == MV_ADD) {
-                    y[base + c] += w * ac;
-                } else {
-                    const TY r = b[base + c] - ac;
-                    const TY xo = (TY)x[base + c];
-                    y[base + c] = RECIP ? xo + r * d[row[q]] : xo + r / d[row[q]];
-                }
-            }
+        for (int c = 0; c < NV; ++c) acc[c] = TA(0);
+        double a[R], an[R];
+        int cn[R];
+        bool on[R];
+        TX xv[R][NV];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {  // round 0: values, columns, gathers; round 1: values, columns
+            const int k = e + 32 * u;
+            a[u] = k < e1 ? v[k] : 0.0;
+            const int c0 = k < e1 ? ci[k] : -1;
+            on[u] = c0 >= 0;
+            if (on[u]) gather(c0, xv[u]);
+            const int k1 = k + 32 * R;
+            an[u] = k1 < e1 ? v[k1] : 0.0;
+            cn[u] = k1 < e1 ? ci[k1] : -1;
         }
+        while (e < e1) {
+            double a2[R];
+            int c2[R];
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                const int k = e + 64 * R + 32 * u;
+                a2[u] = k < e1 ? v[k] : 0.0;
+                c2[u] = k < e1 ? ci[k] : -1;
+            }
+            TX xn[R][NV];
+            bool onn[R];
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                onn[u] = cn[u] >= 0;
+                if (onn[u]) gather(cn[u], xn[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < R; ++u)
+                if (on[u])
+#pragma unroll
+                    for (int c = 0; c < NV; ++c) acc[c] += (TA)a[u] * (TA)xv[u][c];
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                a[u] = an[u];
+                on[u] = onn[u];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) xv[u][c] = xn[u][c];
+                an[u] = a2[u];
+                cn[u] = c2[u];
+            }
+            e += 32 * R;
+        }
+        if (row >= 0) sell_store<TX, TY, NV, MODE, RECIP>(row, acc, x, y, b, d, w);
     }
 }
 
@@ -1060,9 +1145,11 @@ constexpr int kShapeU[] = {1, 1, 1, 1, 1, 2, 2, 2, 4, 4};
 constexpr int kShapes = 10;
 constexpr int kUnrollMinRows = 65536;
 // sliced-ELL launch shapes: steps per round R (2, 4, 8), | kSellPair for two
-// slices per warp (R = 2, 4)
+// slices per warp (R = 2, 4), | kSellDeep for the three-stage form (R = 2, 4;
+// one or two columns)
 constexpr int kSellPair = 16;
-constexpr int kSellShapes[] = {2, 4, 8, kSellPair | 2, kSellPair | 4};
+constexpr int kSellDeep = 32;
+constexpr int kSellShapes[] = {2, 4, 8, kSellPair | 2, kSellPair | 4, kSellDeep | 2, kSellDeep | 4};
 
 template <typename TV, typename TX, typename TY, int NV, int MODE, bool RECIP>
 static void launch_mv(int lanes, int u, int grid, cudaStream_t s, int n, const int* rp, const int* ci, const TV* v,
@@ -1098,6 +1185,17 @@ static void launch_sell(const DevSell& S, int shape, cudaStream_t s, const TX* x
     const int grid = std::max(1, (S.slices + per_block - 1) / per_block);
 #define SSV_SELL_ARGS grid, kBlock, s, S.slices, S.off.get(), S.rows.get(), S.ci.get(), S.v.get(), x, y, b, d, w, st, \
                       S.pat_n
+    if constexpr (NV <= 2) {
+        if (shape == (kSellDeep | 2)) {
+            launch_k(k_sell_spmv_deep<TX, TY, NV, MODE, RECIP, 2>, SSV_SELL_ARGS);
+            return;
+        }
+        if (shape == (kSellDeep | 4)) {
+            launch_k(k_sell_spmv_deep<TX, TY, NV, MODE, RECIP, 4>, SSV_SELL_ARGS);
+            return;
+        }
+    }
+    shape &= ~kSellDeep;  // (the three-stage form is built for NV <= 2 only)
     if (shape == (kSellPair | 2)) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 2, 2>, SSV_SELL_ARGS);
     else if (shape == (kSellPair | 4)) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 4, 2>, SSV_SELL_ARGS);
     else if (shape == 2) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 2>, SSV_SELL_ARGS);
@@ -1874,6 +1972,7 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
         if (A.sell.slices > 0 && sell_enabled()) {
             for (int R : kSellShapes) {
                 if (sell_shape_forced() && R != sell_shape_forced()) continue;
+                if ((R & kSellDeep) && NV > 2) continue;
                 auto launch = [&] {
                     if (two)
                         launch_sell<TX, TY, NV, MV_TWO, false>(A.sell, R, s, x, y, b, nullptr, TY(0), nullptr);
@@ -1907,8 +2006,9 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
         std::fprintf(stderr, "ams tune: n=%d nnz=%lld nv=%d %s -> lanes %d rows/group %d (%.2f us)", A.n,
                      (long long)A.nnz, NV, cold ? "cold" : "warm", pick, pick_u, 1e3 * best / (cold ? 5 : 4));
         if (sell_pick)
-            std::fprintf(stderr, "; sliced-ELL %d steps/round%s %.2f us%s", sell_pick & ~kSellPair,
-                         (sell_pick & kSellPair) ? " two slices/warp" : "", 1e3 * sell_best / (cold ? 5 : 4),
+            std::fprintf(stderr, "; sliced-ELL %d steps/round%s %.2f us%s", sell_pick & 15,
+                         (sell_pick & kSellPair) ? " two slices/warp" : (sell_pick & kSellDeep) ? " three-stage" : "",
+                         1e3 * sell_best / (cold ? 5 : 4),
                          A.tuned_sell[slot] ? " -> sliced-ELL" : "");
         std::fprintf(stderr, "\n");
     }

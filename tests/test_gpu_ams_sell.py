@@ -106,7 +106,8 @@ np.savez(sys.argv[1], **out)
 
 def test_sell_shapes_bitwise_equal(tmp_path):
     """Every sliced-ELL launch shape (2, 4 or 8 steps per round; two slices
-    per warp at 2 and 4 steps) sums each row in its CSR column order, so the
+    per warp, or the three-stage form, at 2 and 4 steps) sums each row in its
+    CSR column order, so the
     applies and a PCG solve are bitwise the same whichever shape runs. The
     first child records the tuner's choices; the others replay them with every
     sliced-ELL choice replaced by one shape."""
@@ -124,7 +125,7 @@ def test_sell_shapes_bitwise_equal(tmp_path):
     base = run(tmp_path / "base.npz", SSV_AMS_TUNE_SAVE=str(rec))
     lines = rec.read_text().splitlines()
     assert any(ln.startswith("csr") and ln.split()[6] != "0" for ln in lines), lines
-    for shape in (2, 8, 16 | 2, 16 | 4):
+    for shape in (2, 8, 16 | 2, 16 | 4, 32 | 2, 32 | 4):
         forced = tmp_path / f"tune_{shape}.txt"
         forced.write_text("\n".join(
             " ".join(f[:6] + [str(shape)]) if f[0] == "csr" and f[6] != "0" else " ".join(f)
