@@ -7,7 +7,7 @@
 // sorted), CreateTranspose, Mult/MultAdd (row loops), SPARSECHOLESKY (an exact
 // dense Cholesky solve of the small coarsest matrix). Agreement with NGSolve
 // itself cannot be checked in this image ("parity unpinned" for the AMS part).
-// Serial; used only by tests/ and bench.py's CPU-baseline leg as the checker.
+// Serial test infrastructure: used only by tests/ and bench.py's CPU-baseline leg, to check results.
 #include <algorithm>
 #include <cmath>
 #include <complex>

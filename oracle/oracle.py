@@ -3,7 +3,7 @@
 Loads ``oracle/_build/libssv_oracle.so`` (the C restatement, rebuilt with gcc
 when missing) and, where present, ``oracle/_ref/libssv_ref.so`` (the
 reference's own headers). Only tests/, the smoke check and bench.py's CPU
-baseline use this module, as the checker.
+baseline use this module, to check results (test infrastructure).
 """
 from __future__ import annotations
 

@@ -6,7 +6,7 @@
  * NGSolve COCRSolver loop), each routine citing the reference file:line it
  * follows (paths relative to the reference's include/sparsesolv/ unless
  * stated). Only tests/, the smoke check and bench.py's CPU-baseline leg load
- * it, as the checker; the product never links or calls it.
+ * it, to check results (test infrastructure); the product never links or calls it.
  *
  * Pinned against the reference itself: oracle/ref_driver.cpp compiles the
  * reference's own headers into oracle/_ref/libssv_ref.so, and

@@ -1,6 +1,6 @@
 """The fused V-cycle level products (R = P^T (I - A D^-1) for the down sweep,
 U = [D^-1 (2I - A D^-1) | (I - D^-1 A) P] for the up sweep) are built on the
-host; this CPU test compiles the host set-up source with a small checker
+host; this CPU test compiles the host set-up source with a small test driver
 (tests/host/fused_level_check.cpp) and compares both products with the
 step-by-step level (first sweep, residual, restriction; prolongation, post
 sweep) on random sparse levels, to 1e-13."""
