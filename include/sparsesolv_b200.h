@@ -14,7 +14,7 @@
  * of the last failure on the calling thread is ssv_last_error(). The Python
  * layer maps SSV_ERR_RUNTIME -> RuntimeError (reference std::runtime_error),
  * SSV_ERR_INVALID_ARG -> ValueError (std::invalid_argument), SSV_ERR_TYPE ->
- * TypeError (py::type_error).
+ * TypeError (py::type_error), SSV_ERR_ALLOC -> MemoryError (std::bad_alloc).
  *
  * Scalars: SSV_F64 = double, SSV_C128 = complex<double> stored as interleaved
  * (re, im) doubles, exactly the layout of std::complex<double>.
@@ -139,6 +139,13 @@ const char* ssv_last_error(void);
  * max_loops > 0 sets that cap for every later solve of the process; 0
  * restores the default. */
 void ssv_set_loop_guard(int32_t max_loops);
+/* Device-allocation budget (new: no reference counterpart; a test hook for
+ * the allocation-failure paths). bytes >= 0: every later device allocation of
+ * the library is charged against the remaining budget, and one that does not
+ * fit fails with SSV_ERR_ALLOC before any CUDA allocation is tried, the call
+ * returning that code with its objects left as they were before it; bytes < 0
+ * removes the limit (the default). Process-wide. */
+void ssv_set_alloc_budget(int64_t bytes);
 /* Number of CUDA devices and the name of device 0 (no allocation). */
 int ssv_device_info(int* count, char* name, int name_cap);
 /* Reference defaults of SolverConfig (solver_config.hpp:39-157). */

@@ -473,20 +473,24 @@ __global__ void k_pmis_finish(int n, int* __restrict__ cf, int* __restrict__ isc
 const double* pmis_random(int n, cudaStream_t s) {
     // shared by concurrent set-ups: a grown table never frees the one that kernels
     // on other streams may still read, and it is allocated outside any
-    // stream-ordered scope
+    // stream-ordered scope; the table is replaced only once its successor is
+    // on the device (a failed allocation leaves the previous one in place)
+    if (n <= 0) return nullptr;
     static std::mutex mu;
-    static std::vector<double> host;
+    static int have = 0;
     static std::vector<DevBuf<double>> dev;
     std::lock_guard<std::mutex> lk(mu);
-    if ((int)host.size() < n) {
-        host.resize(n);
+    if (have < n) {
+        std::vector<double> host(n);
         std::mt19937 rng(42);
         std::uniform_real_distribution<double> dist(0.0, 1.0);
         for (int i = 0; i < n; ++i) host[i] = dist(rng);
         AllocScope plain(nullptr);
-        dev.emplace_back();
-        dev.back().upload(host.data(), host.size(), s);
+        DevBuf<double> next;
+        next.upload(host.data(), host.size(), s);
         SSV_CUDA(cudaStreamSynchronize(s));
+        dev.push_back(std::move(next));
+        have = n;
     }
     return dev.back().get();
 }
@@ -900,7 +904,7 @@ bool d_fused_level(const DCsr& A, const DCsr& P, const DCsr& Pt, const double* d
 }
 
 bool d_amg_setup(const DCsr& A0, double theta, int max_levels, int min_coarse, std::vector<DAmgLevel>& out,
-                 cudaStream_t s, std::thread* coarse) {
+                 cudaStream_t s, WorkerThread* coarse) {
     SetupLog log(s);
     out.clear();
     out.emplace_back();
@@ -990,7 +994,7 @@ bool d_amg_setup(const DCsr& A0, double theta, int max_levels, int min_coarse, s
     if (co.A.n <= min_coarse * 10) {
         co.direct = true;
         if (coarse) {  // the level object stays where it is: out is not resized again
-            *coarse = std::thread([&co, H = co.A.to_host(s)] {
+            coarse->start([&co, H = co.A.to_host(s)] {
                 co.piv_min = dense_ldlt_pseudo(H, co.linv, co.linvt, co.piv);
             });
         } else {

@@ -9,10 +9,10 @@
 #pragma once
 
 #include <cstdint>
-#include <thread>
 #include <vector>
 
 #include "amg_setup.hpp"
+#include "host_threads.hpp"
 #include "ssv_common.cuh"
 
 namespace ssv {
@@ -65,7 +65,7 @@ void d_fine_l1(const DCsr& A, DevBuf<double>& out, cudaStream_t s);
 // `coarse` is given, on a host thread stored there (the caller joins it
 // before the factors are read), so it overlaps the device work that follows.
 bool d_amg_setup(const DCsr& A0, double theta, int max_levels, int min_coarse, std::vector<DAmgLevel>& out,
-                 cudaStream_t s, std::thread* coarse = nullptr);
+                 cudaStream_t s, WorkerThread* coarse = nullptr);
 // fused_level (amg_setup.hpp) on the device: R = P^T (I - A D^{-1}),
 // U = [D^{-1}(2I - A D^{-1}) | (I - D^{-1} A) P]
 bool d_fused_level(const DCsr& A, const DCsr& P, const DCsr& Pt, const double* d, DCsr& R, DCsr& U,

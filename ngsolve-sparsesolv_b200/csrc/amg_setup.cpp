@@ -5,6 +5,7 @@
 // direct interpolation with lumping of the non-interpolatory connections and
 // the injection fall-back, Galerkin P^T A P, plain l1 row norms.
 #include "amg_setup.hpp"
+#include "host_threads.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -388,9 +389,7 @@ double dense_ldlt_pseudo(const HostCsr& A, std::vector<double>& linv, std::vecto
     if (n < 256 || nt == 1) {
         columns(0, n);
     } else {
-        std::vector<std::thread> th;
-        for (int t = 0; t < nt; ++t) th.emplace_back(columns, n * t / nt, n * (t + 1) / nt);
-        for (auto& x : th) x.join();
+        run_threads(nt, [&](int t) { columns(n * t / nt, n * (t + 1) / nt); });
     }
     return kept_min;
 }
@@ -473,9 +472,7 @@ void AmsHost::rebuild(const HostCsr& A, const uint8_t* fd) {
         amg[s].num_smooth = 1;
         amg[s].setup(M);
     };
-    std::vector<std::thread> th;
-    for (int s = 0; s < 4; ++s) th.emplace_back(galerkin, s);
-    for (auto& t : th) t.join();
+    run_threads(4, galerkin);
     // truncated l1 of the fine smoother (:395-413)
     fine_l1.resize(nhc);
     for (int i = 0; i < nhc; ++i) {

@@ -990,15 +990,29 @@ struct DevSell : SellPattern {
     // the layout built on the device from a device CSR (a_rp, a_ci, a_v)
     void build_dev(int n, int64_t nnz, const int* a_rp, const int* a_ci, const double* a_v, cudaStream_t s) {
         if (!build_pattern(n, nnz, a_rp, a_ci, s)) return;
-        v.alloc((size_t)std::max<int64_t>(entries, 1));
-        sell_gather(*this, a_v, 1, v.get(), s);
-        SSV_CUDA(cudaStreamSynchronize(s));
+        try {
+            v.alloc((size_t)std::max<int64_t>(entries, 1));
+            sell_gather(*this, a_v, 1, v.get(), s);
+            SSV_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            invalidate();  // a layout without its values is no layout
+            throw;
+        }
     }
     void build(const HostCsr& A, cudaStream_t s) {
-        pat_n = A.n;
-        pat_nnz = A.nnz();
+        invalidate();
+        try {
+            build_host(A, s);
+        } catch (...) {
+            invalidate();
+            throw;
+        }
+    }
+
+private:
+    void build_host(const HostCsr& A, cudaStream_t s) {
         const int n = A.n;
-        slices = (n + 31) / 32;
+        int slices = (n + 31) / 32;  // the members are set once everything is on the device
         std::vector<int> order(n);
         for (int i = 0; i < n; ++i) order[i] = i;
         auto len = [&](int r) { return A.rp[r + 1] - A.rp[r]; };
@@ -1014,14 +1028,10 @@ struct DevSell : SellPattern {
                 h_rows[(size_t)sl * 32 + t] = r;
                 wmax = std::max(wmax, len(r));
             }
-            if ((int64_t)h_off[sl] + 32 * (int64_t)wmax > (int64_t)INT32_MAX - 4096) {  // int offsets: no copy
-                slices = 0;
-                entries = 0;
-                return;
-            }
+            if ((int64_t)h_off[sl] + 32 * (int64_t)wmax > (int64_t)INT32_MAX - 4096) return;  // int offsets: no copy
             h_off[sl + 1] = h_off[sl] + 32 * wmax;
         }
-        entries = h_off[slices];
+        const int64_t entries = h_off[slices];
         std::vector<int> h_ci((size_t)entries, -1), h_src((size_t)entries, -1);
         std::vector<double> h_v((size_t)entries, 0.0);
         for (int sl = 0; sl < slices; ++sl)
@@ -1041,6 +1051,10 @@ struct DevSell : SellPattern {
         src.upload(h_src.data(), h_src.size(), s);
         v.upload(h_v.data(), h_v.size(), s);
         SSV_CUDA(cudaStreamSynchronize(s));  // pageable sources
+        this->slices = slices;
+        this->entries = entries;
+        pat_n = A.n;
+        pat_nnz = A.nnz();
     }
 };
 
@@ -1611,8 +1625,23 @@ static void pi_prolong(const AmsState& a, const T* gx, const T* gy, const T* gz,
 // One AMS cycle (CompactAMS::Mult, compact_ams.hpp:136-195, or the fused
 // ComplexCompactAMS::Mult, complex_compact_ams.hpp:112-154): in -> out, both
 // FP64 with NV columns.
+static void ams_reserve(AmsState& a, int nv);
+
+// The work vectors of NV columns before a cycle: missing only after an
+// allocation that failed; outside a capture they are allocated again here,
+// inside one the cycle refuses to run (no kernel may see a released buffer).
+static void ams_need_columns(AmsState& a, int nv, cudaStream_t s) {
+    if (nv <= a.nv_alloc) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    SSV_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+        fail(SSV_ERR_RUNTIME, "AMS cycle: work vectors missing after a failed allocation (call Update())");
+    ams_reserve(a, nv);
+}
+
 template <typename TG, typename TN, int NV, bool RECIP>
 static void ams_cycle(AmsState& a, const double* in, double* out, const KState* st, cudaStream_t s) {
+    ams_need_columns(a, NV, s);
     const int n = a.nhc;
     const uint8_t* fd = a.has_fd ? a.fd.get() : nullptr;
     const double* d = RECIP ? a.fine_il1.get() : a.fine_l1.get();
@@ -1729,10 +1758,15 @@ static void l2_flush(cudaStream_t s) {
         const char* e = std::getenv("SSV_PROFILE_FLUSH");
         return e && std::strcmp(e, "write") == 0;
     }();
+    static bool zeroed = false;  // each step is retried by the next call after a failure
+    if (!sink.get()) sink.alloc(1);
     if (!buf.get()) {
+        zeroed = false;
         buf.alloc((size_t)256 << 20);
-        sink.alloc(1);
+    }
+    if (!zeroed) {
         buf.zero(s);
+        zeroed = true;
     }
     if (write_form) {
         SSV_CUDA(cudaMemsetAsync(buf.get(), 0, buf.size(), s));
@@ -2145,21 +2179,29 @@ static void tune_lanes(AmsState& a) {
 // cycle itself never allocates and can be captured).
 static void ams_reserve(AmsState& a, int nv) {
     if (nv <= a.nv_alloc) return;
-    for (int s = 0; s < 4; ++s)
-        for (auto& lv : a.amg[s]) {
-            const size_t m = (size_t)lv.A.n * nv;
-            lv.b.alloc(m);
-            lv.xa.alloc(m);
-            lv.xb.alloc(m);
-            lv.r.alloc(m);
-            if (lv.direct) lv.cz.alloc(m);
-        }
-    const size_t mh = (size_t)a.nhc * nv, m1 = (size_t)a.nh1 * nv;
-    a.b0.alloc(mh);
-    a.xa.alloc(mh);
-    a.xb.alloc(mh);
-    a.r.alloc(mh);
-    for (int s = 0; s < 4; ++s) a.rs[s].alloc(m1);
+    try {
+        for (int s = 0; s < 4; ++s)
+            for (auto& lv : a.amg[s]) {
+                const size_t m = (size_t)lv.A.n * nv;
+                lv.b.alloc(m);
+                lv.xa.alloc(m);
+                lv.xb.alloc(m);
+                lv.r.alloc(m);
+                if (lv.direct) lv.cz.alloc(m);
+            }
+        const size_t mh = (size_t)a.nhc * nv, m1 = (size_t)a.nh1 * nv;
+        a.b0.alloc(mh);
+        a.xa.alloc(mh);
+        a.xb.alloc(mh);
+        a.r.alloc(mh);
+        for (int s = 0; s < 4; ++s) a.rs[s].alloc(m1);
+    } catch (...) {
+        // some buffers were released and not replaced: no column count is
+        // usable until a later reserve succeeds
+        a.nv_alloc = 0;
+        ++a.gen;
+        throw;
+    }
     a.nv_alloc = nv;
     ++a.gen;  // new work buffers: graphs that captured the old ones must be rebuilt
     const double t0 = wall_seconds();
@@ -2362,10 +2404,8 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
     std::vector<FusedLevel> fused[4];
     const double tf0 = wall_seconds();
     if (fused_enabled()) {
-        std::vector<std::thread> th;
-        for (int sub = 0; sub < 4; ++sub) {
-            if (sub_lo(a, sub) && sub == 0) continue;  // FP32 gradient hierarchies keep the four passes
-            th.emplace_back([&a, &fused, sub] {
+        run_threads(4, [&a, &fused](int sub) {
+                if (sub_lo(a, sub) && sub == 0) return;  // FP32 gradient hierarchies keep the four passes
                 const bool lo = sub_lo(a, sub);
                 const auto& hl = a.host.amg[sub].levels;
                 fused[sub].resize(hl.empty() ? 0 : hl.size() - 1);
@@ -2386,9 +2426,7 @@ static void ams_upload_matrix(AmsState& a, cudaStream_t s) {
                         fused_level(scaled_csr(hl[l].A, &isc[l], &isc[l]), scaled_csr(hl[l].P, &sc[l], &isc[l + 1]),
                                     scaled_csr(hl[l].Pt, &isc[l + 1], &sc[l]), l1s);
                 }
-            });
-        }
-        for (auto& t : th) t.join();
+        });
     }
     a.t_fused = wall_seconds() - tf0;
     for (int sub = 0; sub < 4; ++sub) {
@@ -2591,11 +2629,10 @@ static bool ams_device_setup(AmsState& a, const ssv_matrix* A, cudaStream_t s) {
                 Abc, s);
     log.mark("BC matrix");
     std::vector<DAmgLevel> amg[4];
-    std::thread coarse[4];  // the coarsest factorisations, on host threads while the device goes on
+    WorkerThread coarse[4];  // the coarsest factorisations, on host threads while the device goes on
     bool ok[4] = {true, true, true, true};
-    auto join = [&] {
-        for (auto& t : coarse)
-            if (t.joinable()) t.join();
+    auto wait = [&] {
+        for (auto& t : coarse) t.wait();
     };
     try {
         for_subspaces(s, [&](int sub, cudaStream_t ss) {
@@ -2613,10 +2650,10 @@ static bool ams_device_setup(AmsState& a, const ssv_matrix* A, cudaStream_t s) {
             slog.mark("subspace %d hierarchy (%zu levels)", sub, amg[sub].size());
         });
     } catch (...) {
-        join();
+        wait();
         throw;
     }
-    join();
+    for (auto& t : coarse) t.join();  // rethrows a factorisation's exception
     log.mark("subspace hierarchies and coarsest factorisations");
     for (bool o : ok)
         if (!o) return false;

@@ -85,6 +85,8 @@ const char* ssv_last_error(void) { return g_last_error.c_str(); }
 
 void ssv_set_loop_guard(int32_t max_loops) { ssv::set_loop_guard(max_loops); }
 
+void ssv_set_alloc_budget(int64_t bytes) { ssv::alloc_budget().store(bytes < 0 ? -1 : (long long)bytes); }
+
 int ssv_device_info(int* count, char* name, int name_cap) {
     return guarded([&] {
         int c = 0;
@@ -447,7 +449,9 @@ int ssv_ams_update(ssv_precond* p, ssv_matrix* new_A) {
             if (new_A->dtype != SSV_F64) ssv::fail(SSV_ERR_TYPE, "CompactAMS::Update: expected a real matrix");
             p->A = new_A;
         }
+        p->ready = false;  // an update that fails part way leaves nothing to apply until one succeeds
         ssv::ams_update(p->ams.get(), p->A);
+        p->ready = true;
     });
 }
 
@@ -698,8 +702,10 @@ int ssv_ic_set_config(ssv_precond* p, const ssv_config* cfg) {
 int ssv_precond_update(ssv_precond* p) {
     return guarded([&] {
         if (!p) ssv::fail(SSV_ERR_INVALID_ARG, "ssv_precond_update: NULL preconditioner");
+        p->ready = false;  // an update that fails part way leaves nothing to apply until one succeeds
         if (p->ams) ssv::ams_update(p->ams.get(), p->A);
         else ssv::precond_update(p);
+        p->ready = true;
     });
 }
 

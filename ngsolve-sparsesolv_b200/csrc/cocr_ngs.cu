@@ -153,10 +153,19 @@ static bool krylov_sell_enabled() {
 // outside any capture.
 static const double* krylov_sell(ssv_matrix* A, cudaStream_t s) {
     if (!krylov_sell_enabled() || A->rows < 65536) return nullptr;
-    if (!A->sell_tried) {
+    if (!A->sell_tried) {  // marked tried only once the layout and its value array exist
+        if (!A->sell.build_pattern(A->rows, A->nnz, A->rp.get(), A->ci.get(), s)) {
+            A->sell_tried = true;
+            return nullptr;
+        }
+        try {
+            A->sell_v.alloc((size_t)std::max<int64_t>(A->sell.entries, 1) * (A->dtype == SSV_F64 ? 1 : 2));
+        } catch (...) {
+            A->sell.invalidate();
+            throw;
+        }
+        A->sell_vgen = ~A->vgen;  // gather below
         A->sell_tried = true;
-        if (!A->sell.build_pattern(A->rows, A->nnz, A->rp.get(), A->ci.get(), s)) return nullptr;
-        A->sell_v.alloc((size_t)std::max<int64_t>(A->sell.entries, 1) * (A->dtype == SSV_F64 ? 1 : 2));
     }
     if (A->sell.slices <= 0) return nullptr;
     if (A->sell_vgen != A->vgen) {

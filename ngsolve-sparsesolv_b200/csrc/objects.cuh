@@ -125,12 +125,20 @@ struct GraphLoop {
 
 bool graph_while_mode();
 
+// Ends a capture that a thrown exception interrupted (the stream leaves
+// capture mode; the partial graph is dropped).
+inline void abandon_capture(cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+        cudaGraph_t partial = nullptr;
+        cudaStreamEndCapture(s, &partial);
+        if (partial) cudaGraphDestroy(partial);
+    }
+    cudaGetLastError();
+}
+
 template <typename F>
-void build_graph_loop(GraphLoop& g, const std::string& key_in, F&& body) {
-    const std::string key = key_in + (graph_while_mode() ? "|while" : "|chunk");
-    if (g.exec && g.key == key) return;
-    g.reset();
-    cudaStream_t s = stream();
+void build_graph_loop_body(GraphLoop& g, cudaStream_t s, F& body) {
     if (graph_while_mode()) {
         SSV_CUDA(cudaGraphCreate(&g.graph, 0));
         cudaGraphConditionalHandle h;
@@ -159,8 +167,24 @@ void build_graph_loop(GraphLoop& g, const std::string& key_in, F&& body) {
         SSV_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
         g.cond = false;
     }
+}
+
+template <typename F>
+void build_graph_loop(GraphLoop& g, const std::string& key_in, F&& body) {
+    const std::string key = key_in + (graph_while_mode() ? "|while" : "|chunk");
+    if (g.exec && g.key == key) return;
+    g.reset();
+    cudaStream_t s = stream();
+    try {
+        build_graph_loop_body(g, s, body);
+    } catch (...) {  // a failure inside the body (an allocation, a refused argument)
+        abandon_capture(s);
+        g.reset();
+        throw;
+    }
     g.key = key;
 }
+
 
 // Runs the loop until the device state reports done (bounded).
 void run_graph_loop(GraphLoop& g, KState* d_st, int max_iters);

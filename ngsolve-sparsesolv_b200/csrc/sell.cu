@@ -66,34 +66,32 @@ __global__ void k_sell_gather(int64_t entries, const int* __restrict__ src, cons
 }  // namespace
 
 bool SellPattern::build_pattern(int n, int64_t nnz, const int* rp, const int* a_ci, cudaStream_t s) {
-    pat_n = n;
-    pat_nnz = nnz;
-    slices = (n + 31) / 32;
-    DevBuf<int> order(std::max(n, 1)), width(std::max(slices, 1));
-    off.alloc(slices + 1);
-    rows.alloc((size_t)std::max(slices, 1) * 32);
+    invalidate();  // until every array below is in place
+    const int nsl = (n + 31) / 32;
+    DevBuf<int> order(std::max(n, 1)), width(std::max(nsl, 1));
+    off.alloc(nsl + 1);
+    rows.alloc((size_t)std::max(nsl, 1) * 32);
     if (n) {
         k_sell_order<<<(n + kSellWindow - 1) / kSellWindow, kSellWindow, 0, s>>>(n, rp, order.get());
-        k_sell_width<<<grid_for(slices, 128), 128, 0, s>>>(n, slices, rp, order.get(), rows.get(), width.get());
+        k_sell_width<<<grid_for(nsl, 128), 128, 0, s>>>(n, nsl, rp, order.get(), rows.get(), width.get());
         SSV_LAUNCH_CHECK();
     }
-    const int total = sell_offsets(slices, width.get(), off.get(), s);
-    if (total < 0) {  // int offsets would overflow: no copy
-        slices = 0;
-        entries = 0;
-        return false;
-    }
-    entries = total;
-    const size_t cap = (size_t)std::max<int64_t>(entries, 1);
+    const int total = sell_offsets(nsl, width.get(), off.get(), s);
+    if (total < 0) return false;  // int offsets would overflow: no copy
+    const size_t cap = (size_t)std::max(total, 1);
     ci.alloc(cap);
     src.alloc(cap);
     SSV_CUDA(cudaMemsetAsync(ci.get(), 0xff, sizeof(int) * cap, s));  // -1: padding
     SSV_CUDA(cudaMemsetAsync(src.get(), 0xff, sizeof(int) * cap, s));
-    if (slices)
-        k_sell_fill<<<grid_for((int64_t)slices * 32, 256), 256, 0, s>>>(slices, rp, a_ci, rows.get(), off.get(),
-                                                                         ci.get(), src.get());
+    if (nsl)
+        k_sell_fill<<<grid_for((int64_t)nsl * 32, 256), 256, 0, s>>>(nsl, rp, a_ci, rows.get(), off.get(), ci.get(),
+                                                                     src.get());
     SSV_LAUNCH_CHECK();
     SSV_CUDA(cudaStreamSynchronize(s));  // the temporaries go out of scope
+    slices = nsl;
+    entries = total;
+    pat_n = n;
+    pat_nnz = nnz;
     return true;
 }
 

@@ -32,6 +32,14 @@ struct SellPattern {
     // copy: slices = 0) when the padded size exceeds the int range
     bool build_pattern(int n, int64_t nnz, const int* rp, const int* ci, cudaStream_t s);
     bool same_pattern(int n, int64_t nnz) const { return slices > 0 && pat_n == n && pat_nnz == nnz; }
+    // no usable layout (set before a build, so that one that fails part way,
+    // on an allocation, is never taken for a finished one)
+    void invalidate() {
+        slices = 0;
+        entries = 0;
+        pat_n = -1;
+        pat_nnz = -1;
+    }
 };
 
 // v[e] = csr_v[src[e]] for `words` doubles per entry (2 for complex), 0 on padding

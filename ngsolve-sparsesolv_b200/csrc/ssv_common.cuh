@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -140,6 +141,25 @@ struct AllocScope {
     AllocScope& operator=(const AllocScope&) = delete;
 };
 
+// Device-allocation budget (the test hook ssv_set_alloc_budget): negative =
+// no limit; otherwise every device allocation is charged against it, and one
+// that does not fit fails with SSV_ERR_ALLOC before cudaMalloc is called, so
+// the failure paths of set-up and solves run without exhausting the GPU.
+inline std::atomic<long long>& alloc_budget() {
+    static std::atomic<long long> b{-1};
+    return b;
+}
+inline void charge_alloc(size_t bytes) {
+    std::atomic<long long>& b = alloc_budget();
+    long long cur = b.load(std::memory_order_relaxed);
+    while (cur >= 0) {
+        if ((long long)bytes > cur)
+            fail(SSV_ERR_ALLOC, "device allocation of " + std::to_string(bytes) +
+                                    " bytes refused: over the allocation budget (ssv_set_alloc_budget)");
+        if (b.compare_exchange_weak(cur, cur - (long long)bytes, std::memory_order_relaxed)) return;
+    }
+}
+
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
@@ -162,14 +182,17 @@ struct DevBuf {
     void alloc(size_t count) {
         if (count == n && p) return;
         release();
-        n = count;
         if (!count) return;
+        charge_alloc(sizeof(T) * count);
+        T* q = nullptr;
         if (cudaStream_t as = alloc_stream()) {
-            SSV_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p), sizeof(T) * count, as));
+            SSV_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&q), sizeof(T) * count, as));
             pooled = true;
         } else {
-            SSV_CUDA(cudaMalloc(&p, sizeof(T) * count));
+            SSV_CUDA(cudaMalloc(&q, sizeof(T) * count));
         }
+        p = q;
+        n = count;  // only once the memory is there: a failed alloc leaves an empty buffer
     }
     void release() {
         if (p) {

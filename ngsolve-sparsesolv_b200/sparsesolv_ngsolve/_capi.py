@@ -208,6 +208,7 @@ SIGNATURES = [
     ("ssv_cocr_refined_solve_dev", I32, [P, P, PU8, I32, ctypes.c_double, ctypes.c_double, I32, P, P,
                                          ctypes.POINTER(ssv_refine_info)]),
     ("ssv_set_loop_guard", None, [I32]),
+    ("ssv_set_alloc_budget", None, [ctypes.c_int64]),
     ("ssv_cocr_last_launches", I32, [ctypes.POINTER(ctypes.c_int64)]),
     ("ssv_gmres_solve", I32, [P, P, PU8, I32, ctypes.c_double, I32, P, P, PI32]),
     ("ssv_gmres_solve_dev", I32, [P, P, PU8, I32, ctypes.c_double, I32, P, P, PI32]),
@@ -278,6 +279,8 @@ def check(rc: int):
         raise ValueError(msg)
     if rc == SSV_ERR_TYPE:
         raise TypeError(msg)
+    if rc == SSV_ERR_ALLOC:  # pybind11's translation of std::bad_alloc
+        raise MemoryError(msg)
     raise RuntimeError(msg or f"sparsesolv_b200 error {rc}")
 
 
