@@ -22,7 +22,6 @@
 // has no gradient-space content left and the gradient correction diverges.
 // Kernels that cross between the two accumulate in FP64. The cycle's input
 // and output are FP64 in both forms.
-#include <cooperative_groups.h>
 
 #include <algorithm>
 #include <array>
