@@ -253,7 +253,7 @@ def run_ncu_case(args):
         # the 40^3 eddy family (8 frequencies x 4 sources) in one batched COCR solve, FP64
         # preconditioners; one warm solve (tuners, graph), then the profiled one in "solve"
         from sparsesolv_ngsolve import hcurl as H
-        d = H.eddy_family(40, nrhs=4)
+        d = H.eddy_family(args.family_nc, nrhs=4)
         pres = [ss.ComplexCompactAMSPreconditioner(a, d["G"], freedofs=d["freedofs"], coord_x=d["coords"][0],
                                                    coord_y=d["coords"][1], coord_z=d["coords"][2])
                 for a in d["a_real"]]
@@ -267,7 +267,8 @@ def run_ncu_case(args):
         bs.solve_dev(d_B.data_ptr(), d_X.data_ptr())
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
-        print(json.dumps({"ncu_case": args.workload, "systems": int(d["B"].shape[0] * d["B"].shape[1]),
+        print(json.dumps({"ncu_case": args.workload, "mesh": f"{args.family_nc}^3",
+                          "systems": int(d["B"].shape[0] * d["B"].shape[1]),
                           "max_iterations": int(bs.iterations.max())}))
         return
     if args.workload == "ams40":
@@ -993,6 +994,8 @@ def main():
     ap.add_argument("--eddy-nc", type=int, default=64,
                     help="mesh size of the eddy64 --ncu-case (a smaller mesh for multi-pass ncu sections)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--family-nc", type=int, default=40, help="mesh of the batched40 --ncu-case (smaller for "
+                                                                    "multi-pass captures)")
     ap.add_argument("--ncu-case", action="store_true",
                     help="run exactly one solve of the workload and exit (for ncu captures)")
     args = ap.parse_args()

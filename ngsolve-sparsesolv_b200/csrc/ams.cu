@@ -292,6 +292,100 @@ k_sell_spmv(int slices, const int* __restrict__ off, const int* __restrict__ row
     }
 }
 
+// Column-split form for block vectors (NV = 4 or 8): NV / 2 lanes share a
+// row and each sums two of its columns, so a warp covers 32 / (NV / 2) rows of
+// its slice per pass and walks the slice in NV / 2 passes. The x rows of a
+// step are then gathered as 64- or 32-byte pieces of few rows instead of 32
+// whole rows (a fourth of the L1 wavefronts at NV = 8, where the lane-per-row
+// form is bound by the L1/TEX pipeline); the slice's values and columns are
+// still read once. Each column is summed in its CSR column order, as in
+// k_sell_spmv.
+template <typename TX, typename TY, int NV, int MODE, bool RECIP, int R>
+__global__ void __launch_bounds__(kBlock)
+k_sell_spmv_cs(int slices, const int* __restrict__ off, const int* __restrict__ rows, const int* __restrict__ ci,
+               const double* __restrict__ v, const TX* __restrict__ x, TY* __restrict__ y, const TY* __restrict__ b,
+               const TY* __restrict__ d, TY w, const KState* st, int n) {
+    static_assert(NV == 4 || NV == 8, "column-split form: 4 or 8 columns");
+    constexpr int CS = 2;       // columns per lane
+    constexpr int G = NV / CS;  // lanes per row
+    constexpr int RP = 32 / G;  // rows per pass
+    using TA = wider_t<double, TX>;
+    pdl_gate();
+    if (st && st->done) return;
+    const int lane = threadIdx.x & 31;
+    const int cg = lane % G, rl = lane / G;
+    const int wpb = kBlock / 32;
+    for (int sl = blockIdx.x * wpb + threadIdx.x / 32; sl < slices; sl += gridDim.x * wpb) {
+        const int o0 = off[sl], e1 = off[sl + 1];
+#pragma unroll 1
+        for (int ps = 0; ps < G; ++ps) {
+            const int t = ps * RP + rl;  // this lane's row of the slice
+            const int row = rows[(size_t)sl * 32 + t];
+            int e = o0 + t;
+            TA acc[CS];
+#pragma unroll
+            for (int c = 0; c < CS; ++c) acc[c] = TA(0);
+            double a[R];
+            int col[R];
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                const int k = e + 32 * u;
+                a[u] = k < e1 ? v[k] : 0.0;
+                col[u] = k < e1 ? ci[k] : -1;
+            }
+            while (e < e1) {  // a slice's entry count is a multiple of 32: warp-uniform
+                double an[R];
+                int cn[R];
+#pragma unroll
+                for (int u = 0; u < R; ++u) {
+                    const int k = e + 32 * R + 32 * u;
+                    an[u] = k < e1 ? v[k] : 0.0;
+                    cn[u] = k < e1 ? ci[k] : -1;
+                }
+#pragma unroll
+                for (int u = 0; u < R; ++u) {
+                    if (col[u] >= 0) {
+                        TX xv[CS];
+                        if constexpr (MODE == MV_TWO)  // columns past the row count read the b slot
+                            load_row<CS>(col[u] < n ? x + (size_t)col[u] * NV + cg * CS
+                                                    : reinterpret_cast<const TX*>(b) + (size_t)(col[u] - n) * NV +
+                                                          cg * CS,
+                                         xv);
+                        else
+                            load_row<CS>(x + (size_t)col[u] * NV + cg * CS, xv);
+#pragma unroll
+                        for (int c = 0; c < CS; ++c) acc[c] += (TA)a[u] * (TA)xv[c];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < R; ++u) {
+                    a[u] = an[u];
+                    col[u] = cn[u];
+                }
+                e += 32 * R;
+            }
+            if (row >= 0) {
+                const size_t base = (size_t)row * NV + cg * CS;
+#pragma unroll
+                for (int c = 0; c < CS; ++c) {
+                    const TY ac = (TY)acc[c];
+                    if constexpr (MODE == MV_AX || MODE == MV_TWO) {
+                        y[base + c] = ac;
+                    } else if constexpr (MODE == MV_RES) {
+                        y[base + c] = b[base + c] - ac;
+                    } else if constexpr (MODE == MV_ADD) {
+                        y[base + c] += w * ac;
+                    } else {
+                        const TY r = b[base + c] - ac;
+                        const TY xo = (TY)x[base + c];
+                        y[base + c] = RECIP ? xo + r * d[row] : xo + r / d[row];
+                    }
+                }
+            }
+        }
+    }
+}
+
 // Three-stage form of the one-slice product (NV <= 2): in each round the
 // values and columns of round j+2 are loaded and the x entries of round j+1
 // gathered before the products of round j are summed, so the gather no longer
@@ -1159,10 +1253,13 @@ constexpr int kShapes = 10;
 constexpr int kUnrollMinRows = 65536;
 // sliced-ELL launch shapes: steps per round R (2, 4, 8), | kSellPair for two
 // slices per warp (R = 2, 4), | kSellDeep for the three-stage form (R = 2, 4;
-// one or two columns)
+// one or two columns), | kSellCols for the column-split form (R = 4, 8; four
+// or eight columns)
 constexpr int kSellPair = 16;
 constexpr int kSellDeep = 32;
-constexpr int kSellShapes[] = {2, 4, 8, kSellPair | 2, kSellPair | 4, kSellDeep | 2, kSellDeep | 4};
+constexpr int kSellCols = 64;  // the column-split form (R = 4, 8; four or eight columns)
+constexpr int kSellShapes[] = {2, 4, 8, kSellPair | 2, kSellPair | 4, kSellDeep | 2, kSellDeep | 4,
+                               kSellCols | 4, kSellCols | 8};
 
 template <typename TV, typename TX, typename TY, int NV, int MODE, bool RECIP>
 static void launch_mv(int lanes, int u, int grid, cudaStream_t s, int n, const int* rp, const int* ci, const TV* v,
@@ -1208,7 +1305,17 @@ static void launch_sell(const DevSell& S, int shape, cudaStream_t s, const TX* x
             return;
         }
     }
-    shape &= ~kSellDeep;  // (the three-stage form is built for NV <= 2 only)
+    if constexpr (NV == 4 || NV == 8) {
+        if (shape == (kSellCols | 4)) {
+            launch_k(k_sell_spmv_cs<TX, TY, NV, MODE, RECIP, 4>, SSV_SELL_ARGS);
+            return;
+        }
+        if (shape == (kSellCols | 8)) {
+            launch_k(k_sell_spmv_cs<TX, TY, NV, MODE, RECIP, 8>, SSV_SELL_ARGS);
+            return;
+        }
+    }
+    shape &= ~(kSellDeep | kSellCols);  // (the three-stage and column-split forms exist for some NV only)
     if (shape == (kSellPair | 2)) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 2, 2>, SSV_SELL_ARGS);
     else if (shape == (kSellPair | 4)) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 4, 2>, SSV_SELL_ARGS);
     else if (shape == 2) launch_k(k_sell_spmv<TX, TY, NV, MODE, RECIP, 2>, SSV_SELL_ARGS);
@@ -2006,6 +2113,7 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
             for (int R : kSellShapes) {
                 if (sell_shape_forced() && R != sell_shape_forced()) continue;
                 if ((R & kSellDeep) && NV > 2) continue;
+                if ((R & kSellCols) && NV != 4 && NV != 8) continue;
                 auto launch = [&] {
                     if (two)
                         launch_sell<TX, TY, NV, MV_TWO, false>(A.sell, R, s, x, y, b, nullptr, TY(0), nullptr);
@@ -2040,7 +2148,10 @@ static void tune_csr(DevCsr& A, const TX* x, TY* y, const TY* b, cudaStream_t s,
                      (long long)A.nnz, NV, cold ? "cold" : "warm", pick, pick_u, 1e3 * best / (cold ? 5 : 4));
         if (sell_pick)
             std::fprintf(stderr, "; sliced-ELL %d steps/round%s %.2f us%s", sell_pick & 15,
-                         (sell_pick & kSellPair) ? " two slices/warp" : (sell_pick & kSellDeep) ? " three-stage" : "",
+                         (sell_pick & kSellPair)   ? " two slices/warp"
+                         : (sell_pick & kSellDeep) ? " three-stage"
+                         : (sell_pick & kSellCols) ? " column-split"
+                                                   : "",
                          1e3 * sell_best / (cold ? 5 : 4),
                          A.tuned_sell[slot] ? " -> sliced-ELL" : "");
         std::fprintf(stderr, "\n");

@@ -91,6 +91,7 @@ for prec in ("fp64", "fp32"):
     p = ss.CompactAMSPreconditioner(d["A"], d["G"], freedofs=d["freedofs"], coord_x=d["coords"][0],
                                     coord_y=d["coords"][1], coord_z=d["coords"][2], precision=prec)
     out["mag_" + prec] = p * rng.standard_normal(d["A"].shape[0])
+    out["mag_block_" + prec] = p.MultBlock(rng.standard_normal((4, d["A"].shape[0])))  # four columns
 inv = ss.PCGSolver(d["A"], p, freedofs=d["freedofs"], maxiter=500, tol=1e-10)
 x = np.zeros(d["A"].shape[0])
 inv.Solve(d["f"], x)
@@ -100,14 +101,16 @@ p = ss.ComplexCompactAMSPreconditioner(e["a_real"], e["G"], freedofs=e["freedofs
                                        coord_y=e["coords"][1], coord_z=e["coords"][2])
 n = e["A"].shape[0]
 out["eddy"] = p * (rng.standard_normal(n) + 1j * rng.standard_normal(n))
+out["eddy_block"] = p.MultBlock(rng.standard_normal((4, n)) + 1j * rng.standard_normal((4, n)))  # eight columns
 np.savez(sys.argv[1], **out)
 """
 
 
 def test_sell_shapes_bitwise_equal(tmp_path):
     """Every sliced-ELL launch shape (2, 4 or 8 steps per round; two slices
-    per warp, or the three-stage form, at 2 and 4 steps) sums each row in its
-    CSR column order, so the
+    per warp, or the three-stage form, at 2 and 4 steps; the column-split form
+    of four- and eight-column block applies at 4 and 8 steps) sums each row in
+    its CSR column order, so the
     applies and a PCG solve are bitwise the same whichever shape runs. The
     first child records the tuner's choices; the others replay them with every
     sliced-ELL choice replaced by one shape."""
@@ -125,7 +128,7 @@ def test_sell_shapes_bitwise_equal(tmp_path):
     base = run(tmp_path / "base.npz", SSV_AMS_TUNE_SAVE=str(rec))
     lines = rec.read_text().splitlines()
     assert any(ln.startswith("csr") and ln.split()[6] != "0" for ln in lines), lines
-    for shape in (2, 8, 16 | 2, 16 | 4, 32 | 2, 32 | 4):
+    for shape in (2, 8, 16 | 2, 16 | 4, 32 | 2, 32 | 4, 64 | 4, 64 | 8):
         forced = tmp_path / f"tune_{shape}.txt"
         forced.write_text("\n".join(
             " ".join(f[:6] + [str(shape)]) if f[0] == "csr" and f[6] != "0" else " ".join(f)
